@@ -1,0 +1,189 @@
+"""ctypes mirrors of the records in include/bf200.h.
+
+These are the same byte layouts the C ABI declares; `check_layouts()` asserts the sizes the
+header's static assertions expect so a drift between the two is caught on the CPU.
+"""
+import ctypes as C
+
+u32, u64, f32, f64 = C.c_uint32, C.c_uint64, C.c_float, C.c_double
+
+BLACKFRAME_STATUS = {
+    0: "SUCCESS", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED_ABI", 3: "INTERFACE_NOT_FOUND",
+    4: "INVALID_STATE", 5: "OUT_OF_RANGE", 6: "EXTENSION_FAILURE",
+}
+
+CLOSURE_LAMBERTIAN = 1
+CLOSURE_ROUGH_CONDUCTOR = 3
+CLOSURE_ROUGH_DIELECTRIC = 4
+
+LOBE_DIFFUSE, LOBE_GLOSSY, LOBE_SPECULAR = 0x01, 0x02, 0x04
+LOBE_REFLECTION, LOBE_TRANSMISSION, LOBE_VOLUME = 0x08, 0x10, 0x20
+
+TERMINATIONS = ["escaped_environment", "depth_limit", "outside_bsdf_support",
+                "zero_throughput", "russian_roulette"]
+
+
+class InterfaceId(C.Structure):
+    _fields_ = [("high", u64), ("low", u64)]
+
+
+class Utf8View(C.Structure):
+    _fields_ = [("data", C.c_char_p), ("size", u32), ("reserved", u32)]
+
+
+class ExtensionQuery(C.Structure):
+    _fields_ = [("struct_size", u32), ("abi_major", u32), ("abi_minor", u32), ("reserved", u32)]
+
+
+GetInterfaceFn = C.CFUNCTYPE(u32, C.c_void_p, InterfaceId, u32, u32, C.c_void_p, u32)
+ShutdownFn = C.CFUNCTYPE(None, C.c_void_p)
+
+
+class ExtensionApi(C.Structure):
+    _fields_ = [("struct_size", u32), ("abi_major", u32), ("abi_minor", u32), ("reserved", u32),
+                ("extension_context", C.c_void_p), ("get_interface", GetInterfaceFn),
+                ("shutdown", ShutdownFn)]
+
+
+class XpuDeviceDescriptor(C.Structure):
+    _fields_ = [("struct_size", u32), ("kind", u32), ("identifier_high", u64),
+                ("identifier_low", u64), ("name", Utf8View), ("vendor", Utf8View),
+                ("reserved", u64 * 4)]
+
+
+GetDeviceCountFn = C.CFUNCTYPE(u32, C.c_void_p, C.POINTER(u32))
+GetDeviceDescriptorFn = C.CFUNCTYPE(u32, C.c_void_p, u32, C.POINTER(XpuDeviceDescriptor))
+
+
+class XpuBackendApi(C.Structure):
+    _fields_ = [("struct_size", u32), ("abi_major", u32), ("abi_minor", u32), ("reserved", u32),
+                ("backend_context", C.c_void_p), ("backend_name", Utf8View),
+                ("get_device_count", GetDeviceCountFn),
+                ("get_device_descriptor", GetDeviceDescriptorFn),
+                ("reserved_slots", u64 * 4)]
+
+
+class Closure(C.Structure):
+    _fields_ = [("kind", u32), ("lobes", u32), ("weight", f32 * 4), ("parameters", f32 * 10)]
+
+
+class Material(C.Structure):
+    _fields_ = [("material_id", u32), ("closure_offset", u32), ("closure_count", u32),
+                ("frame_mode", u32), ("tangent_rotation_radians", f32),
+                ("component_probabilities", f32 * 8), ("emitted_radiance", f32 * 4),
+                ("reserved", u32 * 3)]
+
+
+class Geometry(C.Structure):
+    _fields_ = [("geometry_id", u32), ("vertex_offset", u32), ("vertex_count", u32),
+                ("triangle_offset", u32), ("triangle_count", u32), ("reserved", u32 * 3)]
+
+
+class Instance(C.Structure):
+    _fields_ = [("instance_id", u32), ("object_id", u32), ("geometry_index", u32),
+                ("material_index", u32), ("visibility_mask", u32), ("reserved", u32 * 3),
+                ("object_to_world", f32 * 16), ("world_to_object", f32 * 16)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("struct_size", u32), ("geometry_count", u32), ("vertex_count", u32),
+                ("triangle_count", u32), ("material_count", u32), ("closure_count", u32),
+                ("instance_count", u32), ("punctual_light_count", u32),
+                ("geometries", C.POINTER(Geometry)), ("positions", C.POINTER(f32)),
+                ("normals", C.POINTER(f32)), ("texture_coordinates", C.POINTER(f32)),
+                ("triangles", C.POINTER(u32)), ("materials", C.POINTER(Material)),
+                ("closures", C.POINTER(Closure)), ("instances", C.POINTER(Instance)),
+                ("wavelength_nanometers", f32 * 4), ("wavelength_pdf", f32 * 4),
+                ("environment_radiance", f32 * 4), ("reserved", u32 * 4)]
+
+
+class Ray(C.Structure):
+    _fields_ = [("origin", f32 * 3), ("direction", f32 * 3), ("t_min", f32), ("t_max", f32),
+                ("time", f32), ("mask", u32), ("medium", u32), ("reserved", u32)]
+
+
+class SampleIndex(C.Structure):
+    _fields_ = [("pixel_x", u32), ("pixel_y", u32), ("sample_index", u64), ("seed", u64)]
+
+
+class PathInput(C.Structure):
+    _fields_ = [("primary_ray", Ray), ("sample", SampleIndex), ("reserved", u64)]
+
+
+class PathResult(C.Structure):
+    _fields_ = [("beta", f32 * 4), ("radiance", f32 * 4), ("depth", u32),
+                ("depth_counters", u32 * 5), ("eta_scale", f32), ("delta_flags", u32),
+                ("termination", u32), ("blocked_depth_limits", u32), ("lane_status", u32),
+                ("segments", u32), ("terminal_ray", Ray)]
+
+
+class TransportOptions(C.Structure):
+    _fields_ = [("struct_size", u32), ("mis_heuristic", u32), ("depth_limits", u32 * 5),
+                ("roulette_enabled", u32), ("roulette_first_eligible_depth", u32),
+                ("roulette_minimum_survival", f32), ("roulette_maximum_survival", f32),
+                ("reserved", u32 * 5)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("origin", f32 * 3), ("tangent", f32 * 3), ("bitangent", f32 * 3),
+                ("normal", f32 * 3), ("half_width", f32), ("half_height", f32), ("t_min", f32),
+                ("t_max", f32), ("time", f32), ("mask", u32), ("width", u32), ("height", u32),
+                ("jitter_mode", u32), ("reserved", u32)]
+
+
+class Sensor(C.Structure):
+    _fields_ = [("response_xyz", (f32 * 3) * 4), ("wavelength_pdf", f32 * 4),
+                ("normalization", f32), ("reserved", u32 * 3)]
+
+
+class FilmRequest(C.Structure):
+    _fields_ = [("struct_size", u32), ("samples_per_pixel", u32), ("first_sample", u64),
+                ("seed", u64), ("precision", u32), ("reserved", u32 * 3)]
+
+
+class Film(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("precision", u32), ("reserved", u32),
+                ("sums", C.c_void_p), ("sample_counts", C.POINTER(u64))]
+
+
+class Report(C.Structure):
+    _fields_ = [("struct_size", u32), ("registered_light_count", u32), ("path_count", u64),
+                ("extension_segments", u64), ("shadow_segments", u64),
+                ("closure_samples", u64), ("light_samples", u64), ("terminated_paths", u64),
+                ("failed_lanes", u64), ("first_failure_status", u32),
+                ("first_failure_path", u32), ("kernel_launches", u64),
+                ("gpu_milliseconds", f64), ("reserved", u64 * 4)]
+
+
+class Hit(C.Structure):
+    _fields_ = [("t", f32), ("barycentrics", f32 * 3), ("instance_index", u32),
+                ("primitive_index", u32), ("status", u32), ("reserved", u32)]
+
+
+EXPECTED_SIZES = {
+    Closure: 64, Material: 80, Geometry: 32, Instance: 160, Ray: 48, SampleIndex: 24,
+    PathInput: 80, PathResult: 128, TransportOptions: 64, Camera: 88, Sensor: 80,
+    FilmRequest: 40, Report: 120, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
+}
+
+
+def check_layouts():
+    for record, size in EXPECTED_SIZES.items():
+        actual = C.sizeof(record)
+        if actual != size:
+            raise AssertionError(f"{record.__name__}: {actual} bytes, header expects {size}")
+
+
+def default_options(mis="balance", max_depth=8, roulette=True, first_eligible=3,
+                    minimum_survival=0.05, maximum_survival=0.95):
+    options = TransportOptions()
+    options.struct_size = C.sizeof(TransportOptions)
+    options.mis_heuristic = 1 if mis == "power" else 0
+    for lane in range(4):
+        options.depth_limits[lane] = max_depth
+    options.depth_limits[4] = 0
+    options.roulette_enabled = 1 if roulette else 0
+    options.roulette_first_eligible_depth = first_eligible if roulette else 0
+    options.roulette_minimum_survival = minimum_survival if roulette else 0.0
+    options.roulette_maximum_survival = maximum_survival if roulette else 0.0
+    return options

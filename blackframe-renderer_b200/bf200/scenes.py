@@ -1,0 +1,434 @@
+"""Seeded synthetic scenes for the Cornell-box workloads, flattened to bf200 scene records.
+
+A scene here is what a Blackframe caller hands the backend after FrameScene::create: triangle
+meshes, one spectral material per closure mixture (resolved at the frame's single four-lane
+wavelength packet), root instances in identifier order with their object_to_world matrix and
+its inverse, and a constant environment. The inverse is computed with the same Gauss-Jordan
+elimination, in float32, that FrameScene uses (Blackframe/Renderer/Include/Blackframe/
+Renderer/MatrixOperations.hpp:30-94), so the records are bit-identical to the committed scene.
+
+Workloads (scene geometry and transport settings):
+  cornell_plain   : unit box, 5 Lambert walls, two rotated Lambert cuboids, 0.25 x 0.25 emitter
+                    with radiance 17, balance MIS, depth 8, Russian roulette from depth 3.
+  cornell_spheres : the same box plus a GGX conductor sphere (gold-like eta/k, alpha 0.2) and a
+                    GGX rough dielectric sphere (eta 1.5, alpha 0.05), both 64 x 32 UV spheres;
+                    power MIS, depth 16.
+"""
+import ctypes as C
+import math
+import struct
+from fractions import Fraction
+
+import numpy as np
+
+from . import abi
+
+F32 = np.float32
+
+
+# ------------------------------------------------------------------------------------------------
+# float32 helpers with the reference's rounding
+# ------------------------------------------------------------------------------------------------
+
+def f32_round(value):
+    """Round an exact rational (or float) to the nearest float32, ties to even."""
+    if isinstance(value, float):
+        value = Fraction(value)
+    if value == 0:
+        return F32(0.0)
+    # Python's float() of a Fraction is correctly rounded to double; then widen the check.
+    candidate = F32(float(value))
+    exact_candidate = Fraction(float(candidate))
+    if exact_candidate == value:
+        return candidate
+    below = candidate if exact_candidate < value else np.nextafter(candidate, F32(-np.inf))
+    above = np.nextafter(below, F32(np.inf))
+    distance_below = value - Fraction(float(below))
+    distance_above = Fraction(float(above)) - value
+    if distance_below < distance_above:
+        return F32(below)
+    if distance_above < distance_below:
+        return F32(above)
+    bits = struct.unpack("<I", struct.pack("<f", float(below)))[0]
+    return F32(below) if bits % 2 == 0 else F32(above)
+
+
+def f32_fma(a, b, c):
+    """std::fma on float32 operands: one rounding of a*b + c."""
+    return f32_round(Fraction(float(a)) * Fraction(float(b)) + Fraction(float(c)))
+
+
+def sample_uniform_visible_wavelengths(unit_sample):
+    """WavelengthSampling.hpp:61-88: four circularly stratified lanes over 360-830 nm."""
+    u = F32(unit_sample)
+    nanometers, pdfs = [], []
+    pdf = F32(1.0) / F32(470.0)
+    for lane in range(4):
+        offset = F32(lane) / F32(4.0)
+        wrap_threshold = F32(1.0) - offset
+        if lane != 0 and u >= wrap_threshold:
+            shifted = F32(u - wrap_threshold)
+        else:
+            shifted = F32(u + offset)
+        nanometers.append(f32_fma(F32(470.0), shifted, F32(360.0)))
+        pdfs.append(pdf)
+    return nanometers, pdfs
+
+
+def tabulated_spectrum(table, nanometers):
+    """Resolve a piecewise-linear reflectance table [(nm, value), ...] at the packet lanes."""
+    xs = [p[0] for p in table]
+    ys = [p[1] for p in table]
+    return [F32(np.interp(float(nm), xs, ys)) for nm in nanometers]
+
+
+# ------------------------------------------------------------------------------------------------
+# affine transforms in float32
+# ------------------------------------------------------------------------------------------------
+
+def identity():
+    return np.eye(4, dtype=F32)
+
+
+def affine_inverse(matrix):
+    """MatrixOperations.hpp:30-94: partial-pivot Gauss-Jordan on [M | I] in float32."""
+    augmented = np.zeros((4, 8), dtype=F32)
+    augmented[:, :4] = matrix
+    augmented[:, 4:] = np.eye(4, dtype=F32)
+    for pivot_column in range(4):
+        pivot_row = pivot_column
+        pivot_magnitude = abs(augmented[pivot_row, pivot_column])
+        for candidate in range(pivot_column + 1, 4):
+            magnitude = abs(augmented[candidate, pivot_column])
+            if magnitude > pivot_magnitude:
+                pivot_magnitude = magnitude
+                pivot_row = candidate
+        if pivot_magnitude == 0:
+            raise ValueError("A singular matrix has no inverse.")
+        if pivot_row != pivot_column:
+            augmented[[pivot_column, pivot_row]] = augmented[[pivot_row, pivot_column]]
+        pivot = F32(augmented[pivot_column, pivot_column])
+        for column in range(8):
+            augmented[pivot_column, column] = F32(augmented[pivot_column, column] / pivot)
+        for row in range(4):
+            if row == pivot_column:
+                continue
+            factor = F32(augmented[row, pivot_column])
+            for column in range(8):
+                product = F32(factor * augmented[pivot_column, column])
+                augmented[row, column] = F32(augmented[row, column] - product)
+    result = augmented[:, 4:].copy()
+    if not np.all(np.isfinite(result)):
+        raise ValueError("Matrix inversion produced a non-finite result.")
+    return result
+
+
+def rotation_y_scale_translate(angle_degrees, scale, translation):
+    """object_to_world = T * R_y * S, entries rounded to float32 once each."""
+    angle = math.radians(angle_degrees)
+    c, s = math.cos(angle), math.sin(angle)
+    sx, sy, sz = scale
+    m = np.zeros((4, 4), dtype=np.float64)
+    m[0, 0], m[0, 1], m[0, 2] = c * sx, 0.0, s * sz
+    m[1, 0], m[1, 1], m[1, 2] = 0.0, sy, 0.0
+    m[2, 0], m[2, 1], m[2, 2] = -s * sx, 0.0, c * sz
+    m[0, 3], m[1, 3], m[2, 3] = translation
+    m[3, 3] = 1.0
+    return m.astype(F32)
+
+
+def uniform_scale_translate(radius, center):
+    m = identity()
+    m[0, 0] = m[1, 1] = m[2, 2] = F32(radius)
+    m[0, 3], m[1, 3], m[2, 3] = (F32(v) for v in center)
+    return m
+
+
+# ------------------------------------------------------------------------------------------------
+# meshes
+# ------------------------------------------------------------------------------------------------
+
+class Mesh:
+    def __init__(self, positions, normals, uvs, triangles):
+        self.positions = np.asarray(positions, dtype=F32).reshape(-1, 3)
+        self.normals = np.asarray(normals, dtype=F32).reshape(-1, 3)
+        self.uvs = np.asarray(uvs, dtype=F32).reshape(-1, 2)
+        self.triangles = np.asarray(triangles, dtype=np.uint32).reshape(-1, 3)
+
+
+def quad(corners, normal):
+    """Two triangles (0,1,2), (0,2,3) with one normal and unit-square UVs."""
+    return Mesh(corners, [normal] * 4, [(0, 0), (1, 0), (1, 1), (0, 1)], [(0, 1, 2), (0, 2, 3)])
+
+
+def unit_box():
+    """Axis-aligned cube [-0.5, 0.5]^3: 6 faces x 4 vertices, flat normals, 12 triangles."""
+    faces = [
+        ((1, 0, 0), [(0.5, -0.5, -0.5), (0.5, 0.5, -0.5), (0.5, 0.5, 0.5), (0.5, -0.5, 0.5)]),
+        ((-1, 0, 0), [(-0.5, -0.5, -0.5), (-0.5, -0.5, 0.5), (-0.5, 0.5, 0.5), (-0.5, 0.5, -0.5)]),
+        ((0, 1, 0), [(-0.5, 0.5, -0.5), (-0.5, 0.5, 0.5), (0.5, 0.5, 0.5), (0.5, 0.5, -0.5)]),
+        ((0, -1, 0), [(-0.5, -0.5, -0.5), (0.5, -0.5, -0.5), (0.5, -0.5, 0.5), (-0.5, -0.5, 0.5)]),
+        ((0, 0, 1), [(-0.5, -0.5, 0.5), (0.5, -0.5, 0.5), (0.5, 0.5, 0.5), (-0.5, 0.5, 0.5)]),
+        ((0, 0, -1), [(-0.5, -0.5, -0.5), (-0.5, 0.5, -0.5), (0.5, 0.5, -0.5), (0.5, -0.5, -0.5)]),
+    ]
+    positions, normals, uvs, triangles = [], [], [], []
+    for normal, corners in faces:
+        base = len(positions)
+        positions.extend(corners)
+        normals.extend([normal] * 4)
+        uvs.extend([(0, 0), (1, 0), (1, 1), (0, 1)])
+        triangles.extend([(base, base + 1, base + 2), (base, base + 2, base + 3)])
+    return Mesh(positions, normals, uvs, triangles)
+
+
+def uv_sphere(longitude=64, latitude=32):
+    """Unit UV sphere with poles on +-Y, (latitude-1) rings of longitude+1 vertices.
+
+    Same construction as the reference's tessellated test sphere
+    (Tests/Backends/CPU/Embree/CornellWavefrontScene.hpp:110-180): 2*longitude*(latitude-1)
+    triangles; sin/cos evaluated in float32 arithmetic on float32 angles.
+    """
+    stride = longitude + 1
+    positions, normals, uvs, triangles = [(0, 1, 0)], [(0, 1, 0)], [(0.5, 0)], []
+    pi = F32(math.pi)
+    for lat in range(1, latitude):
+        v = F32(lat) / F32(latitude)
+        theta = F32(pi * v)
+        sin_t, cos_t = F32(math.sin(theta)), F32(math.cos(theta))
+        for lon in range(longitude + 1):
+            u = F32(lon) / F32(longitude)
+            phi = F32(F32(F32(2.0) * pi) * u)
+            # cos/sin of the float angle leave residues like cos(pi/2) = -4.4e-8 where the
+            # exact value is zero; they are snapped to zero so the scalar oracle's exact
+            # float-expansion arithmetic does not underflow on them.
+            cos_phi, sin_phi = F32(math.cos(phi)), F32(math.sin(phi))
+            cos_phi = F32(0.0) if abs(cos_phi) < 1e-6 else cos_phi
+            sin_phi = F32(0.0) if abs(sin_phi) < 1e-6 else sin_phi
+            x = F32(sin_t * cos_phi)
+            z = F32(sin_t * sin_phi)
+            positions.append((x, cos_t, z))
+            normals.append((x, cos_t, z))
+            uvs.append((u, v))
+    bottom = len(positions)
+    positions.append((0, -1, 0))
+    normals.append((0, -1, 0))
+    uvs.append((0.5, 1))
+    first = 1
+    for lon in range(longitude):
+        triangles.append((0, first + lon + 1, first + lon))
+    for lat in range(1, latitude - 1):
+        upper_ring = 1 + (lat - 1) * stride
+        lower_ring = upper_ring + stride
+        for lon in range(longitude):
+            upper, lower = upper_ring + lon, lower_ring + lon
+            triangles.append((upper, lower + 1, lower))
+            triangles.append((upper, upper + 1, lower + 1))
+    last = bottom - stride
+    for lon in range(longitude):
+        triangles.append((bottom, last + lon, last + lon + 1))
+    return Mesh(positions, normals, uvs, triangles)
+
+
+# ------------------------------------------------------------------------------------------------
+# scene assembly
+# ------------------------------------------------------------------------------------------------
+
+def lambertian(reflectance):
+    return [(abi.CLOSURE_LAMBERTIAN, abi.LOBE_DIFFUSE | abi.LOBE_REFLECTION,
+             [F32(v) for v in reflectance], [0.0] * 10)]
+
+
+def rough_conductor(coefficient, eta, k, alpha_x, alpha_y):
+    params = list(eta) + list(k) + [alpha_x, alpha_y]
+    return [(abi.CLOSURE_ROUGH_CONDUCTOR, abi.LOBE_GLOSSY | abi.LOBE_REFLECTION,
+             [F32(v) for v in coefficient], [F32(v) for v in params])]
+
+
+def rough_dielectric(coefficient, exterior_eta, interior_eta, alpha_x, alpha_y):
+    params = [exterior_eta, interior_eta, alpha_x, alpha_y] + [0.0] * 6
+    return [(abi.CLOSURE_ROUGH_DIELECTRIC,
+             abi.LOBE_GLOSSY | abi.LOBE_REFLECTION | abi.LOBE_TRANSMISSION,
+             [F32(v) for v in coefficient], [F32(v) for v in params])]
+
+
+class SceneBuilder:
+    """Accumulates meshes, materials and root instances; `desc()` returns a SceneDesc whose
+    arrays stay alive as long as the builder does."""
+
+    def __init__(self, wavelength_sample=0.1, environment=(0.0, 0.0, 0.0, 0.0)):
+        self.nanometers, self.pdfs = sample_uniform_visible_wavelengths(wavelength_sample)
+        self.environment = [F32(v) for v in environment]
+        self.meshes, self.materials, self.instances = [], [], []
+
+    def add_mesh(self, mesh):
+        self.meshes.append(mesh)
+        return len(self.meshes) - 1
+
+    def add_material(self, closures, emission=(0.0, 0.0, 0.0, 0.0), frame_mode=0):
+        self.materials.append((closures, [F32(v) for v in emission], frame_mode))
+        return len(self.materials) - 1
+
+    def add_instance(self, mesh_index, material_index, object_to_world=None, mask=0xFFFFFFFF):
+        matrix = identity() if object_to_world is None else np.asarray(object_to_world, F32)
+        self.instances.append((mesh_index, material_index, matrix, mask))
+        return len(self.instances) - 1
+
+    @property
+    def triangle_count(self):
+        return sum(len(m.triangles) for m in self.meshes)
+
+    def desc(self):
+        geometries = (abi.Geometry * len(self.meshes))()
+        positions, normals, uvs, triangles = [], [], [], []
+        vertex_offset = triangle_offset = 0
+        for index, mesh in enumerate(self.meshes):
+            g = geometries[index]
+            g.geometry_id = 100 + index
+            g.vertex_offset, g.vertex_count = vertex_offset, len(mesh.positions)
+            g.triangle_offset, g.triangle_count = triangle_offset, len(mesh.triangles)
+            positions.append(mesh.positions)
+            normals.append(mesh.normals)
+            uvs.append(mesh.uvs)
+            triangles.append(mesh.triangles)
+            vertex_offset += len(mesh.positions)
+            triangle_offset += len(mesh.triangles)
+        self._positions = np.ascontiguousarray(np.concatenate(positions), F32)
+        self._normals = np.ascontiguousarray(np.concatenate(normals), F32)
+        self._uvs = np.ascontiguousarray(np.concatenate(uvs), F32)
+        self._triangles = np.ascontiguousarray(np.concatenate(triangles), np.uint32)
+
+        closure_records = []
+        materials = (abi.Material * len(self.materials))()
+        for index, (closures, emission, frame_mode) in enumerate(self.materials):
+            m = materials[index]
+            m.material_id = 200 + index
+            m.closure_offset, m.closure_count = len(closure_records), len(closures)
+            m.frame_mode = frame_mode
+            m.tangent_rotation_radians = 0.0
+            for c in range(len(closures)):
+                m.component_probabilities[c] = 1.0 / len(closures)
+            for lane in range(4):
+                m.emitted_radiance[lane] = emission[lane]
+            closure_records.extend(closures)
+        closures = (abi.Closure * max(1, len(closure_records)))()
+        for index, (kind, lobes, weight, params) in enumerate(closure_records):
+            closures[index].kind, closures[index].lobes = kind, lobes
+            for lane in range(4):
+                closures[index].weight[lane] = weight[lane]
+            for p in range(10):
+                closures[index].parameters[p] = params[p]
+
+        instances = (abi.Instance * len(self.instances))()
+        for index, (mesh_index, material_index, matrix, mask) in enumerate(self.instances):
+            inst = instances[index]
+            inst.instance_id = 300 + index
+            inst.object_id = 400 + index
+            inst.geometry_index, inst.material_index = mesh_index, material_index
+            inst.visibility_mask = mask
+            inverse = affine_inverse(matrix)
+            for e in range(16):
+                inst.object_to_world[e] = matrix.flat[e]
+                inst.world_to_object[e] = inverse.flat[e]
+
+        desc = abi.SceneDesc()
+        desc.struct_size = C.sizeof(abi.SceneDesc)
+        desc.geometry_count = len(self.meshes)
+        desc.vertex_count = len(self._positions)
+        desc.triangle_count = len(self._triangles)
+        desc.material_count = len(self.materials)
+        desc.closure_count = len(closure_records)
+        desc.instance_count = len(self.instances)
+        desc.geometries = geometries
+        desc.positions = self._positions.ctypes.data_as(C.POINTER(abi.f32))
+        desc.normals = self._normals.ctypes.data_as(C.POINTER(abi.f32))
+        desc.texture_coordinates = self._uvs.ctypes.data_as(C.POINTER(abi.f32))
+        desc.triangles = self._triangles.ctypes.data_as(C.POINTER(abi.u32))
+        desc.materials = materials
+        desc.closures = closures
+        desc.instances = instances
+        for lane in range(4):
+            desc.wavelength_nanometers[lane] = self.nanometers[lane]
+            desc.wavelength_pdf[lane] = self.pdfs[lane]
+            desc.environment_radiance[lane] = self.environment[lane]
+        self._keep = (geometries, materials, closures, instances)
+        return desc
+
+
+RED_WALL = [(360, 0.05), (560, 0.06), (600, 0.35), (640, 0.60), (830, 0.62)]
+GREEN_WALL = [(360, 0.08), (470, 0.15), (530, 0.55), (580, 0.45), (640, 0.10), (830, 0.08)]
+# Gold-like relative IOR (eta, k) tables; resolved at the packet lanes.
+GOLD_ETA = [(360, 1.5), (450, 1.3), (500, 0.9), (550, 0.40), (600, 0.25), (700, 0.16),
+            (830, 0.19)]
+GOLD_K = [(360, 1.9), (450, 1.85), (500, 1.85), (550, 2.3), (600, 2.9), (700, 3.9), (830, 5.3)]
+
+
+def cornell_box(builder, with_spheres):
+    """Walls, emitter and cuboids of the Cornell workloads; spheres when `with_spheres`."""
+    nm = builder.nanometers
+    white = builder.add_material(lambertian([0.73] * 4))
+    red = builder.add_material(lambertian(tabulated_spectrum(RED_WALL, nm)))
+    green = builder.add_material(lambertian(tabulated_spectrum(GREEN_WALL, nm)))
+    light = builder.add_material(lambertian([0.0] * 4), emission=(17.0, 17.0, 17.0, 17.0))
+
+    floor = builder.add_mesh(quad([(-1, -1, 0), (-1, -1, 2), (1, -1, 2), (1, -1, 0)], (0, 1, 0)))
+    ceiling = builder.add_mesh(quad([(-1, 1, 0), (1, 1, 0), (1, 1, 2), (-1, 1, 2)], (0, -1, 0)))
+    back = builder.add_mesh(quad([(-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0)], (0, 0, 1)))
+    left = builder.add_mesh(quad([(-1, -1, 0), (-1, 1, 0), (-1, 1, 2), (-1, -1, 2)], (1, 0, 0)))
+    right = builder.add_mesh(quad([(1, -1, 0), (1, -1, 2), (1, 1, 2), (1, 1, 0)], (-1, 0, 0)))
+    emitter = builder.add_mesh(quad([(-0.125, 0.985, 0.875), (0.125, 0.985, 0.875),
+                                     (0.125, 0.985, 1.125), (-0.125, 0.985, 1.125)],
+                                    (0, -1, 0)))
+    box = builder.add_mesh(unit_box())
+
+    builder.add_instance(floor, white)
+    builder.add_instance(ceiling, white)
+    builder.add_instance(back, white)
+    builder.add_instance(left, red)
+    builder.add_instance(right, green)
+    builder.add_instance(emitter, light)
+    builder.add_instance(box, white, rotation_y_scale_translate(18.0, (0.6, 1.2, 0.6),
+                                                               (-0.35, -0.4, 0.65)))
+    builder.add_instance(box, white, rotation_y_scale_translate(-15.0, (0.6, 0.6, 0.6),
+                                                               (0.4, -0.7, 1.25)))
+    if with_spheres:
+        sphere = builder.add_mesh(uv_sphere())
+        conductor = builder.add_material(rough_conductor(
+            [1.0] * 4, tabulated_spectrum(GOLD_ETA, nm), tabulated_spectrum(GOLD_K, nm), 0.2, 0.2))
+        dielectric = builder.add_material(rough_dielectric([1.0] * 4, 1.0, 1.5, 0.05, 0.05))
+        builder.add_instance(sphere, conductor, uniform_scale_translate(0.25, (0.4, -0.15, 1.25)))
+        builder.add_instance(sphere, dielectric,
+                             uniform_scale_translate(0.25, (-0.3, -0.75, 1.55)))
+    return builder
+
+
+CAMERA_ORIGIN = (0.0, 0.0, 4.0)
+CAMERA_TARGET = (0.0, -0.05, 0.92)
+CAMERA_VFOV = 0.70
+PATH_TIME = 0.5
+
+
+def camera_frame_inputs():
+    """Camera frame seed of the Cornell workloads: normal = -forward, tangent seed +X
+    (the construction of Tests/Backends/CPU/Embree/CornellWavefrontScene.hpp:380-395)."""
+    origin = np.array(CAMERA_ORIGIN, F32)
+    target = np.array(CAMERA_TARGET, F32)
+    seed = (target - origin).astype(F32)
+    length = np.sqrt(F32(F32(F32(seed[0] * seed[0]) + F32(seed[1] * seed[1])) +
+                         F32(seed[2] * seed[2])))
+    forward = (seed / length).astype(F32)
+    normal = (-forward).astype(F32)
+    return origin, normal, np.array([1.0, 0.0, 0.0], F32)
+
+
+WORKLOADS = {
+    # name: (width, height, spp, max_depth, mis, spheres)
+    "cornell_plain_64": (64, 64, 16, 8, "balance", False),
+    "cornell_spheres_256": (256, 256, 256, 16, "power", True),
+}
+
+
+def build_workload(name):
+    width, height, spp, depth, mis, spheres = WORKLOADS[name]
+    builder = cornell_box(SceneBuilder(), with_spheres=spheres)
+    options = abi.default_options(mis=mis, max_depth=depth)
+    return builder, options, (width, height, spp)

@@ -1,0 +1,506 @@
+/*
+ * bf200 — B200-native (sm_100a) wavefront path-tracing backend for Blackframe.
+ *
+ * This header is the whole drop-in boundary. It has three parts:
+ *
+ *   1. The Blackframe extension ABI v1 and XPU backend ABI v1 (device enumeration). Names,
+ *      values and layouts are the ones a Blackframe host binds:
+ *        - Blackframe/Extensions/Abi/Include/Blackframe/Extensions/ExtensionAbi.h:6-101
+ *        - Blackframe/XPU/BackendAbi/Include/Blackframe/XPU/XpuBackendAbi.h:7-55
+ *      The loader resolves `blackframe_query_extension` and asks `get_interface` for an
+ *      interface id (Blackframe/XPU/Host/Source/XpuBackend.cpp:57-100).
+ *
+ *   2. A versioned render interface (BF200_RENDER_INTERFACE_ID_*), returned by the same
+ *      `get_interface` call. It replaces the C++ entry point
+ *        trace_cuda_wavefront_transport(workspace, CudaSceneSoA, CudaSceneBvh,
+ *                                       span<CudaWavefrontPathInput>, LightSampler, options)
+ *      (Blackframe/Backends/GPU/CUDA/Include/Blackframe/Backends/GPU/CUDA/
+ *       WavefrontTransport.hpp:197-208) and the scene upload / BVH build that precede it
+ *      (SceneSoA.hpp:33, SceneBvh.cpp:1109).
+ *
+ *   3. The same render entry points as plain exported C functions (bf200_*), for FFI callers
+ *      (ctypes, cgo, JNI) that do not want to go through the extension table.
+ *
+ * Conventions follow ExtensionAbi.h: every call returns a blackframe_status, every structure
+ * that can grow carries struct_size first, reserved words must be zero, and no C++ type,
+ * exception or allocator crosses the boundary. Host pointers are plain host memory; functions
+ * with a `_device` suffix take CUDA device pointers instead.
+ */
+#ifndef BF200_H
+#define BF200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__cplusplus)
+#define BF200_EXTERN_C extern "C"
+#define BF200_NOEXCEPT noexcept
+#else
+#define BF200_EXTERN_C
+#define BF200_NOEXCEPT
+#endif
+
+#if defined(__GNUC__) || defined(__clang__)
+#define BF200_EXPORT __attribute__((visibility("default")))
+#else
+#define BF200_EXPORT
+#endif
+
+/* ---------------------------------------------------------------------------------------- */
+/* 1. Extension ABI v1 (layouts and values mirror ExtensionAbi.h:37-101)                    */
+/* ---------------------------------------------------------------------------------------- */
+
+#ifndef BLACKFRAME_EXTENSIONS_EXTENSION_ABI_H
+#define BLACKFRAME_EXTENSION_ABI_MAJOR UINT32_C(1)
+#define BLACKFRAME_EXTENSION_ABI_MINOR UINT32_C(0)
+#define BLACKFRAME_EXTENSION_QUERY_SYMBOL "blackframe_query_extension"
+
+typedef uint32_t blackframe_status;
+#define BLACKFRAME_STATUS_SUCCESS ((blackframe_status)0u)
+#define BLACKFRAME_STATUS_INVALID_ARGUMENT ((blackframe_status)1u)
+#define BLACKFRAME_STATUS_UNSUPPORTED_ABI ((blackframe_status)2u)
+#define BLACKFRAME_STATUS_INTERFACE_NOT_FOUND ((blackframe_status)3u)
+#define BLACKFRAME_STATUS_INVALID_STATE ((blackframe_status)4u)
+#define BLACKFRAME_STATUS_OUT_OF_RANGE ((blackframe_status)5u)
+#define BLACKFRAME_STATUS_EXTENSION_FAILURE ((blackframe_status)6u)
+
+typedef struct blackframe_interface_id {
+    uint64_t high;
+    uint64_t low;
+} blackframe_interface_id;
+
+typedef struct blackframe_utf8_view {
+    const char* data;
+    uint32_t size;
+    uint32_t reserved;
+} blackframe_utf8_view;
+
+typedef struct blackframe_extension_query_v1 {
+    uint32_t struct_size;
+    uint32_t abi_major;
+    uint32_t abi_minor;
+    uint32_t reserved;
+} blackframe_extension_query_v1;
+
+typedef blackframe_status (*blackframe_extension_get_interface_fn)(
+    void* extension_context, blackframe_interface_id interface_id, uint32_t requested_major,
+    uint32_t requested_minor, void* out_interface, uint32_t out_interface_size) BF200_NOEXCEPT;
+
+typedef void (*blackframe_extension_shutdown_fn)(void* extension_context) BF200_NOEXCEPT;
+
+typedef struct blackframe_extension_api_v1 {
+    uint32_t struct_size;
+    uint32_t abi_major;
+    uint32_t abi_minor;
+    uint32_t reserved;
+    void* extension_context;
+    blackframe_extension_get_interface_fn get_interface;
+    blackframe_extension_shutdown_fn shutdown;
+} blackframe_extension_api_v1;
+#endif /* BLACKFRAME_EXTENSIONS_EXTENSION_ABI_H */
+
+/* Replaces ExtensionAbi.h:99-101 — the single symbol a Blackframe host resolves. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status
+blackframe_query_extension(const blackframe_extension_query_v1* query,
+                           blackframe_extension_api_v1* out_extension) BF200_NOEXCEPT;
+
+/* ---------------------------------------------------------------------------------------- */
+/* XPU backend ABI v1 (XpuBackendAbi.h:10-55): enumeration only                             */
+/* ---------------------------------------------------------------------------------------- */
+
+#ifndef BLACKFRAME_XPU_XPU_BACKEND_ABI_H
+#define BLACKFRAME_XPU_BACKEND_ABI_MAJOR UINT32_C(1)
+#define BLACKFRAME_XPU_BACKEND_ABI_MINOR UINT32_C(0)
+#define BLACKFRAME_XPU_BACKEND_INTERFACE_ID_HIGH UINT64_C(0x96c6e70dd06b4b93)
+#define BLACKFRAME_XPU_BACKEND_INTERFACE_ID_LOW UINT64_C(0xa9514ab777f49d37)
+
+typedef uint32_t blackframe_xpu_device_kind;
+#define BLACKFRAME_XPU_DEVICE_KIND_UNKNOWN ((blackframe_xpu_device_kind)0u)
+#define BLACKFRAME_XPU_DEVICE_KIND_CPU ((blackframe_xpu_device_kind)1u)
+#define BLACKFRAME_XPU_DEVICE_KIND_GPU ((blackframe_xpu_device_kind)2u)
+#define BLACKFRAME_XPU_DEVICE_KIND_ACCELERATOR ((blackframe_xpu_device_kind)3u)
+
+typedef struct blackframe_xpu_device_descriptor_v1 {
+    uint32_t struct_size;
+    blackframe_xpu_device_kind kind;
+    uint64_t identifier_high;
+    uint64_t identifier_low;
+    blackframe_utf8_view name;
+    blackframe_utf8_view vendor;
+    uint64_t reserved[4];
+} blackframe_xpu_device_descriptor_v1;
+
+typedef blackframe_status (*blackframe_xpu_get_device_count_fn)(
+    void* backend_context, uint32_t* out_device_count) BF200_NOEXCEPT;
+typedef blackframe_status (*blackframe_xpu_get_device_descriptor_fn)(
+    void* backend_context, uint32_t device_index,
+    blackframe_xpu_device_descriptor_v1* out_descriptor) BF200_NOEXCEPT;
+
+typedef struct blackframe_xpu_backend_api_v1 {
+    uint32_t struct_size;
+    uint32_t abi_major;
+    uint32_t abi_minor;
+    uint32_t reserved;
+    void* backend_context;
+    blackframe_utf8_view backend_name;
+    blackframe_xpu_get_device_count_fn get_device_count;
+    blackframe_xpu_get_device_descriptor_fn get_device_descriptor;
+    uint64_t reserved_slots[4];
+} blackframe_xpu_backend_api_v1;
+#endif /* BLACKFRAME_XPU_XPU_BACKEND_ABI_H */
+
+/* ---------------------------------------------------------------------------------------- */
+/* 2. Render interface v1 records                                                           */
+/* ---------------------------------------------------------------------------------------- */
+
+#define BF200_RENDER_ABI_MAJOR UINT32_C(1)
+#define BF200_RENDER_ABI_MINOR UINT32_C(0)
+#define BF200_RENDER_INTERFACE_ID_HIGH UINT64_C(0x6266323030726e64) /* "bf200rnd" */
+#define BF200_RENDER_INTERFACE_ID_LOW UINT64_C(0x7761766566726e31) /* "wavefrn1" */
+
+/* Closure kinds: renderer::ClosureKind (Blackframe/Renderer/Include/Blackframe/Renderer/
+ * ClosureSet.hpp:15-24). */
+#define BF200_CLOSURE_NONE 0u
+#define BF200_CLOSURE_LAMBERTIAN_REFLECTION 1u
+#define BF200_CLOSURE_ROUGH_DIFFUSE_REFLECTION 2u
+#define BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION 3u
+#define BF200_CLOSURE_ROUGH_DIELECTRIC 4u
+#define BF200_CLOSURE_SPECULAR_REFLECTION 5u
+#define BF200_CLOSURE_SPECULAR_TRANSMISSION 6u
+
+/* Scattering lobe bits: renderer::ScatteringLobe (TransportConventions.hpp:44-52). */
+#define BF200_LOBE_DIFFUSE 0x01u
+#define BF200_LOBE_GLOSSY 0x02u
+#define BF200_LOBE_SPECULAR 0x04u
+#define BF200_LOBE_REFLECTION 0x08u
+#define BF200_LOBE_TRANSMISSION 0x10u
+#define BF200_LOBE_VOLUME 0x20u
+
+/* Path terminations: renderer::BsdfOnlyPathTermination (BsdfOnlyPathLoop.hpp:84-90). */
+#define BF200_TERMINATION_ESCAPED_ENVIRONMENT 0u
+#define BF200_TERMINATION_DEPTH_LIMIT 1u
+#define BF200_TERMINATION_OUTSIDE_BSDF_SUPPORT 2u
+#define BF200_TERMINATION_ZERO_THROUGHPUT 3u
+#define BF200_TERMINATION_RUSSIAN_ROULETTE 4u
+
+/* Per-lane failure codes. A lane that fails keeps its last state and reports the first failure;
+ * nothing is substituted (the reference's "no fallback" rule, WavefrontTransport.cpp:612-617). */
+#define BF200_LANE_OK 0u
+#define BF200_LANE_NUMERICAL_FAILURE 1u   /* a checked float operation was not representable */
+#define BF200_LANE_UNSUPPORTED 2u         /* the lane reached a feature this backend rejects */
+#define BF200_LANE_TRAVERSAL_FAILURE 3u   /* traversal stack overflow / invalid topology */
+
+/* One closure record: renderer::ClosureT (ClosureSet.hpp:45-50), 64 bytes. Parameters follow
+ * the reference's packing: conductor eta[0..3], k[4..7], alpha_x[8], alpha_y[9]; dielectric
+ * exterior eta[0], interior eta[1], alpha_x[2], alpha_y[3]. */
+typedef struct bf200_closure_v1 {
+    uint32_t kind;
+    uint32_t lobes;
+    float weight[4];
+    float parameters[10];
+} bf200_closure_v1;
+
+/* A material: engine::SceneSpectralMaterial (FrameScene.hpp:158-166) resolved at the frame's
+ * single wavelength packet. frame_mode: 0 shading normal, 1 surface tangent
+ * (SceneClosureFrameMode, FrameScene.hpp:81-84). */
+typedef struct bf200_material_v1 {
+    uint32_t material_id;
+    uint32_t closure_offset;
+    uint32_t closure_count;
+    uint32_t frame_mode;
+    float tangent_rotation_radians;
+    float component_probabilities[8];
+    float emitted_radiance[4];
+    uint32_t reserved[3];
+} bf200_material_v1;
+
+typedef struct bf200_geometry_v1 {
+    uint32_t geometry_id;
+    uint32_t vertex_offset;
+    uint32_t vertex_count;
+    uint32_t triangle_offset;
+    uint32_t triangle_count;
+    uint32_t reserved[3];
+} bf200_geometry_v1;
+
+/* An instance after hierarchy resolution, in the committed (identifier-sorted) order. The
+ * matrices are the resolved object_to_world transform and its inverse exactly as FrameScene
+ * stores them (row-major 4x4; SceneSoaAbi.hpp columns instance_local_to_world /
+ * instance_world_to_local). */
+typedef struct bf200_instance_v1 {
+    uint32_t instance_id;
+    uint32_t object_id;
+    uint32_t geometry_index;
+    uint32_t material_index;
+    uint32_t visibility_mask;
+    uint32_t reserved[3];
+    float object_to_world[16];
+    float world_to_object[16];
+} bf200_instance_v1;
+
+/* A committed frame scene (engine::FrameScene, FrameScene.hpp:101-316), flattened. Triangle
+ * vertex indices are local to their geometry. Mesh area lights are derived exactly as
+ * FrameScene derives them (FrameScene.cpp:201-261): one light per instance whose material
+ * emits, in instance order, after the punctual lights. */
+typedef struct bf200_scene_desc_v1 {
+    uint32_t struct_size;
+    uint32_t geometry_count;
+    uint32_t vertex_count;
+    uint32_t triangle_count;
+    uint32_t material_count;
+    uint32_t closure_count;
+    uint32_t instance_count;
+    uint32_t punctual_light_count; /* must be 0 in this version: punctual lights are rejected */
+    const bf200_geometry_v1* geometries;
+    const float* positions;        /* 3 * vertex_count */
+    const float* normals;          /* 3 * vertex_count */
+    const float* texture_coordinates; /* 2 * vertex_count */
+    const uint32_t* triangles;     /* 3 * triangle_count */
+    const bf200_material_v1* materials;
+    const bf200_closure_v1* closures;
+    const bf200_instance_v1* instances;
+    float wavelength_nanometers[4];
+    float wavelength_pdf[4];
+    float environment_radiance[4];
+    uint32_t reserved[4];
+} bf200_scene_desc_v1;
+
+/* renderer::Ray (48 bytes, the same size as the reference TransportRay). */
+typedef struct bf200_ray_v1 {
+    float origin[3];
+    float direction[3];
+    float t_min;
+    float t_max;
+    float time;
+    uint32_t mask;
+    uint32_t medium;
+    uint32_t reserved;
+} bf200_ray_v1;
+
+/* renderer::SampleStreamIndex (SampleStream.hpp:12-18), 24 bytes. */
+typedef struct bf200_sample_index_v1 {
+    uint32_t pixel_x;
+    uint32_t pixel_y;
+    uint64_t sample_index;
+    uint64_t seed;
+} bf200_sample_index_v1;
+
+/* engine::CudaWavefrontPathInput (WavefrontTransport.hpp:27-32) for a primary path whose
+ * initial state is PathState::create_initial (beta 1, no radiance, depth 0, vacuum). */
+typedef struct bf200_path_input_v1 {
+    bf200_ray_v1 primary_ray;
+    bf200_sample_index_v1 sample;
+    uint64_t reserved;
+} bf200_path_input_v1;
+
+/* engine::CudaWavefrontPathResult (WavefrontTransport.hpp:52-57) flattened. */
+typedef struct bf200_path_result_v1 {
+    float beta[4];
+    float radiance[4];
+    uint32_t depth;
+    uint32_t depth_counters[5]; /* diffuse, glossy, specular, transmission, volume */
+    float eta_scale;
+    uint32_t delta_flags;
+    uint32_t termination;
+    uint32_t blocked_depth_limits;
+    uint32_t lane_status;  /* BF200_LANE_* */
+    uint32_t segments;     /* extension segments traced by this path */
+    bf200_ray_v1 terminal_ray;
+} bf200_path_result_v1;
+
+/* engine::CudaWavefrontTransportOptions (WavefrontTransport.hpp:134-142), render subset. */
+typedef struct bf200_transport_options_v1 {
+    uint32_t struct_size;
+    uint32_t mis_heuristic;        /* 0 balance, 1 power (MisHeuristics.hpp:13-16) */
+    uint32_t depth_limits[5];      /* diffuse, glossy, specular, transmission, volume */
+    uint32_t roulette_enabled;
+    uint32_t roulette_first_eligible_depth;
+    float roulette_minimum_survival;
+    float roulette_maximum_survival;
+    uint32_t reserved[5];
+} bf200_transport_options_v1;
+
+/* Pinhole camera (PinholeCamera.hpp:52-306) with the host-side constants already derived:
+ * half_height = tan(fov/2), half_width = half_height * width/height. */
+typedef struct bf200_camera_v1 {
+    float origin[3];
+    float tangent[3];
+    float bitangent[3];
+    float normal[3];
+    float half_width;
+    float half_height;
+    float t_min;
+    float t_max;
+    float time;
+    uint32_t mask;
+    uint32_t width;
+    uint32_t height;
+    uint32_t jitter_mode; /* 0 pixel centre, 1 uniform jitter (PixelJitter.hpp:15-18) */
+    uint32_t reserved;
+} bf200_camera_v1;
+
+/* CIE 1931 sensor constants of the frame's packet (Cie1931Sensor.cpp): per lane the XYZ
+ * colour-matching response at the lane wavelength and the lane wavelength pdf, plus the
+ * normalisation (1/4)/Y-integral. */
+typedef struct bf200_sensor_v1 {
+    float response_xyz[4][3];
+    float wavelength_pdf[4];
+    float normalization;
+    uint32_t reserved[3];
+} bf200_sensor_v1;
+
+/* A film request: W x H pixels, samples [first_sample, first_sample + samples_per_pixel).
+ * Every (pixel, sample) path is traced and added to the film in sample order, exactly as a
+ * caller that loops over samples and calls Film::add_sample(x, y, rgb, 1) would. */
+typedef struct bf200_film_request_v1 {
+    uint32_t struct_size;
+    uint32_t samples_per_pixel;
+    uint64_t first_sample;
+    uint64_t seed;
+    uint32_t precision;        /* 0 float32 film (renderer::Film), 1 float64 Neumaier film */
+    uint32_t reserved[3];
+} bf200_film_request_v1;
+
+/* Film storage. float32: 4 floats per pixel (r, g, b, weight) + count. float64: 8 doubles per
+ * pixel (sum r,g,b, weight; compensation r,g,b, weight) + count. */
+typedef struct bf200_film_v1 {
+    uint32_t width;
+    uint32_t height;
+    uint32_t precision;
+    uint32_t reserved;
+    void* sums;            /* host or device pointer, see each call */
+    uint64_t* sample_counts;
+} bf200_film_v1;
+
+/* engine::CudaWavefrontTransportReport (WavefrontTransport.hpp:97-125), counting subset. */
+typedef struct bf200_report_v1 {
+    uint32_t struct_size;
+    uint32_t registered_light_count;
+    uint64_t path_count;
+    uint64_t extension_segments;
+    uint64_t shadow_segments;
+    uint64_t closure_samples;
+    uint64_t light_samples;
+    uint64_t terminated_paths;
+    uint64_t failed_lanes;
+    uint32_t first_failure_status;
+    uint32_t first_failure_path;
+    uint64_t kernel_launches;
+    double gpu_milliseconds;
+    uint64_t reserved[4];
+} bf200_report_v1;
+
+typedef struct bf200_context bf200_context;
+typedef struct bf200_scene bf200_scene;
+
+/* ---------------------------------------------------------------------------------------- */
+/* 3. Exported render entry points                                                          */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Creates a context on one CUDA device. Replaces CudaWavefrontTransportWorkspace::create
+ * (WavefrontTransport.hpp:160-164): the context owns every device buffer; path capacity is the
+ * number of paths kept in flight per wavefront (0 picks the default). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_context_create(int32_t device_ordinal,
+                                                                    uint64_t path_capacity,
+                                                                    bf200_context** out_context)
+    BF200_NOEXCEPT;
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_context_destroy(bf200_context* context)
+    BF200_NOEXCEPT;
+/* Last error text of a context (UTF-8, owned by the context, valid until the next call). */
+BF200_EXTERN_C BF200_EXPORT const char* bf200_context_last_error(const bf200_context* context)
+    BF200_NOEXCEPT;
+
+/* Validates and uploads a committed scene, derives the mesh-light registry and builds the
+ * BLAS/TLAS on the device. Replaces CudaSceneSoA::upload (SceneSoA.hpp:33) followed by
+ * CudaSceneBvh::build (SceneBvh.cpp:1109). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* context,
+                                                                  const bf200_scene_desc_v1* desc,
+                                                                  bf200_scene** out_scene)
+    BF200_NOEXCEPT;
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_destroy(bf200_scene* scene)
+    BF200_NOEXCEPT;
+
+/* Traces a batch of primary paths from host inputs to host results (one-sample NEE with
+ * balance/power MIS, uniform light selection, Russian roulette). Replaces
+ * trace_cuda_wavefront_transport (WavefrontTransport.hpp:197-208). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths(
+    bf200_context* context, const bf200_scene* scene, const bf200_path_input_v1* inputs,
+    uint64_t path_count, const bf200_transport_options_v1* options,
+    bf200_path_result_v1* results, bf200_report_v1* report) BF200_NOEXCEPT;
+
+/* Same as bf200_trace_paths with inputs and results in device memory. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_device(
+    bf200_context* context, const bf200_scene* scene, const bf200_path_input_v1* device_inputs,
+    uint64_t path_count, const bf200_transport_options_v1* options,
+    bf200_path_result_v1* device_results, bf200_report_v1* report) BF200_NOEXCEPT;
+
+/* Renders pinhole-camera paths on the device (camera rays, transport and film accumulation all
+ * on the GPU) and adds them to a host film. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_film(
+    bf200_context* context, const bf200_scene* scene, const bf200_camera_v1* camera,
+    const bf200_sensor_v1* sensor, const bf200_film_request_v1* request,
+    const bf200_transport_options_v1* options, bf200_film_v1* host_film,
+    bf200_report_v1* report) BF200_NOEXCEPT;
+
+/* Same as bf200_render_film with the film in device memory (sums and counts device pointers). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_film_device(
+    bf200_context* context, const bf200_scene* scene, const bf200_camera_v1* camera,
+    const bf200_sensor_v1* sensor, const bf200_film_request_v1* request,
+    const bf200_transport_options_v1* options, bf200_film_v1* device_film,
+    bf200_report_v1* report) BF200_NOEXCEPT;
+
+/* Closest-hit query for a batch of world rays (trace_cuda_closest_hits, ClosestHit.hpp:21-28).
+ * Per ray writes t, barycentrics b0..b2, instance index and primitive index (0xffffffff on a
+ * miss). Host pointers. */
+typedef struct bf200_hit_v1 {
+    float t;
+    float barycentrics[3];
+    uint32_t instance_index;
+    uint32_t primitive_index;
+    uint32_t status;
+    uint32_t reserved;
+} bf200_hit_v1;
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_closest_hits(bf200_context* context,
+                                                                  const bf200_scene* scene,
+                                                                  const bf200_ray_v1* rays,
+                                                                  uint64_t ray_count,
+                                                                  bf200_hit_v1* hits)
+    BF200_NOEXCEPT;
+/* Any-hit query (trace_cuda_occlusions, Occlusion.hpp:19-26): 1 if occluded, else 0. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_occlusions(bf200_context* context,
+                                                                const bf200_scene* scene,
+                                                                const bf200_ray_v1* rays,
+                                                                uint64_t ray_count,
+                                                                uint32_t* occluded) BF200_NOEXCEPT;
+
+/* The render interface table returned by get_interface(BF200_RENDER_INTERFACE_ID, 1, 0). */
+typedef struct bf200_render_api_v1 {
+    uint32_t struct_size;
+    uint32_t abi_major;
+    uint32_t abi_minor;
+    uint32_t reserved;
+    blackframe_status (*context_create)(int32_t, uint64_t, bf200_context**) BF200_NOEXCEPT;
+    blackframe_status (*context_destroy)(bf200_context*) BF200_NOEXCEPT;
+    const char* (*context_last_error)(const bf200_context*) BF200_NOEXCEPT;
+    blackframe_status (*scene_create)(bf200_context*, const bf200_scene_desc_v1*,
+                                      bf200_scene**) BF200_NOEXCEPT;
+    blackframe_status (*scene_destroy)(bf200_scene*) BF200_NOEXCEPT;
+    blackframe_status (*trace_paths)(bf200_context*, const bf200_scene*,
+                                     const bf200_path_input_v1*, uint64_t,
+                                     const bf200_transport_options_v1*, bf200_path_result_v1*,
+                                     bf200_report_v1*) BF200_NOEXCEPT;
+    blackframe_status (*render_film)(bf200_context*, const bf200_scene*, const bf200_camera_v1*,
+                                     const bf200_sensor_v1*, const bf200_film_request_v1*,
+                                     const bf200_transport_options_v1*, bf200_film_v1*,
+                                     bf200_report_v1*) BF200_NOEXCEPT;
+    blackframe_status (*closest_hits)(bf200_context*, const bf200_scene*, const bf200_ray_v1*,
+                                      uint64_t, bf200_hit_v1*) BF200_NOEXCEPT;
+    blackframe_status (*occlusions)(bf200_context*, const bf200_scene*, const bf200_ray_v1*,
+                                    uint64_t, uint32_t*) BF200_NOEXCEPT;
+    uint64_t reserved_slots[4];
+} bf200_render_api_v1;
+
+/* Library version and build description (sm_100a arch string). */
+BF200_EXTERN_C BF200_EXPORT const char* bf200_build_info(void) BF200_NOEXCEPT;
+
+#endif /* BF200_H */

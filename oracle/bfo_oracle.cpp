@@ -1,0 +1,2629 @@
+// Oracle (test infrastructure only): a CPU restatement of the reference's scalar path tracer.
+//
+// This file is never linked into, loaded by, or called from the product. Tests, the golden
+// fixture generator and bench.py's CPU arm load oracle/liboracle.so as the checker. It restates,
+// function by function, the reference's one-sample NEE + MIS scalar loop
+//   trace_scene_mis -> trace_lambertian_mis_with_query
+//   (Blackframe/Engine/Source/SceneMisPathLoop.cpp:632-1016)
+// for the scene contract of include/bf200.h (triangle meshes, root instances, one closure per
+// material: Lambertian, GGX rough conductor, GGX rough dielectric; mesh area lights with a
+// uniform light sampler; constant environment). Every helper cites the reference lines it
+// follows. Arithmetic is float in the reference's operation order (compiled without FMA
+// contraction); std::fma appears exactly where the reference calls it.
+//
+// Parity of this restatement is pinned against the reference itself (oracle/_ref, built from the
+// reference sources by oracle/Makefile) by tests/test_oracle_vs_reference.py and by the committed
+// fixtures in tests/golden/.
+#include "bfo_exact.h"
+
+#include "../include/bf200.h"
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace bfo {
+namespace {
+
+constexpr float kInfinity = std::numeric_limits<float>::infinity();
+constexpr float kEpsilon = std::numeric_limits<float>::epsilon();
+constexpr float kDenormMin = std::numeric_limits<float>::denorm_min();
+constexpr float kInvPi = 0.318309886183790671538F;  // std::numbers::inv_pi_v<float>
+constexpr float kPi = 3.14159265358979323846F;      // std::numbers::pi_v<float>
+
+using Spectrum = std::array<float, 4>;
+
+// Failure of one path: the reference returns std::unexpected for the whole path.
+struct Failure {
+    const char* message;
+};
+
+[[noreturn]] void fail(const char* message) { throw Failure{message}; }
+
+// ---------------------------------------------------------------------------------------------
+// Sample stream (SampleStream.hpp:23-67) and dimension map (SampleDimensionMap.cpp:47-68)
+// ---------------------------------------------------------------------------------------------
+
+uint64_t mix_bits(uint64_t v) {
+    v ^= v >> 30U;
+    v *= 0xBF58476D1CE4E5B9ULL;
+    v ^= v >> 27U;
+    v *= 0x94D049BB133111EBULL;
+    return v ^ (v >> 31U);
+}
+
+struct Stream {
+    uint32_t px, py;
+    uint64_t sample, seed;
+    float sample_1d(uint64_t dimension) const {
+        const uint64_t packed = (uint64_t(px) << 32U) | uint64_t(py);
+        uint64_t state = mix_bits(seed ^ 0x9E3779B97F4A7C15ULL);
+        state = mix_bits(state ^ packed ^ 0xD1B54A32D192ED03ULL);
+        state = mix_bits(state ^ sample ^ 0x8CB92BA72F3D8DD7ULL);
+        const uint64_t bits = mix_bits(state ^ dimension);
+        return static_cast<float>(bits >> 40U) * 0x1p-24F;
+    }
+};
+
+struct Dims {
+    uint64_t light_selection, light_u, light_v, bsdf_component, bsdf_u, bsdf_v, russian_roulette;
+};
+
+Dims dims_for_bounce(uint64_t bounce) {
+    const uint64_t first = 4 + bounce * 10;
+    return Dims{first + 0, first + 1, first + 2, first + 3, first + 4, first + 5, first + 9};
+}
+
+// ---------------------------------------------------------------------------------------------
+// Scene records
+// ---------------------------------------------------------------------------------------------
+
+struct Mat4 {
+    float m[16];
+    float operator()(int r, int c) const { return m[r * 4 + c]; }
+};
+
+// Transforms.hpp:93-119: point and vector transforms, left-to-right sums.
+V3 transform_point(const Mat4& m, V3 p) {
+    return {m(0, 0) * p.x + m(0, 1) * p.y + m(0, 2) * p.z + m(0, 3),
+            m(1, 0) * p.x + m(1, 1) * p.y + m(1, 2) * p.z + m(1, 3),
+            m(2, 0) * p.x + m(2, 1) * p.y + m(2, 2) * p.z + m(2, 3)};
+}
+V3 transform_vector(const Mat4& m, V3 v) {
+    return {m(0, 0) * v.x + m(0, 1) * v.y + m(0, 2) * v.z,
+            m(1, 0) * v.x + m(1, 1) * v.y + m(1, 2) * v.z,
+            m(2, 0) * v.x + m(2, 1) * v.y + m(2, 2) * v.z};
+}
+
+struct Closure {
+    uint32_t kind, lobes;
+    Spectrum weight;
+    float p[10];
+};
+
+struct Material {
+    Closure closure;
+    uint32_t closure_count;
+    uint32_t frame_mode;
+    float rotation;
+    Spectrum emission;
+};
+
+struct MeshLight {
+    uint32_t instance;
+    std::vector<V3> positions;  // world space
+    std::vector<uint32_t> tris; // 3 per triangle
+    std::vector<V3> normals;    // per-triangle geometric normal
+    std::vector<float> areas, cdf;
+    V3 position_error;
+    float area, inverse_area;
+    Spectrum radiance;
+};
+
+struct Instance {
+    uint32_t geometry, material, mask, instance_id;
+    Mat4 to_world, to_object;
+    std::vector<V3> world_vertices;  // 3 per triangle
+    std::vector<V3> world_normals;   // per triangle
+};
+
+struct Scene {
+    std::vector<bf200_geometry_v1> geometries;
+    std::vector<V3> positions, normals;
+    std::vector<float> uvs;
+    std::vector<uint32_t> triangles;
+    std::vector<Material> materials;
+    std::vector<Instance> instances;
+    std::vector<MeshLight> lights;
+    std::vector<float> light_cdf;  // uniform boundaries, size light_count + 1
+    std::vector<int32_t> light_of_instance;
+    Spectrum environment;
+    float nm[4], pdf[4];
+    bool prefilter = true;
+};
+
+V3 load3(const float* a, uint64_t i) { return {a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
+
+// FrameScene.cpp:138-195: world positions of an emissive mesh and their absolute error bound.
+bool transform_mesh_positions(const Scene& scene, const Instance& inst, MeshLight& light) {
+    const auto& g = scene.geometries[inst.geometry];
+    constexpr double eps = static_cast<double>(kEpsilon);
+    constexpr double gamma7 = (7.0 * eps) / (1.0 - 7.0 * eps);
+    constexpr double underflow = 7.0 * static_cast<double>(kDenormMin);
+    constexpr double maximum = static_cast<double>(std::numeric_limits<float>::max());
+    float max_error[3] = {0.0F, 0.0F, 0.0F};
+    for (uint32_t v = 0; v < g.vertex_count; ++v) {
+        const V3 source = scene.positions[g.vertex_offset + v];
+        const V3 world = transform_point(inst.to_world, source);
+        const float s[3] = {source.x, source.y, source.z};
+        const float w[3] = {world.x, world.y, world.z};
+        for (int row = 0; row < 3; ++row) {
+            double magnitude = std::abs(static_cast<double>(inst.to_world(row, 3)));
+            for (int col = 0; col < 3; ++col) {
+                magnitude += std::abs(static_cast<double>(inst.to_world(row, col))) *
+                             std::abs(static_cast<double>(s[col]));
+            }
+            const double bound = std::fma(gamma7, magnitude, underflow);
+            if (!std::isfinite(static_cast<double>(w[row])) || !std::isfinite(bound) ||
+                bound < 0.0 || bound > maximum) {
+                return false;
+            }
+            float rounded = static_cast<float>(bound);
+            if (static_cast<double>(rounded) < bound) {
+                rounded = std::nextafter(rounded, kInfinity);
+            }
+            max_error[row] = std::max(max_error[row], rounded);
+        }
+        light.positions.push_back(world);
+    }
+    light.position_error = V3{max_error[0], max_error[1], max_error[2]};
+    return true;
+}
+
+// AreaLights.hpp:1023-1183: mesh-light construction (areas, compensated total, float CDF).
+bool build_mesh_light(MeshLight& light) {
+    float sum = 0.0F, comp = 0.0F;
+    const size_t n = light.tris.size() / 3;
+    for (size_t t = 0; t < n; ++t) {
+        const V3 a = light.positions[light.tris[3 * t]], b = light.positions[light.tris[3 * t + 1]],
+                 c = light.positions[light.tris[3 * t + 2]];
+        V3 normal;
+        float area;
+        if (!triangle_normal(a, b, c, normal) || !triangle_area(a, b, c, area)) {
+            return false;
+        }
+        light.normals.push_back(normal);
+        const float next = sum + area;
+        if (std::abs(sum) >= std::abs(area)) {
+            comp += (sum - next) + area;
+        } else {
+            comp += (area - next) + sum;
+        }
+        sum = next;
+        light.areas.push_back(area);
+    }
+    const float total = sum + comp;
+    if (!std::isfinite(total) || !(total > 0.0F)) {
+        return false;
+    }
+    light.area = total;
+    light.inverse_area = 1.0F / total;
+    float cumulative = 0.0F;
+    for (size_t t = 0; t < n; ++t) {
+        float next = 1.0F;
+        if (t + 1 != n) {
+            const float selection = light.areas[t] / light.area;
+            next = cumulative + selection;
+            if (!(selection > 0.0F) || !(next > cumulative) || !(next < 1.0F)) {
+                return false;
+            }
+        }
+        cumulative = next;
+        light.cdf.push_back(cumulative);
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Acceleration queries: the analytic backend (AccelBackend.cpp:43-147)
+// ---------------------------------------------------------------------------------------------
+
+struct Hit {
+    float t;
+    float b0, b1, b2;
+    uint32_t instance, primitive;
+    V3 position, normal;
+};
+
+// Conservative double prefilter: true only when the three edge functions certainly have mixed
+// signs, in which case the exact test is certain to report a miss (or a coplanar skip).
+bool certainly_missed(V3 v0, V3 v1, V3 v2, V3 o, V3 d) {
+    const double ox = o.x, oy = o.y, oz = o.z;
+    const double p[3][3] = {{v0.x - ox, v0.y - oy, v0.z - oz},
+                            {v1.x - ox, v1.y - oy, v1.z - oz},
+                            {v2.x - ox, v2.y - oy, v2.z - oz}};
+    const double dx = d.x, dy = d.y, dz = d.z;
+    int signs[3];
+    const int pairs[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+    for (int e = 0; e < 3; ++e) {
+        const double* a = p[pairs[e][0]];
+        const double* b = p[pairs[e][1]];
+        const double t1 = a[0] * b[1] * dz, t2 = a[1] * b[2] * dx, t3 = a[2] * b[0] * dy;
+        const double t4 = a[2] * b[1] * dx, t5 = a[1] * b[0] * dz, t6 = a[0] * b[2] * dy;
+        const double value = ((t1 + t2) + t3) - ((t4 + t5) + t6);
+        const double permanent = std::abs(t1) + std::abs(t2) + std::abs(t3) + std::abs(t4) +
+                                 std::abs(t5) + std::abs(t6);
+        const double bound = 32.0 * 0x1p-53 * permanent;
+        if (value > bound) {
+            signs[e] = 1;
+        } else if (value < -bound) {
+            signs[e] = -1;
+        } else {
+            signs[e] = 0;
+        }
+    }
+    const bool has_pos = signs[0] > 0 || signs[1] > 0 || signs[2] > 0;
+    const bool has_neg = signs[0] < 0 || signs[1] < 0 || signs[2] < 0;
+    return has_pos && has_neg;
+}
+
+// Closest hit over every instance and triangle in committed order; ties keep the earlier one.
+bool closest_hit(const Scene& scene, V3 origin, V3 dir, float t_min, float t_max, uint32_t mask,
+                 Hit& best) {
+    bool found = false;
+    for (uint32_t i = 0; i < scene.instances.size(); ++i) {
+        const Instance& inst = scene.instances[i];
+        if ((mask & inst.mask) == 0U) {
+            continue;
+        }
+        const V3 lo = transform_point(inst.to_object, origin);
+        const V3 ld = transform_vector(inst.to_object, dir);
+        const auto& g = scene.geometries[inst.geometry];
+        for (uint32_t t = 0; t < g.triangle_count; ++t) {
+            const uint32_t* tri = &scene.triangles[3 * (g.triangle_offset + t)];
+            const V3 v0 = scene.positions[g.vertex_offset + tri[0]];
+            const V3 v1 = scene.positions[g.vertex_offset + tri[1]];
+            const V3 v2 = scene.positions[g.vertex_offset + tri[2]];
+            if (scene.prefilter && certainly_missed(v0, v1, v2, lo, ld)) {
+                continue;
+            }
+            TriHit th;
+            const TriResult r = intersect_triangle(v0, v1, v2, lo, ld, t_min, t_max, th);
+            if (r == TriResult::failure) {
+                fail("A triangle intersection is not representable.");
+            }
+            if (r != TriResult::hit) {
+                continue;
+            }
+            if (found && best.t <= th.t) {
+                continue;
+            }
+            best.t = th.t;
+            best.b0 = th.b0;
+            best.b1 = th.b1;
+            best.b2 = th.b2;
+            best.instance = i;
+            best.primitive = t;
+            best.normal = inst.world_normals[t];
+            best.position = origin + dir * th.t;  // Ray::at (Ray.hpp:81-95)
+            found = true;
+        }
+    }
+    return found;
+}
+
+bool occluded(const Scene& scene, V3 origin, V3 dir, float t_min, float t_max, uint32_t mask) {
+    for (uint32_t i = 0; i < scene.instances.size(); ++i) {
+        const Instance& inst = scene.instances[i];
+        if ((mask & inst.mask) == 0U) {
+            continue;
+        }
+        const V3 lo = transform_point(inst.to_object, origin);
+        const V3 ld = transform_vector(inst.to_object, dir);
+        const auto& g = scene.geometries[inst.geometry];
+        for (uint32_t t = 0; t < g.triangle_count; ++t) {
+            const uint32_t* tri = &scene.triangles[3 * (g.triangle_offset + t)];
+            const V3 v0 = scene.positions[g.vertex_offset + tri[0]];
+            const V3 v1 = scene.positions[g.vertex_offset + tri[1]];
+            const V3 v2 = scene.positions[g.vertex_offset + tri[2]];
+            if (scene.prefilter && certainly_missed(v0, v1, v2, lo, ld)) {
+                continue;
+            }
+            TriHit th;
+            const TriResult r = intersect_triangle(v0, v1, v2, lo, ld, t_min, t_max, th);
+            if (r == TriResult::failure) {
+                fail("A triangle intersection is not representable.");
+            }
+            if (r == TriResult::hit) {
+                return true;
+            }
+        }
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Geometry helpers
+// ---------------------------------------------------------------------------------------------
+
+float max_abs3(V3 v) { return std::max({std::abs(v.x), std::abs(v.y), std::abs(v.z)}); }
+
+// BsdfOnlyPathLoop.hpp:190-209 / PinholeCamera.hpp:27-46: scale by the largest component, then
+// divide by the square root of the scaled length squared.
+V3 robust_unit(V3 d) {
+    if (!finite3(d)) {
+        fail("A path direction must remain finite.");
+    }
+    const float m = max_abs3(d);
+    if (m == 0.0F) {
+        fail("A path direction must remain non-zero.");
+    }
+    const V3 s = d / m;
+    const float magnitude = std::sqrt(dot(s, s));
+    const V3 r = s / magnitude;
+    if (!finite3(r)) {
+        fail("Path normalization is not representable.");
+    }
+    return r;
+}
+
+bool unit_length(V3 d) {  // ClosureMixture.hpp:56-64 and its twins
+    if (!finite3(d)) {
+        return false;
+    }
+    const float sq = std::fma(d.x, d.x, std::fma(d.y, d.y, d.z * d.z));
+    return std::isfinite(sq) && std::abs(sq - 1.0F) <= kEpsilon * 128.0F;
+}
+
+struct Frame {
+    V3 t, b, n;
+    V3 to_local(V3 w) const { return {dot(w, t), dot(w, b), dot(w, n)}; }
+    // LocalFrame.hpp:160-163: tangent*x + bitangent*y + normal*z, per component.
+    V3 to_world(V3 l) const {
+        return {t.x * l.x + b.x * l.y + n.x * l.z, t.y * l.x + b.y * l.y + n.y * l.z,
+                t.z * l.x + b.z * l.y + n.z * l.z};
+    }
+};
+
+// LocalFrame.hpp:8-30.
+V3 robust_unit_normal(V3 v) {
+    const float m = max_abs3(v);
+    if (!finite3(v) || m == 0.0F) {
+        fail("A frame normal must be finite and non-zero.");
+    }
+    const V3 s{v.x / m, v.y / m, v.z / m};
+    const float magnitude = std::sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
+    return V3{s.x / magnitude, s.y / magnitude, s.z / magnitude};
+}
+
+V3 robust_unit_vector(V3 v) {  // LocalFrame.hpp:32-48
+    const float m = max_abs3(v);
+    if (!finite3(v) || m == 0.0F) {
+        fail("A frame tangent must be finite and non-parallel to its normal.");
+    }
+    const V3 s = v / m;
+    const float magnitude = std::sqrt(dot(s, s));
+    return s / magnitude;
+}
+
+bool orthonormal(V3 t, V3 b, V3 n) {  // LocalFrame.hpp:50-62
+    constexpr float tol = kEpsilon * 128.0F;
+    return std::abs(dot(t, t) - 1.0F) <= tol && std::abs(dot(b, b) - 1.0F) <= tol &&
+           std::abs(dot(n, n) - 1.0F) <= tol && std::abs(dot(t, b)) <= tol &&
+           std::abs(dot(t, n)) <= tol && std::abs(dot(b, n)) <= tol &&
+           std::abs(dot(cross(t, b), n) - 1.0F) <= tol;
+}
+
+// LocalFrame.hpp:188-219 (from_unit_normal_and_tangent).
+Frame frame_from_unit_normal_and_tangent(V3 n, V3 tangent) {
+    const V3 td = robust_unit_vector(tangent);
+    const V3 projected = td - n * dot(td, n);
+    V3 ut = robust_unit_vector(projected);
+    const V3 ub = robust_unit_vector(cross(n, ut));
+    ut = robust_unit_vector(cross(ub, n));
+    if (!orthonormal(ut, ub, n)) {
+        fail("The supplied directions cannot form a stable orthonormal frame.");
+    }
+    return Frame{ut, ub, n};
+}
+
+// LocalFrame.hpp:66-80 (from_normal).
+Frame frame_from_normal(V3 normal) {
+    const V3 n = robust_unit_normal(normal);
+    const float sign = std::copysign(1.0F, n.z);
+    const float coefficient = -1.0F / (sign + n.z);
+    const float product = n.x * n.y * coefficient;
+    const V3 seed{1.0F + sign * n.x * n.x * coefficient, sign * product, -sign * n.x};
+    return frame_from_unit_normal_and_tangent(n, seed);
+}
+
+// LocalFrame.hpp:116-135 (rotated_about_normal).
+Frame rotated_about_normal(const Frame& f, float angle) {
+    const float reduced = std::remainder(angle, 2.0F * kPi);
+    const float c = std::cos(reduced);
+    const float s = std::sin(reduced);
+    const V3 rotated = f.t * c + f.b * s;
+    return frame_from_unit_normal_and_tangent(f.n, rotated);
+}
+
+// RayOriginOffset.hpp:58-117 (offset_ray_origin).
+V3 offset_ray_origin(V3 p, V3 err, V3 ng, V3 w) {
+    const float m = max_abs3(ng);
+    const V3 sn = ng / m;
+    const V3 n = sn / std::sqrt(dot(sn, sn));
+    const float d = std::abs(n.x) * err.x + std::abs(n.y) * err.y + std::abs(n.z) * err.z;
+    if (!std::isfinite(d)) {
+        fail("The projected ray origin error is not finite.");
+    }
+    const float ds = max_abs3(w);
+    const V3 sw = w / ds;
+    V3 offset{n.x * d, n.y * d, n.z * d};
+    if (dot(n, sw) < 0.0F) {
+        offset = -offset;
+    }
+    auto outward = [](float value, float off) {
+        if (off > 0.0F) {
+            return std::nextafter(value, kInfinity);
+        }
+        if (off < 0.0F) {
+            return std::nextafter(value, -kInfinity);
+        }
+        return value;
+    };
+    const V3 shifted{outward(p.x + offset.x, offset.x), outward(p.y + offset.y, offset.y),
+                     outward(p.z + offset.z, offset.z)};
+    if (!finite3(shifted)) {
+        fail("The ray origin offset exceeds the finite coordinate range.");
+    }
+    return shifted;
+}
+
+// ShadowRay.hpp:15-48 (offset_surface_point).
+V3 offset_surface_point(V3 p, V3 err, V3 ng, V3 w) {
+    const V3 offset = offset_ray_origin(p, err, ng, w);
+    if (offset != p) {
+        return offset;
+    }
+    V3 oriented = ng;
+    if (dot(ng, w) < 0.0F) {
+        oriented = -oriented;
+    }
+    V3 shifted = p;
+    if (oriented.x != 0.0F) {
+        shifted.x = std::nextafter(p.x, oriented.x > 0.0F ? kInfinity : -kInfinity);
+    }
+    if (oriented.y != 0.0F) {
+        shifted.y = std::nextafter(p.y, oriented.y > 0.0F ? kInfinity : -kInfinity);
+    }
+    if (oriented.z != 0.0F) {
+        shifted.z = std::nextafter(p.z, oriented.z > 0.0F ? kInfinity : -kInfinity);
+    }
+    if (!finite3(shifted) || shifted == p) {
+        fail("A shadow-ray surface offset is not representable in the requested precision.");
+    }
+    return shifted;
+}
+
+// ShadowRay.hpp:107-135 (unit_segment).
+void unit_segment(V3 origin, V3 endpoint, V3 expected, V3& direction, float& length) {
+    const V3 disp = endpoint - origin;
+    const float scale = max_abs3(disp);
+    if (!(scale > 0.0F) || !std::isfinite(scale)) {
+        fail("A finite shadow-ray segment must have positive length.");
+    }
+    const V3 s = disp / scale;
+    const float sq = std::fma(s.x, s.x, std::fma(s.y, s.y, s.z * s.z));
+    const float sl = std::sqrt(sq);
+    length = scale * sl;
+    if (!(sl > 0.0F) || !std::isfinite(sl) || !(length > 0.0F) || !std::isfinite(length)) {
+        fail("A finite shadow-ray length is not representable.");
+    }
+    direction = s / sl;
+    const float alignment = dot(direction, expected);
+    if (!std::isfinite(alignment) || !(alignment > 0.0F)) {
+        fail("Shadow-ray endpoint contraction reversed the sampled light direction.");
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Checked products (frexp/scalbn forms of the reference)
+// ---------------------------------------------------------------------------------------------
+
+// DirectLighting.hpp:21-62 (checked_product_quotient).
+float checked_product_quotient(const float* num, int nn, const float* den, int nd) {
+    float significand = 1.0F;
+    int exponent = 0;
+    for (int i = 0; i < nn; ++i) {
+        const float v = num[i];
+        if (!std::isfinite(v) || v < 0.0F) {
+            fail("Direct-lighting numerator factors must be finite and non-negative.");
+        }
+        if (v == 0.0F) {
+            return 0.0F;
+        }
+        int e = 0;
+        significand *= std::frexp(v, &e);
+        exponent += e;
+    }
+    for (int i = 0; i < nd; ++i) {
+        const float v = den[i];
+        if (!std::isfinite(v) || !(v > 0.0F)) {
+            fail("Direct-lighting PDF factors must be finite and strictly positive.");
+        }
+        int e = 0;
+        significand /= std::frexp(v, &e);
+        exponent -= e;
+    }
+    int ne = 0;
+    significand = std::frexp(significand, &ne);
+    const float result = std::scalbn(significand, exponent + ne);
+    if (!std::isfinite(result) || !(result > 0.0F)) {
+        fail("Direct-lighting contribution is not representable in the requested precision.");
+    }
+    return result;
+}
+
+// RoughDielectric.hpp:52-86 (checked_product_ratio: renormalises after every factor).
+float checked_product_ratio(const float* num, int nn, const float* den, int nd) {
+    bool zero = false;
+    for (int i = 0; i < nn; ++i) {
+        if (!std::isfinite(num[i]) || num[i] < 0.0F) {
+            fail("A rough-dielectric product is not representable.");
+        }
+        zero = zero || num[i] == 0.0F;
+    }
+    for (int i = 0; i < nd; ++i) {
+        if (!std::isfinite(den[i]) || !(den[i] > 0.0F)) {
+            fail("A rough-dielectric product is not representable.");
+        }
+    }
+    if (zero) {
+        return 0.0F;
+    }
+    float significand = 1.0F;
+    int exponent = 0;
+    for (int i = 0; i < nn; ++i) {
+        int ve = 0, ne = 0;
+        const float vs = std::frexp(num[i], &ve);
+        significand = std::frexp(significand * vs, &ne);
+        exponent += ve + ne;
+    }
+    for (int i = 0; i < nd; ++i) {
+        int ve = 0, ne = 0;
+        const float vs = std::frexp(den[i], &ve);
+        significand = std::frexp(significand / vs, &ne);
+        exponent += ne - ve;
+    }
+    const float result = std::scalbn(significand, exponent);
+    if (!std::isfinite(result) || !(result > 0.0F)) {
+        fail("A rough-dielectric product is not representable.");
+    }
+    return result;
+}
+
+// MisHeuristics.hpp:142-172 and ClosureMixture.hpp:249-268: a positive product of two factors.
+float positive_product2(float a, float b) {
+    if (b == 0.0F) {
+        return 0.0F;
+    }
+    int ea = 0, eb = 0, en = 0;
+    const float sa = std::frexp(a, &ea);
+    const float sb = std::frexp(b, &eb);
+    const float n = std::frexp(sa * sb, &en);
+    const float r = std::scalbn(n, ea + eb + en);
+    if (!std::isfinite(r) || !(r > 0.0F)) {
+        fail("A positive probability product is not representable.");
+    }
+    return r;
+}
+
+// MisHeuristics.hpp:44-72.
+float ratio_at_most_one(float n, float d) {
+    int ne = 0, de = 0;
+    const float ns = std::frexp(n, &ne);
+    const float ds = std::frexp(d, &de);
+    return std::scalbn(ns / ds, ne - de);
+}
+float squared_ratio_at_most_one(float n, float d) {
+    int ne = 0, de = 0;
+    const float ns = std::frexp(n, &ne);
+    const float ds = std::frexp(d, &de);
+    const float r = ns / ds;
+    return std::scalbn(r * r, 2 * (ne - de));
+}
+float checked_small_weight(float ratio) {
+    if (!(ratio > 0.0F)) {
+        fail("The positive MIS weight is not representable in the requested precision.");
+    }
+    const float w = ratio / (1.0F + ratio);
+    if (!std::isfinite(w) || !(w > 0.0F)) {
+        fail("The positive MIS weight is not representable in the requested precision.");
+    }
+    return w;
+}
+
+// MisHeuristics.hpp:75-141 (balance/power with validate_pdfs).
+float mis_weight(uint32_t heuristic, float sampled, float competing) {
+    if (!std::isfinite(sampled) || !(sampled > 0.0F)) {
+        fail("The sampled-technique MIS PDF must be finite and strictly positive.");
+    }
+    if (!std::isfinite(competing) || competing < 0.0F) {
+        fail("The competing-technique MIS PDF must be finite and non-negative.");
+    }
+    if (competing == 0.0F) {
+        return 1.0F;
+    }
+    if (heuristic == 0) {
+        if (sampled < competing) {
+            return checked_small_weight(ratio_at_most_one(sampled, competing));
+        }
+        return 1.0F / (1.0F + ratio_at_most_one(competing, sampled));
+    }
+    if (sampled < competing) {
+        return checked_small_weight(squared_ratio_at_most_one(sampled, competing));
+    }
+    return 1.0F / (1.0F + squared_ratio_at_most_one(competing, sampled));
+}
+
+// MisHeuristics.hpp:143-172 (joint_light_pdf).
+float joint_light_pdf(float selection, float conditional) {
+    if (!std::isfinite(selection) || !(selection > 0.0F) || selection > 1.0F) {
+        fail("A joint light PDF requires a discrete selection probability in (0, 1].");
+    }
+    if (!std::isfinite(conditional) || conditional < 0.0F) {
+        fail("A joint light PDF requires a finite non-negative conditional PDF.");
+    }
+    if (conditional == 0.0F) {
+        return 0.0F;
+    }
+    return positive_product2(selection, conditional);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Emission (Emission.hpp:42-108)
+// ---------------------------------------------------------------------------------------------
+
+bool unit_normal(V3 n) {
+    const float sq = std::fma(n.x, n.x, std::fma(n.y, n.y, n.z * n.z));
+    return finite3(n) && std::isfinite(sq) && std::abs(sq - 1.0F) <= kEpsilon * 128.0F;
+}
+
+// Returns +1 (emitting side), 0 (back side / tangent-orthogonal), fails when ambiguous.
+int emission_side(V3 ng, V3 wo) {
+    if (!unit_normal(ng) || !finite3(wo) || (wo.x == 0.0F && wo.y == 0.0F && wo.z == 0.0F)) {
+        fail("Surface emission evaluation requires a unit normal and a non-zero direction.");
+    }
+    const float m = max_abs3(wo);
+    const V3 s = wo / m;
+    const float alignment = std::fma(ng.x, s.x, std::fma(ng.y, s.y, ng.z * s.z));
+    if (!std::isfinite(alignment)) {
+        fail("Surface emission orientation is not representable.");
+    }
+    const bool orthogonal = (ng.x == 0.0F || wo.x == 0.0F) && (ng.y == 0.0F || wo.y == 0.0F) &&
+                            (ng.z == 0.0F || wo.z == 0.0F);
+    if (alignment == 0.0F && orthogonal) {
+        return 0;
+    }
+    const float abs_sum =
+        std::fma(std::abs(ng.x), std::abs(s.x),
+                 std::fma(std::abs(ng.y), std::abs(s.y), std::abs(ng.z) * std::abs(s.z)));
+    const float uncertainty = std::fma(4.0F * kEpsilon, abs_sum, 4.0F * kDenormMin);
+    if (std::abs(alignment) <= uncertainty) {
+        fail("Surface emission orientation is not representable.");
+    }
+    return alignment > 0.0F ? 1 : 0;
+}
+
+bool is_black(const Spectrum& s) { return s[0] == 0 && s[1] == 0 && s[2] == 0 && s[3] == 0; }
+
+// ---------------------------------------------------------------------------------------------
+// Area-light pdf conversion (Light.hpp:75-163, 593-620) and mesh-light sampling
+// ---------------------------------------------------------------------------------------------
+
+float area_to_solid_angle(float area_pdf, V3 ref, V3 surf, V3 ng) {
+    if (!unit_normal(ng)) {
+        fail("Light PDF conversion requires a finite unit surface geometric normal.");
+    }
+    const V3 disp = surf - ref;
+    const float scale = max_abs3(disp);
+    if (!(scale > 0.0F) || !std::isfinite(scale)) {
+        fail("Light PDF conversion requires two distinct positions.");
+    }
+    const V3 s = disp / scale;
+    const float sq = std::fma(s.x, s.x, std::fma(s.y, s.y, s.z * s.z));
+    const float sl = std::sqrt(sq);
+    const float cubed = sq * sl;
+    if (!std::isfinite(sq) || !(sq > 0.0F) || !std::isfinite(cubed) || !(cubed > 0.0F)) {
+        fail("Light PDF conversion distance is not representable.");
+    }
+    const float signed_alignment = std::fma(ng.x, -s.x, std::fma(ng.y, -s.y, ng.z * -s.z));
+    const float alignment = std::abs(signed_alignment);
+    const float term_sum =
+        std::fma(std::abs(ng.x), std::abs(s.x),
+                 std::fma(std::abs(ng.y), std::abs(s.y), std::abs(ng.z) * std::abs(s.z)));
+    const float uncertainty = std::fma(4.0F * kEpsilon, term_sum, 4.0F * kDenormMin);
+    if (!std::isfinite(alignment) || !std::isfinite(term_sum) || alignment <= uncertainty) {
+        fail("Light PDF conversion Jacobian is singular or numerically ambiguous.");
+    }
+    if (area_pdf == 0.0F) {
+        return 0.0F;
+    }
+    int es = 0, ed = 0, ec = 0, ea = 0, en = 0;
+    const float fs = std::frexp(area_pdf, &es);
+    const float fd = std::frexp(scale, &ed);
+    const float fc = std::frexp(cubed, &ec);
+    const float fa = std::frexp(alignment, &ea);
+    const float combined = fs * fd * fd * fc / fa;
+    const int exponent = es + 2 * ed + ec - ea;
+    const float normalized = std::frexp(combined, &en);
+    const float converted = std::scalbn(normalized, exponent + en);
+    if (!std::isfinite(converted) || !(converted > 0.0F)) {
+        fail("Converted light PDF is not representable in the requested precision.");
+    }
+    return converted;
+}
+
+struct LightSample {
+    bool valid = false;
+    V3 position, error, normal;
+    V3 direction;
+    float distance;
+    float pdf;  // solid angle
+    Spectrum radiance;
+};
+
+// IncidentLightSample::create_finite (Light.hpp:401-441): direction and distance.
+void incident_direction(V3 context, V3 endpoint, V3& direction, float& distance) {
+    const V3 disp = endpoint - context;
+    const float scale = max_abs3(disp);
+    if (!(scale > 0.0F) || !std::isfinite(scale)) {
+        fail("A finite incident light sample requires distinct positions.");
+    }
+    const V3 s = disp / scale;
+    const float sq = std::fma(s.x, s.x, std::fma(s.y, s.y, s.z * s.z));
+    const float sl = std::sqrt(sq);
+    distance = scale * sl;
+    if (!std::isfinite(sl) || !(sl > 0.0F) || !std::isfinite(distance) || !(distance > 0.0F)) {
+        fail("Finite incident light sample distance is not representable.");
+    }
+    direction = s / sl;
+    if (!unit_length(direction)) {
+        fail("An incident light sample requires a finite unit direction.");
+    }
+}
+
+// MeshAreaLight::sample_li (AreaLights.hpp:1184-1243) with finish_sample (AreaLights.hpp:329-371).
+LightSample sample_mesh_light(const MeshLight& light, V3 context, float u, float v) {
+    LightSample out;
+    if (!(u >= 0.0F && u < 1.0F && v >= 0.0F && v < 1.0F)) {
+        fail("Area-light sampling requires a canonical sample.");
+    }
+    const auto it = std::upper_bound(light.cdf.begin(), light.cdf.end(), u);
+    if (it == light.cdf.end()) {
+        fail("Mesh area-light selection escaped its cumulative distribution.");
+    }
+    const size_t index = static_cast<size_t>(it - light.cdf.begin());
+    const float previous = index == 0 ? 0.0F : light.cdf[index - 1];
+    const float selection = light.cdf[index] - previous;
+    const float remapped = (u - previous) / selection;
+    if (!std::isfinite(selection) || !(selection > 0.0F) || !std::isfinite(remapped) ||
+        remapped < 0.0F || !(remapped < 1.0F)) {
+        fail("Mesh area-light canonical remapping is not representable.");
+    }
+    const float density = selection / light.areas[index];
+    if (!std::isfinite(density) || !(density > 0.0F)) {
+        fail("Mesh area-light triangle density is not representable.");
+    }
+    const float root = std::sqrt(remapped);
+    const float bary[3] = {1.0F - root, root * (1.0F - v), root * v};
+    const V3 p[3] = {light.positions[light.tris[3 * index]], light.positions[light.tris[3 * index + 1]],
+                     light.positions[light.tris[3 * index + 2]]};
+    // triangle_position_with_error (AreaLights.hpp:260-301).
+    constexpr float gamma12 = (12.0F * kEpsilon) / (1.0F - 12.0F * kEpsilon);
+    constexpr float underflow = 12.0F * kDenormMin;
+    const float base[3] = {light.position_error.x, light.position_error.y, light.position_error.z};
+    float point[3], error[3];
+    for (int axis = 0; axis < 3; ++axis) {
+        const float c0 = axis == 0 ? p[0].x : axis == 1 ? p[0].y : p[0].z;
+        const float c1 = axis == 0 ? p[1].x : axis == 1 ? p[1].y : p[1].z;
+        const float c2 = axis == 0 ? p[2].x : axis == 1 ? p[2].y : p[2].z;
+        const float prod0 = bary[0] * c0, prod1 = bary[1] * c1, prod2 = bary[2] * c2;
+        point[axis] = std::fma(bary[0], c0, std::fma(bary[1], c1, prod2));
+        const float magnitude = std::abs(prod0) + std::abs(prod1) + std::abs(prod2);
+        const float arithmetic = std::fma(gamma12, magnitude, underflow);
+        error[axis] = std::nextafter(base[axis] + arithmetic, kInfinity);
+    }
+    out.position = V3{point[0], point[1], point[2]};
+    out.error = V3{error[0], error[1], error[2]};
+    out.normal = light.normals[index];
+    // one-sided support, then the solid-angle conversion of the triangle's area density.
+    if (emission_side(out.normal, context - out.position) <= 0) {
+        return out;  // no sample
+    }
+    out.pdf = area_to_solid_angle(density, context, out.position, out.normal);
+    incident_direction(context, out.position, out.direction, out.distance);
+    if (!std::isfinite(out.pdf) || !(out.pdf > 0.0F)) {
+        fail("A finite surface light sample requires a solid-angle density.");
+    }
+    out.radiance = light.radiance;
+    out.valid = !is_black(light.radiance);
+    return out;
+}
+
+// MeshAreaLight::pdf_li_at_surface (AreaLights.hpp:1296-1309) via finish_pdf (AreaLights.hpp:373-403).
+float mesh_light_pdf_at_surface(const MeshLight& light, V3 context, V3 surface, V3 ng) {
+    if (emission_side(ng, context - surface) <= 0) {
+        return 0.0F;
+    }
+    const float pdf = area_to_solid_angle(light.inverse_area, context, surface, ng);
+    if (is_black(light.radiance)) {
+        return 0.0F;
+    }
+    return pdf;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Closures
+// ---------------------------------------------------------------------------------------------
+
+struct BsdfSample {
+    bool valid = false;
+    V3 wi;
+    Spectrum value{};
+    float pdf = 0.0F;
+    uint32_t lobes = 0;
+    float eta_scale = 1.0F;
+};
+
+// SamplingMappings.hpp:33-60 and 128-141 (concentric disk, cosine hemisphere).
+V3 map_cosine_hemisphere(float u, float v) {
+    const float ox = 2.0F * u - 1.0F;
+    const float oy = 2.0F * v - 1.0F;
+    float px = 0.0F, py = 0.0F, radius = 0.0F;
+    if (!(ox == 0.0F && oy == 0.0F)) {
+        constexpr float quarter_pi = kPi / 4.0F;
+        float r, phi;
+        if (std::abs(ox) > std::abs(oy)) {
+            r = ox;
+            phi = quarter_pi * (oy / ox);
+        } else {
+            r = oy;
+            phi = 2.0F * quarter_pi - quarter_pi * (ox / oy);
+        }
+        px = r * std::cos(phi);
+        py = r * std::sin(phi);
+        radius = std::abs(r);
+    }
+    const float z = std::sqrt((1.0F - radius) * (1.0F + radius));
+    return V3{px, py, z};
+}
+
+// GGX (GgxMicrofacet.hpp).
+struct Ggx {
+    float ax, ay;
+};
+
+struct SmithTerms {
+    float normal, tangent, radius, normal_over_radius;
+};
+
+// GgxMicrofacet.hpp:134-184.
+SmithTerms smith_terms(const Ggx& g, V3 w) {
+    SmithTerms t{};
+    if (g.ax == g.ay) {
+        const float alpha = g.ax;
+        const float sine = std::hypot(w.x, w.y);
+        const float inverse_alpha = 1.0F / alpha;
+        t.normal = alpha <= 1.0F ? w.z : w.z * inverse_alpha;
+        t.tangent = alpha <= 1.0F ? alpha * sine : sine;
+        t.radius = std::hypot(t.normal, t.tangent);
+    } else {
+        const float common = std::max({1.0F, g.ax, g.ay});
+        t.normal = w.z / common;
+        const float tx = (g.ax / common) * w.x;
+        const float ty = (g.ay / common) * w.y;
+        t.tangent = std::hypot(tx, ty);
+        t.radius = std::hypot(t.normal, t.tangent);
+    }
+    if (!std::isfinite(t.normal) || !std::isfinite(t.tangent) || !std::isfinite(t.radius) ||
+        !(t.normal > 0.0F) || !(t.radius > 0.0F)) {
+        fail("GGX Smith geometry is not representable for the supplied direction.");
+    }
+    t.normal_over_radius = t.normal / t.radius;
+    if (!std::isfinite(t.normal_over_radius) || !(t.normal_over_radius > 0.0F) ||
+        t.normal_over_radius > 1.0F) {
+        fail("GGX Smith geometry is not representable for the supplied direction.");
+    }
+    return t;
+}
+
+// GgxMicrofacet.hpp:232-270 (normal_distribution).
+float ggx_d(const Ggx& g, V3 m) {
+    if (!unit_length(m)) {
+        fail("GGX microfacet normals must be finite unit normals.");
+    }
+    if (!(m.z > 0.0F)) {
+        return 0.0F;
+    }
+    float denominator_root, density_root;
+    if (g.ax == g.ay) {
+        const float radial = std::hypot(m.x, m.y);
+        if (g.ax <= 1.0F) {
+            denominator_root = std::hypot(radial, g.ax * m.z);
+            density_root = (g.ax / denominator_root) / denominator_root;
+        } else {
+            const float inverse_alpha = 1.0F / g.ax;
+            denominator_root = std::hypot(radial * inverse_alpha, m.z);
+            density_root = (inverse_alpha / denominator_root) / denominator_root;
+        }
+        density_root *= std::sqrt(kInvPi);
+    } else {
+        denominator_root = std::hypot(m.x / g.ax, m.y / g.ay, m.z);
+        const float normalization_root = std::sqrt(kInvPi) / (std::sqrt(g.ax) * std::sqrt(g.ay));
+        density_root = (normalization_root / denominator_root) / denominator_root;
+    }
+    const float value = density_root * density_root;
+    if (!std::isfinite(denominator_root) || !(denominator_root > 0.0F) || !std::isfinite(value) ||
+        !(value > 0.0F)) {
+        fail("The GGX normal distribution value is not representable.");
+    }
+    return value;
+}
+
+// GgxMicrofacet.hpp:320-353 (smith_g2).
+float ggx_g2(const Ggx& g, V3 wo, V3 wi) {
+    if (!unit_length(wo) || !unit_length(wi)) {
+        fail("GGX Smith directions must be finite unit vectors.");
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+        return 0.0F;
+    }
+    const SmithTerms o = smith_terms(g, wo);
+    const SmithTerms i = smith_terms(g, wi);
+    const float smaller = std::min(o.normal_over_radius, i.normal_over_radius);
+    const float larger = std::max(o.normal_over_radius, i.normal_over_radius);
+    const float value = 2.0F * smaller / (1.0F + smaller / larger);
+    if (!std::isfinite(value) || !(value > 0.0F) || value > 1.0F) {
+        fail("GGX Smith G2 is not representable for the supplied directions.");
+    }
+    return value;
+}
+
+// GgxMicrofacet.hpp:355-388 (visible_normal_pdf).
+float ggx_vndf_pdf(const Ggx& g, V3 wo, V3 m) {
+    if (!unit_length(wo) || !unit_length(m)) {
+        fail("GGX VNDF queries require finite unit directions and normals.");
+    }
+    const float visible_dot = dot(wo, m);
+    if (!(wo.z > 0.0F) || !(m.z > 0.0F) || !(visible_dot > 0.0F)) {
+        return 0.0F;
+    }
+    const float d = ggx_d(g, m);
+    const float physical_radius = g.ax == g.ay
+                                      ? std::hypot(wo.z, g.ax * std::hypot(wo.x, wo.y))
+                                      : std::hypot(wo.z, g.ax * wo.x, g.ay * wo.y);
+    const float physical_denominator = wo.z + physical_radius;
+    const float visible_factor = 2.0F * visible_dot / physical_denominator;
+    const float value = d * visible_factor;
+    if (!std::isfinite(physical_denominator) || !(physical_denominator > 0.0F) ||
+        !std::isfinite(value) || !(value > 0.0F)) {
+        fail("The GGX visible-normal PDF is not representable.");
+    }
+    return value;
+}
+
+// GgxMicrofacet.hpp:71-103 (normalize_vector / normalize_normal).
+V3 ggx_normalize(V3 v) {
+    const float length = std::hypot(std::hypot(v.x, v.y), v.z);
+    if (!std::isfinite(length) || !(length > 0.0F)) {
+        fail("A GGX VNDF intermediate vector is not normalizable.");
+    }
+    const V3 r{v.x / length, v.y / length, v.z / length};
+    if (!unit_length(r)) {
+        fail("A GGX VNDF intermediate direction is not representable.");
+    }
+    return r;
+}
+
+float nonnegative_roundoff(float value, float scale) {  // GgxMicrofacet.hpp:186-197
+    if (value >= 0.0F) {
+        return value;
+    }
+    const float bound = kEpsilon * 16.0F * std::max(1.0F, std::abs(scale));
+    if (-value <= bound) {
+        return 0.0F;
+    }
+    fail("A GGX VNDF square-root argument is negative beyond round-off.");
+}
+
+// GgxMicrofacet.hpp:390-525 (sample_visible_normal). Returns false when wo.z <= 0.
+bool ggx_sample_vndf(const Ggx& g, V3 wo, float u, float v, V3& m_out, float& pdf_out) {
+    if (!unit_length(wo)) {
+        fail("GGX VNDF sampling requires a finite unit outgoing direction.");
+    }
+    if (!(wo.z > 0.0F)) {
+        return false;
+    }
+    const bool iso = g.ax == g.ay;
+    const float inverse_alpha = 1.0F / g.ax;
+    const float common = std::max({1.0F, g.ax, g.ay});
+    const float sax = g.ax / common, say = g.ay / common;
+    V3 st;
+    if (iso) {
+        st = g.ax <= 1.0F ? V3{g.ax * wo.x, g.ax * wo.y, wo.z}
+                          : V3{wo.x, wo.y, wo.z * inverse_alpha};
+    } else {
+        st = V3{sax * wo.x, say * wo.y, wo.z / common};
+    }
+    if ((iso && g.ax <= 1.0F && ((wo.x != 0.0F && st.x == 0.0F) || (wo.y != 0.0F && st.y == 0.0F))) ||
+        (iso && g.ax > 1.0F && st.z == 0.0F) ||
+        (!iso && ((wo.x != 0.0F && st.x == 0.0F) || (wo.y != 0.0F && st.y == 0.0F) || st.z == 0.0F))) {
+        fail("The GGX VNDF view stretch is not representable.");
+    }
+    const V3 hv = ggx_normalize(st);
+    const float tl = std::hypot(hv.x, hv.y);
+    const V3 tangent = tl > 0.0F ? V3{-hv.y / tl, hv.x / tl, 0.0F} : V3{1.0F, 0.0F, 0.0F};
+    const V3 bitangent = cross(hv, tangent);
+    const float disk_radius = std::sqrt(u);
+    const float azimuth = 2.0F * kPi * v;
+    const float disk_x = disk_radius * std::cos(azimuth);
+    const float initial_disk_y = disk_radius * std::sin(azimuth);
+    const float limit_sq = (1.0F - disk_x) * (1.0F + disk_x);
+    const float checked_limit_sq = nonnegative_roundoff(limit_sq, 1.0F + std::abs(disk_x));
+    const float disk_y_limit = std::sqrt(checked_limit_sq);
+    const float projection = 0.5F * (1.0F + hv.z);
+    const float disk_y = std::fma(projection, initial_disk_y, (1.0F - projection) * disk_y_limit);
+    const float hz_sq = std::fma(-disk_y, disk_y, checked_limit_sq);
+    const float checked_hz_sq = nonnegative_roundoff(hz_sq, checked_limit_sq + std::abs(disk_y * disk_y));
+    const float hz = std::sqrt(checked_hz_sq);
+    const V3 hn{std::fma(disk_x, tangent.x, std::fma(disk_y, bitangent.x, hz * hv.x)),
+                std::fma(disk_x, tangent.y, std::fma(disk_y, bitangent.y, hz * hv.y)),
+                std::fma(disk_x, tangent.z, std::fma(disk_y, bitangent.z, hz * hv.z))};
+    if (!(hn.z > 0.0F)) {
+        fail("The GGX VNDF hemisphere sample is outside its open support.");
+    }
+    V3 un;
+    if (iso) {
+        un = g.ax <= 1.0F ? V3{g.ax * hn.x, g.ax * hn.y, hn.z} : V3{hn.x, hn.y, hn.z * inverse_alpha};
+    } else {
+        un = V3{sax * hn.x, say * hn.y, hn.z / common};
+    }
+    if ((iso && g.ax <= 1.0F && ((hn.x != 0.0F && un.x == 0.0F) || (hn.y != 0.0F && un.y == 0.0F))) ||
+        (iso && g.ax > 1.0F && un.z == 0.0F) ||
+        (!iso && ((hn.x != 0.0F && un.x == 0.0F) || (hn.y != 0.0F && un.y == 0.0F) || un.z == 0.0F))) {
+        fail("The GGX visible-normal unstretch is not representable.");
+    }
+    const V3 m = ggx_normalize(un);
+    if (!(m.z > 0.0F) || !(dot(wo, m) > 0.0F)) {
+        fail("The GGX VNDF sample is outside its visible support.");
+    }
+    m_out = m;
+    pdf_out = ggx_vndf_pdf(g, wo, m);
+    return true;
+}
+
+// Fresnel.hpp:27-104 (conductor, one lane).
+float squared_magnitude_ratio(float nr, float ni, float dr, float di) {
+    const float n = std::hypot(nr, ni);
+    const float d = std::hypot(dr, di);
+    if (!std::isfinite(n) || !std::isfinite(d) || !(d > 0.0F)) {
+        fail("A conductor Fresnel polarization ratio is not representable.");
+    }
+    const float amplitude = n / d;
+    const float r = amplitude * amplitude;
+    if (!std::isfinite(r) || r < 0.0F || r > 1.0F) {
+        fail("A conductor Fresnel polarization ratio is not representable.");
+    }
+    return r;
+}
+
+float conductor_fresnel_lane(float cosine, float eta, float k) {
+    if (eta == 1.0F && k == 0.0F) {
+        return 0.0F;
+    }
+    if (cosine == 0.0F) {
+        return 1.0F;
+    }
+    const float scale = std::max({1.0F, eta, k});
+    const float nie = 1.0F / scale;
+    const float ne = eta / scale;
+    const float nk = k / scale;
+    if (cosine == 1.0F) {
+        const float r = squared_magnitude_ratio(ne - nie, nk, ne + nie, nk);
+        if (!(r > 0.0F)) {
+            fail("Conductor Fresnel reflectance is not representable.");
+        }
+        return r;
+    }
+    const float sin_sq = (1.0F - cosine) * (1.0F + cosine);
+    const float scaled_sin_sq = nie * nie * sin_sq;
+    const float x = std::fma(ne, ne, -std::fma(nk, nk, scaled_sin_sq));
+    const float y = 2.0F * ne * nk;
+    const float magnitude = std::hypot(x, y);
+    float rr, ri;
+    if (x >= 0.0F) {
+        rr = std::sqrt(0.5F * (magnitude + x));
+        ri = rr == 0.0F ? 0.0F : y / (2.0F * rr);
+    } else {
+        ri = std::sqrt(0.5F * (magnitude - x));
+        rr = ri == 0.0F ? 0.0F : y / (2.0F * ri);
+    }
+    const float sc = nie * cosine;
+    const float perpendicular = squared_magnitude_ratio(sc - rr, -ri, sc + rr, ri);
+    const float ser = std::fma(ne, ne, -(nk * nk));
+    const float sei = y;
+    const float srr = nie * rr;
+    const float sri = nie * ri;
+    const float pbr = cosine * ser;
+    const float pbi = cosine * sei;
+    const float parallel = squared_magnitude_ratio(pbr - srr, pbi - sri, pbr + srr, pbi + sri);
+    const float r = 0.5F * (perpendicular + parallel);
+    if (!std::isfinite(r) || !(r > 0.0F) || r > 1.0F) {
+        fail("Conductor Fresnel reflectance is not representable.");
+    }
+    return r;
+}
+
+// Fresnel.hpp:107-170 (dielectric).
+float dielectric_fresnel(float cosine, float eta_i, float eta_t) {
+    if (!std::isfinite(cosine) || cosine < 0.0F || cosine > 1.0F) {
+        fail("Dielectric Fresnel requires an incident-cosine magnitude in [0, 1].");
+    }
+    if (eta_i == eta_t) {
+        return 0.0F;
+    }
+    if (cosine == 0.0F) {
+        return 1.0F;
+    }
+    const bool denser = eta_i > eta_t;
+    const float ne = denser ? eta_t / eta_i : eta_i / eta_t;
+    if (cosine == 1.0F) {
+        const float a = (1.0F - ne) / (1.0F + ne);
+        const float r = a * a;
+        if (!std::isfinite(r) || !(r > 0.0F) || r > 1.0F) {
+            fail("Dielectric Fresnel reflectance is not representable.");
+        }
+        return r;
+    }
+    const float sin_i = std::sqrt((1.0F - cosine) * (1.0F + cosine));
+    float sin_t;
+    if (denser) {
+        if (ne == 0.0F || sin_i >= ne) {
+            return 1.0F;
+        }
+        sin_t = sin_i / ne;
+    } else {
+        sin_t = ne * sin_i;
+    }
+    if (!(sin_t < 1.0F)) {
+        return 1.0F;
+    }
+    const float cos_t = std::sqrt((1.0F - sin_t) * (1.0F + sin_t));
+    const float fec = ne * cos_t;
+    const float fa = (cosine - fec) / (cosine + fec);
+    const float sec = ne * cosine;
+    const float sa = (sec - cos_t) / (sec + cos_t);
+    const float r = 0.5F * std::fma(fa, fa, sa * sa);
+    if (!std::isfinite(r) || !(r > 0.0F) || r > 1.0F) {
+        fail("Dielectric Fresnel reflectance is not representable.");
+    }
+    return r;
+}
+
+// RoughConductorReflection.hpp:68-106 (reflection_geometry: half vector and its cosine).
+void half_vector_geometry(V3 wo, V3 wi, V3& m, float& half_cos) {
+    const V3 h{wo.x + wi.x, wo.y + wi.y, wo.z + wi.z};
+    const float length = std::hypot(std::hypot(h.x, h.y), h.z);
+    if (!std::isfinite(length) || !(length > 0.0F)) {
+        fail("The reflection half-vector is not normalizable.");
+    }
+    m = V3{h.x / length, h.y / length, h.z / length};
+    if (!unit_length(m) || !(m.z > 0.0F)) {
+        fail("The reflection half-vector is not representable.");
+    }
+    half_cos = 0.5F * length;
+    if (!std::isfinite(half_cos) || !(half_cos > 0.0F) || half_cos > 1.0F) {
+        fail("The reflection half-angle cosine is outside [0, 1].");
+    }
+}
+
+// RoughConductorReflection.hpp:167-209 (eval).
+Spectrum conductor_eval(const Closure& c, V3 wo, V3 wi) {
+    Spectrum r{};
+    if (!unit_length(wo) || !unit_length(wi)) {
+        fail("Rough-conductor directions must be finite unit vectors.");
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F) || is_black(c.weight)) {
+        return r;
+    }
+    const Ggx g{c.p[8], c.p[9]};
+    V3 m;
+    float hc;
+    half_vector_geometry(wo, wi, m, hc);
+    const float d = ggx_d(g, m);
+    const float g2 = ggx_g2(g, wo, wi);
+    float fresnel[4];
+    for (int lane = 0; lane < 4; ++lane) {
+        fresnel[lane] = conductor_fresnel_lane(hc, c.p[lane], c.p[4 + lane]);
+    }
+    const float denominator = 4.0F * wo.z * wi.z;
+    const float scale = (d * g2) / denominator;
+    if (!std::isfinite(denominator) || !(denominator > 0.0F) || !std::isfinite(scale) ||
+        !(scale > 0.0F)) {
+        fail("The rough-conductor GGX reflection value is not representable.");
+    }
+    for (int lane = 0; lane < 4; ++lane) {
+        r[lane] = c.weight[lane] * fresnel[lane] * scale;
+    }
+    return r;
+}
+
+// RoughConductorReflection.hpp:211-238 (pdf).
+float conductor_pdf(const Closure& c, V3 wo, V3 wi) {
+    if (!unit_length(wo) || !unit_length(wi)) {
+        fail("Rough-conductor directions must be finite unit vectors.");
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+        return 0.0F;
+    }
+    V3 m;
+    float hc;
+    half_vector_geometry(wo, wi, m, hc);
+    const float visible = ggx_vndf_pdf(Ggx{c.p[8], c.p[9]}, wo, m);
+    const float value = visible / (4.0F * hc);
+    if (!std::isfinite(value) || !(value > 0.0F)) {
+        fail("The rough-conductor reflected-direction PDF is not representable.");
+    }
+    return value;
+}
+
+// RoughConductorReflection.hpp:240-288 (sample).
+BsdfSample conductor_sample(const Closure& c, V3 wo, float u, float v) {
+    BsdfSample s;
+    V3 m;
+    float vpdf;
+    if (!ggx_sample_vndf(Ggx{c.p[8], c.p[9]}, wo, u, v, m, vpdf)) {
+        return s;
+    }
+    const float hc = dot(wo, m);
+    if (!std::isfinite(hc) || !(hc > 0.0F) || hc > 1.0F) {
+        fail("The sampled rough-conductor half-angle cosine is outside [0, 1].");
+    }
+    const V3 wi{2.0F * hc * m.x - wo.x, 2.0F * hc * m.y - wo.y, 2.0F * hc * m.z - wo.z};
+    if (!unit_length(wi)) {
+        fail("The sampled rough-conductor reflection direction is not representable.");
+    }
+    if (!(wi.z > 0.0F)) {
+        return s;
+    }
+    s.wi = wi;
+    s.value = conductor_eval(c, wo, wi);
+    s.pdf = conductor_pdf(c, wo, wi);
+    s.lobes = c.lobes;
+    s.valid = true;
+    return s;
+}
+
+// RoughDielectric.hpp:114-134 (interface_for).
+struct Interface {
+    float face_sign, incident_eta, transmitted_eta, nie, nte;
+};
+Interface interface_for(V3 wo, float ext, float in) {
+    Interface f;
+    f.face_sign = wo.z > 0.0F ? 1.0F : -1.0F;
+    f.incident_eta = f.face_sign > 0.0F ? ext : in;
+    f.transmitted_eta = f.face_sign > 0.0F ? in : ext;
+    const float mx = std::max(f.incident_eta, f.transmitted_eta);
+    f.nie = f.incident_eta / mx;
+    f.nte = f.transmitted_eta / mx;
+    return f;
+}
+
+V3 scaled_dir(V3 d, float s) { return {s * d.x, s * d.y, s * d.z}; }
+
+struct TransmissionGeometry {
+    bool valid;
+    V3 m;
+    float o_dot_m, i_dot_m, length;
+};
+
+// RoughDielectric.hpp:172-223 (transmission_geometry).
+TransmissionGeometry transmission_geometry(V3 of, V3 inf, const Interface& f) {
+    TransmissionGeometry g{};
+    V3 h{std::fma(f.nie, of.x, f.nte * inf.x), std::fma(f.nie, of.y, f.nte * inf.y),
+         std::fma(f.nie, of.z, f.nte * inf.z)};
+    const float length = std::hypot(std::hypot(h.x, h.y), h.z);
+    if (!std::isfinite(length) || !(length > 0.0F)) {
+        fail("The rough-dielectric transmission half-vector is not normalizable.");
+    }
+    h = scaled_dir(h, 1.0F / length);
+    if (h.z < 0.0F) {
+        h = scaled_dir(h, -1.0F);
+    }
+    if (h.z == 0.0F) {
+        return g;
+    }
+    if (!unit_length(h)) {
+        fail("The rough-dielectric transmission half-vector is not representable.");
+    }
+    const float od = dot(of, h);
+    const float id = dot(inf, h);
+    if (!std::isfinite(od) || !std::isfinite(id)) {
+        fail("The rough-dielectric transmission half-angle cosines are not representable.");
+    }
+    if (!(od > 0.0F) || !(id < 0.0F)) {
+        return g;
+    }
+    if (od > 1.0F || id < -1.0F) {
+        fail("The rough-dielectric transmission half-angle cosines are outside [-1, 1].");
+    }
+    g.valid = true;
+    g.m = h;
+    g.o_dot_m = od;
+    g.i_dot_m = id;
+    g.length = length;
+    return g;
+}
+
+Spectrum scale_spectrum(const Spectrum& c, float scale) {  // RoughDielectric.hpp:88-103
+    Spectrum r{};
+    for (int lane = 0; lane < 4; ++lane) {
+        const float num[2] = {c[lane], scale};
+        const float den[1] = {1.0F};
+        r[lane] = checked_product_ratio(num, 2, den, 1);
+    }
+    return r;
+}
+
+// RoughDielectric.hpp:299-381 (eval, radiance mode).
+Spectrum dielectric_eval(const Closure& c, V3 wo, V3 wi) {
+    Spectrum r{};
+    if (!unit_length(wo) || !unit_length(wi)) {
+        fail("Rough-dielectric directions must be finite unit vectors.");
+    }
+    if (wo.z == 0.0F || wi.z == 0.0F) {
+        return r;
+    }
+    const Ggx g{c.p[2], c.p[3]};
+    const Interface f = interface_for(wo, c.p[0], c.p[1]);
+    const V3 of = scaled_dir(wo, f.face_sign);
+    const V3 inf = scaled_dir(wi, f.face_sign);
+    if (inf.z > 0.0F) {
+        V3 m;
+        float od;
+        half_vector_geometry(of, inf, m, od);
+        const float fr = dielectric_fresnel(od, f.incident_eta, f.transmitted_eta);
+        const float d = ggx_d(g, m);
+        const float g2 = ggx_g2(g, of, inf);
+        const float num[3] = {fr, d, g2};
+        const float den[3] = {4.0F, of.z, inf.z};
+        return scale_spectrum(c.weight, checked_product_ratio(num, 3, den, 3));
+    }
+    const TransmissionGeometry tg = transmission_geometry(of, inf, f);
+    if (!tg.valid) {
+        return r;
+    }
+    const float fr = dielectric_fresnel(tg.o_dot_m, f.incident_eta, f.transmitted_eta);
+    if (fr == 1.0F) {
+        return r;
+    }
+    if (!(tg.length > 0.0F)) {
+        fail("The rough-dielectric transmission Jacobian denominator is zero.");
+    }
+    const float d = ggx_d(g, tg.m);
+    const float g2 = ggx_g2(g, of, scaled_dir(inf, -1.0F));
+    const float eta = f.nie;  // radiance mode
+    const float num[7] = {1.0F - fr, d, g2, eta, eta, tg.o_dot_m, -tg.i_dot_m};
+    const float den[4] = {of.z, -inf.z, tg.length, tg.length};
+    return scale_spectrum(c.weight, checked_product_ratio(num, 7, den, 4));
+}
+
+// RoughDielectric.hpp:383-467 (pdf).
+float dielectric_pdf(const Closure& c, V3 wo, V3 wi) {
+    if (!unit_length(wo) || !unit_length(wi)) {
+        fail("Rough-dielectric directions must be finite unit vectors.");
+    }
+    if (wo.z == 0.0F || wi.z == 0.0F) {
+        return 0.0F;
+    }
+    const Ggx g{c.p[2], c.p[3]};
+    const Interface f = interface_for(wo, c.p[0], c.p[1]);
+    const V3 of = scaled_dir(wo, f.face_sign);
+    const V3 inf = scaled_dir(wi, f.face_sign);
+    if (inf.z > 0.0F) {
+        V3 m;
+        float od;
+        half_vector_geometry(of, inf, m, od);
+        const float fr = dielectric_fresnel(od, f.incident_eta, f.transmitted_eta);
+        const float visible = ggx_vndf_pdf(g, of, m);
+        const float num[2] = {fr, visible};
+        const float den[2] = {4.0F, od};
+        return checked_product_ratio(num, 2, den, 2);
+    }
+    const TransmissionGeometry tg = transmission_geometry(of, inf, f);
+    if (!tg.valid) {
+        return 0.0F;
+    }
+    const float fr = dielectric_fresnel(tg.o_dot_m, f.incident_eta, f.transmitted_eta);
+    if (fr == 1.0F) {
+        return 0.0F;
+    }
+    if (!(tg.length > 0.0F)) {
+        fail("The rough-dielectric transmission Jacobian denominator is zero.");
+    }
+    const float visible = ggx_vndf_pdf(g, of, tg.m);
+    const float num[5] = {1.0F - fr, visible, f.nte, f.nte, -tg.i_dot_m};
+    const float den[2] = {tg.length, tg.length};
+    return checked_product_ratio(num, 5, den, 2);
+}
+
+// RoughDielectric.hpp:469-632 (sample, radiance mode).
+BsdfSample dielectric_sample(const Closure& c, V3 wo, float event, float u, float v) {
+    BsdfSample s;
+    if (!unit_length(wo)) {
+        fail("Rough-dielectric directions must be finite unit vectors.");
+    }
+    if (!(event >= 0.0F && event < 1.0F)) {
+        fail("Rough-dielectric event selection requires a finite sample in [0, 1).");
+    }
+    if (wo.z == 0.0F) {
+        return s;
+    }
+    const Ggx g{c.p[2], c.p[3]};
+    const Interface f = interface_for(wo, c.p[0], c.p[1]);
+    const V3 of = scaled_dir(wo, f.face_sign);
+    V3 m;
+    float vpdf;
+    if (!ggx_sample_vndf(g, of, u, v, m, vpdf)) {
+        return s;
+    }
+    const float od = dot(of, m);
+    if (!std::isfinite(od) || !(od > 0.0F) || od > 1.0F) {
+        fail("The sampled rough-dielectric half-angle cosine is outside [0, 1].");
+    }
+    const float fr = dielectric_fresnel(od, f.incident_eta, f.transmitted_eta);
+    V3 inf;
+    uint32_t lobes;
+    float eta_scale = 1.0F;
+    if (event < fr) {
+        inf = V3{2.0F * od * m.x - of.x, 2.0F * od * m.y - of.y, 2.0F * od * m.z - of.z};
+        lobes = BF200_LOBE_GLOSSY | BF200_LOBE_REFLECTION;
+        if (!unit_length(inf)) {
+            fail("The sampled rough-dielectric reflection direction is not representable.");
+        }
+        if (!(inf.z > 0.0F)) {
+            return s;
+        }
+    } else {
+        const V3 tangent{of.x - od * m.x, of.y - od * m.y, of.z - od * m.z};
+        const float incident_sine = std::hypot(std::hypot(tangent.x, tangent.y), tangent.z);
+        if (!std::isfinite(incident_sine) || incident_sine > 1.0F) {
+            fail("The sampled rough-dielectric incident sine is not representable.");
+        }
+        float incoming_cosine = 1.0F, tangent_scale = 0.0F;
+        if (incident_sine > 0.0F) {
+            float transmitted_sine;
+            if (f.incident_eta > f.transmitted_eta) {
+                const float critical = f.transmitted_eta / f.incident_eta;
+                if (critical == 0.0F || incident_sine >= critical) {
+                    fail("Fresnel selected transmission at total internal reflection.");
+                }
+                transmitted_sine = incident_sine / critical;
+            } else {
+                const float ratio = f.incident_eta / f.transmitted_eta;
+                if (ratio == 0.0F) {
+                    fail("The rough-dielectric refraction ratio is not representable.");
+                }
+                transmitted_sine = ratio * incident_sine;
+            }
+            if (!std::isfinite(transmitted_sine) || !(transmitted_sine < 1.0F)) {
+                fail("A subcritical rough-dielectric transmission sine is not representable.");
+            }
+            incoming_cosine = std::sqrt((1.0F - transmitted_sine) * (1.0F + transmitted_sine));
+            tangent_scale = transmitted_sine / incident_sine;
+            if (!std::isfinite(incoming_cosine) || !(incoming_cosine > 0.0F) ||
+                !std::isfinite(tangent_scale) || !(tangent_scale > 0.0F)) {
+                fail("The sampled rough-dielectric transmission direction is not representable.");
+            }
+        }
+        inf = V3{std::fma(-tangent_scale, tangent.x, -incoming_cosine * m.x),
+                 std::fma(-tangent_scale, tangent.y, -incoming_cosine * m.y),
+                 std::fma(-tangent_scale, tangent.z, -incoming_cosine * m.z)};
+        lobes = BF200_LOBE_GLOSSY | BF200_LOBE_TRANSMISSION;
+        if (!unit_length(inf)) {
+            fail("The sampled rough-dielectric transmission direction is not a unit vector.");
+        }
+        if (!(inf.z < 0.0F)) {
+            return s;
+        }
+        const float num[2] = {f.nte, f.nte};
+        const float den[2] = {f.nie, f.nie};
+        eta_scale = checked_product_ratio(num, 2, den, 2);
+    }
+    const V3 wi = scaled_dir(inf, f.face_sign);
+    s.wi = wi;
+    s.value = dielectric_eval(c, wo, wi);
+    s.pdf = dielectric_pdf(c, wo, wi);
+    s.lobes = lobes;
+    s.eta_scale = eta_scale;
+    s.valid = true;
+    return s;
+}
+
+// DepthFilteredClosureMixture.hpp:48-133: a dielectric restricted to one direction has the
+// branch-conditional pdf base / P(branch).
+float dielectric_pdf_masked(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
+    const float base = dielectric_pdf(c, wo, wi);
+    if (wo.z == 0.0F || wi.z == 0.0F || base == 0.0F) {
+        return base;
+    }
+    const bool reflection = (wo.z > 0.0F) == (wi.z > 0.0F);
+    const uint32_t direction = reflection ? BF200_LOBE_REFLECTION : BF200_LOBE_TRANSMISSION;
+    if ((allowed & direction) == 0U) {
+        return 0.0F;
+    }
+    if (allowed == (BF200_LOBE_REFLECTION | BF200_LOBE_TRANSMISSION)) {
+        return base;
+    }
+    const Interface f = interface_for(wo, c.p[0], c.p[1]);
+    const V3 of = scaled_dir(wo, f.face_sign);
+    const V3 inf = scaled_dir(wi, f.face_sign);
+    float branch;
+    if (reflection) {
+        V3 m;
+        float od;
+        half_vector_geometry(of, inf, m, od);
+        branch = dielectric_fresnel(od, f.incident_eta, f.transmitted_eta);
+    } else {
+        const TransmissionGeometry tg = transmission_geometry(of, inf, f);
+        if (!tg.valid) {
+            return 0.0F;
+        }
+        branch = 1.0F - dielectric_fresnel(tg.o_dot_m, f.incident_eta, f.transmitted_eta);
+    }
+    if (!std::isfinite(branch) || !(branch > 0.0F) || branch > 1.0F) {
+        fail("A filtered rough-dielectric branch probability is not representable.");
+    }
+    const float num[1] = {base};
+    const float den[1] = {branch};
+    return checked_product_ratio(num, 1, den, 1);
+}
+
+Spectrum dielectric_eval_masked(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
+    const Spectrum value = dielectric_eval(c, wo, wi);
+    if (wo.z == 0.0F || wi.z == 0.0F) {
+        return value;
+    }
+    const uint32_t direction =
+        (wo.z > 0.0F) == (wi.z > 0.0F) ? BF200_LOBE_REFLECTION : BF200_LOBE_TRANSMISSION;
+    return (allowed & direction) != 0U ? value : Spectrum{};
+}
+
+// ---------------------------------------------------------------------------------------------
+// Depth limits (PathDepthLimits.cpp) and the single-closure depth filter
+// ---------------------------------------------------------------------------------------------
+
+struct Depth {
+    uint32_t c[5];  // diffuse, glossy, specular, transmission, volume
+    uint32_t total() const { return c[0] + c[1] + c[2] + c[4]; }
+};
+
+uint32_t blocked_limits(const uint32_t* limits, const Depth& d, uint32_t lobes) {
+    uint32_t blocked = 0;
+    if ((lobes & BF200_LOBE_DIFFUSE) && d.c[0] >= limits[0]) blocked |= BF200_LOBE_DIFFUSE;
+    if ((lobes & BF200_LOBE_GLOSSY) && d.c[1] >= limits[1]) blocked |= BF200_LOBE_GLOSSY;
+    if ((lobes & BF200_LOBE_SPECULAR) && d.c[2] >= limits[2]) blocked |= BF200_LOBE_SPECULAR;
+    if ((lobes & BF200_LOBE_TRANSMISSION) && d.c[3] >= limits[3]) blocked |= BF200_LOBE_TRANSMISSION;
+    if ((lobes & BF200_LOBE_VOLUME) && d.c[4] >= limits[4]) blocked |= BF200_LOBE_VOLUME;
+    return blocked;
+}
+
+Depth advanced(const Depth& d, uint32_t lobes) {
+    Depth r = d;
+    if (lobes & BF200_LOBE_DIFFUSE) ++r.c[0];
+    if (lobes & BF200_LOBE_GLOSSY) ++r.c[1];
+    if (lobes & BF200_LOBE_SPECULAR) ++r.c[2];
+    if (lobes & BF200_LOBE_TRANSMISSION) ++r.c[3];
+    if (lobes & BF200_LOBE_VOLUME) ++r.c[4];
+    return r;
+}
+
+struct Filtered {
+    bool active = false;
+    uint32_t allowed = 0;  // direction mask
+    uint32_t blocked = 0;
+};
+
+// DepthFilteredClosureMixture.hpp:262-364 for a one-closure mixture.
+Filtered depth_filter(const Closure& c, const uint32_t* limits, const Depth& d) {
+    Filtered f;
+    auto consider = [&](uint32_t event, uint32_t direction) {
+        const uint32_t b = blocked_limits(limits, d, event);
+        if (b == 0U) {
+            f.allowed |= direction;
+        } else {
+            f.blocked |= b;
+        }
+    };
+    if (c.kind == BF200_CLOSURE_ROUGH_DIELECTRIC) {
+        consider(BF200_LOBE_GLOSSY | BF200_LOBE_REFLECTION, BF200_LOBE_REFLECTION);
+        consider(BF200_LOBE_GLOSSY | BF200_LOBE_TRANSMISSION, BF200_LOBE_TRANSMISSION);
+    } else {
+        consider(c.lobes, c.lobes & (BF200_LOBE_REFLECTION | BF200_LOBE_TRANSMISSION));
+    }
+    f.active = f.allowed != 0U;
+    return f;
+}
+
+Spectrum closure_eval(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
+    switch (c.kind) {
+    case BF200_CLOSURE_LAMBERTIAN_REFLECTION: {  // LambertianReflection.hpp:76-85
+        if (!unit_length(wo) || !unit_length(wi)) {
+            fail("Lambertian directions must be finite unit vectors.");
+        }
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return Spectrum{};
+        }
+        return Spectrum{c.weight[0] * kInvPi, c.weight[1] * kInvPi, c.weight[2] * kInvPi,
+                        c.weight[3] * kInvPi};
+    }
+    case BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION:
+        return conductor_eval(c, wo, wi);
+    case BF200_CLOSURE_ROUGH_DIELECTRIC:
+        return dielectric_eval_masked(c, allowed, wo, wi);
+    default:
+        fail("unsupported closure");
+    }
+}
+
+float closure_pdf(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
+    switch (c.kind) {
+    case BF200_CLOSURE_LAMBERTIAN_REFLECTION: {  // LambertianReflection.hpp:87-106
+        if (!unit_length(wo) || !unit_length(wi)) {
+            fail("Lambertian directions must be finite unit vectors.");
+        }
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return 0.0F;
+        }
+        const float v = wi.z * kInvPi;
+        if (!(v > 0.0F) || !std::isfinite(v)) {
+            fail("Lambertian PDF is not representable for the supplied direction.");
+        }
+        return v;
+    }
+    case BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION:
+        return conductor_pdf(c, wo, wi);
+    case BF200_CLOSURE_ROUGH_DIELECTRIC:
+        return dielectric_pdf_masked(c, allowed, wo, wi);
+    default:
+        fail("unsupported closure");
+    }
+}
+
+// DepthFilteredClosureMixture.hpp:460-552 for one active closure: the event sample is the
+// component sample itself; dielectric directions restricted by the depth filter are forced.
+BsdfSample closure_sample(const Closure& c, uint32_t allowed, V3 wo, float component, float u,
+                          float v) {
+    if (!unit_length(wo)) {
+        fail("Closure sampling requires a finite unit direction.");
+    }
+    switch (c.kind) {
+    case BF200_CLOSURE_LAMBERTIAN_REFLECTION: {  // LambertianReflection.hpp:108-140
+        BsdfSample s;
+        const V3 wi = map_cosine_hemisphere(u, v);
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return s;
+        }
+        s.wi = wi;
+        s.value = closure_eval(c, allowed, wo, wi);
+        s.pdf = closure_pdf(c, allowed, wo, wi);
+        s.lobes = c.lobes;
+        s.valid = true;
+        return s;
+    }
+    case BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION:
+        return conductor_sample(c, wo, u, v);
+    case BF200_CLOSURE_ROUGH_DIELECTRIC: {  // DepthFilteredClosureMixture.hpp:135-180
+        float event = component;
+        if (allowed == BF200_LOBE_REFLECTION) {
+            event = 0.0F;
+        } else if (allowed == BF200_LOBE_TRANSMISSION) {
+            event = std::nextafter(1.0F, 0.0F);
+        }
+        BsdfSample s = dielectric_sample(c, wo, event, u, v);
+        if (!s.valid) {
+            return s;
+        }
+        if ((s.lobes & allowed) == 0U) {
+            return BsdfSample{};
+        }
+        s.pdf = dielectric_pdf_masked(c, allowed, wo, s.wi);
+        return s;
+    }
+    default:
+        fail("unsupported closure");
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Surface reconstruction (SceneSurfaceInteraction.cpp:54-350, 804-937)
+// ---------------------------------------------------------------------------------------------
+
+struct Surface {
+    V3 position, error, ng, ns;
+    Frame frame;
+    const Material* material;
+};
+
+Surface resolve_surface(const Scene& scene, const Hit& hit) {
+    Surface s{};
+    const Instance& inst = scene.instances[hit.instance];
+    const auto& g = scene.geometries[inst.geometry];
+    s.material = &scene.materials[inst.material];
+    // validate_barycentrics (:54-76)
+    constexpr float tolerance = 32.0F * kEpsilon;
+    const float bs[3] = {hit.b0, hit.b1, hit.b2};
+    for (float b : bs) {
+        if (!std::isfinite(b) || b < -tolerance || b > 1.0F + tolerance) {
+            fail("An acceleration hit contains invalid triangle barycentric coordinates.");
+        }
+    }
+    const float sum = bs[0] + bs[1] + bs[2];
+    if (!std::isfinite(sum) || std::abs(sum - 1.0F) > tolerance) {
+        fail("An acceleration hit contains barycentric coordinates that do not sum to one.");
+    }
+    const uint32_t* tri = &scene.triangles[3 * (g.triangle_offset + hit.primitive)];
+    V3 op[3], on[3];
+    for (int k = 0; k < 3; ++k) {
+        op[k] = scene.positions[g.vertex_offset + tri[k]];
+        on[k] = scene.normals[g.vertex_offset + tri[k]];
+    }
+    // interpolate_position_with_error (:82-133)
+    constexpr float gamma7 = (7.0F * kEpsilon) / (1.0F - 7.0F * kEpsilon);
+    float scale = 0.0F;
+    const float coords[3][3] = {{op[0].x, op[0].y, op[0].z}, {op[1].x, op[1].y, op[1].z},
+                                {op[2].x, op[2].y, op[2].z}};
+    for (int axis = 0; axis < 3; ++axis) {
+        scale = std::max({scale, std::abs(coords[1][axis] - coords[0][axis]),
+                          std::abs(coords[2][axis] - coords[0][axis])});
+    }
+    const float floor_error = kEpsilon * scale;
+    if (!std::isfinite(scale) || !std::isfinite(floor_error) || !(floor_error > 0.0F)) {
+        fail("A scene triangle position-error scale is not representable.");
+    }
+    float point[3], perr[3];
+    for (int axis = 0; axis < 3; ++axis) {
+        const float p0 = bs[0] * coords[0][axis], p1 = bs[1] * coords[1][axis],
+                    p2 = bs[2] * coords[2][axis];
+        point[axis] = std::fma(bs[0], coords[0][axis], std::fma(bs[1], coords[1][axis], p2));
+        const float magnitude = std::abs(p0) + std::abs(p1) + std::abs(p2);
+        perr[axis] = std::max(gamma7 * magnitude, floor_error);
+    }
+    // transform_position_with_error (:135-189)
+    const V3 object_point{point[0], point[1], point[2]};
+    const V3 world = transform_point(inst.to_world, object_point);
+    {
+        const float src[3] = {point[0], point[1], point[2]};
+        const float w[3] = {world.x, world.y, world.z};
+        const float h[3] = {hit.position.x, hit.position.y, hit.position.z};
+        constexpr double eps = static_cast<double>(kEpsilon);
+        constexpr double g7 = (7.0 * eps) / (1.0 - 7.0 * eps);
+        constexpr double maximum = static_cast<double>(std::numeric_limits<float>::max());
+        float err[3];
+        for (int row = 0; row < 3; ++row) {
+            double magnitude = std::abs(static_cast<double>(inst.to_world(row, 3)));
+            double propagated = 0.0;
+            for (int col = 0; col < 3; ++col) {
+                const double coefficient = std::abs(static_cast<double>(inst.to_world(row, col)));
+                magnitude += coefficient * std::abs(static_cast<double>(src[col]));
+                propagated += coefficient * static_cast<double>(perr[col]);
+            }
+            const double discrepancy = std::abs(static_cast<double>(w[row]) - static_cast<double>(h[row]));
+            const double bound = g7 * magnitude + (1.0 + g7) * propagated + discrepancy;
+            if (!std::isfinite(bound) || bound < 0.0 || bound > maximum) {
+                fail("A transformed scene triangle position error is not representable.");
+            }
+            err[row] = static_cast<float>(bound);
+            if (static_cast<double>(err[row]) < bound) {
+                err[row] = std::nextafter(err[row], kInfinity);
+            }
+        }
+        s.error = V3{err[0], err[1], err[2]};
+    }
+    s.position = world;
+    s.ng = hit.normal;
+    // interpolate_shading_normal (:305-349) with robust_transformed_normal (:252-295)
+    const V3 obj_n{std::fma(bs[0], on[0].x, std::fma(bs[1], on[1].x, bs[2] * on[2].x)),
+                   std::fma(bs[0], on[0].y, std::fma(bs[1], on[1].y, bs[2] * on[2].y)),
+                   std::fma(bs[0], on[0].z, std::fma(bs[1], on[1].z, bs[2] * on[2].z))};
+    const Mat4& inv = inst.to_object;
+    const double n[3] = {obj_n.x, obj_n.y, obj_n.z};
+    const double tr[3] = {
+        std::fma(double(inv(0, 0)), n[0], std::fma(double(inv(1, 0)), n[1], double(inv(2, 0)) * n[2])),
+        std::fma(double(inv(0, 1)), n[0], std::fma(double(inv(1, 1)), n[1], double(inv(2, 1)) * n[2])),
+        std::fma(double(inv(0, 2)), n[0], std::fma(double(inv(1, 2)), n[1], double(inv(2, 2)) * n[2]))};
+    const double mc = std::max({std::abs(tr[0]), std::abs(tr[1]), std::abs(tr[2])});
+    if (!std::isfinite(mc) || mc == 0.0) {
+        fail("A scene shading normal cannot be normalized.");
+    }
+    const double sc[3] = {tr[0] / mc, tr[1] / mc, tr[2] / mc};
+    const double magnitude = std::sqrt(std::fma(sc[0], sc[0], std::fma(sc[1], sc[1], sc[2] * sc[2])));
+    V3 ns{static_cast<float>(sc[0] / magnitude), static_cast<float>(sc[1] / magnitude),
+          static_cast<float>(sc[2] / magnitude)};
+    // transform_orientation (:204-250): sign of det of the upper 3x3 by partial pivoting.
+    {
+        double m[9];
+        for (int r = 0; r < 3; ++r) {
+            for (int c = 0; c < 3; ++c) {
+                m[r * 3 + c] = static_cast<double>(inst.to_world(r, c));
+            }
+        }
+        int orientation = 1;
+        for (int col = 0; col < 3; ++col) {
+            int pr = col;
+            double pm = std::abs(m[col * 3 + col]);
+            for (int cand = col + 1; cand < 3; ++cand) {
+                const double cm = std::abs(m[cand * 3 + col]);
+                if (cm > pm) {
+                    pm = cm;
+                    pr = cand;
+                }
+            }
+            if (!std::isfinite(pm) || pm == 0.0) {
+                fail("A scene instance transform orientation is not representable.");
+            }
+            if (pr != col) {
+                for (int sc2 = col; sc2 < 3; ++sc2) {
+                    std::swap(m[col * 3 + sc2], m[pr * 3 + sc2]);
+                }
+                orientation = -orientation;
+            }
+            const double pivot = m[col * 3 + col];
+            orientation = pivot < 0.0 ? -orientation : orientation;
+            for (int row = col + 1; row < 3; ++row) {
+                const double factor = m[row * 3 + col] / pivot;
+                for (int uc = col + 1; uc < 3; ++uc) {
+                    m[row * 3 + uc] -= factor * m[col * 3 + uc];
+                }
+            }
+        }
+        if (orientation < 0) {
+            ns = -ns;
+        }
+    }
+    if (!(dot(s.ng, ns) > 0.0F)) {
+        fail("A scene shading normal lies outside the geometric-normal hemisphere.");
+    }
+    s.ns = ns;
+    if (s.material->frame_mode != 0) {
+        fail("surface-tangent closure frames are not part of this restatement");
+    }
+    s.frame = rotated_about_normal(frame_from_normal(ns), s.material->rotation);
+    return s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The path loop (SceneMisPathLoop.cpp:632-917)
+// ---------------------------------------------------------------------------------------------
+
+struct Options {
+    uint32_t heuristic;
+    uint32_t limits[5];
+    bool roulette;
+    uint32_t roulette_first;
+    float roulette_min, roulette_max;
+};
+
+struct PrevBsdf {
+    bool valid = false;
+    V3 position;
+    float pdf;
+    V3 direction;
+};
+
+void add_spectrum_product(Spectrum& acc, const Spectrum& a, const Spectrum& b) {
+    // accumulate_emission (BsdfOnlyPathLoop.hpp:148-168) with checked_product (:47-62).
+    for (int lane = 0; lane < 4; ++lane) {
+        const float product = a[lane] * b[lane];
+        if (!std::isfinite(product) || (a[lane] != 0.0F && b[lane] != 0.0F && product == 0.0F)) {
+            fail("Emitted-radiance multiplication is not representable.");
+        }
+        acc[lane] = acc[lane] + product;
+        if (!std::isfinite(acc[lane])) {
+            fail("Radiance accumulation is not representable.");
+        }
+    }
+}
+
+// SceneMisPathLoop.cpp:481-528 (accumulate_weighted_emission).
+void add_weighted_emission(Spectrum& acc, const Spectrum& beta, const Spectrum& le, float w) {
+    if (!std::isfinite(w) || w < 0.0F || w > 1.0F) {
+        fail("An emitted-radiance MIS weight must lie in [0, 1].");
+    }
+    if (w == 1.0F) {
+        add_spectrum_product(acc, beta, le);
+        return;
+    }
+    for (int lane = 0; lane < 4; ++lane) {
+        if (beta[lane] == 0.0F || le[lane] == 0.0F || w == 0.0F) {
+            continue;
+        }
+        int e1 = 0, e2 = 0, e3 = 0, en = 0;
+        const float significand = std::frexp(beta[lane], &e1) * std::frexp(le[lane], &e2) *
+                                  std::frexp(w, &e3);
+        const float normalized = std::frexp(significand, &en);
+        const float contribution = std::scalbn(normalized, e1 + e2 + e3 + en);
+        if (!std::isfinite(contribution) || !(contribution > 0.0F)) {
+            fail("A weighted emitted-radiance contribution is not representable.");
+        }
+        acc[lane] = acc[lane] + contribution;
+        if (!std::isfinite(acc[lane])) {
+            fail("MIS radiance accumulation is not representable.");
+        }
+    }
+}
+
+// LightSampler.cpp:1023-1056 (uniform sample) and :1133-1149 (probability).
+uint32_t select_light(const Scene& scene, float u, float& probability) {
+    const auto begin = scene.light_cdf.begin() + 1;
+    const auto it = std::upper_bound(begin, scene.light_cdf.end(), u);
+    if (it == scene.light_cdf.end()) {
+        fail("Light-selection CDF could not classify a canonical sample.");
+    }
+    const size_t index = static_cast<size_t>(it - scene.light_cdf.begin()) - 1;
+    probability = scene.light_cdf[index + 1] - scene.light_cdf[index];
+    return static_cast<uint32_t>(index);
+}
+
+float light_probability(const Scene& scene, uint32_t index) {
+    return scene.light_cdf[index + 1] - scene.light_cdf[index];
+}
+
+// RussianRoulette.cpp (evaluate): returns false when the path terminates.
+bool russian_roulette(Spectrum& beta, float eta_scale, float u, const Options& o) {
+    float maximum_throughput = 0.0F;
+    for (float lane : beta) {
+        if (!std::isfinite(lane) || lane < 0.0F) {
+            fail("Russian roulette throughput must be finite and non-negative.");
+        }
+        maximum_throughput = std::max(maximum_throughput, lane);
+    }
+    if (maximum_throughput == 0.0F) {
+        fail("Russian roulette cannot evaluate an all-zero continuation throughput.");
+    }
+    float survival;
+    if (maximum_throughput >= o.roulette_max / eta_scale) {
+        survival = o.roulette_max;
+    } else if (maximum_throughput <= o.roulette_min / eta_scale) {
+        survival = o.roulette_min;
+    } else {
+        survival = std::clamp(maximum_throughput * eta_scale, o.roulette_min, o.roulette_max);
+    }
+    if (!(u < survival)) {
+        return false;
+    }
+    for (int lane = 0; lane < 4; ++lane) {
+        const float c = beta[lane] / survival;
+        if (!std::isfinite(c) || (beta[lane] != 0.0F && c == 0.0F)) {
+            fail("Russian roulette compensation is not representable.");
+        }
+        beta[lane] = c;
+    }
+    return true;
+}
+
+// ShadingNormalCorrection.hpp:65-121 in radiance mode: 1 when both directions lie on the same
+// side of both normals, otherwise 0.
+float shading_correction(V3 ng, V3 ns, V3 wo, V3 wi) {
+    const float og = dot(ng, wo), os = dot(ns, wo), ig = dot(ng, wi), is = dot(ns, wi);
+    if (og == 0.0F || os == 0.0F || ig == 0.0F || is == 0.0F ||
+        std::signbit(og) != std::signbit(os) || std::signbit(ig) != std::signbit(is)) {
+        return 0.0F;
+    }
+    return 1.0F;
+}
+
+struct PathOut {
+    Spectrum beta, radiance;
+    Depth depth;
+    float eta_scale;
+    uint32_t delta_flags, termination, blocked, segments;
+    V3 ray_o, ray_d;
+    float ray_tmin, ray_tmax;
+};
+
+// SceneMisPathLoop.cpp:129-275 (estimate): returns the unoccluded-tested direct contribution.
+Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& surf,
+                         const Closure& closure, uint32_t allowed, const Spectrum& beta, V3 wo_world,
+                         const Dims& dims, const Stream& stream, uint32_t mask, float time) {
+    const Spectrum zero{};
+    if (is_black(beta) || is_black(closure.weight)) {
+        return zero;
+    }
+    float selection;
+    const uint32_t light_index = select_light(scene, stream.sample_1d(dims.light_selection), selection);
+    const MeshLight& light = scene.lights[light_index];
+    if ((scene.instances[light.instance].mask & mask) == 0U) {
+        return zero;
+    }
+    const LightSample ls = sample_mesh_light(light, surf.position, stream.sample_1d(dims.light_u),
+                                             stream.sample_1d(dims.light_v));
+    if (!ls.valid) {
+        return zero;
+    }
+    const V3 wo = surf.frame.to_local(wo_world);
+    const V3 wi = surf.frame.to_local(ls.direction);
+    if (wo.z == 0.0F || wi.z == 0.0F) {
+        return zero;
+    }
+    const bool lambert = closure.kind == BF200_CLOSURE_LAMBERTIAN_REFLECTION;
+    Spectrum f{};
+    if (!lambert) {
+        f = closure_eval(closure, allowed, wo, wi);
+        if (is_black(f)) {
+            return zero;
+        }
+    }
+    const float correction = shading_correction(surf.ng, surf.ns, wo_world, ls.direction);
+    if (correction == 0.0F) {
+        return zero;
+    }
+    const float bsdf_pdf = closure_pdf(closure, allowed, wo, wi);
+    const float light_pdf = joint_light_pdf(selection, ls.pdf);
+    const float weight = mis_weight(opt.heuristic, light_pdf, bsdf_pdf);
+    // make_shadow_ray (ShadowRay.hpp:181-253) for a finite surface endpoint.
+    const V3 origin = offset_surface_point(surf.position, surf.error, surf.ng, ls.direction);
+    const V3 endpoint = offset_surface_point(ls.position, ls.error, ls.normal, origin - ls.position);
+    V3 sd;
+    float length;
+    unit_segment(origin, endpoint, ls.direction, sd, length);
+    const float t_max = std::nextafter(length, 0.0F);
+    if (!(t_max > 0.0F) || !std::isfinite(t_max)) {
+        fail("A finite shadow-ray interval is not representable in the requested precision.");
+    }
+    (void)time;
+    const bool blocked = occluded(scene, origin, sd, 0.0F, t_max, mask);
+    const float transmittance = blocked ? 0.0F : 1.0F;
+    Spectrum out{};
+    for (int lane = 0; lane < 4; ++lane) {
+        if (lambert) {
+            // evaluate_lambertian_direct_lighting (DirectLighting.hpp:171-236)
+            if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+                return zero;
+            }
+            if (weight == 1.0F) {
+                const float num[6] = {beta[lane], closure.weight[lane], kInvPi, ls.radiance[lane], wi.z,
+                                      transmittance};
+                const float den[2] = {selection, ls.pdf};
+                out[lane] = checked_product_quotient(num, 6, den, 2);
+            } else {
+                const float num[7] = {beta[lane], closure.weight[lane], kInvPi, ls.radiance[lane], wi.z,
+                                      transmittance, weight};
+                const float den[2] = {selection, ls.pdf};
+                out[lane] = checked_product_quotient(num, 7, den, 2);
+            }
+        } else {
+            // evaluate_bsdf_direct_lighting (DirectLighting.hpp:66-145)
+            const float cosine = std::abs(wi.z);
+            if (weight == 1.0F) {
+                const float num[5] = {beta[lane], f[lane], ls.radiance[lane], cosine, transmittance};
+                const float den[2] = {selection, ls.pdf};
+                out[lane] = checked_product_quotient(num, 5, den, 2);
+            } else {
+                const float num[6] = {beta[lane], f[lane], ls.radiance[lane], cosine, transmittance,
+                                      weight};
+                const float den[2] = {selection, ls.pdf};
+                out[lane] = checked_product_quotient(num, 6, den, 2);
+            }
+        }
+        out[lane] = out[lane] * correction;
+    }
+    return out;
+}
+
+PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Options& opt) {
+    PathOut out{};
+    out.beta = Spectrum{1.0F, 1.0F, 1.0F, 1.0F};
+    out.radiance = Spectrum{};
+    out.depth = Depth{{0, 0, 0, 0, 0}};
+    out.eta_scale = 1.0F;
+    out.delta_flags = 0;
+    out.blocked = 0;
+    out.segments = 0;
+    const Stream stream{input.sample.pixel_x, input.sample.pixel_y, input.sample.sample_index,
+                        input.sample.seed};
+    V3 ro{input.primary_ray.origin[0], input.primary_ray.origin[1], input.primary_ray.origin[2]};
+    V3 rd{input.primary_ray.direction[0], input.primary_ray.direction[1],
+          input.primary_ray.direction[2]};
+    float tmin = input.primary_ray.t_min, tmax = input.primary_ray.t_max;
+    const uint32_t mask = input.primary_ray.mask;
+    const float time = input.primary_ray.time;
+    PrevBsdf prev;
+    auto finish = [&](uint32_t termination) {
+        out.termination = termination;
+        out.ray_o = ro;
+        out.ray_d = rd;
+        out.ray_tmin = tmin;
+        out.ray_tmax = tmax;
+        return out;
+    };
+    while (true) {
+        Hit hit{};
+        ++out.segments;
+        if (!closest_hit(scene, ro, rd, tmin, tmax, mask, hit)) {
+            add_spectrum_product(out.radiance, out.beta, scene.environment);
+            return finish(BF200_TERMINATION_ESCAPED_ENVIRONMENT);
+        }
+        const Surface surf = resolve_surface(scene, hit);
+        const Material& material = *surf.material;
+        // Surface emission and its MIS weight (SceneMisPathLoop.cpp:277-356).
+        Spectrum emitted{};
+        if (emission_side(surf.ng, -rd) > 0) {
+            emitted = material.emission;
+        }
+        float emission_weight = 1.0F;
+        if (!is_black(emitted) && prev.valid) {
+            if (rd != prev.direction) {
+                fail("The emissive hit direction does not match the recorded BSDF sample.");
+            }
+            const int32_t light_index = scene.light_of_instance[hit.instance];
+            if (light_index < 0) {
+                fail("A non-black emissive hit is absent from the committed mesh-light registry.");
+            }
+            const float selection = light_probability(scene, static_cast<uint32_t>(light_index));
+            const float conditional = mesh_light_pdf_at_surface(scene.lights[light_index], prev.position,
+                                                                surf.position, surf.ng);
+            const float light_pdf = joint_light_pdf(selection, conditional);
+            emission_weight = mis_weight(opt.heuristic, prev.pdf, light_pdf);
+        }
+        add_weighted_emission(out.radiance, out.beta, emitted, emission_weight);
+        if (is_black(out.beta)) {
+            return finish(BF200_TERMINATION_ZERO_THROUGHPUT);
+        }
+        if (material.closure_count != 1) {
+            if (material.closure_count == 0) {
+                return finish(BF200_TERMINATION_OUTSIDE_BSDF_SUPPORT);
+            }
+            fail("multi-closure mixtures are not part of this restatement");
+        }
+        const Closure& closure = material.closure;
+        const Filtered filtered = depth_filter(closure, opt.limits, out.depth);
+        if (!filtered.active) {
+            out.blocked = filtered.blocked;
+            return finish(BF200_TERMINATION_DEPTH_LIMIT);
+        }
+        const V3 wo_world = robust_unit(-rd);
+        const V3 wo = surf.frame.to_local(wo_world);
+        const Dims dims = dims_for_bounce(out.depth.total());
+        const float bu = stream.sample_1d(dims.bsdf_u);
+        const float bv = stream.sample_1d(dims.bsdf_v);
+        const float bc = stream.sample_1d(dims.bsdf_component);
+        const BsdfSample bs = closure_sample(closure, filtered.allowed, wo, bc, bu, bv);
+        Depth next_depth = out.depth;
+        if (bs.valid) {
+            if (!std::isfinite(bs.pdf) || !(bs.pdf > 0.0F) || bs.wi.z == 0.0F) {
+                fail("The closure mixture returned an invalid MIS continuation sample.");
+            }
+            if (blocked_limits(opt.limits, out.depth, bs.lobes) != 0U) {
+                fail("A depth-filtered closure selected a blocked MIS continuation event.");
+            }
+            next_depth = advanced(out.depth, bs.lobes);
+        }
+        const Spectrum direct = direct_lighting(scene, opt, surf, closure, filtered.allowed, out.beta,
+                                                wo_world, dims, stream, mask, time);
+        for (int lane = 0; lane < 4; ++lane) {
+            if (!std::isfinite(direct[lane]) || direct[lane] < 0.0F) {
+                fail("A direct-lighting contribution must be finite and non-negative.");
+            }
+            out.radiance[lane] = out.radiance[lane] + direct[lane];
+        }
+        if (!bs.valid) {
+            return finish(BF200_TERMINATION_OUTSIDE_BSDF_SUPPORT);
+        }
+        const V3 wi_world = robust_unit(surf.frame.to_world(bs.wi));
+        const float correction = shading_correction(surf.ng, surf.ns, wo_world, wi_world);
+        if (correction == 0.0F) {
+            return finish(BF200_TERMINATION_OUTSIDE_BSDF_SUPPORT);
+        }
+        // update_closure_throughput (BsdfOnlyPathLoop.hpp:64-131)
+        Spectrum next_beta{};
+        const float cosine = std::abs(bs.wi.z);
+        if (closure.kind == BF200_CLOSURE_LAMBERTIAN_REFLECTION && correction == 1.0F) {
+            for (int lane = 0; lane < 4; ++lane) {
+                next_beta[lane] = out.beta[lane] * closure.weight[lane];
+                if (!std::isfinite(next_beta[lane]) ||
+                    (out.beta[lane] != 0.0F && closure.weight[lane] != 0.0F && next_beta[lane] == 0.0F)) {
+                    fail("Lambertian path throughput is not representable.");
+                }
+            }
+        } else {
+            for (int lane = 0; lane < 4; ++lane) {
+                const float num[4] = {out.beta[lane], bs.value[lane], cosine, correction};
+                float significand = 1.0F;
+                int exponent = 0;
+                bool zero = false;
+                for (float factor : num) {
+                    if (!std::isfinite(factor) || factor < 0.0F) {
+                        fail("Closure factors must be finite and non-negative.");
+                    }
+                    if (factor == 0.0F) {
+                        zero = true;
+                        break;
+                    }
+                    int fe = 0;
+                    significand *= std::frexp(factor, &fe);
+                    exponent += fe;
+                }
+                if (zero) {
+                    next_beta[lane] = 0.0F;
+                    continue;
+                }
+                int pe = 0, ne = 0;
+                significand /= std::frexp(bs.pdf, &pe);
+                exponent -= pe;
+                significand = std::frexp(significand, &ne);
+                const float value = std::scalbn(significand, exponent + ne);
+                if (!std::isfinite(value) || !(value > 0.0F)) {
+                    fail("Closure throughput is not representable.");
+                }
+                next_beta[lane] = value;
+            }
+        }
+        const float next_eta = out.eta_scale * bs.eta_scale;
+        if (!std::isfinite(next_eta) || !(next_eta > 0.0F)) {
+            fail("A closure eta-scale update is not representable.");
+        }
+        const V3 origin = offset_ray_origin(surf.position, surf.error, surf.ng, wi_world);
+        if (origin == surf.position) {
+            fail("The derived triangle error did not move the MIS continuation-ray origin.");
+        }
+        // record_bsdf_sample (SceneMisPathLoop.cpp:358-390): continuous lobes only here.
+        prev.valid = true;
+        prev.position = surf.position;
+        prev.pdf = bs.pdf;
+        prev.direction = wi_world;
+        out.beta = next_beta;
+        out.depth = next_depth;
+        out.eta_scale = next_eta;
+        out.delta_flags = 2U;  // any_non_delta_bounces (continuous lobes only)
+        ro = origin;
+        rd = wi_world;
+        tmin = 0.0F;
+        tmax = kInfinity;
+        if (is_black(out.beta)) {
+            return finish(BF200_TERMINATION_ZERO_THROUGHPUT);
+        }
+        if (opt.roulette && out.depth.total() >= opt.roulette_first) {
+            if (!russian_roulette(out.beta, out.eta_scale, stream.sample_1d(dims.russian_roulette), opt)) {
+                return finish(BF200_TERMINATION_RUSSIAN_ROULETTE);
+            }
+        }
+    }
+}
+
+std::mutex g_error_mutex;
+std::string g_error;
+
+void set_error(const char* message) {
+    std::lock_guard<std::mutex> lock{g_error_mutex};
+    g_error = message;
+}
+
+Options make_options(const bf200_transport_options_v1& o) {
+    Options r{};
+    r.heuristic = o.mis_heuristic;
+    for (int i = 0; i < 5; ++i) {
+        r.limits[i] = o.depth_limits[i];
+    }
+    r.roulette = o.roulette_enabled != 0;
+    r.roulette_first = o.roulette_first_eligible_depth;
+    r.roulette_min = o.roulette_minimum_survival;
+    r.roulette_max = o.roulette_maximum_survival;
+    return r;
+}
+
+void store_result(const PathOut& p, bf200_path_result_v1& r, float time, uint32_t mask) {
+    std::memset(&r, 0, sizeof(r));
+    for (int lane = 0; lane < 4; ++lane) {
+        r.beta[lane] = p.beta[lane];
+        r.radiance[lane] = p.radiance[lane];
+    }
+    r.depth = p.depth.total();
+    for (int i = 0; i < 5; ++i) {
+        r.depth_counters[i] = p.depth.c[i];
+    }
+    r.eta_scale = p.eta_scale;
+    r.delta_flags = p.delta_flags;
+    r.termination = p.termination;
+    r.blocked_depth_limits = p.blocked;
+    r.lane_status = BF200_LANE_OK;
+    r.segments = p.segments;
+    r.terminal_ray.origin[0] = p.ray_o.x;
+    r.terminal_ray.origin[1] = p.ray_o.y;
+    r.terminal_ray.origin[2] = p.ray_o.z;
+    r.terminal_ray.direction[0] = p.ray_d.x;
+    r.terminal_ray.direction[1] = p.ray_d.y;
+    r.terminal_ray.direction[2] = p.ray_d.z;
+    r.terminal_ray.t_min = p.ray_tmin;
+    r.terminal_ray.t_max = p.ray_tmax;
+    r.terminal_ray.time = time;
+    r.terminal_ray.mask = mask;
+}
+
+}  // namespace
+}  // namespace bfo
+
+using namespace bfo;
+
+extern "C" {
+
+__attribute__((visibility("default"))) const char* bfo_last_error() { return g_error.c_str(); }
+
+__attribute__((visibility("default"))) int bfo_scene_create(const bf200_scene_desc_v1* d, void** out) {
+    try {
+        auto* s = new Scene{};
+        s->geometries.assign(d->geometries, d->geometries + d->geometry_count);
+        for (uint32_t v = 0; v < d->vertex_count; ++v) {
+            s->positions.push_back(load3(d->positions, v));
+            s->normals.push_back(load3(d->normals, v));
+        }
+        s->uvs.assign(d->texture_coordinates, d->texture_coordinates + 2 * d->vertex_count);
+        s->triangles.assign(d->triangles, d->triangles + 3 * d->triangle_count);
+        for (uint32_t m = 0; m < d->material_count; ++m) {
+            const auto& src = d->materials[m];
+            Material mat{};
+            mat.closure_count = src.closure_count;
+            mat.frame_mode = src.frame_mode;
+            mat.rotation = src.tangent_rotation_radians;
+            for (int lane = 0; lane < 4; ++lane) {
+                mat.emission[lane] = src.emitted_radiance[lane];
+            }
+            if (src.closure_count >= 1) {
+                const auto& c = d->closures[src.closure_offset];
+                mat.closure.kind = c.kind;
+                mat.closure.lobes = c.lobes;
+                for (int lane = 0; lane < 4; ++lane) {
+                    mat.closure.weight[lane] = c.weight[lane];
+                }
+                std::memcpy(mat.closure.p, c.parameters, sizeof(mat.closure.p));
+            }
+            s->materials.push_back(mat);
+        }
+        for (uint32_t i = 0; i < d->instance_count; ++i) {
+            const auto& src = d->instances[i];
+            Instance inst{};
+            inst.geometry = src.geometry_index;
+            inst.material = src.material_index;
+            inst.mask = src.visibility_mask;
+            inst.instance_id = src.instance_id;
+            std::memcpy(inst.to_world.m, src.object_to_world, sizeof(inst.to_world.m));
+            std::memcpy(inst.to_object.m, src.world_to_object, sizeof(inst.to_object.m));
+            const auto& g = s->geometries[inst.geometry];
+            for (uint32_t t = 0; t < g.triangle_count; ++t) {
+                const uint32_t* tri = &s->triangles[3 * (g.triangle_offset + t)];
+                V3 w[3];
+                for (int k = 0; k < 3; ++k) {
+                    w[k] = transform_point(inst.to_world, s->positions[g.vertex_offset + tri[k]]);
+                    inst.world_vertices.push_back(w[k]);
+                }
+                V3 n;
+                if (!triangle_normal(w[0], w[1], w[2], n)) {
+                    set_error("A world-space triangle normal is not representable.");
+                    delete s;
+                    return 2;
+                }
+                inst.world_normals.push_back(n);
+            }
+            s->instances.push_back(std::move(inst));
+        }
+        // Mesh-light registry (FrameScene.cpp:201-261): one light per emissive instance.
+        s->light_of_instance.assign(d->instance_count, -1);
+        for (uint32_t i = 0; i < d->instance_count; ++i) {
+            const Material& mat = s->materials[s->instances[i].material];
+            if (is_black(mat.emission)) {
+                continue;
+            }
+            MeshLight light{};
+            light.instance = i;
+            if (!transform_mesh_positions(*s, s->instances[i], light)) {
+                set_error("An emissive mesh world position is not representable.");
+                delete s;
+                return 3;
+            }
+            const auto& g = s->geometries[s->instances[i].geometry];
+            light.tris.assign(&s->triangles[3 * g.triangle_offset],
+                              &s->triangles[3 * (g.triangle_offset + g.triangle_count)]);
+            if (!build_mesh_light(light)) {
+                set_error("A mesh area light could not be built.");
+                delete s;
+                return 4;
+            }
+            light.radiance = mat.emission;
+            s->light_of_instance[i] = static_cast<int32_t>(s->lights.size());
+            s->lights.push_back(std::move(light));
+        }
+        // LightSampler::create_uniform (LightSampler.cpp:574-602).
+        const size_t count = s->lights.size();
+        if (count == 0) {
+            set_error("MIS requires at least one emissive mesh light.");
+            delete s;
+            return 5;
+        }
+        s->light_cdf.assign(count + 1, 0.0F);
+        for (size_t k = 1; k < count; ++k) {
+            s->light_cdf[k] = static_cast<float>(k) / static_cast<float>(count);
+        }
+        s->light_cdf[count] = 1.0F;
+        for (int lane = 0; lane < 4; ++lane) {
+            s->environment[lane] = d->environment_radiance[lane];
+            s->nm[lane] = d->wavelength_nanometers[lane];
+            s->pdf[lane] = d->wavelength_pdf[lane];
+        }
+        *out = s;
+        return 0;
+    } catch (const Failure& f) {
+        set_error(f.message);
+        return 1;
+    }
+}
+
+__attribute__((visibility("default"))) void bfo_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
+
+__attribute__((visibility("default"))) void bfo_scene_set_prefilter(void* s, int enabled) {
+    static_cast<Scene*>(s)->prefilter = enabled != 0;
+}
+
+// Writes the world-space geometric normal of (instance, primitive) as the backend resolves it.
+__attribute__((visibility("default"))) int bfo_scene_world_normal(void* h, uint32_t instance,
+                                                                  uint32_t primitive, float* out3) {
+    const auto* s = static_cast<Scene*>(h);
+    if (instance >= s->instances.size() || primitive >= s->instances[instance].world_normals.size()) {
+        return 1;
+    }
+    const V3 n = s->instances[instance].world_normals[primitive];
+    out3[0] = n.x;
+    out3[1] = n.y;
+    out3[2] = n.z;
+    return 0;
+}
+
+// Traces paths; returns how many failed (lane_status 1, first message in bfo_last_error()).
+__attribute__((visibility("default"))) int64_t bfo_trace_paths(void* h, const bf200_path_input_v1* in,
+                                                               uint64_t n,
+                                                               const bf200_transport_options_v1* o,
+                                                               bf200_path_result_v1* res, int threads) {
+    const auto* s = static_cast<Scene*>(h);
+    const Options opt = make_options(*o);
+    std::atomic<uint64_t> next{0};
+    std::atomic<int64_t> failures{0};
+    auto worker = [&] {
+        for (uint64_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {
+            try {
+                const PathOut p = trace(*s, in[i], opt);
+                store_result(p, res[i], in[i].primary_ray.time, in[i].primary_ray.mask);
+            } catch (const Failure& f) {
+                std::memset(&res[i], 0, sizeof(res[i]));
+                res[i].lane_status = BF200_LANE_NUMERICAL_FAILURE;
+                if (failures.fetch_add(1) == 0) {
+                    set_error(f.message);
+                }
+            }
+        }
+    };
+    if (threads <= 1) {
+        worker();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; ++t) {
+            pool.emplace_back(worker);
+        }
+        for (auto& t : pool) {
+            t.join();
+        }
+    }
+    return failures.load();
+}
+
+// Closest hits for world rays (the accel contract; AccelBackend.cpp:43-112).
+__attribute__((visibility("default"))) int bfo_closest_hits(void* h, const bf200_ray_v1* rays, uint64_t n,
+                                                            bf200_hit_v1* hits) {
+    const auto* s = static_cast<Scene*>(h);
+    for (uint64_t i = 0; i < n; ++i) {
+        std::memset(&hits[i], 0, sizeof(hits[i]));
+        hits[i].instance_index = 0xFFFFFFFFU;
+        hits[i].primitive_index = 0xFFFFFFFFU;
+        try {
+            Hit hit{};
+            const V3 o{rays[i].origin[0], rays[i].origin[1], rays[i].origin[2]};
+            const V3 d{rays[i].direction[0], rays[i].direction[1], rays[i].direction[2]};
+            if (closest_hit(*s, o, d, rays[i].t_min, rays[i].t_max, rays[i].mask, hit)) {
+                hits[i].t = hit.t;
+                hits[i].barycentrics[0] = hit.b0;
+                hits[i].barycentrics[1] = hit.b1;
+                hits[i].barycentrics[2] = hit.b2;
+                hits[i].instance_index = hit.instance;
+                hits[i].primitive_index = hit.primitive;
+            }
+        } catch (const Failure& f) {
+            hits[i].status = BF200_LANE_NUMERICAL_FAILURE;
+            set_error(f.message);
+        }
+    }
+    return 0;
+}
+
+// Float32 or Neumaier float64 film of the caller-side path: CIE XYZ (Cie1931Sensor.cpp:104-176),
+// linear sRGB (Color.hpp:77-88), add_sample(x, y, rgb, 1) (Film.hpp:150-182). `sums` holds
+// (r, g, b, weight) per pixel as double; for precision 1 also the compensations are applied.
+__attribute__((visibility("default"))) int bfo_film_accumulate(const float* radiance,
+                                                               const bf200_sample_index_v1* samples,
+                                                               uint64_t n, const bf200_sensor_v1* sensor,
+                                                               uint32_t width, uint32_t height,
+                                                               uint32_t precision, double* out_sums,
+                                                               uint64_t* out_counts) {
+    const size_t pixels = size_t(width) * height;
+    std::vector<float> f32(4 * pixels, 0.0F);
+    std::vector<double> f64(8 * pixels, 0.0);
+    std::vector<uint64_t> counts(pixels, 0);
+    for (uint64_t i = 0; i < n; ++i) {
+        float xyz[3] = {0.0F, 0.0F, 0.0F};
+        for (int lane = 0; lane < 4; ++lane) {
+            const float c = radiance[4 * i + lane];
+            for (int k = 0; k < 3; ++k) {
+                const float r = sensor->response_xyz[lane][k];
+                float term = 0.0F;
+                if (c != 0.0F && r != 0.0F) {
+                    int ec = 0, er = 0, en = 0, ep = 0;
+                    const float mc = std::frexp(c, &ec);
+                    const float mr = std::frexp(r, &er);
+                    const float mn = std::frexp(sensor->normalization, &en);
+                    const float mp = std::frexp(sensor->wavelength_pdf[lane], &ep);
+                    const float mantissa = mc * mr * mn / mp;
+                    term = std::ldexp(mantissa, ec + er + en - ep);
+                }
+                xyz[k] += term;
+            }
+        }
+        const float red = 3.2404542F * xyz[0] - 1.5371385F * xyz[1] - 0.4985314F * xyz[2];
+        const float green = -0.9692660F * xyz[0] + 1.8760108F * xyz[1] + 0.0415560F * xyz[2];
+        const float blue = 0.0556434F * xyz[0] - 0.2040259F * xyz[1] + 1.0572252F * xyz[2];
+        const size_t p = size_t(samples[i].pixel_y) * width + samples[i].pixel_x;
+        if (precision == 0) {
+            f32[4 * p + 0] += red * 1.0F;
+            f32[4 * p + 1] += green * 1.0F;
+            f32[4 * p + 2] += blue * 1.0F;
+            f32[4 * p + 3] += 1.0F;
+        } else {
+            const double values[4] = {double(red) * 1.0, double(green) * 1.0, double(blue) * 1.0, 1.0};
+            for (int k = 0; k < 4; ++k) {
+                double& sum = f64[8 * p + k];
+                double& comp = f64[8 * p + 4 + k];
+                const double updated = sum + values[k];
+                if (std::abs(sum) >= std::abs(values[k])) {
+                    comp += (sum - updated) + values[k];
+                } else {
+                    comp += (values[k] - updated) + sum;
+                }
+                sum = updated;
+            }
+        }
+        ++counts[p];
+    }
+    for (size_t p = 0; p < pixels; ++p) {
+        for (int k = 0; k < 4; ++k) {
+            out_sums[4 * p + k] = precision == 0 ? double(f32[4 * p + k]) : f64[8 * p + k] + f64[8 * p + 4 + k];
+        }
+        out_counts[p] = counts[p];
+    }
+    return 0;
+}
+
+}  // extern "C"

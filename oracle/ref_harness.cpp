@@ -1,0 +1,565 @@
+// Test-infrastructure harness around the reference implementation itself.
+//
+// This translation unit is compiled together with the reference's own Core, Renderer and
+// Engine sources (see oracle/Makefile) into oracle/_ref/libbfref.so. It is never shipped and
+// never called by the product: only tests, the golden-fixture generator and bench.py's
+// reference arm load it, as the checker / CPU baseline. It turns the flat bf200 scene and path
+// records into the reference's own objects and runs the reference's own scalar path tracer:
+//
+//   * FrameScene::create                   (Blackframe/Engine/Source/FrameScene.cpp:390-528)
+//   * create_analytic_accel_backend        (Blackframe/Engine/Source/AccelBackend.cpp:348)
+//   * LightSampler::create_uniform         (Blackframe/Renderer/Source/LightSampler.cpp:574)
+//   * trace_scene_mis                      (Blackframe/Engine/Source/SceneMisPathLoop.cpp:1009)
+//   * PinholeCamera::generate_primary_ray  (Blackframe/Renderer/Include/.../PinholeCamera.hpp)
+//   * cie_1931_spectrum_to_xyz, xyz_to_linear_rgb, Film/ReferenceFilm::add_sample
+//     (the caller-side film path of Tests/Backends/GPU/CUDA/CudaTransportParityTest.cpp:906-927)
+//
+// The CIE sensor source is included here (rather than linked) so the harness can read the
+// colour-matching response at the frame's packet wavelengths.
+#include "Cie1931Sensor.cpp"
+
+#include "../include/bf200.h"
+
+#include <Blackframe/Engine/AccelBackend.hpp>
+#include <Blackframe/Engine/FrameScene.hpp>
+#include <Blackframe/Engine/SceneMisPathLoop.hpp>
+#include <Blackframe/Engine/TriangleMesh.hpp>
+#include <Blackframe/Renderer/Color.hpp>
+#include <Blackframe/Renderer/Film.hpp>
+#include <Blackframe/Renderer/IndependentSampler.hpp>
+#include <Blackframe/Renderer/LightSampler.hpp>
+#include <Blackframe/Renderer/PinholeCamera.hpp>
+#include <Blackframe/Renderer/WavelengthSampling.hpp>
+
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+using namespace blackframe;
+
+std::mutex g_error_mutex;
+std::string g_last_error;
+
+void set_error(const std::string& message) {
+    std::lock_guard<std::mutex> lock{g_error_mutex};
+    g_last_error = message;
+}
+
+struct RefScene {
+    engine::FrameSceneHandle scene;
+    std::unique_ptr<engine::AccelBackend> accel;
+    std::unique_ptr<renderer::LightSampler> sampler;
+    renderer::SampledWavelengths wavelengths{};
+};
+
+renderer::SampledWavelengths make_wavelengths(const float* nm, const float* pdf) {
+    auto result = renderer::SampledWavelengths{};
+    for (std::size_t lane = 0; lane < 4; ++lane) {
+        result[lane].nanometers = nm[lane];
+        result[lane].probability.value = pdf[lane];
+        result[lane].probability.measure = renderer::ProbabilityMeasure::wavelength;
+    }
+    return result;
+}
+
+renderer::TransportSpectrum spectrum4(const float* values) {
+    auto result = renderer::TransportSpectrum{};
+    for (std::size_t lane = 0; lane < 4; ++lane) {
+        result.values[lane] = values[lane];
+    }
+    return result;
+}
+
+core::Result<engine::SceneClosureMixture> make_mixture(const bf200_material_v1& material,
+                                                       const bf200_closure_v1* closures) {
+    auto set = renderer::ClosureSet{};
+    for (uint32_t index = 0; index < material.closure_count; ++index) {
+        const auto& record = closures[material.closure_offset + index];
+        const auto weight = spectrum4(record.weight);
+        auto status = renderer::ClosureAppendStatus::invalid_payload;
+        switch (record.kind) {
+        case BF200_CLOSURE_LAMBERTIAN_REFLECTION:
+            status = set.append_lambertian_reflection(weight);
+            break;
+        case BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION:
+            status = set.append_rough_conductor_reflection(weight, spectrum4(record.parameters),
+                                                           spectrum4(record.parameters + 4),
+                                                           record.parameters[8],
+                                                           record.parameters[9]);
+            break;
+        case BF200_CLOSURE_ROUGH_DIELECTRIC:
+            status = set.append_rough_dielectric(weight, record.parameters[0],
+                                                 record.parameters[1], record.parameters[2],
+                                                 record.parameters[3]);
+            break;
+        default:
+            break;
+        }
+        if (status != renderer::ClosureAppendStatus::appended) {
+            return std::unexpected(core::Error{.code = core::StatusCode::invalid_argument,
+                                               .message = "closure record rejected"});
+        }
+    }
+    return engine::SceneClosureMixture::create(
+        set,
+        std::span<const float>{material.component_probabilities, material.closure_count},
+        material.frame_mode == 1 ? engine::SceneClosureFrameMode::surface_tangent
+                                 : engine::SceneClosureFrameMode::shading_normal,
+        material.tangent_rotation_radians);
+}
+
+renderer::Ray make_ray(const bf200_ray_v1& ray) {
+    const auto created = renderer::Ray::create(
+        renderer::Point3{.x = ray.origin[0], .y = ray.origin[1], .z = ray.origin[2]},
+        renderer::Vector3{.x = ray.direction[0], .y = ray.direction[1], .z = ray.direction[2]},
+        ray.t_min, ray.t_max, ray.time, ray.mask, renderer::MediumId{.value = ray.medium});
+    return *created;
+}
+
+void store_ray(const renderer::Ray& ray, bf200_ray_v1& out) {
+    out.origin[0] = ray.origin().x;
+    out.origin[1] = ray.origin().y;
+    out.origin[2] = ray.origin().z;
+    out.direction[0] = ray.direction().x;
+    out.direction[1] = ray.direction().y;
+    out.direction[2] = ray.direction().z;
+    out.t_min = ray.t_min();
+    out.t_max = ray.t_max();
+    out.time = ray.time();
+    out.mask = ray.mask();
+    out.medium = ray.current_medium().value;
+    out.reserved = 0;
+}
+
+core::Result<renderer::RussianRoulettePolicy> make_policy(const bf200_transport_options_v1& o) {
+    if (o.roulette_enabled == 0) {
+        return renderer::RussianRoulettePolicy::disabled();
+    }
+    return renderer::RussianRoulettePolicy::create_enabled(o.roulette_first_eligible_depth,
+                                                           o.roulette_minimum_survival,
+                                                           o.roulette_maximum_survival);
+}
+
+// Traces one path through the reference; lane_status 0 on success, 1 with the path zeroed when
+// the reference itself returns an error for this path.
+void trace_one(const RefScene& scene, const bf200_path_input_v1& input,
+               const bf200_transport_options_v1& options,
+               const renderer::RussianRoulettePolicy& policy, bf200_path_result_v1& out,
+               std::string* error) {
+    std::memset(&out, 0, sizeof(out));
+    const auto state = renderer::PathState::create_initial(scene.wavelengths, renderer::VacuumMedium);
+    const auto stream = renderer::SampleStream{renderer::SampleStreamIndex{
+        .pixel_x = input.sample.pixel_x,
+        .pixel_y = input.sample.pixel_y,
+        .sample_index = input.sample.sample_index,
+        .seed = input.sample.seed,
+    }};
+    const auto limits = renderer::PathDepthLimits{
+        .diffuse = options.depth_limits[0],
+        .glossy = options.depth_limits[1],
+        .specular = options.depth_limits[2],
+        .transmission = options.depth_limits[3],
+        .volume = options.depth_limits[4],
+    };
+    const auto result = engine::trace_scene_mis(
+        make_ray(input.primary_ray), *state, stream, *scene.accel, *scene.sampler,
+        options.mis_heuristic == 1 ? renderer::MisHeuristic::power : renderer::MisHeuristic::balance,
+        limits, policy);
+    if (!result) {
+        out.lane_status = BF200_LANE_NUMERICAL_FAILURE;
+        if (error != nullptr && error->empty()) {
+            *error = result.error().message;
+        }
+        return;
+    }
+    const auto& path_state = result->state;
+    for (std::size_t lane = 0; lane < 4; ++lane) {
+        out.beta[lane] = path_state.beta()[lane];
+        out.radiance[lane] = path_state.accumulated_radiance()[lane];
+    }
+    out.depth = path_state.depth();
+    out.depth_counters[0] = path_state.depth_counters().diffuse;
+    out.depth_counters[1] = path_state.depth_counters().glossy;
+    out.depth_counters[2] = path_state.depth_counters().specular;
+    out.depth_counters[3] = path_state.depth_counters().transmission;
+    out.depth_counters[4] = path_state.depth_counters().volume;
+    out.eta_scale = path_state.eta_scale();
+    out.delta_flags = static_cast<uint32_t>(path_state.delta_flags());
+    out.termination = static_cast<uint32_t>(result->termination);
+    out.blocked_depth_limits = static_cast<uint32_t>(result->blocked_depth_limits);
+    out.lane_status = BF200_LANE_OK;
+    store_ray(result->terminal_ray, out.terminal_ray);
+}
+
+template <typename Body> void parallel_for(uint64_t count, int threads, Body body) {
+    if (threads <= 1 || count < 2) {
+        for (uint64_t index = 0; index < count; ++index) {
+            body(index);
+        }
+        return;
+    }
+    std::atomic<uint64_t> next{0};
+    std::vector<std::thread> pool;
+    for (int worker = 0; worker < threads; ++worker) {
+        pool.emplace_back([&] {
+            for (uint64_t index = next.fetch_add(1); index < count; index = next.fetch_add(1)) {
+                body(index);
+            }
+        });
+    }
+    for (auto& thread : pool) {
+        thread.join();
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+__attribute__((visibility("default"))) const char* bfr_last_error() {
+    return g_last_error.c_str();
+}
+
+__attribute__((visibility("default"))) int bfr_scene_create(const bf200_scene_desc_v1* desc,
+                                                            void** out_scene) {
+    if (desc == nullptr || out_scene == nullptr) {
+        set_error("null argument");
+        return 1;
+    }
+    auto description = engine::FrameSceneDescription{};
+    const auto wavelengths = make_wavelengths(desc->wavelength_nanometers, desc->wavelength_pdf);
+    for (uint32_t g = 0; g < desc->geometry_count; ++g) {
+        const auto& geometry = desc->geometries[g];
+        auto positions = std::vector<renderer::Point3>{};
+        auto normals = std::vector<renderer::Normal3>{};
+        auto uvs = std::vector<renderer::Point2>{};
+        for (uint32_t v = 0; v < geometry.vertex_count; ++v) {
+            const auto i = geometry.vertex_offset + v;
+            positions.push_back(renderer::Point3{.x = desc->positions[3 * i],
+                                                 .y = desc->positions[3 * i + 1],
+                                                 .z = desc->positions[3 * i + 2]});
+            normals.push_back(renderer::Normal3{.x = desc->normals[3 * i],
+                                                .y = desc->normals[3 * i + 1],
+                                                .z = desc->normals[3 * i + 2]});
+            uvs.push_back(renderer::Point2{.x = desc->texture_coordinates[2 * i],
+                                           .y = desc->texture_coordinates[2 * i + 1]});
+        }
+        auto triangles = std::vector<engine::TriangleVertexIndices>{};
+        for (uint32_t t = 0; t < geometry.triangle_count; ++t) {
+            const auto i = geometry.triangle_offset + t;
+            triangles.push_back(engine::TriangleVertexIndices{
+                .vertices = {desc->triangles[3 * i], desc->triangles[3 * i + 1],
+                             desc->triangles[3 * i + 2]}});
+        }
+        auto mesh = engine::TriangleMesh::create(std::move(positions), std::move(normals),
+                                                 std::move(uvs), std::move(triangles));
+        if (!mesh) {
+            set_error("mesh: " + mesh.error().message);
+            return 2;
+        }
+        description.geometries.push_back(engine::SceneGeometry{
+            .id = {.value = geometry.geometry_id},
+            .mesh = std::make_shared<const engine::TriangleMesh>(std::move(*mesh))});
+    }
+    for (uint32_t m = 0; m < desc->material_count; ++m) {
+        const auto& material = desc->materials[m];
+        auto mixture = make_mixture(material, desc->closures);
+        if (!mixture) {
+            set_error("material: " + mixture.error().message);
+            return 3;
+        }
+        description.materials.push_back(engine::SceneMaterial{
+            .id = {.value = material.material_id},
+            .spectral =
+                engine::SceneSpectralMaterial{
+                    .wavelengths = wavelengths,
+                    .closure_mixture = *mixture,
+                    .emitted_radiance = spectrum4(material.emitted_radiance),
+                },
+        });
+    }
+    auto object_ids = std::vector<uint32_t>{};
+    for (uint32_t i = 0; i < desc->instance_count; ++i) {
+        const auto& instance = desc->instances[i];
+        if (std::find(object_ids.begin(), object_ids.end(), instance.object_id) ==
+            object_ids.end()) {
+            object_ids.push_back(instance.object_id);
+            description.objects.push_back(engine::SceneObject{.id = {.value = instance.object_id}});
+        }
+        auto matrix = renderer::Matrix4{};
+        for (std::size_t r = 0; r < 4; ++r) {
+            for (std::size_t c = 0; c < 4; ++c) {
+                matrix(r, c) = instance.object_to_world[r * 4 + c];
+            }
+        }
+        description.instances.push_back(engine::SceneInstance{
+            .id = {.value = instance.instance_id},
+            .parent = std::nullopt,
+            .object = {.value = instance.object_id},
+            .geometry = {.value = desc->geometries[instance.geometry_index].geometry_id},
+            .material = {.value = desc->materials[instance.material_index].material_id},
+            .local_to_parent = matrix,
+            .visibility_mask = instance.visibility_mask,
+        });
+    }
+    description.spectral_environment = engine::SceneSpectralEnvironment{
+        .wavelengths = wavelengths,
+        .radiance = spectrum4(desc->environment_radiance),
+    };
+    auto scene = engine::FrameScene::create(std::move(description));
+    if (!scene) {
+        set_error("frame scene: " + scene.error().message);
+        return 4;
+    }
+    auto accel = engine::create_analytic_accel_backend(*scene);
+    if (!accel) {
+        set_error("accel: " + accel.error().message);
+        return 5;
+    }
+    auto sampler = renderer::LightSampler::create_uniform((*scene)->punctual_lights().size() +
+                                                          (*scene)->mesh_area_lights().size());
+    if (!sampler) {
+        set_error("light sampler: " + sampler.error().message);
+        return 6;
+    }
+    auto* result = new RefScene{};
+    result->scene = *scene;
+    result->accel = std::move(*accel);
+    result->sampler = std::make_unique<renderer::LightSampler>(std::move(*sampler));
+    result->wavelengths = wavelengths;
+    *out_scene = result;
+    return 0;
+}
+
+__attribute__((visibility("default"))) void bfr_scene_destroy(void* scene) {
+    delete static_cast<RefScene*>(scene);
+}
+
+// Writes the committed world_to_object (inverse) matrix of instance `index` (sorted order).
+__attribute__((visibility("default"))) int bfr_scene_world_to_object(void* handle, uint32_t index,
+                                                                     float* out16) {
+    const auto* scene = static_cast<RefScene*>(handle);
+    const auto instances = scene->scene->instances();
+    if (index >= instances.size()) {
+        return 1;
+    }
+    const auto transform = scene->scene->world_transform(instances[index].id);
+    if (!transform) {
+        return 2;
+    }
+    for (std::size_t r = 0; r < 4; ++r) {
+        for (std::size_t c = 0; c < 4; ++c) {
+            out16[r * 4 + c] = transform->get().inverse_matrix()(r, c);
+        }
+    }
+    return 0;
+}
+
+__attribute__((visibility("default"))) uint32_t bfr_scene_light_count(void* handle) {
+    const auto* scene = static_cast<RefScene*>(handle);
+    return static_cast<uint32_t>(scene->scene->mesh_area_lights().size() +
+                                 scene->scene->punctual_lights().size());
+}
+
+// Runs trace_scene_mis for every input. Returns the number of paths the reference rejected
+// with an error (those carry lane_status 1 and zeroed outputs).
+__attribute__((visibility("default"))) int64_t
+bfr_trace_paths(void* handle, const bf200_path_input_v1* inputs, uint64_t count,
+                const bf200_transport_options_v1* options, bf200_path_result_v1* results,
+                int threads) {
+    const auto* scene = static_cast<RefScene*>(handle);
+    const auto policy = make_policy(*options);
+    if (!policy) {
+        set_error(policy.error().message);
+        return -1;
+    }
+    std::atomic<int64_t> failures{0};
+    std::string first_error;
+    std::mutex error_mutex;
+    parallel_for(count, threads, [&](uint64_t index) {
+        std::string error;
+        trace_one(*scene, inputs[index], *options, *policy, results[index], &error);
+        if (results[index].lane_status != 0) {
+            failures.fetch_add(1);
+            std::lock_guard<std::mutex> lock{error_mutex};
+            if (first_error.empty()) {
+                first_error = error;
+            }
+        }
+    });
+    if (!first_error.empty()) {
+        set_error(first_error);
+    }
+    return failures.load();
+}
+
+// Builds the reference pinhole camera (origin, frame from normal + tangent seed, vertical fov)
+// and reports the derived constants in bf200_camera_v1 form.
+__attribute__((visibility("default"))) int bfr_camera(const float* origin, const float* normal,
+                                                      const float* tangent, uint32_t width,
+                                                      uint32_t height, float vfov, float t_min,
+                                                      float t_max, float time, uint32_t mask,
+                                                      bf200_camera_v1* out) {
+    const auto frame = renderer::OrthonormalFrame::from_normal_and_tangent(
+        renderer::Normal3{.x = normal[0], .y = normal[1], .z = normal[2]},
+        renderer::Vector3{.x = tangent[0], .y = tangent[1], .z = tangent[2]});
+    if (!frame) {
+        set_error(frame.error().message);
+        return 1;
+    }
+    const auto camera = renderer::PinholeCamera::create(
+        renderer::Point3{.x = origin[0], .y = origin[1], .z = origin[2]}, *frame,
+        renderer::RenderExtent{.width = width, .height = height}, vfov, t_min, t_max, mask,
+        renderer::VacuumMedium);
+    if (!camera) {
+        set_error(camera.error().message);
+        return 2;
+    }
+    std::memset(out, 0, sizeof(*out));
+    for (int a = 0; a < 3; ++a) {
+        out->origin[a] = origin[a];
+    }
+    out->tangent[0] = frame->tangent().x;
+    out->tangent[1] = frame->tangent().y;
+    out->tangent[2] = frame->tangent().z;
+    out->bitangent[0] = frame->bitangent().x;
+    out->bitangent[1] = frame->bitangent().y;
+    out->bitangent[2] = frame->bitangent().z;
+    out->normal[0] = frame->normal().x;
+    out->normal[1] = frame->normal().y;
+    out->normal[2] = frame->normal().z;
+    const auto half_height = std::tan(vfov / 2.0F);
+    out->half_height = half_height;
+    out->half_width = half_height * (static_cast<float>(width) / static_cast<float>(height));
+    out->t_min = t_min;
+    out->t_max = t_max;
+    out->time = time;
+    out->mask = mask;
+    out->width = width;
+    out->height = height;
+    out->jitter_mode = 1;
+    return 0;
+}
+
+// Generates reference primary rays for (pixel, sample) indices with uniform jitter.
+__attribute__((visibility("default"))) int
+bfr_camera_rays(const float* origin, const float* normal, const float* tangent, uint32_t width,
+                uint32_t height, float vfov, float time, const bf200_sample_index_v1* samples,
+                uint64_t count, bf200_ray_v1* rays) {
+    const auto frame = renderer::OrthonormalFrame::from_normal_and_tangent(
+        renderer::Normal3{.x = normal[0], .y = normal[1], .z = normal[2]},
+        renderer::Vector3{.x = tangent[0], .y = tangent[1], .z = tangent[2]});
+    const auto camera = renderer::PinholeCamera::create(
+        renderer::Point3{.x = origin[0], .y = origin[1], .z = origin[2]}, *frame,
+        renderer::RenderExtent{.width = width, .height = height}, vfov, 0.0F,
+        std::numeric_limits<float>::infinity(), renderer::AllRayVisibility,
+        renderer::VacuumMedium);
+    if (!camera) {
+        set_error(camera.error().message);
+        return 1;
+    }
+    for (uint64_t index = 0; index < count; ++index) {
+        const auto pixel_sample = renderer::PixelSampleIndex{
+            .pixel_x = samples[index].pixel_x,
+            .pixel_y = samples[index].pixel_y,
+            .sample_index = samples[index].sample_index,
+            .seed = samples[index].seed,
+        };
+        const auto ray =
+            camera->generate_primary_ray(pixel_sample, renderer::PixelJitterMode::uniform, time);
+        if (!ray) {
+            set_error(ray.error().message);
+            return 2;
+        }
+        store_ray(*ray, rays[index]);
+    }
+    return 0;
+}
+
+// CIE 1931 sensor constants at a packet: response at each lane, lane pdf, normalisation.
+__attribute__((visibility("default"))) int bfr_sensor(const float* nm, const float* pdf,
+                                                      bf200_sensor_v1* out) {
+    std::memset(out, 0, sizeof(*out));
+    for (std::size_t lane = 0; lane < 4; ++lane) {
+        const auto response = renderer::color_matching_functions<float>(nm[lane]);
+        out->response_xyz[lane][0] = response.x;
+        out->response_xyz[lane][1] = response.y;
+        out->response_xyz[lane][2] = response.z;
+        out->wavelength_pdf[lane] = pdf[lane];
+    }
+    constexpr auto inverse_lane_count = 1.0F / 4.0F;
+    out->normalization = inverse_lane_count / static_cast<float>(renderer::Cie1931YIntegralNanometers);
+    return 0;
+}
+
+// Reference caller-side film path: spectrum -> XYZ -> linear RGB -> add_sample(x, y, rgb, 1).
+// Radiance lanes per path; pixels and samples given per path in the order they are added.
+// precision 0: renderer::Film (float32), 1: renderer::ReferenceFilm (float64, Neumaier).
+// out_sums receives the resolved snapshot sums (r, g, b, weight) per pixel as double.
+__attribute__((visibility("default"))) int
+bfr_film_accumulate(const float* radiance, const bf200_sample_index_v1* samples, uint64_t count,
+                    const float* nm, const float* pdf, uint32_t width, uint32_t height,
+                    uint32_t precision, double* out_sums, uint64_t* out_counts) {
+    const auto wavelengths = make_wavelengths(nm, pdf);
+    auto run = [&](auto& film) -> int {
+        for (uint64_t index = 0; index < count; ++index) {
+            const auto spectrum = spectrum4(radiance + 4 * index);
+            const auto xyz = renderer::cie_1931_spectrum_to_xyz(spectrum, wavelengths);
+            if (!xyz) {
+                set_error(xyz.error().message);
+                return 2;
+            }
+            const auto rgb = renderer::xyz_to_linear_rgb(*xyz);
+            if (!rgb) {
+                set_error(rgb.error().message);
+                return 3;
+            }
+            using Film = std::remove_reference_t<decltype(film)>;
+            const auto status = film.add_sample(
+                samples[index].pixel_x, samples[index].pixel_y,
+                typename Film::Color{.red = static_cast<typename Film::Scalar>(rgb->red),
+                                     .green = static_cast<typename Film::Scalar>(rgb->green),
+                                     .blue = static_cast<typename Film::Scalar>(rgb->blue)},
+                typename Film::Scalar{1});
+            if (!status) {
+                set_error(status.error().message);
+                return 4;
+            }
+        }
+        for (uint32_t y = 0; y < height; ++y) {
+            for (uint32_t x = 0; x < width; ++x) {
+                const auto pixel = film.pixel(x, y);
+                const auto i = static_cast<std::size_t>(y) * width + x;
+                out_sums[4 * i + 0] = static_cast<double>(pixel->weighted_sum.red);
+                out_sums[4 * i + 1] = static_cast<double>(pixel->weighted_sum.green);
+                out_sums[4 * i + 2] = static_cast<double>(pixel->weighted_sum.blue);
+                out_sums[4 * i + 3] = static_cast<double>(pixel->weight_sum);
+                out_counts[i] = pixel->sample_count;
+            }
+        }
+        return 0;
+    };
+    const auto extent = renderer::RenderExtent{.width = width, .height = height};
+    if (precision == 0) {
+        auto film = renderer::Film::create(extent);
+        if (!film) {
+            set_error(film.error().message);
+            return 1;
+        }
+        return run(*film);
+    }
+    auto film = renderer::ReferenceFilm::create(extent);
+    if (!film) {
+        set_error(film.error().message);
+        return 1;
+    }
+    return run(*film);
+}
+
+} // extern "C"
