@@ -1,0 +1,336 @@
+"""Benchmark of the wavefront path-tracing hot path (one JSON line on rank 0).
+
+Workload (one step = one full frame): the Cornell box at 256 x 256, 256 samples per pixel, with
+a GGX conductor sphere and a GGX rough dielectric sphere (64 x 32 UV spheres), power MIS, depth
+16, Russian roulette from depth 3 — 16,777,216 path samples per frame and GPU. The scene,
+camera rays, transport and film accumulation all run on the device (inputs resident in HBM);
+`e2e` times the public C-ABI call with host film buffers (bf200_render_film), copies included.
+
+Metric: path samples per second (whole job; weak scaling: every rank renders its own disjoint
+sample range of the same frame and the per-GPU films are summed with one NCCL all-reduce).
+
+`--impl reference` times the reference's own CPU implementation of the path (oracle/_ref: the
+reference sources compiled as-is, trace_scene_mis + analytic accel + caller-side film) on the
+host cores over a bounded sample of the same workload.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "blackframe-renderer_b200"))
+sys.path.insert(0, os.path.join(REPO, "tests"))
+sys.path.insert(0, REPO)
+
+import numpy as np  # noqa: E402
+
+from bf200 import abi, runtime, scenes  # noqa: E402
+
+WORKLOAD = "cornell_spheres_256"
+METRIC = "path samples/s"
+# algorithmic bytes (the per-unit model of the path: rays, hits, path state, queue slots, film)
+CAMERA_RAY_BYTES = 28
+EXTENSION_SEGMENT_BYTES = 240
+SHADOW_SEGMENT_BYTES = 96
+FILM_SAMPLE_BYTES = 24
+# per-launch algorithmic bytes of the traversal kernel: camera ray write, ray read + hit write
+INTERSECT_SEGMENT_BYTES = 48
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+        return float(data.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        query = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={query}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 3 + k and s[3 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons}
+
+
+def workload_setup():
+    builder, options, (width, height, spp) = scenes.build_workload(WORKLOAD)
+    g = np.load(os.path.join(REPO, "tests", "golden", f"{WORKLOAD}.npz"))
+    from helpers import sensor_from_golden
+    sensor = sensor_from_golden(g)
+    camera = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV,
+                                   scenes.PATH_TIME)
+    return builder, options, camera, sensor, (width, height, spp)
+
+
+def cpu_sample_rate(target_seconds=15.0):
+    """Times the reference CPU path (oracle/_ref when built, else the oracle restatement) on a
+    bounded sample of the workload's paths; returns (paths/s, threads, kind, sample text)."""
+    from oracle.bindings import Oracle, Reference, reference_available
+    builder, options, (width, height, spp) = scenes.build_workload(WORKLOAD)
+    checker = Reference() if reference_available() else Oracle()
+    kind = "reference" if reference_available() else "port"
+    threads = os.cpu_count() or 1
+    handle = checker.scene(builder)
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV,
+                                scenes.PATH_TIME)
+    rng = np.random.default_rng(5)
+
+    def batch(n):
+        samples = (abi.SampleIndex * n)()
+        for k in range(n):
+            samples[k].pixel_x, samples[k].pixel_y = int(rng.integers(width)), int(rng.integers(height))
+            samples[k].sample_index = int(rng.integers(spp))
+        from oracle.bindings import Oracle as _O
+        rays = _O().camera_rays(cam, samples)
+        inputs = (abi.PathInput * n)()
+        for k in range(n):
+            inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
+        return inputs
+
+    probe = batch(threads)
+    t0 = time.perf_counter()
+    checker.trace(handle, probe, options, threads)
+    per_path = max(1e-6, (time.perf_counter() - t0) / len(probe))
+    n = int(max(threads, min(200000, target_seconds / per_path)))
+    inputs = batch(n)
+    t0 = time.perf_counter()
+    checker.trace(handle, inputs, options, threads)
+    elapsed = time.perf_counter() - t0
+    checker.destroy(handle)
+    sample = f"{n} random (pixel, sample) paths of {WORKLOAD} ({elapsed:.1f} s, {threads} threads)"
+    return n / elapsed, threads, kind, sample, n, elapsed
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    rates = []
+    for step in range(args.warmup + args.steps):
+        rate, threads, kind, sample, n, elapsed = cpu_sample_rate(target_seconds=args.reference_seconds)
+        if step >= args.warmup:
+            rates.append((rate, threads, kind, sample, elapsed))
+    value = statistics.median(r[0] for r in rates)
+    ms_per_step = statistics.median(r[4] for r in rates) * 1000.0
+    _, threads, kind, sample, _ = rates[-1]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "width": 256, "height": 256, "spp": 256, "max_depth": 16,
+                   "mis": "power", "sample_per_step": sample},
+        "cpu_baseline": {"value": value, "unit": "path samples/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "path samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", default="bf200", choices=["bf200", "reference"])
+    parser.add_argument("--capacity", type=int, default=1 << 21)
+    parser.add_argument("--reference-seconds", type=float, default=8.0)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local_rank)
+    distributed = world > 1
+    if distributed:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    builder, options, camera, sensor, (width, height, spp) = workload_setup()
+    options.instrumentation = 1
+    pixels = width * height
+    paths_per_step = pixels * spp
+    ctx = runtime.Context(local_rank, path_capacity=args.capacity)
+    scene = ctx.create_scene(builder)
+    lib = runtime.library()
+    film = torch.zeros((height, width, 4), dtype=torch.float32, device="cuda")
+    counts = torch.zeros((height, width), dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def render_device(step):
+        film.zero_()
+        counts.zero_()
+        torch.cuda.synchronize()
+        f = abi.Film(width, height, 0, 0, film.data_ptr(), C.cast(counts.data_ptr(), C.POINTER(abi.u64)))
+        first = (step * world + rank) * spp  # disjoint sample ranges per rank and step
+        request = abi.FilmRequest(C.sizeof(abi.FilmRequest), spp, first, 0, 0)
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        status = lib.bf200_render_film_device(ctx.handle, scene.handle, C.byref(camera), C.byref(sensor),
+                                              C.byref(request), C.byref(options), C.byref(f), C.byref(report))
+        if status != 0:
+            raise runtime.Bf200Error(status, lib.bf200_context_last_error(ctx.handle).decode())
+        if distributed:
+            dist.all_reduce(film)  # per-GPU films summed (the only exchange of the path)
+        return report
+
+    for step in range(args.warmup):
+        render_device(step)
+    torch.cuda.synchronize()
+
+    # timed region: device-resident inputs, K full frames; L2 flushed between frames
+    reports = []
+    step_ms = []
+    with ClockSampler(local_rank) as clocks:
+        if distributed:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for step in range(args.steps):
+            flush.fill_(step & 0xFF)
+            torch.cuda.synchronize()
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            report = render_device(args.warmup + step)
+            reports.append(report)
+            step_ms.append(report.gpu_milliseconds)
+        torch.cuda.synchronize()
+        if distributed:
+            dist.barrier()
+    total_ms = sum(step_ms)
+    if distributed:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = paths_per_step * world * args.steps / (total_ms / 1000.0)
+    failed = sum(r.failed_lanes for r in reports)
+    launches = sum(r.kernel_launches for r in reports)
+    ext = sum(r.extension_segments for r in reports)
+    shadow = sum(r.shadow_segments for r in reports)
+    iterations = sum(r.iterations for r in reports)
+    stage = {"k_intersect": sum(r.intersect_milliseconds for r in reports),
+             "k_shade": sum(r.shade_milliseconds for r in reports),
+             "k_occlude": sum(r.occlude_milliseconds for r in reports),
+             "k_film": sum(r.film_milliseconds for r in reports)}
+
+    # e2e: the public C-ABI call with host film buffers (copies in the timed region)
+    host_film = np.zeros((height, width, 4), np.float32)
+    host_counts = np.zeros((height, width), np.uint64)
+    h2d = host_film.nbytes + host_counts.nbytes
+    e2e_ms = []
+    for step in range(max(1, min(args.steps, 3))):
+        host_film[:] = 0
+        host_counts[:] = 0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.render_film(scene, camera, sensor, options, spp, seed=0,
+                        first_sample=(1000 + step * world + rank) * spp, film=(host_film, host_counts))
+        e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+    e2e_total = sum(e2e_ms)
+    if distributed:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = paths_per_step * world * len(e2e_ms) / (e2e_total / 1000.0)
+
+    # roofline of the dominant kernel: algorithmic bytes per launch / average launch time
+    peak, peak_kind = measured_peaks()
+    dominant = max(("k_intersect", "k_shade", "k_occlude"), key=lambda k: stage[k])
+    per_launch_ms = stage[dominant] / max(1, iterations)
+    if dominant == "k_intersect":
+        bytes_total = CAMERA_RAY_BYTES * paths_per_step * args.steps + INTERSECT_SEGMENT_BYTES * ext
+    elif dominant == "k_shade":
+        bytes_total = (EXTENSION_SEGMENT_BYTES - INTERSECT_SEGMENT_BYTES) * ext
+    else:
+        bytes_total = SHADOW_SEGMENT_BYTES * shadow
+    bytes_per_launch = bytes_total / max(1, iterations)
+    achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
+    whole_bytes = (CAMERA_RAY_BYTES * paths_per_step * args.steps + EXTENSION_SEGMENT_BYTES * ext +
+                   SHADOW_SEGMENT_BYTES * shadow + FILM_SAMPLE_BYTES * paths_per_step * args.steps)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "width": width, "height": height, "spp": spp, "max_depth": 16,
+                   "mis": "power", "paths_per_step_per_gpu": paths_per_step, "path_capacity": args.capacity,
+                   "l2": "flushed between steps (256 MiB write); path state > L2",
+                   "parallelism": f"sample-partitioned x{world}" if world > 1 else "single GPU"},
+        "rays_per_s": (ext + shadow) / (total_ms / 1000.0) * (world if distributed else 1),
+        "segments": {"extension": ext, "shadow": shadow, "iterations": iterations},
+        "stage_ms": stage, "failed_lanes": failed,
+        "clocks": clocks.summary(),
+        "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": h2d},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                     "whole_path_algorithmic_gbs": whole_bytes / (total_ms / 1000.0) / 1e9},
+    }
+    scene.close()
+    ctx.close()
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, threads, kind, sample, _, _ = cpu_sample_rate()
+        line["cpu_baseline"] = {"value": rate, "unit": "path samples/s", "cores": threads, "kind": kind,
+                                "sample": sample}
+    if distributed:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

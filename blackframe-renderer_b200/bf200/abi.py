@@ -121,7 +121,7 @@ class TransportOptions(C.Structure):
     _fields_ = [("struct_size", u32), ("mis_heuristic", u32), ("depth_limits", u32 * 5),
                 ("roulette_enabled", u32), ("roulette_first_eligible_depth", u32),
                 ("roulette_minimum_survival", f32), ("roulette_maximum_survival", f32),
-                ("reserved", u32 * 5)]
+                ("instrumentation", u32), ("reserved", u32 * 4)]
 
 
 class Camera(C.Structure):
@@ -152,7 +152,9 @@ class Report(C.Structure):
                 ("closure_samples", u64), ("light_samples", u64), ("terminated_paths", u64),
                 ("failed_lanes", u64), ("first_failure_status", u32),
                 ("first_failure_path", u32), ("kernel_launches", u64),
-                ("gpu_milliseconds", f64), ("reserved", u64 * 4)]
+                ("gpu_milliseconds", f64), ("intersect_milliseconds", f64), ("shade_milliseconds", f64),
+                ("occlude_milliseconds", f64), ("film_milliseconds", f64), ("iterations", u64),
+                ("reserved", u64 * 3)]
 
 
 class Hit(C.Structure):
@@ -163,7 +165,7 @@ class Hit(C.Structure):
 EXPECTED_SIZES = {
     Closure: 64, Material: 80, Geometry: 32, Instance: 160, Ray: 48, SampleIndex: 24,
     PathInput: 80, PathResult: 128, TransportOptions: 64, Camera: 88, Sensor: 80,
-    FilmRequest: 40, Report: 120, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
+    FilmRequest: 40, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
 }
 
 

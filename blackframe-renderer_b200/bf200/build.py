@@ -1,0 +1,64 @@
+"""Builds the in-tree shared libraries.
+
+* bf200/libbf200.so : the product — host runtime + sm_100a kernels (nvcc, -gencode
+  arch=compute_100a,code=sm_100a, no FMA contraction so float arithmetic keeps the reference's
+  operation order).
+* oracle/liboracle.so, oracle/_ref/libbfref.so : the CPU checkers (oracle/Makefile); the second
+  only when the reference tree is available to compile from.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(PACKAGE_DIR), "csrc")
+REPO = os.path.dirname(os.path.dirname(PACKAGE_DIR))
+INCLUDE = os.path.join(REPO, "include")
+LIBRARY = os.path.join(PACKAGE_DIR, "libbf200.so")
+SOURCES = ["bf200_kernels.cu", "bf200_host.cu"]
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-std=c++17", "-O3", "-lineinfo", "-fmad=false",
+    "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off",
+    "-shared",
+]
+
+
+def nvcc():
+    path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(path):
+        raise RuntimeError("nvcc not found: the CUDA toolkit is required to build bf200")
+    return path
+
+
+def _stale(target, inputs):
+    if not os.path.exists(target):
+        return True
+    mtime = os.path.getmtime(target)
+    return any(os.path.getmtime(p) > mtime for p in inputs)
+
+
+def build_library(force=False, verbose=False):
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "bf200.h")]
+    if not force and not _stale(LIBRARY, deps):
+        return LIBRARY
+    cmd = [nvcc()] + NVCC_FLAGS + ["-I" + INCLUDE, "-I" + CSRC, "-o", LIBRARY]
+    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return LIBRARY
+
+
+def build_oracle(reference_root=None, verbose=False):
+    oracle_dir = os.path.join(REPO, "oracle")
+    subprocess.run(["make", "-s", "-C", oracle_dir, "oracle"], check=True)
+    reference_root = reference_root or os.environ.get("BF200_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(reference_root, "Blackframe")):
+        subprocess.run(["make", "-s", "-j8", "-C", oracle_dir, "ref", "REF=" + reference_root], check=True)
+
+
+if __name__ == "__main__":
+    build_library(force="--force" in sys.argv, verbose=True)
+    build_oracle(verbose=True)

@@ -1,0 +1,184 @@
+"""Python binding of the bf200 C ABI (include/bf200.h) over ctypes.
+
+This mirrors the reference's call shape for the wavefront path:
+  CudaSceneSoA::upload + CudaSceneBvh::build -> Context.create_scene
+  trace_cuda_wavefront_transport             -> Context.trace_paths
+  caller-side film accumulation              -> Context.render_film
+The library is the in-tree bf200/libbf200.so; there is no fallback implementation — if it is
+missing or a call fails the error is raised.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_LIB = None
+LIBRARY_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libbf200.so")
+
+EXPORTED_SYMBOLS = [
+    "blackframe_query_extension", "bf200_context_create", "bf200_context_destroy",
+    "bf200_context_last_error", "bf200_scene_create", "bf200_scene_destroy", "bf200_trace_paths",
+    "bf200_trace_paths_device", "bf200_render_film", "bf200_render_film_device",
+    "bf200_closest_hits", "bf200_occlusions", "bf200_build_info", "bf200_camera_create",
+]
+
+
+class Bf200Error(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{abi.BLACKFRAME_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+def library():
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIBRARY_PATH):
+        raise Bf200Error(6, f"{LIBRARY_PATH} is not built (run __graft_entry__.build())")
+    lib = C.CDLL(LIBRARY_PATH)
+    vp = C.c_void_p
+    lib.bf200_build_info.restype = C.c_char_p
+    lib.bf200_context_create.argtypes = [C.c_int32, C.c_uint64, C.POINTER(vp)]
+    lib.bf200_context_create.restype = C.c_uint32
+    lib.bf200_context_destroy.argtypes = [vp]
+    lib.bf200_context_destroy.restype = C.c_uint32
+    lib.bf200_context_last_error.argtypes = [vp]
+    lib.bf200_context_last_error.restype = C.c_char_p
+    lib.bf200_scene_create.argtypes = [vp, C.POINTER(abi.SceneDesc), C.POINTER(vp)]
+    lib.bf200_scene_create.restype = C.c_uint32
+    lib.bf200_scene_destroy.argtypes = [vp]
+    lib.bf200_scene_destroy.restype = C.c_uint32
+    for name in ("bf200_trace_paths", "bf200_trace_paths_device"):
+        f = getattr(lib, name)
+        f.argtypes = [vp, vp, vp, C.c_uint64, C.POINTER(abi.TransportOptions), vp, C.POINTER(abi.Report)]
+        f.restype = C.c_uint32
+    for name in ("bf200_render_film", "bf200_render_film_device"):
+        f = getattr(lib, name)
+        f.argtypes = [vp, vp, C.POINTER(abi.Camera), C.POINTER(abi.Sensor), C.POINTER(abi.FilmRequest),
+                      C.POINTER(abi.TransportOptions), C.POINTER(abi.Film), C.POINTER(abi.Report)]
+        f.restype = C.c_uint32
+    lib.bf200_closest_hits.argtypes = [vp, vp, vp, C.c_uint64, vp]
+    lib.bf200_closest_hits.restype = C.c_uint32
+    lib.bf200_occlusions.argtypes = [vp, vp, vp, C.c_uint64, vp]
+    lib.bf200_occlusions.restype = C.c_uint32
+    lib.bf200_camera_create.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_uint32, C.c_uint32, C.c_float,
+                                                                      C.c_float, C.c_uint32, C.POINTER(abi.Camera)]
+    lib.bf200_camera_create.restype = C.c_uint32
+    lib.blackframe_query_extension.argtypes = [C.POINTER(abi.ExtensionQuery), C.POINTER(abi.ExtensionApi)]
+    lib.blackframe_query_extension.restype = C.c_uint32
+    _LIB = lib
+    return lib
+
+
+def query_extension():
+    """blackframe_query_extension as a Blackframe host calls it (XpuBackend.cpp:57-100)."""
+    lib = library()
+    query = abi.ExtensionQuery(C.sizeof(abi.ExtensionQuery), 1, 0, 0)
+    api = abi.ExtensionApi()
+    api.struct_size = C.sizeof(abi.ExtensionApi)
+    status = lib.blackframe_query_extension(C.byref(query), C.byref(api))
+    return status, api
+
+
+class Scene:
+    def __init__(self, context, handle, builder):
+        self.context = context
+        self.handle = handle
+        self.builder = builder
+
+    def close(self):
+        if self.handle:
+            library().bf200_scene_destroy(self.handle)
+            self.handle = None
+
+
+class Context:
+    def __init__(self, device=0, path_capacity=0):
+        lib = library()
+        handle = C.c_void_p()
+        status = lib.bf200_context_create(device, path_capacity, C.byref(handle))
+        if status != 0:
+            raise Bf200Error(status, f"context creation on device {device} failed")
+        self.handle = handle
+
+    def _check(self, status, what):
+        if status != 0:
+            message = library().bf200_context_last_error(self.handle)
+            raise Bf200Error(status, f"{what}: {message.decode() if message else ''}")
+
+    def close(self):
+        if self.handle:
+            library().bf200_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def create_scene(self, builder):
+        desc = builder.desc()
+        handle = C.c_void_p()
+        self._check(library().bf200_scene_create(self.handle, C.byref(desc), C.byref(handle)), "scene")
+        return Scene(self, handle, builder)
+
+    def trace_paths(self, scene, inputs, options):
+        n = len(inputs)
+        results = (abi.PathResult * n)()
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_trace_paths(self.handle, scene.handle, C.cast(inputs, C.c_void_p), n,
+                                                C.byref(options), C.cast(results, C.c_void_p),
+                                                C.byref(report)), "trace_paths")
+        return results, report
+
+    def render_film(self, scene, camera, sensor, options, samples_per_pixel, seed=0, first_sample=0,
+                    precision=0, film=None):
+        """Adds (pixel, sample) paths for samples [first_sample, first_sample + spp) to a film.
+
+        Returns (sums, counts, report): sums is float32 [H, W, 4] (r, g, b, weight) or float64
+        [H, W, 8] (sums, compensations) for precision 1.
+        """
+        w, h = camera.width, camera.height
+        if film is None:
+            sums = np.zeros((h, w, 4 if precision == 0 else 8), np.float32 if precision == 0 else np.float64)
+            counts = np.zeros((h, w), np.uint64)
+        else:
+            sums, counts = film
+        f = abi.Film(w, h, precision, 0, sums.ctypes.data_as(C.c_void_p),
+                     counts.ctypes.data_as(C.POINTER(abi.u64)))
+        request = abi.FilmRequest(C.sizeof(abi.FilmRequest), samples_per_pixel, first_sample, seed, precision)
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_render_film(self.handle, scene.handle, C.byref(camera), C.byref(sensor),
+                                                C.byref(request), C.byref(options), C.byref(f),
+                                                C.byref(report)), "render_film")
+        return sums, counts, report
+
+    def closest_hits(self, scene, rays):
+        n = len(rays)
+        hits = (abi.Hit * n)()
+        self._check(library().bf200_closest_hits(self.handle, scene.handle, C.cast(rays, C.c_void_p), n,
+                                                 C.cast(hits, C.c_void_p)), "closest_hits")
+        return hits
+
+    def occlusions(self, scene, rays):
+        n = len(rays)
+        out = np.zeros(n, np.uint32)
+        self._check(library().bf200_occlusions(self.handle, scene.handle, C.cast(rays, C.c_void_p), n,
+                                               out.ctypes.data_as(C.c_void_p)), "occlusions")
+        return out
+
+
+def camera_create(origin, normal, tangent_seed, width, height, vfov, time=0.5, jitter=1):
+    """bf200_camera_create: a pinhole camera derived exactly as PinholeCamera::create does."""
+    f3 = lambda a: (C.c_float * 3)(*[float(x) for x in a])
+    cam = abi.Camera()
+    status = library().bf200_camera_create(f3(origin), f3(normal), f3(tangent_seed), width, height,
+                                           vfov, time, jitter, C.byref(cam))
+    if status != 0:
+        raise Bf200Error(status, "camera creation")
+    return cam

@@ -1,0 +1,123 @@
+// Device-side scene layout and wavefront state of the bf200 backend.
+#pragma once
+
+#include <cstdint>
+
+#include "bf200.h"
+#include "bf200_shading.cuh"
+
+namespace bf200 {
+
+// BVH2 node, 64 bytes, both children's boxes in one node (one 64-byte fetch per step):
+//   a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   d = (child0, child1, -, -) as int bits. child >= 0: internal node index (global);
+//       child < 0: leaf, ~child = first_leaf_triangle << 3 | (count - 1).
+struct alignas(16) BvhNode {
+    float4 a, b, c;
+    int4 d;
+};
+
+constexpr int kLeafCountBits = 3;
+constexpr int kMaxLeafSize = 1 << kLeafCountBits;
+constexpr int kTraversalStack = 64;
+
+struct LightInfo {
+    uint32_t instance;
+    uint32_t tri_offset;  // into light_tri_* arrays
+    uint32_t tri_count;
+    float area;
+    float inverse_area;
+    float err_x, err_y, err_z;  // world position error of the emitter mesh
+    float radiance[4];
+};
+
+// Everything a kernel needs about a committed scene; passed by value as a kernel parameter.
+struct SceneView {
+    uint32_t instance_count;
+    uint32_t light_count;
+    const float4* inst_to_object;  // 3 rows (m0..m3) per instance
+    const float4* inst_to_world;   // 3 rows per instance
+    const uint4* inst_info;        // geometry, material, visibility mask, light index or ~0
+    const uint32_t* inst_normal_offset;
+    const uint4* geom_info;        // vertex offset, triangle offset, bvh root node, -
+    const float* positions;        // object space, 3 per vertex
+    const float* normals;          // 3 per vertex
+    const uint32_t* triangles;     // geometry-local vertex indices, 3 per triangle
+    const BvhNode* nodes;
+    const float4* leaf_tris;       // 3 per leaf triangle: v0 (w = primitive index bits), v1, v2
+    const float4* world_normals;   // per instance triangle
+    const ClosureData* closures;   // one per material
+    const float4* emission;        // per material
+    const uint4* material_info;    // closure count, frame mode, rotation bits, -
+    const float* light_select_cdf; // light_count + 1 uniform boundaries
+    const LightInfo* lights;
+    const float4* light_tri_vertices;  // 3 per light triangle, world space
+    const float4* light_tri_normals;
+    const float* light_tri_areas;
+    const float* light_tri_cdf;
+    float4 environment;
+};
+
+// Transport options resolved for the device.
+struct TransportParams {
+    uint32_t heuristic;
+    uint32_t limits[5];
+    uint32_t roulette;
+    uint32_t roulette_first;
+    float roulette_min;
+    float roulette_max;
+};
+
+// Slot states of the persistent wavefront.
+constexpr uint8_t kSlotEmpty = 0, kSlotActive = 1, kSlotDone = 2;
+
+// Path sources: film (camera rays generated on the device) or an explicit input batch.
+struct PathSource {
+    uint32_t mode;  // 0 film, 1 batch
+    uint64_t total;
+    // film
+    uint32_t width, height;
+    uint64_t first_sample;
+    uint64_t seed;
+    float cam_origin[3], cam_t[3], cam_b[3], cam_n[3];
+    float half_width, half_height, t_min, t_max, time;
+    uint32_t mask;
+    uint32_t jitter;
+    // batch
+    const bf200_path_input_v1* inputs;
+    bf200_path_result_v1* results;
+    float4* path_radiance;  // film mode: radiance per path id of the chunk
+};
+
+// Per-slot wavefront state, structure of arrays in HBM.
+struct Wavefront {
+    uint32_t capacity;
+    uint8_t* state;
+    uint64_t* path_id;
+    float4* ray_o;      // origin, t_max
+    float4* ray_d;      // direction, t_min
+    float4* beta;
+    float4* radiance;
+    uint32_t* depth;    // diffuse | glossy << 8 | specular << 16 | transmission << 24
+    float* eta;
+    float4* prev;       // previous continuous BSDF vertex position, pdf (0 = none)
+    uint32_t* flags;    // delta flags | termination << 8 | blocked << 16
+    uint32_t* status;   // lane failure code | segments << 8
+    uint2* stream;      // sample-stream prefix state (64-bit), split
+    uint32_t* mask;     // ray visibility mask of the path
+    float4* hit_tb;     // t, b0, b1, b2
+    uint2* hit_id;      // instance, primitive (instance = ~0 on a miss)
+    // shadow queue (compacted)
+    uint32_t* shadow_slot;
+    float4* shadow_o;   // origin, t_max
+    float4* shadow_d;   // direction, mask bits
+    float4* shadow_c;   // contribution (unoccluded)
+    // counters: [0] shadow queue size, [1] next path to claim, [2] active slots,
+    //           [3] extension segments, [4] shadow segments, [5] failed lanes,
+    //           [6] first failure path (min), [7] first failure code
+    unsigned long long* counters;
+};
+
+}  // namespace bf200

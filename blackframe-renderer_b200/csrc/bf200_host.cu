@@ -1,0 +1,1431 @@
+// bf200 host runtime and C ABI: context, scene build, wavefront driver, extension tables.
+//
+// Replaces, behind the C ABI of include/bf200.h:
+//   CudaSceneSoA::upload + CudaSceneBvh::build (Blackframe/Backends/GPU/CUDA/Source/SceneSoA.cpp,
+//   SceneBvh.cpp:1109-1146) -> bf200_scene_create: validation, mesh-light registry, per-geometry
+//   BLAS build (binned SAH) and the device upload;
+//   trace_cuda_wavefront_transport (WavefrontTransport.cpp:1984-2835) -> bf200_trace_paths /
+//   bf200_render_film: a persistent wavefront with in-place path regeneration. The host touches
+//   the device once per wavefront iteration (an 8-byte counter read), never per stage.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bf200.h"
+#include "bf200_device.cuh"
+#include "bf200_kernels.h"
+
+using namespace bf200;
+
+struct bf200_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t sm_count = 148;
+    uint64_t capacity = 0;
+    std::string last_error;
+    // wavefront buffers
+    void* arena = nullptr;
+    Wavefront w{};
+    unsigned long long* pinned_counters = nullptr;
+};
+
+struct bf200_scene {
+    bf200_context* context = nullptr;
+    SceneView view{};
+    std::vector<void*> allocations;
+    uint32_t light_count = 0;
+    uint64_t triangle_count = 0;
+    uint64_t node_count = 0;
+};
+
+namespace {
+
+blackframe_status fail(bf200_context* c, blackframe_status status, const std::string& message) {
+    if (c != nullptr) {
+        c->last_error = message;
+    }
+    return status;
+}
+
+blackframe_status cuda_fail(bf200_context* c, cudaError_t e, const char* what) {
+    return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host helpers restating the reference's scene-side arithmetic
+// ---------------------------------------------------------------------------------------------
+
+F3 transform_point_h(const float* m, F3 p) {  // Transforms.hpp:93-101
+    return {m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
+            m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]};
+}
+
+// SceneSurfaceInteraction.cpp:204-250 (transform_orientation): sign of the upper 3x3
+// determinant by partial-pivot elimination in double.
+bool transform_orientation(const float* m4, int& orientation) {
+    double m[9];
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) {
+            m[r * 3 + c] = static_cast<double>(m4[r * 4 + c]);
+        }
+    }
+    orientation = 1;
+    for (int col = 0; col < 3; ++col) {
+        int pr = col;
+        double pm = std::abs(m[col * 3 + col]);
+        for (int cand = col + 1; cand < 3; ++cand) {
+            const double cm = std::abs(m[cand * 3 + col]);
+            if (cm > pm) {
+                pm = cm;
+                pr = cand;
+            }
+        }
+        if (!std::isfinite(pm) || pm == 0.0) {
+            return false;
+        }
+        if (pr != col) {
+            for (int k = col; k < 3; ++k) {
+                std::swap(m[col * 3 + k], m[pr * 3 + k]);
+            }
+            orientation = -orientation;
+        }
+        const double pivot = m[col * 3 + col];
+        orientation = pivot < 0.0 ? -orientation : orientation;
+        for (int row = col + 1; row < 3; ++row) {
+            const double factor = m[row * 3 + col] / pivot;
+            for (int k = col + 1; k < 3; ++k) {
+                m[row * 3 + k] -= factor * m[col * 3 + k];
+            }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// BLAS build: binned SAH over triangle boxes, leaves of at most 4 triangles, BVH2 nodes that
+// carry both children's boxes.
+// ---------------------------------------------------------------------------------------------
+
+struct Box {
+    float lo[3] = {std::numeric_limits<float>::infinity(), std::numeric_limits<float>::infinity(),
+                   std::numeric_limits<float>::infinity()};
+    float hi[3] = {-std::numeric_limits<float>::infinity(), -std::numeric_limits<float>::infinity(),
+                   -std::numeric_limits<float>::infinity()};
+    void grow(const Box& b) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], b.lo[a]);
+            hi[a] = std::max(hi[a], b.hi[a]);
+        }
+    }
+    void grow(const float* p) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], p[a]);
+            hi[a] = std::max(hi[a], p[a]);
+        }
+    }
+    double area() const {
+        if (!(lo[0] <= hi[0])) {
+            return 0.0;
+        }
+        const double dx = double(hi[0]) - lo[0], dy = double(hi[1]) - lo[1], dz = double(hi[2]) - lo[2];
+        return 2.0 * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
+struct Prim {
+    Box box;
+    float c[3];
+    uint32_t index;
+};
+
+constexpr int kLeafSize = 4;
+constexpr int kBins = 16;
+
+struct Builder {
+    std::vector<Prim>& prims;
+    std::vector<BvhNode>& nodes;
+    std::vector<float4>& leaf_tris;
+    const float* positions;  // geometry-local base
+    const uint32_t* tris;
+    uint32_t max_depth = 0;
+
+    int make_leaf(int begin, int end) {
+        const uint32_t first = static_cast<uint32_t>(leaf_tris.size() / 3);
+        for (int i = begin; i < end; ++i) {
+            const uint32_t t = prims[i].index;
+            for (int k = 0; k < 3; ++k) {
+                const float* p = positions + 3ULL * tris[3ULL * t + k];
+                float w = 0.0F;
+                if (k == 0) {
+                    std::memcpy(&w, &t, 4);
+                }
+                leaf_tris.push_back(make_float4(p[0], p[1], p[2], w));
+            }
+        }
+        const uint32_t packed = (first << kLeafCountBits) | static_cast<uint32_t>(end - begin - 1);
+        return ~static_cast<int>(packed);
+    }
+
+    Box bounds(int begin, int end) const {
+        Box b;
+        for (int i = begin; i < end; ++i) {
+            b.grow(prims[i].box);
+        }
+        return b;
+    }
+
+    // Returns the child encoding for prims[begin, end).
+    int build(int begin, int end, uint32_t depth) {
+        max_depth = std::max(max_depth, depth);
+        const int n = end - begin;
+        if (n <= kLeafSize) {
+            return make_leaf(begin, end);
+        }
+        Box cb;
+        for (int i = begin; i < end; ++i) {
+            cb.grow(prims[i].c);
+        }
+        int best_axis = -1, best_bin = -1;
+        double best_cost = std::numeric_limits<double>::infinity();
+        for (int axis = 0; axis < 3; ++axis) {
+            const float extent = cb.hi[axis] - cb.lo[axis];
+            if (!(extent > 0.0F)) {
+                continue;
+            }
+            Box bin_box[kBins];
+            int bin_count[kBins] = {};
+            for (int i = begin; i < end; ++i) {
+                int b = static_cast<int>(kBins * ((prims[i].c[axis] - cb.lo[axis]) / extent));
+                b = std::min(std::max(b, 0), kBins - 1);
+                bin_box[b].grow(prims[i].box);
+                ++bin_count[b];
+            }
+            Box left_box[kBins];
+            int left_count[kBins];
+            Box acc;
+            int cnt = 0;
+            for (int b = 0; b < kBins; ++b) {
+                acc.grow(bin_box[b]);
+                cnt += bin_count[b];
+                left_box[b] = acc;
+                left_count[b] = cnt;
+            }
+            acc = Box{};
+            cnt = 0;
+            for (int b = kBins - 1; b > 0; --b) {
+                acc.grow(bin_box[b]);
+                cnt += bin_count[b];
+                const int lc = left_count[b - 1];
+                if (lc == 0 || cnt == 0) {
+                    continue;
+                }
+                const double cost = left_box[b - 1].area() * lc + acc.area() * cnt;
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_axis = axis;
+                    best_bin = b;
+                }
+            }
+        }
+        int mid;
+        if (best_axis < 0) {
+            mid = begin + n / 2;  // coincident centroids: split in index order
+        } else {
+            const float extent = cb.hi[best_axis] - cb.lo[best_axis];
+            auto it = std::partition(prims.begin() + begin, prims.begin() + end, [&](const Prim& p) {
+                int b = static_cast<int>(kBins * ((p.c[best_axis] - cb.lo[best_axis]) / extent));
+                b = std::min(std::max(b, 0), kBins - 1);
+                return b < best_bin;
+            });
+            mid = static_cast<int>(it - prims.begin());
+            if (mid == begin || mid == end) {
+                mid = begin + n / 2;
+            }
+        }
+        const int node_index = static_cast<int>(nodes.size());
+        nodes.push_back(BvhNode{});
+        const Box lb = bounds(begin, mid), rb = bounds(mid, end);
+        const int left = build(begin, mid, depth + 1);
+        const int right = build(mid, end, depth + 1);
+        BvhNode& node = nodes[node_index];
+        node.a = make_float4(lb.lo[0], lb.hi[0], lb.lo[1], lb.hi[1]);
+        node.b = make_float4(rb.lo[0], rb.hi[0], rb.lo[1], rb.hi[1]);
+        node.c = make_float4(lb.lo[2], lb.hi[2], rb.lo[2], rb.hi[2]);
+        node.d = make_int4(left, right, 0, 0);
+        return node_index;
+    }
+};
+
+// Builds the BLAS of one geometry; returns the root node index.
+uint32_t build_blas(const bf200_scene_desc_v1& d, uint32_t g, std::vector<BvhNode>& nodes,
+                    std::vector<float4>& leaf_tris, uint32_t& depth) {
+    const auto& geom = d.geometries[g];
+    const float* positions = d.positions + 3ULL * geom.vertex_offset;
+    const uint32_t* tris = d.triangles + 3ULL * geom.triangle_offset;
+    std::vector<Prim> prims(geom.triangle_count);
+    for (uint32_t t = 0; t < geom.triangle_count; ++t) {
+        Prim& p = prims[t];
+        for (int k = 0; k < 3; ++k) {
+            p.box.grow(positions + 3ULL * tris[3ULL * t + k]);
+        }
+        for (int a = 0; a < 3; ++a) {
+            p.c[a] = 0.5F * p.box.lo[a] + 0.5F * p.box.hi[a];
+        }
+        p.index = t;
+    }
+    Builder b{prims, nodes, leaf_tris, positions, tris};
+    const uint32_t root = static_cast<uint32_t>(nodes.size());
+    if (static_cast<int>(prims.size()) <= kLeafSize) {
+        nodes.push_back(BvhNode{});
+        const Box lb = b.bounds(0, static_cast<int>(prims.size()));
+        const int leaf = b.make_leaf(0, static_cast<int>(prims.size()));
+        const float inf = std::numeric_limits<float>::infinity();
+        BvhNode& node = nodes[root];
+        node.a = make_float4(lb.lo[0], lb.hi[0], lb.lo[1], lb.hi[1]);
+        node.b = make_float4(inf, -inf, inf, -inf);
+        node.c = make_float4(lb.lo[2], lb.hi[2], inf, -inf);
+        node.d = make_int4(leaf, leaf, 0, 0);
+        depth = 1;
+        return root;
+    }
+    const int r = b.build(0, static_cast<int>(prims.size()), 1);
+    depth = b.max_depth;
+    return static_cast<uint32_t>(r);
+}
+
+template <typename T> blackframe_status upload(bf200_scene* s, const std::vector<T>& host, const T*& out) {
+    const size_t bytes = std::max<size_t>(host.size() * sizeof(T), 16);
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        return cuda_fail(s->context, e, "device allocation");
+    }
+    s->allocations.push_back(p);
+    if (!host.empty()) {
+        e = cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            return cuda_fail(s->context, e, "scene upload");
+        }
+    }
+    out = static_cast<const T*>(p);
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+bool is_black4(const float* v) { return v[0] == 0.0F && v[1] == 0.0F && v[2] == 0.0F && v[3] == 0.0F; }
+
+// FrameScene.cpp:138-195 and AreaLights.hpp:1023-1183: one mesh light of an emissive instance.
+bool build_light(const bf200_scene_desc_v1& d, uint32_t inst_index, LightInfo& info,
+                 std::vector<float4>& tri_vertices, std::vector<float4>& tri_normals, std::vector<float>& areas,
+                 std::vector<float>& cdf, std::string& error) {
+    const auto& inst = d.instances[inst_index];
+    const auto& geom = d.geometries[inst.geometry_index];
+    const float* m = inst.object_to_world;
+    constexpr double eps = static_cast<double>(std::numeric_limits<float>::epsilon());
+    constexpr double gamma7 = (7.0 * eps) / (1.0 - 7.0 * eps);
+    constexpr double underflow = 7.0 * static_cast<double>(std::numeric_limits<float>::denorm_min());
+    float max_error[3] = {0.0F, 0.0F, 0.0F};
+    std::vector<F3> world(geom.vertex_count);
+    for (uint32_t v = 0; v < geom.vertex_count; ++v) {
+        const float* p = d.positions + 3ULL * (geom.vertex_offset + v);
+        const F3 src{p[0], p[1], p[2]};
+        world[v] = transform_point_h(m, src);
+        const float s[3] = {src.x, src.y, src.z};
+        for (int row = 0; row < 3; ++row) {
+            double magnitude = std::abs(static_cast<double>(m[row * 4 + 3]));
+            for (int col = 0; col < 3; ++col) {
+                magnitude += std::abs(static_cast<double>(m[row * 4 + col])) * std::abs(static_cast<double>(s[col]));
+            }
+            const double bound = std::fma(gamma7, magnitude, underflow);
+            float rounded = static_cast<float>(bound);
+            if (static_cast<double>(rounded) < bound) {
+                rounded = std::nextafter(rounded, std::numeric_limits<float>::infinity());
+            }
+            max_error[row] = std::max(max_error[row], rounded);
+        }
+    }
+    info.err_x = max_error[0];
+    info.err_y = max_error[1];
+    info.err_z = max_error[2];
+    info.tri_offset = static_cast<uint32_t>(areas.size());
+    info.tri_count = geom.triangle_count;
+    float sum = 0.0F, comp = 0.0F;
+    std::vector<float> local_areas;
+    for (uint32_t t = 0; t < geom.triangle_count; ++t) {
+        const uint32_t* tri = d.triangles + 3ULL * (geom.triangle_offset + t);
+        const F3 a = world[tri[0]], b = world[tri[1]], c = world[tri[2]];
+        F3 n;
+        float area;
+        if (!triangle_normal(a, b, c, n) || !triangle_area(a, b, c, area)) {
+            error = "A mesh-light triangle is not representable.";
+            return false;
+        }
+        tri_vertices.push_back(make_float4(a.x, a.y, a.z, 0.0F));
+        tri_vertices.push_back(make_float4(b.x, b.y, b.z, 0.0F));
+        tri_vertices.push_back(make_float4(c.x, c.y, c.z, 0.0F));
+        tri_normals.push_back(make_float4(n.x, n.y, n.z, 0.0F));
+        const float next = sum + area;
+        if (std::abs(sum) >= std::abs(area)) {
+            comp += (sum - next) + area;
+        } else {
+            comp += (area - next) + sum;
+        }
+        sum = next;
+        local_areas.push_back(area);
+        areas.push_back(area);
+    }
+    const float total = sum + comp;
+    if (!std::isfinite(total) || !(total > 0.0F)) {
+        error = "Mesh area-light total area is not representable.";
+        return false;
+    }
+    info.area = total;
+    info.inverse_area = 1.0F / total;
+    float cumulative = 0.0F;
+    for (size_t t = 0; t < local_areas.size(); ++t) {
+        float next = 1.0F;
+        if (t + 1 != local_areas.size()) {
+            const float selection = local_areas[t] / info.area;
+            next = cumulative + selection;
+            if (!(selection > 0.0F) || !(next > cumulative) || !(next < 1.0F)) {
+                error = "Mesh area-light selection probabilities are not distinguishable.";
+                return false;
+            }
+        }
+        cumulative = next;
+        cdf.push_back(cumulative);
+    }
+    const auto& mat = d.materials[inst.material_index];
+    for (int l = 0; l < 4; ++l) {
+        info.radiance[l] = mat.emitted_radiance[l];
+    }
+    info.instance = inst_index;
+    return true;
+}
+
+blackframe_status validate_desc(bf200_context* c, const bf200_scene_desc_v1* d) {
+    if (d == nullptr || d->struct_size < sizeof(bf200_scene_desc_v1)) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "scene description missing or too small");
+    }
+    if (d->punctual_light_count != 0) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
+                    "punctual lights are not supported by this backend version (no substitution)");
+    }
+    if (d->instance_count == 0 || d->geometry_count == 0 || d->material_count == 0) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "a scene needs geometry, materials and instances");
+    }
+    for (uint32_t g = 0; g < d->geometry_count; ++g) {
+        const auto& geom = d->geometries[g];
+        if (geom.vertex_offset + static_cast<uint64_t>(geom.vertex_count) > d->vertex_count ||
+            geom.triangle_offset + static_cast<uint64_t>(geom.triangle_count) > d->triangle_count ||
+            geom.triangle_count == 0) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "geometry range outside the scene arrays");
+        }
+        for (uint32_t t = 0; t < geom.triangle_count; ++t) {
+            for (int k = 0; k < 3; ++k) {
+                if (d->triangles[3ULL * (geom.triangle_offset + t) + k] >= geom.vertex_count) {
+                    return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "triangle vertex index out of range");
+                }
+            }
+        }
+    }
+    for (uint32_t m = 0; m < d->material_count; ++m) {
+        const auto& mat = d->materials[m];
+        if (mat.closure_count > 1) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
+                        "closure mixtures with more than one closure are not supported (no substitution)");
+        }
+        if (mat.frame_mode != 0) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "surface-tangent closure frames are not supported");
+        }
+        if (mat.closure_count == 1) {
+            if (mat.closure_offset >= d->closure_count) {
+                return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "closure index out of range");
+            }
+            const uint32_t kind = d->closures[mat.closure_offset].kind;
+            if (kind != BF200_CLOSURE_LAMBERTIAN_REFLECTION && kind != BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION &&
+                kind != BF200_CLOSURE_ROUGH_DIELECTRIC) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "closure kind not supported by this backend");
+            }
+        }
+    }
+    for (uint32_t i = 0; i < d->instance_count; ++i) {
+        const auto& inst = d->instances[i];
+        if (inst.geometry_index >= d->geometry_count || inst.material_index >= d->material_count) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "instance references out of range");
+        }
+        const float* m = inst.object_to_world;
+        if (m[12] != 0.0F || m[13] != 0.0F || m[14] != 0.0F || m[15] != 1.0F) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "an instance transform must be affine");
+        }
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+blackframe_status ensure_capacity(bf200_context* c) {
+    if (c->arena != nullptr) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    const uint64_t n = c->capacity;
+    const size_t bytes_per_slot = 1 + 8 + 16 * 4 + 4 + 4 + 16 + 4 + 4 + 8 + 4 + 16 + 8 + 4 + 16 * 3;
+    const size_t total = n * bytes_per_slot + 64 * 16 + 8 * sizeof(unsigned long long) + 4096;
+    cudaError_t e = cudaMalloc(&c->arena, total);
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "wavefront allocation");
+    }
+    char* p = static_cast<char*>(c->arena);
+    auto take = [&](size_t size) {
+        p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+        char* r = p;
+        p += size;
+        return r;
+    };
+    Wavefront& w = c->w;
+    w.capacity = static_cast<uint32_t>(n);
+    w.ray_o = reinterpret_cast<float4*>(take(16 * n));
+    w.ray_d = reinterpret_cast<float4*>(take(16 * n));
+    w.beta = reinterpret_cast<float4*>(take(16 * n));
+    w.radiance = reinterpret_cast<float4*>(take(16 * n));
+    w.prev = reinterpret_cast<float4*>(take(16 * n));
+    w.hit_tb = reinterpret_cast<float4*>(take(16 * n));
+    w.shadow_o = reinterpret_cast<float4*>(take(16 * n));
+    w.shadow_d = reinterpret_cast<float4*>(take(16 * n));
+    w.shadow_c = reinterpret_cast<float4*>(take(16 * n));
+    w.path_id = reinterpret_cast<uint64_t*>(take(8 * n));
+    w.stream = reinterpret_cast<uint2*>(take(8 * n));
+    w.hit_id = reinterpret_cast<uint2*>(take(8 * n));
+    w.depth = reinterpret_cast<uint32_t*>(take(4 * n));
+    w.eta = reinterpret_cast<float*>(take(4 * n));
+    w.flags = reinterpret_cast<uint32_t*>(take(4 * n));
+    w.status = reinterpret_cast<uint32_t*>(take(4 * n));
+    w.mask = reinterpret_cast<uint32_t*>(take(4 * n));
+    w.shadow_slot = reinterpret_cast<uint32_t*>(take(4 * n));
+    w.state = reinterpret_cast<uint8_t*>(take(n));
+    w.counters = reinterpret_cast<unsigned long long*>(take(8 * sizeof(unsigned long long)));
+    if (static_cast<size_t>(p - static_cast<char*>(c->arena)) > total) {
+        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "wavefront arena layout overflow");
+    }
+    e = cudaMallocHost(&c->pinned_counters, 8 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "pinned counters");
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+TransportParams make_params(const bf200_transport_options_v1& o) {
+    TransportParams p{};
+    p.heuristic = o.mis_heuristic;
+    for (int i = 0; i < 5; ++i) {
+        p.limits[i] = o.depth_limits[i];
+    }
+    p.roulette = o.roulette_enabled;
+    p.roulette_first = o.roulette_first_eligible_depth;
+    p.roulette_min = o.roulette_minimum_survival;
+    p.roulette_max = o.roulette_maximum_survival;
+    return p;
+}
+
+blackframe_status validate_options(bf200_context* c, const bf200_transport_options_v1* o) {
+    if (o == nullptr || o->struct_size < sizeof(bf200_transport_options_v1)) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "transport options missing or too small");
+    }
+    if (o->mis_heuristic > 1) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "unknown MIS heuristic");
+    }
+    for (int i = 0; i < 4; ++i) {
+        if (o->depth_limits[i] > 255) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "depth limits above 255 are not supported");
+        }
+    }
+    if (o->roulette_enabled != 0) {
+        // RussianRoulette.hpp:24-55 (create_enabled)
+        if (o->roulette_first_eligible_depth == 0 || !std::isfinite(o->roulette_minimum_survival) ||
+            !std::isfinite(o->roulette_maximum_survival) || !(o->roulette_minimum_survival > 0.0F) ||
+            !(o->roulette_minimum_survival < 1.0F) ||
+            o->roulette_maximum_survival < o->roulette_minimum_survival || o->roulette_maximum_survival > 1.0F) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "invalid Russian roulette policy");
+        }
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+// Runs the persistent wavefront until every path of `src` has been traced and retired.
+blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSource src, const TransportParams& p,
+                                bool instrument, bf200_report_v1* report) {
+    Wavefront& w = c->w;
+    cudaStream_t st = c->stream;
+    cudaError_t e = cudaMemsetAsync(w.state, 0, w.capacity, st);
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), st);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "wavefront reset");
+    }
+    // counters[6] holds the minimum failing path id
+    static const unsigned long long kNone = ~0ULL;
+    cudaMemcpyAsync(w.counters + 6, &kNone, sizeof(kNone), cudaMemcpyHostToDevice, st);
+    const uint32_t grid =
+        std::max<uint32_t>(1, std::min<uint32_t>((w.capacity + 255U) / 256U, c->sm_count * 8U));
+    cudaEvent_t ev[4];
+    for (auto& x : ev) {
+        cudaEventCreate(&x);
+    }
+    cudaEventRecord(ev[0], st);
+    const cudaEvent_t start = ev[0];
+    cudaEvent_t stop;
+    cudaEventCreate(&stop);
+    uint64_t iterations = 0, launches = 0, shadow_segments = 0;
+    double stage_ms[3] = {0.0, 0.0, 0.0};
+    // every path finishes within (sum of surface depth limits + 1) extension segments, and a
+    // slot hosts at most ceil(total / capacity) + 1 paths: bound the host loop accordingly
+    const uint64_t depth_bound = static_cast<uint64_t>(p.limits[0]) + p.limits[1] + p.limits[2] + 2;
+    const uint64_t max_iterations = 64 + 2 * (src.total / w.capacity + 2) * depth_bound;
+    while (iterations < max_iterations) {
+        // the shadow queue and the active count are per iteration
+        cudaMemsetAsync(w.counters + 0, 0, sizeof(unsigned long long), st);
+        cudaMemsetAsync(w.counters + 2, 0, sizeof(unsigned long long), st);
+        for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage) {
+            if (instrument) {
+                cudaEventRecord(ev[stage], st);
+            }
+            e = launch_stage(stage, s->view, w, src, p, grid, st);
+        }
+        if (instrument) {
+            cudaEventRecord(ev[3], st);
+        }
+        launches += 3;
+        ++iterations;
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "wavefront launch");
+        }
+        e = cudaMemcpyAsync(c->pinned_counters, w.counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            st);
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(st);
+        }
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "wavefront iteration");
+        }
+        if (instrument) {
+            for (int stage = 0; stage < 3; ++stage) {
+                float ms = 0.0F;
+                cudaEventElapsedTime(&ms, ev[stage], ev[stage + 1]);
+                stage_ms[stage] += ms;
+            }
+        }
+        shadow_segments += c->pinned_counters[0];
+        const unsigned long long active = c->pinned_counters[2];
+        const unsigned long long claimed = c->pinned_counters[1];
+        if (active == 0 && claimed >= src.total) {
+            break;
+        }
+    }
+    if (iterations >= max_iterations) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "the wavefront did not drain within its iteration bound");
+    }
+    // retire the last finished slots
+    e = launch_retire(s->view, w, src, grid, st);
+    ++launches;
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(c->pinned_counters, w.counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            st);
+    }
+    cudaEventRecord(stop, st);
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "wavefront retire");
+    }
+    float ms = 0.0F;
+    cudaEventElapsedTime(&ms, start, stop);
+    for (auto& x : ev) {
+        cudaEventDestroy(x);
+    }
+    cudaEventDestroy(stop);
+    if (report != nullptr) {
+        report->struct_size = sizeof(bf200_report_v1);
+        report->registered_light_count = s->light_count;
+        report->path_count += src.total;
+        report->extension_segments += c->pinned_counters[3];
+        report->shadow_segments += shadow_segments;
+        report->failed_lanes += c->pinned_counters[5];
+        if (c->pinned_counters[5] != 0 && report->first_failure_status == 0) {
+            report->first_failure_status = static_cast<uint32_t>(c->pinned_counters[7]);
+            report->first_failure_path = static_cast<uint32_t>(c->pinned_counters[6]);
+        }
+        report->kernel_launches += launches;
+        report->gpu_milliseconds += ms;
+        report->intersect_milliseconds += stage_ms[0];
+        report->shade_milliseconds += stage_ms[1];
+        report->occlude_milliseconds += stage_ms[2];
+        report->iterations += iterations;
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+
+extern "C" {
+
+BF200_EXPORT const char* bf200_build_info(void) noexcept {
+    return "bf200 wavefront path tracer, sm_100a, render ABI 1.0";
+}
+
+namespace {
+
+// LocalFrame.hpp:32-48 (robust_unit_vector) on the host.
+bool host_unit(const float* v, float* out) {
+    const float m = std::max({std::abs(v[0]), std::abs(v[1]), std::abs(v[2])});
+    if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]) || m == 0.0F) {
+        return false;
+    }
+    const float s[3] = {v[0] / m, v[1] / m, v[2] / m};
+    const float magnitude = std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    out[0] = s[0] / magnitude;
+    out[1] = s[1] / magnitude;
+    out[2] = s[2] / magnitude;
+    return true;
+}
+
+void host_cross(const float* a, const float* b, float* out) {
+    out[0] = a[1] * b[2] - a[2] * b[1];
+    out[1] = a[2] * b[0] - a[0] * b[2];
+    out[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+}  // namespace
+
+BF200_EXPORT blackframe_status bf200_camera_create(const float origin[3], const float normal[3],
+                                                    const float tangent_seed[3], uint32_t width, uint32_t height,
+                                                    float vfov, float time, uint32_t jitter_mode,
+                                                    bf200_camera_v1* out) noexcept {
+    if (origin == nullptr || normal == nullptr || tangent_seed == nullptr || out == nullptr || width == 0 ||
+        height == 0 || !std::isfinite(vfov) || vfov <= 0.0F || vfov >= 3.14159265358979323846F) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    // from_normal_and_tangent: robust_unit_normal (LocalFrame.hpp:8-30), then
+    // from_unit_normal_and_tangent (LocalFrame.hpp:188-219)
+    float n[3], td[3], t[3], b[3];
+    {
+        const float m = std::max({std::abs(normal[0]), std::abs(normal[1]), std::abs(normal[2])});
+        if (m == 0.0F) {
+            return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+        }
+        const float s[3] = {normal[0] / m, normal[1] / m, normal[2] / m};
+        const float magnitude = std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+        n[0] = s[0] / magnitude;
+        n[1] = s[1] / magnitude;
+        n[2] = s[2] / magnitude;
+    }
+    if (!host_unit(tangent_seed, td)) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    const float d = td[0] * n[0] + td[1] * n[1] + td[2] * n[2];
+    const float projected[3] = {td[0] - n[0] * d, td[1] - n[1] * d, td[2] - n[2] * d};
+    float c[3];
+    if (!host_unit(projected, t)) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    host_cross(n, t, c);
+    if (!host_unit(c, b)) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    host_cross(b, n, c);
+    if (!host_unit(c, t)) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    *out = bf200_camera_v1{};
+    for (int a = 0; a < 3; ++a) {
+        out->origin[a] = origin[a];
+        out->tangent[a] = t[a];
+        out->bitangent[a] = b[a];
+        out->normal[a] = n[a];
+    }
+    const float half_height = std::tan(vfov / 2.0F);
+    out->half_height = half_height;
+    out->half_width = half_height * (static_cast<float>(width) / static_cast<float>(height));
+    out->t_min = 0.0F;
+    out->t_max = std::numeric_limits<float>::infinity();
+    out->time = time;
+    out->mask = 0xFFFFFFFFU;
+    out->width = width;
+    out->height = height;
+    out->jitter_mode = jitter_mode;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT blackframe_status bf200_context_create(int32_t device_ordinal, uint64_t path_capacity,
+                                                     bf200_context** out_context) noexcept {
+    if (out_context == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    *out_context = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device_ordinal < 0 || device_ordinal >= count) {
+        return BLACKFRAME_STATUS_OUT_OF_RANGE;
+    }
+    auto* c = new (std::nothrow) bf200_context{};
+    if (c == nullptr) {
+        return BLACKFRAME_STATUS_EXTENSION_FAILURE;
+    }
+    c->device = device_ordinal;
+    cudaSetDevice(device_ordinal);
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device_ordinal) != cudaSuccess || prop.major < 10) {
+        delete c;
+        return BLACKFRAME_STATUS_INVALID_STATE;
+    }
+    c->sm_count = static_cast<uint32_t>(prop.multiProcessorCount);
+    c->capacity = path_capacity != 0 ? path_capacity : (1ULL << 21);
+    if (c->capacity > (1ULL << 26)) {
+        delete c;
+        return BLACKFRAME_STATUS_OUT_OF_RANGE;
+    }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return BLACKFRAME_STATUS_EXTENSION_FAILURE;
+    }
+    *out_context = c;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT blackframe_status bf200_context_destroy(bf200_context* c) noexcept {
+    if (c == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(c->device);
+    if (c->stream != nullptr) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
+    if (c->arena != nullptr) {
+        cudaFree(c->arena);
+    }
+    if (c->pinned_counters != nullptr) {
+        cudaFreeHost(c->pinned_counters);
+    }
+    delete c;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT const char* bf200_context_last_error(const bf200_context* c) noexcept {
+    return c == nullptr ? "null context" : c->last_error.c_str();
+}
+
+BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_scene_desc_v1* d,
+                                                   bf200_scene** out_scene) noexcept {
+    if (c == nullptr || out_scene == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    *out_scene = nullptr;
+    if (const auto st = validate_desc(c, d); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    cudaSetDevice(c->device);
+    auto scene = std::make_unique<bf200_scene>();
+    scene->context = c;
+    try {
+        // BLAS per geometry
+        std::vector<BvhNode> nodes;
+        std::vector<float4> leaf_tris;
+        std::vector<uint4> geom_info(d->geometry_count);
+        for (uint32_t g = 0; g < d->geometry_count; ++g) {
+            uint32_t depth = 0;
+            const uint32_t root = build_blas(*d, g, nodes, leaf_tris, depth);
+            if (depth + 2 >= kTraversalStack) {
+                return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "BLAS deeper than the traversal stack");
+            }
+            geom_info[g] = make_uint4(d->geometries[g].vertex_offset, d->geometries[g].triangle_offset, root, 0);
+        }
+        scene->node_count = nodes.size();
+        scene->triangle_count = leaf_tris.size() / 3;
+        // instances, mesh lights (FrameScene.cpp:201-261) and the uniform light sampler
+        std::vector<float4> to_object(3ULL * d->instance_count), to_world(3ULL * d->instance_count);
+        std::vector<uint4> inst_info(d->instance_count);
+        std::vector<uint32_t> normal_offset(d->instance_count);
+        std::vector<uint32_t> tri_instance, tri_local;
+        std::vector<LightInfo> lights;
+        std::vector<float4> light_vertices, light_normals;
+        std::vector<float> light_areas, light_cdf;
+        for (uint32_t i = 0; i < d->instance_count; ++i) {
+            const auto& inst = d->instances[i];
+            for (int r = 0; r < 3; ++r) {
+                const float* a = inst.world_to_object + 4 * r;
+                const float* b = inst.object_to_world + 4 * r;
+                to_object[3ULL * i + r] = make_float4(a[0], a[1], a[2], a[3]);
+                to_world[3ULL * i + r] = make_float4(b[0], b[1], b[2], b[3]);
+            }
+            int orientation = 1;
+            if (!transform_orientation(inst.object_to_world, orientation)) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "instance transform orientation is singular");
+            }
+            uint32_t light_index = 0x7FFFFFFFU;
+            if (is_black4(d->materials[inst.material_index].emitted_radiance) == false) {
+                LightInfo info{};
+                std::string error;
+                if (!build_light(*d, i, info, light_vertices, light_normals, light_areas, light_cdf, error)) {
+                    return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, error);
+                }
+                light_index = static_cast<uint32_t>(lights.size());
+                lights.push_back(info);
+            }
+            inst_info[i] = make_uint4(inst.geometry_index, inst.material_index, inst.visibility_mask,
+                                      light_index | (orientation < 0 ? 0x80000000U : 0U));
+            normal_offset[i] = static_cast<uint32_t>(tri_instance.size());
+            for (uint32_t t = 0; t < d->geometries[inst.geometry_index].triangle_count; ++t) {
+                tri_instance.push_back(i);
+                tri_local.push_back(t);
+            }
+        }
+        if (lights.empty()) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
+                        "MIS requires at least one emissive mesh light in the committed scene");
+        }
+        // LightSampler::create_uniform (LightSampler.cpp:574-602)
+        std::vector<float> select(lights.size() + 1, 0.0F);
+        for (size_t k = 1; k < lights.size(); ++k) {
+            select[k] = static_cast<float>(k) / static_cast<float>(lights.size());
+        }
+        select[lights.size()] = 1.0F;
+        scene->light_count = static_cast<uint32_t>(lights.size());
+        // materials
+        std::vector<ClosureData> closures(d->material_count);
+        std::vector<float4> emission(d->material_count);
+        std::vector<uint4> material_info(d->material_count);
+        for (uint32_t m = 0; m < d->material_count; ++m) {
+            const auto& mat = d->materials[m];
+            ClosureData cd{};
+            if (mat.closure_count == 1) {
+                const auto& src = d->closures[mat.closure_offset];
+                cd.kind = src.kind;
+                cd.lobes = src.lobes;
+                std::memcpy(cd.w, src.weight, sizeof(cd.w));
+                std::memcpy(cd.p, src.parameters, sizeof(cd.p));
+            }
+            closures[m] = cd;
+            emission[m] = make_float4(mat.emitted_radiance[0], mat.emitted_radiance[1], mat.emitted_radiance[2],
+                                      mat.emitted_radiance[3]);
+            uint32_t rotation_bits;
+            std::memcpy(&rotation_bits, &mat.tangent_rotation_radians, 4);
+            material_info[m] = make_uint4(mat.closure_count, mat.frame_mode, rotation_bits, 0);
+        }
+        std::vector<float> positions(d->positions, d->positions + 3ULL * d->vertex_count);
+        std::vector<float> normals(d->normals, d->normals + 3ULL * d->vertex_count);
+        std::vector<uint32_t> triangles(d->triangles, d->triangles + 3ULL * d->triangle_count);
+        SceneView& v = scene->view;
+        v.instance_count = d->instance_count;
+        v.light_count = scene->light_count;
+        blackframe_status st = BLACKFRAME_STATUS_SUCCESS;
+        auto up = [&](auto& host, auto& dst) {
+            if (st == BLACKFRAME_STATUS_SUCCESS) {
+                st = upload(scene.get(), host, dst);
+            }
+        };
+        up(to_object, v.inst_to_object);
+        up(to_world, v.inst_to_world);
+        up(inst_info, v.inst_info);
+        up(normal_offset, v.inst_normal_offset);
+        up(geom_info, v.geom_info);
+        up(positions, v.positions);
+        up(normals, v.normals);
+        up(triangles, v.triangles);
+        up(nodes, v.nodes);
+        up(leaf_tris, v.leaf_tris);
+        up(closures, v.closures);
+        up(emission, v.emission);
+        up(material_info, v.material_info);
+        up(select, v.light_select_cdf);
+        up(lights, v.lights);
+        up(light_vertices, v.light_tri_vertices);
+        up(light_normals, v.light_tri_normals);
+        up(light_areas, v.light_tri_areas);
+        up(light_cdf, v.light_tri_cdf);
+        const uint32_t* d_tri_instance = nullptr;
+        const uint32_t* d_tri_local = nullptr;
+        up(tri_instance, d_tri_instance);
+        up(tri_local, d_tri_local);
+        if (st != BLACKFRAME_STATUS_SUCCESS) {
+            return st;
+        }
+        v.environment = make_float4(d->environment_radiance[0], d->environment_radiance[1],
+                                    d->environment_radiance[2], d->environment_radiance[3]);
+        // world-space geometric normals of every instance triangle, on the device
+        float4* world_normals = nullptr;
+        uint32_t* failures = nullptr;
+        cudaError_t e = cudaMalloc(&world_normals, std::max<size_t>(16, tri_instance.size() * sizeof(float4)));
+        if (e == cudaSuccess) {
+            scene->allocations.push_back(world_normals);
+            e = cudaMalloc(&failures, sizeof(uint32_t));
+        }
+        if (e == cudaSuccess) {
+            scene->allocations.push_back(failures);
+            e = cudaMemsetAsync(failures, 0, sizeof(uint32_t), c->stream);
+        }
+        if (e == cudaSuccess) {
+            e = launch_world_normals(v, d_tri_instance, d_tri_local, static_cast<uint32_t>(tri_instance.size()),
+                                     world_normals, failures, c->stream);
+        }
+        uint32_t host_failures = 0;
+        if (e == cudaSuccess) {
+            e = cudaMemcpyAsync(&host_failures, failures, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream);
+        }
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(c->stream);
+        }
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "scene build");
+        }
+        if (host_failures != 0) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "a world-space triangle normal is not representable");
+        }
+        v.world_normals = world_normals;
+    } catch (const std::bad_alloc&) {
+        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "scene build exhausted host memory");
+    }
+    *out_scene = scene.release();
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT blackframe_status bf200_scene_destroy(bf200_scene* s) noexcept {
+    if (s == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(s->context->device);
+    cudaStreamSynchronize(s->context->stream);
+    for (void* p : s->allocations) {
+        cudaFree(p);
+    }
+    delete s;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT blackframe_status bf200_trace_paths_device(bf200_context* c, const bf200_scene* s,
+                                                         const bf200_path_input_v1* device_inputs,
+                                                         uint64_t path_count, const bf200_transport_options_v1* o,
+                                                         bf200_path_result_v1* device_results,
+                                                         bf200_report_v1* report) noexcept {
+    if (c == nullptr || s == nullptr || (path_count != 0 && (device_inputs == nullptr || device_results == nullptr))) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (s->context != c) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "scene belongs to another context");
+    }
+    if (const auto st = validate_options(c, o); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    if (report != nullptr) {
+        std::memset(report, 0, sizeof(*report));
+    }
+    if (path_count == 0) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    cudaSetDevice(c->device);
+    if (const auto st = ensure_capacity(c); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    PathSource src{};
+    src.mode = 1;
+    src.total = path_count;
+    src.inputs = device_inputs;
+    src.results = device_results;
+    return run_wavefront(c, s, src, make_params(*o), o->instrumentation != 0, report);
+}
+
+BF200_EXPORT blackframe_status bf200_trace_paths(bf200_context* c, const bf200_scene* s,
+                                                  const bf200_path_input_v1* inputs, uint64_t path_count,
+                                                  const bf200_transport_options_v1* o, bf200_path_result_v1* results,
+                                                  bf200_report_v1* report) noexcept {
+    if (c == nullptr || s == nullptr || (path_count != 0 && (inputs == nullptr || results == nullptr))) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (path_count == 0) {
+        return bf200_trace_paths_device(c, s, nullptr, 0, o, nullptr, report);
+    }
+    cudaSetDevice(c->device);
+    bf200_path_input_v1* d_in = nullptr;
+    bf200_path_result_v1* d_out = nullptr;
+    cudaError_t e = cudaMalloc(&d_in, path_count * sizeof(bf200_path_input_v1));
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&d_out, path_count * sizeof(bf200_path_result_v1));
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(d_in, inputs, path_count * sizeof(bf200_path_input_v1), cudaMemcpyHostToDevice,
+                            c->stream);
+    }
+    blackframe_status st = e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "batch upload");
+    if (st == BLACKFRAME_STATUS_SUCCESS) {
+        st = bf200_trace_paths_device(c, s, d_in, path_count, o, d_out, report);
+    }
+    if (st == BLACKFRAME_STATUS_SUCCESS) {
+        e = cudaMemcpyAsync(results, d_out, path_count * sizeof(bf200_path_result_v1), cudaMemcpyDeviceToHost,
+                            c->stream);
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(c->stream);
+        }
+        if (e != cudaSuccess) {
+            st = cuda_fail(c, e, "batch download");
+        }
+    }
+    cudaFree(d_in);
+    cudaFree(d_out);
+    return st;
+}
+
+BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const bf200_scene* s,
+                                                         const bf200_camera_v1* cam, const bf200_sensor_v1* sensor,
+                                                         const bf200_film_request_v1* req,
+                                                         const bf200_transport_options_v1* o, bf200_film_v1* film,
+                                                         bf200_report_v1* report) noexcept {
+    if (c == nullptr || s == nullptr || cam == nullptr || sensor == nullptr || req == nullptr || film == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (req->struct_size < sizeof(bf200_film_request_v1) || req->precision > 1 || film->precision != req->precision ||
+        film->width != cam->width || film->height != cam->height || cam->width == 0 || cam->height == 0 ||
+        film->sums == nullptr || film->sample_counts == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "inconsistent film request");
+    }
+    if (const auto st = validate_options(c, o); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    if (report != nullptr) {
+        std::memset(report, 0, sizeof(*report));
+    }
+    cudaSetDevice(c->device);
+    if (const auto st = ensure_capacity(c); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    const uint64_t pixels = static_cast<uint64_t>(cam->width) * cam->height;
+    if (pixels > 0xFFFFFFFFULL) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "film too large");
+    }
+    // chunks of whole sample passes, at most ~64M paths of radiance per chunk
+    const uint64_t max_chunk_paths = 1ULL << 26;
+    uint64_t samples_per_chunk = std::max<uint64_t>(1, max_chunk_paths / pixels);
+    samples_per_chunk = std::min<uint64_t>(samples_per_chunk, req->samples_per_pixel);
+    float4* radiance = nullptr;
+    unsigned long long* skipped = nullptr;
+    cudaError_t e = cudaMalloc(&radiance, std::max<uint64_t>(1, samples_per_chunk * pixels) * sizeof(float4));
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&skipped, sizeof(unsigned long long));
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(skipped, 0, sizeof(unsigned long long), c->stream);
+    }
+    if (e != cudaSuccess) {
+        cudaFree(radiance);
+        return cuda_fail(c, e, "film chunk allocation");
+    }
+    const TransportParams params = make_params(*o);
+    blackframe_status st = BLACKFRAME_STATUS_SUCCESS;
+    for (uint64_t first = 0; first < req->samples_per_pixel && st == BLACKFRAME_STATUS_SUCCESS;
+         first += samples_per_chunk) {
+        const uint64_t chunk = std::min<uint64_t>(samples_per_chunk, req->samples_per_pixel - first);
+        PathSource src{};
+        src.mode = 0;
+        src.total = chunk * pixels;
+        src.width = cam->width;
+        src.height = cam->height;
+        src.first_sample = req->first_sample + first;
+        src.seed = req->seed;
+        for (int a = 0; a < 3; ++a) {
+            src.cam_origin[a] = cam->origin[a];
+            src.cam_t[a] = cam->tangent[a];
+            src.cam_b[a] = cam->bitangent[a];
+            src.cam_n[a] = cam->normal[a];
+        }
+        src.half_width = cam->half_width;
+        src.half_height = cam->half_height;
+        src.t_min = cam->t_min;
+        src.t_max = cam->t_max;
+        src.time = cam->time;
+        src.mask = cam->mask;
+        src.jitter = cam->jitter_mode;
+        src.path_radiance = radiance;
+        st = run_wavefront(c, s, src, params, o->instrumentation != 0, report);
+        cudaEvent_t film_start = nullptr, film_stop = nullptr;
+        if (st == BLACKFRAME_STATUS_SUCCESS && o->instrumentation != 0) {
+            cudaEventCreate(&film_start);
+            cudaEventCreate(&film_stop);
+            cudaEventRecord(film_start, c->stream);
+        }
+        if (st == BLACKFRAME_STATUS_SUCCESS) {
+            e = launch_film(radiance, static_cast<uint32_t>(pixels), static_cast<uint32_t>(chunk),
+                            &sensor->response_xyz[0][0], sensor->wavelength_pdf, sensor->normalization,
+                            req->precision, req->precision == 0 ? static_cast<float4*>(film->sums) : nullptr,
+                            req->precision == 1 ? static_cast<double*>(film->sums) : nullptr,
+                            reinterpret_cast<unsigned long long*>(film->sample_counts), skipped, c->stream);
+            if (report != nullptr) {
+                report->kernel_launches += 1;
+            }
+            if (e != cudaSuccess) {
+                st = cuda_fail(c, e, "film accumulation");
+            }
+        }
+        if (film_start != nullptr) {
+            cudaEventRecord(film_stop, c->stream);
+            cudaEventSynchronize(film_stop);
+            float fms = 0.0F;
+            cudaEventElapsedTime(&fms, film_start, film_stop);
+            if (report != nullptr) {
+                report->film_milliseconds += fms;
+                report->gpu_milliseconds += fms;
+            }
+            cudaEventDestroy(film_start);
+            cudaEventDestroy(film_stop);
+        }
+    }
+    if (st == BLACKFRAME_STATUS_SUCCESS) {
+        e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            st = cuda_fail(c, e, "film synchronisation");
+        }
+    }
+    cudaFree(radiance);
+    cudaFree(skipped);
+    return st;
+}
+
+BF200_EXPORT blackframe_status bf200_render_film(bf200_context* c, const bf200_scene* s, const bf200_camera_v1* cam,
+                                                  const bf200_sensor_v1* sensor, const bf200_film_request_v1* req,
+                                                  const bf200_transport_options_v1* o, bf200_film_v1* host_film,
+                                                  bf200_report_v1* report) noexcept {
+    if (c == nullptr || host_film == nullptr || host_film->sums == nullptr || host_film->sample_counts == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    cudaSetDevice(c->device);
+    const uint64_t pixels = static_cast<uint64_t>(host_film->width) * host_film->height;
+    const size_t sum_bytes = pixels * (host_film->precision == 0 ? 16 : 64);
+    void* d_sums = nullptr;
+    uint64_t* d_counts = nullptr;
+    cudaError_t e = cudaMalloc(&d_sums, std::max<size_t>(16, sum_bytes));
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&d_counts, std::max<size_t>(8, pixels * 8));
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(d_sums, host_film->sums, sum_bytes, cudaMemcpyHostToDevice, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(d_counts, host_film->sample_counts, pixels * 8, cudaMemcpyHostToDevice, c->stream);
+    }
+    blackframe_status st = e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "film upload");
+    if (st == BLACKFRAME_STATUS_SUCCESS) {
+        bf200_film_v1 dev = *host_film;
+        dev.sums = d_sums;
+        dev.sample_counts = d_counts;
+        st = bf200_render_film_device(c, s, cam, sensor, req, o, &dev, report);
+    }
+    if (st == BLACKFRAME_STATUS_SUCCESS) {
+        e = cudaMemcpyAsync(host_film->sums, d_sums, sum_bytes, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) {
+            e = cudaMemcpyAsync(host_film->sample_counts, d_counts, pixels * 8, cudaMemcpyDeviceToHost, c->stream);
+        }
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(c->stream);
+        }
+        if (e != cudaSuccess) {
+            st = cuda_fail(c, e, "film download");
+        }
+    }
+    cudaFree(d_sums);
+    cudaFree(d_counts);
+    return st;
+}
+
+static blackframe_status run_queries(bf200_context* c, const bf200_scene* s, const bf200_ray_v1* rays, uint64_t n,
+                                     bf200_hit_v1* hits, uint32_t* occluded) {
+    if (c == nullptr || s == nullptr || (n != 0 && rays == nullptr)) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (n == 0) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    cudaSetDevice(c->device);
+    bf200_ray_v1* d_rays = nullptr;
+    void* d_out = nullptr;
+    const size_t out_bytes = n * (hits != nullptr ? sizeof(bf200_hit_v1) : sizeof(uint32_t));
+    cudaError_t e = cudaMalloc(&d_rays, n * sizeof(bf200_ray_v1));
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&d_out, out_bytes);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(d_rays, rays, n * sizeof(bf200_ray_v1), cudaMemcpyHostToDevice, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = launch_queries(s->view, d_rays, n, hits != nullptr ? static_cast<bf200_hit_v1*>(d_out) : nullptr,
+                           hits != nullptr ? nullptr : static_cast<uint32_t*>(d_out), c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(hits != nullptr ? static_cast<void*>(hits) : static_cast<void*>(occluded), d_out, out_bytes,
+                            cudaMemcpyDeviceToHost, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(d_rays);
+    cudaFree(d_out);
+    return e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "query");
+}
+
+BF200_EXPORT blackframe_status bf200_closest_hits(bf200_context* c, const bf200_scene* s, const bf200_ray_v1* rays,
+                                                   uint64_t n, bf200_hit_v1* hits) noexcept {
+    if (hits == nullptr && n != 0) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null hits");
+    }
+    return run_queries(c, s, rays, n, hits, nullptr);
+}
+
+BF200_EXPORT blackframe_status bf200_occlusions(bf200_context* c, const bf200_scene* s, const bf200_ray_v1* rays,
+                                                 uint64_t n, uint32_t* occluded) noexcept {
+    if (occluded == nullptr && n != 0) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null output");
+    }
+    return run_queries(c, s, rays, n, nullptr, occluded);
+}
+
+// --------------------------------------------------------------------------------------------
+// Extension ABI v1 + XPU v1 enumeration + render interface v1
+// --------------------------------------------------------------------------------------------
+
+namespace {
+
+constexpr char kBackendName[] = "bf200 B200 wavefront";
+constexpr char kVendorName[] = "NVIDIA";
+
+struct DeviceNames {
+    char name[256];
+};
+DeviceNames g_device_names[64];
+
+blackframe_utf8_view view_of(const char* text) {
+    return blackframe_utf8_view{text, static_cast<uint32_t>(std::strlen(text)), 0};
+}
+
+blackframe_status xpu_device_count(void*, uint32_t* out) noexcept {
+    if (out == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        count = 0;
+    }
+    *out = static_cast<uint32_t>(std::min(count, 64));
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+blackframe_status xpu_device_descriptor(void*, uint32_t index, blackframe_xpu_device_descriptor_v1* out) noexcept {
+    if (out == nullptr || out->struct_size < sizeof(blackframe_xpu_device_descriptor_v1)) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    uint32_t count = 0;
+    xpu_device_count(nullptr, &count);
+    if (index >= count) {
+        return BLACKFRAME_STATUS_OUT_OF_RANGE;
+    }
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, static_cast<int>(index)) != cudaSuccess) {
+        return BLACKFRAME_STATUS_EXTENSION_FAILURE;
+    }
+    std::snprintf(g_device_names[index].name, sizeof(g_device_names[index].name), "%s", prop.name);
+    uint64_t high = 0, low = 0;
+    std::memcpy(&high, prop.uuid.bytes, 8);
+    std::memcpy(&low, prop.uuid.bytes + 8, 8);
+    *out = blackframe_xpu_device_descriptor_v1{};
+    out->struct_size = sizeof(blackframe_xpu_device_descriptor_v1);
+    out->kind = BLACKFRAME_XPU_DEVICE_KIND_GPU;
+    out->identifier_high = high;
+    out->identifier_low = low;
+    out->name = view_of(g_device_names[index].name);
+    out->vendor = view_of(kVendorName);
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+blackframe_status get_interface(void*, blackframe_interface_id id, uint32_t major, uint32_t, void* out,
+                                uint32_t out_size) noexcept {
+    if (out == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    if (id.high == BLACKFRAME_XPU_BACKEND_INTERFACE_ID_HIGH && id.low == BLACKFRAME_XPU_BACKEND_INTERFACE_ID_LOW) {
+        if (out_size < sizeof(blackframe_xpu_backend_api_v1)) {
+            return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+        }
+        if (major != BLACKFRAME_XPU_BACKEND_ABI_MAJOR) {
+            return BLACKFRAME_STATUS_UNSUPPORTED_ABI;
+        }
+        auto* api = static_cast<blackframe_xpu_backend_api_v1*>(out);
+        *api = blackframe_xpu_backend_api_v1{};
+        api->struct_size = sizeof(blackframe_xpu_backend_api_v1);
+        api->abi_major = BLACKFRAME_XPU_BACKEND_ABI_MAJOR;
+        api->abi_minor = BLACKFRAME_XPU_BACKEND_ABI_MINOR;
+        api->backend_name = view_of(kBackendName);
+        api->get_device_count = &xpu_device_count;
+        api->get_device_descriptor = &xpu_device_descriptor;
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    if (id.high == BF200_RENDER_INTERFACE_ID_HIGH && id.low == BF200_RENDER_INTERFACE_ID_LOW) {
+        if (out_size < sizeof(bf200_render_api_v1)) {
+            return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+        }
+        if (major != BF200_RENDER_ABI_MAJOR) {
+            return BLACKFRAME_STATUS_UNSUPPORTED_ABI;
+        }
+        auto* api = static_cast<bf200_render_api_v1*>(out);
+        *api = bf200_render_api_v1{};
+        api->struct_size = sizeof(bf200_render_api_v1);
+        api->abi_major = BF200_RENDER_ABI_MAJOR;
+        api->abi_minor = BF200_RENDER_ABI_MINOR;
+        api->context_create = &bf200_context_create;
+        api->context_destroy = &bf200_context_destroy;
+        api->context_last_error = &bf200_context_last_error;
+        api->scene_create = &bf200_scene_create;
+        api->scene_destroy = &bf200_scene_destroy;
+        api->trace_paths = &bf200_trace_paths;
+        api->render_film = &bf200_render_film;
+        api->closest_hits = &bf200_closest_hits;
+        api->occlusions = &bf200_occlusions;
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    return BLACKFRAME_STATUS_INTERFACE_NOT_FOUND;
+}
+
+void shutdown_extension(void*) noexcept {}
+
+}  // namespace
+
+BF200_EXPORT blackframe_status blackframe_query_extension(const blackframe_extension_query_v1* query,
+                                                           blackframe_extension_api_v1* out) noexcept {
+    if (query == nullptr || out == nullptr || query->struct_size < sizeof(blackframe_extension_query_v1) ||
+        out->struct_size < sizeof(blackframe_extension_api_v1)) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    if (query->abi_major != BLACKFRAME_EXTENSION_ABI_MAJOR) {
+        return BLACKFRAME_STATUS_UNSUPPORTED_ABI;
+    }
+    *out = blackframe_extension_api_v1{};
+    out->struct_size = sizeof(blackframe_extension_api_v1);
+    out->abi_major = BLACKFRAME_EXTENSION_ABI_MAJOR;
+    out->abi_minor = BLACKFRAME_EXTENSION_ABI_MINOR;
+    out->extension_context = nullptr;
+    out->get_interface = &get_interface;
+    out->shutdown = &shutdown_extension;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+}  // extern "C"
+
+static_assert(sizeof(bf200_closure_v1) == 64, "closure record layout");
+static_assert(sizeof(bf200_path_input_v1) == 80, "path input layout");
+static_assert(sizeof(bf200_path_result_v1) == 128, "path result layout");
+static_assert(sizeof(bf200_ray_v1) == 48, "ray layout");
+static_assert(sizeof(bf200_instance_v1) == 160, "instance layout");

@@ -1,0 +1,1609 @@
+// bf200 device kernels: scene setup, exact-robust BVH traversal, the persistent wavefront
+// (intersect -> shade with NEE -> occlusion) and film accumulation.
+//
+// Hot-path mapping to the reference CUDA backend (Blackframe/XPU/CUDA/Source):
+//   k_intersect : scene_closest_hit_kernel + classify/miss stages (CudaSceneClosestHit.cu:1199,
+//                 CudaWavefrontStages.cu:1434, :3962), plus camera generation and path
+//                 regeneration (seed/camera stages, :1269-1406) fused in.
+//   k_shade     : shade_stage_kernel (CudaWavefrontStages.cu:4107-4727) with the shadow-queue
+//                 compaction (CudaWavefrontQueueCompaction.cu) done by warp ballot/popc and one
+//                 block-level scan.
+//   k_occlude   : scene_occlusion_kernel + process_shadow_kernel (CudaSceneClosestHit.cu:1243,
+//                 CudaWavefrontStages.cu:4772-4908).
+//   k_film      : the caller-side CIE XYZ -> linear RGB -> Film::add_sample loop
+//                 (Tests/Backends/GPU/CUDA/CudaTransportParityTest.cpp:906-927), on the device.
+// Arithmetic follows the reference scalar loop (Blackframe/Engine/Source/SceneMisPathLoop.cpp)
+// operation for operation; this file is compiled with -fmad=false.
+#include <cuda_runtime.h>
+
+#include "bf200_device.cuh"
+#include "bf200_kernels.h"
+
+namespace bf200 {
+
+// ------------------------------------------------------------------------------------------------
+// Scene setup
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ F3 xform_point(const float4* m, F3 p) {
+    const float4 r0 = m[0], r1 = m[1], r2 = m[2];
+    return {r0.x * p.x + r0.y * p.y + r0.z * p.z + r0.w, r1.x * p.x + r1.y * p.y + r1.z * p.z + r1.w,
+            r2.x * p.x + r2.y * p.y + r2.z * p.z + r2.w};
+}
+__device__ __forceinline__ F3 xform_vector(const float4* m, F3 v) {
+    const float4 r0 = m[0], r1 = m[1], r2 = m[2];
+    return {r0.x * v.x + r0.y * v.y + r0.z * v.z, r1.x * v.x + r1.y * v.y + r1.z * v.z,
+            r2.x * v.x + r2.y * v.y + r2.z * v.z};
+}
+
+__device__ __forceinline__ F3 load_vertex(const float* p, uint32_t i) { return {p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+
+// World-space geometric normal of every instance triangle: the normal the analytic accel
+// reports for a hit (AccelBackend.cpp:84-97, Triangle.hpp:374-481).
+__global__ void k_world_normals(SceneView s, const uint32_t* tri_instance, const uint32_t* tri_local,
+                                uint32_t total, float4* out, uint32_t* failures) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const uint32_t inst = tri_instance[i];
+        const uint32_t prim = tri_local[i];
+        const uint4 info = s.inst_info[inst];
+        const uint4 geom = s.geom_info[info.x];
+        const uint32_t* tri = s.triangles + 3ULL * (geom.y + prim);
+        const float4* m = s.inst_to_world + 3ULL * inst;
+        const F3 w0 = xform_point(m, load_vertex(s.positions, geom.x + tri[0]));
+        const F3 w1 = xform_point(m, load_vertex(s.positions, geom.x + tri[1]));
+        const F3 w2 = xform_point(m, load_vertex(s.positions, geom.x + tri[2]));
+        F3 n{0.0F, 0.0F, 0.0F};
+        if (!triangle_normal(w0, w1, w2, n)) {
+            atomicAdd(failures, 1U);
+        }
+        out[i] = make_float4(n.x, n.y, n.z, 0.0F);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Ray / triangle test: exact edge signs, correctly rounded parameter and barycentrics
+// ------------------------------------------------------------------------------------------------
+
+constexpr double kU = 1.1102230246251565e-16;  // 2^-53
+
+struct Dets {
+    double e[3];
+    double bound[3];
+    double vol, vol_bound;
+    double p[3][3];
+    double d[3];
+};
+
+__device__ __forceinline__ double det_terms(const double* a, const double* b, const double* c, double& perm) {
+    const double t1 = a[0] * b[1] * c[2], t2 = a[1] * b[2] * c[0], t3 = a[2] * b[0] * c[1];
+    const double t4 = a[2] * b[1] * c[0], t5 = a[1] * b[0] * c[2], t6 = a[0] * b[2] * c[1];
+    perm = fabs(t1) + fabs(t2) + fabs(t3) + fabs(t4) + fabs(t5) + fabs(t6);
+    return ((t1 + t2) + t3) - ((t4 + t5) + t6);
+}
+
+// Exact evaluation of the four determinants as double expansions and an exact decision.
+// Returns kTriHit with t (and barycentrics if requested), kTriMiss, or kTriFailure when a
+// coordinate difference is not exact in double (exponent gap above 29 bits).
+__device__ __noinline__ int exact_triangle_slow(const Dets& q, float t_min, float t_max, float approx_t,
+                                                bool want_bary, TriangleHit& hit) {
+    Expansion<double, 32> e0, e1, e2, vol;
+    if (!exp_det3(e0, q.p[1], q.p[2], q.d) || !exp_det3(e1, q.p[2], q.p[0], q.d) ||
+        !exp_det3(e2, q.p[0], q.p[1], q.d) || !exp_det3(vol, q.p[0], q.p[1], q.p[2])) {
+        return kTriFailure;
+    }
+    Expansion<double, 96> det;
+    det.size = 0;
+    if (!exp_add_expansion(det, e0, 1.0) || !exp_add_expansion(det, e1, 1.0) || !exp_add_expansion(det, e2, 1.0)) {
+        return kTriFailure;
+    }
+    const int ds = exp_sign(det);
+    if (ds == 0) {
+        return kTriMiss;  // coplanar or parallel: the accel skips both
+    }
+    const int s0 = exp_sign(e0), s1 = exp_sign(e1), s2 = exp_sign(e2);
+    const bool nonneg = s0 >= 0 && s1 >= 0 && s2 >= 0;
+    const bool nonpos = s0 <= 0 && s1 <= 0 && s2 <= 0;
+    if (!nonneg && !nonpos) {
+        return kTriMiss;
+    }
+    double dv = 0.0, vv = 0.0;
+    for (int i = 0; i < det.size; ++i) dv += det.c[i];
+    for (int i = 0; i < vol.size; ++i) vv += vol.c[i];
+    float seed = isfinite(approx_t) && approx_t != 0.0F ? approx_t : static_cast<float>(vv / dv);
+    float t = 0.0F;
+    if (exp_sign(vol) == 0) {
+        t = 0.0F;
+    } else {
+        if (seed == 0.0F || !isfinite(seed)) {
+            return kTriFailure;
+        }
+        if (!exact_round_quotient(vol, det, seed, t)) {
+            return kTriFailure;
+        }
+    }
+    if (isnan(t) || t < t_min || t > t_max) {
+        return kTriMiss;
+    }
+    hit.t = t;
+    if (want_bary) {
+        const Expansion<double, 32>* es[3] = {&e0, &e1, &e2};
+        float out[3];
+        for (int k = 0; k < 3; ++k) {
+            if (exp_sign(*es[k]) == 0) {
+                out[k] = 0.0F;
+                continue;
+            }
+            double ev = 0.0;
+            for (int i = 0; i < es[k]->size; ++i) ev += es[k]->c[i];
+            if (!exact_round_quotient(*es[k], det, static_cast<float>(ev / dv), out[k])) {
+                return kTriFailure;
+            }
+        }
+        hit.b0 = out[0];
+        hit.b1 = out[1];
+        hit.b2 = out[2];
+    }
+    return kTriHit;
+}
+
+// The float nearest to num/den when a forward error bound proves it; otherwise NaN.
+__device__ __forceinline__ float certain_round(double num, double num_bound, double den, double den_bound) {
+    if (!(fabs(num) > 2.0 * num_bound) || !(fabs(den) > 2.0 * den_bound)) {
+        return __int_as_float(0x7fc00000);
+    }
+    const double q = num / den;
+    const double rel = num_bound / fabs(num) + den_bound / fabs(den) + 4.0 * kU;
+    if (!(rel < 0x1p-27)) {
+        return __int_as_float(0x7fc00000);
+    }
+    const double lo = q - fabs(q) * (2.0 * rel);
+    const double hi = q + fabs(q) * (2.0 * rel);
+    const float flo = __double2float_rn(lo);
+    const float fhi = __double2float_rn(hi);
+    return flo == fhi ? flo : __int_as_float(0x7fc00000);
+}
+
+// Returns kTriHit (t set), kTriMiss or kTriFailure. Object-space floats in; the decision and
+// the parameter equal those of the exact test in Triangle.hpp:683-822.
+__device__ __forceinline__ int triangle_test(float4 v0, float4 v1, float4 v2, F3 o, F3 d, float t_min, float t_max,
+                                             bool want_bary, TriangleHit& hit) {
+    Dets q;
+    const double ox = o.x, oy = o.y, oz = o.z;
+    q.p[0][0] = double(v0.x) - ox; q.p[0][1] = double(v0.y) - oy; q.p[0][2] = double(v0.z) - oz;
+    q.p[1][0] = double(v1.x) - ox; q.p[1][1] = double(v1.y) - oy; q.p[1][2] = double(v1.z) - oz;
+    q.p[2][0] = double(v2.x) - ox; q.p[2][1] = double(v2.y) - oy; q.p[2][2] = double(v2.z) - oz;
+    q.d[0] = d.x; q.d[1] = d.y; q.d[2] = d.z;
+    double perm;
+    q.e[0] = det_terms(q.p[1], q.p[2], q.d, perm);
+    q.bound[0] = 16.0 * kU * perm;
+    q.e[1] = det_terms(q.p[2], q.p[0], q.d, perm);
+    q.bound[1] = 16.0 * kU * perm;
+    q.e[2] = det_terms(q.p[0], q.p[1], q.d, perm);
+    q.bound[2] = 16.0 * kU * perm;
+    int pos = 0, neg = 0;
+    bool ambiguous = false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (q.e[k] > q.bound[k]) {
+            ++pos;
+        } else if (q.e[k] < -q.bound[k]) {
+            ++neg;
+        } else {
+            ambiguous = true;
+        }
+    }
+    if (pos > 0 && neg > 0) {
+        return kTriMiss;
+    }
+    // A coordinate difference that is not exact in double makes the slow path unusable; such
+    // inputs (exponent gaps above 29 bits) are reported as a lane failure.
+    const bool exact_diffs =
+        (q.p[0][0] + ox == double(v0.x)) && (q.p[0][1] + oy == double(v0.y)) && (q.p[0][2] + oz == double(v0.z)) &&
+        (q.p[1][0] + ox == double(v1.x)) && (q.p[1][1] + oy == double(v1.y)) && (q.p[1][2] + oz == double(v1.z)) &&
+        (q.p[2][0] + ox == double(v2.x)) && (q.p[2][1] + oy == double(v2.y)) && (q.p[2][2] + oz == double(v2.z));
+    if (ambiguous) {
+        if (!exact_diffs) {
+            return kTriFailure;
+        }
+        return exact_triangle_slow(q, t_min, t_max, __int_as_float(0x7fc00000), want_bary, hit);
+    }
+    q.vol = det_terms(q.p[0], q.p[1], q.p[2], perm);
+    q.vol_bound = 16.0 * kU * perm;
+    const double det = (q.e[0] + q.e[1]) + q.e[2];
+    const double det_bound = q.bound[0] + q.bound[1] + q.bound[2] + 4.0 * kU * fabs(det);
+    float t = certain_round(q.vol, q.vol_bound, det, det_bound);
+    if (isnan(t)) {
+        if (!exact_diffs) {
+            return kTriFailure;
+        }
+        return exact_triangle_slow(q, t_min, t_max, __double2float_rn(q.vol / det), want_bary, hit);
+    }
+    if (t < t_min || t > t_max) {
+        return kTriMiss;
+    }
+    hit.t = t;
+    if (want_bary) {
+        const float b0 = certain_round(q.e[0], q.bound[0], det, det_bound);
+        const float b1 = certain_round(q.e[1], q.bound[1], det, det_bound);
+        const float b2 = certain_round(q.e[2], q.bound[2], det, det_bound);
+        if (isnan(b0) || isnan(b1) || isnan(b2)) {
+            if (!exact_diffs) {
+                return kTriFailure;
+            }
+            return exact_triangle_slow(q, t_min, t_max, t, true, hit);
+        }
+        hit.b0 = b0;
+        hit.b1 = b1;
+        hit.b2 = b2;
+    }
+    return kTriHit;
+}
+
+// ------------------------------------------------------------------------------------------------
+// BVH traversal
+// ------------------------------------------------------------------------------------------------
+
+constexpr float kGamma3 = 3.0F * 5.96046448e-8F / (1.0F - 3.0F * 5.96046448e-8F);
+constexpr float kSlackLo = 1.0F - 2.0F * kGamma3;
+constexpr float kSlackHi = 1.0F + 2.0F * kGamma3;
+
+struct RayInv {
+    F3 o;
+    F3 inv;
+    bool px, py, pz;  // axis-parallel components
+};
+
+__device__ __forceinline__ RayInv make_ray_inv(F3 o, F3 d) {
+    RayInv r;
+    r.o = o;
+    r.px = d.x == 0.0F;
+    r.py = d.y == 0.0F;
+    r.pz = d.z == 0.0F;
+    r.inv = F3{r.px ? 0.0F : 1.0F / d.x, r.py ? 0.0F : 1.0F / d.y, r.pz ? 0.0F : 1.0F / d.z};
+    return r;
+}
+
+// Conservative slab test: never rejects a box that contains a point of the ray with parameter
+// in [t_min, t_max] (each computed slab parameter is within a relative gamma(3) of the exact one,
+// and its sign is exact).
+__device__ __forceinline__ bool slab(const RayInv& r, float lox, float hix, float loy, float hiy, float loz, float hiz,
+                                     float t_min, float t_max, float& near_out) {
+    float near = t_min, far = t_max;
+    bool inside = true;
+    if (r.px) {
+        inside = inside && lox <= r.o.x && r.o.x <= hix;
+    } else {
+        const float a = (lox - r.o.x) * r.inv.x, b = (hix - r.o.x) * r.inv.x;
+        near = fmaxf(near, fminf(a, b) * kSlackLo);
+        far = fminf(far, fmaxf(a, b) * kSlackHi);
+    }
+    if (r.py) {
+        inside = inside && loy <= r.o.y && r.o.y <= hiy;
+    } else {
+        const float a = (loy - r.o.y) * r.inv.y, b = (hiy - r.o.y) * r.inv.y;
+        near = fmaxf(near, fminf(a, b) * kSlackLo);
+        far = fminf(far, fmaxf(a, b) * kSlackHi);
+    }
+    if (r.pz) {
+        inside = inside && loz <= r.o.z && r.o.z <= hiz;
+    } else {
+        const float a = (loz - r.o.z) * r.inv.z, b = (hiz - r.o.z) * r.inv.z;
+        near = fmaxf(near, fminf(a, b) * kSlackLo);
+        far = fminf(far, fmaxf(a, b) * kSlackHi);
+    }
+    near_out = near;
+    return inside && near <= far;
+}
+
+// The slack factors only widen positive parameters; a negative lower bound is harmless because
+// t_min >= 0 clamps it, and a negative upper bound means the box is entirely behind the origin.
+
+struct ClosestResult {
+    float t;
+    uint32_t instance, primitive;
+    uint32_t leaf;  // leaf triangle index of the winner
+    bool failed;
+};
+
+__device__ __forceinline__ bool precedes(float t, uint32_t inst, uint32_t prim, const ClosestResult& best) {
+    if (t != best.t) {
+        return t < best.t;
+    }
+    if (inst != best.instance) {
+        return inst < best.instance;
+    }
+    return prim < best.primitive;
+}
+
+// Closest hit over every visible instance (committed order) and its BLAS; ties keep the hit
+// that comes first in (instance, primitive) order, as the analytic accel's in-order scan does.
+__device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask) {
+    ClosestResult best;
+    best.t = t_max;
+    best.instance = 0xFFFFFFFFU;
+    best.primitive = 0xFFFFFFFFU;
+    best.leaf = 0xFFFFFFFFU;
+    best.failed = false;
+    bool found = false;
+    int stack[kTraversalStack];
+    for (uint32_t inst = 0; inst < s.instance_count; ++inst) {
+        const uint4 info = s.inst_info[inst];
+        if ((mask & info.z) == 0U) {
+            continue;
+        }
+        const float4* m = s.inst_to_object + 3ULL * inst;
+        const F3 lo = xform_point(m, o);
+        const F3 ld = xform_vector(m, d);
+        const RayInv r = make_ray_inv(lo, ld);
+        const uint4 geom = s.geom_info[info.x];
+        int sp = 0;
+        stack[sp++] = static_cast<int>(geom.z);
+        while (sp > 0) {
+            const int node_index = stack[--sp];
+            const BvhNode node = s.nodes[node_index];
+            const float limit = found ? best.t : t_max;
+            float n0, n1;
+            const bool h0 = slab(r, node.a.x, node.a.y, node.a.z, node.a.w, node.c.x, node.c.y, t_min, limit, n0);
+            const bool h1 = slab(r, node.b.x, node.b.y, node.b.z, node.b.w, node.c.z, node.c.w, t_min, limit, n1);
+            int children[2];
+            int count = 0;
+            if (h0 && h1) {
+                const bool swap = n1 < n0;
+                children[0] = swap ? node.d.y : node.d.x;
+                children[1] = swap ? node.d.x : node.d.y;
+                count = 2;
+            } else if (h0) {
+                children[0] = node.d.x;
+                count = 1;
+            } else if (h1) {
+                children[0] = node.d.y;
+                count = 1;
+            }
+            // push far child first so the near one is visited next
+            for (int k = count - 1; k >= 0; --k) {
+                const int child = children[k];
+                if (child >= 0) {
+                    if (sp < kTraversalStack) {
+                        stack[sp++] = child;
+                    } else {
+                        best.failed = true;
+                    }
+                    continue;
+                }
+                const uint32_t packed = static_cast<uint32_t>(~child);
+                const uint32_t first = packed >> kLeafCountBits;
+                const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
+                for (uint32_t j = 0; j < n; ++j) {
+                    const uint32_t leaf = first + j;
+                    const float4 v0 = s.leaf_tris[3ULL * leaf];
+                    const float4 v1 = s.leaf_tris[3ULL * leaf + 1];
+                    const float4 v2 = s.leaf_tris[3ULL * leaf + 2];
+                    TriangleHit th;
+                    const float cur_limit = found ? best.t : t_max;
+                    const int res = triangle_test(v0, v1, v2, lo, ld, t_min, cur_limit, false, th);
+                    if (res == kTriFailure) {
+                        best.failed = true;
+                        continue;
+                    }
+                    if (res != kTriHit) {
+                        continue;
+                    }
+                    const uint32_t prim = __float_as_uint(v0.w);
+                    if (!found || precedes(th.t, inst, prim, best)) {
+                        best.t = th.t;
+                        best.instance = inst;
+                        best.primitive = prim;
+                        best.leaf = leaf;
+                        found = true;
+                    }
+                }
+            }
+        }
+    }
+    if (!found) {
+        best.instance = 0xFFFFFFFFU;
+    }
+    return best;
+}
+
+// Any hit in [t_min, t_max] (AccelBackend.cpp:114-147). Returns 1 occluded, 0 clear, -1 failure.
+__device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask) {
+    int stack[kTraversalStack];
+    bool failed = false;
+    for (uint32_t inst = 0; inst < s.instance_count; ++inst) {
+        const uint4 info = s.inst_info[inst];
+        if ((mask & info.z) == 0U) {
+            continue;
+        }
+        const float4* m = s.inst_to_object + 3ULL * inst;
+        const F3 lo = xform_point(m, o);
+        const F3 ld = xform_vector(m, d);
+        const RayInv r = make_ray_inv(lo, ld);
+        const uint4 geom = s.geom_info[info.x];
+        int sp = 0;
+        stack[sp++] = static_cast<int>(geom.z);
+        while (sp > 0) {
+            const int node_index = stack[--sp];
+            const BvhNode node = s.nodes[node_index];
+            float n0, n1;
+            const bool h0 = slab(r, node.a.x, node.a.y, node.a.z, node.a.w, node.c.x, node.c.y, t_min, t_max, n0);
+            const bool h1 = slab(r, node.b.x, node.b.y, node.b.z, node.b.w, node.c.z, node.c.w, t_min, t_max, n1);
+            const int kids[2] = {h0 ? node.d.x : 0, h1 ? node.d.y : 0};
+            const bool hits[2] = {h0, h1};
+            for (int k = 0; k < 2; ++k) {
+                if (!hits[k]) {
+                    continue;
+                }
+                const int child = kids[k];
+                if (child >= 0) {
+                    if (sp < kTraversalStack) {
+                        stack[sp++] = child;
+                    } else {
+                        failed = true;
+                    }
+                    continue;
+                }
+                const uint32_t packed = static_cast<uint32_t>(~child);
+                const uint32_t first = packed >> kLeafCountBits;
+                const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
+                for (uint32_t j = 0; j < n; ++j) {
+                    const uint32_t leaf = first + j;
+                    TriangleHit th;
+                    const int res = triangle_test(s.leaf_tris[3ULL * leaf], s.leaf_tris[3ULL * leaf + 1],
+                                                  s.leaf_tris[3ULL * leaf + 2], lo, ld, t_min, t_max, false, th);
+                    if (res == kTriHit) {
+                        return 1;
+                    }
+                    if (res == kTriFailure) {
+                        failed = true;
+                    }
+                }
+            }
+        }
+    }
+    return failed ? -1 : 0;
+}
+
+// Barycentrics of the winning triangle (correctly rounded e_i / det).
+__device__ bool hit_barycentrics(const SceneView& s, const ClosestResult& c, F3 o, F3 d, float t_min, float t_max,
+                                 TriangleHit& th) {
+    const float4* m = s.inst_to_object + 3ULL * c.instance;
+    const F3 lo = xform_point(m, o);
+    const F3 ld = xform_vector(m, d);
+    const int res = triangle_test(s.leaf_tris[3ULL * c.leaf], s.leaf_tris[3ULL * c.leaf + 1],
+                                  s.leaf_tris[3ULL * c.leaf + 2], lo, ld, t_min, t_max, true, th);
+    return res == kTriHit && th.t == c.t;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Wavefront helpers
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t depth_total(uint32_t packed) {
+    return (packed & 0xFFU) + ((packed >> 8) & 0xFFU) + ((packed >> 16) & 0xFFU);
+}
+
+__device__ __forceinline__ uint32_t depth_blocked(const TransportParams& p, uint32_t packed, uint32_t lobes) {
+    uint32_t blocked = 0;
+    if ((lobes & kLobeDiffuse) && (packed & 0xFFU) >= p.limits[0]) blocked |= kLobeDiffuse;
+    if ((lobes & kLobeGlossy) && ((packed >> 8) & 0xFFU) >= p.limits[1]) blocked |= kLobeGlossy;
+    if ((lobes & kLobeSpecular) && ((packed >> 16) & 0xFFU) >= p.limits[2]) blocked |= kLobeSpecular;
+    if ((lobes & kLobeTransmission) && ((packed >> 24) & 0xFFU) >= p.limits[3]) blocked |= kLobeTransmission;
+    if ((lobes & kLobeVolume) && 0U >= p.limits[4]) blocked |= kLobeVolume;
+    return blocked;
+}
+
+__device__ __forceinline__ uint32_t depth_advance(uint32_t packed, uint32_t lobes) {
+    if (lobes & kLobeDiffuse) packed += 1U;
+    if (lobes & kLobeGlossy) packed += 1U << 8;
+    if (lobes & kLobeSpecular) packed += 1U << 16;
+    if (lobes & kLobeTransmission) packed += 1U << 24;
+    return packed;
+}
+
+__device__ __forceinline__ Stream load_stream(const Wavefront& w, uint32_t slot) {
+    const uint2 v = w.stream[slot];
+    return Stream{(static_cast<uint64_t>(v.y) << 32) | v.x};
+}
+
+__device__ __forceinline__ void record_failure(const Wavefront& w, uint32_t slot, uint32_t code) {
+    atomicAdd(&w.counters[5], 1ULL);
+    atomicMin(&w.counters[6], static_cast<unsigned long long>(w.path_id[slot]));
+    atomicCAS(&w.counters[7], 0ULL, static_cast<unsigned long long>(code));
+}
+
+// PinholeCamera.hpp:194-283: jittered primary ray of (pixel, sample).
+__device__ bool camera_ray(const PathSource& src, uint32_t px, uint32_t py, const Stream& stream, F3& o, F3& d,
+                           Lane& lane) {
+    float ox = 0.5F, oy = 0.5F;
+    if (src.jitter != 0U) {
+        ox = stream.sample_1d(kCameraRasterX);
+        oy = stream.sample_1d(kCameraRasterY);
+    }
+    const float rw = static_cast<float>(src.width), rh = static_cast<float>(src.height);
+    const float tpx = 2.0F * static_cast<float>(px);
+    const float tpy = 2.0F * static_cast<float>(py);
+    const float nx = (tpx + 2.0F * ox) / rw - 1.0F;
+    const float ny = 1.0F - (tpy + 2.0F * oy) / rh;
+    const F3 cd{nx * src.half_width, ny * src.half_height, -1.0F};
+    const F3 uc = robust_unit(cd, lane);
+    const F3 t{src.cam_t[0], src.cam_t[1], src.cam_t[2]};
+    const F3 b{src.cam_b[0], src.cam_b[1], src.cam_b[2]};
+    const F3 n{src.cam_n[0], src.cam_n[1], src.cam_n[2]};
+    const F3 world{t.x * uc.x + b.x * uc.y + n.x * uc.z, t.y * uc.x + b.y * uc.y + n.y * uc.z,
+                   t.z * uc.x + b.z * uc.y + n.z * uc.z};
+    d = robust_unit(world, lane);
+    o = F3{src.cam_origin[0], src.cam_origin[1], src.cam_origin[2]};
+    return lane.err == 0;
+}
+
+// Claims the next path of the job into `slot` and writes its primary ray and initial state.
+// Returns false when the job has no more paths.
+__device__ bool start_path(const Wavefront& w, const PathSource& src, uint32_t slot, uint64_t id) {
+    Lane lane;
+    F3 o, d;
+    float tmin, tmax;
+    Stream stream;
+    uint32_t mask;
+    if (src.mode == 0U) {
+        const uint64_t pixels = static_cast<uint64_t>(src.width) * src.height;
+        const uint64_t pixel = id % pixels;
+        const uint64_t sample = src.first_sample + id / pixels;
+        const uint32_t px = static_cast<uint32_t>(pixel % src.width);
+        const uint32_t py = static_cast<uint32_t>(pixel / src.width);
+        stream = Stream::make(px, py, sample, src.seed);
+        // the jitter uses the independent stream of the same index (PixelJitter.hpp:47-64)
+        camera_ray(src, px, py, stream, o, d, lane);
+        tmin = src.t_min;
+        tmax = src.t_max;
+        mask = src.mask;
+    } else {
+        const bf200_path_input_v1& in = src.inputs[id];
+        stream = Stream::make(in.sample.pixel_x, in.sample.pixel_y, in.sample.sample_index, in.sample.seed);
+        o = F3{in.primary_ray.origin[0], in.primary_ray.origin[1], in.primary_ray.origin[2]};
+        d = F3{in.primary_ray.direction[0], in.primary_ray.direction[1], in.primary_ray.direction[2]};
+        tmin = in.primary_ray.t_min;
+        tmax = in.primary_ray.t_max;
+        mask = in.primary_ray.mask;
+    }
+    w.path_id[slot] = id;
+    w.ray_o[slot] = make_float4(o.x, o.y, o.z, tmax);
+    w.ray_d[slot] = make_float4(d.x, d.y, d.z, tmin);
+    w.beta[slot] = make_float4(1.0F, 1.0F, 1.0F, 1.0F);
+    w.radiance[slot] = make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+    w.depth[slot] = 0U;
+    w.eta[slot] = 1.0F;
+    w.prev[slot] = make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+    w.flags[slot] = 0U;
+    w.status[slot] = lane.err;
+    w.stream[slot] = make_uint2(static_cast<uint32_t>(stream.state), static_cast<uint32_t>(stream.state >> 32));
+    w.mask[slot] = mask;
+    w.state[slot] = kSlotActive;
+    return true;
+}
+
+// Writes a finished path's outputs (film radiance or the full result record).
+__device__ void finish_path(const Wavefront& w, const PathSource& src, uint32_t slot) {
+    const uint64_t id = w.path_id[slot];
+    const uint32_t status = w.status[slot];
+    if ((status & 0xFFU) != 0U) {
+        record_failure(w, slot, status & 0xFFU);
+    }
+    if (src.mode == 0U) {
+        src.path_radiance[id] = (status & 0xFFU) != 0U ? make_float4(__int_as_float(0x7fc00000), 0.0F, 0.0F, 0.0F)
+                                                        : w.radiance[slot];
+        return;
+    }
+    bf200_path_result_v1 r;
+    const float4 beta = w.beta[slot], rad = w.radiance[slot];
+    r.beta[0] = beta.x; r.beta[1] = beta.y; r.beta[2] = beta.z; r.beta[3] = beta.w;
+    r.radiance[0] = rad.x; r.radiance[1] = rad.y; r.radiance[2] = rad.z; r.radiance[3] = rad.w;
+    const uint32_t dp = w.depth[slot];
+    r.depth = depth_total(dp);
+    r.depth_counters[0] = dp & 0xFFU;
+    r.depth_counters[1] = (dp >> 8) & 0xFFU;
+    r.depth_counters[2] = (dp >> 16) & 0xFFU;
+    r.depth_counters[3] = (dp >> 24) & 0xFFU;
+    r.depth_counters[4] = 0U;
+    r.eta_scale = w.eta[slot];
+    const uint32_t flags = w.flags[slot];
+    r.delta_flags = flags & 0xFFU;
+    r.termination = (flags >> 8) & 0xFFU;
+    r.blocked_depth_limits = (flags >> 16) & 0xFFU;
+    r.lane_status = status & 0xFFU;
+    r.segments = status >> 8;
+    const float4 o = w.ray_o[slot], dd = w.ray_d[slot];
+    r.terminal_ray.origin[0] = o.x; r.terminal_ray.origin[1] = o.y; r.terminal_ray.origin[2] = o.z;
+    r.terminal_ray.direction[0] = dd.x; r.terminal_ray.direction[1] = dd.y; r.terminal_ray.direction[2] = dd.z;
+    r.terminal_ray.t_min = dd.w;
+    r.terminal_ray.t_max = o.w;
+    r.terminal_ray.time = src.mode == 1U ? src.inputs[id].primary_ray.time : src.time;
+    r.terminal_ray.mask = src.mode == 1U ? src.inputs[id].primary_ray.mask : src.mask;
+    r.terminal_ray.medium = 0U;
+    r.terminal_ray.reserved = 0U;
+    src.results[id] = r;
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_intersect: retire finished slots, regenerate from the job, closest hit for active slots
+// ------------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_intersect(SceneView s, Wavefront w, PathSource src) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
+    // every thread of a warp runs the same number of iterations so the warp-wide claim below is
+    // entered by whole warps
+    const uint32_t rounds = (w.capacity + stride - 1U) / stride;
+    for (uint32_t round = 0; round < rounds; ++round) {
+        const uint32_t slot = first + round * stride;
+        const bool in_range = slot < w.capacity;
+        uint8_t state = in_range ? w.state[slot] : kSlotActive + 16;
+        if (state == kSlotDone) {
+            finish_path(w, src, slot);
+            state = kSlotEmpty;
+            w.state[slot] = kSlotEmpty;
+        }
+        // claim new paths for empty slots: one atomic per warp (ballot / popc)
+        const bool wants = in_range && state == kSlotEmpty;
+        const unsigned want_mask = __ballot_sync(0xFFFFFFFFU, wants);
+        unsigned long long base = 0;
+        if (want_mask != 0U) {
+            const int leader = __ffs(want_mask) - 1;
+            if (static_cast<int>(threadIdx.x & 31U) == leader) {
+                base = atomicAdd(&w.counters[1], static_cast<unsigned long long>(__popc(want_mask)));
+            }
+            base = __shfl_sync(0xFFFFFFFFU, base, leader);
+        }
+        if (wants) {
+            const unsigned rank = __popc(want_mask & ((1U << (threadIdx.x & 31U)) - 1U));
+            const uint64_t id = base + rank;
+            if (id < src.total) {
+                start_path(w, src, slot, id);
+                if ((w.status[slot] & 0xFFU) != 0U) {
+                    w.state[slot] = kSlotDone;
+                } else {
+                    state = kSlotActive;
+                }
+            }
+        }
+        if (!in_range || state != kSlotActive) {
+            continue;
+        }
+        const unsigned tracing = __activemask();
+        if ((threadIdx.x & 31U) == static_cast<unsigned>(__ffs(tracing) - 1)) {
+            atomicAdd(&w.counters[3], static_cast<unsigned long long>(__popc(tracing)));
+        }
+        const float4 o4 = w.ray_o[slot], d4 = w.ray_d[slot];
+        const uint32_t mask = w.mask[slot];
+        const ClosestResult c = closest_hit(s, ld3(o4), ld3(d4), d4.w, o4.w, mask);
+        w.status[slot] += 1U << 8;  // one extension segment
+        if (c.failed) {
+            w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneTraversal;
+            w.state[slot] = kSlotDone;
+            continue;
+        }
+        if (c.instance == 0xFFFFFFFFU) {
+            w.hit_id[slot] = make_uint2(0xFFFFFFFFU, 0U);
+            continue;
+        }
+        TriangleHit th;
+        if (!hit_barycentrics(s, c, ld3(o4), ld3(d4), d4.w, o4.w, th)) {
+            w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneNumerical;
+            w.state[slot] = kSlotDone;
+            continue;
+        }
+        w.hit_tb[slot] = make_float4(c.t, th.b0, th.b1, th.b2);
+        w.hit_id[slot] = make_uint2(c.instance, c.primitive);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Surface reconstruction (SceneSurfaceInteraction.cpp:54-350, 804-937)
+// ------------------------------------------------------------------------------------------------
+
+struct Surface {
+    F3 position, error, ng, ns;
+    Frame frame;
+};
+
+__device__ bool resolve_surface(const SceneView& s, uint32_t inst, uint32_t prim, const float4 tb, F3 hit_position,
+                                uint32_t material, Surface& out, Lane& lane) {
+    const float b0 = tb.y, b1 = tb.z, b2 = tb.w;
+    const float tolerance = 32.0F * kEps;
+    if (!isfinite(b0) || b0 < -tolerance || b0 > 1.0F + tolerance || !isfinite(b1) || b1 < -tolerance ||
+        b1 > 1.0F + tolerance || !isfinite(b2) || b2 < -tolerance || b2 > 1.0F + tolerance) {
+        lane.fail();
+        return false;
+    }
+    const float sum = b0 + b1 + b2;
+    if (!isfinite(sum) || fabsf(sum - 1.0F) > tolerance) {
+        lane.fail();
+        return false;
+    }
+    const uint4 info = s.inst_info[inst];
+    const uint4 geom = s.geom_info[info.x];
+    const uint32_t* tri = s.triangles + 3ULL * (geom.y + prim);
+    const F3 p0 = load_vertex(s.positions, geom.x + tri[0]);
+    const F3 p1 = load_vertex(s.positions, geom.x + tri[1]);
+    const F3 p2 = load_vertex(s.positions, geom.x + tri[2]);
+    const F3 n0 = load_vertex(s.normals, geom.x + tri[0]);
+    const F3 n1 = load_vertex(s.normals, geom.x + tri[1]);
+    const F3 n2 = load_vertex(s.normals, geom.x + tri[2]);
+    // interpolate_position_with_error (:82-133)
+    const float gamma7 = (7.0F * kEps) / (1.0F - 7.0F * kEps);
+    const float c[3][3] = {{p0.x, p0.y, p0.z}, {p1.x, p1.y, p1.z}, {p2.x, p2.y, p2.z}};
+    float scale = 0.0F;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        scale = bf_max(scale, fabsf(c[1][a] - c[0][a]));
+        scale = bf_max(scale, fabsf(c[2][a] - c[0][a]));
+    }
+    const float floor_error = kEps * scale;
+    if (!isfinite(scale) || !isfinite(floor_error) || !(floor_error > 0.0F)) {
+        lane.fail();
+        return false;
+    }
+    float point[3], perr[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float q0 = b0 * c[0][a], q1 = b1 * c[1][a], q2 = b2 * c[2][a];
+        point[a] = fmaf(b0, c[0][a], fmaf(b1, c[1][a], q2));
+        const float magnitude = fabsf(q0) + fabsf(q1) + fabsf(q2);
+        perr[a] = bf_max(gamma7 * magnitude, floor_error);
+    }
+    // transform_position_with_error (:135-189)
+    const float4* mw = s.inst_to_world + 3ULL * inst;
+    const F3 world = xform_point(mw, F3{point[0], point[1], point[2]});
+    const float wv[3] = {world.x, world.y, world.z};
+    const float hv[3] = {hit_position.x, hit_position.y, hit_position.z};
+    const double eps = static_cast<double>(kEps);
+    const double g7 = (7.0 * eps) / (1.0 - 7.0 * eps);
+    float err[3];
+#pragma unroll
+    for (int row = 0; row < 3; ++row) {
+        const float4 r = mw[row];
+        const float rr[4] = {r.x, r.y, r.z, r.w};
+        double magnitude = fabs(static_cast<double>(rr[3]));
+        double propagated = 0.0;
+#pragma unroll
+        for (int col = 0; col < 3; ++col) {
+            const double coefficient = fabs(static_cast<double>(rr[col]));
+            magnitude += coefficient * fabs(static_cast<double>(point[col]));
+            propagated += coefficient * static_cast<double>(perr[col]);
+        }
+        const double discrepancy = fabs(static_cast<double>(wv[row]) - static_cast<double>(hv[row]));
+        const double bound = g7 * magnitude + (1.0 + g7) * propagated + discrepancy;
+        if (!isfinite(bound) || bound < 0.0 || bound > 3.4028234663852886e38) {
+            lane.fail();
+            return false;
+        }
+        err[row] = __double2float_rn(bound);
+        if (static_cast<double>(err[row]) < bound) {
+            err[row] = nextafterf(err[row], kInf);
+        }
+    }
+    out.position = world;
+    out.error = F3{err[0], err[1], err[2]};
+    const float4 ngw = s.world_normals[s.inst_normal_offset[inst] + prim];
+    out.ng = F3{ngw.x, ngw.y, ngw.z};
+    // interpolate_shading_normal (:305-349) with robust_transformed_normal (:252-295)
+    const F3 on{fmaf(b0, n0.x, fmaf(b1, n1.x, b2 * n2.x)), fmaf(b0, n0.y, fmaf(b1, n1.y, b2 * n2.y)),
+                fmaf(b0, n0.z, fmaf(b1, n1.z, b2 * n2.z))};
+    const float4* mi = s.inst_to_object + 3ULL * inst;
+    const float4 i0 = mi[0], i1 = mi[1], i2 = mi[2];
+    const double n[3] = {on.x, on.y, on.z};
+    const double tr[3] = {fma(double(i0.x), n[0], fma(double(i1.x), n[1], double(i2.x) * n[2])),
+                          fma(double(i0.y), n[0], fma(double(i1.y), n[1], double(i2.y) * n[2])),
+                          fma(double(i0.z), n[0], fma(double(i1.z), n[1], double(i2.z) * n[2]))};
+    double mc = fabs(tr[0]);
+    mc = mc < fabs(tr[1]) ? fabs(tr[1]) : mc;
+    mc = mc < fabs(tr[2]) ? fabs(tr[2]) : mc;
+    if (!isfinite(mc) || mc == 0.0) {
+        lane.fail();
+        return false;
+    }
+    const double sc[3] = {tr[0] / mc, tr[1] / mc, tr[2] / mc};
+    const double mag = sqrt(fma(sc[0], sc[0], fma(sc[1], sc[1], sc[2] * sc[2])));
+    F3 ns{__double2float_rn(sc[0] / mag), __double2float_rn(sc[1] / mag), __double2float_rn(sc[2] / mag)};
+    if (info.w >> 31) {  // orientation flag precomputed at scene build (transform_orientation)
+        ns = -ns;
+    }
+    if (!(dot(out.ng, ns) > 0.0F)) {
+        lane.fail();
+        return false;
+    }
+    out.ns = ns;
+    const uint4 minfo = s.material_info[material];
+    if (minfo.y != 0U) {
+        lane.fail(kLaneUnsupported);
+        return false;
+    }
+    out.frame = rotated_about_normal(frame_from_normal(ns, lane), __uint_as_float(minfo.z), lane);
+    return lane.err == 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Mesh-light sampling (AreaLights.hpp:1184-1243, 1296-1309) and uniform light selection
+// ------------------------------------------------------------------------------------------------
+
+struct LightSample {
+    bool valid;
+    F3 position, error, normal, direction;
+    float pdf;
+    float radiance[4];
+};
+
+__device__ __forceinline__ uint32_t upper_bound(const float* a, uint32_t n, float u) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (u < a[mid]) {
+            hi = mid;
+        } else {
+            lo = mid + 1U;
+        }
+    }
+    return lo;
+}
+
+__device__ void sample_mesh_light(const SceneView& s, const LightInfo& light, F3 context, float u, float v,
+                                  LightSample& out, Lane& lane) {
+    out.valid = false;
+    const float* cdf = s.light_tri_cdf + light.tri_offset;
+    const uint32_t index = upper_bound(cdf, light.tri_count, u);
+    if (index >= light.tri_count) {
+        lane.fail();
+        return;
+    }
+    const float previous = index == 0 ? 0.0F : cdf[index - 1];
+    const float selection = cdf[index] - previous;
+    const float remapped = (u - previous) / selection;
+    if (!isfinite(selection) || !(selection > 0.0F) || !isfinite(remapped) || remapped < 0.0F || !(remapped < 1.0F)) {
+        lane.fail();
+        return;
+    }
+    const float density = selection / s.light_tri_areas[light.tri_offset + index];
+    if (!isfinite(density) || !(density > 0.0F)) {
+        lane.fail();
+        return;
+    }
+    const float root = sqrtf(remapped);
+    const float bary[3] = {1.0F - root, root * (1.0F - v), root * v};
+    const float4* tv = s.light_tri_vertices + 3ULL * (light.tri_offset + index);
+    const float4 a = tv[0], b = tv[1], c = tv[2];
+    const float cs[3][3] = {{a.x, a.y, a.z}, {b.x, b.y, b.z}, {c.x, c.y, c.z}};
+    const float gamma12 = (12.0F * kEps) / (1.0F - 12.0F * kEps);
+    const float underflow = 12.0F * kDenormMin;
+    const float base[3] = {light.err_x, light.err_y, light.err_z};
+    float point[3], error[3];
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        const float q0 = bary[0] * cs[0][axis], q1 = bary[1] * cs[1][axis], q2 = bary[2] * cs[2][axis];
+        point[axis] = fmaf(bary[0], cs[0][axis], fmaf(bary[1], cs[1][axis], q2));
+        const float magnitude = fabsf(q0) + fabsf(q1) + fabsf(q2);
+        const float arithmetic = fmaf(gamma12, magnitude, underflow);
+        error[axis] = nextafterf(base[axis] + arithmetic, kInf);
+    }
+    out.position = F3{point[0], point[1], point[2]};
+    out.error = F3{error[0], error[1], error[2]};
+    const float4 ln = s.light_tri_normals[light.tri_offset + index];
+    out.normal = F3{ln.x, ln.y, ln.z};
+    if (emission_side(out.normal, context - out.position, lane) <= 0) {
+        return;
+    }
+    out.pdf = area_to_solid_angle(density, context, out.position, out.normal, lane);
+    // IncidentLightSample::create_finite (Light.hpp:401-441)
+    const F3 disp = out.position - context;
+    const float scale = max_abs3(disp);
+    if (!(scale > 0.0F) || !isfinite(scale)) {
+        lane.fail();
+        return;
+    }
+    const F3 sd = disp / scale;
+    const float sq = fmaf(sd.x, sd.x, fmaf(sd.y, sd.y, sd.z * sd.z));
+    const float sl = sqrtf(sq);
+    const float distance = scale * sl;
+    if (!isfinite(sl) || !(sl > 0.0F) || !isfinite(distance) || !(distance > 0.0F)) {
+        lane.fail();
+        return;
+    }
+    out.direction = sd / sl;
+    if (!unit_length(out.direction) || !isfinite(out.pdf) || !(out.pdf > 0.0F)) {
+        lane.fail();
+        return;
+    }
+    bool black = true;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        out.radiance[l] = light.radiance[l];
+        black = black && light.radiance[l] == 0.0F;
+    }
+    out.valid = !black && lane.err == 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_shade: one bounce of the scalar MIS loop (SceneMisPathLoop.cpp:685-916) per active slot
+// ------------------------------------------------------------------------------------------------
+
+struct ShadowRecord {
+    bool valid;
+    F3 origin, direction;
+    float t_max;
+    float contribution[4];
+};
+
+__device__ __forceinline__ void terminate(const Wavefront& w, uint32_t slot, uint32_t termination, uint32_t blocked) {
+    w.flags[slot] = (w.flags[slot] & 0xFFU) | (termination << 8) | (blocked << 16);
+    w.state[slot] = kSlotDone;
+}
+
+__device__ __forceinline__ void add_product(float4& acc, const float4 a, const float (&b)[4], Lane& lane) {
+    const float av[4] = {a.x, a.y, a.z, a.w};
+    float r[4] = {acc.x, acc.y, acc.z, acc.w};
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        const float p = av[l] * b[l];
+        if (!isfinite(p) || (av[l] != 0.0F && b[l] != 0.0F && p == 0.0F)) {
+            lane.fail();
+        }
+        r[l] = r[l] + p;
+        if (!isfinite(r[l])) {
+            lane.fail();
+        }
+    }
+    acc = make_float4(r[0], r[1], r[2], r[3]);
+}
+
+// SceneMisPathLoop.cpp:481-528
+__device__ __forceinline__ void add_weighted_emission(float4& acc, const float4 beta, const float (&le)[4], float wgt,
+                                                      Lane& lane) {
+    if (!isfinite(wgt) || wgt < 0.0F || wgt > 1.0F) {
+        lane.fail();
+        return;
+    }
+    if (wgt == 1.0F) {
+        add_product(acc, beta, le, lane);
+        return;
+    }
+    const float bv[4] = {beta.x, beta.y, beta.z, beta.w};
+    float r[4] = {acc.x, acc.y, acc.z, acc.w};
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        if (bv[l] == 0.0F || le[l] == 0.0F || wgt == 0.0F) {
+            continue;
+        }
+        int e1 = 0, e2 = 0, e3 = 0, en = 0;
+        const float significand = frexpf(bv[l], &e1) * frexpf(le[l], &e2) * frexpf(wgt, &e3);
+        const float normalized = frexpf(significand, &en);
+        const float contribution = scalbnf(normalized, e1 + e2 + e3 + en);
+        if (!isfinite(contribution) || !(contribution > 0.0F)) {
+            lane.fail();
+        }
+        r[l] = r[l] + contribution;
+    }
+    acc = make_float4(r[0], r[1], r[2], r[3]);
+}
+
+__device__ __forceinline__ bool is_black4(const float (&v)[4]) {
+    return v[0] == 0.0F && v[1] == 0.0F && v[2] == 0.0F && v[3] == 0.0F;
+}
+
+// SceneMisPathLoop.cpp:136-275 (estimate) without the visibility query: the record carries the
+// shadow ray and the contribution it adds when unoccluded (transmittance 1).
+__device__ void direct_lighting(const SceneView& s, const TransportParams& p, const Surface& surf,
+                                const ClosureData& closure, uint32_t allowed, const float4 beta4, F3 wo_world,
+                                uint64_t dims, const Stream& stream, uint32_t mask, ShadowRecord& rec, Lane& lane) {
+    rec.valid = false;
+    const float beta[4] = {beta4.x, beta4.y, beta4.z, beta4.w};
+    if (is_black4(beta) || is_black4(closure.w)) {
+        return;
+    }
+    const float u_sel = stream.sample_1d(dims + 0);
+    const uint32_t b = upper_bound(s.light_select_cdf + 1, s.light_count, u_sel);
+    if (b >= s.light_count) {
+        lane.fail();
+        return;
+    }
+    const float selection = s.light_select_cdf[b + 1] - s.light_select_cdf[b];
+    const LightInfo light = s.lights[b];
+    if ((s.inst_info[light.instance].z & mask) == 0U) {
+        return;
+    }
+    LightSample ls;
+    sample_mesh_light(s, light, surf.position, stream.sample_1d(dims + 1), stream.sample_1d(dims + 2), ls, lane);
+    if (!ls.valid) {
+        return;
+    }
+    const F3 wo = surf.frame.to_local(wo_world);
+    const F3 wi = surf.frame.to_local(ls.direction);
+    if (wo.z == 0.0F || wi.z == 0.0F) {
+        return;
+    }
+    const bool lambert = closure.kind == kClosureLambert;
+    float f[4] = {0.0F, 0.0F, 0.0F, 0.0F};
+    if (!lambert) {
+        closure_eval(closure, allowed, wo, wi, f, lane);
+        if (is_black4(f)) {
+            return;
+        }
+    }
+    // shading_normal_correction in radiance mode (ShadingNormalCorrection.hpp:65-121)
+    {
+        const float og = dot(surf.ng, wo_world), os = dot(surf.ns, wo_world);
+        const float ig = dot(surf.ng, ls.direction), is = dot(surf.ns, ls.direction);
+        if (og == 0.0F || os == 0.0F || ig == 0.0F || is == 0.0F || signbit(og) != signbit(os) ||
+            signbit(ig) != signbit(is)) {
+            return;
+        }
+    }
+    const float bsdf_pdf = closure_pdf(closure, allowed, wo, wi, lane);
+    const float light_pdf = joint_light_pdf(selection, ls.pdf, lane);
+    const float weight = mis_weight(p.heuristic, light_pdf, bsdf_pdf, lane);
+    // make_shadow_ray (ShadowRay.hpp:181-253) for a finite surface endpoint
+    const F3 origin = offset_surface_point(surf.position, surf.error, surf.ng, ls.direction, lane);
+    const F3 endpoint = offset_surface_point(ls.position, ls.error, ls.normal, origin - ls.position, lane);
+    F3 sd{0.0F, 0.0F, 1.0F};
+    float length = 1.0F;
+    unit_segment(origin, endpoint, ls.direction, sd, length, lane);
+    const float t_max = nextafterf(length, 0.0F);
+    if (!(t_max > 0.0F) || !isfinite(t_max)) {
+        lane.fail();
+    }
+    if (lane.err != 0) {
+        return;
+    }
+    float out[4];
+    if (lambert) {
+        // evaluate_lambertian_direct_lighting (DirectLighting.hpp:171-236)
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return;
+        }
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const float den[2] = {selection, ls.pdf};
+            if (weight == 1.0F) {
+                const float num[6] = {beta[l], closure.w[l], kInvPi, ls.radiance[l], wi.z, 1.0F};
+                out[l] = checked_product_quotient(num, den, lane);
+            } else {
+                const float num[7] = {beta[l], closure.w[l], kInvPi, ls.radiance[l], wi.z, 1.0F, weight};
+                out[l] = checked_product_quotient(num, den, lane);
+            }
+        }
+    } else {
+        // evaluate_bsdf_direct_lighting (DirectLighting.hpp:66-145)
+        const float cosine = fabsf(wi.z);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const float den[2] = {selection, ls.pdf};
+            if (weight == 1.0F) {
+                const float num[5] = {beta[l], f[l], ls.radiance[l], cosine, 1.0F};
+                out[l] = checked_product_quotient(num, den, lane);
+            } else {
+                const float num[6] = {beta[l], f[l], ls.radiance[l], cosine, 1.0F, weight};
+                out[l] = checked_product_quotient(num, den, lane);
+            }
+        }
+    }
+    rec.valid = true;
+    rec.origin = origin;
+    rec.direction = sd;
+    rec.t_max = t_max;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        rec.contribution[l] = out[l];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSource src, TransportParams p) {
+    __shared__ uint32_t warp_counts[8];
+    __shared__ unsigned long long block_base;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t rounds = (w.capacity + stride - 1U) / stride;
+    uint32_t active_here = 0;
+    for (uint32_t round = 0; round < rounds; ++round) {
+        const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x + round * stride;
+        ShadowRecord rec;
+        rec.valid = false;
+        if (slot < w.capacity && w.state[slot] == kSlotActive) {
+            Lane lane;
+            const uint2 id = w.hit_id[slot];
+            const float4 o4 = w.ray_o[slot], d4 = w.ray_d[slot];
+            float4 beta = w.beta[slot];
+            float4 rad = w.radiance[slot];
+            const uint32_t depth = w.depth[slot];
+            const float eta = w.eta[slot];
+            const float4 prev = w.prev[slot];
+            const uint32_t mask = w.mask[slot];
+            const Stream stream = load_stream(w, slot);
+            const F3 ro = ld3(o4), rd = ld3(d4);
+            if (id.x == 0xFFFFFFFFU) {
+                const float env[4] = {s.environment.x, s.environment.y, s.environment.z, s.environment.w};
+                add_product(rad, beta, env, lane);
+                w.radiance[slot] = rad;
+                if (lane.err) {
+                    w.status[slot] |= lane.err;
+                }
+                terminate(w, slot, 0U /*escaped*/, 0U);
+            } else {
+                const float4 tb = w.hit_tb[slot];
+                const uint4 inst = s.inst_info[id.x];
+                const uint32_t material = inst.y;
+                // Ray::at (Ray.hpp:81-95)
+                const F3 hit_position = ro + rd * tb.x;
+                Surface surf;
+                bool done = false;
+                uint32_t termination = 0U, blocked = 0U;
+                if (!resolve_surface(s, id.x, id.y, tb, hit_position, material, surf, lane)) {
+                    done = true;
+                }
+                float4 emission4 = make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+                if (!done) {
+                    const int side = emission_side(surf.ng, -rd, lane);
+                    if (side > 0) {
+                        emission4 = s.emission[material];
+                    }
+                    const float emitted[4] = {emission4.x, emission4.y, emission4.z, emission4.w};
+                    float emission_weight = 1.0F;
+                    if (!is_black4(emitted) && prev.w > 0.0F) {
+                        const uint32_t light_index = inst.w & 0x7FFFFFFFU;
+                        if (light_index >= s.light_count) {
+                            lane.fail();
+                        } else {
+                            const LightInfo light = s.lights[light_index];
+                            const float selection = s.light_select_cdf[light_index + 1] - s.light_select_cdf[light_index];
+                            const F3 pp = ld3(prev);
+                            float conditional = 0.0F;
+                            if (emission_side(surf.ng, pp - surf.position, lane) > 0) {
+                                conditional = area_to_solid_angle(light.inverse_area, pp, surf.position, surf.ng, lane);
+                            }
+                            const float light_pdf = joint_light_pdf(selection, conditional, lane);
+                            emission_weight = mis_weight(p.heuristic, prev.w, light_pdf, lane);
+                        }
+                    }
+                    add_weighted_emission(rad, beta, emitted, emission_weight, lane);
+                    if (lane.err) {
+                        done = true;
+                    }
+                }
+                ClosureData closure;
+                uint32_t allowed = 0U;
+                if (!done) {
+                    if (beta.x == 0.0F && beta.y == 0.0F && beta.z == 0.0F && beta.w == 0.0F) {
+                        done = true;
+                        termination = 3U;  // zero_throughput
+                    }
+                }
+                if (!done) {
+                    const uint4 minfo = s.material_info[material];
+                    if (minfo.x == 0U) {
+                        done = true;
+                        termination = 2U;  // outside_bsdf_support
+                    } else if (minfo.x != 1U) {
+                        lane.fail(kLaneUnsupported);
+                        done = true;
+                    } else {
+                        closure = s.closures[material];
+                        // depth filter of one closure (DepthFilteredClosureMixture.hpp:262-364)
+                        uint32_t block_mask = 0U;
+                        if (closure.kind == kClosureDielectric) {
+                            const uint32_t br = depth_blocked(p, depth, kLobeGlossy | kLobeReflection);
+                            const uint32_t bt = depth_blocked(p, depth, kLobeGlossy | kLobeTransmission);
+                            if (br == 0U) allowed |= kLobeReflection; else block_mask |= br;
+                            if (bt == 0U) allowed |= kLobeTransmission; else block_mask |= bt;
+                        } else {
+                            const uint32_t bl = depth_blocked(p, depth, closure.lobes);
+                            if (bl == 0U) allowed |= closure.lobes & (kLobeReflection | kLobeTransmission);
+                            else block_mask |= bl;
+                        }
+                        if (allowed == 0U) {
+                            done = true;
+                            termination = 1U;  // depth_limit
+                            blocked = block_mask;
+                        }
+                    }
+                }
+                if (!done) {
+                    const F3 wo_world = robust_unit(-rd, lane);
+                    const F3 wo = surf.frame.to_local(wo_world);
+                    const uint64_t dims = bounce_base(depth_total(depth));
+                    BsdfSample bs;
+                    closure_sample(closure, allowed, wo, stream.sample_1d(dims + 3), stream.sample_1d(dims + 4),
+                                   stream.sample_1d(dims + 5), bs, lane);
+                    uint32_t next_depth = depth;
+                    if (bs.valid) {
+                        if (!isfinite(bs.pdf) || !(bs.pdf > 0.0F) || bs.wi.z == 0.0F ||
+                            depth_blocked(p, depth, bs.lobes) != 0U) {
+                            lane.fail();
+                        }
+                        next_depth = depth_advance(depth, bs.lobes);
+                    }
+                    if (lane.err == 0) {
+                        direct_lighting(s, p, surf, closure, allowed, beta, wo_world, dims, stream, mask, rec, lane);
+                    }
+                    if (lane.err != 0) {
+                        rec.valid = false;
+                        done = true;
+                    } else if (!bs.valid) {
+                        done = true;
+                        termination = 2U;
+                    } else {
+                        const F3 wi_world = robust_unit(surf.frame.to_world(bs.wi), lane);
+                        const float og = dot(surf.ng, wo_world), os = dot(surf.ns, wo_world);
+                        const float ig = dot(surf.ng, wi_world), is = dot(surf.ns, wi_world);
+                        const bool corr_zero = og == 0.0F || os == 0.0F || ig == 0.0F || is == 0.0F ||
+                                               signbit(og) != signbit(os) || signbit(ig) != signbit(is);
+                        if (corr_zero) {
+                            done = true;
+                            termination = 2U;
+                        } else {
+                            // update_closure_throughput (BsdfOnlyPathLoop.hpp:64-131), correction 1
+                            const float bv[4] = {beta.x, beta.y, beta.z, beta.w};
+                            float nb[4];
+                            if (closure.kind == kClosureLambert) {
+#pragma unroll
+                                for (int l = 0; l < 4; ++l) {
+                                    nb[l] = bv[l] * closure.w[l];
+                                    if (!isfinite(nb[l]) || (bv[l] != 0.0F && closure.w[l] != 0.0F && nb[l] == 0.0F)) {
+                                        lane.fail();
+                                    }
+                                }
+                            } else {
+                                const float cosine = fabsf(bs.wi.z);
+#pragma unroll
+                                for (int l = 0; l < 4; ++l) {
+                                    const float num[4] = {bv[l], bs.value[l], cosine, 1.0F};
+                                    float significand = 1.0F;
+                                    int exponent = 0;
+                                    bool zero = false;
+#pragma unroll
+                                    for (int k = 0; k < 4; ++k) {
+                                        if (!isfinite(num[k]) || num[k] < 0.0F) {
+                                            lane.fail();
+                                        }
+                                        if (num[k] == 0.0F) {
+                                            zero = true;
+                                        }
+                                        if (!zero) {
+                                            int fe = 0;
+                                            significand *= frexpf(num[k], &fe);
+                                            exponent += fe;
+                                        }
+                                    }
+                                    if (zero) {
+                                        nb[l] = 0.0F;
+                                        continue;
+                                    }
+                                    int pe = 0, ne = 0;
+                                    significand /= frexpf(bs.pdf, &pe);
+                                    exponent -= pe;
+                                    significand = frexpf(significand, &ne);
+                                    nb[l] = scalbnf(significand, exponent + ne);
+                                    if (!isfinite(nb[l]) || !(nb[l] > 0.0F)) {
+                                        lane.fail();
+                                    }
+                                }
+                            }
+                            const float next_eta = eta * bs.eta_scale;
+                            if (!isfinite(next_eta) || !(next_eta > 0.0F)) {
+                                lane.fail();
+                            }
+                            const F3 origin = offset_ray_origin(surf.position, surf.error, surf.ng, wi_world, lane);
+                            if (origin == surf.position) {
+                                lane.fail();
+                            }
+                            if (lane.err == 0) {
+                                beta = make_float4(nb[0], nb[1], nb[2], nb[3]);
+                                w.beta[slot] = beta;
+                                w.depth[slot] = next_depth;
+                                w.eta[slot] = next_eta;
+                                w.prev[slot] = make_float4(surf.position.x, surf.position.y, surf.position.z, bs.pdf);
+                                w.flags[slot] = (w.flags[slot] & ~0xFFU) | 2U;  // any_non_delta_bounces
+                                w.ray_o[slot] = make_float4(origin.x, origin.y, origin.z, kInf);
+                                w.ray_d[slot] = make_float4(wi_world.x, wi_world.y, wi_world.z, 0.0F);
+                                if (nb[0] == 0.0F && nb[1] == 0.0F && nb[2] == 0.0F && nb[3] == 0.0F) {
+                                    done = true;
+                                    termination = 3U;
+                                } else if (p.roulette != 0U && depth_total(next_depth) >= p.roulette_first) {
+                                    // evaluate_russian_roulette (RussianRoulette.cpp)
+                                    float mt = 0.0F;
+#pragma unroll
+                                    for (int l = 0; l < 4; ++l) mt = bf_max(mt, nb[l]);
+                                    float survival;
+                                    if (mt >= p.roulette_max / next_eta) {
+                                        survival = p.roulette_max;
+                                    } else if (mt <= p.roulette_min / next_eta) {
+                                        survival = p.roulette_min;
+                                    } else {
+                                        const float v = mt * next_eta;
+                                        survival = v < p.roulette_min ? p.roulette_min
+                                                                      : (p.roulette_max < v ? p.roulette_max : v);
+                                    }
+                                    const float u = stream.sample_1d(dims + 9);
+                                    if (!(u < survival)) {
+                                        done = true;
+                                        termination = 4U;  // russian_roulette
+                                    } else {
+                                        float cb[4];
+#pragma unroll
+                                        for (int l = 0; l < 4; ++l) {
+                                            cb[l] = nb[l] / survival;
+                                            if (!isfinite(cb[l]) || (nb[l] != 0.0F && cb[l] == 0.0F)) {
+                                                lane.fail();
+                                            }
+                                        }
+                                        w.beta[slot] = make_float4(cb[0], cb[1], cb[2], cb[3]);
+                                    }
+                                }
+                            } else {
+                                done = true;
+                            }
+                        }
+                    }
+                }
+                w.radiance[slot] = rad;
+                if (lane.err != 0) {
+                    rec.valid = false;
+                    w.status[slot] = (w.status[slot] & ~0xFFU) | lane.err;
+                    w.state[slot] = kSlotDone;
+                } else if (done) {
+                    terminate(w, slot, termination, blocked);
+                } else {
+                    ++active_here;
+                }
+            }
+        }
+        // shadow-queue compaction: warp ballot / popc, block scan of warp totals, one atomic per block
+        const unsigned ballot = __ballot_sync(0xFFFFFFFFU, rec.valid);
+        const uint32_t warp = threadIdx.x >> 5, lane_id = threadIdx.x & 31U;
+        if (lane_id == 0U) {
+            warp_counts[warp] = __popc(ballot);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0U) {
+            uint32_t total = 0;
+            for (uint32_t k = 0; k < blockDim.x / 32U; ++k) {
+                const uint32_t c = warp_counts[k];
+                warp_counts[k] = total;
+                total += c;
+            }
+            block_base = total > 0U ? atomicAdd(&w.counters[0], static_cast<unsigned long long>(total)) : 0ULL;
+        }
+        __syncthreads();
+        if (rec.valid) {
+            const uint32_t index = static_cast<uint32_t>(block_base) + warp_counts[warp] +
+                                   __popc(ballot & ((1U << lane_id) - 1U));
+            w.shadow_slot[index] = slot;
+            w.shadow_o[index] = make_float4(rec.origin.x, rec.origin.y, rec.origin.z, rec.t_max);
+            w.shadow_d[index] = make_float4(rec.direction.x, rec.direction.y, rec.direction.z, 0.0F);
+            w.shadow_c[index] = make_float4(rec.contribution[0], rec.contribution[1], rec.contribution[2],
+                                            rec.contribution[3]);
+        }
+        __syncthreads();
+    }
+    // active-slot count for the host's termination test
+    for (int off = 16; off > 0; off >>= 1) {
+        active_here += __shfl_down_sync(0xFFFFFFFFU, active_here, off);
+    }
+    if ((threadIdx.x & 31U) == 0U && active_here != 0U) {
+        atomicAdd(&w.counters[2], static_cast<unsigned long long>(active_here));
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_occlude: shadow rays of the compacted queue; unoccluded contributions join the path radiance
+// ------------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_occlude(SceneView s, Wavefront w) {
+    const uint32_t count = static_cast<uint32_t>(w.counters[0]);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const uint32_t slot = w.shadow_slot[i];
+        const float4 o = w.shadow_o[i], d = w.shadow_d[i];
+        const int occluded = any_hit(s, ld3(o), ld3(d), 0.0F, o.w, w.mask[slot]);
+        if (occluded < 0) {
+            w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneTraversal;
+            w.state[slot] = kSlotDone;
+            continue;
+        }
+        if (occluded == 0) {
+            const float4 c = w.shadow_c[i];
+            float4 r = w.radiance[slot];
+            r.x = r.x + c.x;
+            r.y = r.y + c.y;
+            r.z = r.z + c.z;
+            r.w = r.w + c.w;
+            w.radiance[slot] = r;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_film: CIE 1931 XYZ -> linear sRGB -> add_sample(x, y, rgb, 1) in sample order per pixel
+// ------------------------------------------------------------------------------------------------
+
+struct SensorView {
+    float response[4][3];
+    float pdf[4];
+    float normalization;
+};
+
+__device__ __forceinline__ float sensor_term(float c, float r, float n, float p) {
+    if (c == 0.0F || r == 0.0F) {
+        return 0.0F;
+    }
+    int ec = 0, er = 0, en = 0, ep = 0;
+    const float mc = frexpf(c, &ec), mr = frexpf(r, &er), mn = frexpf(n, &en), mp = frexpf(p, &ep);
+    const float mantissa = mc * mr * mn / mp;
+    return ldexpf(mantissa, ec + er + en - ep);
+}
+
+__global__ void k_film(const float4* path_radiance, uint32_t pixels, uint32_t samples, SensorView sensor,
+                       uint32_t precision, float4* film32, double* film64, unsigned long long* counts,
+                       unsigned long long* skipped) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pixels) {
+        return;
+    }
+    float4 f = precision == 0U ? film32[p] : make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+    double sum[4] = {0, 0, 0, 0}, comp[4] = {0, 0, 0, 0};
+    if (precision != 0U) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            sum[k] = film64[8ULL * p + k];
+            comp[k] = film64[8ULL * p + 4 + k];
+        }
+    }
+    unsigned long long count = counts[p];
+    for (uint32_t s = 0; s < samples; ++s) {
+        const float4 L = path_radiance[static_cast<uint64_t>(s) * pixels + p];
+        if (isnan(L.x)) {
+            atomicAdd(skipped, 1ULL);
+            continue;
+        }
+        const float lv[4] = {L.x, L.y, L.z, L.w};
+        float xyz[3] = {0.0F, 0.0F, 0.0F};
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                xyz[k] += sensor_term(lv[l], sensor.response[l][k], sensor.normalization, sensor.pdf[l]);
+            }
+        }
+        const float red = 3.2404542F * xyz[0] - 1.5371385F * xyz[1] - 0.4985314F * xyz[2];
+        const float green = -0.9692660F * xyz[0] + 1.8760108F * xyz[1] + 0.0415560F * xyz[2];
+        const float blue = 0.0556434F * xyz[0] - 0.2040259F * xyz[1] + 1.0572252F * xyz[2];
+        if (precision == 0U) {
+            f.x += red * 1.0F;
+            f.y += green * 1.0F;
+            f.z += blue * 1.0F;
+            f.w += 1.0F;
+        } else {
+            const double v[4] = {static_cast<double>(red), static_cast<double>(green), static_cast<double>(blue), 1.0};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double updated = sum[k] + v[k];
+                if (fabs(sum[k]) >= fabs(v[k])) {
+                    comp[k] += (sum[k] - updated) + v[k];
+                } else {
+                    comp[k] += (v[k] - updated) + sum[k];
+                }
+                sum[k] = updated;
+            }
+        }
+        ++count;
+    }
+    if (precision == 0U) {
+        film32[p] = f;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            film64[8ULL * p + k] = sum[k];
+            film64[8ULL * p + 4 + k] = comp[k];
+        }
+    }
+    counts[p] = count;
+}
+
+// Standalone closest-hit / occlusion queries (ClosestHit.hpp:21-28, Occlusion.hpp:19-26).
+__global__ void k_query_closest(SceneView s, const bf200_ray_v1* rays, uint64_t n, bf200_hit_v1* hits) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const bf200_ray_v1 r = rays[i];
+        const F3 o{r.origin[0], r.origin[1], r.origin[2]}, d{r.direction[0], r.direction[1], r.direction[2]};
+        const ClosestResult c = closest_hit(s, o, d, r.t_min, r.t_max, r.mask);
+        bf200_hit_v1 h;
+        h.t = 0.0F;
+        h.barycentrics[0] = h.barycentrics[1] = h.barycentrics[2] = 0.0F;
+        h.instance_index = 0xFFFFFFFFU;
+        h.primitive_index = 0xFFFFFFFFU;
+        h.status = c.failed ? kLaneTraversal : 0U;
+        h.reserved = 0U;
+        if (!c.failed && c.instance != 0xFFFFFFFFU) {
+            TriangleHit th;
+            if (hit_barycentrics(s, c, o, d, r.t_min, r.t_max, th)) {
+                h.t = c.t;
+                h.barycentrics[0] = th.b0;
+                h.barycentrics[1] = th.b1;
+                h.barycentrics[2] = th.b2;
+                h.instance_index = c.instance;
+                h.primitive_index = c.primitive;
+            } else {
+                h.status = kLaneNumerical;
+            }
+        }
+        hits[i] = h;
+    }
+}
+
+__global__ void k_query_occlusion(SceneView s, const bf200_ray_v1* rays, uint64_t n, uint32_t* out) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const bf200_ray_v1 r = rays[i];
+        const F3 o{r.origin[0], r.origin[1], r.origin[2]}, d{r.direction[0], r.direction[1], r.direction[2]};
+        const int occ = any_hit(s, o, d, r.t_min, r.t_max, r.mask);
+        out[i] = occ < 0 ? 2U : static_cast<uint32_t>(occ);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Host-side launchers
+// ------------------------------------------------------------------------------------------------
+
+cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instance, const uint32_t* tri_local,
+                                 uint32_t total, float4* out, uint32_t* failures, cudaStream_t stream) {
+    if (total == 0U) {
+        return cudaSuccess;
+    }
+    const uint32_t blocks = (total + 127U) / 128U;
+    k_world_normals<<<blocks < 4096U ? blocks : 4096U, 128, 0, stream>>>(s, tri_instance, tri_local, total, out,
+                                                                          failures);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
+                         const TransportParams& p, uint32_t grid, cudaStream_t stream) {
+    if (stage == 0) {
+        k_intersect<<<grid, 256, 0, stream>>>(s, w, src);
+    } else if (stage == 1) {
+        k_shade<<<grid, 256, 0, stream>>>(s, w, src, p);
+    } else {
+        k_occlude<<<grid, 256, 0, stream>>>(s, w);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_retire(const SceneView& s, const Wavefront& w, const PathSource& src, uint32_t grid,
+                          cudaStream_t stream) {
+    k_intersect<<<grid, 256, 0, stream>>>(s, w, src);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_film(const float4* path_radiance, uint32_t pixels, uint32_t samples, const float* response12,
+                        const float* pdf4, float normalization, uint32_t precision, float4* film32, double* film64,
+                        unsigned long long* counts, unsigned long long* skipped, cudaStream_t stream) {
+    SensorView sv;
+    for (int l = 0; l < 4; ++l) {
+        for (int k = 0; k < 3; ++k) {
+            sv.response[l][k] = response12[3 * l + k];
+        }
+        sv.pdf[l] = pdf4[l];
+    }
+    sv.normalization = normalization;
+    k_film<<<(pixels + 127U) / 128U, 128, 0, stream>>>(path_radiance, pixels, samples, sv, precision, film32, film64,
+                                                      counts, skipped);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_queries(const SceneView& s, const bf200_ray_v1* rays, uint64_t n, bf200_hit_v1* hits,
+                           uint32_t* occluded, cudaStream_t stream) {
+    const uint64_t blocks64 = (n + 127U) / 128U;
+    const uint32_t blocks = static_cast<uint32_t>(blocks64 < 65535U ? (blocks64 == 0 ? 1 : blocks64) : 65535U);
+    if (hits != nullptr) {
+        k_query_closest<<<blocks, 128, 0, stream>>>(s, rays, n, hits);
+    } else {
+        k_query_occlusion<<<blocks, 128, 0, stream>>>(s, rays, n, occluded);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace bf200

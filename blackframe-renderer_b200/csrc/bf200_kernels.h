@@ -1,0 +1,23 @@
+// Host-side launchers of the bf200 device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bf200_device.cuh"
+
+namespace bf200 {
+
+cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instance, const uint32_t* tri_local,
+                                 uint32_t total, float4* out, uint32_t* failures, cudaStream_t stream);
+// stage 0: k_intersect, 1: k_shade, 2: k_occlude
+cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
+                         const TransportParams& p, uint32_t grid, cudaStream_t stream);
+cudaError_t launch_retire(const SceneView& s, const Wavefront& w, const PathSource& src, uint32_t grid,
+                          cudaStream_t stream);
+cudaError_t launch_film(const float4* path_radiance, uint32_t pixels, uint32_t samples, const float* response12,
+                        const float* pdf4, float normalization, uint32_t precision, float4* film32, double* film64,
+                        unsigned long long* counts, unsigned long long* skipped, cudaStream_t stream);
+cudaError_t launch_queries(const SceneView& s, const bf200_ray_v1* rays, uint64_t n, bf200_hit_v1* hits,
+                           uint32_t* occluded, cudaStream_t stream);
+
+}  // namespace bf200

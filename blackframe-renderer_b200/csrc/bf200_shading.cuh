@@ -1,0 +1,1339 @@
+// Device numerics of the transport: sampler, frames, closures, lights, MIS, Russian roulette.
+//
+// Every function keeps the operation order of the reference's scalar loop so that a lane's float
+// results match the scalar oracle bit for bit; the file is compiled without FMA contraction and
+// fmaf() appears exactly where the reference calls std::fma. References are to the reference
+// repository (Blackframe/Renderer/Include/Blackframe/Renderer/...). A failed check sets the
+// lane's error code (the reference returns an error for the whole path); the wavefront then
+// retires the lane with that status instead of substituting a value.
+#pragma once
+
+#include "bf200_geometry.cuh"
+
+namespace bf200 {
+
+constexpr float kInf = __builtin_huge_valf();
+constexpr float kEps = 1.1920928955078125e-7F;
+constexpr float kDenormMin = 1.40129846e-45F;
+constexpr float kInvPi = 0.318309886183790671538F;
+constexpr float kPi = 3.14159265358979323846F;
+
+constexpr uint32_t kLobeDiffuse = 0x01U, kLobeGlossy = 0x02U, kLobeSpecular = 0x04U;
+constexpr uint32_t kLobeReflection = 0x08U, kLobeTransmission = 0x10U, kLobeVolume = 0x20U;
+constexpr uint32_t kClosureLambert = 1U, kClosureConductor = 3U, kClosureDielectric = 4U;
+
+// Lane failure codes (include/bf200.h BF200_LANE_*)
+constexpr uint32_t kLaneNumerical = 1U, kLaneUnsupported = 2U, kLaneTraversal = 3U;
+
+struct Lane {
+    uint32_t err = 0;
+    __device__ __forceinline__ void fail(uint32_t code = kLaneNumerical) {
+        if (err == 0) {
+            err = code;
+        }
+    }
+};
+
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ F3 operator*(F3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ F3 operator/(F3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ bool operator==(F3 a, F3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+__device__ __forceinline__ bool operator!=(F3 a, F3 b) { return !(a == b); }
+__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ F3 cross(F3 a, F3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ bool finite3(F3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+__device__ __forceinline__ float max_abs3(F3 v) {
+    return bf_max(bf_max(fabsf(v.x), fabsf(v.y)), fabsf(v.z));
+}
+__device__ __forceinline__ F3 ld3(const float4 v) { return {v.x, v.y, v.z}; }
+
+// Sine and cosine of a float angle: the double-precision functions rounded once to float.
+__device__ __forceinline__ float sin_f(float a) { return static_cast<float>(sin(static_cast<double>(a))); }
+__device__ __forceinline__ float cos_f(float a) { return static_cast<float>(cos(static_cast<double>(a))); }
+
+// ------------------------------------------------------------------------------------------------
+// SampleStream (SampleStream.hpp:23-67) and SampleDimensionMap (SampleDimensionMap.cpp:47-68)
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint64_t mix_bits(uint64_t v) {
+    v ^= v >> 30U;
+    v *= 0xBF58476D1CE4E5B9ULL;
+    v ^= v >> 27U;
+    v *= 0x94D049BB133111EBULL;
+    return v ^ (v >> 31U);
+}
+
+struct Stream {
+    uint64_t state;  // the (seed, pixel, sample) prefix of indexed_bits
+    __device__ __forceinline__ static Stream make(uint32_t px, uint32_t py, uint64_t sample, uint64_t seed) {
+        const uint64_t packed = (static_cast<uint64_t>(px) << 32U) | static_cast<uint64_t>(py);
+        uint64_t s = mix_bits(seed ^ 0x9E3779B97F4A7C15ULL);
+        s = mix_bits(s ^ packed ^ 0xD1B54A32D192ED03ULL);
+        s = mix_bits(s ^ sample ^ 0x8CB92BA72F3D8DD7ULL);
+        return Stream{s};
+    }
+    __device__ __forceinline__ float sample_1d(uint64_t dimension) const {
+        const uint64_t bits = mix_bits(state ^ dimension);
+        return static_cast<float>(bits >> 40U) * 0x1p-24F;
+    }
+};
+
+constexpr uint64_t kCameraRasterX = 0xA24BAED4963EE407ULL;
+constexpr uint64_t kCameraRasterY = 0x9FB21C651E98DF25ULL;
+
+__device__ __forceinline__ uint64_t bounce_base(uint32_t bounce) { return 4ULL + 10ULL * bounce; }
+
+// ------------------------------------------------------------------------------------------------
+// Frames and directions (LocalFrame.hpp, BsdfOnlyPathLoop.hpp:190-209)
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ F3 robust_unit(F3 d, Lane& lane) {
+    if (!finite3(d)) {
+        lane.fail();
+        return d;
+    }
+    const float m = max_abs3(d);
+    if (m == 0.0F) {
+        lane.fail();
+        return d;
+    }
+    const F3 s = d / m;
+    const float magnitude = sqrtf(dot(s, s));
+    const F3 r = s / magnitude;
+    if (!finite3(r)) {
+        lane.fail();
+    }
+    return r;
+}
+
+__device__ __forceinline__ bool unit_length(F3 d) {
+    if (!finite3(d)) {
+        return false;
+    }
+    const float sq = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    return isfinite(sq) && fabsf(sq - 1.0F) <= kEps * 128.0F;
+}
+
+struct Frame {
+    F3 t, b, n;
+    __device__ __forceinline__ F3 to_local(F3 w) const { return {dot(w, t), dot(w, b), dot(w, n)}; }
+    __device__ __forceinline__ F3 to_world(F3 l) const {
+        return {t.x * l.x + b.x * l.y + n.x * l.z, t.y * l.x + b.y * l.y + n.y * l.z,
+                t.z * l.x + b.z * l.y + n.z * l.z};
+    }
+};
+
+__device__ __forceinline__ F3 robust_unit_vector(F3 v, Lane& lane) {
+    const float m = max_abs3(v);
+    if (!finite3(v) || m == 0.0F) {
+        lane.fail();
+        return v;
+    }
+    const F3 s = v / m;
+    const float magnitude = sqrtf(dot(s, s));
+    return s / magnitude;
+}
+
+__device__ __forceinline__ bool orthonormal(F3 t, F3 b, F3 n) {
+    const float tol = kEps * 128.0F;
+    return fabsf(dot(t, t) - 1.0F) <= tol && fabsf(dot(b, b) - 1.0F) <= tol &&
+           fabsf(dot(n, n) - 1.0F) <= tol && fabsf(dot(t, b)) <= tol && fabsf(dot(t, n)) <= tol &&
+           fabsf(dot(b, n)) <= tol && fabsf(dot(cross(t, b), n) - 1.0F) <= tol;
+}
+
+// LocalFrame.hpp:188-219
+__device__ __forceinline__ Frame frame_from_unit_normal_and_tangent(F3 n, F3 tangent, Lane& lane) {
+    const F3 td = robust_unit_vector(tangent, lane);
+    const F3 projected = td - n * dot(td, n);
+    F3 ut = robust_unit_vector(projected, lane);
+    const F3 ub = robust_unit_vector(cross(n, ut), lane);
+    ut = robust_unit_vector(cross(ub, n), lane);
+    if (!orthonormal(ut, ub, n)) {
+        lane.fail();
+    }
+    return Frame{ut, ub, n};
+}
+
+// LocalFrame.hpp:66-80 (from_normal), LocalFrame.hpp:8-30 (robust_unit_normal)
+__device__ __forceinline__ Frame frame_from_normal(F3 v, Lane& lane) {
+    const float m = max_abs3(v);
+    if (!finite3(v) || m == 0.0F) {
+        lane.fail();
+        return Frame{};
+    }
+    const F3 s{v.x / m, v.y / m, v.z / m};
+    const float magnitude = sqrtf(s.x * s.x + s.y * s.y + s.z * s.z);
+    const F3 n{s.x / magnitude, s.y / magnitude, s.z / magnitude};
+    const float sign = copysignf(1.0F, n.z);
+    const float coefficient = -1.0F / (sign + n.z);
+    const float product = n.x * n.y * coefficient;
+    const F3 seed{1.0F + sign * n.x * n.x * coefficient, sign * product, -sign * n.x};
+    return frame_from_unit_normal_and_tangent(n, seed, lane);
+}
+
+// LocalFrame.hpp:116-135
+__device__ __forceinline__ Frame rotated_about_normal(const Frame& f, float angle, Lane& lane) {
+    const float reduced = remainderf(angle, 2.0F * kPi);
+    const float c = cos_f(reduced);
+    const float s = sin_f(reduced);
+    const F3 rotated = f.t * c + f.b * s;
+    return frame_from_unit_normal_and_tangent(f.n, rotated, lane);
+}
+
+// RayOriginOffset.hpp:58-117
+__device__ __forceinline__ float outward(float value, float off) {
+    if (off > 0.0F) {
+        return nextafterf(value, kInf);
+    }
+    if (off < 0.0F) {
+        return nextafterf(value, -kInf);
+    }
+    return value;
+}
+
+__device__ __forceinline__ F3 offset_ray_origin(F3 p, F3 err, F3 ng, F3 w, Lane& lane) {
+    const float m = max_abs3(ng);
+    const F3 sn = ng / m;
+    const F3 n = sn / sqrtf(dot(sn, sn));
+    const float d = fabsf(n.x) * err.x + fabsf(n.y) * err.y + fabsf(n.z) * err.z;
+    if (!isfinite(d)) {
+        lane.fail();
+    }
+    const float ds = max_abs3(w);
+    const F3 sw = w / ds;
+    F3 offset{n.x * d, n.y * d, n.z * d};
+    if (dot(n, sw) < 0.0F) {
+        offset = -offset;
+    }
+    const F3 shifted{outward(p.x + offset.x, offset.x), outward(p.y + offset.y, offset.y),
+                     outward(p.z + offset.z, offset.z)};
+    if (!finite3(shifted)) {
+        lane.fail();
+    }
+    return shifted;
+}
+
+// ShadowRay.hpp:15-48
+__device__ __forceinline__ F3 offset_surface_point(F3 p, F3 err, F3 ng, F3 w, Lane& lane) {
+    const F3 offset = offset_ray_origin(p, err, ng, w, lane);
+    if (offset != p) {
+        return offset;
+    }
+    F3 oriented = ng;
+    if (dot(ng, w) < 0.0F) {
+        oriented = -oriented;
+    }
+    F3 s = p;
+    if (oriented.x != 0.0F) s.x = nextafterf(p.x, oriented.x > 0.0F ? kInf : -kInf);
+    if (oriented.y != 0.0F) s.y = nextafterf(p.y, oriented.y > 0.0F ? kInf : -kInf);
+    if (oriented.z != 0.0F) s.z = nextafterf(p.z, oriented.z > 0.0F ? kInf : -kInf);
+    if (!finite3(s) || s == p) {
+        lane.fail();
+    }
+    return s;
+}
+
+// ShadowRay.hpp:107-135
+__device__ __forceinline__ void unit_segment(F3 origin, F3 endpoint, F3 expected, F3& direction,
+                                             float& length, Lane& lane) {
+    const F3 disp = endpoint - origin;
+    const float scale = max_abs3(disp);
+    if (!(scale > 0.0F) || !isfinite(scale)) {
+        lane.fail();
+        return;
+    }
+    const F3 s = disp / scale;
+    const float sq = fmaf(s.x, s.x, fmaf(s.y, s.y, s.z * s.z));
+    const float sl = sqrtf(sq);
+    length = scale * sl;
+    if (!(sl > 0.0F) || !isfinite(sl) || !(length > 0.0F) || !isfinite(length)) {
+        lane.fail();
+        return;
+    }
+    direction = s / sl;
+    const float alignment = dot(direction, expected);
+    if (!isfinite(alignment) || !(alignment > 0.0F)) {
+        lane.fail();
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Checked products (frexp / scalbn forms)
+// ------------------------------------------------------------------------------------------------
+
+// DirectLighting.hpp:21-62
+template <int NN, int ND>
+__device__ __forceinline__ float checked_product_quotient(const float (&num)[NN], const float (&den)[ND],
+                                                          Lane& lane) {
+    float significand = 1.0F;
+    int exponent = 0;
+#pragma unroll
+    for (int i = 0; i < NN; ++i) {
+        const float v = num[i];
+        if (!isfinite(v) || v < 0.0F) {
+            lane.fail();
+            return 0.0F;
+        }
+        if (v == 0.0F) {
+            return 0.0F;
+        }
+        int e = 0;
+        significand *= frexpf(v, &e);
+        exponent += e;
+    }
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+        const float v = den[i];
+        if (!isfinite(v) || !(v > 0.0F)) {
+            lane.fail();
+            return 0.0F;
+        }
+        int e = 0;
+        significand /= frexpf(v, &e);
+        exponent -= e;
+    }
+    int ne = 0;
+    significand = frexpf(significand, &ne);
+    const float result = scalbnf(significand, exponent + ne);
+    if (!isfinite(result) || !(result > 0.0F)) {
+        lane.fail();
+    }
+    return result;
+}
+
+// RoughDielectric.hpp:52-86
+template <int NN, int ND>
+__device__ __forceinline__ float checked_product_ratio(const float (&num)[NN], const float (&den)[ND],
+                                                       Lane& lane) {
+    bool zero = false;
+#pragma unroll
+    for (int i = 0; i < NN; ++i) {
+        if (!isfinite(num[i]) || num[i] < 0.0F) {
+            lane.fail();
+            return 0.0F;
+        }
+        zero = zero || num[i] == 0.0F;
+    }
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+        if (!isfinite(den[i]) || !(den[i] > 0.0F)) {
+            lane.fail();
+            return 0.0F;
+        }
+    }
+    if (zero) {
+        return 0.0F;
+    }
+    float significand = 1.0F;
+    int exponent = 0;
+#pragma unroll
+    for (int i = 0; i < NN; ++i) {
+        int ve = 0, ne = 0;
+        const float vs = frexpf(num[i], &ve);
+        significand = frexpf(significand * vs, &ne);
+        exponent += ve + ne;
+    }
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+        int ve = 0, ne = 0;
+        const float vs = frexpf(den[i], &ve);
+        significand = frexpf(significand / vs, &ne);
+        exponent += ne - ve;
+    }
+    const float result = scalbnf(significand, exponent);
+    if (!isfinite(result) || !(result > 0.0F)) {
+        lane.fail();
+    }
+    return result;
+}
+
+// MisHeuristics.hpp:142-172
+__device__ __forceinline__ float positive_product2(float a, float b, Lane& lane) {
+    if (b == 0.0F) {
+        return 0.0F;
+    }
+    int ea = 0, eb = 0, en = 0;
+    const float sa = frexpf(a, &ea);
+    const float sb = frexpf(b, &eb);
+    const float n = frexpf(sa * sb, &en);
+    const float r = scalbnf(n, ea + eb + en);
+    if (!isfinite(r) || !(r > 0.0F)) {
+        lane.fail();
+    }
+    return r;
+}
+
+// MisHeuristics.hpp:44-141
+__device__ __forceinline__ float mis_weight(uint32_t heuristic, float sampled, float competing, Lane& lane) {
+    if (!isfinite(sampled) || !(sampled > 0.0F) || !isfinite(competing) || competing < 0.0F) {
+        lane.fail();
+        return 1.0F;
+    }
+    if (competing == 0.0F) {
+        return 1.0F;
+    }
+    const bool small = sampled < competing;
+    const float n = small ? sampled : competing;
+    const float d = small ? competing : sampled;
+    int ne = 0, de = 0;
+    const float ns = frexpf(n, &ne);
+    const float ds = frexpf(d, &de);
+    float ratio;
+    if (heuristic == 0U) {
+        ratio = scalbnf(ns / ds, ne - de);
+    } else {
+        const float r = ns / ds;
+        ratio = scalbnf(r * r, 2 * (ne - de));
+    }
+    if (small) {
+        if (!(ratio > 0.0F)) {
+            lane.fail();
+            return 1.0F;
+        }
+        const float w = ratio / (1.0F + ratio);
+        if (!isfinite(w) || !(w > 0.0F)) {
+            lane.fail();
+        }
+        return w;
+    }
+    return 1.0F / (1.0F + ratio);
+}
+
+// MisHeuristics.hpp:143-172
+__device__ __forceinline__ float joint_light_pdf(float selection, float conditional, Lane& lane) {
+    if (!isfinite(selection) || !(selection > 0.0F) || selection > 1.0F || !isfinite(conditional) ||
+        conditional < 0.0F) {
+        lane.fail();
+        return 0.0F;
+    }
+    if (conditional == 0.0F) {
+        return 0.0F;
+    }
+    return positive_product2(selection, conditional, lane);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Emission (Emission.hpp:42-108) and area-pdf conversion (Light.hpp:75-163, 593-620)
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ bool unit_normal(F3 n) {
+    const float sq = fmaf(n.x, n.x, fmaf(n.y, n.y, n.z * n.z));
+    return finite3(n) && isfinite(sq) && fabsf(sq - 1.0F) <= kEps * 128.0F;
+}
+
+// +1 emitting side, 0 back side or exactly tangent; fails when the orientation is ambiguous.
+__device__ __forceinline__ int emission_side(F3 ng, F3 wo, Lane& lane) {
+    if (!unit_normal(ng) || !finite3(wo) || (wo.x == 0.0F && wo.y == 0.0F && wo.z == 0.0F)) {
+        lane.fail();
+        return 0;
+    }
+    const float m = max_abs3(wo);
+    const F3 s = wo / m;
+    const float alignment = fmaf(ng.x, s.x, fmaf(ng.y, s.y, ng.z * s.z));
+    if (!isfinite(alignment)) {
+        lane.fail();
+        return 0;
+    }
+    const bool orthogonal = (ng.x == 0.0F || wo.x == 0.0F) && (ng.y == 0.0F || wo.y == 0.0F) &&
+                            (ng.z == 0.0F || wo.z == 0.0F);
+    if (alignment == 0.0F && orthogonal) {
+        return 0;
+    }
+    const float abs_sum = fmaf(fabsf(ng.x), fabsf(s.x), fmaf(fabsf(ng.y), fabsf(s.y), fabsf(ng.z) * fabsf(s.z)));
+    const float uncertainty = fmaf(4.0F * kEps, abs_sum, 4.0F * kDenormMin);
+    if (fabsf(alignment) <= uncertainty) {
+        lane.fail();
+        return 0;
+    }
+    return alignment > 0.0F ? 1 : 0;
+}
+
+__device__ __forceinline__ float area_to_solid_angle(float area_pdf, F3 ref, F3 surf, F3 ng, Lane& lane) {
+    if (!unit_normal(ng)) {
+        lane.fail();
+        return 0.0F;
+    }
+    const F3 disp = surf - ref;
+    const float scale = max_abs3(disp);
+    if (!(scale > 0.0F) || !isfinite(scale)) {
+        lane.fail();
+        return 0.0F;
+    }
+    const F3 s = disp / scale;
+    const float sq = fmaf(s.x, s.x, fmaf(s.y, s.y, s.z * s.z));
+    const float sl = sqrtf(sq);
+    const float cubed = sq * sl;
+    if (!isfinite(sq) || !(sq > 0.0F) || !isfinite(cubed) || !(cubed > 0.0F)) {
+        lane.fail();
+        return 0.0F;
+    }
+    const float signed_alignment = fmaf(ng.x, -s.x, fmaf(ng.y, -s.y, ng.z * -s.z));
+    const float alignment = fabsf(signed_alignment);
+    const float term_sum = fmaf(fabsf(ng.x), fabsf(s.x), fmaf(fabsf(ng.y), fabsf(s.y), fabsf(ng.z) * fabsf(s.z)));
+    const float uncertainty = fmaf(4.0F * kEps, term_sum, 4.0F * kDenormMin);
+    if (!isfinite(alignment) || !isfinite(term_sum) || alignment <= uncertainty) {
+        lane.fail();
+        return 0.0F;
+    }
+    if (area_pdf == 0.0F) {
+        return 0.0F;
+    }
+    int es = 0, ed = 0, ec = 0, ea = 0, en = 0;
+    const float fs = frexpf(area_pdf, &es);
+    const float fd = frexpf(scale, &ed);
+    const float fc = frexpf(cubed, &ec);
+    const float fa = frexpf(alignment, &ea);
+    const float combined = fs * fd * fd * fc / fa;
+    const int exponent = es + 2 * ed + ec - ea;
+    const float normalized = frexpf(combined, &en);
+    const float converted = scalbnf(normalized, exponent + en);
+    if (!isfinite(converted) || !(converted > 0.0F)) {
+        lane.fail();
+    }
+    return converted;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Closures
+// ------------------------------------------------------------------------------------------------
+
+struct ClosureData {
+    uint32_t kind, lobes;
+    float w[4];
+    float p[10];
+};
+
+struct BsdfSample {
+    bool valid;
+    F3 wi;
+    float value[4];
+    float pdf;
+    uint32_t lobes;
+    float eta_scale;
+};
+
+// SamplingMappings.hpp:33-60, 128-141
+__device__ __forceinline__ F3 map_cosine_hemisphere(float u, float v) {
+    const float ox = 2.0F * u - 1.0F;
+    const float oy = 2.0F * v - 1.0F;
+    float px = 0.0F, py = 0.0F, radius = 0.0F;
+    if (!(ox == 0.0F && oy == 0.0F)) {
+        const float quarter_pi = kPi / 4.0F;
+        float r, phi;
+        if (fabsf(ox) > fabsf(oy)) {
+            r = ox;
+            phi = quarter_pi * (oy / ox);
+        } else {
+            r = oy;
+            phi = 2.0F * quarter_pi - quarter_pi * (ox / oy);
+        }
+        px = r * cos_f(phi);
+        py = r * sin_f(phi);
+        radius = fabsf(r);
+    }
+    const float z = sqrtf((1.0F - radius) * (1.0F + radius));
+    return F3{px, py, z};
+}
+
+struct Smith {
+    float normal, tangent, radius, nor;
+};
+
+// GgxMicrofacet.hpp:134-184
+__device__ __forceinline__ Smith smith_terms(float ax, float ay, F3 w, Lane& lane) {
+    Smith t;
+    if (ax == ay) {
+        const float sine = hypot2f(w.x, w.y);
+        const float inverse_alpha = 1.0F / ax;
+        t.normal = ax <= 1.0F ? w.z : w.z * inverse_alpha;
+        t.tangent = ax <= 1.0F ? ax * sine : sine;
+        t.radius = hypot2f(t.normal, t.tangent);
+    } else {
+        const float common = bf_max(bf_max(1.0F, ax), ay);
+        t.normal = w.z / common;
+        const float tx = (ax / common) * w.x;
+        const float ty = (ay / common) * w.y;
+        t.tangent = hypot2f(tx, ty);
+        t.radius = hypot2f(t.normal, t.tangent);
+    }
+    if (!isfinite(t.normal) || !isfinite(t.tangent) || !isfinite(t.radius) || !(t.normal > 0.0F) ||
+        !(t.radius > 0.0F)) {
+        lane.fail();
+        t.nor = 1.0F;
+        return t;
+    }
+    t.nor = t.normal / t.radius;
+    if (!isfinite(t.nor) || !(t.nor > 0.0F) || t.nor > 1.0F) {
+        lane.fail();
+    }
+    return t;
+}
+
+// GgxMicrofacet.hpp:232-270
+__device__ __forceinline__ float ggx_d(float ax, float ay, F3 m, Lane& lane) {
+    if (!unit_length(m)) {
+        lane.fail();
+        return 0.0F;
+    }
+    if (!(m.z > 0.0F)) {
+        return 0.0F;
+    }
+    float denominator_root, density_root;
+    if (ax == ay) {
+        const float radial = hypot2f(m.x, m.y);
+        if (ax <= 1.0F) {
+            denominator_root = hypot2f(radial, ax * m.z);
+            density_root = (ax / denominator_root) / denominator_root;
+        } else {
+            const float inverse_alpha = 1.0F / ax;
+            denominator_root = hypot2f(radial * inverse_alpha, m.z);
+            density_root = (inverse_alpha / denominator_root) / denominator_root;
+        }
+        density_root *= sqrtf(kInvPi);
+    } else {
+        denominator_root = hypot3f(m.x / ax, m.y / ay, m.z);
+        const float normalization_root = sqrtf(kInvPi) / (sqrtf(ax) * sqrtf(ay));
+        density_root = (normalization_root / denominator_root) / denominator_root;
+    }
+    const float value = density_root * density_root;
+    if (!isfinite(denominator_root) || !(denominator_root > 0.0F) || !isfinite(value) || !(value > 0.0F)) {
+        lane.fail();
+    }
+    return value;
+}
+
+// GgxMicrofacet.hpp:320-353
+__device__ __forceinline__ float ggx_g2(float ax, float ay, F3 wo, F3 wi, Lane& lane) {
+    if (!unit_length(wo) || !unit_length(wi)) {
+        lane.fail();
+        return 0.0F;
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+        return 0.0F;
+    }
+    const Smith o = smith_terms(ax, ay, wo, lane);
+    const Smith i = smith_terms(ax, ay, wi, lane);
+    const float smaller = bf_min(o.nor, i.nor);
+    const float larger = bf_max(o.nor, i.nor);
+    const float value = 2.0F * smaller / (1.0F + smaller / larger);
+    if (!isfinite(value) || !(value > 0.0F) || value > 1.0F) {
+        lane.fail();
+    }
+    return value;
+}
+
+// GgxMicrofacet.hpp:355-388
+__device__ __forceinline__ float ggx_vndf_pdf(float ax, float ay, F3 wo, F3 m, Lane& lane) {
+    if (!unit_length(wo) || !unit_length(m)) {
+        lane.fail();
+        return 0.0F;
+    }
+    const float visible_dot = dot(wo, m);
+    if (!(wo.z > 0.0F) || !(m.z > 0.0F) || !(visible_dot > 0.0F)) {
+        return 0.0F;
+    }
+    const float d = ggx_d(ax, ay, m, lane);
+    const float physical_radius = ax == ay ? hypot2f(wo.z, ax * hypot2f(wo.x, wo.y))
+                                           : hypot3f(wo.z, ax * wo.x, ay * wo.y);
+    const float physical_denominator = wo.z + physical_radius;
+    const float visible_factor = 2.0F * visible_dot / physical_denominator;
+    const float value = d * visible_factor;
+    if (!isfinite(physical_denominator) || !(physical_denominator > 0.0F) || !isfinite(value) ||
+        !(value > 0.0F)) {
+        lane.fail();
+    }
+    return value;
+}
+
+// GgxMicrofacet.hpp:71-103
+__device__ __forceinline__ F3 ggx_normalize(F3 v, Lane& lane) {
+    const float length = hypot2f(hypot2f(v.x, v.y), v.z);
+    if (!isfinite(length) || !(length > 0.0F)) {
+        lane.fail();
+        return F3{0.0F, 0.0F, 1.0F};
+    }
+    const F3 r{v.x / length, v.y / length, v.z / length};
+    if (!unit_length(r)) {
+        lane.fail();
+    }
+    return r;
+}
+
+__device__ __forceinline__ float nonnegative_roundoff(float value, float scale, Lane& lane) {
+    if (value >= 0.0F) {
+        return value;
+    }
+    const float bound = kEps * 16.0F * bf_max(1.0F, fabsf(scale));
+    if (-value <= bound) {
+        return 0.0F;
+    }
+    lane.fail();
+    return 0.0F;
+}
+
+// GgxMicrofacet.hpp:390-525
+static __device__ bool ggx_sample_vndf(float ax, float ay, F3 wo, float u, float v, F3& m_out, Lane& lane) {
+    if (!unit_length(wo)) {
+        lane.fail();
+        return false;
+    }
+    if (!(wo.z > 0.0F)) {
+        return false;
+    }
+    const bool iso = ax == ay;
+    const float inverse_alpha = 1.0F / ax;
+    const float common = bf_max(bf_max(1.0F, ax), ay);
+    const float sax = ax / common, say = ay / common;
+    F3 st;
+    if (iso) {
+        st = ax <= 1.0F ? F3{ax * wo.x, ax * wo.y, wo.z} : F3{wo.x, wo.y, wo.z * inverse_alpha};
+    } else {
+        st = F3{sax * wo.x, say * wo.y, wo.z / common};
+    }
+    if ((iso && ax <= 1.0F && ((wo.x != 0.0F && st.x == 0.0F) || (wo.y != 0.0F && st.y == 0.0F))) ||
+        (iso && ax > 1.0F && st.z == 0.0F) ||
+        (!iso && ((wo.x != 0.0F && st.x == 0.0F) || (wo.y != 0.0F && st.y == 0.0F) || st.z == 0.0F))) {
+        lane.fail();
+        return false;
+    }
+    const F3 hv = ggx_normalize(st, lane);
+    const float tl = hypot2f(hv.x, hv.y);
+    const F3 tangent = tl > 0.0F ? F3{-hv.y / tl, hv.x / tl, 0.0F} : F3{1.0F, 0.0F, 0.0F};
+    const F3 bitangent = cross(hv, tangent);
+    const float disk_radius = sqrtf(u);
+    const float azimuth = 2.0F * kPi * v;
+    const float disk_x = disk_radius * cos_f(azimuth);
+    const float initial_disk_y = disk_radius * sin_f(azimuth);
+    const float limit_sq = (1.0F - disk_x) * (1.0F + disk_x);
+    const float checked_limit_sq = nonnegative_roundoff(limit_sq, 1.0F + fabsf(disk_x), lane);
+    const float disk_y_limit = sqrtf(checked_limit_sq);
+    const float projection = 0.5F * (1.0F + hv.z);
+    const float disk_y = fmaf(projection, initial_disk_y, (1.0F - projection) * disk_y_limit);
+    const float hz_sq = fmaf(-disk_y, disk_y, checked_limit_sq);
+    const float checked_hz_sq = nonnegative_roundoff(hz_sq, checked_limit_sq + fabsf(disk_y * disk_y), lane);
+    const float hz = sqrtf(checked_hz_sq);
+    const F3 hn{fmaf(disk_x, tangent.x, fmaf(disk_y, bitangent.x, hz * hv.x)),
+                fmaf(disk_x, tangent.y, fmaf(disk_y, bitangent.y, hz * hv.y)),
+                fmaf(disk_x, tangent.z, fmaf(disk_y, bitangent.z, hz * hv.z))};
+    if (!(hn.z > 0.0F)) {
+        lane.fail();
+        return false;
+    }
+    F3 un;
+    if (iso) {
+        un = ax <= 1.0F ? F3{ax * hn.x, ax * hn.y, hn.z} : F3{hn.x, hn.y, hn.z * inverse_alpha};
+    } else {
+        un = F3{sax * hn.x, say * hn.y, hn.z / common};
+    }
+    if ((iso && ax <= 1.0F && ((hn.x != 0.0F && un.x == 0.0F) || (hn.y != 0.0F && un.y == 0.0F))) ||
+        (iso && ax > 1.0F && un.z == 0.0F) ||
+        (!iso && ((hn.x != 0.0F && un.x == 0.0F) || (hn.y != 0.0F && un.y == 0.0F) || un.z == 0.0F))) {
+        lane.fail();
+        return false;
+    }
+    const F3 m = ggx_normalize(un, lane);
+    if (!(m.z > 0.0F) || !(dot(wo, m) > 0.0F)) {
+        lane.fail();
+        return false;
+    }
+    m_out = m;
+    return true;
+}
+
+// Fresnel.hpp:27-104
+__device__ __forceinline__ float squared_magnitude_ratio(float nr, float ni, float dr, float di, Lane& lane) {
+    const float n = hypot2f(nr, ni);
+    const float d = hypot2f(dr, di);
+    if (!isfinite(n) || !isfinite(d) || !(d > 0.0F)) {
+        lane.fail();
+        return 0.0F;
+    }
+    const float amplitude = n / d;
+    const float r = amplitude * amplitude;
+    if (!isfinite(r) || r < 0.0F || r > 1.0F) {
+        lane.fail();
+    }
+    return r;
+}
+
+static __device__ float conductor_fresnel_lane(float cosine, float eta, float k, Lane& lane) {
+    if (eta == 1.0F && k == 0.0F) {
+        return 0.0F;
+    }
+    if (cosine == 0.0F) {
+        return 1.0F;
+    }
+    const float scale = bf_max(bf_max(1.0F, eta), k);
+    const float nie = 1.0F / scale;
+    const float ne = eta / scale;
+    const float nk = k / scale;
+    if (cosine == 1.0F) {
+        const float r = squared_magnitude_ratio(ne - nie, nk, ne + nie, nk, lane);
+        if (!(r > 0.0F)) {
+            lane.fail();
+        }
+        return r;
+    }
+    const float sin_sq = (1.0F - cosine) * (1.0F + cosine);
+    const float scaled_sin_sq = nie * nie * sin_sq;
+    const float x = fmaf(ne, ne, -fmaf(nk, nk, scaled_sin_sq));
+    const float y = 2.0F * ne * nk;
+    const float magnitude = hypot2f(x, y);
+    float rr, ri;
+    if (x >= 0.0F) {
+        rr = sqrtf(0.5F * (magnitude + x));
+        ri = rr == 0.0F ? 0.0F : y / (2.0F * rr);
+    } else {
+        ri = sqrtf(0.5F * (magnitude - x));
+        rr = ri == 0.0F ? 0.0F : y / (2.0F * ri);
+    }
+    const float sc = nie * cosine;
+    const float perpendicular = squared_magnitude_ratio(sc - rr, -ri, sc + rr, ri, lane);
+    const float ser = fmaf(ne, ne, -(nk * nk));
+    const float sei = y;
+    const float srr = nie * rr;
+    const float sri = nie * ri;
+    const float pbr = cosine * ser;
+    const float pbi = cosine * sei;
+    const float parallel = squared_magnitude_ratio(pbr - srr, pbi - sri, pbr + srr, pbi + sri, lane);
+    const float r = 0.5F * (perpendicular + parallel);
+    if (!isfinite(r) || !(r > 0.0F) || r > 1.0F) {
+        lane.fail();
+    }
+    return r;
+}
+
+// Fresnel.hpp:107-170
+static __device__ float dielectric_fresnel(float cosine, float eta_i, float eta_t, Lane& lane) {
+    if (!isfinite(cosine) || cosine < 0.0F || cosine > 1.0F) {
+        lane.fail();
+        return 1.0F;
+    }
+    if (eta_i == eta_t) {
+        return 0.0F;
+    }
+    if (cosine == 0.0F) {
+        return 1.0F;
+    }
+    const bool denser = eta_i > eta_t;
+    const float ne = denser ? eta_t / eta_i : eta_i / eta_t;
+    if (cosine == 1.0F) {
+        const float a = (1.0F - ne) / (1.0F + ne);
+        const float r = a * a;
+        if (!isfinite(r) || !(r > 0.0F) || r > 1.0F) {
+            lane.fail();
+        }
+        return r;
+    }
+    const float sin_i = sqrtf((1.0F - cosine) * (1.0F + cosine));
+    float sin_t;
+    if (denser) {
+        if (ne == 0.0F || sin_i >= ne) {
+            return 1.0F;
+        }
+        sin_t = sin_i / ne;
+    } else {
+        sin_t = ne * sin_i;
+    }
+    if (!(sin_t < 1.0F)) {
+        return 1.0F;
+    }
+    const float cos_t = sqrtf((1.0F - sin_t) * (1.0F + sin_t));
+    const float fec = ne * cos_t;
+    const float fa = (cosine - fec) / (cosine + fec);
+    const float sec = ne * cosine;
+    const float sa = (sec - cos_t) / (sec + cos_t);
+    const float r = 0.5F * fmaf(fa, fa, sa * sa);
+    if (!isfinite(r) || !(r > 0.0F) || r > 1.0F) {
+        lane.fail();
+    }
+    return r;
+}
+
+// RoughConductorReflection.hpp:68-106 / RoughDielectric.hpp:136-170
+__device__ __forceinline__ void half_vector_geometry(F3 wo, F3 wi, F3& m, float& half_cos, Lane& lane) {
+    const F3 h{wo.x + wi.x, wo.y + wi.y, wo.z + wi.z};
+    const float length = hypot2f(hypot2f(h.x, h.y), h.z);
+    if (!isfinite(length) || !(length > 0.0F)) {
+        lane.fail();
+        m = F3{0.0F, 0.0F, 1.0F};
+        half_cos = 1.0F;
+        return;
+    }
+    m = F3{h.x / length, h.y / length, h.z / length};
+    if (!unit_length(m) || !(m.z > 0.0F)) {
+        lane.fail();
+    }
+    half_cos = 0.5F * length;
+    if (!isfinite(half_cos) || !(half_cos > 0.0F) || half_cos > 1.0F) {
+        lane.fail();
+    }
+}
+
+// RoughConductorReflection.hpp:167-238
+static __device__ void conductor_eval(const ClosureData& c, F3 wo, F3 wi, float (&out)[4], Lane& lane) {
+    out[0] = out[1] = out[2] = out[3] = 0.0F;
+    if (!unit_length(wo) || !unit_length(wi)) {
+        lane.fail();
+        return;
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+        return;
+    }
+    if (c.w[0] == 0.0F && c.w[1] == 0.0F && c.w[2] == 0.0F && c.w[3] == 0.0F) {
+        return;
+    }
+    F3 m;
+    float hc;
+    half_vector_geometry(wo, wi, m, hc, lane);
+    const float d = ggx_d(c.p[8], c.p[9], m, lane);
+    const float g2 = ggx_g2(c.p[8], c.p[9], wo, wi, lane);
+    float fresnel[4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        fresnel[l] = conductor_fresnel_lane(hc, c.p[l], c.p[4 + l], lane);
+    }
+    const float denominator = 4.0F * wo.z * wi.z;
+    const float scale = (d * g2) / denominator;
+    if (!isfinite(denominator) || !(denominator > 0.0F) || !isfinite(scale) || !(scale > 0.0F)) {
+        lane.fail();
+        return;
+    }
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        out[l] = c.w[l] * fresnel[l] * scale;
+    }
+}
+
+static __device__ float conductor_pdf(const ClosureData& c, F3 wo, F3 wi, Lane& lane) {
+    if (!unit_length(wo) || !unit_length(wi)) {
+        lane.fail();
+        return 0.0F;
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+        return 0.0F;
+    }
+    F3 m;
+    float hc;
+    half_vector_geometry(wo, wi, m, hc, lane);
+    const float visible = ggx_vndf_pdf(c.p[8], c.p[9], wo, m, lane);
+    const float value = visible / (4.0F * hc);
+    if (!isfinite(value) || !(value > 0.0F)) {
+        lane.fail();
+    }
+    return value;
+}
+
+struct Interface {
+    float face_sign, incident_eta, transmitted_eta, nie, nte;
+};
+
+// RoughDielectric.hpp:114-134
+__device__ __forceinline__ Interface interface_for(F3 wo, float ext, float in) {
+    Interface f;
+    f.face_sign = wo.z > 0.0F ? 1.0F : -1.0F;
+    f.incident_eta = f.face_sign > 0.0F ? ext : in;
+    f.transmitted_eta = f.face_sign > 0.0F ? in : ext;
+    const float mx = bf_max(f.incident_eta, f.transmitted_eta);
+    f.nie = f.incident_eta / mx;
+    f.nte = f.transmitted_eta / mx;
+    return f;
+}
+
+__device__ __forceinline__ F3 scaled_dir(F3 d, float s) { return {s * d.x, s * d.y, s * d.z}; }
+
+struct TransmissionGeometry {
+    bool valid;
+    F3 m;
+    float od, id, length;
+};
+
+// RoughDielectric.hpp:172-223
+static __device__ TransmissionGeometry transmission_geometry(F3 of, F3 inf, const Interface& f, Lane& lane) {
+    TransmissionGeometry g{};
+    g.valid = false;
+    F3 h{fmaf(f.nie, of.x, f.nte * inf.x), fmaf(f.nie, of.y, f.nte * inf.y), fmaf(f.nie, of.z, f.nte * inf.z)};
+    const float length = hypot2f(hypot2f(h.x, h.y), h.z);
+    if (!isfinite(length) || !(length > 0.0F)) {
+        lane.fail();
+        return g;
+    }
+    h = scaled_dir(h, 1.0F / length);
+    if (h.z < 0.0F) {
+        h = scaled_dir(h, -1.0F);
+    }
+    if (h.z == 0.0F) {
+        return g;
+    }
+    if (!unit_length(h)) {
+        lane.fail();
+        return g;
+    }
+    const float od = dot(of, h);
+    const float id = dot(inf, h);
+    if (!isfinite(od) || !isfinite(id)) {
+        lane.fail();
+        return g;
+    }
+    if (!(od > 0.0F) || !(id < 0.0F)) {
+        return g;
+    }
+    if (od > 1.0F || id < -1.0F) {
+        lane.fail();
+        return g;
+    }
+    g.valid = true;
+    g.m = h;
+    g.od = od;
+    g.id = id;
+    g.length = length;
+    return g;
+}
+
+__device__ __forceinline__ void scale_spectrum(const float (&c)[4], float scale, float (&out)[4], Lane& lane) {
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        const float num[2] = {c[l], scale};
+        const float den[1] = {1.0F};
+        out[l] = checked_product_ratio(num, den, lane);
+    }
+}
+
+// RoughDielectric.hpp:299-381 (radiance mode)
+static __device__ void dielectric_eval(const ClosureData& c, F3 wo, F3 wi, float (&out)[4], Lane& lane) {
+    out[0] = out[1] = out[2] = out[3] = 0.0F;
+    if (!unit_length(wo) || !unit_length(wi)) {
+        lane.fail();
+        return;
+    }
+    if (wo.z == 0.0F || wi.z == 0.0F) {
+        return;
+    }
+    const float ax = c.p[2], ay = c.p[3];
+    const Interface f = interface_for(wo, c.p[0], c.p[1]);
+    const F3 of = scaled_dir(wo, f.face_sign);
+    const F3 inf = scaled_dir(wi, f.face_sign);
+    if (inf.z > 0.0F) {
+        F3 m;
+        float od;
+        half_vector_geometry(of, inf, m, od, lane);
+        const float fr = dielectric_fresnel(od, f.incident_eta, f.transmitted_eta, lane);
+        const float d = ggx_d(ax, ay, m, lane);
+        const float g2 = ggx_g2(ax, ay, of, inf, lane);
+        const float num[3] = {fr, d, g2};
+        const float den[3] = {4.0F, of.z, inf.z};
+        scale_spectrum(c.w, checked_product_ratio(num, den, lane), out, lane);
+        return;
+    }
+    const TransmissionGeometry tg = transmission_geometry(of, inf, f, lane);
+    if (!tg.valid) {
+        return;
+    }
+    const float fr = dielectric_fresnel(tg.od, f.incident_eta, f.transmitted_eta, lane);
+    if (fr == 1.0F) {
+        return;
+    }
+    if (!(tg.length > 0.0F)) {
+        lane.fail();
+        return;
+    }
+    const float d = ggx_d(ax, ay, tg.m, lane);
+    const float g2 = ggx_g2(ax, ay, of, scaled_dir(inf, -1.0F), lane);
+    const float eta = f.nie;
+    const float num[7] = {1.0F - fr, d, g2, eta, eta, tg.od, -tg.id};
+    const float den[4] = {of.z, -inf.z, tg.length, tg.length};
+    scale_spectrum(c.w, checked_product_ratio(num, den, lane), out, lane);
+}
+
+// RoughDielectric.hpp:383-467
+static __device__ float dielectric_pdf(const ClosureData& c, F3 wo, F3 wi, Lane& lane) {
+    if (!unit_length(wo) || !unit_length(wi)) {
+        lane.fail();
+        return 0.0F;
+    }
+    if (wo.z == 0.0F || wi.z == 0.0F) {
+        return 0.0F;
+    }
+    const float ax = c.p[2], ay = c.p[3];
+    const Interface f = interface_for(wo, c.p[0], c.p[1]);
+    const F3 of = scaled_dir(wo, f.face_sign);
+    const F3 inf = scaled_dir(wi, f.face_sign);
+    if (inf.z > 0.0F) {
+        F3 m;
+        float od;
+        half_vector_geometry(of, inf, m, od, lane);
+        const float fr = dielectric_fresnel(od, f.incident_eta, f.transmitted_eta, lane);
+        const float visible = ggx_vndf_pdf(ax, ay, of, m, lane);
+        const float num[2] = {fr, visible};
+        const float den[2] = {4.0F, od};
+        return checked_product_ratio(num, den, lane);
+    }
+    const TransmissionGeometry tg = transmission_geometry(of, inf, f, lane);
+    if (!tg.valid) {
+        return 0.0F;
+    }
+    const float fr = dielectric_fresnel(tg.od, f.incident_eta, f.transmitted_eta, lane);
+    if (fr == 1.0F) {
+        return 0.0F;
+    }
+    if (!(tg.length > 0.0F)) {
+        lane.fail();
+        return 0.0F;
+    }
+    const float visible = ggx_vndf_pdf(ax, ay, of, tg.m, lane);
+    const float num[5] = {1.0F - fr, visible, f.nte, f.nte, -tg.id};
+    const float den[2] = {tg.length, tg.length};
+    return checked_product_ratio(num, den, lane);
+}
+
+// DepthFilteredClosureMixture.hpp:48-133
+static __device__ float dielectric_pdf_masked(const ClosureData& c, uint32_t allowed, F3 wo, F3 wi, Lane& lane) {
+    const float base = dielectric_pdf(c, wo, wi, lane);
+    if (wo.z == 0.0F || wi.z == 0.0F || base == 0.0F) {
+        return base;
+    }
+    const bool reflection = (wo.z > 0.0F) == (wi.z > 0.0F);
+    const uint32_t direction = reflection ? kLobeReflection : kLobeTransmission;
+    if ((allowed & direction) == 0U) {
+        return 0.0F;
+    }
+    if (allowed == (kLobeReflection | kLobeTransmission)) {
+        return base;
+    }
+    const Interface f = interface_for(wo, c.p[0], c.p[1]);
+    const F3 of = scaled_dir(wo, f.face_sign);
+    const F3 inf = scaled_dir(wi, f.face_sign);
+    float branch;
+    if (reflection) {
+        F3 m;
+        float od;
+        half_vector_geometry(of, inf, m, od, lane);
+        branch = dielectric_fresnel(od, f.incident_eta, f.transmitted_eta, lane);
+    } else {
+        const TransmissionGeometry tg = transmission_geometry(of, inf, f, lane);
+        if (!tg.valid) {
+            return 0.0F;
+        }
+        branch = 1.0F - dielectric_fresnel(tg.od, f.incident_eta, f.transmitted_eta, lane);
+    }
+    if (!isfinite(branch) || !(branch > 0.0F) || branch > 1.0F) {
+        lane.fail();
+        return 0.0F;
+    }
+    const float num[1] = {base};
+    const float den[1] = {branch};
+    return checked_product_ratio(num, den, lane);
+}
+
+static __device__ void closure_eval(const ClosureData& c, uint32_t allowed, F3 wo, F3 wi, float (&out)[4], Lane& lane) {
+    if (c.kind == kClosureLambert) {  // LambertianReflection.hpp:76-85
+        out[0] = out[1] = out[2] = out[3] = 0.0F;
+        if (!unit_length(wo) || !unit_length(wi)) {
+            lane.fail();
+            return;
+        }
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return;
+        }
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            out[l] = c.w[l] * kInvPi;
+        }
+        return;
+    }
+    if (c.kind == kClosureConductor) {
+        conductor_eval(c, wo, wi, out, lane);
+        return;
+    }
+    dielectric_eval(c, wo, wi, out, lane);
+    if (wo.z == 0.0F || wi.z == 0.0F) {
+        return;
+    }
+    const uint32_t direction = (wo.z > 0.0F) == (wi.z > 0.0F) ? kLobeReflection : kLobeTransmission;
+    if ((allowed & direction) == 0U) {
+        out[0] = out[1] = out[2] = out[3] = 0.0F;
+    }
+}
+
+static __device__ float closure_pdf(const ClosureData& c, uint32_t allowed, F3 wo, F3 wi, Lane& lane) {
+    if (c.kind == kClosureLambert) {  // LambertianReflection.hpp:87-106
+        if (!unit_length(wo) || !unit_length(wi)) {
+            lane.fail();
+            return 0.0F;
+        }
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return 0.0F;
+        }
+        return wi.z * kInvPi;
+    }
+    if (c.kind == kClosureConductor) {
+        return conductor_pdf(c, wo, wi, lane);
+    }
+    return dielectric_pdf_masked(c, allowed, wo, wi, lane);
+}
+
+// RoughDielectric.hpp:469-632 (radiance mode)
+static __device__ void dielectric_sample(const ClosureData& c, F3 wo, float event, float u, float v, BsdfSample& s,
+                                  Lane& lane) {
+    s.valid = false;
+    if (!unit_length(wo) || !(event >= 0.0F && event < 1.0F)) {
+        lane.fail();
+        return;
+    }
+    if (wo.z == 0.0F) {
+        return;
+    }
+    const float ax = c.p[2], ay = c.p[3];
+    const Interface f = interface_for(wo, c.p[0], c.p[1]);
+    const F3 of = scaled_dir(wo, f.face_sign);
+    F3 m;
+    if (!ggx_sample_vndf(ax, ay, of, u, v, m, lane)) {
+        return;
+    }
+    const float od = dot(of, m);
+    if (!isfinite(od) || !(od > 0.0F) || od > 1.0F) {
+        lane.fail();
+        return;
+    }
+    const float fr = dielectric_fresnel(od, f.incident_eta, f.transmitted_eta, lane);
+    F3 inf;
+    uint32_t lobes;
+    float eta_scale = 1.0F;
+    if (event < fr) {
+        inf = F3{2.0F * od * m.x - of.x, 2.0F * od * m.y - of.y, 2.0F * od * m.z - of.z};
+        lobes = kLobeGlossy | kLobeReflection;
+        if (!unit_length(inf)) {
+            lane.fail();
+            return;
+        }
+        if (!(inf.z > 0.0F)) {
+            return;
+        }
+    } else {
+        const F3 tangent{of.x - od * m.x, of.y - od * m.y, of.z - od * m.z};
+        const float incident_sine = hypot2f(hypot2f(tangent.x, tangent.y), tangent.z);
+        if (!isfinite(incident_sine) || incident_sine > 1.0F) {
+            lane.fail();
+            return;
+        }
+        float incoming_cosine = 1.0F, tangent_scale = 0.0F;
+        if (incident_sine > 0.0F) {
+            float transmitted_sine;
+            if (f.incident_eta > f.transmitted_eta) {
+                const float critical = f.transmitted_eta / f.incident_eta;
+                if (critical == 0.0F || incident_sine >= critical) {
+                    lane.fail();
+                    return;
+                }
+                transmitted_sine = incident_sine / critical;
+            } else {
+                const float ratio = f.incident_eta / f.transmitted_eta;
+                if (ratio == 0.0F) {
+                    lane.fail();
+                    return;
+                }
+                transmitted_sine = ratio * incident_sine;
+            }
+            if (!isfinite(transmitted_sine) || !(transmitted_sine < 1.0F)) {
+                lane.fail();
+                return;
+            }
+            incoming_cosine = sqrtf((1.0F - transmitted_sine) * (1.0F + transmitted_sine));
+            tangent_scale = transmitted_sine / incident_sine;
+            if (!isfinite(incoming_cosine) || !(incoming_cosine > 0.0F) || !isfinite(tangent_scale) ||
+                !(tangent_scale > 0.0F)) {
+                lane.fail();
+                return;
+            }
+        }
+        inf = F3{fmaf(-tangent_scale, tangent.x, -incoming_cosine * m.x),
+                 fmaf(-tangent_scale, tangent.y, -incoming_cosine * m.y),
+                 fmaf(-tangent_scale, tangent.z, -incoming_cosine * m.z)};
+        lobes = kLobeGlossy | kLobeTransmission;
+        if (!unit_length(inf)) {
+            lane.fail();
+            return;
+        }
+        if (!(inf.z < 0.0F)) {
+            return;
+        }
+        const float num[2] = {f.nte, f.nte};
+        const float den[2] = {f.nie, f.nie};
+        eta_scale = checked_product_ratio(num, den, lane);
+    }
+    s.wi = scaled_dir(inf, f.face_sign);
+    dielectric_eval(c, wo, s.wi, s.value, lane);
+    s.pdf = dielectric_pdf(c, wo, s.wi, lane);
+    s.lobes = lobes;
+    s.eta_scale = eta_scale;
+    s.valid = true;
+}
+
+// DepthFilteredClosureMixture.hpp:460-552 for a single active closure.
+static __device__ void closure_sample(const ClosureData& c, uint32_t allowed, F3 wo, float component, float u, float v,
+                               BsdfSample& s, Lane& lane) {
+    s.valid = false;
+    s.eta_scale = 1.0F;
+    s.lobes = c.lobes;
+    if (!unit_length(wo)) {
+        lane.fail();
+        return;
+    }
+    if (c.kind == kClosureLambert) {  // LambertianReflection.hpp:108-140
+        const F3 wi = map_cosine_hemisphere(u, v);
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return;
+        }
+        s.wi = wi;
+        closure_eval(c, allowed, wo, wi, s.value, lane);
+        s.pdf = closure_pdf(c, allowed, wo, wi, lane);
+        s.valid = true;
+        return;
+    }
+    if (c.kind == kClosureConductor) {  // RoughConductorReflection.hpp:240-288
+        F3 m;
+        if (!ggx_sample_vndf(c.p[8], c.p[9], wo, u, v, m, lane)) {
+            return;
+        }
+        const float hc = dot(wo, m);
+        if (!isfinite(hc) || !(hc > 0.0F) || hc > 1.0F) {
+            lane.fail();
+            return;
+        }
+        const F3 wi{2.0F * hc * m.x - wo.x, 2.0F * hc * m.y - wo.y, 2.0F * hc * m.z - wo.z};
+        if (!unit_length(wi)) {
+            lane.fail();
+            return;
+        }
+        if (!(wi.z > 0.0F)) {
+            return;
+        }
+        s.wi = wi;
+        conductor_eval(c, wo, wi, s.value, lane);
+        s.pdf = conductor_pdf(c, wo, wi, lane);
+        s.valid = true;
+        return;
+    }
+    // rough dielectric with a depth-restricted direction (DepthFilteredClosureMixture.hpp:135-180)
+    float event = component;
+    if (allowed == kLobeReflection) {
+        event = 0.0F;
+    } else if (allowed == kLobeTransmission) {
+        event = nextafterf(1.0F, 0.0F);
+    }
+    dielectric_sample(c, wo, event, u, v, s, lane);
+    if (!s.valid) {
+        return;
+    }
+    if ((s.lobes & allowed) == 0U) {
+        s.valid = false;
+        return;
+    }
+    s.pdf = dielectric_pdf_masked(c, allowed, wo, s.wi, lane);
+}
+
+}  // namespace bf200

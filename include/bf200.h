@@ -317,7 +317,8 @@ typedef struct bf200_transport_options_v1 {
     uint32_t roulette_first_eligible_depth;
     float roulette_minimum_survival;
     float roulette_maximum_survival;
-    uint32_t reserved[5];
+    uint32_t instrumentation; /* 1: time every stage with CUDA events (CudaWavefrontInstrumentationMode::nsight) */
+    uint32_t reserved[4];
 } bf200_transport_options_v1;
 
 /* Pinhole camera (PinholeCamera.hpp:52-306) with the host-side constants already derived:
@@ -387,7 +388,13 @@ typedef struct bf200_report_v1 {
     uint32_t first_failure_path;
     uint64_t kernel_launches;
     double gpu_milliseconds;
-    uint64_t reserved[4];
+    /* with instrumentation: summed GPU time of each stage kernel, and the iteration count */
+    double intersect_milliseconds;
+    double shade_milliseconds;
+    double occlude_milliseconds;
+    double film_milliseconds;
+    uint64_t iterations;
+    uint64_t reserved[3];
 } bf200_report_v1;
 
 typedef struct bf200_context bf200_context;
@@ -499,6 +506,14 @@ typedef struct bf200_render_api_v1 {
                                     uint64_t, uint32_t*) BF200_NOEXCEPT;
     uint64_t reserved_slots[4];
 } bf200_render_api_v1;
+
+/* Derives a pinhole camera the way PinholeCamera::create does (PinholeCamera.hpp:60-99): the
+ * orientation frame is OrthonormalFrame::from_normal_and_tangent(normal, tangent_seed)
+ * (LocalFrame.hpp:82-89), half_height = tan(vertical_fov / 2), half_width = half_height * W/H. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_camera_create(
+    const float origin[3], const float normal[3], const float tangent_seed[3], uint32_t width,
+    uint32_t height, float vertical_fov_radians, float time, uint32_t jitter_mode,
+    bf200_camera_v1* out_camera) BF200_NOEXCEPT;
 
 /* Library version and build description (sm_100a arch string). */
 BF200_EXTERN_C BF200_EXPORT const char* bf200_build_info(void) BF200_NOEXCEPT;

@@ -2560,6 +2560,48 @@ __attribute__((visibility("default"))) int bfo_closest_hits(void* h, const bf200
     return 0;
 }
 
+// PinholeCamera::generate_primary_ray with uniform pixel jitter (PinholeCamera.hpp:144-283,
+// PixelJitter.hpp:47-64) for a camera whose frame and half extents are given.
+__attribute__((visibility("default"))) int bfo_camera_rays(const bf200_camera_v1* cam,
+                                                           const bf200_sample_index_v1* samples, uint64_t n,
+                                                           bf200_ray_v1* rays) {
+    try {
+        for (uint64_t i = 0; i < n; ++i) {
+            const Stream stream{samples[i].pixel_x, samples[i].pixel_y, samples[i].sample_index, samples[i].seed};
+            float ox = 0.5F, oy = 0.5F;
+            if (cam->jitter_mode != 0) {
+                ox = stream.sample_1d(0xA24BAED4963EE407ULL);
+                oy = stream.sample_1d(0x9FB21C651E98DF25ULL);
+            }
+            const float rw = static_cast<float>(cam->width), rh = static_cast<float>(cam->height);
+            const float tpx = 2.0F * static_cast<float>(samples[i].pixel_x);
+            const float tpy = 2.0F * static_cast<float>(samples[i].pixel_y);
+            const float nx = (tpx + 2.0F * ox) / rw - 1.0F;
+            const float ny = 1.0F - (tpy + 2.0F * oy) / rh;
+            const V3 local = robust_unit(V3{nx * cam->half_width, ny * cam->half_height, -1.0F});
+            const Frame frame{V3{cam->tangent[0], cam->tangent[1], cam->tangent[2]},
+                              V3{cam->bitangent[0], cam->bitangent[1], cam->bitangent[2]},
+                              V3{cam->normal[0], cam->normal[1], cam->normal[2]}};
+            const V3 d = robust_unit(frame.to_world(local));
+            std::memset(&rays[i], 0, sizeof(rays[i]));
+            for (int a = 0; a < 3; ++a) {
+                rays[i].origin[a] = cam->origin[a];
+            }
+            rays[i].direction[0] = d.x;
+            rays[i].direction[1] = d.y;
+            rays[i].direction[2] = d.z;
+            rays[i].t_min = cam->t_min;
+            rays[i].t_max = cam->t_max;
+            rays[i].time = cam->time;
+            rays[i].mask = cam->mask;
+        }
+        return 0;
+    } catch (const Failure& f) {
+        set_error(f.message);
+        return 1;
+    }
+}
+
 // Float32 or Neumaier float64 film of the caller-side path: CIE XYZ (Cie1931Sensor.cpp:104-176),
 // linear sRGB (Color.hpp:77-88), add_sample(x, y, rgb, 1) (Film.hpp:150-182). `sums` holds
 // (r, g, b, weight) per pixel as double; for precision 1 also the compensations are applied.

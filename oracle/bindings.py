@@ -1,0 +1,180 @@
+"""ctypes bindings of the CPU checkers (test infrastructure only).
+
+* Oracle: oracle/liboracle.so, this repository's restatement of the reference scalar path tracer
+  (oracle/bfo_oracle.cpp).
+* Reference: oracle/_ref/libbfref.so, the reference's own sources compiled by oracle/Makefile
+  with a thin harness (oracle/ref_harness.cpp). Present only where it was built.
+
+Only tests, __graft_entry__.smoke() and bench.py's CPU arms use these, as checkers; the product
+never loads them.
+"""
+import ctypes as C
+import os
+import sys
+
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(ORACLE_DIR)
+sys.path.insert(0, os.path.join(REPO, "blackframe-renderer_b200"))
+
+from bf200 import abi  # noqa: E402
+
+ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
+REFERENCE_LIB = os.path.join(ORACLE_DIR, "_ref", "libbfref.so")
+
+
+class CheckerError(RuntimeError):
+    pass
+
+
+class _Checker:
+    prefix = ""
+
+    def __init__(self, path):
+        if not os.path.exists(path):
+            raise CheckerError(f"{path} is not built")
+        self.lib = C.CDLL(path)
+        p = self.prefix
+        self.lib[p + "_last_error"].restype = C.c_char_p
+        f = self.lib[p + "_scene_create"]
+        f.argtypes = [C.POINTER(abi.SceneDesc), C.POINTER(C.c_void_p)]
+        f.restype = C.c_int
+        self.lib[p + "_scene_destroy"].argtypes = [C.c_void_p]
+        f = self.lib[p + "_trace_paths"]
+        f.argtypes = [C.c_void_p, C.POINTER(abi.PathInput), C.c_uint64, C.POINTER(abi.TransportOptions),
+                      C.POINTER(abi.PathResult), C.c_int]
+        f.restype = C.c_int64
+
+    def last_error(self):
+        return self.lib[self.prefix + "_last_error"]().decode()
+
+    def scene(self, builder):
+        desc = builder.desc()
+        handle = C.c_void_p()
+        rc = self.lib[self.prefix + "_scene_create"](C.byref(desc), C.byref(handle))
+        if rc != 0:
+            raise CheckerError(f"scene creation failed ({rc}): {self.last_error()}")
+        return handle
+
+    def destroy(self, handle):
+        self.lib[self.prefix + "_scene_destroy"](handle)
+
+    def trace(self, handle, inputs, options, threads=None):
+        n = len(inputs)
+        results = (abi.PathResult * n)()
+        threads = threads or os.cpu_count() or 1
+        failures = self.lib[self.prefix + "_trace_paths"](handle, inputs, n, C.byref(options), results, threads)
+        if failures < 0:
+            raise CheckerError(self.last_error())
+        return results, failures
+
+
+class Oracle(_Checker):
+    prefix = "bfo"
+
+    def __init__(self):
+        super().__init__(ORACLE_LIB)
+        f = self.lib.bfo_film_accumulate
+        f.argtypes = [C.c_void_p, C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(abi.Sensor), C.c_uint32,
+                      C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+        f.restype = C.c_int
+        self.lib.bfo_closest_hits.argtypes = [C.c_void_p, C.POINTER(abi.Ray), C.c_uint64, C.POINTER(abi.Hit)]
+        self.lib.bfo_scene_world_normal.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]
+        self.lib.bfo_scene_set_prefilter.argtypes = [C.c_void_p, C.c_int]
+        self.lib.bfo_camera_rays.argtypes = [C.POINTER(abi.Camera), C.POINTER(abi.SampleIndex), C.c_uint64,
+                                             C.POINTER(abi.Ray)]
+        self.lib.bfo_camera_rays.restype = C.c_int
+
+    def camera_rays(self, camera, samples):
+        rays = (abi.Ray * len(samples))()
+        if self.lib.bfo_camera_rays(C.byref(camera), samples, len(samples), rays) != 0:
+            raise CheckerError(self.last_error())
+        return rays
+
+    def closest_hits(self, handle, rays):
+        hits = (abi.Hit * len(rays))()
+        self.lib.bfo_closest_hits(handle, rays, len(rays), hits)
+        return hits
+
+    def film(self, radiance, samples, sensor, width, height, precision):
+        import numpy as np
+        n = len(samples)
+        sums = np.zeros((height, width, 4), np.float64)
+        counts = np.zeros((height, width), np.uint64)
+        rad = np.ascontiguousarray(radiance, np.float32)
+        rc = self.lib.bfo_film_accumulate(rad.ctypes.data_as(C.c_void_p), samples, n, C.byref(sensor), width,
+                                          height, precision, sums.ctypes.data_as(C.c_void_p),
+                                          counts.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise CheckerError("film accumulation failed")
+        return sums, counts
+
+
+class Reference(_Checker):
+    prefix = "bfr"
+
+    def __init__(self):
+        super().__init__(REFERENCE_LIB)
+        f = self.lib.bfr_camera_rays
+        f.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_uint32, C.c_uint32, C.c_float, C.c_float,
+                                                  C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(abi.Ray)]
+        f.restype = C.c_int
+        f = self.lib.bfr_camera
+        f.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float,
+                                                  C.c_float, C.c_uint32, C.POINTER(abi.Camera)]
+        f.restype = C.c_int
+        self.lib.bfr_sensor.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(abi.Sensor)]
+        self.lib.bfr_scene_world_to_object.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_float)]
+        f = self.lib.bfr_film_accumulate
+        f.argtypes = [C.c_void_p, C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(C.c_float),
+                      C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+        f.restype = C.c_int
+
+    @staticmethod
+    def _f3(values):
+        return (C.c_float * 3)(*[float(v) for v in values])
+
+    def camera_rays(self, origin, normal, tangent, width, height, vfov, time, samples):
+        rays = (abi.Ray * len(samples))()
+        rc = self.lib.bfr_camera_rays(self._f3(origin), self._f3(normal), self._f3(tangent), width, height, vfov,
+                                      time, samples, len(samples), rays)
+        if rc != 0:
+            raise CheckerError(self.last_error())
+        return rays
+
+    def camera(self, origin, normal, tangent, width, height, vfov, time):
+        cam = abi.Camera()
+        rc = self.lib.bfr_camera(self._f3(origin), self._f3(normal), self._f3(tangent), width, height, vfov, 0.0,
+                                 float("inf"), time, 0xFFFFFFFF, C.byref(cam))
+        if rc != 0:
+            raise CheckerError(self.last_error())
+        return cam
+
+    def sensor(self, nanometers, pdfs):
+        out = abi.Sensor()
+        nm = (C.c_float * 4)(*[float(v) for v in nanometers])
+        pdf = (C.c_float * 4)(*[float(v) for v in pdfs])
+        self.lib.bfr_sensor(nm, pdf, C.byref(out))
+        return out
+
+    def world_to_object(self, handle, index):
+        out = (C.c_float * 16)()
+        self.lib.bfr_scene_world_to_object(handle, index, out)
+        return list(out)
+
+    def film(self, radiance, samples, nanometers, pdfs, width, height, precision):
+        import numpy as np
+        sums = np.zeros((height, width, 4), np.float64)
+        counts = np.zeros((height, width), np.uint64)
+        rad = np.ascontiguousarray(radiance, np.float32)
+        nm = (C.c_float * 4)(*[float(v) for v in nanometers])
+        pdf = (C.c_float * 4)(*[float(v) for v in pdfs])
+        rc = self.lib.bfr_film_accumulate(rad.ctypes.data_as(C.c_void_p), samples, len(samples), nm, pdf, width,
+                                          height, precision, sums.ctypes.data_as(C.c_void_p),
+                                          counts.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise CheckerError(self.last_error())
+        return sums, counts
+
+
+def reference_available():
+    return os.path.exists(REFERENCE_LIB)

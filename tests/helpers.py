@@ -1,0 +1,55 @@
+"""Shared helpers of the test suite: golden inputs as C records, result comparison."""
+import numpy as np
+
+from bf200 import abi, scenes
+
+
+def golden_inputs(g):
+    n = len(g["pixel_x"])
+    inputs = (abi.PathInput * n)()
+    for k in range(n):
+        r = inputs[k].primary_ray
+        for a in range(3):
+            r.origin[a] = float(g["ray_origin"][k, a])
+            r.direction[a] = float(g["ray_direction"][k, a])
+        r.t_min, r.t_max, r.time = 0.0, float("inf"), scenes.PATH_TIME
+        r.mask, r.medium = 0xFFFFFFFF, 0
+        inputs[k].sample.pixel_x = int(g["pixel_x"][k])
+        inputs[k].sample.pixel_y = int(g["pixel_y"][k])
+        inputs[k].sample.sample_index = int(g["sample_index"][k])
+        inputs[k].sample.seed = 0
+    return inputs
+
+
+def arrays(results):
+    n = len(results)
+    return {
+        "radiance": np.array([list(r.radiance) for r in results], np.float32).reshape(n, 4),
+        "beta": np.array([list(r.beta) for r in results], np.float32).reshape(n, 4),
+        "depth": np.array([r.depth for r in results], np.uint32),
+        "termination": np.array([r.termination for r in results], np.uint32),
+        "lane_status": np.array([r.lane_status for r in results], np.uint32),
+        "eta": np.array([r.eta_scale for r in results], np.float32),
+    }
+
+
+def bit_equal(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return a.view(np.uint32) == b.view(np.uint32)
+
+
+def relative_error(a, b, floor=1e-6):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), floor)
+
+
+def sensor_from_golden(g):
+    s = abi.Sensor()
+    for lane in range(4):
+        for k in range(3):
+            s.response_xyz[lane][k] = float(g["sensor_response"][lane, k])
+        s.wavelength_pdf[lane] = float(g["sensor_pdf"][lane])
+    s.normalization = float(g["sensor_normalization"])
+    return s

@@ -1,0 +1,185 @@
+"""Parity of the sm_100a backend with the oracle and the reference's golden outputs.
+
+Tolerances: per-path spectral radiance is compared bit for bit, and within 1e-5 relative
+(absolute floor 1e-6); a path may differ when a sine or cosine of a sampled angle rounds
+differently on the device (the device uses the correctly rounded value, glibc's sinf/cosf are
+within 0.56 ulp), so at most 1 % of paths may exceed the tolerance. Hit identifiers, parameters
+and barycentrics must be bit-exact.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from bf200 import abi, runtime, scenes
+from helpers import arrays, bit_equal, golden_inputs, relative_error, sensor_from_golden
+from oracle.bindings import Oracle
+
+pytestmark = pytest.mark.gpu
+WORKLOADS = ["cornell_plain_64", "cornell_spheres_256"]
+RELATIVE_TOLERANCE = 1e-5
+DIVERGED_FRACTION = 0.01
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    with runtime.Context(0, path_capacity=1 << 18) as c:
+        yield c
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    return Oracle()
+
+
+def check_paths(got, expected, label):
+    same = bit_equal(got["radiance"], expected["radiance"]).all(axis=1)
+    close = (relative_error(got["radiance"], expected["radiance"]) <= RELATIVE_TOLERANCE).all(axis=1)
+    term = got["termination"] == expected["termination"]
+    n = len(same)
+    assert (got["lane_status"] == 0).all(), f"{label}: failed lanes {np.nonzero(got['lane_status'])[0][:10]}"
+    assert close.mean() >= 1.0 - DIVERGED_FRACTION, f"{label}: only {close.sum()}/{n} within tolerance"
+    assert term.mean() >= 1.0 - DIVERGED_FRACTION, f"{label}: terminations differ on {n - term.sum()}/{n}"
+    return same.mean(), close.mean()
+
+
+@pytest.mark.parametrize("name", WORKLOADS)
+def test_trace_paths_matches_reference_golden(ctx, golden, name):
+    g = golden(name)
+    builder, options, _ = scenes.build_workload(name)
+    scene = ctx.create_scene(builder)
+    results, report = ctx.trace_paths(scene, golden_inputs(g), options)
+    scene.close()
+    exact, close = check_paths(arrays(results), g, name)
+    assert exact >= 0.95, f"{name}: bit-exact fraction {exact}"
+    assert report.path_count == len(g["pixel_x"]) and report.failed_lanes == 0
+
+
+@pytest.mark.parametrize("name", WORKLOADS)
+def test_trace_paths_matches_oracle_on_fresh_seeds(ctx, oracle, name):
+    builder, options, (width, height, spp) = scenes.build_workload(name)
+    rng = np.random.default_rng(2024)
+    n = 4096 if name == "cornell_plain_64" else 1024
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+    samples = (abi.SampleIndex * n)()
+    for k in range(n):
+        samples[k].pixel_x, samples[k].pixel_y = int(rng.integers(width)), int(rng.integers(height))
+        samples[k].sample_index, samples[k].seed = int(rng.integers(1 << 40)), 0x243F6A8885A308D3
+    rays = oracle.camera_rays(cam, samples)
+    inputs = (abi.PathInput * n)()
+    for k in range(n):
+        inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
+    handle = oracle.scene(builder)
+    expected, failures = oracle.trace(handle, inputs, options)
+    oracle.destroy(handle)
+    assert failures == 0
+    scene = ctx.create_scene(builder)
+    got, _ = ctx.trace_paths(scene, inputs, options)
+    scene.close()
+    check_paths(arrays(got), arrays(expected), name)
+
+
+@pytest.mark.parametrize("name", WORKLOADS)
+def test_closest_hits_bit_exact(ctx, oracle, name):
+    builder, _, _ = scenes.build_workload(name)
+    rng = np.random.default_rng(11)
+    n = 20000
+    origins = rng.uniform(-0.99, 0.99, (n, 3)).astype(np.float32)
+    origins[:, 2] = rng.uniform(0.01, 3.5, n).astype(np.float32)
+    directions = rng.normal(size=(n, 3)).astype(np.float32)
+    directions /= np.linalg.norm(directions, axis=1, keepdims=True)
+    rays = (abi.Ray * n)()
+    for k in range(n):
+        for a in range(3):
+            rays[k].origin[a], rays[k].direction[a] = float(origins[k, a]), float(directions[k, a])
+        rays[k].t_min, rays[k].t_max, rays[k].time, rays[k].mask = 0.0, float("inf"), 0.5, 0xFFFFFFFF
+    handle = oracle.scene(builder)
+    expected = oracle.closest_hits(handle, rays)
+    oracle.destroy(handle)
+    scene = ctx.create_scene(builder)
+    got = ctx.closest_hits(scene, rays)
+    scene.close()
+    e_ids = np.array([(h.instance_index, h.primitive_index) for h in expected], np.uint32)
+    g_ids = np.array([(h.instance_index, h.primitive_index) for h in got], np.uint32)
+    assert (np.array([h.status for h in got]) == 0).all()
+    assert (e_ids == g_ids).all(), f"{(e_ids != g_ids).any(axis=1).sum()} hit-ID mismatches"
+    e_t = np.array([[h.t] + list(h.barycentrics) for h in expected], np.float32)
+    g_t = np.array([[h.t] + list(h.barycentrics) for h in got], np.float32)
+    assert bit_equal(e_t, g_t).all()
+
+
+@pytest.mark.parametrize("name", WORKLOADS)
+@pytest.mark.parametrize("precision", [0, 1])
+def test_render_film_matches_reference_film(ctx, golden, name, precision):
+    g = golden(name)
+    builder, options, _ = scenes.build_workload(name)
+    fw, fh, fspp = (int(v) for v in g["film_size"])
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), fw, fh, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+    scene = ctx.create_scene(builder)
+    sums, counts, report = ctx.render_film(scene, cam, sensor_from_golden(g), options, fspp, seed=0,
+                                           precision=precision)
+    scene.close()
+    expected = g["film32"] if precision == 0 else g["film64"]
+    got = sums[..., :4].astype(np.float64) if precision == 0 else sums[..., :4] + sums[..., 4:]
+    assert (counts == fspp).all()
+    assert report.failed_lanes == 0
+    err = relative_error(got, expected)
+    assert (err <= RELATIVE_TOLERANCE).mean() >= 1.0 - DIVERGED_FRACTION
+    rmse = np.sqrt(np.mean((got[..., :3] - expected[..., :3]) ** 2))
+    assert rmse <= 1e-2 * max(1e-6, np.sqrt(np.mean(expected[..., :3] ** 2)))
+
+
+def test_full_plain_frame_film_matches_oracle(ctx, oracle):
+    """The plain Cornell workload at its full size (64 x 64 x 16 spp = 65,536 paths)."""
+    builder, options, (width, height, spp) = scenes.build_workload("cornell_plain_64")
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+    scene = ctx.create_scene(builder)
+    sensor = runtime_sensor = None
+    from helpers import sensor_from_golden as sfg
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "cornell_plain_64.npz"))
+    sensor = sfg(g)
+    sums, counts, report = ctx.render_film(scene, cam, sensor, options, spp, seed=0)
+    scene.close()
+    px, py, s = np.meshgrid(np.arange(width), np.arange(height), np.arange(spp), indexing="ij")
+    order = np.lexsort((px.ravel(), py.ravel(), s.ravel()))
+    px, py, s = px.ravel()[order], py.ravel()[order], s.ravel()[order]
+    samples = (abi.SampleIndex * len(px))()
+    for k in range(len(px)):
+        samples[k].pixel_x, samples[k].pixel_y, samples[k].sample_index = int(px[k]), int(py[k]), int(s[k])
+    rays = oracle.camera_rays(cam, samples)
+    inputs = (abi.PathInput * len(px))()
+    for k in range(len(px)):
+        inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
+    handle = oracle.scene(builder)
+    results, failures = oracle.trace(handle, inputs, options)
+    oracle.destroy(handle)
+    expected, _ = oracle.film(arrays(results)["radiance"], samples, sensor, width, height, 0)
+    assert (counts == spp).all() and report.path_count == width * height * spp
+    err = relative_error(sums.astype(np.float64), expected)
+    assert (err <= RELATIVE_TOLERANCE).mean() >= 1.0 - DIVERGED_FRACTION
+
+
+def test_unsupported_features_are_rejected(ctx):
+    builder = scenes.cornell_box(scenes.SceneBuilder(), with_spheres=False)
+    closures = scenes.lambertian([0.5] * 4) + scenes.lambertian([0.2] * 4)
+    builder.add_material(closures)
+    with pytest.raises(runtime.Bf200Error) as info:
+        ctx.create_scene(builder)
+    assert info.value.status == 4  # INVALID_STATE: no substitution
+
+
+def test_scene_without_emitters_is_rejected(ctx):
+    builder = scenes.SceneBuilder()
+    white = builder.add_material(scenes.lambertian([0.5] * 4))
+    builder.add_instance(builder.add_mesh(scenes.unit_box()), white)
+    with pytest.raises(runtime.Bf200Error):
+        ctx.create_scene(builder)
+
+
+def test_empty_batch_and_reuse(ctx):
+    builder, options, _ = scenes.build_workload("cornell_plain_64")
+    scene = ctx.create_scene(builder)
+    results, report = ctx.trace_paths(scene, (abi.PathInput * 0)(), options)
+    assert len(results) == 0 and report.path_count == 0
+    scene.close()
