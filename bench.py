@@ -180,6 +180,7 @@ def main():
     parser.add_argument("--capacity", type=int, default=1 << 21)
     parser.add_argument("--reference-seconds", type=float, default=8.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's 256)")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -201,6 +202,8 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
 
     builder, options, camera, sensor, (width, height, spp) = workload_setup()
+    if args.spp > 0:
+        spp = args.spp
     options.instrumentation = 1
     pixels = width * height
     paths_per_step = pixels * spp

@@ -577,10 +577,10 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
     for (auto& x : ev) {
         cudaEventCreate(&x);
     }
-    cudaEventRecord(ev[0], st);
-    const cudaEvent_t start = ev[0];
-    cudaEvent_t stop;
+    cudaEvent_t start, stop;
+    cudaEventCreate(&start);
     cudaEventCreate(&stop);
+    cudaEventRecord(start, st);
     uint64_t iterations = 0, launches = 0, shadow_segments = 0;
     double stage_ms[3] = {0.0, 0.0, 0.0};
     // every path finishes within (sum of surface depth limits + 1) extension segments, and a
@@ -649,6 +649,7 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
     for (auto& x : ev) {
         cudaEventDestroy(x);
     }
+    cudaEventDestroy(start);
     cudaEventDestroy(stop);
     if (report != nullptr) {
         report->struct_size = sizeof(bf200_report_v1);
