@@ -41,6 +41,11 @@ SHADOW_SEGMENT_BYTES = 96
 FILM_SAMPLE_BYTES = 24
 # per-launch algorithmic bytes of the traversal kernel: camera ray write, ray read + hit write
 INTERSECT_SEGMENT_BYTES = 48
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per processed segment, from one ncu
+# capture of a full-wavefront launch (2,097,152 segments) of each stage kernel of this build;
+# profiles/stages_cornell_spheres_256_spp64.md holds the capture and its command
+MEASURED_TRAFFIC_PER_SEGMENT = {"k_intersect": 479.3, "k_shade": 229.4, "k_occlude": None}
+TRAFFIC_SOURCE = "profiles/stages_cornell_spheres_256_spp64.md"
 
 
 def measured_peaks():
@@ -300,6 +305,9 @@ def main():
         bytes_total = SHADOW_SEGMENT_BYTES * shadow
     bytes_per_launch = bytes_total / max(1, iterations)
     achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
+    units_per_launch = (shadow if dominant == "k_occlude" else ext) / max(1, iterations)
+    traffic_per_unit = MEASURED_TRAFFIC_PER_SEGMENT.get(dominant)
+    traffic = traffic_per_unit * units_per_launch if traffic_per_unit is not None else None
     whole_bytes = (CAMERA_RAY_BYTES * paths_per_step * args.steps + EXTENSION_SEGMENT_BYTES * ext +
                    SHADOW_SEGMENT_BYTES * shadow + FILM_SAMPLE_BYTES * paths_per_step * args.steps)
 
@@ -319,7 +327,8 @@ def main():
                 "d2h_bytes_per_step": h2d},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                     "frac": achieved / peak, "traffic": traffic, "traffic_source": TRAFFIC_SOURCE,
+                     "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind,
                      "whole_path_algorithmic_gbs": whole_bytes / (total_ms / 1000.0) / 1e9},
     }
     scene.close()
