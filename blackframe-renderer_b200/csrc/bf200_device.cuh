@@ -40,6 +40,7 @@ struct SceneView {
     const float4* inst_to_object;  // 3 rows (m0..m3) per instance
     const float4* inst_to_world;   // 3 rows per instance
     const uint4* inst_info;        // geometry, material, visibility mask, light index or ~0
+    const uint8_t* inst_route;     // shading route of a hit on the instance (kRoute*)
     const uint32_t* inst_normal_offset;
     const uint4* geom_info;        // vertex offset, triangle offset, bvh root node, -
     const float* positions;        // object space, 3 per vertex
@@ -69,6 +70,16 @@ struct TransportParams {
     float roulette_min;
     float roulette_max;
 };
+
+// Shading routes. A hit is shaded by the kernel specialised for its material's single closure
+// kind; misses and every other material take the generic kernel.
+constexpr uint32_t kRouteGeneric = 0U, kRouteLambert = 1U, kRouteConductor = 2U, kRouteDielectric = 3U;
+constexpr uint32_t kRouteCount = 4U;
+constexpr uint8_t kRouteNone = 0xFFU;  // slot not shaded this iteration / no shadow ray
+
+// Stable compaction tiles: one 256-thread block per 4096 consecutive slots.
+constexpr uint32_t kCompactTile = 4096U;
+constexpr uint32_t kCompactMaxRoutes = 4U;
 
 // Slot states of the persistent wavefront.
 constexpr uint8_t kSlotEmpty = 0, kSlotActive = 1, kSlotDone = 2;
@@ -109,11 +120,18 @@ struct Wavefront {
     uint32_t* mask;     // ray visibility mask of the path
     float4* hit_tb;     // t, b0, b1, b2
     uint2* hit_id;      // instance, primitive (instance = ~0 on a miss)
-    // shadow queue (compacted)
-    uint32_t* shadow_slot;
+    // routing: shading route per slot, and the slots of every route in slot order
+    uint8_t* route;
+    uint32_t* route_queue;
+    uint32_t* route_offsets;  // kRouteCount + 1 queue boundaries
+    // shadow rays, stored at their slot; shadow_key 0 marks a slot with a shadow ray
+    uint8_t* shadow_key;
     float4* shadow_o;   // origin, t_max
-    float4* shadow_d;   // direction, mask bits
+    float4* shadow_d;   // direction
     float4* shadow_c;   // contribution (unoccluded)
+    uint32_t* shadow_queue;    // slots with a shadow ray, in slot order
+    uint32_t* shadow_offsets;  // 2 queue boundaries
+    uint32_t* tile_counts;     // compaction scratch: kCompactMaxRoutes x tiles
     // counters: [0] shadow queue size, [1] next path to claim, [2] active slots,
     //           [3] extension segments, [4] shadow segments, [5] failed lanes,
     //           [6] first failure path (min), [7] first failure code

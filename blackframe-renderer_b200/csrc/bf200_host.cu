@@ -469,26 +469,20 @@ blackframe_status validate_desc(bf200_context* c, const bf200_scene_desc_v1* d) 
     return BLACKFRAME_STATUS_SUCCESS;
 }
 
-blackframe_status ensure_capacity(bf200_context* c) {
-    if (c->arena != nullptr) {
-        return BLACKFRAME_STATUS_SUCCESS;
-    }
-    const uint64_t n = c->capacity;
-    const size_t bytes_per_slot = 1 + 8 + 16 * 4 + 4 + 4 + 16 + 4 + 4 + 8 + 4 + 16 + 8 + 4 + 16 * 3;
-    const size_t total = n * bytes_per_slot + 64 * 16 + 8 * sizeof(unsigned long long) + 4096;
-    cudaError_t e = cudaMalloc(&c->arena, total);
-    if (e != cudaSuccess) {
-        return cuda_fail(c, e, "wavefront allocation");
-    }
-    char* p = static_cast<char*>(c->arena);
+// Carves the wavefront arrays of `capacity` slots out of one arena starting at `base` (16-byte
+// aligned pieces). With base == nullptr only the size is computed. Returns the bytes used.
+size_t carve_wavefront(char* base, uint32_t capacity, Wavefront* out) {
+    const size_t n = capacity;
+    const size_t tiles = (n + kCompactTile - 1) / kCompactTile;
+    size_t offset = 0;
     auto take = [&](size_t size) {
-        p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
-        char* r = p;
-        p += size;
+        offset = (offset + 255) & ~size_t(255);
+        char* r = base == nullptr ? nullptr : base + offset;
+        offset += size;
         return r;
     };
-    Wavefront& w = c->w;
-    w.capacity = static_cast<uint32_t>(n);
+    Wavefront w{};
+    w.capacity = capacity;
     w.ray_o = reinterpret_cast<float4*>(take(16 * n));
     w.ray_d = reinterpret_cast<float4*>(take(16 * n));
     w.beta = reinterpret_cast<float4*>(take(16 * n));
@@ -506,12 +500,32 @@ blackframe_status ensure_capacity(bf200_context* c) {
     w.flags = reinterpret_cast<uint32_t*>(take(4 * n));
     w.status = reinterpret_cast<uint32_t*>(take(4 * n));
     w.mask = reinterpret_cast<uint32_t*>(take(4 * n));
-    w.shadow_slot = reinterpret_cast<uint32_t*>(take(4 * n));
+    w.route_queue = reinterpret_cast<uint32_t*>(take(4 * n));
+    w.shadow_queue = reinterpret_cast<uint32_t*>(take(4 * n));
     w.state = reinterpret_cast<uint8_t*>(take(n));
+    w.route = reinterpret_cast<uint8_t*>(take(n));
+    w.shadow_key = reinterpret_cast<uint8_t*>(take(n));
+    w.tile_counts = reinterpret_cast<uint32_t*>(take(4 * kCompactMaxRoutes * (tiles == 0 ? 1 : tiles)));
+    w.route_offsets = reinterpret_cast<uint32_t*>(take(4 * (kRouteCount + 1)));
+    w.shadow_offsets = reinterpret_cast<uint32_t*>(take(4 * 2));
     w.counters = reinterpret_cast<unsigned long long*>(take(8 * sizeof(unsigned long long)));
-    if (static_cast<size_t>(p - static_cast<char*>(c->arena)) > total) {
-        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "wavefront arena layout overflow");
+    if (out != nullptr) {
+        *out = w;
     }
+    return offset;
+}
+
+blackframe_status ensure_capacity(bf200_context* c) {
+    if (c->arena != nullptr) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    const uint32_t n = static_cast<uint32_t>(c->capacity);
+    const size_t total = carve_wavefront(nullptr, n, nullptr);
+    cudaError_t e = cudaMalloc(&c->arena, total);
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "wavefront allocation");
+    }
+    carve_wavefront(static_cast<char*>(c->arena), n, &c->w);
     e = cudaMallocHost(&c->pinned_counters, 8 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         return cuda_fail(c, e, "pinned counters");
@@ -591,16 +605,17 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
         // the shadow queue and the active count are per iteration
         cudaMemsetAsync(w.counters + 0, 0, sizeof(unsigned long long), st);
         cudaMemsetAsync(w.counters + 2, 0, sizeof(unsigned long long), st);
+        uint32_t stage_launches = 0;
         for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage) {
             if (instrument) {
                 cudaEventRecord(ev[stage], st);
             }
-            e = launch_stage(stage, s->view, w, src, p, grid, st);
+            e = launch_stage(stage, s->view, w, src, p, grid, st, &stage_launches);
         }
         if (instrument) {
             cudaEventRecord(ev[3], st);
         }
-        launches += 3;
+        launches += stage_launches;
         ++iterations;
         if (e != cudaSuccess) {
             return cuda_fail(c, e, "wavefront launch");
@@ -631,7 +646,7 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
         return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "the wavefront did not drain within its iteration bound");
     }
     // retire the last finished slots
-    e = launch_retire(s->view, w, src, grid, st);
+    e = launch_retire(w, src, grid, st);
     ++launches;
     if (e == cudaSuccess) {
         e = cudaMemcpyAsync(c->pinned_counters, w.counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -922,6 +937,21 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
             std::memcpy(&rotation_bits, &mat.tangent_rotation_radians, 4);
             material_info[m] = make_uint4(mat.closure_count, mat.frame_mode, rotation_bits, 0);
         }
+        // shading route of a hit on each instance: the kernel specialised for its material's single
+        // closure kind, or the generic one
+        std::vector<uint8_t> inst_route(d->instance_count, static_cast<uint8_t>(kRouteGeneric));
+        for (uint32_t i = 0; i < d->instance_count; ++i) {
+            const uint32_t m = d->instances[i].material_index;
+            if (d->materials[m].closure_count != 1) {
+                continue;
+            }
+            switch (closures[m].kind) {
+                case kClosureLambert: inst_route[i] = static_cast<uint8_t>(kRouteLambert); break;
+                case kClosureConductor: inst_route[i] = static_cast<uint8_t>(kRouteConductor); break;
+                case kClosureDielectric: inst_route[i] = static_cast<uint8_t>(kRouteDielectric); break;
+                default: break;
+            }
+        }
         std::vector<float> positions(d->positions, d->positions + 3ULL * d->vertex_count);
         std::vector<float> normals(d->normals, d->normals + 3ULL * d->vertex_count);
         std::vector<uint32_t> triangles(d->triangles, d->triangles + 3ULL * d->triangle_count);
@@ -937,6 +967,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         up(to_object, v.inst_to_object);
         up(to_world, v.inst_to_world);
         up(inst_info, v.inst_info);
+        up(inst_route, v.inst_route);
         up(normal_offset, v.inst_normal_offset);
         up(geom_info, v.geom_info);
         up(positions, v.positions);

@@ -1,23 +1,34 @@
 // bf200 device kernels: scene setup, exact-robust BVH traversal, the persistent wavefront
-// (intersect -> shade with NEE -> occlusion) and film accumulation.
+// (regenerate -> trace -> route -> shade with NEE -> occlusion) and film accumulation.
 //
 // Hot-path mapping to the reference CUDA backend (Blackframe/XPU/CUDA/Source):
-//   k_intersect : scene_closest_hit_kernel + classify/miss stages (CudaSceneClosestHit.cu:1199,
-//                 CudaWavefrontStages.cu:1434, :3962), plus camera generation and path
-//                 regeneration (seed/camera stages, :1269-1406) fused in.
-//   k_shade     : shade_stage_kernel (CudaWavefrontStages.cu:4107-4727) with the shadow-queue
-//                 compaction (CudaWavefrontQueueCompaction.cu) done by warp ballot/popc and one
-//                 block-level scan.
-//   k_occlude   : scene_occlusion_kernel + process_shadow_kernel (CudaSceneClosestHit.cu:1243,
-//                 CudaWavefrontStages.cu:4772-4908).
-//   k_film      : the caller-side CIE XYZ -> linear RGB -> Film::add_sample loop
-//                 (Tests/Backends/GPU/CUDA/CudaTransportParityTest.cpp:906-927), on the device.
+//   k_regenerate : path retirement and regeneration with device camera rays (seed/camera stages,
+//                  CudaWavefrontStages.cu:1269-1406)
+//   k_trace      : scene_closest_hit_kernel + classify/miss stages (CudaSceneClosestHit.cu:1199,
+//                  CudaWavefrontStages.cu:1434, :3962); writes each slot's shading route
+//   k_shade<K>   : shade_stage_kernel (CudaWavefrontStages.cu:4107-4727), one instantiation per
+//                  closure kind over that route's queue (bf200_compact.cu builds the queues)
+//   k_occlude    : scene_occlusion_kernel + process_shadow_kernel (CudaSceneClosestHit.cu:1243,
+//                  CudaWavefrontStages.cu:4772-4908) over the compacted shadow queue
+//   k_film       : the caller-side CIE XYZ -> linear RGB -> Film::add_sample loop
+//                  (Tests/Backends/GPU/CUDA/CudaTransportParityTest.cpp:906-927), on the device.
 // Arithmetic follows the reference scalar loop (Blackframe/Engine/Source/SceneMisPathLoop.cpp)
 // operation for operation; this file is compiled with -fmad=false.
 #include <cuda_runtime.h>
 
 #include "bf200_device.cuh"
 #include "bf200_kernels.h"
+
+// Resident 256-thread blocks per SM the register allocation must allow, per stage kernel.
+#ifndef BF200_INTERSECT_MIN_BLOCKS
+#define BF200_INTERSECT_MIN_BLOCKS 2
+#endif
+#ifndef BF200_SHADE_MIN_BLOCKS
+#define BF200_SHADE_MIN_BLOCKS 2
+#endif
+#ifndef BF200_OCCLUDE_MIN_BLOCKS
+#define BF200_OCCLUDE_MIN_BLOCKS 2
+#endif
 
 namespace bf200 {
 
@@ -67,9 +78,6 @@ __global__ void k_world_normals(SceneView s, const uint32_t* tri_instance, const
 constexpr double kU = 1.1102230246251565e-16;  // 2^-53
 
 struct Dets {
-    double e[3];
-    double bound[3];
-    double vol, vol_bound;
     double p[3][3];
     double d[3];
 };
@@ -84,8 +92,14 @@ __device__ __forceinline__ double det_terms(const double* a, const double* b, co
 // Exact evaluation of the four determinants as double expansions and an exact decision.
 // Returns kTriHit with t (and barycentrics if requested), kTriMiss, or kTriFailure when a
 // coordinate difference is not exact in double (exponent gap above 29 bits).
-__device__ __noinline__ int exact_triangle_slow(const Dets& q, float t_min, float t_max, float approx_t,
-                                                bool want_bary, TriangleHit& hit) {
+__device__ __forceinline__ int slow_triangle_decision(float4 v0, float4 v1, float4 v2, F3 o, F3 d, float t_min,
+                                                      float t_max, float approx_t, bool want_bary, TriangleHit& hit) {
+    Dets q;
+    const double ox = o.x, oy = o.y, oz = o.z;
+    q.p[0][0] = double(v0.x) - ox; q.p[0][1] = double(v0.y) - oy; q.p[0][2] = double(v0.z) - oz;
+    q.p[1][0] = double(v1.x) - ox; q.p[1][1] = double(v1.y) - oy; q.p[1][2] = double(v1.z) - oz;
+    q.p[2][0] = double(v2.x) - ox; q.p[2][1] = double(v2.y) - oy; q.p[2][2] = double(v2.z) - oz;
+    q.d[0] = d.x; q.d[1] = d.y; q.d[2] = d.z;
     Expansion<double, 32> e0, e1, e2, vol;
     if (!exp_det3(e0, q.p[1], q.p[2], q.d) || !exp_det3(e1, q.p[2], q.p[0], q.d) ||
         !exp_det3(e2, q.p[0], q.p[1], q.d) || !exp_det3(vol, q.p[0], q.p[1], q.p[2])) {
@@ -146,6 +160,30 @@ __device__ __noinline__ int exact_triangle_slow(const Dets& q, float t_min, floa
     return kTriHit;
 }
 
+// The out-of-line copy of the exact test. It takes the vertices and the ray by value, rebuilds the
+// differences itself and returns its result by value, so the fast path that calls it keeps
+// everything in registers.
+struct SlowResult {
+    int code;
+    TriangleHit hit;
+};
+
+__device__ __noinline__ SlowResult exact_triangle_slow(float4 v0, float4 v1, float4 v2, F3 o, F3 d, float t_min,
+                                                       float t_max, float approx_t, bool want_bary) {
+    SlowResult r;
+    r.code = slow_triangle_decision(v0, v1, v2, o, d, t_min, t_max, approx_t, want_bary, r.hit);
+    return r;
+}
+
+__device__ __forceinline__ int slow_path(float4 v0, float4 v1, float4 v2, F3 o, F3 d, float t_min, float t_max,
+                                         float approx_t, bool want_bary, TriangleHit& hit) {
+    const SlowResult r = exact_triangle_slow(v0, v1, v2, o, d, t_min, t_max, approx_t, want_bary);
+    if (r.code == kTriHit) {
+        hit = r.hit;
+    }
+    return r.code;
+}
+
 // The float nearest to num/den when a forward error bound proves it; otherwise NaN.
 __device__ __forceinline__ float certain_round(double num, double num_bound, double den, double den_bound) {
     if (!(fabs(num) > 2.0 * num_bound) || !(fabs(den) > 2.0 * den_bound)) {
@@ -167,26 +205,26 @@ __device__ __forceinline__ float certain_round(double num, double num_bound, dou
 // the parameter equal those of the exact test in Triangle.hpp:683-822.
 __device__ __forceinline__ int triangle_test(float4 v0, float4 v1, float4 v2, F3 o, F3 d, float t_min, float t_max,
                                              bool want_bary, TriangleHit& hit) {
-    Dets q;
     const double ox = o.x, oy = o.y, oz = o.z;
-    q.p[0][0] = double(v0.x) - ox; q.p[0][1] = double(v0.y) - oy; q.p[0][2] = double(v0.z) - oz;
-    q.p[1][0] = double(v1.x) - ox; q.p[1][1] = double(v1.y) - oy; q.p[1][2] = double(v1.z) - oz;
-    q.p[2][0] = double(v2.x) - ox; q.p[2][1] = double(v2.y) - oy; q.p[2][2] = double(v2.z) - oz;
-    q.d[0] = d.x; q.d[1] = d.y; q.d[2] = d.z;
+    const double p0[3] = {double(v0.x) - ox, double(v0.y) - oy, double(v0.z) - oz};
+    const double p1[3] = {double(v1.x) - ox, double(v1.y) - oy, double(v1.z) - oz};
+    const double p2[3] = {double(v2.x) - ox, double(v2.y) - oy, double(v2.z) - oz};
+    const double dd[3] = {d.x, d.y, d.z};
     double perm;
-    q.e[0] = det_terms(q.p[1], q.p[2], q.d, perm);
-    q.bound[0] = 16.0 * kU * perm;
-    q.e[1] = det_terms(q.p[2], q.p[0], q.d, perm);
-    q.bound[1] = 16.0 * kU * perm;
-    q.e[2] = det_terms(q.p[0], q.p[1], q.d, perm);
-    q.bound[2] = 16.0 * kU * perm;
+    double e[3], bound[3];
+    e[0] = det_terms(p1, p2, dd, perm);
+    bound[0] = 16.0 * kU * perm;
+    e[1] = det_terms(p2, p0, dd, perm);
+    bound[1] = 16.0 * kU * perm;
+    e[2] = det_terms(p0, p1, dd, perm);
+    bound[2] = 16.0 * kU * perm;
     int pos = 0, neg = 0;
     bool ambiguous = false;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        if (q.e[k] > q.bound[k]) {
+        if (e[k] > bound[k]) {
             ++pos;
-        } else if (q.e[k] < -q.bound[k]) {
+        } else if (e[k] < -bound[k]) {
             ++neg;
         } else {
             ambiguous = true;
@@ -197,40 +235,41 @@ __device__ __forceinline__ int triangle_test(float4 v0, float4 v1, float4 v2, F3
     }
     // A coordinate difference that is not exact in double makes the slow path unusable; such
     // inputs (exponent gaps above 29 bits) are reported as a lane failure.
-    const bool exact_diffs =
-        (q.p[0][0] + ox == double(v0.x)) && (q.p[0][1] + oy == double(v0.y)) && (q.p[0][2] + oz == double(v0.z)) &&
-        (q.p[1][0] + ox == double(v1.x)) && (q.p[1][1] + oy == double(v1.y)) && (q.p[1][2] + oz == double(v1.z)) &&
-        (q.p[2][0] + ox == double(v2.x)) && (q.p[2][1] + oy == double(v2.y)) && (q.p[2][2] + oz == double(v2.z));
+    const auto exact_diffs = [&]() {
+        return (p0[0] + ox == double(v0.x)) && (p0[1] + oy == double(v0.y)) && (p0[2] + oz == double(v0.z)) &&
+               (p1[0] + ox == double(v1.x)) && (p1[1] + oy == double(v1.y)) && (p1[2] + oz == double(v1.z)) &&
+               (p2[0] + ox == double(v2.x)) && (p2[1] + oy == double(v2.y)) && (p2[2] + oz == double(v2.z));
+    };
     if (ambiguous) {
-        if (!exact_diffs) {
+        if (!exact_diffs()) {
             return kTriFailure;
         }
-        return exact_triangle_slow(q, t_min, t_max, __int_as_float(0x7fc00000), want_bary, hit);
+        return slow_path(v0, v1, v2, o, d, t_min, t_max, __int_as_float(0x7fc00000), want_bary, hit);
     }
-    q.vol = det_terms(q.p[0], q.p[1], q.p[2], perm);
-    q.vol_bound = 16.0 * kU * perm;
-    const double det = (q.e[0] + q.e[1]) + q.e[2];
-    const double det_bound = q.bound[0] + q.bound[1] + q.bound[2] + 4.0 * kU * fabs(det);
-    float t = certain_round(q.vol, q.vol_bound, det, det_bound);
+    const double vol = det_terms(p0, p1, p2, perm);
+    const double vol_bound = 16.0 * kU * perm;
+    const double det = (e[0] + e[1]) + e[2];
+    const double det_bound = bound[0] + bound[1] + bound[2] + 4.0 * kU * fabs(det);
+    float t = certain_round(vol, vol_bound, det, det_bound);
     if (isnan(t)) {
-        if (!exact_diffs) {
+        if (!exact_diffs()) {
             return kTriFailure;
         }
-        return exact_triangle_slow(q, t_min, t_max, __double2float_rn(q.vol / det), want_bary, hit);
+        return slow_path(v0, v1, v2, o, d, t_min, t_max, __double2float_rn(vol / det), want_bary, hit);
     }
     if (t < t_min || t > t_max) {
         return kTriMiss;
     }
     hit.t = t;
     if (want_bary) {
-        const float b0 = certain_round(q.e[0], q.bound[0], det, det_bound);
-        const float b1 = certain_round(q.e[1], q.bound[1], det, det_bound);
-        const float b2 = certain_round(q.e[2], q.bound[2], det, det_bound);
+        const float b0 = certain_round(e[0], bound[0], det, det_bound);
+        const float b1 = certain_round(e[1], bound[1], det, det_bound);
+        const float b2 = certain_round(e[2], bound[2], det, det_bound);
         if (isnan(b0) || isnan(b1) || isnan(b2)) {
-            if (!exact_diffs) {
+            if (!exact_diffs()) {
                 return kTriFailure;
             }
-            return exact_triangle_slow(q, t_min, t_max, t, true, hit);
+            return slow_path(v0, v1, v2, o, d, t_min, t_max, t, true, hit);
         }
         hit.b0 = b0;
         hit.b1 = b1;
@@ -298,6 +337,35 @@ __device__ __forceinline__ bool slab(const RayInv& r, float lox, float hix, floa
 // The slack factors only widen positive parameters; a negative lower bound is harmless because
 // t_min >= 0 clamps it, and a negative upper bound means the box is entirely behind the origin.
 
+// Traversal stack of one thread. The first kSharedStackEntries entries live in shared memory in
+// thread-interleaved columns (entry k of thread t at k * blockDim.x + t: every lane of a warp hits
+// its own bank at any depth); deeper entries, which the shallow BVHs of small scenes never reach,
+// go to a local array.
+constexpr int kSharedStackEntries = 32;
+
+struct TraversalStack {
+    int* column;
+    uint32_t stride;
+    int deep[kTraversalStack - kSharedStackEntries];
+    __device__ __forceinline__ void set(int sp, int v) {
+        if (sp < kSharedStackEntries) {
+            column[sp * stride] = v;
+        } else {
+            deep[sp - kSharedStackEntries] = v;
+        }
+    }
+    __device__ __forceinline__ int get(int sp) const {
+        return sp < kSharedStackEntries ? column[sp * stride] : deep[sp - kSharedStackEntries];
+    }
+};
+
+__device__ __forceinline__ TraversalStack thread_stack(int* shared) {
+    TraversalStack st;
+    st.column = shared + threadIdx.x;
+    st.stride = blockDim.x;
+    return st;
+}
+
 struct ClosestResult {
     float t;
     uint32_t instance, primitive;
@@ -317,7 +385,8 @@ __device__ __forceinline__ bool precedes(float t, uint32_t inst, uint32_t prim, 
 
 // Closest hit over every visible instance (committed order) and its BLAS; ties keep the hit
 // that comes first in (instance, primitive) order, as the analytic accel's in-order scan does.
-__device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask) {
+__device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
+                                     TraversalStack& stack) {
     ClosestResult best;
     best.t = t_max;
     best.instance = 0xFFFFFFFFU;
@@ -325,7 +394,6 @@ __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min
     best.leaf = 0xFFFFFFFFU;
     best.failed = false;
     bool found = false;
-    int stack[kTraversalStack];
     for (uint32_t inst = 0; inst < s.instance_count; ++inst) {
         const uint4 info = s.inst_info[inst];
         if ((mask & info.z) == 0U) {
@@ -337,9 +405,9 @@ __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min
         const RayInv r = make_ray_inv(lo, ld);
         const uint4 geom = s.geom_info[info.x];
         int sp = 0;
-        stack[sp++] = static_cast<int>(geom.z);
+        stack.set(sp++, static_cast<int>(geom.z));
         while (sp > 0) {
-            const int node_index = stack[--sp];
+            const int node_index = stack.get(--sp);
             const BvhNode node = s.nodes[node_index];
             const float limit = found ? best.t : t_max;
             float n0, n1;
@@ -364,7 +432,7 @@ __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min
                 const int child = children[k];
                 if (child >= 0) {
                     if (sp < kTraversalStack) {
-                        stack[sp++] = child;
+                        stack.set(sp++, child);
                     } else {
                         best.failed = true;
                     }
@@ -407,8 +475,8 @@ __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min
 }
 
 // Any hit in [t_min, t_max] (AccelBackend.cpp:114-147). Returns 1 occluded, 0 clear, -1 failure.
-__device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask) {
-    int stack[kTraversalStack];
+__device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
+                       TraversalStack& stack) {
     bool failed = false;
     for (uint32_t inst = 0; inst < s.instance_count; ++inst) {
         const uint4 info = s.inst_info[inst];
@@ -421,9 +489,9 @@ __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
         const RayInv r = make_ray_inv(lo, ld);
         const uint4 geom = s.geom_info[info.x];
         int sp = 0;
-        stack[sp++] = static_cast<int>(geom.z);
+        stack.set(sp++, static_cast<int>(geom.z));
         while (sp > 0) {
-            const int node_index = stack[--sp];
+            const int node_index = stack.get(--sp);
             const BvhNode node = s.nodes[node_index];
             float n0, n1;
             const bool h0 = slab(r, node.a.x, node.a.y, node.a.z, node.a.w, node.c.x, node.c.y, t_min, t_max, n0);
@@ -437,7 +505,7 @@ __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
                 const int child = kids[k];
                 if (child >= 0) {
                     if (sp < kTraversalStack) {
-                        stack[sp++] = child;
+                        stack.set(sp++, child);
                     } else {
                         failed = true;
                     }
@@ -625,10 +693,10 @@ __device__ void finish_path(const Wavefront& w, const PathSource& src, uint32_t 
 }
 
 // ------------------------------------------------------------------------------------------------
-// k_intersect: retire finished slots, regenerate from the job, closest hit for active slots
+// k_regenerate: retire finished slots and start new paths in empty ones (camera rays or inputs)
 // ------------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256) k_intersect(SceneView s, Wavefront w, PathSource src) {
+__global__ void __launch_bounds__(256) k_regenerate(Wavefront w, PathSource src) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
     // every thread of a warp runs the same number of iterations so the warp-wide claim below is
@@ -661,12 +729,23 @@ __global__ void __launch_bounds__(256) k_intersect(SceneView s, Wavefront w, Pat
                 start_path(w, src, slot, id);
                 if ((w.status[slot] & 0xFFU) != 0U) {
                     w.state[slot] = kSlotDone;
-                } else {
-                    state = kSlotActive;
                 }
             }
         }
-        if (!in_range || state != kSlotActive) {
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_trace: closest hit of every active slot's ray; writes the hit and the slot's shading route
+// ------------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256, BF200_INTERSECT_MIN_BLOCKS) k_trace(SceneView s, Wavefront w) {
+    __shared__ int stack_columns[kSharedStackEntries * 256];
+    TraversalStack stack = thread_stack(stack_columns);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.capacity; slot += stride) {
+        if (w.state[slot] != kSlotActive) {
+            w.route[slot] = kRouteNone;
             continue;
         }
         const unsigned tracing = __activemask();
@@ -675,25 +754,29 @@ __global__ void __launch_bounds__(256) k_intersect(SceneView s, Wavefront w, Pat
         }
         const float4 o4 = w.ray_o[slot], d4 = w.ray_d[slot];
         const uint32_t mask = w.mask[slot];
-        const ClosestResult c = closest_hit(s, ld3(o4), ld3(d4), d4.w, o4.w, mask);
+        const ClosestResult c = closest_hit(s, ld3(o4), ld3(d4), d4.w, o4.w, mask, stack);
         w.status[slot] += 1U << 8;  // one extension segment
         if (c.failed) {
             w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneTraversal;
             w.state[slot] = kSlotDone;
+            w.route[slot] = kRouteNone;
             continue;
         }
         if (c.instance == 0xFFFFFFFFU) {
             w.hit_id[slot] = make_uint2(0xFFFFFFFFU, 0U);
+            w.route[slot] = static_cast<uint8_t>(kRouteGeneric);
             continue;
         }
         TriangleHit th;
         if (!hit_barycentrics(s, c, ld3(o4), ld3(d4), d4.w, o4.w, th)) {
             w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneNumerical;
             w.state[slot] = kSlotDone;
+            w.route[slot] = kRouteNone;
             continue;
         }
         w.hit_tb[slot] = make_float4(c.t, th.b0, th.b1, th.b2);
         w.hit_id[slot] = make_uint2(c.instance, c.primitive);
+        w.route[slot] = s.inst_route[c.instance];
     }
 }
 
@@ -990,6 +1073,7 @@ __device__ __forceinline__ bool is_black4(const float (&v)[4]) {
 
 // SceneMisPathLoop.cpp:136-275 (estimate) without the visibility query: the record carries the
 // shadow ray and the contribution it adds when unoccluded (transmittance 1).
+template <int K>
 __device__ void direct_lighting(const SceneView& s, const TransportParams& p, const Surface& surf,
                                 const ClosureData& closure, uint32_t allowed, const float4 beta4, F3 wo_world,
                                 uint64_t dims, const Stream& stream, uint32_t mask, ShadowRecord& rec, Lane& lane) {
@@ -1019,10 +1103,10 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
     if (wo.z == 0.0F || wi.z == 0.0F) {
         return;
     }
-    const bool lambert = closure.kind == kClosureLambert;
+    const bool lambert = kind_is<K>(closure, kClosureLambert);
     float f[4] = {0.0F, 0.0F, 0.0F, 0.0F};
     if (!lambert) {
-        closure_eval(closure, allowed, wo, wi, f, lane);
+        closure_eval<K>(closure, allowed, wo, wi, f, lane);
         if (is_black4(f)) {
             return;
         }
@@ -1036,7 +1120,7 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
             return;
         }
     }
-    const float bsdf_pdf = closure_pdf(closure, allowed, wo, wi, lane);
+    const float bsdf_pdf = closure_pdf<K>(closure, allowed, wo, wi, lane);
     const float light_pdf = joint_light_pdf(selection, ls.pdf, lane);
     const float weight = mis_weight(p.heuristic, light_pdf, bsdf_pdf, lane);
     // make_shadow_ray (ShadowRay.hpp:181-253) for a finite surface endpoint
@@ -1094,17 +1178,19 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
     }
 }
 
-__global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSource src, TransportParams p) {
-    __shared__ uint32_t warp_counts[8];
-    __shared__ unsigned long long block_base;
+// One launch per route: K is the closure kind the route's slots all share (0: generic route,
+// misses and any other material). The route queue lists the route's slots in slot order.
+template <int K>
+__global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView s, Wavefront w, PathSource src, TransportParams p,
+                                               uint32_t route) {
+    const uint32_t begin = w.route_offsets[route], end = w.route_offsets[route + 1U];
     const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t rounds = (w.capacity + stride - 1U) / stride;
     uint32_t active_here = 0;
-    for (uint32_t round = 0; round < rounds; ++round) {
-        const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x + round * stride;
+    for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+        const uint32_t slot = w.route_queue[i];
         ShadowRecord rec;
         rec.valid = false;
-        if (slot < w.capacity && w.state[slot] == kSlotActive) {
+        {
             Lane lane;
             const uint2 id = w.hit_id[slot];
             const float4 o4 = w.ray_o[slot], d4 = w.ray_d[slot];
@@ -1116,7 +1202,7 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSou
             const uint32_t mask = w.mask[slot];
             const Stream stream = load_stream(w, slot);
             const F3 ro = ld3(o4), rd = ld3(d4);
-            if (id.x == 0xFFFFFFFFU) {
+            if (K == 0 && id.x == 0xFFFFFFFFU) {
                 const float env[4] = {s.environment.x, s.environment.y, s.environment.z, s.environment.w};
                 add_product(rad, beta, env, lane);
                 w.radiance[slot] = rad;
@@ -1185,7 +1271,7 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSou
                         closure = s.closures[material];
                         // depth filter of one closure (DepthFilteredClosureMixture.hpp:262-364)
                         uint32_t block_mask = 0U;
-                        if (closure.kind == kClosureDielectric) {
+                        if (kind_is<K>(closure, kClosureDielectric)) {
                             const uint32_t br = depth_blocked(p, depth, kLobeGlossy | kLobeReflection);
                             const uint32_t bt = depth_blocked(p, depth, kLobeGlossy | kLobeTransmission);
                             if (br == 0U) allowed |= kLobeReflection; else block_mask |= br;
@@ -1207,7 +1293,7 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSou
                     const F3 wo = surf.frame.to_local(wo_world);
                     const uint64_t dims = bounce_base(depth_total(depth));
                     BsdfSample bs;
-                    closure_sample(closure, allowed, wo, stream.sample_1d(dims + 3), stream.sample_1d(dims + 4),
+                    closure_sample<K>(closure, allowed, wo, stream.sample_1d(dims + 3), stream.sample_1d(dims + 4),
                                    stream.sample_1d(dims + 5), bs, lane);
                     uint32_t next_depth = depth;
                     if (bs.valid) {
@@ -1218,7 +1304,7 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSou
                         next_depth = depth_advance(depth, bs.lobes);
                     }
                     if (lane.err == 0) {
-                        direct_lighting(s, p, surf, closure, allowed, beta, wo_world, dims, stream, mask, rec, lane);
+                        direct_lighting<K>(s, p, surf, closure, allowed, beta, wo_world, dims, stream, mask, rec, lane);
                     }
                     if (lane.err != 0) {
                         rec.valid = false;
@@ -1239,7 +1325,7 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSou
                             // update_closure_throughput (BsdfOnlyPathLoop.hpp:64-131), correction 1
                             const float bv[4] = {beta.x, beta.y, beta.z, beta.w};
                             float nb[4];
-                            if (closure.kind == kClosureLambert) {
+                            if (kind_is<K>(closure, kClosureLambert)) {
 #pragma unroll
                                 for (int l = 0; l < 4; ++l) {
                                     nb[l] = bv[l] * closure.w[l];
@@ -1352,33 +1438,13 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSou
                 }
             }
         }
-        // shadow-queue compaction: warp ballot / popc, block scan of warp totals, one atomic per block
-        const unsigned ballot = __ballot_sync(0xFFFFFFFFU, rec.valid);
-        const uint32_t warp = threadIdx.x >> 5, lane_id = threadIdx.x & 31U;
-        if (lane_id == 0U) {
-            warp_counts[warp] = __popc(ballot);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0U) {
-            uint32_t total = 0;
-            for (uint32_t k = 0; k < blockDim.x / 32U; ++k) {
-                const uint32_t c = warp_counts[k];
-                warp_counts[k] = total;
-                total += c;
-            }
-            block_base = total > 0U ? atomicAdd(&w.counters[0], static_cast<unsigned long long>(total)) : 0ULL;
-        }
-        __syncthreads();
         if (rec.valid) {
-            const uint32_t index = static_cast<uint32_t>(block_base) + warp_counts[warp] +
-                                   __popc(ballot & ((1U << lane_id) - 1U));
-            w.shadow_slot[index] = slot;
-            w.shadow_o[index] = make_float4(rec.origin.x, rec.origin.y, rec.origin.z, rec.t_max);
-            w.shadow_d[index] = make_float4(rec.direction.x, rec.direction.y, rec.direction.z, 0.0F);
-            w.shadow_c[index] = make_float4(rec.contribution[0], rec.contribution[1], rec.contribution[2],
-                                            rec.contribution[3]);
+            w.shadow_o[slot] = make_float4(rec.origin.x, rec.origin.y, rec.origin.z, rec.t_max);
+            w.shadow_d[slot] = make_float4(rec.direction.x, rec.direction.y, rec.direction.z, 0.0F);
+            w.shadow_c[slot] = make_float4(rec.contribution[0], rec.contribution[1], rec.contribution[2],
+                                           rec.contribution[3]);
+            w.shadow_key[slot] = 0U;
         }
-        __syncthreads();
     }
     // active-slot count for the host's termination test
     for (int off = 16; off > 0; off >>= 1) {
@@ -1393,20 +1459,22 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, Wavefront w, PathSou
 // k_occlude: shadow rays of the compacted queue; unoccluded contributions join the path radiance
 // ------------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256) k_occlude(SceneView s, Wavefront w) {
-    const uint32_t count = static_cast<uint32_t>(w.counters[0]);
+__global__ void __launch_bounds__(256, BF200_OCCLUDE_MIN_BLOCKS) k_occlude(SceneView s, Wavefront w) {
+    __shared__ int stack_columns[kSharedStackEntries * 256];
+    TraversalStack stack = thread_stack(stack_columns);
+    const uint32_t count = w.shadow_offsets[1];
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
-        const uint32_t slot = w.shadow_slot[i];
-        const float4 o = w.shadow_o[i], d = w.shadow_d[i];
-        const int occluded = any_hit(s, ld3(o), ld3(d), 0.0F, o.w, w.mask[slot]);
+        const uint32_t slot = w.shadow_queue[i];
+        const float4 o = w.shadow_o[slot], d = w.shadow_d[slot];
+        const int occluded = any_hit(s, ld3(o), ld3(d), 0.0F, o.w, w.mask[slot], stack);
         if (occluded < 0) {
             w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneTraversal;
             w.state[slot] = kSlotDone;
             continue;
         }
         if (occluded == 0) {
-            const float4 c = w.shadow_c[i];
+            const float4 c = w.shadow_c[slot];
             float4 r = w.radiance[slot];
             r.x = r.x + c.x;
             r.y = r.y + c.y;
@@ -1505,12 +1573,15 @@ __global__ void k_film(const float4* path_radiance, uint32_t pixels, uint32_t sa
 }
 
 // Standalone closest-hit / occlusion queries (ClosestHit.hpp:21-28, Occlusion.hpp:19-26).
-__global__ void k_query_closest(SceneView s, const bf200_ray_v1* rays, uint64_t n, bf200_hit_v1* hits) {
+__global__ void __launch_bounds__(128) k_query_closest(SceneView s, const bf200_ray_v1* rays, uint64_t n,
+                                                      bf200_hit_v1* hits) {
+    __shared__ int stack_columns[kSharedStackEntries * 128];
+    TraversalStack stack = thread_stack(stack_columns);
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const bf200_ray_v1 r = rays[i];
         const F3 o{r.origin[0], r.origin[1], r.origin[2]}, d{r.direction[0], r.direction[1], r.direction[2]};
-        const ClosestResult c = closest_hit(s, o, d, r.t_min, r.t_max, r.mask);
+        const ClosestResult c = closest_hit(s, o, d, r.t_min, r.t_max, r.mask, stack);
         bf200_hit_v1 h;
         h.t = 0.0F;
         h.barycentrics[0] = h.barycentrics[1] = h.barycentrics[2] = 0.0F;
@@ -1535,12 +1606,15 @@ __global__ void k_query_closest(SceneView s, const bf200_ray_v1* rays, uint64_t 
     }
 }
 
-__global__ void k_query_occlusion(SceneView s, const bf200_ray_v1* rays, uint64_t n, uint32_t* out) {
+__global__ void __launch_bounds__(128) k_query_occlusion(SceneView s, const bf200_ray_v1* rays, uint64_t n,
+                                                        uint32_t* out) {
+    __shared__ int stack_columns[kSharedStackEntries * 128];
+    TraversalStack stack = thread_stack(stack_columns);
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const bf200_ray_v1 r = rays[i];
         const F3 o{r.origin[0], r.origin[1], r.origin[2]}, d{r.direction[0], r.direction[1], r.direction[2]};
-        const int occ = any_hit(s, o, d, r.t_min, r.t_max, r.mask);
+        const int occ = any_hit(s, o, d, r.t_min, r.t_max, r.mask, stack);
         out[i] = occ < 0 ? 2U : static_cast<uint32_t>(occ);
     }
 }
@@ -1561,20 +1635,39 @@ cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instanc
 }
 
 cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
-                         const TransportParams& p, uint32_t grid, cudaStream_t stream) {
+                         const TransportParams& p, uint32_t grid, cudaStream_t stream, uint32_t* launches) {
+    cudaError_t e = cudaSuccess;
     if (stage == 0) {
-        k_intersect<<<grid, 256, 0, stream>>>(s, w, src);
-    } else if (stage == 1) {
-        k_shade<<<grid, 256, 0, stream>>>(s, w, src, p);
-    } else {
-        k_occlude<<<grid, 256, 0, stream>>>(s, w);
+        k_regenerate<<<grid, 256, 0, stream>>>(w, src);
+        k_trace<<<grid, 256, 0, stream>>>(s, w);
+        *launches += 2U;
+        return cudaGetLastError();
     }
+    if (stage == 1) {
+        // route the traced slots, shade each route with its own kernel, then queue the shadow rays
+        e = launch_compaction(w.route, w.capacity, kRouteCount, w.tile_counts, w.route_queue, w.route_offsets,
+                              nullptr, w.shadow_key, stream, launches);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        k_shade<0><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteGeneric);
+        k_shade<static_cast<int>(kClosureLambert)><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteLambert);
+        k_shade<static_cast<int>(kClosureConductor)><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteConductor);
+        k_shade<static_cast<int>(kClosureDielectric)><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteDielectric);
+        *launches += 4U;
+        if ((e = cudaGetLastError()) != cudaSuccess) {
+            return e;
+        }
+        return launch_compaction(w.shadow_key, w.capacity, 1U, w.tile_counts, w.shadow_queue, w.shadow_offsets,
+                                 w.counters + 0, nullptr, stream, launches);
+    }
+    k_occlude<<<grid, 256, 0, stream>>>(s, w);
+    *launches += 1U;
     return cudaGetLastError();
 }
 
-cudaError_t launch_retire(const SceneView& s, const Wavefront& w, const PathSource& src, uint32_t grid,
-                          cudaStream_t stream) {
-    k_intersect<<<grid, 256, 0, stream>>>(s, w, src);
+cudaError_t launch_retire(const Wavefront& w, const PathSource& src, uint32_t grid, cudaStream_t stream) {
+    k_regenerate<<<grid, 256, 0, stream>>>(w, src);
     return cudaGetLastError();
 }
 

@@ -9,11 +9,19 @@ namespace bf200 {
 
 cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instance, const uint32_t* tri_local,
                                  uint32_t total, float4* out, uint32_t* failures, cudaStream_t stream);
-// stage 0: k_intersect, 1: k_shade, 2: k_occlude
+// stage 0: k_regenerate, k_trace; 1: route compaction, the per-route k_shade kernels, shadow compaction;
+// 2: k_occlude. Adds the number of kernels launched to *launches.
 cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
-                         const TransportParams& p, uint32_t grid, cudaStream_t stream);
-cudaError_t launch_retire(const SceneView& s, const Wavefront& w, const PathSource& src, uint32_t grid,
-                          cudaStream_t stream);
+                         const TransportParams& p, uint32_t grid, cudaStream_t stream, uint32_t* launches);
+// Stable compaction of n one-byte keys: the indices whose key is r < routes go to
+// queue[offsets[r] .. offsets[r + 1]) in increasing order. tile_counts holds routes x
+// ceil(n / kCompactTile) words of scratch. When total is given it receives the queue length; when
+// reset_keys is given every one of its n bytes is set to kRouteNone. Three launches.
+cudaError_t launch_compaction(const uint8_t* keys, uint32_t n, uint32_t routes, uint32_t* tile_counts,
+                              uint32_t* queue, uint32_t* offsets, unsigned long long* total, uint8_t* reset_keys,
+                              cudaStream_t stream, uint32_t* launches);
+// Retires the slots the last iteration finished (k_regenerate; nothing is left to claim).
+cudaError_t launch_retire(const Wavefront& w, const PathSource& src, uint32_t grid, cudaStream_t stream);
 cudaError_t launch_film(const float4* path_radiance, uint32_t pixels, uint32_t samples, const float* response12,
                         const float* pdf4, float normalization, uint32_t precision, float4* film32, double* film64,
                         unsigned long long* counts, unsigned long long* skipped, cudaStream_t stream);

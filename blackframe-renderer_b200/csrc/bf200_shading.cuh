@@ -51,9 +51,13 @@ __device__ __forceinline__ float max_abs3(F3 v) {
 }
 __device__ __forceinline__ F3 ld3(const float4 v) { return {v.x, v.y, v.z}; }
 
-// Sine and cosine of a float angle: the double-precision functions rounded once to float.
-__device__ __forceinline__ float sin_f(float a) { return static_cast<float>(sin(static_cast<double>(a))); }
-__device__ __forceinline__ float cos_f(float a) { return static_cast<float>(cos(static_cast<double>(a))); }
+// Sine and cosine of a float angle: the double-precision values rounded once to float. One
+// out-of-line copy shared by every call site (one argument reduction for both values).
+static __device__ __noinline__ float2 sincos_f(float a) {
+    double s = 0.0, c = 0.0;
+    sincos(static_cast<double>(a), &s, &c);
+    return make_float2(static_cast<float>(s), static_cast<float>(c));
+}
 
 // ------------------------------------------------------------------------------------------------
 // SampleStream (SampleStream.hpp:23-67) and SampleDimensionMap (SampleDimensionMap.cpp:47-68)
@@ -178,8 +182,9 @@ __device__ __forceinline__ Frame frame_from_normal(F3 v, Lane& lane) {
 // LocalFrame.hpp:116-135
 __device__ __forceinline__ Frame rotated_about_normal(const Frame& f, float angle, Lane& lane) {
     const float reduced = remainderf(angle, 2.0F * kPi);
-    const float c = cos_f(reduced);
-    const float s = sin_f(reduced);
+    const float2 sc = sincos_f(reduced);
+    const float c = sc.y;
+    const float s = sc.x;
     const F3 rotated = f.t * c + f.b * s;
     return frame_from_unit_normal_and_tangent(f.n, rotated, lane);
 }
@@ -531,8 +536,9 @@ __device__ __forceinline__ F3 map_cosine_hemisphere(float u, float v) {
             r = oy;
             phi = 2.0F * quarter_pi - quarter_pi * (ox / oy);
         }
-        px = r * cos_f(phi);
-        py = r * sin_f(phi);
+        const float2 sc = sincos_f(phi);
+        px = r * sc.y;
+        py = r * sc.x;
         radius = fabsf(r);
     }
     const float z = sqrtf((1.0F - radius) * (1.0F + radius));
@@ -706,8 +712,9 @@ static __device__ bool ggx_sample_vndf(float ax, float ay, F3 wo, float u, float
     const F3 bitangent = cross(hv, tangent);
     const float disk_radius = sqrtf(u);
     const float azimuth = 2.0F * kPi * v;
-    const float disk_x = disk_radius * cos_f(azimuth);
-    const float initial_disk_y = disk_radius * sin_f(azimuth);
+    const float2 sc = sincos_f(azimuth);
+    const float disk_x = disk_radius * sc.y;
+    const float initial_disk_y = disk_radius * sc.x;
     const float limit_sq = (1.0F - disk_x) * (1.0F + disk_x);
     const float checked_limit_sq = nonnegative_roundoff(limit_sq, 1.0F + fabsf(disk_x), lane);
     const float disk_y_limit = sqrtf(checked_limit_sq);
@@ -1129,8 +1136,20 @@ static __device__ float dielectric_pdf_masked(const ClosureData& c, uint32_t all
     return checked_product_ratio(num, den, lane);
 }
 
+// Closure kind fixed at compile time (K = the kind) or read from the record (K = 0). The shading
+// kernels are instantiated per kind so each one carries only its own closure's code.
+template <int K>
+__device__ __forceinline__ bool kind_is(const ClosureData& c, uint32_t kind) {
+    if constexpr (K == 0) {
+        return c.kind == kind;
+    } else {
+        return static_cast<uint32_t>(K) == kind;
+    }
+}
+
+template <int K>
 static __device__ void closure_eval(const ClosureData& c, uint32_t allowed, F3 wo, F3 wi, float (&out)[4], Lane& lane) {
-    if (c.kind == kClosureLambert) {  // LambertianReflection.hpp:76-85
+    if (kind_is<K>(c, kClosureLambert)) {  // LambertianReflection.hpp:76-85
         out[0] = out[1] = out[2] = out[3] = 0.0F;
         if (!unit_length(wo) || !unit_length(wi)) {
             lane.fail();
@@ -1145,7 +1164,7 @@ static __device__ void closure_eval(const ClosureData& c, uint32_t allowed, F3 w
         }
         return;
     }
-    if (c.kind == kClosureConductor) {
+    if (kind_is<K>(c, kClosureConductor)) {
         conductor_eval(c, wo, wi, out, lane);
         return;
     }
@@ -1159,8 +1178,9 @@ static __device__ void closure_eval(const ClosureData& c, uint32_t allowed, F3 w
     }
 }
 
+template <int K>
 static __device__ float closure_pdf(const ClosureData& c, uint32_t allowed, F3 wo, F3 wi, Lane& lane) {
-    if (c.kind == kClosureLambert) {  // LambertianReflection.hpp:87-106
+    if (kind_is<K>(c, kClosureLambert)) {  // LambertianReflection.hpp:87-106
         if (!unit_length(wo) || !unit_length(wi)) {
             lane.fail();
             return 0.0F;
@@ -1170,7 +1190,7 @@ static __device__ float closure_pdf(const ClosureData& c, uint32_t allowed, F3 w
         }
         return wi.z * kInvPi;
     }
-    if (c.kind == kClosureConductor) {
+    if (kind_is<K>(c, kClosureConductor)) {
         return conductor_pdf(c, wo, wi, lane);
     }
     return dielectric_pdf_masked(c, allowed, wo, wi, lane);
@@ -1274,6 +1294,7 @@ static __device__ void dielectric_sample(const ClosureData& c, F3 wo, float even
 }
 
 // DepthFilteredClosureMixture.hpp:460-552 for a single active closure.
+template <int K>
 static __device__ void closure_sample(const ClosureData& c, uint32_t allowed, F3 wo, float component, float u, float v,
                                BsdfSample& s, Lane& lane) {
     s.valid = false;
@@ -1283,18 +1304,18 @@ static __device__ void closure_sample(const ClosureData& c, uint32_t allowed, F3
         lane.fail();
         return;
     }
-    if (c.kind == kClosureLambert) {  // LambertianReflection.hpp:108-140
+    if (kind_is<K>(c, kClosureLambert)) {  // LambertianReflection.hpp:108-140
         const F3 wi = map_cosine_hemisphere(u, v);
         if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
             return;
         }
         s.wi = wi;
-        closure_eval(c, allowed, wo, wi, s.value, lane);
-        s.pdf = closure_pdf(c, allowed, wo, wi, lane);
+        closure_eval<K>(c, allowed, wo, wi, s.value, lane);
+        s.pdf = closure_pdf<K>(c, allowed, wo, wi, lane);
         s.valid = true;
         return;
     }
-    if (c.kind == kClosureConductor) {  // RoughConductorReflection.hpp:240-288
+    if (kind_is<K>(c, kClosureConductor)) {  // RoughConductorReflection.hpp:240-288
         F3 m;
         if (!ggx_sample_vndf(c.p[8], c.p[9], wo, u, v, m, lane)) {
             return;
