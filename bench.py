@@ -39,12 +39,16 @@ CAMERA_RAY_BYTES = 28
 EXTENSION_SEGMENT_BYTES = 240
 SHADOW_SEGMENT_BYTES = 96
 FILM_SAMPLE_BYTES = 24
-# per-launch algorithmic bytes of the traversal kernel: camera ray write, ray read + hit write
-INTERSECT_SEGMENT_BYTES = 48
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per processed segment, from one ncu
-# capture of a full-wavefront launch (2,097,152 segments) of each stage kernel of this build;
+# algorithmic bytes per unit of each stage (unit: extension segment for trace and shade, shadow
+# segment for occlude): trace reads the ray (28) and writes the hit (20); shade owns the rest of the
+# extension segment's 240 B; occlude the whole shadow segment
+STAGE_BYTES_PER_UNIT = {"trace": 48, "shade": EXTENSION_SEGMENT_BYTES - 48, "occlude": SHADOW_SEGMENT_BYTES}
+STAGE_KERNELS = {"trace": "k_trace", "shade": "k_shade<kind> x4 + route/shadow compaction",
+                 "occlude": "k_occlude"}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per processed unit, from one ncu
+# capture of a full-wavefront launch (2,097,152 segments) of each stage's kernels in this build;
 # profiles/stages_cornell_spheres_256_spp64.md holds the capture and its command
-MEASURED_TRAFFIC_PER_SEGMENT = {"k_intersect": 479.3, "k_shade": 229.4, "k_occlude": None}
+MEASURED_TRAFFIC_PER_UNIT = {"trace": 57.7, "shade": 350.0, "occlude": None}
 TRAFFIC_SOURCE = "profiles/stages_cornell_spheres_256_spp64.md"
 
 
@@ -268,10 +272,11 @@ def main():
     ext = sum(r.extension_segments for r in reports)
     shadow = sum(r.shadow_segments for r in reports)
     iterations = sum(r.iterations for r in reports)
-    stage = {"k_intersect": sum(r.intersect_milliseconds for r in reports),
-             "k_shade": sum(r.shade_milliseconds for r in reports),
-             "k_occlude": sum(r.occlude_milliseconds for r in reports),
-             "k_film": sum(r.film_milliseconds for r in reports)}
+    stage = {"regenerate": sum(r.regenerate_milliseconds for r in reports),
+             "trace": sum(r.intersect_milliseconds for r in reports),
+             "shade": sum(r.shade_milliseconds for r in reports),
+             "occlude": sum(r.occlude_milliseconds for r in reports),
+             "film": sum(r.film_milliseconds for r in reports)}
 
     # e2e: the public C-ABI call with host film buffers (copies in the timed region)
     host_film = np.zeros((height, width, 4), np.float32)
@@ -293,20 +298,17 @@ def main():
         e2e_total = float(t.item())
     e2e_value = paths_per_step * world * len(e2e_ms) / (e2e_total / 1000.0)
 
-    # roofline of the dominant kernel: algorithmic bytes per launch / average launch time
+    # roofline of the dominant stage: algorithmic bytes per launch / average launch time (CUDA events
+    # around the stage's launches on the wavefront stream, summed by the library per iteration)
     peak, peak_kind = measured_peaks()
-    dominant = max(("k_intersect", "k_shade", "k_occlude"), key=lambda k: stage[k])
+    dominant = max(("trace", "shade", "occlude"), key=lambda k: stage[k])
     per_launch_ms = stage[dominant] / max(1, iterations)
-    if dominant == "k_intersect":
-        bytes_total = CAMERA_RAY_BYTES * paths_per_step * args.steps + INTERSECT_SEGMENT_BYTES * ext
-    elif dominant == "k_shade":
-        bytes_total = (EXTENSION_SEGMENT_BYTES - INTERSECT_SEGMENT_BYTES) * ext
-    else:
-        bytes_total = SHADOW_SEGMENT_BYTES * shadow
+    units = shadow if dominant == "occlude" else ext
+    bytes_total = STAGE_BYTES_PER_UNIT[dominant] * units
     bytes_per_launch = bytes_total / max(1, iterations)
     achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
-    units_per_launch = (shadow if dominant == "k_occlude" else ext) / max(1, iterations)
-    traffic_per_unit = MEASURED_TRAFFIC_PER_SEGMENT.get(dominant)
+    units_per_launch = units / max(1, iterations)
+    traffic_per_unit = MEASURED_TRAFFIC_PER_UNIT.get(dominant)
     traffic = traffic_per_unit * units_per_launch if traffic_per_unit is not None else None
     whole_bytes = (CAMERA_RAY_BYTES * paths_per_step * args.steps + EXTENSION_SEGMENT_BYTES * ext +
                    SHADOW_SEGMENT_BYTES * shadow + FILM_SAMPLE_BYTES * paths_per_step * args.steps)
@@ -326,7 +328,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": STAGE_KERNELS[dominant], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "traffic_source": TRAFFIC_SOURCE,
                      "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind,
                      "whole_path_algorithmic_gbs": whole_bytes / (total_ms / 1000.0) / 1e9},

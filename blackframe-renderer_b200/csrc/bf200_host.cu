@@ -587,7 +587,7 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
     cudaMemcpyAsync(w.counters + 6, &kNone, sizeof(kNone), cudaMemcpyHostToDevice, st);
     const uint32_t grid =
         std::max<uint32_t>(1, std::min<uint32_t>((w.capacity + 255U) / 256U, c->sm_count * 8U));
-    cudaEvent_t ev[4];
+    cudaEvent_t ev[5];
     for (auto& x : ev) {
         cudaEventCreate(&x);
     }
@@ -596,7 +596,7 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
     cudaEventCreate(&stop);
     cudaEventRecord(start, st);
     uint64_t iterations = 0, launches = 0, shadow_segments = 0;
-    double stage_ms[3] = {0.0, 0.0, 0.0};
+    double stage_ms[4] = {0.0, 0.0, 0.0, 0.0};
     // every path finishes within (sum of surface depth limits + 1) extension segments, and a
     // slot hosts at most ceil(total / capacity) + 1 paths: bound the host loop accordingly
     const uint64_t depth_bound = static_cast<uint64_t>(p.limits[0]) + p.limits[1] + p.limits[2] + 2;
@@ -606,14 +606,14 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
         cudaMemsetAsync(w.counters + 0, 0, sizeof(unsigned long long), st);
         cudaMemsetAsync(w.counters + 2, 0, sizeof(unsigned long long), st);
         uint32_t stage_launches = 0;
-        for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage) {
+        for (int stage = 0; stage < 4 && e == cudaSuccess; ++stage) {
             if (instrument) {
                 cudaEventRecord(ev[stage], st);
             }
             e = launch_stage(stage, s->view, w, src, p, grid, st, &stage_launches);
         }
         if (instrument) {
-            cudaEventRecord(ev[3], st);
+            cudaEventRecord(ev[4], st);
         }
         launches += stage_launches;
         ++iterations;
@@ -629,7 +629,7 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
             return cuda_fail(c, e, "wavefront iteration");
         }
         if (instrument) {
-            for (int stage = 0; stage < 3; ++stage) {
+            for (int stage = 0; stage < 4; ++stage) {
                 float ms = 0.0F;
                 cudaEventElapsedTime(&ms, ev[stage], ev[stage + 1]);
                 stage_ms[stage] += ms;
@@ -679,9 +679,10 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
         }
         report->kernel_launches += launches;
         report->gpu_milliseconds += ms;
-        report->intersect_milliseconds += stage_ms[0];
-        report->shade_milliseconds += stage_ms[1];
-        report->occlude_milliseconds += stage_ms[2];
+        report->regenerate_milliseconds += stage_ms[0];
+        report->intersect_milliseconds += stage_ms[1];
+        report->shade_milliseconds += stage_ms[2];
+        report->occlude_milliseconds += stage_ms[3];
         report->iterations += iterations;
     }
     return BLACKFRAME_STATUS_SUCCESS;

@@ -1639,11 +1639,15 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
     cudaError_t e = cudaSuccess;
     if (stage == 0) {
         k_regenerate<<<grid, 256, 0, stream>>>(w, src);
-        k_trace<<<grid, 256, 0, stream>>>(s, w);
-        *launches += 2U;
+        *launches += 1U;
         return cudaGetLastError();
     }
     if (stage == 1) {
+        k_trace<<<grid, 256, 0, stream>>>(s, w);
+        *launches += 1U;
+        return cudaGetLastError();
+    }
+    if (stage == 2) {
         // route the traced slots, shade each route with its own kernel, then queue the shadow rays
         e = launch_compaction(w.route, w.capacity, kRouteCount, w.tile_counts, w.route_queue, w.route_offsets,
                               nullptr, w.shadow_key, stream, launches);

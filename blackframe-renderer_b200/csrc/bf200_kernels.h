@@ -9,8 +9,8 @@ namespace bf200 {
 
 cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instance, const uint32_t* tri_local,
                                  uint32_t total, float4* out, uint32_t* failures, cudaStream_t stream);
-// stage 0: k_regenerate, k_trace; 1: route compaction, the per-route k_shade kernels, shadow compaction;
-// 2: k_occlude. Adds the number of kernels launched to *launches.
+// stage 0: k_regenerate; 1: k_trace; 2: route compaction, the per-route k_shade kernels, shadow
+// compaction; 3: k_occlude. Adds the number of kernels launched to *launches.
 cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
                          const TransportParams& p, uint32_t grid, cudaStream_t stream, uint32_t* launches);
 // Stable compaction of n one-byte keys: the indices whose key is r < routes go to

@@ -388,13 +388,16 @@ typedef struct bf200_report_v1 {
     uint32_t first_failure_path;
     uint64_t kernel_launches;
     double gpu_milliseconds;
-    /* with instrumentation: summed GPU time of each stage kernel, and the iteration count */
+    /* with instrumentation: summed GPU time of each stage, and the iteration count. intersect:
+     * closest-hit traversal; shade: routing, the per-closure shading kernels and the shadow-queue
+     * compaction; occlude: shadow rays; regenerate: path retirement and camera-ray generation */
     double intersect_milliseconds;
     double shade_milliseconds;
     double occlude_milliseconds;
     double film_milliseconds;
     uint64_t iterations;
-    uint64_t reserved[3];
+    double regenerate_milliseconds;
+    uint64_t reserved[2];
 } bf200_report_v1;
 
 typedef struct bf200_context bf200_context;
