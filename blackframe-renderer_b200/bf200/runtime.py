@@ -22,6 +22,7 @@ EXPORTED_SYMBOLS = [
     "bf200_context_last_error", "bf200_scene_create", "bf200_scene_destroy", "bf200_trace_paths",
     "bf200_trace_paths_device", "bf200_render_film", "bf200_render_film_device",
     "bf200_closest_hits", "bf200_occlusions", "bf200_build_info", "bf200_camera_create",
+    "bf200_trace_paths_device_noalloc",
 ]
 
 
@@ -54,6 +55,9 @@ def library():
         f = getattr(lib, name)
         f.argtypes = [vp, vp, vp, C.c_uint64, C.POINTER(abi.TransportOptions), vp, C.POINTER(abi.Report)]
         f.restype = C.c_uint32
+    lib.bf200_trace_paths_device_noalloc.argtypes = [vp, vp, vp, C.c_uint64, C.POINTER(abi.TransportOptions), vp,
+                                                     C.c_uint32, C.POINTER(abi.Report)]
+    lib.bf200_trace_paths_device_noalloc.restype = C.c_uint32
     for name in ("bf200_render_film", "bf200_render_film_device"):
         f = getattr(lib, name)
         f.argtypes = [vp, vp, C.POINTER(abi.Camera), C.POINTER(abi.Sensor), C.POINTER(abi.FilmRequest),
@@ -134,6 +138,27 @@ class Context:
                                                 C.byref(options), C.cast(results, C.c_void_p),
                                                 C.byref(report)), "trace_paths")
         return results, report
+
+    def trace_paths_device(self, scene, device_inputs, path_count, options, device_results):
+        """bf200_trace_paths_device: inputs and results are device pointers (ints)."""
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_trace_paths_device(self.handle, scene.handle, device_inputs, path_count,
+                                                       C.byref(options), device_results, C.byref(report)),
+                    "trace_paths_device")
+        return report
+
+    def trace_paths_device_noalloc(self, scene, device_inputs, path_count, options, device_results,
+                                   path_capacity=0):
+        """bf200_trace_paths_device_noalloc: the allocation-free variant over the library's static
+        scratch array (path_capacity slots, 0 = the maximum)."""
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_trace_paths_device_noalloc(self.handle, scene.handle, device_inputs, path_count,
+                                                               C.byref(options), device_results, path_capacity,
+                                                               C.byref(report)),
+                    "trace_paths_device_noalloc")
+        return report
 
     def render_film(self, scene, camera, sensor, options, samples_per_pixel, seed=0, first_sample=0,
                     precision=0, film=None):

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1074,6 +1075,166 @@ BF200_EXPORT blackframe_status bf200_trace_paths_device(bf200_context* c, const 
     src.inputs = device_inputs;
     src.results = device_results;
     return run_wavefront(c, s, src, make_params(*o), o->instrumentation != 0, report);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free trace: the same wavefront over a scratch array compiled into the library
+// ---------------------------------------------------------------------------------------------
+
+}  // extern "C"
+
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BF200_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kScratchDevices = 64;
+std::mutex g_scratch_mutex;
+void* g_scratch_address[kScratchDevices] = {};
+
+// Device address of the scratch array on the context's device, looked up once per device.
+blackframe_status noalloc_scratch(bf200_context* c, void** out) {
+    if (c->device < 0 || c->device >= kScratchDevices) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "device ordinal outside the scratch address table");
+    }
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (g_scratch_address[c->device] == nullptr) {
+        void* address = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&address, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "scratch symbol address");
+        }
+        g_scratch_address[c->device] = address;
+    }
+    *out = g_scratch_address[c->device];
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+// The wavefront loop of run_wavefront without its allocations: no events (no stage timing), and
+// the per-iteration counters are read into host stack memory instead of pinned memory.
+blackframe_status run_wavefront_noalloc(bf200_context* c, const bf200_scene* s, const Wavefront& w, PathSource src,
+                                        const TransportParams& p, bf200_report_v1* report) {
+    cudaStream_t st = c->stream;
+    // what must start at zero: slot states (all empty) and the counters; the first failing path
+    // (counters[6], a minimum) starts at all ones
+    cudaError_t e = cudaMemsetAsync(w.state, 0, w.capacity, st);
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), st);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(w.counters + 6, 0xFF, sizeof(unsigned long long), st);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "scratch reset");
+    }
+    const uint32_t grid =
+        std::max<uint32_t>(1, std::min<uint32_t>((w.capacity + 255U) / 256U, c->sm_count * 8U));
+    unsigned long long counters[8] = {};
+    uint64_t iterations = 0, launches = 0, shadow_segments = 0;
+    const uint64_t depth_bound = static_cast<uint64_t>(p.limits[0]) + p.limits[1] + p.limits[2] + 2;
+    const uint64_t max_iterations = 64 + 2 * (src.total / w.capacity + 2) * depth_bound;
+    while (iterations < max_iterations) {
+        e = cudaMemsetAsync(w.counters + 0, 0, sizeof(unsigned long long), st);
+        if (e == cudaSuccess) {
+            e = cudaMemsetAsync(w.counters + 2, 0, sizeof(unsigned long long), st);
+        }
+        uint32_t stage_launches = 0;
+        for (int stage = 0; stage < 4 && e == cudaSuccess; ++stage) {
+            e = launch_stage(stage, s->view, w, src, p, grid, st, &stage_launches);
+        }
+        launches += stage_launches;
+        ++iterations;
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "wavefront launch");
+        }
+        e = cudaMemcpyAsync(counters, w.counters, sizeof(counters), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(st);
+        }
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "wavefront iteration");
+        }
+        shadow_segments += counters[0];
+        if (counters[2] == 0 && counters[1] >= src.total) {
+            break;
+        }
+    }
+    if (iterations >= max_iterations) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "the wavefront did not drain within its iteration bound");
+    }
+    e = launch_retire(w, src, grid, st);
+    ++launches;
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(counters, w.counters, sizeof(counters), cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "wavefront retire");
+    }
+    if (report != nullptr) {
+        report->struct_size = sizeof(bf200_report_v1);
+        report->registered_light_count = s->light_count;
+        report->path_count = src.total;
+        report->extension_segments = counters[3];
+        report->shadow_segments = shadow_segments;
+        report->failed_lanes = counters[5];
+        if (counters[5] != 0) {
+            report->first_failure_status = static_cast<uint32_t>(counters[7]);
+            report->first_failure_path = static_cast<uint32_t>(counters[6]);
+        }
+        report->kernel_launches = launches;
+        report->iterations = iterations;
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+BF200_EXPORT blackframe_status bf200_trace_paths_device_noalloc(bf200_context* c, const bf200_scene* s,
+                                                                 const bf200_path_input_v1* device_inputs,
+                                                                 uint64_t path_count,
+                                                                 const bf200_transport_options_v1* o,
+                                                                 bf200_path_result_v1* device_results,
+                                                                 uint32_t path_capacity,
+                                                                 bf200_report_v1* report) noexcept {
+    if (c == nullptr || s == nullptr || (path_count != 0 && (device_inputs == nullptr || device_results == nullptr))) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (s->context != c) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "scene belongs to another context");
+    }
+    if (const auto st = validate_options(c, o); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    if (path_capacity > BF200_NOALLOC_MAX_SLOTS) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE,
+                    "path_capacity exceeds the allocation-free scratch limit of 65536 slots (16 MiB of device scratch)");
+    }
+    const uint32_t capacity = path_capacity == 0 ? BF200_NOALLOC_MAX_SLOTS : path_capacity;
+    if (report != nullptr) {
+        std::memset(report, 0, sizeof(*report));
+    }
+    if (path_count == 0) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    cudaSetDevice(c->device);
+    void* base = nullptr;
+    if (const auto st = noalloc_scratch(c, &base); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    Wavefront w{};
+    if (carve_wavefront(static_cast<char*>(base), capacity, &w) > BF200_NOALLOC_SCRATCH_BYTES) {
+        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "scratch layout exceeds the static scratch array");
+    }
+    PathSource src{};
+    src.mode = 1;
+    src.total = path_count;
+    src.inputs = device_inputs;
+    src.results = device_results;
+    return run_wavefront_noalloc(c, s, w, src, make_params(*o), report);
 }
 
 BF200_EXPORT blackframe_status bf200_trace_paths(bf200_context* c, const bf200_scene* s,

@@ -444,6 +444,39 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_device(
     uint64_t path_count, const bf200_transport_options_v1* options,
     bf200_path_result_v1* device_results, bf200_report_v1* report) BF200_NOEXCEPT;
 
+/* Allocation-free variant of bf200_trace_paths_device. It has no counterpart in the reference.
+ *
+ * Why: the ordinary entry point sizes its wavefront arena on first use with cudaMalloc and
+ * cudaMallocHost. Some callers cannot let a trace allocate:
+ *   - a renderer that has committed the device's memory to its own pools before the first frame,
+ *     where a late allocation can fail with out-of-memory halfway through a frame;
+ *   - a host that keeps other streams busy, where cudaFree and, often, cudaMalloc synchronise the
+ *     whole device and stall unrelated work;
+ *   - an interactive loop that cannot absorb the allocator's unpredictable host latency.
+ * This call uses a fixed scratch array compiled into the library: a file-scope __device__ array of
+ * BF200_NOALLOC_SCRATCH_BYTES, holding at most BF200_NOALLOC_MAX_SLOTS path slots. It makes no
+ * cudaMalloc, cudaMallocHost, cudaFree, event or stream creation, or other allocating call. It
+ * clears the slot states and counters it needs with cudaMemsetAsync on the context's stream, and
+ * reads its per-iteration counters back into host stack memory.
+ *
+ * path_capacity: slots kept in flight, 0 = BF200_NOALLOC_MAX_SLOTS. A larger value is refused with
+ * BLACKFRAME_STATUS_OUT_OF_RANGE. Any path_count is accepted, because finished slots are refilled.
+ * Results are identical to bf200_trace_paths_device for the same inputs.
+ *
+ * The device address of the scratch array is looked up once per device with
+ * cudaGetSymbolAddress, at the first call on that device. That first call can also make the CUDA
+ * driver load the library's device code, so make it during setup, before any stream capture
+ * begins. All calls on one device share the one scratch array: calls that overlap in time, from
+ * any context or thread, race and corrupt each other's results, so the caller must serialise
+ * them. instrumentation is ignored (no events); the report's timing fields are zero. */
+#define BF200_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define BF200_NOALLOC_MAX_SLOTS 65536u
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_device_noalloc(
+    bf200_context* context, const bf200_scene* scene, const bf200_path_input_v1* device_inputs,
+    uint64_t path_count, const bf200_transport_options_v1* options,
+    bf200_path_result_v1* device_results, uint32_t path_capacity,
+    bf200_report_v1* report) BF200_NOEXCEPT;
+
 /* Renders pinhole-camera paths on the device (camera rays, transport and film accumulation all
  * on the GPU) and adds them to a host film. */
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_film(
