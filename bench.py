@@ -213,7 +213,6 @@ def main():
     builder, options, camera, sensor, (width, height, spp) = workload_setup()
     if args.spp > 0:
         spp = args.spp
-    options.instrumentation = 1
     pixels = width * height
     paths_per_step = pixels * spp
     ctx = runtime.Context(local_rank, path_capacity=args.capacity)
@@ -223,10 +222,8 @@ def main():
     counts = torch.zeros((height, width), dtype=torch.int64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
-    def render_device(step):
-        film.zero_()
-        counts.zero_()
-        torch.cuda.synchronize()
+    def render_device(step, instrument=False):
+        options.instrumentation = 1 if instrument else 0
         f = abi.Film(width, height, 0, 0, film.data_ptr(), C.cast(counts.data_ptr(), C.POINTER(abi.u64)))
         first = (step * world + rank) * spp  # disjoint sample ranges per rank and step
         request = abi.FilmRequest(C.sizeof(abi.FilmRequest), spp, first, 0, 0)
@@ -241,10 +238,14 @@ def main():
         return report
 
     for step in range(args.warmup):
+        film.zero_()
+        counts.zero_()
         render_device(step)
     torch.cuda.synchronize()
 
-    # timed region: device-resident inputs, K full frames; L2 flushed between frames
+    # timed region: device-resident inputs, K full frames; L2 flushed between frames. Each frame is
+    # timed with CUDA events bracketing the whole library call (which returns after its stream has
+    # finished), so launch gaps and per-iteration host round trips are inside the measurement.
     reports = []
     step_ms = []
     with ClockSampler(local_rank) as clocks:
@@ -252,16 +253,28 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
         for step in range(args.steps):
+            film.zero_()
+            counts.zero_()
             flush.fill_(step & 0xFF)
             torch.cuda.synchronize()
             start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
             report = render_device(args.warmup + step)
+            stop.record()
+            torch.cuda.synchronize()
             reports.append(report)
-            step_ms.append(report.gpu_milliseconds)
+            step_ms.append(start.elapsed_time(stop))
         torch.cuda.synchronize()
         if distributed:
             dist.barrier()
     total_ms = sum(step_ms)
+    # one more frame, untimed, with per-stage CUDA events inside the library (the stage breakdown
+    # and the roofline's per-launch times come from it)
+    film.zero_()
+    counts.zero_()
+    flush.fill_(0x5A)
+    torch.cuda.synchronize()
+    staged = render_device(args.warmup + args.steps, instrument=True)
     if distributed:
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -272,13 +285,12 @@ def main():
     ext = sum(r.extension_segments for r in reports)
     shadow = sum(r.shadow_segments for r in reports)
     iterations = sum(r.iterations for r in reports)
-    stage = {"regenerate": sum(r.regenerate_milliseconds for r in reports),
-             "trace": sum(r.intersect_milliseconds for r in reports),
-             "shade": sum(r.shade_milliseconds for r in reports),
-             "occlude": sum(r.occlude_milliseconds for r in reports),
-             "film": sum(r.film_milliseconds for r in reports)}
+    stage = {"regenerate": staged.regenerate_milliseconds, "trace": staged.intersect_milliseconds,
+             "shade": staged.shade_milliseconds, "occlude": staged.occlude_milliseconds,
+             "film": staged.film_milliseconds}
 
     # e2e: the public C-ABI call with host film buffers (copies in the timed region)
+    options.instrumentation = 0
     host_film = np.zeros((height, width, 4), np.float32)
     host_counts = np.zeros((height, width), np.uint64)
     h2d = host_film.nbytes + host_counts.nbytes
@@ -302,12 +314,11 @@ def main():
     # around the stage's launches on the wavefront stream, summed by the library per iteration)
     peak, peak_kind = measured_peaks()
     dominant = max(("trace", "shade", "occlude"), key=lambda k: stage[k])
-    per_launch_ms = stage[dominant] / max(1, iterations)
-    units = shadow if dominant == "occlude" else ext
-    bytes_total = STAGE_BYTES_PER_UNIT[dominant] * units
-    bytes_per_launch = bytes_total / max(1, iterations)
+    per_launch_ms = stage[dominant] / max(1, staged.iterations)
+    units = staged.shadow_segments if dominant == "occlude" else staged.extension_segments
+    bytes_per_launch = STAGE_BYTES_PER_UNIT[dominant] * units / max(1, staged.iterations)
     achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
-    units_per_launch = units / max(1, iterations)
+    units_per_launch = units / max(1, staged.iterations)
     traffic_per_unit = MEASURED_TRAFFIC_PER_UNIT.get(dominant)
     traffic = traffic_per_unit * units_per_launch if traffic_per_unit is not None else None
     whole_bytes = (CAMERA_RAY_BYTES * paths_per_step * args.steps + EXTENSION_SEGMENT_BYTES * ext +
@@ -323,7 +334,7 @@ def main():
                    "parallelism": f"sample-partitioned x{world}" if world > 1 else "single GPU"},
         "rays_per_s": (ext + shadow) / (total_ms / 1000.0) * (world if distributed else 1),
         "segments": {"extension": ext, "shadow": shadow, "iterations": iterations},
-        "stage_ms": stage, "failed_lanes": failed,
+        "stage_ms_one_frame": stage, "failed_lanes": failed,
         "clocks": clocks.summary(),
         "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d},

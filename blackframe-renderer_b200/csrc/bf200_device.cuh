@@ -21,7 +21,7 @@ struct alignas(16) BvhNode {
 
 constexpr int kLeafCountBits = 3;
 constexpr int kMaxLeafSize = 1 << kLeafCountBits;
-constexpr int kTraversalStack = 64;
+constexpr int kTraversalStack = 128;  // instance entries of one ray plus one BLAS path
 
 struct LightInfo {
     uint32_t instance;
@@ -37,6 +37,7 @@ struct LightInfo {
 struct SceneView {
     uint32_t instance_count;
     uint32_t light_count;
+    const float4* inst_world_box;  // padded world box per instance: lo (xyz, w = visibility mask bits), hi
     const float4* inst_to_object;  // 3 rows (m0..m3) per instance
     const float4* inst_to_world;   // 3 rows per instance
     const uint4* inst_info;        // geometry, material, visibility mask, light index or ~0

@@ -36,6 +36,13 @@ struct bf200_context {
     void* arena = nullptr;
     Wavefront w{};
     unsigned long long* pinned_counters = nullptr;
+    // grow-only workspaces of the film and batch entry points, kept across calls
+    void* film_radiance = nullptr;  // per-path radiance of one film chunk, then the skipped counter
+    size_t film_radiance_bytes = 0;
+    void* film_staging = nullptr;   // device copy of a host film
+    size_t film_staging_bytes = 0;
+    void* batch_staging = nullptr;  // device copies of host path inputs and results
+    size_t batch_staging_bytes = 0;
 };
 
 struct bf200_scene {
@@ -71,6 +78,25 @@ F3 transform_point_h(const float* m, F3 p) {  // Transforms.hpp:93-101
 
 // SceneSurfaceInteraction.cpp:204-250 (transform_orientation): sign of the upper 3x3
 // determinant by partial-pivot elimination in double.
+// Grows a context workspace to at least `need` bytes (contents are not kept).
+blackframe_status grow_workspace(bf200_context* c, void** buffer, size_t* have, size_t need, const char* what) {
+    if (need <= *have && *buffer != nullptr) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    if (*buffer != nullptr) {
+        cudaFree(*buffer);
+        *buffer = nullptr;
+        *have = 0;
+    }
+    const cudaError_t e = cudaMalloc(buffer, need);
+    if (e != cudaSuccess) {
+        *buffer = nullptr;
+        return cuda_fail(c, e, what);
+    }
+    *have = need;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
 bool transform_orientation(const float* m4, int& orientation) {
     double m[9];
     for (int r = 0; r < 3; ++r) {
@@ -300,6 +326,50 @@ uint32_t build_blas(const bf200_scene_desc_v1& d, uint32_t g, std::vector<BvhNod
     const int r = b.build(0, static_cast<int>(prims.size()), 1);
     depth = b.max_depth;
     return static_cast<uint32_t>(r);
+}
+
+// Rounds a double down (dir < 0) or up (dir > 0) to a float.
+float round_outward(double x, int dir) {
+    float f = static_cast<float>(x);
+    if (dir < 0 && static_cast<double>(f) > x) {
+        f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+    }
+    if (dir > 0 && static_cast<double>(f) < x) {
+        f = std::nextafter(f, std::numeric_limits<float>::infinity());
+    }
+    return f;
+}
+
+// World box of an instance: the object box's eight corners through object_to_world in double,
+// padded by 1e-4 of the box's largest coordinate magnitude. Triangles are tested against the
+// object-space ray, whose transform rounding moves it by a few ulps of those magnitudes; the pad
+// is thousands of times larger, so a world-space cull never drops an instance the object-space
+// test would hit.
+Box instance_world_box(const Box& object, const float* m4) {
+    double lo[3] = {std::numeric_limits<double>::infinity(), std::numeric_limits<double>::infinity(),
+                    std::numeric_limits<double>::infinity()};
+    double hi[3] = {-lo[0], -lo[1], -lo[2]};
+    for (int corner = 0; corner < 8; ++corner) {
+        const double p[3] = {(corner & 1) ? object.hi[0] : object.lo[0], (corner & 2) ? object.hi[1] : object.lo[1],
+                             (corner & 4) ? object.hi[2] : object.lo[2]};
+        for (int r = 0; r < 3; ++r) {
+            const double w = double(m4[4 * r]) * p[0] + double(m4[4 * r + 1]) * p[1] + double(m4[4 * r + 2]) * p[2] +
+                             double(m4[4 * r + 3]);
+            lo[r] = std::min(lo[r], w);
+            hi[r] = std::max(hi[r], w);
+        }
+    }
+    double scale = 0.0;
+    for (int r = 0; r < 3; ++r) {
+        scale = std::max(scale, std::max(std::fabs(lo[r]), std::fabs(hi[r])));
+    }
+    const double pad = 1e-4 * scale + 1e-30;
+    Box b;
+    for (int r = 0; r < 3; ++r) {
+        b.lo[r] = round_outward(lo[r] - pad, -1);
+        b.hi[r] = round_outward(hi[r] + pad, 1);
+    }
+    return b;
 }
 
 template <typename T> blackframe_status upload(bf200_scene* s, const std::vector<T>& host, const T*& out) {
@@ -834,6 +904,11 @@ BF200_EXPORT blackframe_status bf200_context_destroy(bf200_context* c) noexcept 
     if (c->pinned_counters != nullptr) {
         cudaFreeHost(c->pinned_counters);
     }
+    for (void* p : {c->film_radiance, c->film_staging, c->batch_staging}) {
+        if (p != nullptr) {
+            cudaFree(p);
+        }
+    }
     delete c;
     return BLACKFRAME_STATUS_SUCCESS;
 }
@@ -859,13 +934,32 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         std::vector<BvhNode> nodes;
         std::vector<float4> leaf_tris;
         std::vector<uint4> geom_info(d->geometry_count);
+        std::vector<Box> object_box(d->geometry_count);
+        uint32_t blas_depth = 0;
         for (uint32_t g = 0; g < d->geometry_count; ++g) {
             uint32_t depth = 0;
             const uint32_t root = build_blas(*d, g, nodes, leaf_tris, depth);
-            if (depth + 2 >= kTraversalStack) {
-                return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "BLAS deeper than the traversal stack");
-            }
+            blas_depth = std::max(blas_depth, depth);
             geom_info[g] = make_uint4(d->geometries[g].vertex_offset, d->geometries[g].triangle_offset, root, 0);
+            const auto& geom = d->geometries[g];
+            const uint32_t* local = d->triangles + 3ULL * geom.triangle_offset;
+            for (uint32_t t = 0; t < 3 * geom.triangle_count; ++t) {
+                object_box[g].grow(d->positions + 3ULL * (geom.vertex_offset + local[t]));
+            }
+        }
+        // the traversal stack holds every instance entry of a ray plus one BLAS walk
+        if (static_cast<uint64_t>(d->instance_count) + blas_depth + 2 >= kTraversalStack) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE,
+                        "instance count plus BLAS depth exceeds the traversal stack (128 entries)");
+        }
+        // instance level: the padded world box of every instance, tested before its ray transform
+        std::vector<float4> world_box(2ULL * d->instance_count);
+        for (uint32_t i = 0; i < d->instance_count; ++i) {
+            const Box b = instance_world_box(object_box[d->instances[i].geometry_index],
+                                             d->instances[i].object_to_world);
+            world_box[2ULL * i] = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.0F);
+            std::memcpy(&world_box[2ULL * i].w, &d->instances[i].visibility_mask, 4);  // mask bits, not a number
+            world_box[2ULL * i + 1] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.0F);
         }
         scene->node_count = nodes.size();
         scene->triangle_count = leaf_tris.size() / 3;
@@ -970,6 +1064,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         up(to_world, v.inst_to_world);
         up(inst_info, v.inst_info);
         up(inst_route, v.inst_route);
+        up(world_box, v.inst_world_box);
         up(normal_offset, v.inst_normal_offset);
         up(geom_info, v.geom_info);
         up(positions, v.positions);
@@ -1248,16 +1343,16 @@ BF200_EXPORT blackframe_status bf200_trace_paths(bf200_context* c, const bf200_s
         return bf200_trace_paths_device(c, s, nullptr, 0, o, nullptr, report);
     }
     cudaSetDevice(c->device);
-    bf200_path_input_v1* d_in = nullptr;
-    bf200_path_result_v1* d_out = nullptr;
-    cudaError_t e = cudaMalloc(&d_in, path_count * sizeof(bf200_path_input_v1));
-    if (e == cudaSuccess) {
-        e = cudaMalloc(&d_out, path_count * sizeof(bf200_path_result_v1));
+    const size_t in_bytes = path_count * sizeof(bf200_path_input_v1);
+    const size_t in_span = (in_bytes + 255) & ~size_t(255);
+    if (const auto st = grow_workspace(c, &c->batch_staging, &c->batch_staging_bytes,
+                                       in_span + path_count * sizeof(bf200_path_result_v1), "batch staging");
+        st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
     }
-    if (e == cudaSuccess) {
-        e = cudaMemcpyAsync(d_in, inputs, path_count * sizeof(bf200_path_input_v1), cudaMemcpyHostToDevice,
-                            c->stream);
-    }
+    auto* d_in = static_cast<bf200_path_input_v1*>(c->batch_staging);
+    auto* d_out = reinterpret_cast<bf200_path_result_v1*>(static_cast<char*>(c->batch_staging) + in_span);
+    cudaError_t e = cudaMemcpyAsync(d_in, inputs, in_bytes, cudaMemcpyHostToDevice, c->stream);
     blackframe_status st = e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "batch upload");
     if (st == BLACKFRAME_STATUS_SUCCESS) {
         st = bf200_trace_paths_device(c, s, d_in, path_count, o, d_out, report);
@@ -1272,8 +1367,6 @@ BF200_EXPORT blackframe_status bf200_trace_paths(bf200_context* c, const bf200_s
             st = cuda_fail(c, e, "batch download");
         }
     }
-    cudaFree(d_in);
-    cudaFree(d_out);
     return st;
 }
 
@@ -1308,18 +1401,17 @@ BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const 
     const uint64_t max_chunk_paths = 1ULL << 26;
     uint64_t samples_per_chunk = std::max<uint64_t>(1, max_chunk_paths / pixels);
     samples_per_chunk = std::min<uint64_t>(samples_per_chunk, req->samples_per_pixel);
-    float4* radiance = nullptr;
-    unsigned long long* skipped = nullptr;
-    cudaError_t e = cudaMalloc(&radiance, std::max<uint64_t>(1, samples_per_chunk * pixels) * sizeof(float4));
-    if (e == cudaSuccess) {
-        e = cudaMalloc(&skipped, sizeof(unsigned long long));
+    const size_t radiance_bytes = std::max<uint64_t>(1, samples_per_chunk * pixels) * sizeof(float4);
+    if (const auto st = grow_workspace(c, &c->film_radiance, &c->film_radiance_bytes, radiance_bytes + 256,
+                                       "film chunk workspace");
+        st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
     }
-    if (e == cudaSuccess) {
-        e = cudaMemsetAsync(skipped, 0, sizeof(unsigned long long), c->stream);
-    }
+    auto* radiance = static_cast<float4*>(c->film_radiance);
+    auto* skipped = reinterpret_cast<unsigned long long*>(static_cast<char*>(c->film_radiance) + radiance_bytes);
+    cudaError_t e = cudaMemsetAsync(skipped, 0, sizeof(unsigned long long), c->stream);
     if (e != cudaSuccess) {
-        cudaFree(radiance);
-        return cuda_fail(c, e, "film chunk allocation");
+        return cuda_fail(c, e, "film chunk workspace");
     }
     const TransportParams params = make_params(*o);
     blackframe_status st = BLACKFRAME_STATUS_SUCCESS;
@@ -1386,8 +1478,6 @@ BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const 
             st = cuda_fail(c, e, "film synchronisation");
         }
     }
-    cudaFree(radiance);
-    cudaFree(skipped);
     return st;
 }
 
@@ -1401,15 +1491,15 @@ BF200_EXPORT blackframe_status bf200_render_film(bf200_context* c, const bf200_s
     cudaSetDevice(c->device);
     const uint64_t pixels = static_cast<uint64_t>(host_film->width) * host_film->height;
     const size_t sum_bytes = pixels * (host_film->precision == 0 ? 16 : 64);
-    void* d_sums = nullptr;
-    uint64_t* d_counts = nullptr;
-    cudaError_t e = cudaMalloc(&d_sums, std::max<size_t>(16, sum_bytes));
-    if (e == cudaSuccess) {
-        e = cudaMalloc(&d_counts, std::max<size_t>(8, pixels * 8));
+    const size_t sum_span = (std::max<size_t>(16, sum_bytes) + 255) & ~size_t(255);
+    if (const auto st = grow_workspace(c, &c->film_staging, &c->film_staging_bytes,
+                                       sum_span + std::max<size_t>(8, pixels * 8), "film staging");
+        st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
     }
-    if (e == cudaSuccess) {
-        e = cudaMemcpyAsync(d_sums, host_film->sums, sum_bytes, cudaMemcpyHostToDevice, c->stream);
-    }
+    void* d_sums = c->film_staging;
+    auto* d_counts = reinterpret_cast<uint64_t*>(static_cast<char*>(c->film_staging) + sum_span);
+    cudaError_t e = cudaMemcpyAsync(d_sums, host_film->sums, sum_bytes, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) {
         e = cudaMemcpyAsync(d_counts, host_film->sample_counts, pixels * 8, cudaMemcpyHostToDevice, c->stream);
     }
@@ -1432,8 +1522,6 @@ BF200_EXPORT blackframe_status bf200_render_film(bf200_context* c, const bf200_s
             st = cuda_fail(c, e, "film download");
         }
     }
-    cudaFree(d_sums);
-    cudaFree(d_counts);
     return st;
 }
 

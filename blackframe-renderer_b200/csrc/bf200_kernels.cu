@@ -383,8 +383,50 @@ __device__ __forceinline__ bool precedes(float t, uint32_t inst, uint32_t prim, 
     return prim < best.primitive;
 }
 
-// Closest hit over every visible instance (committed order) and its BLAS; ties keep the hit
-// that comes first in (instance, primitive) order, as the analytic accel's in-order scan does.
+// Children of a node whose boxes the ray meets within [t_min, limit], the nearer one first.
+__device__ __forceinline__ int hit_children(const RayInv& r, const BvhNode& node, float t_min, float limit,
+                                            int (&kids)[2]) {
+    float n0, n1;
+    const bool h0 = slab(r, node.a.x, node.a.y, node.a.z, node.a.w, node.c.x, node.c.y, t_min, limit, n0);
+    const bool h1 = slab(r, node.b.x, node.b.y, node.b.z, node.b.w, node.c.z, node.c.w, t_min, limit, n1);
+    if (h0 && h1) {
+        const bool swap = n1 < n0;
+        kids[0] = swap ? node.d.y : node.d.x;
+        kids[1] = swap ? node.d.x : node.d.y;
+        return 2;
+    }
+    kids[0] = h0 ? node.d.x : node.d.y;
+    return h0 || h1 ? 1 : 0;
+}
+
+// Instance level of both traversals: every visible instance whose padded world box the ray meets
+// within [t_min, t_max] goes onto the stack as ~instance, the lowest index on top. All lanes of a
+// warp run this pass in step. Returns false when the stack is full.
+__device__ __forceinline__ bool push_instances(const SceneView& s, const RayInv& world, float t_min, float t_max,
+                                               uint32_t mask, TraversalStack& stack, int& sp) {
+    for (int inst = static_cast<int>(s.instance_count) - 1; inst >= 0; --inst) {
+        const float4 blo = s.inst_world_box[2 * inst], bhi = s.inst_world_box[2 * inst + 1];
+        float near;
+        if (!slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, t_max, near) ||
+            (mask & __float_as_uint(blo.w)) == 0U) {
+            continue;
+        }
+        if (sp >= kTraversalStack) {
+            return false;
+        }
+        stack.set(sp++, ~inst);
+    }
+    return true;
+}
+
+// Closest hit over the instances and their BLAS. After the instance pass, one loop serves both
+// levels, so lanes at different levels still run the same loop body: popping ~instance re-tests
+// the instance's world box against the current closest t, transforms the ray into object space and
+// pushes the BLAS root above the remaining instance entries; BLAS nodes are tested against that
+// object-space ray, and BLAS leaves (negative children) are tested when met. Ties keep the hit that
+// comes first in (instance, primitive) order, as the analytic accel's in-order scan does; boxes are
+// culled only when they start strictly beyond the current closest t, so neither the order nor the
+// culling changes the winner.
 __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
                                      TraversalStack& stack) {
     ClosestResult best;
@@ -394,76 +436,69 @@ __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min
     best.leaf = 0xFFFFFFFFU;
     best.failed = false;
     bool found = false;
-    for (uint32_t inst = 0; inst < s.instance_count; ++inst) {
-        const uint4 info = s.inst_info[inst];
-        if ((mask & info.z) == 0U) {
+    const RayInv world = make_ray_inv(o, d);
+    int sp = 0;
+    if (!push_instances(s, world, t_min, t_max, mask, stack, sp)) {
+        best.failed = true;
+    }
+    RayInv r = world;
+    F3 ro = o, rd = d;
+    uint32_t inst = 0xFFFFFFFFU;
+    while (sp > 0) {
+        const int entry = stack.get(--sp);
+        const float limit = found ? best.t : t_max;
+        if (entry < 0) {
+            inst = static_cast<uint32_t>(~entry);
+            const float4 blo = s.inst_world_box[2ULL * inst], bhi = s.inst_world_box[2ULL * inst + 1];
+            float near;
+            if (!slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, limit, near)) {
+                continue;
+            }
+            const float4* m = s.inst_to_object + 3ULL * inst;
+            ro = xform_point(m, o);
+            rd = xform_vector(m, d);
+            r = make_ray_inv(ro, rd);
+            stack.set(sp++, static_cast<int>(s.geom_info[s.inst_info[inst].x].z));
             continue;
         }
-        const float4* m = s.inst_to_object + 3ULL * inst;
-        const F3 lo = xform_point(m, o);
-        const F3 ld = xform_vector(m, d);
-        const RayInv r = make_ray_inv(lo, ld);
-        const uint4 geom = s.geom_info[info.x];
-        int sp = 0;
-        stack.set(sp++, static_cast<int>(geom.z));
-        while (sp > 0) {
-            const int node_index = stack.get(--sp);
-            const BvhNode node = s.nodes[node_index];
-            const float limit = found ? best.t : t_max;
-            float n0, n1;
-            const bool h0 = slab(r, node.a.x, node.a.y, node.a.z, node.a.w, node.c.x, node.c.y, t_min, limit, n0);
-            const bool h1 = slab(r, node.b.x, node.b.y, node.b.z, node.b.w, node.c.z, node.c.w, t_min, limit, n1);
-            int children[2];
-            int count = 0;
-            if (h0 && h1) {
-                const bool swap = n1 < n0;
-                children[0] = swap ? node.d.y : node.d.x;
-                children[1] = swap ? node.d.x : node.d.y;
-                count = 2;
-            } else if (h0) {
-                children[0] = node.d.x;
-                count = 1;
-            } else if (h1) {
-                children[0] = node.d.y;
-                count = 1;
+        int kids[2];
+        const int count = hit_children(r, s.nodes[entry], t_min, limit, kids);
+        // far child first onto the stack so the near one is visited next
+        for (int k = count - 1; k >= 0; --k) {
+            const int child = kids[k];
+            if (child >= 0) {
+                if (sp < kTraversalStack) {
+                    stack.set(sp++, child);
+                } else {
+                    best.failed = true;
+                }
+                continue;
             }
-            // push far child first so the near one is visited next
-            for (int k = count - 1; k >= 0; --k) {
-                const int child = children[k];
-                if (child >= 0) {
-                    if (sp < kTraversalStack) {
-                        stack.set(sp++, child);
-                    } else {
-                        best.failed = true;
-                    }
+            const uint32_t packed = static_cast<uint32_t>(~child);
+            const uint32_t first = packed >> kLeafCountBits;
+            const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
+            for (uint32_t j = 0; j < n; ++j) {
+                const uint32_t leaf = first + j;
+                const float4 v0 = s.leaf_tris[3ULL * leaf];
+                const float4 v1 = s.leaf_tris[3ULL * leaf + 1];
+                const float4 v2 = s.leaf_tris[3ULL * leaf + 2];
+                TriangleHit th;
+                const float cur_limit = found ? best.t : t_max;
+                const int res = triangle_test(v0, v1, v2, ro, rd, t_min, cur_limit, false, th);
+                if (res == kTriFailure) {
+                    best.failed = true;
                     continue;
                 }
-                const uint32_t packed = static_cast<uint32_t>(~child);
-                const uint32_t first = packed >> kLeafCountBits;
-                const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
-                for (uint32_t j = 0; j < n; ++j) {
-                    const uint32_t leaf = first + j;
-                    const float4 v0 = s.leaf_tris[3ULL * leaf];
-                    const float4 v1 = s.leaf_tris[3ULL * leaf + 1];
-                    const float4 v2 = s.leaf_tris[3ULL * leaf + 2];
-                    TriangleHit th;
-                    const float cur_limit = found ? best.t : t_max;
-                    const int res = triangle_test(v0, v1, v2, lo, ld, t_min, cur_limit, false, th);
-                    if (res == kTriFailure) {
-                        best.failed = true;
-                        continue;
-                    }
-                    if (res != kTriHit) {
-                        continue;
-                    }
-                    const uint32_t prim = __float_as_uint(v0.w);
-                    if (!found || precedes(th.t, inst, prim, best)) {
-                        best.t = th.t;
-                        best.instance = inst;
-                        best.primitive = prim;
-                        best.leaf = leaf;
-                        found = true;
-                    }
+                if (res != kTriHit) {
+                    continue;
+                }
+                const uint32_t prim = __float_as_uint(v0.w);
+                if (!found || precedes(th.t, inst, prim, best)) {
+                    best.t = th.t;
+                    best.instance = inst;
+                    best.primitive = prim;
+                    best.leaf = leaf;
+                    found = true;
                 }
             }
         }
@@ -474,57 +509,54 @@ __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min
     return best;
 }
 
-// Any hit in [t_min, t_max] (AccelBackend.cpp:114-147). Returns 1 occluded, 0 clear, -1 failure.
+// Any hit in [t_min, t_max] (AccelBackend.cpp:114-147), walked like closest_hit. Returns 1
+// occluded, 0 clear, -1 failure.
 __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
                        TraversalStack& stack) {
     bool failed = false;
-    for (uint32_t inst = 0; inst < s.instance_count; ++inst) {
-        const uint4 info = s.inst_info[inst];
-        if ((mask & info.z) == 0U) {
+    const RayInv world = make_ray_inv(o, d);
+    int sp = 0;
+    if (!push_instances(s, world, t_min, t_max, mask, stack, sp)) {
+        failed = true;
+    }
+    RayInv r = world;
+    F3 ro = o, rd = d;
+    while (sp > 0) {
+        const int entry = stack.get(--sp);
+        if (entry < 0) {
+            const uint32_t inst = static_cast<uint32_t>(~entry);
+            const float4* m = s.inst_to_object + 3ULL * inst;
+            ro = xform_point(m, o);
+            rd = xform_vector(m, d);
+            r = make_ray_inv(ro, rd);
+            stack.set(sp++, static_cast<int>(s.geom_info[s.inst_info[inst].x].z));
             continue;
         }
-        const float4* m = s.inst_to_object + 3ULL * inst;
-        const F3 lo = xform_point(m, o);
-        const F3 ld = xform_vector(m, d);
-        const RayInv r = make_ray_inv(lo, ld);
-        const uint4 geom = s.geom_info[info.x];
-        int sp = 0;
-        stack.set(sp++, static_cast<int>(geom.z));
-        while (sp > 0) {
-            const int node_index = stack.get(--sp);
-            const BvhNode node = s.nodes[node_index];
-            float n0, n1;
-            const bool h0 = slab(r, node.a.x, node.a.y, node.a.z, node.a.w, node.c.x, node.c.y, t_min, t_max, n0);
-            const bool h1 = slab(r, node.b.x, node.b.y, node.b.z, node.b.w, node.c.z, node.c.w, t_min, t_max, n1);
-            const int kids[2] = {h0 ? node.d.x : 0, h1 ? node.d.y : 0};
-            const bool hits[2] = {h0, h1};
-            for (int k = 0; k < 2; ++k) {
-                if (!hits[k]) {
-                    continue;
+        int kids[2];
+        const int count = hit_children(r, s.nodes[entry], t_min, t_max, kids);
+        for (int k = 0; k < count; ++k) {
+            const int child = kids[k];
+            if (child >= 0) {
+                if (sp < kTraversalStack) {
+                    stack.set(sp++, child);
+                } else {
+                    failed = true;
                 }
-                const int child = kids[k];
-                if (child >= 0) {
-                    if (sp < kTraversalStack) {
-                        stack.set(sp++, child);
-                    } else {
-                        failed = true;
-                    }
-                    continue;
+                continue;
+            }
+            const uint32_t packed = static_cast<uint32_t>(~child);
+            const uint32_t first = packed >> kLeafCountBits;
+            const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
+            for (uint32_t j = 0; j < n; ++j) {
+                const uint32_t leaf = first + j;
+                TriangleHit th;
+                const int res = triangle_test(s.leaf_tris[3ULL * leaf], s.leaf_tris[3ULL * leaf + 1],
+                                              s.leaf_tris[3ULL * leaf + 2], ro, rd, t_min, t_max, false, th);
+                if (res == kTriHit) {
+                    return 1;
                 }
-                const uint32_t packed = static_cast<uint32_t>(~child);
-                const uint32_t first = packed >> kLeafCountBits;
-                const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
-                for (uint32_t j = 0; j < n; ++j) {
-                    const uint32_t leaf = first + j;
-                    TriangleHit th;
-                    const int res = triangle_test(s.leaf_tris[3ULL * leaf], s.leaf_tris[3ULL * leaf + 1],
-                                                  s.leaf_tris[3ULL * leaf + 2], lo, ld, t_min, t_max, false, th);
-                    if (res == kTriHit) {
-                        return 1;
-                    }
-                    if (res == kTriFailure) {
-                        failed = true;
-                    }
+                if (res == kTriFailure) {
+                    failed = true;
                 }
             }
         }
