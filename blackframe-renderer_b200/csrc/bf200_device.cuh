@@ -21,7 +21,7 @@ struct alignas(16) BvhNode {
 
 constexpr int kLeafCountBits = 3;
 constexpr int kMaxLeafSize = 1 << kLeafCountBits;
-constexpr int kTraversalStack = 128;  // instance entries of one ray plus one BLAS path
+constexpr int kTraversalStack = 96;  // up to 32 instance entries plus one BLAS path
 
 struct LightInfo {
     uint32_t instance;
@@ -135,7 +135,7 @@ struct Wavefront {
     uint32_t* tile_counts;     // compaction scratch: kCompactMaxRoutes x tiles
     // counters: [0] shadow queue size, [1] next path to claim, [2] active slots,
     //           [3] extension segments, [4] shadow segments, [5] failed lanes,
-    //           [6] first failure path (min), [7] first failure code
+    //           [6] first failure path (min), [7] first failure code, [8] k_trace fetch cursor
     unsigned long long* counters;
 };
 

@@ -579,7 +579,7 @@ size_t carve_wavefront(char* base, uint32_t capacity, Wavefront* out) {
     w.tile_counts = reinterpret_cast<uint32_t*>(take(4 * kCompactMaxRoutes * (tiles == 0 ? 1 : tiles)));
     w.route_offsets = reinterpret_cast<uint32_t*>(take(4 * (kRouteCount + 1)));
     w.shadow_offsets = reinterpret_cast<uint32_t*>(take(4 * 2));
-    w.counters = reinterpret_cast<unsigned long long*>(take(8 * sizeof(unsigned long long)));
+    w.counters = reinterpret_cast<unsigned long long*>(take(16 * sizeof(unsigned long long)));
     if (out != nullptr) {
         *out = w;
     }
@@ -947,10 +947,13 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
                 object_box[g].grow(d->positions + 3ULL * (geom.vertex_offset + local[t]));
             }
         }
-        // the traversal stack holds every instance entry of a ray plus one BLAS walk
-        if (static_cast<uint64_t>(d->instance_count) + blas_depth + 2 >= kTraversalStack) {
-            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE,
-                        "instance count plus BLAS depth exceeds the traversal stack (128 entries)");
+        // the traversal stack holds one instance-range entry plus one BLAS walk; instance ranges
+        // carry 15-bit indices
+        if (blas_depth + 3 + 32 >= kTraversalStack) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "BLAS deeper than the traversal stack allows");
+        }
+        if (d->instance_count >= (1U << 15)) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "more than 32767 instances");
         }
         // instance level: the padded world box of every instance, tested before its ray transform
         std::vector<float4> world_box(2ULL * d->instance_count);
@@ -963,6 +966,10 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         }
         scene->node_count = nodes.size();
         scene->triangle_count = leaf_tris.size() / 3;
+        // leaf codes must stay inside their traversal-stack tag range (first leaf triangle < 2^27)
+        if (scene->triangle_count >= (1ULL << 27) || nodes.size() >= (1ULL << 30)) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "scene exceeds 2^27 triangles or 2^30 BVH nodes");
+        }
         // instances, mesh lights (FrameScene.cpp:201-261) and the uniform light sampler
         std::vector<float4> to_object(3ULL * d->instance_count), to_world(3ULL * d->instance_count);
         std::vector<uint4> inst_info(d->instance_count);

@@ -16,6 +16,8 @@
 // operation for operation; this file is compiled with -fmad=false.
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include "bf200_device.cuh"
 #include "bf200_kernels.h"
 
@@ -399,132 +401,218 @@ __device__ __forceinline__ int hit_children(const RayInv& r, const BvhNode& node
     return h0 || h1 ? 1 : 0;
 }
 
-// Instance level of both traversals: every visible instance whose padded world box the ray meets
-// within [t_min, t_max] goes onto the stack as ~instance, the lowest index on top. All lanes of a
-// warp run this pass in step. Returns false when the stack is full.
-__device__ __forceinline__ bool push_instances(const SceneView& s, const RayInv& world, float t_min, float t_max,
+// Stack entries of both traversals: a BLAS node index (>= 0), a BLAS leaf (the node's child code,
+// in [-2^30, 0): ~child = first_leaf_triangle << 3 | (count - 1)), or an instance range
+// (kInstanceEntry + (first << 15 | count), below -2^30): the instances [first, first + count)
+// still to visit, in index order. One entry stands for all instances, so starting a ray costs
+// one push, and each instance's world box is tested when its turn comes.
+constexpr int kInstanceEntry = INT_MIN;
+constexpr int kLeafEntryMin = -(1 << 30);
+constexpr int kInstanceBits = 15;
+// Scenes with at most this many instances test every instance box up front in any_hit.
+constexpr uint32_t kEagerInstances = 32;
+
+__device__ __forceinline__ int instance_range(uint32_t first, uint32_t count) {
+    return kInstanceEntry + static_cast<int>((first << kInstanceBits) | count);
+}
+
+// Starts a walk's stack. With few instances every visible instance whose world box the ray meets
+// within [t_min, t_max] goes on as a one-instance range, the lowest index on top, with the warp in
+// step; otherwise one range entry stands for all instances and their boxes are tested as they come.
+__device__ __forceinline__ void push_instances(const SceneView& s, const RayInv& world, float t_min, float t_max,
                                                uint32_t mask, TraversalStack& stack, int& sp) {
+    if (s.instance_count > kEagerInstances) {
+        stack.set(sp++, instance_range(0U, s.instance_count));
+        return;
+    }
     for (int inst = static_cast<int>(s.instance_count) - 1; inst >= 0; --inst) {
         const float4 blo = s.inst_world_box[2 * inst], bhi = s.inst_world_box[2 * inst + 1];
         float near;
-        if (!slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, t_max, near) ||
-            (mask & __float_as_uint(blo.w)) == 0U) {
+        if ((mask & __float_as_uint(blo.w)) == 0U ||
+            !slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, t_max, near)) {
             continue;
         }
-        if (sp >= kTraversalStack) {
-            return false;
+        stack.set(sp++, instance_range(static_cast<uint32_t>(inst), 1U));
+    }
+}
+
+// Per-lane walk state shared by the two traversals.
+struct Walk {
+    RayInv r;       // current ray (object space of the current instance)
+    F3 ro, rd;
+    uint32_t inst;  // current instance
+    int sp;
+    bool failed;
+};
+
+// Advances the walk until this lane holds a leaf (returned, in [-2^30, 0)) or its stack is empty
+// (returns 0). An instance range yields its first instance: skipped when the ray's visibility mask
+// excludes it or its world box is not met within [t_min, limit], otherwise the ray moves into its
+// object space and its BLAS root is pushed above the rest of the range. Children are pushed far
+// first, so the nearer one comes next.
+__device__ __forceinline__ int next_leaf(const SceneView& s, const RayInv& world, F3 o, F3 d, float t_min,
+                                         float limit, uint32_t mask, TraversalStack& stack, Walk& w) {
+    while (w.sp > 0) {
+        const int entry = stack.get(--w.sp);
+        if (entry < kLeafEntryMin) {
+            const uint32_t code = static_cast<uint32_t>(entry - kInstanceEntry);
+            const uint32_t inst = code >> kInstanceBits, count = code & ((1U << kInstanceBits) - 1U);
+            if (count > 1U) {
+                stack.set(w.sp++, instance_range(inst + 1U, count - 1U));
+            }
+            const float4 blo = s.inst_world_box[2ULL * inst], bhi = s.inst_world_box[2ULL * inst + 1];
+            float near;
+            if ((mask & __float_as_uint(blo.w)) == 0U ||
+                !slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, limit, near)) {
+                continue;
+            }
+            if (w.sp >= kTraversalStack) {
+                w.failed = true;
+                continue;
+            }
+            w.inst = inst;
+            const float4* m = s.inst_to_object + 3ULL * inst;
+            w.ro = xform_point(m, o);
+            w.rd = xform_vector(m, d);
+            w.r = make_ray_inv(w.ro, w.rd);
+            stack.set(w.sp++, static_cast<int>(s.geom_info[s.inst_info[inst].x].z));
+            continue;
         }
-        stack.set(sp++, ~inst);
+        if (entry < 0) {
+            return entry;
+        }
+        int kids[2];
+        const int count = hit_children(w.r, s.nodes[entry], t_min, limit, kids);
+        for (int k = count - 1; k >= 0; --k) {
+            if (w.sp < kTraversalStack) {
+                stack.set(w.sp++, kids[k]);
+            } else {
+                w.failed = true;
+            }
+        }
+    }
+    return 0;
+}
+
+// Closest-hit walk of one ray, in steps. closest_begin pushes the instance entries; each
+// closest_step advances the lane through nodes and instance entries to its next leaf ("while-
+// while": the warp reconverges before the leaf) and runs the exact triangle tests of that leaf;
+// it returns false once the ray's stack is empty. Ties keep the hit that comes first in
+// (instance, primitive) order, as the analytic accel's in-order scan does; boxes are culled only
+// when they start strictly beyond the current closest t, so neither the order nor the culling
+// changes the winner.
+struct ClosestWalk {
+    F3 o, d;
+    float t_min, t_max;
+    uint32_t mask;
+    RayInv world;
+    Walk w;
+    ClosestResult best;
+    bool found;
+};
+
+__device__ __forceinline__ void closest_begin(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
+                                              uint32_t mask, TraversalStack& stack, ClosestWalk& c) {
+    c.o = o;
+    c.d = d;
+    c.t_min = t_min;
+    c.t_max = t_max;
+    c.mask = mask;
+    c.world = make_ray_inv(o, d);
+    c.w = Walk{c.world, o, d, 0xFFFFFFFFU, 0, false};
+    c.best.t = t_max;
+    c.best.instance = 0xFFFFFFFFU;
+    c.best.primitive = 0xFFFFFFFFU;
+    c.best.leaf = 0xFFFFFFFFU;
+    c.best.failed = false;
+    c.found = false;
+    push_instances(s, c.world, t_min, t_max, mask, stack, c.w.sp);
+}
+
+__device__ __forceinline__ bool closest_step(const SceneView& s, TraversalStack& stack, ClosestWalk& c) {
+    const int leaf_code =
+        next_leaf(s, c.world, c.o, c.d, c.t_min, c.found ? c.best.t : c.t_max, c.mask, stack, c.w);
+    if (leaf_code == 0) {
+        return false;
+    }
+    const uint32_t packed = static_cast<uint32_t>(~leaf_code);
+    const uint32_t first = packed >> kLeafCountBits;
+    const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
+    for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t leaf = first + j;
+        const float4 v0 = s.leaf_tris[3ULL * leaf];
+        const float4 v1 = s.leaf_tris[3ULL * leaf + 1];
+        const float4 v2 = s.leaf_tris[3ULL * leaf + 2];
+        TriangleHit th;
+        const int res =
+            triangle_test(v0, v1, v2, c.w.ro, c.w.rd, c.t_min, c.found ? c.best.t : c.t_max, false, th);
+        if (res == kTriFailure) {
+            c.w.failed = true;
+            continue;
+        }
+        if (res != kTriHit) {
+            continue;
+        }
+        const uint32_t prim = __float_as_uint(v0.w);
+        if (!c.found || precedes(th.t, c.w.inst, prim, c.best)) {
+            c.best.t = th.t;
+            c.best.instance = c.w.inst;
+            c.best.primitive = prim;
+            c.best.leaf = leaf;
+            c.found = true;
+        }
     }
     return true;
 }
 
-// Closest hit over the instances and their BLAS. After the instance pass, one loop serves both
-// levels, so lanes at different levels still run the same loop body: popping ~instance re-tests
-// the instance's world box against the current closest t, transforms the ray into object space and
-// pushes the BLAS root above the remaining instance entries; BLAS nodes are tested against that
-// object-space ray, and BLAS leaves (negative children) are tested when met. Ties keep the hit that
-// comes first in (instance, primitive) order, as the analytic accel's in-order scan does; boxes are
-// culled only when they start strictly beyond the current closest t, so neither the order nor the
-// culling changes the winner.
-__device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
-                                     TraversalStack& stack) {
-    ClosestResult best;
-    best.t = t_max;
-    best.instance = 0xFFFFFFFFU;
-    best.primitive = 0xFFFFFFFFU;
-    best.leaf = 0xFFFFFFFFU;
-    best.failed = false;
-    bool found = false;
-    const RayInv world = make_ray_inv(o, d);
-    int sp = 0;
-    if (!push_instances(s, world, t_min, t_max, mask, stack, sp)) {
-        best.failed = true;
+__device__ __forceinline__ ClosestResult closest_end(ClosestWalk& c) {
+    c.best.failed = c.w.failed;
+    if (!c.found) {
+        c.best.instance = 0xFFFFFFFFU;
     }
-    RayInv r = world;
-    F3 ro = o, rd = d;
-    uint32_t inst = 0xFFFFFFFFU;
-    while (sp > 0) {
-        const int entry = stack.get(--sp);
-        const float limit = found ? best.t : t_max;
-        if (entry < 0) {
-            inst = static_cast<uint32_t>(~entry);
-            const float4 blo = s.inst_world_box[2ULL * inst], bhi = s.inst_world_box[2ULL * inst + 1];
-            float near;
-            if (!slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, limit, near)) {
-                continue;
-            }
-            const float4* m = s.inst_to_object + 3ULL * inst;
-            ro = xform_point(m, o);
-            rd = xform_vector(m, d);
-            r = make_ray_inv(ro, rd);
-            stack.set(sp++, static_cast<int>(s.geom_info[s.inst_info[inst].x].z));
-            continue;
-        }
-        int kids[2];
-        const int count = hit_children(r, s.nodes[entry], t_min, limit, kids);
-        // far child first onto the stack so the near one is visited next
-        for (int k = count - 1; k >= 0; --k) {
-            const int child = kids[k];
-            if (child >= 0) {
-                if (sp < kTraversalStack) {
-                    stack.set(sp++, child);
-                } else {
-                    best.failed = true;
-                }
-                continue;
-            }
-            const uint32_t packed = static_cast<uint32_t>(~child);
-            const uint32_t first = packed >> kLeafCountBits;
-            const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
-            for (uint32_t j = 0; j < n; ++j) {
-                const uint32_t leaf = first + j;
-                const float4 v0 = s.leaf_tris[3ULL * leaf];
-                const float4 v1 = s.leaf_tris[3ULL * leaf + 1];
-                const float4 v2 = s.leaf_tris[3ULL * leaf + 2];
-                TriangleHit th;
-                const float cur_limit = found ? best.t : t_max;
-                const int res = triangle_test(v0, v1, v2, ro, rd, t_min, cur_limit, false, th);
-                if (res == kTriFailure) {
-                    best.failed = true;
-                    continue;
-                }
-                if (res != kTriHit) {
-                    continue;
-                }
-                const uint32_t prim = __float_as_uint(v0.w);
-                if (!found || precedes(th.t, inst, prim, best)) {
-                    best.t = th.t;
-                    best.instance = inst;
-                    best.primitive = prim;
-                    best.leaf = leaf;
-                    found = true;
-                }
-            }
-        }
-    }
-    if (!found) {
-        best.instance = 0xFFFFFFFFU;
-    }
-    return best;
+    return c.best;
 }
 
-// Any hit in [t_min, t_max] (AccelBackend.cpp:114-147), walked like closest_hit. Returns 1
-// occluded, 0 clear, -1 failure.
+// Closest hit of one ray (the standalone query kernel); k_trace runs the same steps with dynamic
+// ray fetch.
+__device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
+                                     TraversalStack& stack) {
+    ClosestWalk c;
+    closest_begin(s, o, d, t_min, t_max, mask, stack, c);
+    while (closest_step(s, stack, c)) {
+    }
+    return closest_end(c);
+}
+
+// Any hit in [t_min, t_max] (AccelBackend.cpp:114-147). One loop serves both levels, and leaves
+// are tested as soon as they are met so a lane stops at its first hit. Returns 1 occluded,
+// 0 clear, -1 failure.
 __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
                        TraversalStack& stack) {
     bool failed = false;
     const RayInv world = make_ray_inv(o, d);
     int sp = 0;
-    if (!push_instances(s, world, t_min, t_max, mask, stack, sp)) {
-        failed = true;
-    }
+    push_instances(s, world, t_min, t_max, mask, stack, sp);
     RayInv r = world;
     F3 ro = o, rd = d;
     while (sp > 0) {
         const int entry = stack.get(--sp);
-        if (entry < 0) {
-            const uint32_t inst = static_cast<uint32_t>(~entry);
+        if (entry < kLeafEntryMin) {
+            const uint32_t code = static_cast<uint32_t>(entry - kInstanceEntry);
+            const uint32_t inst = code >> kInstanceBits, count = code & ((1U << kInstanceBits) - 1U);
+            if (count > 1U) {
+                stack.set(sp++, instance_range(inst + 1U, count - 1U));
+            }
+            const float4 blo = s.inst_world_box[2ULL * inst], bhi = s.inst_world_box[2ULL * inst + 1];
+            float near;
+            if ((mask & __float_as_uint(blo.w)) == 0U ||
+                !slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, t_max, near)) {
+                continue;
+            }
+            if (sp >= kTraversalStack) {
+                failed = true;
+                continue;
+            }
             const float4* m = s.inst_to_object + 3ULL * inst;
             ro = xform_point(m, o);
             rd = xform_vector(m, d);
@@ -729,6 +817,9 @@ __device__ void finish_path(const Wavefront& w, const PathSource& src, uint32_t 
 // ------------------------------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(256) k_regenerate(Wavefront w, PathSource src) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.counters[8] = 0ULL;  // k_trace's fetch cursor for this iteration
+    }
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
     // every thread of a warp runs the same number of iterations so the warp-wide claim below is
@@ -771,44 +862,89 @@ __global__ void __launch_bounds__(256) k_regenerate(Wavefront w, PathSource src)
 // k_trace: closest hit of every active slot's ray; writes the hit and the slot's shading route
 // ------------------------------------------------------------------------------------------------
 
+// Finishes one slot's trace: writes the hit (t and the barycentrics of the winning triangle) or
+// the miss or failure, and the slot's shading route.
+__device__ __forceinline__ void trace_finish(const SceneView& s, const Wavefront& w, uint32_t slot,
+                                             const ClosestResult& c, F3 o, F3 d, float t_min, float t_max) {
+    if (c.failed) {
+        w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneTraversal;
+        w.state[slot] = kSlotDone;
+        w.route[slot] = kRouteNone;
+        return;
+    }
+    if (c.instance == 0xFFFFFFFFU) {
+        w.hit_id[slot] = make_uint2(0xFFFFFFFFU, 0U);
+        w.route[slot] = static_cast<uint8_t>(kRouteGeneric);
+        return;
+    }
+    TriangleHit th;
+    if (!hit_barycentrics(s, c, o, d, t_min, t_max, th)) {
+        w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneNumerical;
+        w.state[slot] = kSlotDone;
+        w.route[slot] = kRouteNone;
+        return;
+    }
+    w.hit_tb[slot] = make_float4(c.t, th.b0, th.b1, th.b2);
+    w.hit_id[slot] = make_uint2(c.instance, c.primitive);
+    w.route[slot] = s.inst_route[c.instance];
+}
+
+// Persistent traversal with dynamic ray fetch: every lane keeps one ray in flight and, when its ray
+// is finished, takes the next slot from a cursor over [0, capacity) (one atomic per warp for all
+// of the warp's idle lanes), so a warp's lanes stay busy instead of waiting for its slowest ray.
+// Slots that are not active are marked unrouted as they are fetched.
 __global__ void __launch_bounds__(256, BF200_INTERSECT_MIN_BLOCKS) k_trace(SceneView s, Wavefront w) {
     __shared__ int stack_columns[kSharedStackEntries * 256];
     TraversalStack stack = thread_stack(stack_columns);
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.capacity; slot += stride) {
-        if (w.state[slot] != kSlotActive) {
-            w.route[slot] = kRouteNone;
+    const uint32_t lane = threadIdx.x & 31U;
+    const uint32_t below = (1U << lane) - 1U;
+    uint32_t slot = 0xFFFFFFFFU;
+    bool drained = false;
+    ClosestWalk c;
+    while (true) {
+        const bool idle = slot == 0xFFFFFFFFU;
+        const unsigned idle_mask = __ballot_sync(0xFFFFFFFFU, idle);
+        if (idle_mask != 0U && !drained) {
+            unsigned long long base = 0;
+            if (lane == static_cast<uint32_t>(__ffs(idle_mask) - 1)) {
+                base = atomicAdd(&w.counters[8], static_cast<unsigned long long>(__popc(idle_mask)));
+            }
+            base = __shfl_sync(0xFFFFFFFFU, base, __ffs(idle_mask) - 1);
+            drained = base + __popc(idle_mask) >= w.capacity;
+            if (idle) {
+                const unsigned long long index = base + __popc(idle_mask & below);
+                if (index < w.capacity) {
+                    const uint32_t candidate = static_cast<uint32_t>(index);
+                    if (w.state[candidate] == kSlotActive) {
+                        slot = candidate;
+                        const float4 o4 = w.ray_o[slot], d4 = w.ray_d[slot];
+                        closest_begin(s, ld3(o4), ld3(d4), d4.w, o4.w, w.mask[slot], stack, c);
+                        w.status[slot] += 1U << 8;  // one extension segment
+                    } else {
+                        w.route[candidate] = kRouteNone;
+                    }
+                }
+            }
+        }
+        const bool busy = slot != 0xFFFFFFFFU;
+        const unsigned busy_mask = __ballot_sync(0xFFFFFFFFU, busy);
+        if (busy_mask == 0U) {
+            if (drained) {
+                break;
+            }
             continue;
         }
-        const unsigned tracing = __activemask();
-        if ((threadIdx.x & 31U) == static_cast<unsigned>(__ffs(tracing) - 1)) {
-            atomicAdd(&w.counters[3], static_cast<unsigned long long>(__popc(tracing)));
+        if (lane == static_cast<uint32_t>(__ffs(busy_mask) - 1) && idle_mask != 0U) {
+            // extension segments started in this round (lanes that took an active slot)
+            const unsigned started = busy_mask & idle_mask;
+            if (started != 0U) {
+                atomicAdd(&w.counters[3], static_cast<unsigned long long>(__popc(started)));
+            }
         }
-        const float4 o4 = w.ray_o[slot], d4 = w.ray_d[slot];
-        const uint32_t mask = w.mask[slot];
-        const ClosestResult c = closest_hit(s, ld3(o4), ld3(d4), d4.w, o4.w, mask, stack);
-        w.status[slot] += 1U << 8;  // one extension segment
-        if (c.failed) {
-            w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneTraversal;
-            w.state[slot] = kSlotDone;
-            w.route[slot] = kRouteNone;
-            continue;
+        if (busy && !closest_step(s, stack, c)) {
+            trace_finish(s, w, slot, closest_end(c), c.o, c.d, c.t_min, c.t_max);
+            slot = 0xFFFFFFFFU;
         }
-        if (c.instance == 0xFFFFFFFFU) {
-            w.hit_id[slot] = make_uint2(0xFFFFFFFFU, 0U);
-            w.route[slot] = static_cast<uint8_t>(kRouteGeneric);
-            continue;
-        }
-        TriangleHit th;
-        if (!hit_barycentrics(s, c, ld3(o4), ld3(d4), d4.w, o4.w, th)) {
-            w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneNumerical;
-            w.state[slot] = kSlotDone;
-            w.route[slot] = kRouteNone;
-            continue;
-        }
-        w.hit_tb[slot] = make_float4(c.t, th.b0, th.b1, th.b2);
-        w.hit_id[slot] = make_uint2(c.instance, c.primitive);
-        w.route[slot] = s.inst_route[c.instance];
     }
 }
 
