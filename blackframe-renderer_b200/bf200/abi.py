@@ -121,7 +121,7 @@ class TransportOptions(C.Structure):
     _fields_ = [("struct_size", u32), ("mis_heuristic", u32), ("depth_limits", u32 * 5),
                 ("roulette_enabled", u32), ("roulette_first_eligible_depth", u32),
                 ("roulette_minimum_survival", f32), ("roulette_maximum_survival", f32),
-                ("instrumentation", u32), ("reserved", u32 * 4)]
+                ("instrumentation", u32), ("sampler", u32), ("reserved", u32 * 3)]
 
 
 class Camera(C.Structure):

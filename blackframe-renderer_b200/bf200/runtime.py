@@ -22,7 +22,7 @@ EXPORTED_SYMBOLS = [
     "bf200_context_last_error", "bf200_scene_create", "bf200_scene_destroy", "bf200_trace_paths",
     "bf200_trace_paths_device", "bf200_render_film", "bf200_render_film_device",
     "bf200_closest_hits", "bf200_occlusions", "bf200_build_info", "bf200_camera_create",
-    "bf200_trace_paths_device_noalloc",
+    "bf200_trace_paths_device_noalloc", "bf200_sobol_bits", "bf200_owen_sobol_bits",
 ]
 
 
@@ -70,6 +70,10 @@ def library():
     lib.bf200_camera_create.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_uint32, C.c_uint32, C.c_float,
                                                                       C.c_float, C.c_uint32, C.POINTER(abi.Camera)]
     lib.bf200_camera_create.restype = C.c_uint32
+    lib.bf200_sobol_bits.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
+    lib.bf200_sobol_bits.restype = C.c_uint32
+    lib.bf200_owen_sobol_bits.argtypes = [C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(C.c_uint64)]
+    lib.bf200_owen_sobol_bits.restype = C.c_uint32
     lib.blackframe_query_extension.argtypes = [C.POINTER(abi.ExtensionQuery), C.POINTER(abi.ExtensionApi)]
     lib.blackframe_query_extension.restype = C.c_uint32
     _LIB = lib
@@ -207,3 +211,22 @@ def camera_create(origin, normal, tangent_seed, width, height, vfov, time=0.5, j
     if status != 0:
         raise Bf200Error(status, "camera creation")
     return cam
+
+
+def sobol_bits(sample_index, sobol_dimension):
+    """bf200_sobol_bits: the 64-bit Sobol coordinate (sobol_sample_bits)."""
+    out = C.c_uint64()
+    status = library().bf200_sobol_bits(sample_index, sobol_dimension, C.byref(out))
+    if status != 0:
+        raise Bf200Error(status, f"Sobol dimension {sobol_dimension}")
+    return out.value
+
+
+def owen_sobol_bits(pixel_x, pixel_y, sample_index, seed, sobol_dimension):
+    """bf200_owen_sobol_bits: the Owen-scrambled Sobol coordinate (owen_scrambled_sobol_bits)."""
+    index = abi.SampleIndex(pixel_x, pixel_y, sample_index, seed)
+    out = C.c_uint64()
+    status = library().bf200_owen_sobol_bits(C.byref(index), sobol_dimension, C.byref(out))
+    if status != 0:
+        raise Bf200Error(status, f"Sobol dimension {sobol_dimension}")
+    return out.value

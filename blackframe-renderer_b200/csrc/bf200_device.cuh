@@ -101,7 +101,14 @@ struct PathSource {
     const bf200_path_input_v1* inputs;
     bf200_path_result_v1* results;
     float4* path_radiance;  // film mode: radiance per path id of the chunk
+    // sampler: null for the hash SampleStream; otherwise the Owen-scrambled Sobol direction heads
+    // (kDeviceSobolDimensions x 64 leading 32-bit direction numbers)
+    const uint32_t* sobol;
 };
+
+// Sobol dimensions carried on the device: the raster pair, the four primary dimensions and
+// 256 bounces of 10 dimensions each.
+constexpr uint32_t kDeviceSobolDimensions = 2U + 4U + 10U * 256U;
 
 // Per-slot wavefront state, structure of arrays in HBM.
 struct Wavefront {
@@ -118,6 +125,8 @@ struct Wavefront {
     uint32_t* flags;    // delta flags | termination << 8 | blocked << 16
     uint32_t* status;   // lane failure code | segments << 8
     uint2* stream;      // sample-stream prefix state (64-bit), split
+    uint4* sobol_index; // Owen-Sobol sampler only: sample index, seed (64-bit each, split)
+    uint2* pixel_hash;  // Owen-Sobol sampler only: mix_bits of the packed pixel
     uint32_t* mask;     // ray visibility mask of the path
     float4* hit_tb;     // t, b0, b1, b2
     uint2* hit_id;      // instance, primitive (instance = ~0 on a miss)

@@ -23,6 +23,7 @@
 #include "bf200.h"
 #include "bf200_device.cuh"
 #include "bf200_kernels.h"
+#include "bf200_sobol.h"
 
 using namespace bf200;
 
@@ -566,6 +567,8 @@ size_t carve_wavefront(char* base, uint32_t capacity, Wavefront* out) {
     w.path_id = reinterpret_cast<uint64_t*>(take(8 * n));
     w.stream = reinterpret_cast<uint2*>(take(8 * n));
     w.hit_id = reinterpret_cast<uint2*>(take(8 * n));
+    w.sobol_index = reinterpret_cast<uint4*>(take(16 * n));
+    w.pixel_hash = reinterpret_cast<uint2*>(take(8 * n));
     w.depth = reinterpret_cast<uint32_t*>(take(4 * n));
     w.eta = reinterpret_cast<float*>(take(4 * n));
     w.flags = reinterpret_cast<uint32_t*>(take(4 * n));
@@ -624,6 +627,14 @@ blackframe_status validate_options(bf200_context* c, const bf200_transport_optio
     if (o->mis_heuristic > 1) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "unknown MIS heuristic");
     }
+    if (o->sampler > BF200_SAMPLER_OWEN_SOBOL) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "unknown sampler");
+    }
+    if (o->sampler == BF200_SAMPLER_OWEN_SOBOL &&
+        static_cast<uint64_t>(o->depth_limits[0]) + o->depth_limits[1] + o->depth_limits[2] > 255U) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE,
+                    "the Owen-Sobol sampler carries Sobol dimensions for total path depths up to 255");
+    }
     for (int i = 0; i < 4; ++i) {
         if (o->depth_limits[i] > 255) {
             return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "depth limits above 255 are not supported");
@@ -638,6 +649,37 @@ blackframe_status validate_options(bf200_context* c, const bf200_transport_optio
             return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "invalid Russian roulette policy");
         }
     }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+// Owen-Sobol direction heads: one static device table per device, filled on the first trace that
+// selects the sampler (a synchronous copy, made before that trace's first launch).
+static __device__ uint32_t g_sobol_heads[kDeviceSobolDimensions * 64U];
+std::mutex g_sobol_mutex;
+const uint32_t* g_sobol_address[64] = {};
+
+blackframe_status sobol_table(bf200_context* c, const bf200_transport_options_v1& o, const uint32_t** out) {
+    *out = nullptr;
+    if (o.sampler != BF200_SAMPLER_OWEN_SOBOL) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    if (c->device < 0 || c->device >= 64) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "device ordinal outside the Sobol table registry");
+    }
+    std::lock_guard<std::mutex> lock(g_sobol_mutex);
+    if (g_sobol_address[c->device] == nullptr) {
+        const std::vector<uint32_t>& heads = device_sobol_heads();
+        cudaError_t e = cudaMemcpyToSymbol(g_sobol_heads, heads.data(), heads.size() * sizeof(uint32_t));
+        void* address = nullptr;
+        if (e == cudaSuccess) {
+            e = cudaGetSymbolAddress(&address, g_sobol_heads);
+        }
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "Sobol direction table");
+        }
+        g_sobol_address[c->device] = static_cast<const uint32_t*>(address);
+    }
+    *out = g_sobol_address[c->device];
     return BLACKFRAME_STATUS_SUCCESS;
 }
 
@@ -1176,6 +1218,9 @@ BF200_EXPORT blackframe_status bf200_trace_paths_device(bf200_context* c, const 
     src.total = path_count;
     src.inputs = device_inputs;
     src.results = device_results;
+    if (const auto st = sobol_table(c, *o, &src.sobol); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
     return run_wavefront(c, s, src, make_params(*o), o->instrumentation != 0, report);
 }
 
@@ -1336,6 +1381,9 @@ BF200_EXPORT blackframe_status bf200_trace_paths_device_noalloc(bf200_context* c
     src.total = path_count;
     src.inputs = device_inputs;
     src.results = device_results;
+    if (const auto st = sobol_table(c, *o, &src.sobol); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
     return run_wavefront_noalloc(c, s, w, src, make_params(*o), report);
 }
 
@@ -1421,6 +1469,10 @@ BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const 
         return cuda_fail(c, e, "film chunk workspace");
     }
     const TransportParams params = make_params(*o);
+    const uint32_t* sobol = nullptr;
+    if (const auto sst = sobol_table(c, *o, &sobol); sst != BLACKFRAME_STATUS_SUCCESS) {
+        return sst;
+    }
     blackframe_status st = BLACKFRAME_STATUS_SUCCESS;
     for (uint64_t first = 0; first < req->samples_per_pixel && st == BLACKFRAME_STATUS_SUCCESS;
          first += samples_per_chunk) {
@@ -1446,6 +1498,7 @@ BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const 
         src.mask = cam->mask;
         src.jitter = cam->jitter_mode;
         src.path_radiance = radiance;
+        src.sobol = sobol;
         st = run_wavefront(c, s, src, params, o->instrumentation != 0, report);
         cudaEvent_t film_start = nullptr, film_stop = nullptr;
         if (st == BLACKFRAME_STATUS_SUCCESS && o->instrumentation != 0) {

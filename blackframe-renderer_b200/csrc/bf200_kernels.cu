@@ -689,9 +689,20 @@ __device__ __forceinline__ uint32_t depth_advance(uint32_t packed, uint32_t lobe
     return packed;
 }
 
-__device__ __forceinline__ Stream load_stream(const Wavefront& w, uint32_t slot) {
+__device__ __forceinline__ Stream load_stream(const Wavefront& w, const PathSource& src, uint32_t slot) {
     const uint2 v = w.stream[slot];
-    return Stream{(static_cast<uint64_t>(v.y) << 32) | v.x};
+    Stream r;
+    r.state = (static_cast<uint64_t>(v.y) << 32) | v.x;
+    r.sobol = src.sobol;
+    r.sample = r.seed = r.pixel_hash = 0U;
+    if (src.sobol != nullptr) {
+        const uint4 q = w.sobol_index[slot];
+        const uint2 h = w.pixel_hash[slot];
+        r.sample = (static_cast<uint64_t>(q.y) << 32) | q.x;
+        r.seed = (static_cast<uint64_t>(q.w) << 32) | q.z;
+        r.pixel_hash = (static_cast<uint64_t>(h.y) << 32) | h.x;
+    }
+    return r;
 }
 
 __device__ __forceinline__ void record_failure(const Wavefront& w, uint32_t slot, uint32_t code) {
@@ -739,7 +750,7 @@ __device__ bool start_path(const Wavefront& w, const PathSource& src, uint32_t s
         const uint64_t sample = src.first_sample + id / pixels;
         const uint32_t px = static_cast<uint32_t>(pixel % src.width);
         const uint32_t py = static_cast<uint32_t>(pixel / src.width);
-        stream = Stream::make(px, py, sample, src.seed);
+        stream = Stream::make(px, py, sample, src.seed, src.sobol);
         // the jitter uses the independent stream of the same index (PixelJitter.hpp:47-64)
         camera_ray(src, px, py, stream, o, d, lane);
         tmin = src.t_min;
@@ -747,7 +758,8 @@ __device__ bool start_path(const Wavefront& w, const PathSource& src, uint32_t s
         mask = src.mask;
     } else {
         const bf200_path_input_v1& in = src.inputs[id];
-        stream = Stream::make(in.sample.pixel_x, in.sample.pixel_y, in.sample.sample_index, in.sample.seed);
+        stream = Stream::make(in.sample.pixel_x, in.sample.pixel_y, in.sample.sample_index, in.sample.seed,
+                              src.sobol);
         o = F3{in.primary_ray.origin[0], in.primary_ray.origin[1], in.primary_ray.origin[2]};
         d = F3{in.primary_ray.direction[0], in.primary_ray.direction[1], in.primary_ray.direction[2]};
         tmin = in.primary_ray.t_min;
@@ -765,6 +777,12 @@ __device__ bool start_path(const Wavefront& w, const PathSource& src, uint32_t s
     w.flags[slot] = 0U;
     w.status[slot] = lane.err;
     w.stream[slot] = make_uint2(static_cast<uint32_t>(stream.state), static_cast<uint32_t>(stream.state >> 32));
+    if (src.sobol != nullptr) {
+        w.sobol_index[slot] = make_uint4(static_cast<uint32_t>(stream.sample), static_cast<uint32_t>(stream.sample >> 32),
+                                         static_cast<uint32_t>(stream.seed), static_cast<uint32_t>(stream.seed >> 32));
+        w.pixel_hash[slot] = make_uint2(static_cast<uint32_t>(stream.pixel_hash),
+                                        static_cast<uint32_t>(stream.pixel_hash >> 32));
+    }
     w.mask[slot] = mask;
     w.state[slot] = kSlotActive;
     return true;
@@ -1368,7 +1386,7 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
             const float eta = w.eta[slot];
             const float4 prev = w.prev[slot];
             const uint32_t mask = w.mask[slot];
-            const Stream stream = load_stream(w, slot);
+            const Stream stream = load_stream(w, src, slot);
             const F3 ro = ld3(o4), rd = ld3(d4);
             if (K == 0 && id.x == 0xFFFFFFFFU) {
                 const float env[4] = {s.environment.x, s.environment.y, s.environment.z, s.environment.w};

@@ -63,7 +63,7 @@ static __device__ __noinline__ float2 sincos_f(float a) {
 // SampleStream (SampleStream.hpp:23-67) and SampleDimensionMap (SampleDimensionMap.cpp:47-68)
 // ------------------------------------------------------------------------------------------------
 
-__device__ __forceinline__ uint64_t mix_bits(uint64_t v) {
+BF_HD uint64_t mix_bits(uint64_t v) {
     v ^= v >> 30U;
     v *= 0xBF58476D1CE4E5B9ULL;
     v ^= v >> 27U;
@@ -71,23 +71,90 @@ __device__ __forceinline__ uint64_t mix_bits(uint64_t v) {
     return v ^ (v >> 31U);
 }
 
+// ------------------------------------------------------------------------------------------------
+// Owen-scrambled Sobol (SobolSampling.cpp:51-117, OwenScrambling.cpp:8-44). No reference transport
+// draws from it; as a selectable transport sampler its dimension mapping is this backend's own:
+// the two hashed camera-raster dimensions take Sobol dimensions 0 and 1, and every other sample
+// dimension d (lens, time, wavelength 0..3; bounce b at 4 + 10 b + offset) takes Sobol dimension
+// d + 2.
+// ------------------------------------------------------------------------------------------------
+
+constexpr uint64_t kSobolDimensions = 21201;
+
+BF_HD uint64_t owen_pixel_hash(uint32_t px, uint32_t py) {
+    return mix_bits((static_cast<uint64_t>(px) << 32U) | static_cast<uint64_t>(py));
+}
+
+// Key of the nested permutation of one (seed, pixel, Sobol dimension) (OwenScrambling.cpp:10-17).
+BF_HD uint64_t owen_tree_key(uint64_t pixel_hash, uint64_t seed, uint64_t sobol_dimension) {
+    return mix_bits(seed ^ mix_bits(sobol_dimension + 1U)) ^ pixel_hash;
+}
+
+// Nested binary scramble of the leading `depths` bits of a 64-bit coordinate (OwenScrambling.cpp:
+// 19-33): the output bit at depth k flips with the hash of the tree node addressed by the input's
+// first k bits. Output bits below the scrambled depths are zero.
+BF_HD uint64_t owen_scramble(uint64_t input, uint64_t key, uint32_t depths) {
+    uint64_t prefix = 0, output = 0;
+    for (uint32_t depth = 0; depth < depths; ++depth) {
+        const uint32_t shift = 63U - depth;
+        const uint64_t bit = (input >> shift) & 1U;
+        const uint64_t node = (1ULL << depth) | prefix;
+        const uint64_t flip = mix_bits(key ^ node) >> 63U;
+        output |= (bit ^ flip) << shift;
+        prefix = (prefix << 1U) | bit;
+    }
+    return output;
+}
+
+constexpr uint64_t kCameraRasterX = 0xA24BAED4963EE407ULL;
+constexpr uint64_t kCameraRasterY = 0x9FB21C651E98DF25ULL;
+
+BF_HD uint64_t transport_sobol_dimension(uint64_t dimension) {
+    return dimension == kCameraRasterX ? 0U : (dimension == kCameraRasterY ? 1U : dimension + 2U);
+}
+
+// Per-path sampler. The hash stream draws indexed_bits(seed, pixel, sample, dimension)
+// (SampleStream.hpp:31-67); with `sobol` set it draws the Owen-scrambled Sobol coordinate of the
+// path's sample index instead. `sobol` holds, per Sobol dimension, the leading 32 bits of the 64
+// direction numbers: the 24 bits a float sample keeps (bits >> 40 of the 64-bit coordinate) depend
+// only on the directions' leading bits, so only those and the first 24 scramble depths are
+// evaluated, which leaves every float sample identical to the 64-bit computation.
 struct Stream {
     uint64_t state;  // the (seed, pixel, sample) prefix of indexed_bits
-    __device__ __forceinline__ static Stream make(uint32_t px, uint32_t py, uint64_t sample, uint64_t seed) {
+    const uint32_t* sobol;
+    uint64_t sample, seed, pixel_hash;
+    __device__ __forceinline__ static Stream make(uint32_t px, uint32_t py, uint64_t sample, uint64_t seed,
+                                                  const uint32_t* sobol) {
         const uint64_t packed = (static_cast<uint64_t>(px) << 32U) | static_cast<uint64_t>(py);
         uint64_t s = mix_bits(seed ^ 0x9E3779B97F4A7C15ULL);
         s = mix_bits(s ^ packed ^ 0xD1B54A32D192ED03ULL);
         s = mix_bits(s ^ sample ^ 0x8CB92BA72F3D8DD7ULL);
-        return Stream{s};
+        Stream r;
+        r.state = s;
+        r.sobol = sobol;
+        r.sample = sample;
+        r.seed = seed;
+        r.pixel_hash = sobol != nullptr ? owen_pixel_hash(px, py) : 0U;
+        return r;
     }
     __device__ __forceinline__ float sample_1d(uint64_t dimension) const {
-        const uint64_t bits = mix_bits(state ^ dimension);
+        if (sobol == nullptr) {
+            const uint64_t bits = mix_bits(state ^ dimension);
+            return static_cast<float>(bits >> 40U) * 0x1p-24F;
+        }
+        const uint64_t sd = transport_sobol_dimension(dimension);
+        const uint32_t* heads = sobol + 64ULL * sd;
+        uint64_t gray = sample ^ (sample >> 1U);
+        uint32_t point = 0U;
+        while (gray != 0U) {
+            point ^= heads[__ffsll(static_cast<long long>(gray)) - 1];
+            gray &= gray - 1U;
+        }
+        const uint64_t bits = owen_scramble(static_cast<uint64_t>(point) << 32U,
+                                            owen_tree_key(pixel_hash, seed, sd), 24U);
         return static_cast<float>(bits >> 40U) * 0x1p-24F;
     }
 };
-
-constexpr uint64_t kCameraRasterX = 0xA24BAED4963EE407ULL;
-constexpr uint64_t kCameraRasterY = 0x9FB21C651E98DF25ULL;
 
 __device__ __forceinline__ uint64_t bounce_base(uint32_t bounce) { return 4ULL + 10ULL * bounce; }
 

@@ -318,8 +318,18 @@ typedef struct bf200_transport_options_v1 {
     float roulette_minimum_survival;
     float roulette_maximum_survival;
     uint32_t instrumentation; /* 1: time every stage with CUDA events (CudaWavefrontInstrumentationMode::nsight) */
-    uint32_t reserved[4];
+    uint32_t sampler;         /* BF200_SAMPLER_*: 0 hash SampleStream (reference parity), 1 Owen-scrambled Sobol */
+    uint32_t reserved[3];
 } bf200_transport_options_v1;
+
+/* Transport samplers. BF200_SAMPLER_HASH draws SampleStream::indexed_bits (SampleStream.hpp:31-67)
+ * exactly as the reference transport does. BF200_SAMPLER_OWEN_SOBOL draws the Owen-scrambled Sobol
+ * coordinate owen_scrambled_sobol_bits(index, d') (OwenScrambling.hpp:11-22) of the same sample
+ * index, where d' = 0 and 1 for the two camera-raster dimensions and d + 2 for every other sample
+ * dimension d. No reference transport uses Sobol, so this mapping has no reference counterpart;
+ * it supports total path depths up to 255. */
+#define BF200_SAMPLER_HASH 0u
+#define BF200_SAMPLER_OWEN_SOBOL 1u
 
 /* Pinhole camera (PinholeCamera.hpp:52-306) with the host-side constants already derived:
  * half_height = tan(fov/2), half_width = half_height * width/height. */
@@ -550,6 +560,17 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_camera_create(
     const float origin[3], const float normal[3], const float tangent_seed[3], uint32_t width,
     uint32_t height, float vertical_fov_radians, float time, uint32_t jitter_mode,
     bf200_camera_v1* out_camera) BF200_NOEXCEPT;
+
+/* Sobol coordinate of a sample index in one of the 21,201 Joe-Kuo D6 dimensions, as a 64-bit
+ * fixed-point fraction (sobol_sample_bits, SobolSampling.hpp:16-19). Dimensions from 21201 up
+ * return BLACKFRAME_STATUS_OUT_OF_RANGE. Host computation. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_sobol_bits(uint64_t sample_index, uint64_t sobol_dimension,
+                                                               uint64_t* out_bits) BF200_NOEXCEPT;
+/* Owen-scrambled Sobol coordinate of (pixel, sample index, seed) in one Sobol dimension
+ * (owen_scrambled_sobol_bits, OwenScrambling.hpp:11-13). Host computation. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_owen_sobol_bits(const bf200_sample_index_v1* index,
+                                                                    uint64_t sobol_dimension,
+                                                                    uint64_t* out_bits) BF200_NOEXCEPT;
 
 /* Library version and build description (sm_100a arch string). */
 BF200_EXTERN_C BF200_EXPORT const char* bf200_build_info(void) BF200_NOEXCEPT;

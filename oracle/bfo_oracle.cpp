@@ -60,10 +60,90 @@ uint64_t mix_bits(uint64_t v) {
     return v ^ (v >> 31U);
 }
 
+// Sobol coordinates (SobolSampling.cpp:51-117) over the Joe-Kuo D6 parameters, and the nested
+// binary Owen scramble (OwenScrambling.cpp:8-44).
+const uint64_t kJoeKuoRows[21200][3] = {
+#include "bf200_sobol_table.inc"
+};
+
+uint64_t sobol_coordinate(uint64_t sample_index, uint64_t dimension) {
+    uint64_t v[64];
+    if (dimension == 0) {
+        for (uint32_t j = 0; j < 64; ++j) {
+            v[j] = 1ULL << (63U - j);
+        }
+    } else {
+        static const uint32_t row_end[18] = {1,   2,   4,   6,    12,   18,   36,   52,    100,
+                                             160, 336, 480, 1110, 1866, 3666, 5714, 13424, 21200};
+        const uint64_t row = dimension - 1;
+        uint32_t degree = 1;
+        while (row >= row_end[degree - 1]) {
+            ++degree;
+        }
+        // the row's three words as one 192-bit little-endian integer
+        auto bits = [&](uint32_t offset, uint32_t width) -> uint64_t {
+            uint64_t value = 0;
+            for (uint32_t k = 0; k < width; ++k) {
+                const uint32_t pos = offset + k;
+                value |= ((kJoeKuoRows[row][pos / 64U] >> (pos % 64U)) & 1ULL) << k;
+            }
+            return value;
+        };
+        const uint64_t a = bits(0, degree - 1);
+        uint32_t offset = degree - 1;
+        for (uint32_t j = 0; j < degree; ++j) {
+            v[j] = bits(offset, j + 1) << (63U - j);
+            offset += j + 1;
+        }
+        for (uint32_t j = degree; j < 64; ++j) {
+            uint64_t d = v[j - degree] ^ (v[j - degree] >> degree);
+            for (uint32_t k = 1; k < degree; ++k) {
+                if ((a >> (degree - 1U - k)) & 1U) {
+                    d ^= v[j - k];
+                }
+            }
+            v[j] = d;
+        }
+    }
+    uint64_t gray = sample_index ^ (sample_index >> 1U);
+    uint64_t point = 0;
+    for (uint32_t j = 0; gray != 0; ++j, gray >>= 1U) {
+        if (gray & 1U) {
+            point ^= v[j];
+        }
+    }
+    return point;
+}
+
+uint64_t owen_coordinate(uint32_t px, uint32_t py, uint64_t sample_index, uint64_t seed, uint64_t dimension) {
+    const uint64_t packed = (uint64_t(px) << 32U) | uint64_t(py);
+    const uint64_t key = mix_bits(seed ^ mix_bits(dimension + 1U)) ^ mix_bits(packed);
+    const uint64_t input = sobol_coordinate(sample_index, dimension);
+    uint64_t prefix = 0, output = 0;
+    for (uint32_t depth = 0; depth < 64; ++depth) {
+        const uint64_t bit = (input >> (63U - depth)) & 1U;
+        const uint64_t flip = mix_bits(key ^ ((1ULL << depth) | prefix)) >> 63U;
+        output |= (bit ^ flip) << (63U - depth);
+        prefix = (prefix << 1U) | bit;
+    }
+    return output;
+}
+
+// The transport's Sobol dimension of a sample dimension (the mapping of BF200_SAMPLER_OWEN_SOBOL):
+// camera raster x, y -> 0, 1; every other dimension d -> d + 2.
+uint64_t transport_sobol_dimension(uint64_t d) {
+    return d == 0xA24BAED4963EE407ULL ? 0U : (d == 0x9FB21C651E98DF25ULL ? 1U : d + 2U);
+}
+
 struct Stream {
     uint32_t px, py;
     uint64_t sample, seed;
+    bool owen = false;  // Owen-scrambled Sobol instead of the hash stream
     float sample_1d(uint64_t dimension) const {
+        if (owen) {
+            const uint64_t bits = owen_coordinate(px, py, sample, seed, transport_sobol_dimension(dimension));
+            return static_cast<float>(bits >> 40U) * 0x1p-24F;
+        }
         const uint64_t packed = (uint64_t(px) << 32U) | uint64_t(py);
         uint64_t state = mix_bits(seed ^ 0x9E3779B97F4A7C15ULL);
         state = mix_bits(state ^ packed ^ 0xD1B54A32D192ED03ULL);
@@ -1915,6 +1995,7 @@ Surface resolve_surface(const Scene& scene, const Hit& hit) {
 // ---------------------------------------------------------------------------------------------
 
 struct Options {
+    uint32_t sampler;
     uint32_t heuristic;
     uint32_t limits[5];
     bool roulette;
@@ -2139,7 +2220,7 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
     out.blocked = 0;
     out.segments = 0;
     const Stream stream{input.sample.pixel_x, input.sample.pixel_y, input.sample.sample_index,
-                        input.sample.seed};
+                        input.sample.seed, opt.sampler == 1U};
     V3 ro{input.primary_ray.origin[0], input.primary_ray.origin[1], input.primary_ray.origin[2]};
     V3 rd{input.primary_ray.direction[0], input.primary_ray.direction[1],
           input.primary_ray.direction[2]};
@@ -2319,6 +2400,7 @@ void set_error(const char* message) {
 
 Options make_options(const bf200_transport_options_v1& o) {
     Options r{};
+    r.sampler = o.sampler;
     r.heuristic = o.mis_heuristic;
     for (int i = 0; i < 5; ++i) {
         r.limits[i] = o.depth_limits[i];
@@ -2562,12 +2644,14 @@ __attribute__((visibility("default"))) int bfo_closest_hits(void* h, const bf200
 
 // PinholeCamera::generate_primary_ray with uniform pixel jitter (PinholeCamera.hpp:144-283,
 // PixelJitter.hpp:47-64) for a camera whose frame and half extents are given.
-__attribute__((visibility("default"))) int bfo_camera_rays(const bf200_camera_v1* cam,
-                                                           const bf200_sample_index_v1* samples, uint64_t n,
-                                                           bf200_ray_v1* rays) {
+// `sampler` selects the jitter's sampler (BF200_SAMPLER_*).
+__attribute__((visibility("default"))) int bfo_camera_rays_sampled(const bf200_camera_v1* cam,
+                                                                   const bf200_sample_index_v1* samples, uint64_t n,
+                                                                   uint32_t sampler, bf200_ray_v1* rays) {
     try {
         for (uint64_t i = 0; i < n; ++i) {
-            const Stream stream{samples[i].pixel_x, samples[i].pixel_y, samples[i].sample_index, samples[i].seed};
+            const Stream stream{samples[i].pixel_x, samples[i].pixel_y, samples[i].sample_index, samples[i].seed,
+                                sampler == 1U};
             float ox = 0.5F, oy = 0.5F;
             if (cam->jitter_mode != 0) {
                 ox = stream.sample_1d(0xA24BAED4963EE407ULL);
@@ -2600,6 +2684,21 @@ __attribute__((visibility("default"))) int bfo_camera_rays(const bf200_camera_v1
         set_error(f.message);
         return 1;
     }
+}
+
+__attribute__((visibility("default"))) int bfo_camera_rays(const bf200_camera_v1* cam,
+                                                           const bf200_sample_index_v1* samples, uint64_t n,
+                                                           bf200_ray_v1* rays) {
+    return bfo_camera_rays_sampled(cam, samples, n, 0U, rays);
+}
+
+__attribute__((visibility("default"))) uint64_t bfo_sobol_bits(uint64_t sample_index, uint64_t dimension) {
+    return sobol_coordinate(sample_index, dimension);
+}
+
+__attribute__((visibility("default"))) uint64_t bfo_owen_sobol_bits(uint32_t px, uint32_t py, uint64_t sample_index,
+                                                                    uint64_t seed, uint64_t dimension) {
+    return owen_coordinate(px, py, sample_index, seed, dimension);
 }
 
 // Float32 or Neumaier float64 film of the caller-side path: CIE XYZ (Cie1931Sensor.cpp:104-176),

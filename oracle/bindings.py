@@ -80,15 +80,25 @@ class Oracle(_Checker):
         self.lib.bfo_closest_hits.argtypes = [C.c_void_p, C.POINTER(abi.Ray), C.c_uint64, C.POINTER(abi.Hit)]
         self.lib.bfo_scene_world_normal.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]
         self.lib.bfo_scene_set_prefilter.argtypes = [C.c_void_p, C.c_int]
-        self.lib.bfo_camera_rays.argtypes = [C.POINTER(abi.Camera), C.POINTER(abi.SampleIndex), C.c_uint64,
-                                             C.POINTER(abi.Ray)]
-        self.lib.bfo_camera_rays.restype = C.c_int
+        self.lib.bfo_camera_rays_sampled.argtypes = [C.POINTER(abi.Camera), C.POINTER(abi.SampleIndex), C.c_uint64,
+                                                     C.c_uint32, C.POINTER(abi.Ray)]
+        self.lib.bfo_camera_rays_sampled.restype = C.c_int
+        self.lib.bfo_sobol_bits.argtypes = [C.c_uint64, C.c_uint64]
+        self.lib.bfo_sobol_bits.restype = C.c_uint64
+        self.lib.bfo_owen_sobol_bits.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]
+        self.lib.bfo_owen_sobol_bits.restype = C.c_uint64
 
-    def camera_rays(self, camera, samples):
+    def camera_rays(self, camera, samples, sampler=0):
         rays = (abi.Ray * len(samples))()
-        if self.lib.bfo_camera_rays(C.byref(camera), samples, len(samples), rays) != 0:
+        if self.lib.bfo_camera_rays_sampled(C.byref(camera), samples, len(samples), sampler, rays) != 0:
             raise CheckerError(self.last_error())
         return rays
+
+    def sobol_bits(self, sample_index, dimension):
+        return self.lib.bfo_sobol_bits(sample_index, dimension)
+
+    def owen_sobol_bits(self, px, py, sample_index, seed, dimension):
+        return self.lib.bfo_owen_sobol_bits(px, py, sample_index, seed, dimension)
 
     def closest_hits(self, handle, rays):
         hits = (abi.Hit * len(rays))()
@@ -128,6 +138,24 @@ class Reference(_Checker):
         f.argtypes = [C.c_void_p, C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(C.c_float),
                       C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
         f.restype = C.c_int
+
+    def sobol_bits(self, sample_index, dimension):
+        f = self.lib.bfr_sobol_bits
+        f.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
+        f.restype = C.c_int
+        out = C.c_uint64()
+        if f(sample_index, dimension, C.byref(out)) != 0:
+            raise CheckerError(self.last_error())
+        return out.value
+
+    def owen_sobol_bits(self, px, py, sample_index, seed, dimension):
+        f = self.lib.bfr_owen_sobol_bits
+        f.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
+        f.restype = C.c_int
+        out = C.c_uint64()
+        if f(px, py, sample_index, seed, dimension, C.byref(out)) != 0:
+            raise CheckerError(self.last_error())
+        return out.value
 
     @staticmethod
     def _f3(values):

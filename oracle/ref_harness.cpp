@@ -28,6 +28,7 @@
 #include <Blackframe/Renderer/Film.hpp>
 #include <Blackframe/Renderer/IndependentSampler.hpp>
 #include <Blackframe/Renderer/LightSampler.hpp>
+#include <Blackframe/Renderer/OwenScrambling.hpp>
 #include <Blackframe/Renderer/PinholeCamera.hpp>
 #include <Blackframe/Renderer/WavelengthSampling.hpp>
 
@@ -560,6 +561,33 @@ bfr_film_accumulate(const float* radiance, const bf200_sample_index_v1* samples,
         return 1;
     }
     return run(*film);
+}
+
+// sobol_sample_bits / owen_scrambled_sobol_bits of the reference library; 0 on success, 1 when the
+// dimension is outside the table.
+__attribute__((visibility("default"))) int bfr_sobol_bits(std::uint64_t sample_index, std::uint64_t dimension,
+                                                          std::uint64_t* out) {
+    const auto bits = renderer::sobol_sample_bits(sample_index, dimension);
+    if (!bits) {
+        set_error(bits.error().message);
+        return 1;
+    }
+    *out = *bits;
+    return 0;
+}
+
+__attribute__((visibility("default"))) int bfr_owen_sobol_bits(std::uint32_t pixel_x, std::uint32_t pixel_y,
+                                                               std::uint64_t sample_index, std::uint64_t seed,
+                                                               std::uint64_t dimension, std::uint64_t* out) {
+    const auto index = renderer::SampleStreamIndex{
+        .pixel_x = pixel_x, .pixel_y = pixel_y, .sample_index = sample_index, .seed = seed};
+    const auto bits = renderer::owen_scrambled_sobol_bits(index, dimension);
+    if (!bits) {
+        set_error(bits.error().message);
+        return 1;
+    }
+    *out = *bits;
+    return 0;
 }
 
 } // extern "C"

@@ -12,13 +12,12 @@ import numpy as np
 import pytest
 
 from bf200 import abi, runtime, scenes
-from helpers import arrays, bit_equal, golden_inputs, relative_error, sensor_from_golden
+from helpers import (DIVERGED_FRACTION, RELATIVE_TOLERANCE, arrays, bit_equal, check_paths, golden_inputs,
+                     relative_error, sensor_from_golden)
 from oracle.bindings import Oracle
 
 pytestmark = pytest.mark.gpu
 WORKLOADS = ["cornell_plain_64", "cornell_spheres_256"]
-RELATIVE_TOLERANCE = 1e-5
-DIVERGED_FRACTION = 0.01
 
 
 @pytest.fixture(scope="module")
@@ -30,17 +29,6 @@ def ctx():
 @pytest.fixture(scope="module")
 def oracle():
     return Oracle()
-
-
-def check_paths(got, expected, label):
-    same = bit_equal(got["radiance"], expected["radiance"]).all(axis=1)
-    close = (relative_error(got["radiance"], expected["radiance"]) <= RELATIVE_TOLERANCE).all(axis=1)
-    term = got["termination"] == expected["termination"]
-    n = len(same)
-    assert (got["lane_status"] == 0).all(), f"{label}: failed lanes {np.nonzero(got['lane_status'])[0][:10]}"
-    assert close.mean() >= 1.0 - DIVERGED_FRACTION, f"{label}: only {close.sum()}/{n} within tolerance"
-    assert term.mean() >= 1.0 - DIVERGED_FRACTION, f"{label}: terminations differ on {n - term.sum()}/{n}"
-    return same.mean(), close.mean()
 
 
 @pytest.mark.parametrize("name", WORKLOADS)
