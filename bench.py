@@ -30,7 +30,7 @@ sys.path.insert(0, REPO)
 
 import numpy as np  # noqa: E402
 
-from bf200 import abi, runtime, scenes  # noqa: E402
+from bf200 import abi, multigpu, runtime, scenes  # noqa: E402
 
 WORKLOAD = "cornell_spheres_256"
 METRIC = "path samples/s"
@@ -225,7 +225,7 @@ def main():
     def render_device(step, instrument=False):
         options.instrumentation = 1 if instrument else 0
         f = abi.Film(width, height, 0, 0, film.data_ptr(), C.cast(counts.data_ptr(), C.POINTER(abi.u64)))
-        first = (step * world + rank) * spp  # disjoint sample ranges per rank and step
+        first, _ = multigpu.rank_sample_range(step, rank, world, spp)  # disjoint per rank and step
         request = abi.FilmRequest(C.sizeof(abi.FilmRequest), spp, first, 0, 0)
         report = abi.Report()
         report.struct_size = C.sizeof(abi.Report)
@@ -234,7 +234,7 @@ def main():
         if status != 0:
             raise runtime.Bf200Error(status, lib.bf200_context_last_error(ctx.handle).decode())
         if distributed:
-            dist.all_reduce(film)  # per-GPU films summed (the only exchange of the path)
+            multigpu.reduce_film(film, counts)  # per-GPU films summed (the only exchange of the path)
         return report
 
     for step in range(args.warmup):
