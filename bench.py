@@ -107,13 +107,15 @@ class ClockSampler:
                 "reasons": reasons}
 
 
-def workload_setup():
-    builder, options, (width, height, spp) = scenes.build_workload(WORKLOAD)
+def workload_setup(workload):
+    builder, options, (width, height, spp) = scenes.build_workload(workload)
+    # every workload resolves its materials at the same wavelength packet (sample 0.1), whose CIE
+    # sensor constants the reference computed into the Cornell fixture
     g = np.load(os.path.join(REPO, "tests", "golden", f"{WORKLOAD}.npz"))
     from helpers import sensor_from_golden
     sensor = sensor_from_golden(g)
-    camera = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV,
-                                   scenes.PATH_TIME)
+    origin, normal, tangent, vfov = scenes.workload_camera(workload)
+    camera = runtime.camera_create(origin, normal, tangent, width, height, vfov, scenes.PATH_TIME)
     return builder, options, camera, sensor, (width, height, spp)
 
 
@@ -189,7 +191,9 @@ def main():
     parser.add_argument("--capacity", type=int, default=1 << 21)
     parser.add_argument("--reference-seconds", type=float, default=8.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
-    parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's 256)")
+    parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's)")
+    parser.add_argument("--workload", default=WORKLOAD, choices=sorted(scenes.WORKLOADS),
+                        help="scene and frame (default: the headline Cornell + spheres frame)")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -210,7 +214,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
-    builder, options, camera, sensor, (width, height, spp) = workload_setup()
+    builder, options, camera, sensor, (width, height, spp) = workload_setup(args.workload)
     if args.spp > 0:
         spp = args.spp
     pixels = width * height
@@ -328,13 +332,15 @@ def main():
         "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "width": width, "height": height, "spp": spp, "max_depth": 16,
+        "config": {"workload": args.workload, "width": width, "height": height, "spp": spp, "max_depth": 16,
                    "mis": "power", "paths_per_step_per_gpu": paths_per_step, "path_capacity": args.capacity,
                    "l2": "flushed between steps (256 MiB write); path state > L2",
                    "parallelism": f"sample-partitioned x{world}" if world > 1 else "single GPU"},
         "rays_per_s": (ext + shadow) / (total_ms / 1000.0) * (world if distributed else 1),
         "segments": {"extension": ext, "shadow": shadow, "iterations": iterations},
         "stage_ms_one_frame": stage, "failed_lanes": failed,
+        "first_failure": next(({"status": r.first_failure_status, "path": r.first_failure_path}
+                               for r in reports if r.failed_lanes), None),
         "clocks": clocks.summary(),
         "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d},
@@ -347,7 +353,7 @@ def main():
     }
     scene.close()
     ctx.close()
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and args.workload == WORKLOAD:
         rate, threads, kind, sample, _, _ = cpu_sample_rate()
         line["cpu_baseline"] = {"value": rate, "unit": "path samples/s", "cores": threads, "kind": kind,
                                 "sample": sample}

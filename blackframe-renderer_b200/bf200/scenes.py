@@ -407,11 +407,12 @@ CAMERA_VFOV = 0.70
 PATH_TIME = 0.5
 
 
-def camera_frame_inputs():
-    """Camera frame seed of the Cornell workloads: normal = -forward, tangent seed +X
-    (the construction of Tests/Backends/CPU/Embree/CornellWavefrontScene.hpp:380-395)."""
-    origin = np.array(CAMERA_ORIGIN, F32)
-    target = np.array(CAMERA_TARGET, F32)
+def camera_frame_inputs(origin=CAMERA_ORIGIN, target=CAMERA_TARGET):
+    """Camera frame seed looking from `origin` at `target` (default: the Cornell workloads):
+    normal = -forward, tangent seed +X (the construction of
+    Tests/Backends/CPU/Embree/CornellWavefrontScene.hpp:380-395)."""
+    origin = np.array(origin, F32)
+    target = np.array(target, F32)
     seed = (target - origin).astype(F32)
     length = np.sqrt(F32(F32(F32(seed[0] * seed[0]) + F32(seed[1] * seed[1])) +
                          F32(seed[2] * seed[2])))
@@ -420,15 +421,136 @@ def camera_frame_inputs():
     return origin, normal, np.array([1.0, 0.0, 0.0], F32)
 
 
+# ------------------------------------------------------------------------------------------------
+# BVH-stress scene: seeded displaced icospheres, instanced with random affine transforms
+# ------------------------------------------------------------------------------------------------
+
+def icosphere(subdivisions):
+    """Unit icosphere: the icosahedron with every triangle split in four `subdivisions` times,
+    new vertices projected to the sphere (20 * 4^s triangles, 10 * 4^s + 2 vertices); float64."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    v = np.array([(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t),
+                  (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+                  (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+                  (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)], np.int64)
+    for _ in range(subdivisions):
+        n = len(f)
+        edges = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        unique, inverse = np.unique(np.sort(edges, axis=1), axis=0, return_inverse=True)
+        mid = v[unique[:, 0]] + v[unique[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        index = len(v) + inverse.reshape(-1)
+        v = np.concatenate([v, mid])
+        a, b, c = index[:n], index[n:2 * n], index[2 * n:]
+        f = np.concatenate([np.stack([f[:, 0], a, c], 1), np.stack([a, f[:, 1], b], 1),
+                            np.stack([c, b, f[:, 2]], 1), np.stack([a, b, c], 1)])
+    return v, f
+
+
+def displaced_icosphere(subdivisions, amplitude, seed):
+    """Icosphere with every vertex moved along its normal by amplitude * U[-1, 1] (seeded).
+
+    At subdivision 7 the edges are about 0.01 long, so a 0.05 displacement makes neighbouring
+    faces point in very different directions, and averaged vertex normals would leave the
+    geometric-normal hemisphere of some faces, which the surface reconstruction rejects
+    (no substitution). Faces are therefore flat-shaded: every triangle gets its own three
+    vertices (the displaced positions, so the surface stays watertight) carrying its face normal.
+    """
+    v, f = icosphere(subdivisions)
+    rng = np.random.default_rng(seed)
+    v = v * (1.0 + amplitude * rng.uniform(-1.0, 1.0, len(v)))[:, None]
+    v32 = v.astype(F32)
+    corners = v32[f].reshape(-1, 3)
+    p = v32[f].astype(np.float64)
+    face_n = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+    face_n /= np.linalg.norm(face_n, axis=1, keepdims=True)
+    normals = np.repeat(face_n, 3, axis=0).astype(F32)
+    triangles = np.arange(3 * len(f), dtype=np.uint32).reshape(-1, 3)
+    return Mesh(corners, normals, np.zeros((len(corners), 2), F32), triangles)
+
+
+def grid_quad(center, size, divisions, y, normal_down=True):
+    """Square of divisions x divisions cells (2 triangles each) in the plane y, facing -y."""
+    xs = np.linspace(center[0] - size / 2, center[0] + size / 2, divisions + 1)
+    zs = np.linspace(center[1] - size / 2, center[1] + size / 2, divisions + 1)
+    gx, gz = np.meshgrid(xs, zs, indexing="ij")
+    positions = np.stack([gx.ravel(), np.full(gx.size, y), gz.ravel()], 1)
+    idx = np.arange((divisions + 1) ** 2).reshape(divisions + 1, divisions + 1)
+    a, b = idx[:-1, :-1].ravel(), idx[1:, :-1].ravel()
+    c, d = idx[1:, 1:].ravel(), idx[:-1, 1:].ravel()
+    if normal_down:  # counter-clockwise seen from below
+        tris = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)])
+    else:
+        tris = np.concatenate([np.stack([a, c, b], 1), np.stack([a, d, c], 1)])
+    normal = (0.0, -1.0, 0.0) if normal_down else (0.0, 1.0, 0.0)
+    return Mesh(positions.astype(F32), np.tile(np.array(normal, F32), (len(positions), 1)),
+                np.zeros((len(positions), 2), F32), tris.astype(np.uint32))
+
+
+def random_rotation(rng):
+    """Uniform random rotation matrix (normalised Gaussian quaternion)."""
+    q = rng.normal(size=4)
+    w, x, y, z = q / np.linalg.norm(q)
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                     [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                     [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+
+
+def bvh_stress(builder, subdivisions=7, instances=40, light_divisions=32):
+    """The BVH-stress scene: 3 displaced icospheres (amplitude 0.05, seed k) instanced
+    `instances` times with uniform rotation, scale U[0.5, 1.5] and translation U[-10, 10]^3
+    (seed 1234); materials 50 % Lambert (albedo U[0.2, 0.8] per lane), 30 % anisotropic GGX
+    conductor (alpha_x, alpha_y U[0.05, 0.6]), 20 % GGX dielectric (eta 1.5); a ground quad; one
+    emissive 2 * light_divisions^2-triangle grid above; the environment is set by the builder."""
+    nm = builder.nanometers
+    meshes = [builder.add_mesh(displaced_icosphere(subdivisions, 0.05, k)) for k in range(3)]
+    rng = np.random.default_rng(1234)
+    gold_eta, gold_k = tabulated_spectrum(GOLD_ETA, nm), tabulated_spectrum(GOLD_K, nm)
+    for i in range(instances):
+        kind = rng.uniform()
+        if kind < 0.5:
+            material = builder.add_material(lambertian(rng.uniform(0.2, 0.8, 4)))
+        elif kind < 0.8:
+            ax, ay = rng.uniform(0.05, 0.6, 2)
+            material = builder.add_material(rough_conductor([1.0] * 4, gold_eta, gold_k, ax, ay))
+        else:
+            material = builder.add_material(rough_dielectric([1.0] * 4, 1.0, 1.5, 0.1, 0.1))
+        m = identity()
+        m[:3, :3] = (random_rotation(rng) * rng.uniform(0.5, 1.5)).astype(F32)
+        m[:3, 3] = rng.uniform(-10.0, 10.0, 3).astype(F32)
+        builder.add_instance(meshes[i % 3], material, m)
+    ground = builder.add_mesh(quad([(-40, -12, -40), (-40, -12, 40), (40, -12, 40), (40, -12, -40)], (0, 1, 0)))
+    builder.add_instance(ground, builder.add_material(lambertian([0.5] * 4)))
+    light = builder.add_mesh(grid_quad((0.0, 0.0), 16.0, light_divisions, 14.0))
+    builder.add_instance(light, builder.add_material(lambertian([0.0] * 4), emission=(10.0, 10.0, 10.0, 10.0)))
+    return builder
+
+
+BVH_STRESS_CAMERA = ((0.0, 2.0, 24.0), (0.0, -3.0, 0.0))  # origin, target
+BVH_STRESS_VFOV = 0.9
+
 WORKLOADS = {
-    # name: (width, height, spp, max_depth, mis, spheres)
-    "cornell_plain_64": (64, 64, 16, 8, "balance", False),
-    "cornell_spheres_256": (256, 256, 256, 16, "power", True),
+    # name: (width, height, spp, max_depth, mis, scene)
+    "cornell_plain_64": (64, 64, 16, 8, "balance", "cornell"),
+    "cornell_spheres_256": (256, 256, 256, 16, "power", "cornell_spheres"),
+    "bvh_stress_1080p": (1920, 1080, 64, 16, "power", "bvh_stress"),
 }
 
 
 def build_workload(name):
-    width, height, spp, depth, mis, spheres = WORKLOADS[name]
-    builder = cornell_box(SceneBuilder(), with_spheres=spheres)
+    width, height, spp, depth, mis, scene = WORKLOADS[name]
+    if scene == "bvh_stress":
+        builder = bvh_stress(SceneBuilder(environment=(0.5, 0.5, 0.5, 0.5)))
+    else:
+        builder = cornell_box(SceneBuilder(), with_spheres=scene == "cornell_spheres")
     options = abi.default_options(mis=mis, max_depth=depth)
     return builder, options, (width, height, spp)
+
+
+def workload_camera(name):
+    """(origin, normal, tangent seed, vertical fov) of a workload's camera."""
+    if WORKLOADS[name][5] == "bvh_stress":
+        return (*camera_frame_inputs(*BVH_STRESS_CAMERA), BVH_STRESS_VFOV)
+    return (*camera_frame_inputs(), CAMERA_VFOV)

@@ -34,35 +34,35 @@ class _Checker:
             raise CheckerError(f"{path} is not built")
         self.lib = C.CDLL(path)
         p = self.prefix
-        self.lib[p + "_last_error"].restype = C.c_char_p
-        f = self.lib[p + "_scene_create"]
+        getattr(self.lib, p + "_last_error").restype = C.c_char_p
+        f = getattr(self.lib, p + "_scene_create")
         f.argtypes = [C.POINTER(abi.SceneDesc), C.POINTER(C.c_void_p)]
         f.restype = C.c_int
-        self.lib[p + "_scene_destroy"].argtypes = [C.c_void_p]
-        f = self.lib[p + "_trace_paths"]
+        getattr(self.lib, p + "_scene_destroy").argtypes = [C.c_void_p]
+        f = getattr(self.lib, p + "_trace_paths")
         f.argtypes = [C.c_void_p, C.POINTER(abi.PathInput), C.c_uint64, C.POINTER(abi.TransportOptions),
                       C.POINTER(abi.PathResult), C.c_int]
         f.restype = C.c_int64
 
     def last_error(self):
-        return self.lib[self.prefix + "_last_error"]().decode()
+        return getattr(self.lib, self.prefix + "_last_error")().decode()
 
     def scene(self, builder):
         desc = builder.desc()
         handle = C.c_void_p()
-        rc = self.lib[self.prefix + "_scene_create"](C.byref(desc), C.byref(handle))
+        rc = getattr(self.lib, self.prefix + "_scene_create")(C.byref(desc), C.byref(handle))
         if rc != 0:
             raise CheckerError(f"scene creation failed ({rc}): {self.last_error()}")
         return handle
 
     def destroy(self, handle):
-        self.lib[self.prefix + "_scene_destroy"](handle)
+        getattr(self.lib, self.prefix + "_scene_destroy")(handle)
 
     def trace(self, handle, inputs, options, threads=None):
         n = len(inputs)
         results = (abi.PathResult * n)()
         threads = threads or os.cpu_count() or 1
-        failures = self.lib[self.prefix + "_trace_paths"](handle, inputs, n, C.byref(options), results, threads)
+        failures = getattr(self.lib, self.prefix + "_trace_paths")(handle, inputs, n, C.byref(options), results, threads)
         if failures < 0:
             raise CheckerError(self.last_error())
         return results, failures
