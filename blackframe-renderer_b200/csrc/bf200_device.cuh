@@ -19,9 +19,20 @@ struct alignas(16) BvhNode {
     int4 d;
 };
 
+// BVH4 node, 128 bytes (one L2 line): the boxes of up to four children in structure-of-arrays
+// form, so one node is eight 16-byte loads. child[k] >= 0: internal node index (always greater
+// than this node's own index, so a walk cannot revisit a node); child[k] < 0: leaf, the same code
+// as BvhNode. The used slots come first and info.x counts them; unused slots are never tested
+// (their boxes are not meaningful to the slab test).
+struct alignas(128) BvhNode4 {
+    float4 lo_x, hi_x, lo_y, hi_y, lo_z, hi_z;
+    int4 child;
+    int4 info;  // x: used child slots (1..4)
+};
+
 constexpr int kLeafCountBits = 3;
 constexpr int kMaxLeafSize = 1 << kLeafCountBits;
-constexpr int kTraversalStack = 96;  // up to 32 instance entries plus one BLAS path
+constexpr int kTraversalStack = 128;  // up to 32 instance entries plus one BLAS walk
 
 struct LightInfo {
     uint32_t instance;
@@ -47,7 +58,7 @@ struct SceneView {
     const float* positions;        // object space, 3 per vertex
     const float* normals;          // 3 per vertex
     const uint32_t* triangles;     // geometry-local vertex indices, 3 per triangle
-    const BvhNode* nodes;
+    const BvhNode4* nodes;
     const float4* leaf_tris;       // 3 per leaf triangle: v0 (w = primitive index bits), v1, v2
     const float4* world_normals;   // per instance triangle
     const ClosureData* closures;   // one per material

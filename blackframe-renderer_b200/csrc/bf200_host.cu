@@ -373,6 +373,125 @@ Box instance_world_box(const Box& object, const float* m4) {
     return b;
 }
 
+// ---------------------------------------------------------------------------------------------
+// BVH4 collapse: every BVH4 node takes a BVH2 node's two children and repeatedly opens the
+// internal child with the largest box surface area until it holds four children (or only
+// leaves). Halving the tree depth halves the dependent node fetches of a traversal.
+// ---------------------------------------------------------------------------------------------
+
+struct Collapser {
+    const std::vector<BvhNode>& bvh2;
+    std::vector<BvhNode4>& out;
+
+    struct Slot {
+        int code;
+        Box box;
+    };
+
+    static Box child_box(const BvhNode& n, int k) {
+        Box b;
+        if (k == 0) {
+            b.lo[0] = n.a.x; b.hi[0] = n.a.y; b.lo[1] = n.a.z; b.hi[1] = n.a.w; b.lo[2] = n.c.x; b.hi[2] = n.c.y;
+        } else {
+            b.lo[0] = n.b.x; b.hi[0] = n.b.y; b.lo[1] = n.b.z; b.hi[1] = n.b.w; b.lo[2] = n.c.z; b.hi[2] = n.c.w;
+        }
+        return b;
+    }
+
+    static bool empty(const Box& b) { return !(b.lo[0] <= b.hi[0] && b.lo[1] <= b.hi[1] && b.lo[2] <= b.hi[2]); }
+
+    // Builds the BVH4 node for BVH2 node `index`; returns its index in `out`.
+    int collapse(int index, uint32_t depth, uint32_t& max_depth) {
+        max_depth = std::max(max_depth, depth);
+        std::vector<Slot> slots;
+        for (int k = 0; k < 2; ++k) {
+            const Box b = child_box(bvh2[index], k);
+            if (!empty(b)) {
+                slots.push_back(Slot{k == 0 ? bvh2[index].d.x : bvh2[index].d.y, b});
+            }
+        }
+        while (slots.size() < 4) {
+            int open = -1;
+            double best = -1.0;
+            for (int k = 0; k < static_cast<int>(slots.size()); ++k) {
+                if (slots[k].code >= 0 && slots[k].box.area() > best) {
+                    best = slots[k].box.area();
+                    open = k;
+                }
+            }
+            if (open < 0) {
+                break;
+            }
+            const BvhNode& n = bvh2[slots[open].code];
+            slots.erase(slots.begin() + open);
+            for (int k = 0; k < 2; ++k) {
+                const Box b = child_box(n, k);
+                if (!empty(b)) {
+                    slots.push_back(Slot{k == 0 ? n.d.x : n.d.y, b});
+                }
+            }
+        }
+        const int me = static_cast<int>(out.size());
+        out.push_back(BvhNode4{});
+        int child[4] = {0, 0, 0, 0};
+        for (size_t k = 0; k < slots.size(); ++k) {
+            child[k] = slots[k].code >= 0 ? collapse(slots[k].code, depth + 1, max_depth) : slots[k].code;
+        }
+        const float inf = std::numeric_limits<float>::infinity();
+        float lo[3][4], hi[3][4];
+        for (int k = 0; k < 4; ++k) {
+            for (int a = 0; a < 3; ++a) {
+                lo[a][k] = k < static_cast<int>(slots.size()) ? slots[k].box.lo[a] : inf;
+                hi[a][k] = k < static_cast<int>(slots.size()) ? slots[k].box.hi[a] : -inf;
+            }
+        }
+        BvhNode4& node = out[me];
+        node.lo_x = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+        node.hi_x = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+        node.lo_y = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+        node.hi_y = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+        node.lo_z = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+        node.hi_z = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+        node.child = make_int4(child[0], child[1], child[2], child[3]);
+        node.info = make_int4(static_cast<int>(slots.size()), 0, 0, 0);
+        return me;
+    }
+};
+
+// Structural check of a collapsed BVH4 before upload: every node uses 1..4 slots, every internal
+// child index lies inside the array and above its parent's (so no walk can cycle), and every node
+// is reached exactly once from the roots.
+bool valid_bvh4(const std::vector<BvhNode4>& nodes, const std::vector<uint4>& geom_info) {
+    std::vector<uint32_t> refs(nodes.size(), 0);
+    for (const uint4& g : geom_info) {
+        if (g.z >= nodes.size()) {
+            return false;
+        }
+        ++refs[g.z];
+    }
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        const int used = nodes[i].info.x;
+        if (used < 1 || used > 4) {
+            return false;
+        }
+        const int child[4] = {nodes[i].child.x, nodes[i].child.y, nodes[i].child.z, nodes[i].child.w};
+        for (int k = 0; k < used; ++k) {
+            if (child[k] >= 0) {
+                if (static_cast<size_t>(child[k]) >= nodes.size() || static_cast<size_t>(child[k]) <= i) {
+                    return false;
+                }
+                ++refs[static_cast<size_t>(child[k])];
+            }
+        }
+    }
+    for (uint32_t r : refs) {
+        if (r != 1) {
+            return false;
+        }
+    }
+    return true;
+}
+
 template <typename T> blackframe_status upload(bf200_scene* s, const std::vector<T>& host, const T*& out) {
     const size_t bytes = std::max<size_t>(host.size() * sizeof(T), 16);
     void* p = nullptr;
@@ -977,12 +1096,17 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         std::vector<float4> leaf_tris;
         std::vector<uint4> geom_info(d->geometry_count);
         std::vector<Box> object_box(d->geometry_count);
+        std::vector<BvhNode4> nodes4;
         uint32_t blas_depth = 0;
         for (uint32_t g = 0; g < d->geometry_count; ++g) {
             uint32_t depth = 0;
             const uint32_t root = build_blas(*d, g, nodes, leaf_tris, depth);
-            blas_depth = std::max(blas_depth, depth);
-            geom_info[g] = make_uint4(d->geometries[g].vertex_offset, d->geometries[g].triangle_offset, root, 0);
+            uint32_t depth4 = 1;
+            Collapser collapser{nodes, nodes4};
+            const int root4 = collapser.collapse(static_cast<int>(root), 1, depth4);
+            blas_depth = std::max(blas_depth, 3 * depth4 + 1);  // at most 3 net entries per level
+            geom_info[g] = make_uint4(d->geometries[g].vertex_offset, d->geometries[g].triangle_offset,
+                                      static_cast<uint32_t>(root4), 0);
             const auto& geom = d->geometries[g];
             const uint32_t* local = d->triangles + 3ULL * geom.triangle_offset;
             for (uint32_t t = 0; t < 3 * geom.triangle_count; ++t) {
@@ -991,6 +1115,9 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         }
         // the traversal stack holds one instance-range entry plus one BLAS walk; instance ranges
         // carry 15-bit indices
+        if (!valid_bvh4(nodes4, geom_info)) {
+            return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "internal error: malformed BVH4");
+        }
         if (blas_depth + 3 + 32 >= kTraversalStack) {
             return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "BLAS deeper than the traversal stack allows");
         }
@@ -1006,10 +1133,10 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
             std::memcpy(&world_box[2ULL * i].w, &d->instances[i].visibility_mask, 4);  // mask bits, not a number
             world_box[2ULL * i + 1] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.0F);
         }
-        scene->node_count = nodes.size();
+        scene->node_count = nodes4.size();
         scene->triangle_count = leaf_tris.size() / 3;
         // leaf codes must stay inside their traversal-stack tag range (first leaf triangle < 2^27)
-        if (scene->triangle_count >= (1ULL << 27) || nodes.size() >= (1ULL << 30)) {
+        if (scene->triangle_count >= (1ULL << 27) || nodes4.size() >= (1ULL << 30)) {
             return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "scene exceeds 2^27 triangles or 2^30 BVH nodes");
         }
         // instances, mesh lights (FrameScene.cpp:201-261) and the uniform light sampler
@@ -1119,7 +1246,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         up(positions, v.positions);
         up(normals, v.normals);
         up(triangles, v.triangles);
-        up(nodes, v.nodes);
+        up(nodes4, v.nodes);
         up(leaf_tris, v.leaf_tris);
         up(closures, v.closures);
         up(emission, v.emission);

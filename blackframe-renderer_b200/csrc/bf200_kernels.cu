@@ -385,20 +385,52 @@ __device__ __forceinline__ bool precedes(float t, uint32_t inst, uint32_t prim, 
     return prim < best.primitive;
 }
 
-// Children of a node whose boxes the ray meets within [t_min, limit], the nearer one first.
-__device__ __forceinline__ int hit_children(const RayInv& r, const BvhNode& node, float t_min, float limit,
-                                            int (&kids)[2]) {
-    float n0, n1;
-    const bool h0 = slab(r, node.a.x, node.a.y, node.a.z, node.a.w, node.c.x, node.c.y, t_min, limit, n0);
-    const bool h1 = slab(r, node.b.x, node.b.y, node.b.z, node.b.w, node.c.z, node.c.w, t_min, limit, n1);
-    if (h0 && h1) {
-        const bool swap = n1 < n0;
-        kids[0] = swap ? node.d.y : node.d.x;
-        kids[1] = swap ? node.d.x : node.d.y;
-        return 2;
+// Children of a BVH4 node whose boxes the ray meets within [t_min, limit], ordered near to far
+// (a five-comparator sorting network on fixed slots, so everything stays in registers); returns
+// how many. Unused slots (k >= info.x) are never tested; missed and unused slots sort last with an
+// infinite distance.
+__device__ __forceinline__ void order_pair(float& na, int& ca, float& nb, int& cb) {
+    if (nb < na) {
+        const float tn = na;
+        na = nb;
+        nb = tn;
+        const int tc = ca;
+        ca = cb;
+        cb = tc;
     }
-    kids[0] = h0 ? node.d.x : node.d.y;
-    return h0 || h1 ? 1 : 0;
+}
+
+__device__ __forceinline__ int hit_children(const RayInv& r, const BvhNode4& n, float t_min, float limit,
+                                            int (&kids)[4]) {
+    float near[4];
+    int code[4];
+    int count = 0;
+    const float lox[4] = {n.lo_x.x, n.lo_x.y, n.lo_x.z, n.lo_x.w};
+    const float hix[4] = {n.hi_x.x, n.hi_x.y, n.hi_x.z, n.hi_x.w};
+    const float loy[4] = {n.lo_y.x, n.lo_y.y, n.lo_y.z, n.lo_y.w};
+    const float hiy[4] = {n.hi_y.x, n.hi_y.y, n.hi_y.z, n.hi_y.w};
+    const float loz[4] = {n.lo_z.x, n.lo_z.y, n.lo_z.z, n.lo_z.w};
+    const float hiz[4] = {n.hi_z.x, n.hi_z.y, n.hi_z.z, n.hi_z.w};
+    const int child[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
+    const int used = n.info.x;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float t = 0.0F;
+        const bool hit = k < used && slab(r, lox[k], hix[k], loy[k], hiy[k], loz[k], hiz[k], t_min, limit, t);
+        near[k] = hit ? t : kInf;
+        code[k] = child[k];
+        count += hit ? 1 : 0;
+    }
+    order_pair(near[0], code[0], near[1], code[1]);
+    order_pair(near[2], code[2], near[3], code[3]);
+    order_pair(near[0], code[0], near[2], code[2]);
+    order_pair(near[1], code[1], near[3], code[3]);
+    order_pair(near[1], code[1], near[2], code[2]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        kids[k] = code[k];
+    }
+    return count;
 }
 
 // Stack entries of both traversals: a BLAS node index (>= 0), a BLAS leaf (the node's child code,
@@ -481,13 +513,16 @@ __device__ __forceinline__ int next_leaf(const SceneView& s, const RayInv& world
         if (entry < 0) {
             return entry;
         }
-        int kids[2];
+        int kids[4];
         const int count = hit_children(w.r, s.nodes[entry], t_min, limit, kids);
-        for (int k = count - 1; k >= 0; --k) {
-            if (w.sp < kTraversalStack) {
-                stack.set(w.sp++, kids[k]);
-            } else {
-                w.failed = true;
+#pragma unroll
+        for (int k = 3; k >= 0; --k) {
+            if (k < count) {
+                if (w.sp < kTraversalStack) {
+                    stack.set(w.sp++, kids[k]);
+                } else {
+                    w.failed = true;
+                }
             }
         }
     }
@@ -620,9 +655,13 @@ __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
             stack.set(sp++, static_cast<int>(s.geom_info[s.inst_info[inst].x].z));
             continue;
         }
-        int kids[2];
+        int kids[4];
         const int count = hit_children(r, s.nodes[entry], t_min, t_max, kids);
-        for (int k = 0; k < count; ++k) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k >= count) {
+                break;
+            }
             const int child = kids[k];
             if (child >= 0) {
                 if (sp < kTraversalStack) {
