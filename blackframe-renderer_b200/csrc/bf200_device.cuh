@@ -31,6 +31,9 @@ struct alignas(128) BvhNode4 {
 };
 
 constexpr int kLeafCountBits = 3;
+// Scenes with at most this many instances test every instance box up front; larger ones walk a
+// TLAS over the instances' world boxes.
+constexpr uint32_t kEagerInstances = 32;
 constexpr int kMaxLeafSize = 1 << kLeafCountBits;
 constexpr int kTraversalStack = 128;  // up to 32 instance entries plus one BLAS walk
 
@@ -49,6 +52,7 @@ struct SceneView {
     uint32_t instance_count;
     uint32_t light_count;
     const float4* inst_world_box;  // padded world box per instance: lo (xyz, w = visibility mask bits), hi
+    int32_t tlas_root;             // BVH4 over the instances' world boxes (leaves ~instance), or -1
     const float4* inst_to_object;  // 3 rows (m0..m3) per instance
     const float4* inst_to_world;   // 3 rows per instance
     const uint4* inst_info;        // geometry, material, visibility mask, light index or ~0

@@ -184,8 +184,13 @@ struct Builder {
     const float* positions;  // geometry-local base
     const uint32_t* tris;
     uint32_t max_depth = 0;
+    int leaf_limit = kLeafSize;
+    bool instance_leaves = false;  // TLAS: one instance per leaf, encoded as ~instance
 
     int make_leaf(int begin, int end) {
+        if (instance_leaves) {
+            return ~static_cast<int>(prims[begin].index);
+        }
         const uint32_t first = static_cast<uint32_t>(leaf_tris.size() / 3);
         for (int i = begin; i < end; ++i) {
             const uint32_t t = prims[i].index;
@@ -214,7 +219,7 @@ struct Builder {
     int build(int begin, int end, uint32_t depth) {
         max_depth = std::max(max_depth, depth);
         const int n = end - begin;
-        if (n <= kLeafSize) {
+        if (n <= leaf_limit) {
             return make_leaf(begin, end);
         }
         Box cb;
@@ -373,6 +378,24 @@ Box instance_world_box(const Box& object, const float* m4) {
     return b;
 }
 
+// TLAS over the instances' padded world boxes: binned SAH, one instance per leaf (~instance).
+// Returns the BVH2 root index in `nodes`.
+int build_tlas(const std::vector<Box>& world, std::vector<BvhNode>& nodes) {
+    std::vector<Prim> prims(world.size());
+    for (size_t i = 0; i < world.size(); ++i) {
+        prims[i].box = world[i];
+        for (int a = 0; a < 3; ++a) {
+            prims[i].c[a] = 0.5F * world[i].lo[a] + 0.5F * world[i].hi[a];
+        }
+        prims[i].index = static_cast<uint32_t>(i);
+    }
+    std::vector<float4> unused;
+    Builder b{prims, nodes, unused, nullptr, nullptr};
+    b.leaf_limit = 1;
+    b.instance_leaves = true;
+    return b.build(0, static_cast<int>(prims.size()), 1);
+}
+
 // ---------------------------------------------------------------------------------------------
 // BVH4 collapse: every BVH4 node takes a BVH2 node's two children and repeatedly opens the
 // internal child with the largest box surface area until it holds four children (or only
@@ -461,13 +484,13 @@ struct Collapser {
 // Structural check of a collapsed BVH4 before upload: every node uses 1..4 slots, every internal
 // child index lies inside the array and above its parent's (so no walk can cycle), and every node
 // is reached exactly once from the roots.
-bool valid_bvh4(const std::vector<BvhNode4>& nodes, const std::vector<uint4>& geom_info) {
+bool valid_bvh4(const std::vector<BvhNode4>& nodes, const std::vector<uint32_t>& roots) {
     std::vector<uint32_t> refs(nodes.size(), 0);
-    for (const uint4& g : geom_info) {
-        if (g.z >= nodes.size()) {
+    for (const uint32_t root : roots) {
+        if (root >= nodes.size()) {
             return false;
         }
-        ++refs[g.z];
+        ++refs[root];
     }
     for (size_t i = 0; i < nodes.size(); ++i) {
         const int used = nodes[i].info.x;
@@ -1113,31 +1136,53 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
                 object_box[g].grow(d->positions + 3ULL * (geom.vertex_offset + local[t]));
             }
         }
-        // the traversal stack holds one instance-range entry plus one BLAS walk; instance ranges
-        // carry 15-bit indices
-        if (!valid_bvh4(nodes4, geom_info)) {
+        // instance ranges on the traversal stack carry 14-bit first indices
+        if (d->instance_count >= (1U << 14)) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "more than 16383 instances");
+        }
+        // instance level: the padded world box of every instance, tested before its ray transform;
+        // beyond kEagerInstances instances a BVH4 over those boxes (TLAS) leads to them
+        std::vector<Box> world_boxes(d->instance_count);
+        for (uint32_t i = 0; i < d->instance_count; ++i) {
+            world_boxes[i] = instance_world_box(object_box[d->instances[i].geometry_index],
+                                                d->instances[i].object_to_world);
+        }
+        int tlas_root = -1;
+        uint32_t instance_level_depth = kEagerInstances;  // entries an eager instance pass may push
+        if (d->instance_count > kEagerInstances) {
+            std::vector<BvhNode> tlas2;
+            const int root2 = build_tlas(world_boxes, tlas2);
+            uint32_t tlas_depth4 = 1;
+            Collapser collapser{tlas2, nodes4};
+            tlas_root = collapser.collapse(root2, 1, tlas_depth4);
+            instance_level_depth = 3 * tlas_depth4 + 1;
+        }
+        std::vector<uint32_t> roots;
+        for (const uint4& g : geom_info) {
+            roots.push_back(g.z);
+        }
+        if (tlas_root >= 0) {
+            roots.push_back(static_cast<uint32_t>(tlas_root));
+        }
+        if (!valid_bvh4(nodes4, roots)) {
             return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "internal error: malformed BVH4");
         }
-        if (blas_depth + 3 + 32 >= kTraversalStack) {
+        if (blas_depth + instance_level_depth + 3 >= kTraversalStack) {
             return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "BLAS deeper than the traversal stack allows");
         }
-        if (d->instance_count >= (1U << 15)) {
-            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "more than 32767 instances");
-        }
-        // instance level: the padded world box of every instance, tested before its ray transform
         std::vector<float4> world_box(2ULL * d->instance_count);
         for (uint32_t i = 0; i < d->instance_count; ++i) {
-            const Box b = instance_world_box(object_box[d->instances[i].geometry_index],
-                                             d->instances[i].object_to_world);
+            const Box& b = world_boxes[i];
             world_box[2ULL * i] = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.0F);
             std::memcpy(&world_box[2ULL * i].w, &d->instances[i].visibility_mask, 4);  // mask bits, not a number
             world_box[2ULL * i + 1] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.0F);
         }
         scene->node_count = nodes4.size();
         scene->triangle_count = leaf_tris.size() / 3;
-        // leaf codes must stay inside their traversal-stack tag range (first leaf triangle < 2^27)
-        if (scene->triangle_count >= (1ULL << 27) || nodes4.size() >= (1ULL << 30)) {
-            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "scene exceeds 2^27 triangles or 2^30 BVH nodes");
+        // leaf codes and TLAS node indices must stay inside their traversal-stack tag ranges
+        // (first leaf triangle < 2^27, node index < 2^29)
+        if (scene->triangle_count >= (1ULL << 27) || nodes4.size() >= (1ULL << 29)) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "scene exceeds 2^27 triangles or 2^29 BVH nodes");
         }
         // instances, mesh lights (FrameScene.cpp:201-261) and the uniform light sampler
         std::vector<float4> to_object(3ULL * d->instance_count), to_world(3ULL * d->instance_count);
@@ -1230,6 +1275,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         SceneView& v = scene->view;
         v.instance_count = d->instance_count;
         v.light_count = scene->light_count;
+        v.tlas_root = tlas_root;
         blackframe_status st = BLACKFRAME_STATUS_SUCCESS;
         auto up = [&](auto& host, auto& dst) {
             if (st == BLACKFRAME_STATUS_SUCCESS) {

@@ -248,10 +248,24 @@ __device__ __forceinline__ int triangle_test(float4 v0, float4 v1, float4 v2, F3
         }
         return slow_path(v0, v1, v2, o, d, t_min, t_max, __int_as_float(0x7fc00000), want_bary, hit);
     }
-    const double vol = det_terms(p0, p1, p2, perm);
-    const double vol_bound = 16.0 * kU * perm;
-    const double det = (e[0] + e[1]) + e[2];
-    const double det_bound = bound[0] + bound[1] + bound[2] + 4.0 * kU * fabs(det);
+    // vol = det(p0, p1, p2) and det = e0 + e1 + e2 have the exact values p0 . N and d . N with
+    // N = (v1 - v0) x (v2 - v0) (the scalar triple product identities). Evaluated in that form
+    // their rounding error scales with the triangle's own size instead of its distance from the ray
+    // origin, so small distant triangles certify their parameter without the exact fallback; the
+    // quotient certified is still the exact one, so t is unchanged. Error bound: each edge
+    // difference and product rounds once (u), each cross component and three-term dot product
+    // rounds twice and three times more, at most 8u of the magnitudes summed below; 16u is used.
+    const double e1x = double(v1.x) - double(v0.x), e1y = double(v1.y) - double(v0.y),
+                 e1z = double(v1.z) - double(v0.z);
+    const double e2x = double(v2.x) - double(v0.x), e2y = double(v2.y) - double(v0.y),
+                 e2z = double(v2.z) - double(v0.z);
+    const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    const double ax = fabs(e1y * e2z) + fabs(e1z * e2y), ay = fabs(e1z * e2x) + fabs(e1x * e2z),
+                 az = fabs(e1x * e2y) + fabs(e1y * e2x);
+    const double vol = (p0[0] * nx + p0[1] * ny) + p0[2] * nz;
+    const double vol_bound = 16.0 * kU * ((fabs(p0[0]) * ax + fabs(p0[1]) * ay) + fabs(p0[2]) * az);
+    const double det = (dd[0] * nx + dd[1] * ny) + dd[2] * nz;
+    const double det_bound = 16.0 * kU * ((fabs(dd[0]) * ax + fabs(dd[1]) * ay) + fabs(dd[2]) * az);
     float t = certain_round(vol, vol_bound, det, det_bound);
     if (isnan(t)) {
         if (!exact_diffs()) {
@@ -434,27 +448,29 @@ __device__ __forceinline__ int hit_children(const RayInv& r, const BvhNode4& n, 
 }
 
 // Stack entries of both traversals: a BLAS node index (>= 0), a BLAS leaf (the node's child code,
-// in [-2^30, 0): ~child = first_leaf_triangle << 3 | (count - 1)), or an instance range
-// (kInstanceEntry + (first << 15 | count), below -2^30): the instances [first, first + count)
-// still to visit, in index order. One entry stands for all instances, so starting a ray costs
-// one push, and each instance's world box is tested when its turn comes.
+// in [-2^30, 0): ~child = first_leaf_triangle << 3 | (count - 1)), or an instance-level entry
+// below -2^30, kInstanceEntry + code with code < 2^30: a TLAS node (code = kTlasFlag | node) or an
+// instance range (code = first << 15 | count: the instances [first, first + count), index order).
 constexpr int kInstanceEntry = INT_MIN;
 constexpr int kLeafEntryMin = -(1 << 30);
 constexpr int kInstanceBits = 15;
-// Scenes with at most this many instances test every instance box up front in any_hit.
-constexpr uint32_t kEagerInstances = 32;
+constexpr uint32_t kTlasFlag = 1U << 29;
 
 __device__ __forceinline__ int instance_range(uint32_t first, uint32_t count) {
     return kInstanceEntry + static_cast<int>((first << kInstanceBits) | count);
 }
 
+__device__ __forceinline__ int tlas_entry(int node) {
+    return kInstanceEntry + static_cast<int>(kTlasFlag | static_cast<uint32_t>(node));
+}
+
 // Starts a walk's stack. With few instances every visible instance whose world box the ray meets
 // within [t_min, t_max] goes on as a one-instance range, the lowest index on top, with the warp in
-// step; otherwise one range entry stands for all instances and their boxes are tested as they come.
+// step; otherwise the TLAS root goes on and the instance boxes are met through it.
 __device__ __forceinline__ void push_instances(const SceneView& s, const RayInv& world, float t_min, float t_max,
                                                uint32_t mask, TraversalStack& stack, int& sp) {
-    if (s.instance_count > kEagerInstances) {
-        stack.set(sp++, instance_range(0U, s.instance_count));
+    if (s.tlas_root >= 0) {
+        stack.set(sp++, tlas_entry(s.tlas_root));
         return;
     }
     for (int inst = static_cast<int>(s.instance_count) - 1; inst >= 0; --inst) {
@@ -466,6 +482,55 @@ __device__ __forceinline__ void push_instances(const SceneView& s, const RayInv&
         }
         stack.set(sp++, instance_range(static_cast<uint32_t>(inst), 1U));
     }
+}
+
+// One instance-level entry of a walk. A TLAS node pushes the children the world ray meets within
+// [t_min, limit] (nodes as TLAS entries, instance leaves as one-instance ranges, the nearest on
+// top) and returns false. An instance range yields its first instance: false when the ray's
+// visibility mask excludes it or its world box is not met; otherwise the ray moves into its
+// object space, its BLAS root goes on above the rest of the range, and the call returns true.
+__device__ __forceinline__ bool instance_step(const SceneView& s, int entry, const RayInv& world, F3 o, F3 d,
+                                              float t_min, float limit, uint32_t mask, TraversalStack& stack,
+                                              int& sp, bool& failed, uint32_t& inst_out, F3& ro, F3& rd,
+                                              RayInv& r) {
+    const uint32_t code = static_cast<uint32_t>(entry - kInstanceEntry);
+    if (code & kTlasFlag) {
+        int kids[4];
+        const int count = hit_children(world, s.nodes[code & (kTlasFlag - 1U)], t_min, limit, kids);
+#pragma unroll
+        for (int k = 3; k >= 0; --k) {
+            if (k < count) {
+                if (sp < kTraversalStack) {
+                    stack.set(sp++, kids[k] >= 0 ? tlas_entry(kids[k])
+                                                 : instance_range(static_cast<uint32_t>(~kids[k]), 1U));
+                } else {
+                    failed = true;
+                }
+            }
+        }
+        return false;
+    }
+    const uint32_t inst = code >> kInstanceBits, count = code & ((1U << kInstanceBits) - 1U);
+    if (count > 1U) {
+        stack.set(sp++, instance_range(inst + 1U, count - 1U));
+    }
+    const float4 blo = s.inst_world_box[2ULL * inst], bhi = s.inst_world_box[2ULL * inst + 1];
+    float near;
+    if ((mask & __float_as_uint(blo.w)) == 0U ||
+        !slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, limit, near)) {
+        return false;
+    }
+    if (sp >= kTraversalStack) {
+        failed = true;
+        return false;
+    }
+    inst_out = inst;
+    const float4* m = s.inst_to_object + 3ULL * inst;
+    ro = xform_point(m, o);
+    rd = xform_vector(m, d);
+    r = make_ray_inv(ro, rd);
+    stack.set(sp++, static_cast<int>(s.geom_info[s.inst_info[inst].x].z));
+    return true;
 }
 
 // Per-lane walk state shared by the two traversals.
@@ -487,27 +552,7 @@ __device__ __forceinline__ int next_leaf(const SceneView& s, const RayInv& world
     while (w.sp > 0) {
         const int entry = stack.get(--w.sp);
         if (entry < kLeafEntryMin) {
-            const uint32_t code = static_cast<uint32_t>(entry - kInstanceEntry);
-            const uint32_t inst = code >> kInstanceBits, count = code & ((1U << kInstanceBits) - 1U);
-            if (count > 1U) {
-                stack.set(w.sp++, instance_range(inst + 1U, count - 1U));
-            }
-            const float4 blo = s.inst_world_box[2ULL * inst], bhi = s.inst_world_box[2ULL * inst + 1];
-            float near;
-            if ((mask & __float_as_uint(blo.w)) == 0U ||
-                !slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, limit, near)) {
-                continue;
-            }
-            if (w.sp >= kTraversalStack) {
-                w.failed = true;
-                continue;
-            }
-            w.inst = inst;
-            const float4* m = s.inst_to_object + 3ULL * inst;
-            w.ro = xform_point(m, o);
-            w.rd = xform_vector(m, d);
-            w.r = make_ray_inv(w.ro, w.rd);
-            stack.set(w.sp++, static_cast<int>(s.geom_info[s.inst_info[inst].x].z));
+            instance_step(s, entry, world, o, d, t_min, limit, mask, stack, w.sp, w.failed, w.inst, w.ro, w.rd, w.r);
             continue;
         }
         if (entry < 0) {
@@ -633,26 +678,8 @@ __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
     while (sp > 0) {
         const int entry = stack.get(--sp);
         if (entry < kLeafEntryMin) {
-            const uint32_t code = static_cast<uint32_t>(entry - kInstanceEntry);
-            const uint32_t inst = code >> kInstanceBits, count = code & ((1U << kInstanceBits) - 1U);
-            if (count > 1U) {
-                stack.set(sp++, instance_range(inst + 1U, count - 1U));
-            }
-            const float4 blo = s.inst_world_box[2ULL * inst], bhi = s.inst_world_box[2ULL * inst + 1];
-            float near;
-            if ((mask & __float_as_uint(blo.w)) == 0U ||
-                !slab(world, blo.x, bhi.x, blo.y, bhi.y, blo.z, bhi.z, t_min, t_max, near)) {
-                continue;
-            }
-            if (sp >= kTraversalStack) {
-                failed = true;
-                continue;
-            }
-            const float4* m = s.inst_to_object + 3ULL * inst;
-            ro = xform_point(m, o);
-            rd = xform_vector(m, d);
-            r = make_ray_inv(ro, rd);
-            stack.set(sp++, static_cast<int>(s.geom_info[s.inst_info[inst].x].z));
+            uint32_t inst = 0U;
+            instance_step(s, entry, world, o, d, t_min, t_max, mask, stack, sp, failed, inst, ro, rd, r);
             continue;
         }
         int kids[4];
