@@ -84,13 +84,6 @@ struct Dets {
     double d[3];
 };
 
-__device__ __forceinline__ double det_terms(const double* a, const double* b, const double* c, double& perm) {
-    const double t1 = a[0] * b[1] * c[2], t2 = a[1] * b[2] * c[0], t3 = a[2] * b[0] * c[1];
-    const double t4 = a[2] * b[1] * c[0], t5 = a[1] * b[0] * c[2], t6 = a[0] * b[2] * c[1];
-    perm = fabs(t1) + fabs(t2) + fabs(t3) + fabs(t4) + fabs(t5) + fabs(t6);
-    return ((t1 + t2) + t3) - ((t4 + t5) + t6);
-}
-
 // Exact evaluation of the four determinants as double expansions and an exact decision.
 // Returns kTriHit with t (and barycentrics if requested), kTriMiss, or kTriFailure when a
 // coordinate difference is not exact in double (exponent gap above 29 bits).
@@ -205,6 +198,18 @@ __device__ __forceinline__ float certain_round(double num, double num_bound, dou
 
 // Returns kTriHit (t set), kTriMiss or kTriFailure. Object-space floats in; the decision and
 // the parameter equal those of the exact test in Triangle.hpp:683-822.
+// d . (p x f) and a bound on its evaluation error: edge differences, products and the two
+// subtractions / additions round at most seven times along any term, so the error is below
+// 8u * sum |d_i| (|p_j f_k| + |p_k f_j|); 16u of that sum is returned as the bound.
+__device__ __forceinline__ double edge_function(const double (&p)[3], double fx, double fy, double fz,
+                                                const double (&dd)[3], double& bound) {
+    const double cx = p[1] * fz - p[2] * fy, cy = p[2] * fx - p[0] * fz, cz = p[0] * fy - p[1] * fx;
+    const double bx = fabs(p[1] * fz) + fabs(p[2] * fy), by = fabs(p[2] * fx) + fabs(p[0] * fz),
+                 bz = fabs(p[0] * fy) + fabs(p[1] * fx);
+    bound = 16.0 * kU * ((fabs(dd[0]) * bx + fabs(dd[1]) * by) + fabs(dd[2]) * bz);
+    return (dd[0] * cx + dd[1] * cy) + dd[2] * cz;
+}
+
 __device__ __forceinline__ int triangle_test(float4 v0, float4 v1, float4 v2, F3 o, F3 d, float t_min, float t_max,
                                              bool want_bary, TriangleHit& hit) {
     const double ox = o.x, oy = o.y, oz = o.z;
@@ -212,14 +217,17 @@ __device__ __forceinline__ int triangle_test(float4 v0, float4 v1, float4 v2, F3
     const double p1[3] = {double(v1.x) - ox, double(v1.y) - oy, double(v1.z) - oz};
     const double p2[3] = {double(v2.x) - ox, double(v2.y) - oy, double(v2.z) - oz};
     const double dd[3] = {d.x, d.y, d.z};
-    double perm;
+    // Edge functions e0 = det(p1, p2, d), e1 = det(p2, p0, d), e2 = det(p0, p1, d), evaluated as
+    // e0 = d . (p1 x (v2 - v1)), e1 = d . (p2 x (v0 - v2)), e2 = d . (p0 x (v1 - v0)): the same
+    // exact values (p_j = p_i + v_j - v_i), with terms of the size (distance x edge) instead of
+    // distance squared, so their error bounds stay small for small distant triangles.
     double e[3], bound[3];
-    e[0] = det_terms(p1, p2, dd, perm);
-    bound[0] = 16.0 * kU * perm;
-    e[1] = det_terms(p2, p0, dd, perm);
-    bound[1] = 16.0 * kU * perm;
-    e[2] = det_terms(p0, p1, dd, perm);
-    bound[2] = 16.0 * kU * perm;
+    e[0] = edge_function(p1, double(v2.x) - double(v1.x), double(v2.y) - double(v1.y),
+                         double(v2.z) - double(v1.z), dd, bound[0]);
+    e[1] = edge_function(p2, double(v0.x) - double(v2.x), double(v0.y) - double(v2.y),
+                         double(v0.z) - double(v2.z), dd, bound[1]);
+    e[2] = edge_function(p0, double(v1.x) - double(v0.x), double(v1.y) - double(v0.y),
+                         double(v1.z) - double(v0.z), dd, bound[2]);
     int pos = 0, neg = 0;
     bool ambiguous = false;
 #pragma unroll
