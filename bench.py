@@ -48,7 +48,7 @@ STAGE_KERNELS = {"trace": "k_trace", "shade": "k_shade<kind> x4 + route/shadow c
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per processed unit, from one ncu
 # capture of a full-wavefront launch (2,097,152 segments) of each stage's kernels in this build;
 # profiles/stages_cornell_spheres_256_spp64.md holds the capture and its command
-MEASURED_TRAFFIC_PER_UNIT = {"trace": 57.7, "shade": 350.0, "occlude": None}
+MEASURED_TRAFFIC_PER_UNIT = {"trace": 56.5, "shade": 372.0, "occlude": None}
 TRAFFIC_SOURCE = "profiles/stages_cornell_spheres_256_spp64.md"
 
 
