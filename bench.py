@@ -158,6 +158,81 @@ def cpu_sample_rate(target_seconds=15.0):
     return n / elapsed, threads, kind, sample, n, elapsed
 
 
+BATCH_WORKLOAD = "batch64"
+
+
+def run_batch(args, torch, rank):
+    """The 64-scene batch: one bf200_render_films_device call over 64 uneven jobs against the same
+    64 jobs rendered one after another with bf200_render_film_device. Each step renders every job
+    once; both arms are timed with CUDA events around the whole step (films zeroed before)."""
+    if rank != 0:
+        return
+    g = np.load(os.path.join(REPO, "tests", "golden", f"{WORKLOAD}.npz"))
+    from helpers import sensor_from_golden
+    sensor = sensor_from_golden(g)
+    ctx = runtime.Context(0, path_capacity=args.capacity)
+    jobs, films, paths, triangles = [], [], 0, 0
+    for seed in range(64):
+        builder, options, (w, h, spp) = scenes.batch_job(seed)
+        scene = ctx.create_scene(builder)
+        cam = runtime.camera_create(*scenes.camera_frame_inputs(), w, h, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+        sums = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+        counts = torch.zeros((h, w), dtype=torch.int64, device="cuda")
+        jobs.append([scene, cam, sensor, options, spp, 0, 0, 0, sums.data_ptr(), counts.data_ptr(), builder])
+        films.append((sums, counts))
+        paths += w * h * spp
+        triangles += builder.triangle_count
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def batched():
+        return ctx.render_films_device([j[:10] for j in jobs], lanes=args.lanes)
+
+    def serial():
+        return [ctx.render_film_device(*j[:10]) for j in jobs]
+
+    def timed(fn, step):
+        for sums, counts in films:
+            sums.zero_()
+            counts.zero_()
+        flush.fill_(step & 0xFF)
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        reports = fn()
+        stop.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop), reports
+
+    for step in range(args.warmup):
+        timed(batched, step)
+        timed(serial, step)
+    batch_ms, serial_ms, failed = [], [], 0
+    with ClockSampler(0) as clocks:
+        for step in range(args.steps):
+            ms, reports = timed(batched, step)
+            batch_ms.append(ms)
+            failed += sum(r.failed_lanes for r in reports)
+            ms, _ = timed(serial, step)
+            serial_ms.append(ms)
+    batch_total, serial_total = sum(batch_ms), sum(serial_ms)
+    value = paths * args.steps / (batch_total / 1000.0)
+    serial_value = paths * args.steps / (serial_total / 1000.0)
+    line = {
+        "metric": "batched path samples/s", "value": value, "unit": "path samples/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "jobs": 64, "paths_per_step": paths, "unique_triangles": triangles,
+                   "lanes": args.lanes or "autotuned", "path_capacity": args.capacity,
+                   "l2": "flushed between steps (256 MiB write)"},
+        "serial": {"value": serial_value, "ms_per_step": serial_total / args.steps},
+        "batched_vs_serial": value / serial_value, "failed_lanes": failed, "clocks": clocks.summary(),
+    }
+    for j in jobs:
+        j[0].close()
+    ctx.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -192,8 +267,10 @@ def main():
     parser.add_argument("--reference-seconds", type=float, default=8.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's)")
-    parser.add_argument("--workload", default=WORKLOAD, choices=sorted(scenes.WORKLOADS),
-                        help="scene and frame (default: the headline Cornell + spheres frame)")
+    parser.add_argument("--workload", default=WORKLOAD, choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD],
+                        help="scene and frame (default: the headline Cornell + spheres frame); "
+                             f"{BATCH_WORKLOAD}: the 64-scene batch against 64 serial renders")
+    parser.add_argument("--lanes", type=int, default=0, help="batch lanes (0: autotuned)")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -209,6 +286,9 @@ def main():
     from datetime import timedelta
 
     torch.cuda.set_device(local_rank)
+    if args.workload == BATCH_WORKLOAD:
+        run_batch(args, torch, rank)
+        return
     distributed = world > 1
     if distributed:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),

@@ -146,6 +146,13 @@ class Film(C.Structure):
                 ("sums", C.c_void_p), ("sample_counts", C.POINTER(u64))]
 
 
+class FilmJob(C.Structure):
+    _fields_ = [("struct_size", u32), ("reserved", u32), ("scene", C.c_void_p),
+                ("camera", C.POINTER(Camera)), ("sensor", C.POINTER(Sensor)),
+                ("request", C.POINTER(FilmRequest)), ("options", C.c_void_p), ("film", C.POINTER(Film)),
+                ("report", C.c_void_p)]
+
+
 class Report(C.Structure):
     _fields_ = [("struct_size", u32), ("registered_light_count", u32), ("path_count", u64),
                 ("extension_segments", u64), ("shadow_segments", u64),
@@ -165,7 +172,7 @@ class Hit(C.Structure):
 EXPECTED_SIZES = {
     Closure: 64, Material: 80, Geometry: 32, Instance: 160, Ray: 48, SampleIndex: 24,
     PathInput: 80, PathResult: 128, TransportOptions: 64, Camera: 88, Sensor: 80,
-    FilmRequest: 40, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
+    FilmRequest: 40, FilmJob: 64, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
 }
 
 

@@ -23,6 +23,7 @@ EXPORTED_SYMBOLS = [
     "bf200_trace_paths_device", "bf200_render_film", "bf200_render_film_device",
     "bf200_closest_hits", "bf200_occlusions", "bf200_build_info", "bf200_camera_create",
     "bf200_trace_paths_device_noalloc", "bf200_sobol_bits", "bf200_owen_sobol_bits",
+    "bf200_render_films_device",
 ]
 
 
@@ -70,6 +71,8 @@ def library():
     lib.bf200_camera_create.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_uint32, C.c_uint32, C.c_float,
                                                                       C.c_float, C.c_uint32, C.POINTER(abi.Camera)]
     lib.bf200_camera_create.restype = C.c_uint32
+    lib.bf200_render_films_device.argtypes = [vp, C.POINTER(abi.FilmJob), C.c_uint32, C.c_uint32]
+    lib.bf200_render_films_device.restype = C.c_uint32
     lib.bf200_sobol_bits.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
     lib.bf200_sobol_bits.restype = C.c_uint32
     lib.bf200_owen_sobol_bits.argtypes = [C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(C.c_uint64)]
@@ -162,6 +165,45 @@ class Context:
                                                                C.byref(options), device_results, path_capacity,
                                                                C.byref(report)),
                     "trace_paths_device_noalloc")
+        return report
+
+    def render_films_device(self, jobs, lanes=0):
+        """bf200_render_films_device. `jobs`: (scene, camera, sensor, options, samples_per_pixel,
+        seed, first_sample, precision, sums_ptr, counts_ptr) tuples with device film pointers.
+        Returns one report per job."""
+        n = len(jobs)
+        records = (abi.FilmJob * n)()
+        keep = []
+        reports = [abi.Report() for _ in range(n)]
+        for k, (scene, camera, sensor, options, spp, seed, first, precision, sums, counts) in enumerate(jobs):
+            request = abi.FilmRequest(C.sizeof(abi.FilmRequest), spp, first, seed, precision)
+            film = abi.Film(camera.width, camera.height, precision, 0, C.c_void_p(sums),
+                            C.cast(C.c_void_p(counts), C.POINTER(abi.u64)))
+            keep += [request, film, camera, sensor, options]
+            r = records[k]
+            r.struct_size = C.sizeof(abi.FilmJob)
+            r.scene = scene.handle
+            r.camera = C.pointer(camera)
+            r.sensor = C.pointer(sensor)
+            r.request = C.pointer(request)
+            r.options = C.cast(C.pointer(options), C.c_void_p)
+            r.film = C.pointer(film)
+            reports[k].struct_size = C.sizeof(abi.Report)
+            r.report = C.cast(C.pointer(reports[k]), C.c_void_p)
+        self._check(library().bf200_render_films_device(self.handle, records, n, lanes), "render_films_device")
+        return reports
+
+    def render_film_device(self, scene, camera, sensor, options, samples_per_pixel, seed, first_sample, precision,
+                           sums, counts):
+        """bf200_render_film_device with device film pointers; returns the report."""
+        request = abi.FilmRequest(C.sizeof(abi.FilmRequest), samples_per_pixel, first_sample, seed, precision)
+        film = abi.Film(camera.width, camera.height, precision, 0, C.c_void_p(sums),
+                        C.cast(C.c_void_p(counts), C.POINTER(abi.u64)))
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_render_film_device(self.handle, scene.handle, C.byref(camera), C.byref(sensor),
+                                                       C.byref(request), C.byref(options), C.byref(film),
+                                                       C.byref(report)), "render_film_device")
         return report
 
     def render_film(self, scene, camera, sensor, options, samples_per_pixel, seed=0, first_sample=0,

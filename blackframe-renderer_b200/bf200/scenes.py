@@ -528,6 +528,59 @@ def bvh_stress(builder, subdivisions=7, instances=40, light_divisions=32):
     return builder
 
 
+# ------------------------------------------------------------------------------------------------
+# Batch of uneven scenes: seeded Cornell shells holding displaced icospheres
+# ------------------------------------------------------------------------------------------------
+
+def batch_job(seed):
+    """One job of the 64-scene batch (seed s = 0..63): film side log-uniform in [64, 512],
+    unique triangle count log-uniform in [1k, 200k] reached with displaced icospheres (the largest
+    subdivision with 20 * 4^s below the target, as many as round to it) inside the Cornell walls
+    and light,
+    spp log-uniform in [8, 128], depth uniform in {4..16}, materials drawn like the BVH-stress
+    scene's. Returns (builder, options, (width, height, spp))."""
+    rng = np.random.default_rng(10_000 + seed)
+    side = int(round(math.exp(rng.uniform(math.log(64), math.log(512)))))
+    target = math.exp(rng.uniform(math.log(1_000), math.log(200_000)))
+    spp = int(round(math.exp(rng.uniform(math.log(8), math.log(128)))))
+    depth = int(rng.integers(4, 17))
+    builder = SceneBuilder()
+    nm = builder.nanometers
+    white = builder.add_material(lambertian([0.73] * 4))
+    red = builder.add_material(lambertian(tabulated_spectrum(RED_WALL, nm)))
+    green = builder.add_material(lambertian(tabulated_spectrum(GREEN_WALL, nm)))
+    light = builder.add_material(lambertian([0.0] * 4), emission=(17.0, 17.0, 17.0, 17.0))
+    walls = [
+        (quad([(-1, -1, 0), (-1, -1, 2), (1, -1, 2), (1, -1, 0)], (0, 1, 0)), white),
+        (quad([(-1, 1, 0), (1, 1, 0), (1, 1, 2), (-1, 1, 2)], (0, -1, 0)), white),
+        (quad([(-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0)], (0, 0, 1)), white),
+        (quad([(-1, -1, 0), (-1, 1, 0), (-1, 1, 2), (-1, -1, 2)], (1, 0, 0)), red),
+        (quad([(1, -1, 0), (1, -1, 2), (1, 1, 2), (1, 1, 0)], (-1, 0, 0)), green),
+        (quad([(-0.125, 0.985, 0.875), (0.125, 0.985, 0.875), (0.125, 0.985, 1.125), (-0.125, 0.985, 1.125)],
+              (0, -1, 0)), light),
+    ]
+    for mesh, material in walls:
+        builder.add_instance(builder.add_mesh(mesh), material)
+    subdivision = max(1, int(math.floor(math.log(target / 20.0, 4))))
+    copies = max(1, int(round(target / (20 * 4 ** subdivision))))
+    gold_eta, gold_k = tabulated_spectrum(GOLD_ETA, nm), tabulated_spectrum(GOLD_K, nm)
+    for c in range(copies):
+        kind = rng.uniform()
+        if kind < 0.5:
+            material = builder.add_material(lambertian(rng.uniform(0.2, 0.8, 4)))
+        elif kind < 0.8:
+            ax, ay = rng.uniform(0.05, 0.6, 2)
+            material = builder.add_material(rough_conductor([1.0] * 4, gold_eta, gold_k, ax, ay))
+        else:
+            material = builder.add_material(rough_dielectric([1.0] * 4, 1.0, 1.5, 0.1, 0.1))
+        radius = 0.25 if copies == 1 else 0.2
+        centre = (rng.uniform(-0.6, 0.6), rng.uniform(-0.7, 0.3), rng.uniform(0.5, 1.6))
+        sphere = builder.add_mesh(displaced_icosphere(subdivision, 0.05, 100 * seed + c))
+        builder.add_instance(sphere, material, uniform_scale_translate(radius, centre))
+    options = abi.default_options(mis="power", max_depth=depth)
+    return builder, options, (side, side, spp)
+
+
 BVH_STRESS_CAMERA = ((0.0, 2.0, 24.0), (0.0, -3.0, 0.0))  # origin, target
 BVH_STRESS_VFOV = 0.9
 

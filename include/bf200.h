@@ -502,6 +502,32 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_film_device(
     const bf200_transport_options_v1* options, bf200_film_v1* device_film,
     bf200_report_v1* report) BF200_NOEXCEPT;
 
+/* One film of a batch: the arguments of one bf200_render_film_device call. */
+typedef struct bf200_film_job_v1 {
+    uint32_t struct_size;
+    uint32_t reserved;
+    const bf200_scene* scene;
+    const bf200_camera_v1* camera;
+    const bf200_sensor_v1* sensor;
+    const bf200_film_request_v1* request;
+    const bf200_transport_options_v1* options;
+    bf200_film_v1* film;      /* device film of this job */
+    bf200_report_v1* report;  /* optional */
+} bf200_film_job_v1;
+
+/* Renders many films, of any scenes of the context, in one call: the batch rendering the
+ * reference's benchmark plan asks of a new backend (many scenes and views of uneven size). Every
+ * job's film equals, bit for bit, the film of a bf200_render_film_device call with the same
+ * arguments. Jobs run concurrently in `lanes` wavefront lanes (0: chosen from the jobs' path
+ * counts and the context's path capacity): each lane has its own CUDA stream, a slice of the
+ * path slots and its own radiance buffer, and the host keeps every lane busy without waiting
+ * on any single one. Jobs must not share a film (their accumulation order across jobs would be
+ * unspecified). Reports carry counts, not stage timings. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_films_device(bf200_context* context,
+                                                                        const bf200_film_job_v1* jobs,
+                                                                        uint32_t job_count, uint32_t lanes)
+    BF200_NOEXCEPT;
+
 /* Closest-hit query for a batch of world rays (trace_cuda_closest_hits, ClosestHit.hpp:21-28).
  * Per ray writes t, barycentrics b0..b2, instance index and primitive index (0xffffffff on a
  * miss). Host pointers. */
