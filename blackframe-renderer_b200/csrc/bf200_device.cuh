@@ -159,7 +159,8 @@ struct Wavefront {
     uint32_t* tile_counts;     // compaction scratch: kCompactMaxRoutes x tiles
     // counters: [0] shadow queue size, [1] next path to claim, [2] active slots,
     //           [3] extension segments, [4] shadow segments, [5] failed lanes,
-    //           [6] first failure path (min), [7] first failure code, [8] k_trace fetch cursor
+    //           [6] first failure path (min), [7] first failure code, [8] k_trace fetch cursor,
+    //           [9] iterations and [10] iteration-bound flag of a device-side loop
     unsigned long long* counters;
 };
 

@@ -753,7 +753,7 @@ blackframe_status ensure_capacity(bf200_context* c) {
         return cuda_fail(c, e, "wavefront allocation");
     }
     carve_wavefront(static_cast<char*>(c->arena), n, &c->w);
-    e = cudaMallocHost(&c->pinned_counters, 8 * sizeof(unsigned long long));
+    e = cudaMallocHost(&c->pinned_counters, 16 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         return cuda_fail(c, e, "pinned counters");
     }
@@ -836,9 +836,115 @@ blackframe_status sobol_table(bf200_context* c, const bf200_transport_options_v1
     return BLACKFRAME_STATUS_SUCCESS;
 }
 
-// Runs the persistent wavefront until every path of `src` has been traced and retired.
+// The persistent wavefront as one CUDA graph: a conditional WHILE node whose body is one iteration
+// (the stage kernels and k_iteration_gate, which decides on the device whether another iteration
+// runs), so the whole trace is one graph launch with no host round trip per iteration. The gate
+// stops at the same iteration bound as the host loop.
+blackframe_status run_wavefront_graph(bf200_context* c, const bf200_scene* s, PathSource src,
+                                      const TransportParams& p, bf200_report_v1* report) {
+    Wavefront& w = c->w;
+    cudaStream_t st = c->stream;
+    cudaError_t e = cudaMemsetAsync(w.state, 0, w.capacity, st);
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(w.counters, 0, 16 * sizeof(unsigned long long), st);
+    }
+    if (e == cudaSuccess) {  // counters[6], the first failing path, is a minimum
+        e = cudaMemsetAsync(w.counters + 6, 0xFF, sizeof(unsigned long long), st);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "wavefront reset");
+    }
+    const uint32_t grid =
+        std::max<uint32_t>(1, std::min<uint32_t>((w.capacity + 255U) / 256U, c->sm_count * 8U));
+    const uint64_t depth_bound = static_cast<uint64_t>(p.limits[0]) + p.limits[1] + p.limits[2] + 2;
+    const uint64_t max_iterations = 64 + 2 * (src.total / w.capacity + 2) * depth_bound;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle loop = 0;
+    uint32_t per_iteration = 0;
+    e = cudaGraphCreate(&graph, 0);
+    if (e == cudaSuccess) {
+        e = cudaGraphConditionalHandleCreate(&loop, graph, 1U, cudaGraphCondAssignDefault);
+    }
+    cudaGraphNode_t node = nullptr;
+    cudaGraphNodeParams params{};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = loop;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    if (e == cudaSuccess) {
+        e = cudaGraphAddNode(&node, graph, nullptr, 0, &params);
+    }
+    if (e == cudaSuccess) {
+        cudaGraph_t body = params.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        for (int stage = 0; stage < 4 && e == cudaSuccess; ++stage) {
+            e = launch_stage(stage, s->view, w, src, p, grid, st, &per_iteration);
+        }
+        if (e == cudaSuccess) {
+            e = launch_gate(w, src.total, max_iterations, loop, st);
+            ++per_iteration;
+        }
+        cudaGraph_t captured = nullptr;
+        const cudaError_t end = cudaStreamEndCapture(st, &captured);
+        if (e == cudaSuccess) {
+            e = end;
+        }
+    }
+    if (e == cudaSuccess) {
+        e = cudaGraphInstantiate(&exec, graph, 0);
+    }
+    if (e == cudaSuccess) {
+        e = cudaGraphLaunch(exec, st);
+    }
+    if (e == cudaSuccess) {
+        e = launch_retire(w, src, grid, st);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(c->pinned_counters, w.counters, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            st);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(st);
+    }
+    if (exec != nullptr) {
+        cudaGraphExecDestroy(exec);
+    }
+    if (graph != nullptr) {
+        cudaGraphDestroy(graph);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "wavefront graph");
+    }
+    const unsigned long long* k = c->pinned_counters;
+    if (k[10] != 0ULL) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "the wavefront did not drain within its iteration bound");
+    }
+    if (report != nullptr) {
+        report->struct_size = sizeof(bf200_report_v1);
+        report->registered_light_count = s->light_count;
+        report->path_count += src.total;
+        report->extension_segments += k[3];
+        report->shadow_segments += k[4];
+        report->failed_lanes += k[5];
+        if (k[5] != 0 && report->first_failure_status == 0) {
+            report->first_failure_status = static_cast<uint32_t>(k[7]);
+            report->first_failure_path = static_cast<uint32_t>(k[6]);
+        }
+        report->kernel_launches += k[9] * per_iteration + 1U;
+        report->iterations += k[9];
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+// Runs the persistent wavefront until every path of `src` has been traced and retired. Without
+// instrumentation the loop runs on the device inside one graph; with it, the host drives every
+// iteration so each stage can be timed with events.
 blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSource src, const TransportParams& p,
                                 bool instrument, bf200_report_v1* report) {
+    if (!instrument) {
+        return run_wavefront_graph(c, s, src, p, report);
+    }
     Wavefront& w = c->w;
     cudaStream_t st = c->stream;
     cudaError_t e = cudaMemsetAsync(w.state, 0, w.capacity, st);

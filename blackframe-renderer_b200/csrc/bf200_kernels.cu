@@ -1880,8 +1880,37 @@ __global__ void __launch_bounds__(128) k_query_occlusion(SceneView s, const bf20
 }
 
 // ------------------------------------------------------------------------------------------------
+// k_iteration_gate: the end of one wavefront iteration inside a graph's device-side loop
+// ------------------------------------------------------------------------------------------------
+
+// One thread. Accumulates the iteration's shadow segments, counts the iteration, clears the
+// per-iteration counters for the next one, and keeps the loop running while paths remain to be
+// claimed or traced -- but never past `max_iterations`, when it raises counters[10] instead.
+__global__ void k_iteration_gate(Wavefront w, uint64_t total, uint64_t max_iterations,
+                                 cudaGraphConditionalHandle loop) {
+    unsigned long long* c = w.counters;
+    c[4] += c[0];
+    const unsigned long long iteration = ++c[9];
+    const bool drained = c[2] == 0ULL && c[1] >= total;
+    const bool bound = iteration >= max_iterations;
+    if (!drained && bound) {
+        c[10] = 1ULL;
+    }
+    c[0] = 0ULL;
+    c[2] = 0ULL;
+    cudaGraphSetConditional(loop, (!drained && !bound) ? 1U : 0U);
+}
+
+// ------------------------------------------------------------------------------------------------
 // Host-side launchers
 // ------------------------------------------------------------------------------------------------
+
+cudaError_t launch_gate(const Wavefront& w, uint64_t total, uint64_t max_iterations, cudaGraphConditionalHandle loop,
+                        cudaStream_t stream) {
+    k_iteration_gate<<<1, 1, 0, stream>>>(w, total, max_iterations, loop);
+    return cudaGetLastError();
+}
+
 
 cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instance, const uint32_t* tri_local,
                                  uint32_t total, float4* out, uint32_t* failures, cudaStream_t stream) {

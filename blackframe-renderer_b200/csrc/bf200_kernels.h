@@ -20,6 +20,12 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
 cudaError_t launch_compaction(const uint8_t* keys, uint32_t n, uint32_t routes, uint32_t* tile_counts,
                               uint32_t* queue, uint32_t* offsets, unsigned long long* total, uint8_t* reset_keys,
                               cudaStream_t stream, uint32_t* launches);
+// Queues k_iteration_gate, which ends one iteration of a graph's device-side wavefront loop: it
+// accumulates the shadow segments (counters[4]), counts iterations (counters[9]), clears the
+// per-iteration counters and sets `loop` to continue until the wavefront drains or
+// `max_iterations` is reached (then counters[10] = 1).
+cudaError_t launch_gate(const Wavefront& w, uint64_t total, uint64_t max_iterations, cudaGraphConditionalHandle loop,
+                        cudaStream_t stream);
 // Retires the slots the last iteration finished (k_regenerate; nothing is left to claim).
 cudaError_t launch_retire(const Wavefront& w, const PathSource& src, uint32_t grid, cudaStream_t stream);
 cudaError_t launch_film(const float4* path_radiance, uint32_t pixels, uint32_t samples, const float* response12,
