@@ -153,6 +153,15 @@ class FilmJob(C.Structure):
                 ("report", C.c_void_p)]
 
 
+class MaterialGradient(C.Structure):
+    _fields_ = [("weight", C.c_double * 4), ("roughness", C.c_double * 2), ("reserved", C.c_double * 2)]
+
+
+class Adjoint(C.Structure):
+    _fields_ = [("struct_size", u32), ("reserved", u32), ("target", C.c_void_p), ("gradients", C.c_void_p),
+                ("emission_gradient", C.c_void_p), ("loss", C.c_double)]
+
+
 class Report(C.Structure):
     _fields_ = [("struct_size", u32), ("registered_light_count", u32), ("path_count", u64),
                 ("extension_segments", u64), ("shadow_segments", u64),
@@ -172,7 +181,7 @@ class Hit(C.Structure):
 EXPECTED_SIZES = {
     Closure: 64, Material: 80, Geometry: 32, Instance: 160, Ray: 48, SampleIndex: 24,
     PathInput: 80, PathResult: 128, TransportOptions: 64, Camera: 88, Sensor: 80,
-    FilmRequest: 40, FilmJob: 64, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
+    FilmRequest: 40, FilmJob: 64, MaterialGradient: 64, Adjoint: 40, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
 }
 
 

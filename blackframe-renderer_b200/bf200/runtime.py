@@ -24,6 +24,7 @@ EXPORTED_SYMBOLS = [
     "bf200_closest_hits", "bf200_occlusions", "bf200_build_info", "bf200_camera_create",
     "bf200_trace_paths_device_noalloc", "bf200_sobol_bits", "bf200_owen_sobol_bits",
     "bf200_render_films_device",
+    "bf200_render_adjoint_device",
 ]
 
 
@@ -73,6 +74,10 @@ def library():
     lib.bf200_camera_create.restype = C.c_uint32
     lib.bf200_render_films_device.argtypes = [vp, C.POINTER(abi.FilmJob), C.c_uint32, C.c_uint32]
     lib.bf200_render_films_device.restype = C.c_uint32
+    lib.bf200_render_adjoint_device.argtypes = [vp, vp, C.POINTER(abi.Camera), C.POINTER(abi.Sensor),
+                                                C.POINTER(abi.FilmRequest), C.POINTER(abi.TransportOptions),
+                                                C.POINTER(abi.Film), C.POINTER(abi.Adjoint), C.POINTER(abi.Report)]
+    lib.bf200_render_adjoint_device.restype = C.c_uint32
     lib.bf200_sobol_bits.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
     lib.bf200_sobol_bits.restype = C.c_uint32
     lib.bf200_owen_sobol_bits.argtypes = [C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(C.c_uint64)]
@@ -205,6 +210,24 @@ class Context:
                                                        C.byref(request), C.byref(options), C.byref(film),
                                                        C.byref(report)), "render_film_device")
         return report
+
+    def render_adjoint_device(self, scene, camera, sensor, options, samples_per_pixel, seed, first_sample, precision,
+                              sums, counts, target, gradients, emission_gradient):
+        """bf200_render_adjoint_device: renders the device film (cleared first) and writes the loss
+        gradients (`gradients`: one 8-double record per material, `emission_gradient`: one double;
+        device pointers, as is `target`, H x W x 3 floats). Returns (loss, report)."""
+        request = abi.FilmRequest(C.sizeof(abi.FilmRequest), samples_per_pixel, first_sample, seed, precision)
+        film = abi.Film(camera.width, camera.height, precision, 0, C.c_void_p(sums),
+                        C.cast(C.c_void_p(counts), C.POINTER(abi.u64)))
+        adjoint = abi.Adjoint(C.sizeof(abi.Adjoint), 0, C.c_void_p(target), C.c_void_p(gradients),
+                              C.c_void_p(emission_gradient), 0.0)
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_render_adjoint_device(self.handle, scene.handle, C.byref(camera),
+                                                          C.byref(sensor), C.byref(request), C.byref(options),
+                                                          C.byref(film), C.byref(adjoint), C.byref(report)),
+                    "render_adjoint_device")
+        return adjoint.loss, report
 
     def render_film(self, scene, camera, sensor, options, samples_per_pixel, seed=0, first_sample=0,
                     precision=0, film=None):

@@ -125,6 +125,25 @@ struct PathSource {
 // 256 bounces of 10 dimensions each.
 constexpr uint32_t kDeviceSobolDimensions = 2U + 4U + 10U * 256U;
 
+// Path-replay adjoint of a film render: the replay launches of the wavefront (and only they) carry
+// this view. The gradient of an image loss is accumulated per material as kAdjointStride doubles:
+// d/d(closure weight lane 0..3), d/d(alpha_x), d/d(alpha_y) and two unused words; the derivative
+// with respect to a common factor on every emitter's radiance follows the last material record.
+constexpr uint32_t kAdjointMaterials = 64U;
+constexpr uint32_t kAdjointStride = 8U;
+constexpr uint32_t kAdjointEmission = kAdjointMaterials * kAdjointStride;
+constexpr uint32_t kAdjointWords = kAdjointEmission + 1U;
+struct AdjointView {
+    const float4* pixel_adjoint;  // per pixel: dLoss/d(pixel rgb) divided by the pixel's weight
+    const float4* forward;        // per path of the chunk: forward radiance (NaN x: failed path)
+    double* gradients;            // kAdjointWords
+    uint4* pending;               // per slot: roughness score of the last continuation (x, y float
+                                  // bits), its material, and the path tag (path id + 1)
+    uint4* shadow_score;          // per slot: roughness score of the queued shadow ray, material, flag
+    float lane_rgb[3][4];         // d(sample rgb c)/d(radiance lane l), the film's sensor map
+    uint32_t pixels;
+};
+
 // Per-slot wavefront state, structure of arrays in HBM.
 struct Wavefront {
     uint32_t capacity;

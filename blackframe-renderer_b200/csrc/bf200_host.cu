@@ -55,6 +55,9 @@ struct bf200_context {
     size_t lane_counter_lanes = 0;
     std::vector<void*> lane_radiance;
     std::vector<size_t> lane_radiance_bytes;
+    // path-replay adjoint: pixel adjoint, gradient sums, loss, per-slot scores
+    void* adjoint_workspace = nullptr;
+    size_t adjoint_workspace_bytes = 0;
 };
 
 struct bf200_scene {
@@ -62,6 +65,7 @@ struct bf200_scene {
     SceneView view{};
     std::vector<void*> allocations;
     uint32_t light_count = 0;
+    uint32_t material_count = 0;
     uint64_t triangle_count = 0;
     uint64_t node_count = 0;
 };
@@ -836,12 +840,47 @@ blackframe_status sobol_table(bf200_context* c, const bf200_transport_options_v1
     return BLACKFRAME_STATUS_SUCCESS;
 }
 
+// Camera paths of film samples [first, first + chunk) of a request, radiance per path into `radiance`.
+PathSource film_source(const bf200_camera_v1* cam, const bf200_film_request_v1* req, uint64_t first, uint64_t chunk,
+                       float4* radiance, const uint32_t* sobol) {
+    PathSource src{};
+    src.mode = 0;
+    src.total = chunk * cam->width * cam->height;
+    src.width = cam->width;
+    src.height = cam->height;
+    src.first_sample = req->first_sample + first;
+    src.seed = req->seed;
+    for (int a = 0; a < 3; ++a) {
+        src.cam_origin[a] = cam->origin[a];
+        src.cam_t[a] = cam->tangent[a];
+        src.cam_b[a] = cam->bitangent[a];
+        src.cam_n[a] = cam->normal[a];
+    }
+    src.half_width = cam->half_width;
+    src.half_height = cam->half_height;
+    src.t_min = cam->t_min;
+    src.t_max = cam->t_max;
+    src.time = cam->time;
+    src.mask = cam->mask;
+    src.jitter = cam->jitter_mode;
+    src.path_radiance = radiance;
+    src.sobol = sobol;
+    return src;
+}
+
+// Samples per film chunk: whole sample passes, at most ~64M paths of radiance per chunk.
+uint64_t film_samples_per_chunk(uint64_t pixels, uint64_t samples_per_pixel) {
+    const uint64_t max_chunk_paths = 1ULL << 26;
+    return std::min<uint64_t>(std::max<uint64_t>(1, max_chunk_paths / pixels), samples_per_pixel);
+}
+
 // The persistent wavefront as one CUDA graph: a conditional WHILE node whose body is one iteration
 // (the stage kernels and k_iteration_gate, which decides on the device whether another iteration
 // runs), so the whole trace is one graph launch with no host round trip per iteration. The gate
 // stops at the same iteration bound as the host loop.
 blackframe_status run_wavefront_graph(bf200_context* c, const bf200_scene* s, PathSource src,
-                                      const TransportParams& p, bf200_report_v1* report) {
+                                      const TransportParams& p, bf200_report_v1* report,
+                                      const AdjointView* adjoint = nullptr) {
     Wavefront& w = c->w;
     cudaStream_t st = c->stream;
     cudaError_t e = cudaMemsetAsync(w.state, 0, w.capacity, st);
@@ -879,7 +918,7 @@ blackframe_status run_wavefront_graph(bf200_context* c, const bf200_scene* s, Pa
         cudaGraph_t body = params.conditional.phGraph_out[0];
         e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
         for (int stage = 0; stage < 4 && e == cudaSuccess; ++stage) {
-            e = launch_stage(stage, s->view, w, src, p, grid, st, &per_iteration);
+            e = launch_stage(stage, s->view, w, src, p, grid, st, &per_iteration, adjoint);
         }
         if (e == cudaSuccess) {
             e = launch_gate(w, src.total, max_iterations, loop, st);
@@ -1205,7 +1244,7 @@ BF200_EXPORT blackframe_status bf200_context_destroy(bf200_context* c) noexcept 
     if (c->pinned_counters != nullptr) {
         cudaFreeHost(c->pinned_counters);
     }
-    for (void* p : {c->film_radiance, c->film_staging, c->batch_staging, c->lane_arena}) {
+    for (void* p : {c->film_radiance, c->film_staging, c->batch_staging, c->lane_arena, c->adjoint_workspace}) {
         if (p != nullptr) {
             cudaFree(p);
         }
@@ -1365,6 +1404,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         }
         select[lights.size()] = 1.0F;
         scene->light_count = static_cast<uint32_t>(lights.size());
+        scene->material_count = d->material_count;
         // materials
         std::vector<ClosureData> closures(d->material_count);
         std::vector<float4> emission(d->material_count);
@@ -1757,10 +1797,7 @@ BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const 
     if (pixels > 0xFFFFFFFFULL) {
         return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "film too large");
     }
-    // chunks of whole sample passes, at most ~64M paths of radiance per chunk
-    const uint64_t max_chunk_paths = 1ULL << 26;
-    uint64_t samples_per_chunk = std::max<uint64_t>(1, max_chunk_paths / pixels);
-    samples_per_chunk = std::min<uint64_t>(samples_per_chunk, req->samples_per_pixel);
+    const uint64_t samples_per_chunk = film_samples_per_chunk(pixels, req->samples_per_pixel);
     const size_t radiance_bytes = std::max<uint64_t>(1, samples_per_chunk * pixels) * sizeof(float4);
     if (const auto st = grow_workspace(c, &c->film_radiance, &c->film_radiance_bytes, radiance_bytes + 256,
                                        "film chunk workspace");
@@ -1782,28 +1819,7 @@ BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const 
     for (uint64_t first = 0; first < req->samples_per_pixel && st == BLACKFRAME_STATUS_SUCCESS;
          first += samples_per_chunk) {
         const uint64_t chunk = std::min<uint64_t>(samples_per_chunk, req->samples_per_pixel - first);
-        PathSource src{};
-        src.mode = 0;
-        src.total = chunk * pixels;
-        src.width = cam->width;
-        src.height = cam->height;
-        src.first_sample = req->first_sample + first;
-        src.seed = req->seed;
-        for (int a = 0; a < 3; ++a) {
-            src.cam_origin[a] = cam->origin[a];
-            src.cam_t[a] = cam->tangent[a];
-            src.cam_b[a] = cam->bitangent[a];
-            src.cam_n[a] = cam->normal[a];
-        }
-        src.half_width = cam->half_width;
-        src.half_height = cam->half_height;
-        src.t_min = cam->t_min;
-        src.t_max = cam->t_max;
-        src.time = cam->time;
-        src.mask = cam->mask;
-        src.jitter = cam->jitter_mode;
-        src.path_radiance = radiance;
-        src.sobol = sobol;
+        const PathSource src = film_source(cam, req, first, chunk, radiance, sobol);
         st = run_wavefront(c, s, src, params, o->instrumentation != 0, report);
         cudaEvent_t film_start = nullptr, film_stop = nullptr;
         if (st == BLACKFRAME_STATUS_SUCCESS && o->instrumentation != 0) {
@@ -1844,6 +1860,131 @@ BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const 
         }
     }
     return st;
+}
+
+// Path-replay adjoint of a film render: forward render, loss and pixel adjoint, then one replay per
+// film chunk. A chunk's forward radiance is still in the chunk buffer after the forward render
+// when the film is a single chunk; otherwise the replay of each chunk re-traces it forward first.
+BF200_EXPORT blackframe_status bf200_render_adjoint_device(bf200_context* c, const bf200_scene* s,
+                                                            const bf200_camera_v1* cam, const bf200_sensor_v1* sensor,
+                                                            const bf200_film_request_v1* req,
+                                                            const bf200_transport_options_v1* o, bf200_film_v1* film,
+                                                            bf200_adjoint_v1* adj, bf200_report_v1* report) noexcept {
+    if (c == nullptr || s == nullptr || cam == nullptr || sensor == nullptr || req == nullptr || film == nullptr ||
+        adj == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (adj->struct_size < sizeof(bf200_adjoint_v1) || adj->reserved != 0U || adj->target == nullptr ||
+        adj->gradients == nullptr || adj->emission_gradient == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "incomplete adjoint request");
+    }
+    if (s->context != c) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "scene belongs to another context");
+    }
+    if (s->material_count > kAdjointMaterials) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "the adjoint takes scenes of at most 64 materials");
+    }
+    if (film->sums == nullptr || film->sample_counts == nullptr || film->precision > 1U) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "inconsistent film request");
+    }
+    cudaSetDevice(c->device);
+    const uint64_t pixels = static_cast<uint64_t>(film->width) * film->height;
+    cudaError_t e = cudaMemsetAsync(film->sums, 0, pixels * (film->precision == 0U ? 16U : 64U), c->stream);
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(film->sample_counts, 0, pixels * 8U, c->stream);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "adjoint film reset");
+    }
+    blackframe_status st = bf200_render_film_device(c, s, cam, sensor, req, o, film, report);
+    if (st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    // workspace: pixel adjoint | gradient sums + loss | pending scores | shadow scores
+    const size_t pixel_bytes = ((pixels * sizeof(float4)) + 255) & ~size_t(255);
+    const size_t sum_bytes = ((kAdjointWords + 1) * sizeof(double) + 255) & ~size_t(255);
+    const size_t slot_bytes = c->capacity * sizeof(uint4);
+    if (const auto gst = grow_workspace(c, &c->adjoint_workspace, &c->adjoint_workspace_bytes,
+                                        pixel_bytes + sum_bytes + 2 * slot_bytes, "adjoint workspace");
+        gst != BLACKFRAME_STATUS_SUCCESS) {
+        return gst;
+    }
+    char* base = static_cast<char*>(c->adjoint_workspace);
+    AdjointView av{};
+    av.pixel_adjoint = reinterpret_cast<float4*>(base);
+    auto* pixel_adjoint = reinterpret_cast<float4*>(base);
+    av.gradients = reinterpret_cast<double*>(base + pixel_bytes);
+    double* loss = av.gradients + kAdjointWords;
+    av.pending = reinterpret_cast<uint4*>(base + pixel_bytes + sum_bytes);
+    av.shadow_score = reinterpret_cast<uint4*>(base + pixel_bytes + sum_bytes + slot_bytes);
+    av.pixels = static_cast<uint32_t>(pixels);
+    av.forward = static_cast<const float4*>(c->film_radiance);
+    // d(sample rgb)/d(radiance lane): the linear map of k_film (sensor term, then XYZ to linear sRGB)
+    static const double kXyzToRgb[3][3] = {{3.2404542, -1.5371385, -0.4985314},
+                                           {-0.9692660, 1.8760108, 0.0415560},
+                                           {0.0556434, -0.2040259, 1.0572252}};
+    for (int ch = 0; ch < 3; ++ch) {
+        for (int l = 0; l < 4; ++l) {
+            double v = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                v += kXyzToRgb[ch][k] * sensor->response_xyz[l][k];
+            }
+            av.lane_rgb[ch][l] = static_cast<float>(v * sensor->normalization / sensor->wavelength_pdf[l]);
+        }
+    }
+    e = cudaMemsetAsync(av.gradients, 0, (kAdjointWords + 1) * sizeof(double), c->stream);
+    if (e == cudaSuccess) {
+        e = launch_adjoint_image(film->precision == 0U ? static_cast<const float4*>(film->sums) : nullptr,
+                                 film->precision == 1U ? static_cast<const double*>(film->sums) : nullptr,
+                                 adj->target, static_cast<uint32_t>(pixels), film->precision, pixel_adjoint, loss,
+                                 c->stream);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "adjoint image");
+    }
+    const TransportParams params = make_params(*o);
+    const uint32_t* sobol = nullptr;
+    if (const auto sst = sobol_table(c, *o, &sobol); sst != BLACKFRAME_STATUS_SUCCESS) {
+        return sst;
+    }
+    const uint64_t samples_per_chunk = film_samples_per_chunk(pixels, req->samples_per_pixel);
+    const bool one_chunk = samples_per_chunk >= req->samples_per_pixel;
+    auto* radiance = static_cast<float4*>(c->film_radiance);
+    for (uint64_t first = 0; first < req->samples_per_pixel && st == BLACKFRAME_STATUS_SUCCESS;
+         first += samples_per_chunk) {
+        const uint64_t chunk = std::min<uint64_t>(samples_per_chunk, req->samples_per_pixel - first);
+        const PathSource src = film_source(cam, req, first, chunk, radiance, sobol);
+        if (!one_chunk) {
+            st = run_wavefront_graph(c, s, src, params, nullptr);
+        }
+        if (st == BLACKFRAME_STATUS_SUCCESS) {
+            // pending tags of an earlier replay must not match this chunk's paths
+            e = cudaMemsetAsync(av.pending, 0, slot_bytes, c->stream);
+            st = e == cudaSuccess ? run_wavefront_graph(c, s, src, params, nullptr, &av)
+                                  : cuda_fail(c, e, "adjoint scores reset");
+        }
+    }
+    if (st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    e = cudaMemcpyAsync(adj->gradients, av.gradients, s->material_count * sizeof(bf200_material_gradient_v1),
+                        cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(adj->emission_gradient, av.gradients + kAdjointEmission, sizeof(double),
+                            cudaMemcpyDeviceToDevice, c->stream);
+    }
+    double host_loss = 0.0;
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(&host_loss, loss, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(c->stream);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "adjoint results");
+    }
+    adj->loss = host_loss;
+    return BLACKFRAME_STATUS_SUCCESS;
 }
 
 BF200_EXPORT blackframe_status bf200_render_film(bf200_context* c, const bf200_scene* s, const bf200_camera_v1* cam,
@@ -2437,4 +2578,6 @@ static_assert(sizeof(bf200_closure_v1) == 64, "closure record layout");
 static_assert(sizeof(bf200_path_input_v1) == 80, "path input layout");
 static_assert(sizeof(bf200_path_result_v1) == 128, "path result layout");
 static_assert(sizeof(bf200_ray_v1) == 48, "ray layout");
+static_assert(sizeof(bf200_material_gradient_v1) == kAdjointStride * sizeof(double), "gradient record layout");
+static_assert(sizeof(bf200_adjoint_v1) == 40, "adjoint request layout");
 static_assert(sizeof(bf200_instance_v1) == 160, "instance layout");

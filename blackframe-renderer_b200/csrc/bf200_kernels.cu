@@ -1438,11 +1438,142 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Path-replay adjoint. A replay traces every path of the forward pass again (same sample indices,
+// so the same vertices) and knows, from the forward pass, the radiance L the path ends with. With
+// the sampled directions held fixed, every contribution a path adds after its vertex v is linear in
+// v's closure weight, so dL/dw(v) = (L - radiance accumulated through v's emission) / w(v): path
+// replay backpropagation (Vicini, Speierer and Jakob, SIGGRAPH 2021) without a reverse pass. The
+// roughness enters only through the BSDF value (the sampling density and MIS weights are held
+// fixed, "detached"), so a vertex contributes (what follows it) x d log f / d alpha; the score of the
+// continuation is applied at the next vertex, once that vertex knows what the shadow ray added. The
+// loss derivative per path lane is g = dLoss/d(pixel rgb) x the film's linear sensor map.
+// ------------------------------------------------------------------------------------------------
+
+struct AdjointLane {
+    bool on;         // false for a path the forward pass failed (it is not in the film)
+    float g[4];      // dLoss / d(path radiance lane l)
+    float4 forward;  // the path's forward radiance
+};
+
+__device__ __forceinline__ AdjointLane adjoint_lane(const AdjointView& a, uint64_t id) {
+    AdjointLane al;
+    al.forward = a.forward[id];
+    al.on = !isnan(al.forward.x);
+    const float4 gp = a.pixel_adjoint[id % a.pixels];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        al.g[l] = gp.x * a.lane_rgb[0][l] + gp.y * a.lane_rgb[1][l] + gp.z * a.lane_rgb[2][l];
+    }
+    return al;
+}
+
+// sum over lanes of g_l (L_l - acc_l): the loss derivative carried by what the path adds after acc
+__device__ __forceinline__ double adjoint_rest(const AdjointLane& al, float4 acc) {
+    return static_cast<double>(al.g[0]) * (static_cast<double>(al.forward.x) - acc.x) +
+           static_cast<double>(al.g[1]) * (static_cast<double>(al.forward.y) - acc.y) +
+           static_cast<double>(al.g[2]) * (static_cast<double>(al.forward.z) - acc.z) +
+           static_cast<double>(al.g[3]) * (static_cast<double>(al.forward.w) - acc.w);
+}
+
+__device__ __forceinline__ double adjoint_dot(const AdjointLane& al, const float (&c)[4]) {
+    return static_cast<double>(al.g[0]) * c[0] + static_cast<double>(al.g[1]) * c[1] +
+           static_cast<double>(al.g[2]) * c[2] + static_cast<double>(al.g[3]) * c[3];
+}
+
+struct D3 {
+    double x, y, z;
+};
+
+__device__ __forceinline__ D3 unit_d3(double x, double y, double z) {
+    const double n = sqrt(x * x + y * y + z * z);
+    return {x / n, y / n, z / n};
+}
+
+__device__ __forceinline__ double smith_root(double ax, double ay, D3 v) {
+    return sqrt(1.0 + (ax * ax * v.x * v.x + ay * ay * v.y * v.y) / (v.z * v.z));
+}
+
+// d log f / d(alpha_x, alpha_y) of a GGX lobe with microfacet normal m whose height-correlated
+// masking pairs the directions a and b (local frame, z > 0). f depends on the roughness only
+// through D(m) = 1 / (pi ax ay A^2), A = mx^2/ax^2 + my^2/ay^2 + mz^2, and G2 = 2 / (q(a) + q(b)),
+// q(v) = sqrt(1 + (ax^2 vx^2 + ay^2 vy^2) / vz^2) (the G2 of ggx_g2, written with q = 1 / nor).
+__device__ double2 ggx_log_roughness_gradient(double ax, double ay, D3 m, D3 a, D3 b) {
+    const double mx2 = m.x * m.x, my2 = m.y * m.y;
+    const double area = mx2 / (ax * ax) + my2 / (ay * ay) + m.z * m.z;
+    double dx = -1.0 / ax + 4.0 * mx2 / (ax * ax * ax * area);
+    double dy = -1.0 / ay + 4.0 * my2 / (ay * ay * ay * area);
+    const double qa = smith_root(ax, ay, a), qb = smith_root(ax, ay, b);
+    const double sum = qa + qb;
+    dx -= (ax * a.x * a.x / (a.z * a.z * qa) + ax * b.x * b.x / (b.z * b.z * qb)) / sum;
+    dy -= (ay * a.y * a.y / (a.z * a.z * qa) + ay * b.y * b.y / (b.z * b.z * qb)) / sum;
+    return make_double2(dx, dy);
+}
+
+// Roughness score of a closure for the local directions (wo, wi): false for closures without a
+// roughness (Lambert) and for direction pairs the closure gives no value.
+__device__ bool closure_roughness_score(const ClosureData& c, F3 wo, F3 wi, double2& out) {
+    if (c.kind == kClosureConductor) {
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return false;
+        }
+        const D3 m = unit_d3(static_cast<double>(wo.x) + wi.x, static_cast<double>(wo.y) + wi.y,
+                             static_cast<double>(wo.z) + wi.z);
+        out = ggx_log_roughness_gradient(c.p[8], c.p[9], m, D3{wo.x, wo.y, wo.z}, D3{wi.x, wi.y, wi.z});
+        return true;
+    }
+    if (c.kind != kClosureDielectric || wo.z == 0.0F || wi.z == 0.0F) {
+        return false;
+    }
+    // the face-oriented pair of dielectric_eval
+    const double sign = wo.z > 0.0F ? 1.0 : -1.0;
+    const D3 of{sign * wo.x, sign * wo.y, sign * wo.z};
+    const D3 in{sign * wi.x, sign * wi.y, sign * wi.z};
+    if (in.z > 0.0) {
+        const D3 m = unit_d3(of.x + in.x, of.y + in.y, of.z + in.z);
+        out = ggx_log_roughness_gradient(c.p[2], c.p[3], m, of, in);
+        return true;
+    }
+    const double incident = sign > 0.0 ? c.p[0] : c.p[1];
+    const double transmitted = sign > 0.0 ? c.p[1] : c.p[0];
+    D3 m = unit_d3(incident * of.x + transmitted * in.x, incident * of.y + transmitted * in.y,
+                   incident * of.z + transmitted * in.z);
+    if (m.z < 0.0) {
+        m = D3{-m.x, -m.y, -m.z};
+    }
+    if (!(m.z > 0.0)) {
+        return false;
+    }
+    out = ggx_log_roughness_gradient(c.p[2], c.p[3], m, of, D3{-in.x, -in.y, -in.z});
+    return true;
+}
+
+__device__ __forceinline__ void adjoint_zero(double* sum) {
+    for (uint32_t i = threadIdx.x; i < kAdjointWords; i += blockDim.x) {
+        sum[i] = 0.0;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void adjoint_flush(double* sum, double* gradients) {
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kAdjointWords; i += blockDim.x) {
+        if (sum[i] != 0.0) {
+            atomicAdd(&gradients[i], sum[i]);
+        }
+    }
+}
+
 // One launch per route: K is the closure kind the route's slots all share (0: generic route,
 // misses and any other material). The route queue lists the route's slots in slot order.
-template <int K>
+// ADJ: the replay of the path-replay adjoint (`a` is read only then).
+template <int K, bool ADJ>
 __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView s, Wavefront w, PathSource src, TransportParams p,
-                                               uint32_t route) {
+                                               uint32_t route, AdjointView a) {
+    __shared__ double adjoint_sum[ADJ ? kAdjointWords : 1];
+    if constexpr (ADJ) {
+        adjoint_zero(adjoint_sum);
+    }
     const uint32_t begin = w.route_offsets[route], end = w.route_offsets[route + 1U];
     const uint32_t stride = gridDim.x * blockDim.x;
     uint32_t active_here = 0;
@@ -1462,6 +1593,21 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
             const uint32_t mask = w.mask[slot];
             const Stream stream = load_stream(w, src, slot);
             const F3 ro = ld3(o4), rd = ld3(d4);
+            AdjointLane al{};
+            uint32_t path_tag = 0U;
+            if constexpr (ADJ) {
+                const uint64_t path = w.path_id[slot];
+                path_tag = static_cast<uint32_t>(path) + 1U;
+                al = adjoint_lane(a, path);
+                const uint4 pend = a.pending[slot];
+                if (al.on && pend.w == path_tag) {
+                    // the previous vertex's continuation: everything from here on
+                    const double rest = adjoint_rest(al, rad);
+                    atomicAdd(&adjoint_sum[pend.z * kAdjointStride + 4U], rest * __uint_as_float(pend.x));
+                    atomicAdd(&adjoint_sum[pend.z * kAdjointStride + 5U], rest * __uint_as_float(pend.y));
+                    a.pending[slot].w = 0U;
+                }
+            }
             if (K == 0 && id.x == 0xFFFFFFFFU) {
                 const float env[4] = {s.environment.x, s.environment.y, s.environment.z, s.environment.w};
                 add_product(rad, beta, env, lane);
@@ -1507,6 +1653,15 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                         }
                     }
                     add_weighted_emission(rad, beta, emitted, emission_weight, lane);
+                    if constexpr (ADJ) {
+                        if (al.on && lane.err == 0 && !is_black4(emitted)) {
+                            const float added[4] = {beta.x * emitted[0] * emission_weight,
+                                                    beta.y * emitted[1] * emission_weight,
+                                                    beta.z * emitted[2] * emission_weight,
+                                                    beta.w * emitted[3] * emission_weight};
+                            atomicAdd(&adjoint_sum[kAdjointEmission], adjoint_dot(al, added));
+                        }
+                    }
                     if (lane.err) {
                         done = true;
                     }
@@ -1549,6 +1704,20 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                     }
                 }
                 if (!done) {
+                    if constexpr (ADJ) {
+                        if (al.on) {  // everything after this vertex scales with its closure weight
+                            const float fv[4] = {al.forward.x, al.forward.y, al.forward.z, al.forward.w};
+                            const float rv[4] = {rad.x, rad.y, rad.z, rad.w};
+#pragma unroll
+                            for (int l = 0; l < 4; ++l) {
+                                if (closure.w[l] != 0.0F) {
+                                    atomicAdd(&adjoint_sum[material * kAdjointStride + l],
+                                              static_cast<double>(al.g[l]) *
+                                                  (static_cast<double>(fv[l]) - rv[l]) / closure.w[l]);
+                                }
+                            }
+                        }
+                    }
                     const F3 wo_world = robust_unit(-rd, lane);
                     const F3 wo = surf.frame.to_local(wo_world);
                     const uint64_t dims = bounce_base(depth_total(depth));
@@ -1565,6 +1734,16 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                     }
                     if (lane.err == 0) {
                         direct_lighting<K>(s, p, surf, closure, allowed, beta, wo_world, dims, stream, mask, rec, lane);
+                        if constexpr (ADJ) {
+                            if (al.on && rec.valid) {
+                                double2 score = make_double2(0.0, 0.0);
+                                const bool rough =
+                                    closure_roughness_score(closure, wo, surf.frame.to_local(rec.direction), score);
+                                a.shadow_score[slot] =
+                                    make_uint4(__float_as_uint(static_cast<float>(score.x)),
+                                               __float_as_uint(static_cast<float>(score.y)), material, rough ? 1U : 0U);
+                            }
+                        }
                     }
                     if (lane.err != 0) {
                         rec.valid = false;
@@ -1680,6 +1859,14 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                                         w.beta[slot] = make_float4(cb[0], cb[1], cb[2], cb[3]);
                                     }
                                 }
+                                if constexpr (ADJ) {
+                                    double2 score;
+                                    if (al.on && !done && closure_roughness_score(closure, wo, bs.wi, score)) {
+                                        a.pending[slot] = make_uint4(__float_as_uint(static_cast<float>(score.x)),
+                                                                     __float_as_uint(static_cast<float>(score.y)),
+                                                                     material, path_tag);
+                                    }
+                                }
                             } else {
                                 done = true;
                             }
@@ -1713,14 +1900,22 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
     if ((threadIdx.x & 31U) == 0U && active_here != 0U) {
         atomicAdd(&w.counters[2], static_cast<unsigned long long>(active_here));
     }
+    if constexpr (ADJ) {
+        adjoint_flush(adjoint_sum, a.gradients);
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
 // k_occlude: shadow rays of the compacted queue; unoccluded contributions join the path radiance
 // ------------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256, BF200_OCCLUDE_MIN_BLOCKS) k_occlude(SceneView s, Wavefront w) {
+template <bool ADJ>
+__global__ void __launch_bounds__(256, BF200_OCCLUDE_MIN_BLOCKS) k_occlude(SceneView s, Wavefront w, AdjointView a) {
     __shared__ int stack_columns[kSharedStackEntries * 256];
+    __shared__ double adjoint_sum[ADJ ? kAdjointWords : 1];
+    if constexpr (ADJ) {
+        adjoint_zero(adjoint_sum);
+    }
     TraversalStack stack = thread_stack(stack_columns);
     const uint32_t count = w.shadow_offsets[1];
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -1741,7 +1936,23 @@ __global__ void __launch_bounds__(256, BF200_OCCLUDE_MIN_BLOCKS) k_occlude(Scene
             r.z = r.z + c.z;
             r.w = r.w + c.w;
             w.radiance[slot] = r;
+            if constexpr (ADJ) {
+                const AdjointLane al = adjoint_lane(a, w.path_id[slot]);
+                if (al.on) {  // the light's radiance scales this contribution; so may the roughness
+                    const float added[4] = {c.x, c.y, c.z, c.w};
+                    const double e = adjoint_dot(al, added);
+                    atomicAdd(&adjoint_sum[kAdjointEmission], e);
+                    const uint4 score = a.shadow_score[slot];
+                    if (score.w != 0U) {
+                        atomicAdd(&adjoint_sum[score.z * kAdjointStride + 4U], e * __uint_as_float(score.x));
+                        atomicAdd(&adjoint_sum[score.z * kAdjointStride + 5U], e * __uint_as_float(score.y));
+                    }
+                }
+            }
         }
+    }
+    if constexpr (ADJ) {
+        adjoint_flush(adjoint_sum, a.gradients);
     }
 }
 
@@ -1830,6 +2041,49 @@ __global__ void k_film(const float4* path_radiance, uint32_t pixels, uint32_t sa
         }
     }
     counts[p] = count;
+}
+
+// Loss of a film against a target image and its adjoint per pixel. The image is the film's
+// weighted mean, rgb / weight (the Neumaier sum plus its compensation for a float64 film). The loss
+// is sum over pixels and channels of (image - target)^2; pixel_adjoint receives
+// dLoss/d(image) / weight = 2 (image - target) / weight, the derivative per unit-weight sample.
+__global__ void __launch_bounds__(256) k_adjoint_image(const float4* film32, const double* film64, const float* target,
+                                                       uint32_t pixels, uint32_t precision, float4* pixel_adjoint,
+                                                       double* loss) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    double part = 0.0;
+    if (p < pixels) {
+        double rgb[3], weight;
+        if (precision == 0U) {
+            const float4 f = film32[p];
+            rgb[0] = f.x;
+            rgb[1] = f.y;
+            rgb[2] = f.z;
+            weight = f.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                rgb[k] = film64[8ULL * p + k] + film64[8ULL * p + 4 + k];
+            }
+            weight = film64[8ULL * p + 3] + film64[8ULL * p + 7];
+        }
+        float adj[3] = {0.0F, 0.0F, 0.0F};
+        if (weight > 0.0) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double d = rgb[k] / weight - static_cast<double>(target[3ULL * p + k]);
+                part += d * d;
+                adj[k] = static_cast<float>(2.0 * d / weight);
+            }
+        }
+        pixel_adjoint[p] = make_float4(adj[0], adj[1], adj[2], 0.0F);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        part += __shfl_down_sync(0xFFFFFFFFU, part, off);
+    }
+    if ((threadIdx.x & 31U) == 0U && part != 0.0) {
+        atomicAdd(loss, part);
+    }
 }
 
 // Standalone closest-hit / occlusion queries (ClosestHit.hpp:21-28, Occlusion.hpp:19-26).
@@ -1923,8 +2177,18 @@ cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instanc
     return cudaGetLastError();
 }
 
+template <bool ADJ>
+void launch_shading(const SceneView& s, const Wavefront& w, const PathSource& src, const TransportParams& p,
+                    uint32_t grid, const AdjointView& a, cudaStream_t stream) {
+    k_shade<0, ADJ><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteGeneric, a);
+    k_shade<static_cast<int>(kClosureLambert), ADJ><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteLambert, a);
+    k_shade<static_cast<int>(kClosureConductor), ADJ><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteConductor, a);
+    k_shade<static_cast<int>(kClosureDielectric), ADJ><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteDielectric, a);
+}
+
 cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
-                         const TransportParams& p, uint32_t grid, cudaStream_t stream, uint32_t* launches) {
+                         const TransportParams& p, uint32_t grid, cudaStream_t stream, uint32_t* launches,
+                         const AdjointView* adjoint) {
     cudaError_t e = cudaSuccess;
     if (stage == 0) {
         k_regenerate<<<grid, 256, 0, stream>>>(w, src);
@@ -1943,10 +2207,11 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
         if (e != cudaSuccess) {
             return e;
         }
-        k_shade<0><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteGeneric);
-        k_shade<static_cast<int>(kClosureLambert)><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteLambert);
-        k_shade<static_cast<int>(kClosureConductor)><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteConductor);
-        k_shade<static_cast<int>(kClosureDielectric)><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteDielectric);
+        if (adjoint != nullptr) {
+            launch_shading<true>(s, w, src, p, grid, *adjoint, stream);
+        } else {
+            launch_shading<false>(s, w, src, p, grid, AdjointView{}, stream);
+        }
         *launches += 4U;
         if ((e = cudaGetLastError()) != cudaSuccess) {
             return e;
@@ -1954,7 +2219,11 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
         return launch_compaction(w.shadow_key, w.capacity, 1U, w.tile_counts, w.shadow_queue, w.shadow_offsets,
                                  w.counters + 0, nullptr, stream, launches);
     }
-    k_occlude<<<grid, 256, 0, stream>>>(s, w);
+    if (adjoint != nullptr) {
+        k_occlude<true><<<grid, 256, 0, stream>>>(s, w, *adjoint);
+    } else {
+        k_occlude<false><<<grid, 256, 0, stream>>>(s, w, AdjointView{});
+    }
     *launches += 1U;
     return cudaGetLastError();
 }
@@ -1977,6 +2246,13 @@ cudaError_t launch_film(const float4* path_radiance, uint32_t pixels, uint32_t s
     sv.normalization = normalization;
     k_film<<<(pixels + 127U) / 128U, 128, 0, stream>>>(path_radiance, pixels, samples, sv, precision, film32, film64,
                                                       counts, skipped);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_image(const float4* film32, const double* film64, const float* target, uint32_t pixels,
+                                 uint32_t precision, float4* pixel_adjoint, double* loss, cudaStream_t stream) {
+    k_adjoint_image<<<(pixels + 255U) / 256U, 256, 0, stream>>>(film32, film64, target, pixels, precision,
+                                                                pixel_adjoint, loss);
     return cudaGetLastError();
 }
 

@@ -10,9 +10,11 @@ namespace bf200 {
 cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instance, const uint32_t* tri_local,
                                  uint32_t total, float4* out, uint32_t* failures, cudaStream_t stream);
 // stage 0: k_regenerate; 1: k_trace; 2: route compaction, the per-route k_shade kernels, shadow
-// compaction; 3: k_occlude. Adds the number of kernels launched to *launches.
+// compaction; 3: k_occlude. Adds the number of kernels launched to *launches. With `adjoint`, the
+// shading and occlusion stages run as the path-replay adjoint's replay.
 cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
-                         const TransportParams& p, uint32_t grid, cudaStream_t stream, uint32_t* launches);
+                         const TransportParams& p, uint32_t grid, cudaStream_t stream, uint32_t* launches,
+                         const AdjointView* adjoint = nullptr);
 // Stable compaction of n one-byte keys: the indices whose key is r < routes go to
 // queue[offsets[r] .. offsets[r + 1]) in increasing order. tile_counts holds routes x
 // ceil(n / kCompactTile) words of scratch. When total is given it receives the queue length; when
@@ -31,6 +33,10 @@ cudaError_t launch_retire(const Wavefront& w, const PathSource& src, uint32_t gr
 cudaError_t launch_film(const float4* path_radiance, uint32_t pixels, uint32_t samples, const float* response12,
                         const float* pdf4, float normalization, uint32_t precision, float4* film32, double* film64,
                         unsigned long long* counts, unsigned long long* skipped, cudaStream_t stream);
+// Loss of a film against a target image (sum of squared rgb differences, added to *loss) and the
+// per-pixel adjoint of the path-replay adjoint.
+cudaError_t launch_adjoint_image(const float4* film32, const double* film64, const float* target, uint32_t pixels,
+                                 uint32_t precision, float4* pixel_adjoint, double* loss, cudaStream_t stream);
 cudaError_t launch_queries(const SceneView& s, const bf200_ray_v1* rays, uint64_t n, bf200_hit_v1* hits,
                            uint32_t* occluded, cudaStream_t stream);
 

@@ -528,6 +528,48 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_films_device(bf200_co
                                                                         uint32_t job_count, uint32_t lanes)
     BF200_NOEXCEPT;
 
+/* Path-replay adjoint (the reference has no differentiation; its benchmark plan asks a new backend
+ * for an adjoint of the film render). One call renders the film, compares the image with a target
+ * and returns the gradient of the loss
+ *     loss = sum over pixels and rgb channels of (image - target)^2,  image = film rgb / film weight,
+ * with respect to every material's closure weight (per packet lane), the GGX roughness alpha_x and
+ * alpha_y of conductor and dielectric closures, and a common factor k on every emitter's radiance
+ * (at k = 1; the constant environment is not scaled).
+ *
+ * Method: the paths are traced once forward into the film, then replayed with the same sample
+ * indices. The replay knows each path's final radiance, so a vertex's share of the gradient is what
+ * the path adds after it (path replay backpropagation, without a reverse pass). With the sampled
+ * directions held fixed, every contribution is linear in the closure weights and the emission, so
+ * those gradients are the exact derivatives of this render's loss (finite differences on the same
+ * samples agree). Sampling densities, MIS weights and Russian-roulette decisions are held fixed:
+ * the roughness gradient is the "detached" estimator, unbiased for the derivative of the expected
+ * loss but not equal per sample to a finite difference, and Russian roulette should be off when
+ * the weight gradients are compared with finite differences.
+ *
+ * The film (device, as in bf200_render_film_device) is cleared and holds this call's render on
+ * return. Gradients are summed in float64 by atomics in no fixed order, so their last bits vary
+ * between calls. At most 64 materials. The report counts the forward render. */
+typedef struct bf200_material_gradient_v1 {
+    double weight[4];     /* dLoss / d(closure weight of packet lane l) */
+    double roughness[2];  /* dLoss / d(alpha_x), dLoss / d(alpha_y); 0 for Lambert */
+    double reserved[2];
+} bf200_material_gradient_v1;
+
+typedef struct bf200_adjoint_v1 {
+    uint32_t struct_size;
+    uint32_t reserved;
+    const float* target;                   /* device: height x width x 3 floats, rgb, row-major */
+    bf200_material_gradient_v1* gradients; /* device: one record per scene material */
+    double* emission_gradient;             /* device: one double, dLoss/dk */
+    double loss;                           /* out */
+} bf200_adjoint_v1;
+
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_adjoint_device(
+    bf200_context* context, const bf200_scene* scene, const bf200_camera_v1* camera,
+    const bf200_sensor_v1* sensor, const bf200_film_request_v1* request,
+    const bf200_transport_options_v1* options, bf200_film_v1* film, bf200_adjoint_v1* adjoint,
+    bf200_report_v1* report) BF200_NOEXCEPT;
+
 /* Closest-hit query for a batch of world rays (trace_cuda_closest_hits, ClosestHit.hpp:21-28).
  * Per ray writes t, barycentrics b0..b2, instance index and primitive index (0xffffffff on a
  * miss). Host pointers. */

@@ -1,0 +1,227 @@
+"""Path-replay adjoint of the film render (bf200_render_adjoint_device).
+
+With the sampled directions held fixed and Russian roulette off, every contribution of a path is
+linear in each closure weight and in the emitted radiance, so those gradients are the exact
+derivatives of the rendered loss. They are compared with central finite differences of the same
+render (same sample indices), with a relative step of 1e-3 on the float32 parameter:
+tolerance 2e-3 of the finite difference, plus 1e-4 of the largest gradient tested. They are also
+compared with finite differences of the oracle's films (the CPU restatement of the reference
+transport). There the tolerance is 3 %, because up to 1 % of paths may take a different route on
+the device (the sine/cosine rounding note of the parity tests).
+
+The roughness gradient is the detached estimator: sampling densities and MIS weights are held
+fixed. It is unbiased for the derivative of the expected loss but differs from a finite difference
+sample by sample. It is compared with finite differences over several seeds: the mean difference
+must lie within four standard errors, plus 3 % of the finite difference.
+"""
+import copy
+import os
+
+import numpy as np
+import pytest
+
+from bf200 import abi, runtime, scenes
+from helpers import arrays, sensor_from_golden
+from oracle.bindings import Oracle
+
+pytestmark = pytest.mark.gpu
+
+WIDTH, HEIGHT, SPP, DEPTH, SEED = 24, 20, 4, 6, 11
+WHITE, RED, GREEN, LIGHT, CONDUCTOR, DIELECTRIC = range(6)
+
+
+def transport_options():
+    return abi.default_options(mis="power", max_depth=DEPTH, roulette=False)
+
+
+def changed(builder, material, lane=None, weight=None, alpha=None, emission=None):
+    """Copy of a scene builder with one material's closure weight lane, GGX roughness (both axes)
+    or emission (all lanes) replaced by a float32 value."""
+    b = copy.copy(builder)
+    b.materials = list(builder.materials)
+    closures, emitted, frame = b.materials[material]
+    kind, lobes, w, params = closures[0]
+    w, params, emitted = list(w), list(params), list(emitted)
+    if weight is not None:
+        w[lane] = np.float32(weight)
+    if alpha is not None:
+        axes = (8, 9) if kind == abi.CLOSURE_ROUGH_CONDUCTOR else (2, 3)
+        for a in axes:
+            params[a] = np.float32(alpha)
+    if emission is not None:
+        emitted = [np.float32(emission)] * 4
+    b.materials[material] = ([(kind, lobes, w, params)] + closures[1:], emitted, frame)
+    return b
+
+
+def film_loss(sums, target):
+    image = (sums[..., :3] + sums[..., 4:7]) / (sums[..., 3:4] + sums[..., 7:8])
+    return float(((image - target) ** 2).sum())
+
+
+@pytest.fixture(scope="module")
+def setup():
+    import torch
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "cornell_spheres_256.npz"))
+    sensor = sensor_from_golden(g)
+    builder = scenes.cornell_box(scenes.SceneBuilder(), with_spheres=True)
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), WIDTH, HEIGHT, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+    target = np.random.default_rng(7).uniform(0.0, 0.3, (HEIGHT, WIDTH, 3)).astype(np.float32)
+    with runtime.Context(0, path_capacity=1 << 16) as ctx:
+        yield torch, ctx, builder, cam, sensor, target
+
+
+def gpu_loss(setup, builder, spp=SPP, seed=SEED):
+    torch, ctx, _, cam, sensor, target = setup
+    scene = ctx.create_scene(builder)
+    sums = torch.zeros((HEIGHT, WIDTH, 8), dtype=torch.float64, device="cuda")
+    counts = torch.zeros((HEIGHT, WIDTH), dtype=torch.int64, device="cuda")
+    ctx.render_film_device(scene, cam, sensor, transport_options(), spp, seed, 0, 1, sums.data_ptr(),
+                           counts.data_ptr())
+    scene.close()
+    return film_loss(sums.cpu().numpy(), target)
+
+
+def gpu_adjoint(setup, builder, spp=SPP, seed=SEED):
+    torch, ctx, _, cam, sensor, target = setup
+    scene = ctx.create_scene(builder)
+    sums = torch.full((HEIGHT, WIDTH, 8), 3.0, dtype=torch.float64, device="cuda")  # cleared by the call
+    counts = torch.zeros((HEIGHT, WIDTH), dtype=torch.int64, device="cuda")
+    grads = torch.zeros((len(builder.materials), 8), dtype=torch.float64, device="cuda")
+    emission = torch.zeros(1, dtype=torch.float64, device="cuda")
+    tgt = torch.tensor(target, device="cuda")
+    loss, report = ctx.render_adjoint_device(scene, cam, sensor, transport_options(), spp, seed, 0, 1,
+                                             sums.data_ptr(), counts.data_ptr(), tgt.data_ptr(), grads.data_ptr(),
+                                             emission.data_ptr())
+    scene.close()
+    # a failed path (a reference-inherent numerical failure, about 1 in 10^5 here) is left out of
+    # the film and of the gradients
+    paths = WIDTH * HEIGHT * spp
+    assert report.path_count == paths and report.failed_lanes <= max(1, paths // 10000)
+    assert int(counts.sum()) == paths - report.failed_lanes
+    return loss, grads.cpu().numpy(), float(emission.cpu()[0]), sums.cpu().numpy()
+
+
+def steps(value, h):
+    lo, hi = np.float32(value * (1.0 - h)), np.float32(value * (1.0 + h))
+    return lo, hi, float(hi) - float(lo)
+
+
+# (material, lane). Lane 3 of the packet (759.5 nm) barely reaches the CIE sensor: a 1e-3 change
+# of its weight moves the film by about as much as float32 rounding does, so it is not tested.
+WEIGHTS = [(WHITE, 0), (WHITE, 2), (RED, 1), (GREEN, 2), (CONDUCTOR, 0), (DIELECTRIC, 1)]
+
+
+def test_weight_and_emission_gradients_match_finite_differences(setup):
+    _, _, builder, _, _, target = setup
+    loss, grads, emission, sums = gpu_adjoint(setup, builder)
+    assert abs(loss - film_loss(sums, target)) <= 1e-9 * loss
+    # the image is linear in the emitted radiance (no environment): dLoss/dk = sum 2 (I - T) I
+    image = (sums[..., :3] + sums[..., 4:7]) / (sums[..., 3:4] + sums[..., 7:8])
+    assert abs(emission - float((2.0 * (image - target) * image).sum())) <= 1e-4 * abs(emission)
+    scale = max(abs(grads[m, l]) for m, l in WEIGHTS)
+    checks = []
+    for m, l in WEIGHTS:
+        w = float(builder.materials[m][0][0][2][l])
+        lo, hi, dw = steps(w, 1e-3)
+        fd = (gpu_loss(setup, changed(builder, m, l, weight=hi)) -
+              gpu_loss(setup, changed(builder, m, l, weight=lo))) / dw
+        print(f"weight ({m}, {l}): adjoint {grads[m, l]:.6g}, finite difference {fd:.6g}")
+        checks.append((m, l, grads[m, l], fd))
+    for m, l, g, fd in checks:
+        assert abs(g - fd) <= 2e-3 * abs(fd) + 1e-4 * scale, (m, l, g, fd)
+    e = float(builder.materials[LIGHT][1][0])
+    lo, hi, de = steps(e, 1e-3)
+    fd = (gpu_loss(setup, changed(builder, LIGHT, emission=hi)) -
+          gpu_loss(setup, changed(builder, LIGHT, emission=lo))) / (de / e)
+    assert abs(emission - fd) <= 2e-3 * abs(fd), (emission, fd)
+
+
+def oracle_loss(oracle, builder, cam, sensor, target):
+    px, py, s = np.meshgrid(np.arange(WIDTH), np.arange(HEIGHT), np.arange(SPP), indexing="ij")
+    order = np.lexsort((px.ravel(), py.ravel(), s.ravel()))
+    px, py, s = px.ravel()[order], py.ravel()[order], s.ravel()[order]
+    samples = (abi.SampleIndex * len(px))()
+    for k in range(len(px)):
+        samples[k].pixel_x, samples[k].pixel_y = int(px[k]), int(py[k])
+        samples[k].sample_index, samples[k].seed = int(s[k]), SEED
+    rays = oracle.camera_rays(cam, samples)
+    inputs = (abi.PathInput * len(px))()
+    for k in range(len(px)):
+        inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
+    handle = oracle.scene(builder)
+    results, failures = oracle.trace(handle, inputs, transport_options())
+    oracle.destroy(handle)
+    assert failures == 0
+    film, _ = oracle.film(arrays(results)["radiance"], samples, sensor, WIDTH, HEIGHT, 1)  # compensated sums
+    image = film[..., :3] / film[..., 3:4]
+    return float(((image - target) ** 2).sum())
+
+
+def test_gradients_match_oracle_finite_differences(setup):
+    _, _, builder, cam, sensor, target = setup
+    oracle = Oracle()
+    _, grads, emission, _ = gpu_adjoint(setup, builder)
+    for m, l in [(WHITE, 1), (RED, 0)]:
+        w = float(builder.materials[m][0][0][2][l])
+        lo, hi, dw = steps(w, 1e-3)
+        fd = (oracle_loss(oracle, changed(builder, m, l, weight=hi), cam, sensor, target) -
+              oracle_loss(oracle, changed(builder, m, l, weight=lo), cam, sensor, target)) / dw
+        assert abs(grads[m, l] - fd) <= 0.03 * abs(fd), (m, l, grads[m, l], fd)
+    e = float(builder.materials[LIGHT][1][0])
+    lo, hi, de = steps(e, 1e-3)
+    fd = (oracle_loss(oracle, changed(builder, LIGHT, emission=hi), cam, sensor, target) -
+          oracle_loss(oracle, changed(builder, LIGHT, emission=lo), cam, sensor, target)) / (de / e)
+    assert abs(emission - fd) <= 0.03 * abs(fd), (emission, fd)
+
+
+def test_roughness_gradient_agrees_with_finite_differences_on_average(setup):
+    """Conductor at alpha 0.2 and, with alpha raised from 0.05 to 0.3, the dielectric (at 0.05 a
+    finite difference is dominated by reflect/transmit choices that flip under the step). Relative
+    step 5e-2: the finite difference's flip noise shrinks with the step, its bias grows as its
+    square (about 3e-3 here)."""
+    _, _, builder, _, _, _ = setup
+    spp, seeds = 128, range(100, 116)
+    rough_glass = changed(builder, DIELECTRIC, alpha=0.3)
+    for m, base, axis, required in [(CONDUCTOR, builder, 8, True), (DIELECTRIC, rough_glass, 2, False)]:
+        alpha = float(base.materials[m][0][0][3][axis])
+        lo, hi, da = steps(alpha, 5e-2)
+        up, down = changed(base, m, alpha=hi), changed(base, m, alpha=lo)
+        diffs, fds = [], []
+        for seed in seeds:
+            _, grads, _, _ = gpu_adjoint(setup, base, spp, seed)
+            fd = (gpu_loss(setup, up, spp, seed) - gpu_loss(setup, down, spp, seed)) / da
+            diffs.append(grads[m, 4] + grads[m, 5] - fd)
+            fds.append(fd)
+        mean_fd = float(np.mean(fds))
+        stderr = float(np.std(diffs, ddof=1) / np.sqrt(len(diffs)))
+        fd_stderr = float(np.std(fds, ddof=1) / np.sqrt(len(fds)))
+        print(f"material {m}: adjoint - fd = {np.mean(diffs):.4g} +- {stderr:.3g}, fd {mean_fd:.4g} +- {fd_stderr:.3g}")
+        assert abs(np.mean(diffs)) <= 4.0 * stderr + 0.03 * abs(mean_fd)
+        if required:  # the comparison has a gradient well above its noise
+            assert abs(mean_fd) > 8.0 * stderr
+
+
+def test_film_is_the_calls_render(setup):
+    _, _, builder, _, _, _ = setup
+    first = gpu_adjoint(setup, builder)
+    second = gpu_adjoint(setup, builder)
+    assert np.array_equal(first[3], second[3]) and first[0] == second[0]
+    assert np.allclose(first[1], second[1], rtol=1e-9, atol=0.0)
+
+
+def test_too_many_materials_is_rejected(setup):
+    torch, ctx, builder, cam, sensor, target = setup
+    b = copy.copy(builder)
+    b.materials = list(builder.materials) + [builder.materials[WHITE]] * 60
+    scene = ctx.create_scene(b)
+    sums = torch.zeros((HEIGHT, WIDTH, 8), dtype=torch.float64, device="cuda")
+    counts = torch.zeros((HEIGHT, WIDTH), dtype=torch.int64, device="cuda")
+    grads = torch.zeros((len(b.materials), 8), dtype=torch.float64, device="cuda")
+    tgt = torch.tensor(target, device="cuda")
+    with pytest.raises(runtime.Bf200Error) as info:
+        ctx.render_adjoint_device(scene, cam, sensor, transport_options(), 1, 0, 0, 1, sums.data_ptr(),
+                                  counts.data_ptr(), tgt.data_ptr(), grads.data_ptr(), grads.data_ptr())
+    scene.close()
+    assert info.value.status == 5  # OUT_OF_RANGE
