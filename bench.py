@@ -233,6 +233,123 @@ def run_batch(args, torch, rank):
     print(json.dumps(line), flush=True)
 
 
+ADJOINT_WORKLOAD = "adjoint_icosphere_256"
+
+
+def run_adjoint(args, torch, rank):
+    """The path-replay adjoint: one step = one bf200_render_adjoint_device call (forward render of
+    256 x 256 x 64 spp, L2 loss against a target rendered at perturbed parameters, replay of every
+    path). Timed with CUDA events around the call; the forward render alone is timed beside it."""
+    if rank != 0:
+        return
+    builder, options, camera, sensor, (width, height, spp) = workload_setup(ADJOINT_WORKLOAD)
+    if args.spp > 0:
+        spp = args.spp
+    target_params = scenes.perturbed_parameters(scenes.adjoint_parameters())
+    target_builder = scenes.adjoint_icosphere(scenes.SceneBuilder(), target_params)
+    ctx = runtime.Context(0, path_capacity=args.capacity)
+    scene, target_scene = ctx.create_scene(builder), ctx.create_scene(target_builder)
+    sums = torch.zeros((height, width, 8), dtype=torch.float64, device="cuda")
+    counts = torch.zeros((height, width), dtype=torch.int64, device="cuda")
+    ctx.render_film_device(target_scene, camera, sensor, options, spp, 7, 0, 1, sums.data_ptr(), counts.data_ptr())
+    torch.cuda.synchronize()
+    target = ((sums[..., :3] + sums[..., 4:7]) / (sums[..., 3:4] + sums[..., 7:8])).float().contiguous()
+    target_scene.close()
+    materials = len(builder.materials)
+    grads = torch.zeros((materials, 8), dtype=torch.float64, device="cuda")
+    emission = torch.zeros(1, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    paths = width * height * spp
+
+    def adjoint():
+        return ctx.render_adjoint_device(scene, camera, sensor, options, spp, 0, 0, 1, sums.data_ptr(),
+                                         counts.data_ptr(), target.data_ptr(), grads.data_ptr(), emission.data_ptr())
+
+    def forward():
+        sums.zero_()
+        counts.zero_()
+        return ctx.render_film_device(scene, camera, sensor, options, spp, 0, 0, 1, sums.data_ptr(),
+                                      counts.data_ptr())
+
+    def timed(fn, step):
+        flush.fill_(step & 0xFF)
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        out = fn()
+        stop.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop), out
+
+    for step in range(args.warmup):
+        timed(adjoint, step)
+        timed(forward, step)
+    adjoint_ms, forward_ms, results = [], [], []
+    with ClockSampler(0) as clocks:
+        for step in range(args.steps):
+            ms, out = timed(adjoint, step)
+            adjoint_ms.append(ms)
+            results.append(out)
+            ms, _ = timed(forward, step)
+            forward_ms.append(ms)
+    total = sum(adjoint_ms)
+    value = paths * args.steps / (total / 1000.0)
+    forward_value = paths * args.steps / (sum(forward_ms) / 1000.0)
+    loss, report = results[-1]
+
+    # e2e: target uploaded from pinned host memory and gradients read back every step
+    host_target = target.cpu().pin_memory()
+    host_grads = torch.empty((materials, 8), dtype=torch.float64).pin_memory()
+    host_emission = torch.empty(1, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for step in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        target.copy_(host_target, non_blocking=True)
+        adjoint()
+        host_grads.copy_(grads, non_blocking=True)
+        host_emission.copy_(emission, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+    e2e_value = paths * len(e2e_ms) / (sum(e2e_ms) / 1000.0)
+    g = host_grads.numpy()
+    basis = scenes.basis_gradients(g, builder.nanometers)
+    ext, shadow = report.extension_segments, report.shadow_segments
+    # both passes move the path's algorithmic bytes (camera ray, segments, film once)
+    alg = 2 * (CAMERA_RAY_BYTES * paths + EXTENSION_SEGMENT_BYTES * ext + SHADOW_SEGMENT_BYTES * shadow) + \
+        FILM_SAMPLE_BYTES * paths
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (total / args.steps / 1000.0) / 1e9
+    line = {
+        "metric": "adjoint path samples/s", "value": value, "unit": "path samples/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": ADJOINT_WORKLOAD, "width": width, "height": height, "spp": spp, "max_depth": 8,
+                   "mis": "power", "russian_roulette": False, "triangles": builder.triangle_count,
+                   "parameters": "albedo 4 materials x 8 basis coefficients, 2 GGX alphas, light scale",
+                   "target": "render at parameters + N(0, 0.1), seed 7", "path_capacity": args.capacity,
+                   "l2": "flushed between steps (256 MiB write); path state > L2"},
+        "forward_only": {"value": forward_value, "ms_per_step": sum(forward_ms) / args.steps},
+        "adjoint_over_forward_time": (total / args.steps) / (sum(forward_ms) / args.steps),
+        "loss": loss, "gradients": {"albedo_basis_norm": float(np.linalg.norm(basis)),
+                                     "alpha": [float(g[scenes.ADJOINT_CONDUCTOR, 4] + g[scenes.ADJOINT_CONDUCTOR, 5]),
+                                               float(g[scenes.ADJOINT_DIELECTRIC, 4] +
+                                                     g[scenes.ADJOINT_DIELECTRIC, 5])],
+                                     "light_scale": float(host_emission[0])},
+        "failed_lanes": report.failed_lanes, "clocks": clocks.summary(),
+        "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": host_target.numel() * 4,
+                "d2h_bytes_per_step": host_grads.numel() * 8 + 8},
+        # the forward render's launches, the loss kernel and the replay (as many launches as the forward)
+        "gpu_launches": (2 * report.kernel_launches + 1) * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "whole adjoint call (forward + replay)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": peak_kind},
+    }
+    scene.close()
+    ctx.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -269,7 +386,8 @@ def main():
     parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's)")
     parser.add_argument("--workload", default=WORKLOAD, choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD],
                         help="scene and frame (default: the headline Cornell + spheres frame); "
-                             f"{BATCH_WORKLOAD}: the 64-scene batch against 64 serial renders")
+                             f"{BATCH_WORKLOAD}: the 64-scene batch against 64 serial renders; "
+                             f"{ADJOINT_WORKLOAD}: the path-replay adjoint")
     parser.add_argument("--lanes", type=int, default=0, help="batch lanes (0: autotuned)")
     args = parser.parse_args()
 
@@ -288,6 +406,9 @@ def main():
     torch.cuda.set_device(local_rank)
     if args.workload == BATCH_WORKLOAD:
         run_batch(args, torch, rank)
+        return
+    if args.workload == ADJOINT_WORKLOAD:
+        run_adjoint(args, torch, rank)
         return
     distributed = world > 1
     if distributed:

@@ -581,6 +581,93 @@ def batch_job(seed):
     return builder, options, (side, side, spp)
 
 
+# ------------------------------------------------------------------------------------------------
+# Adjoint workload: the Cornell box and spheres with a displaced icosphere in place of the cuboids;
+# Lambert albedos from an 8-coefficient spectral basis
+# ------------------------------------------------------------------------------------------------
+
+SPECTRAL_KNOTS = [360.0 + k * 470.0 / 7.0 for k in range(8)]
+ADJOINT_WHITE, ADJOINT_RED, ADJOINT_GREEN, ADJOINT_LIGHT, ADJOINT_CONDUCTOR, ADJOINT_DIELECTRIC, ADJOINT_ICOSPHERE = \
+    range(7)
+ADJOINT_ALBEDO_MATERIALS = (ADJOINT_WHITE, ADJOINT_RED, ADJOINT_GREEN, ADJOINT_ICOSPHERE)
+ADJOINT_LIGHT_RADIANCE = 17.0
+
+
+def spectral_basis(nanometers):
+    """B[k, lane]: 8 piecewise-linear tent functions over 360-830 nm with knots every 470/7 nm (a
+    partition of unity), evaluated at the packet's wavelengths."""
+    step = 470.0 / 7.0
+    basis = np.zeros((8, len(nanometers)))
+    for lane, nm in enumerate(nanometers):
+        for k, knot in enumerate(SPECTRAL_KNOTS):
+            basis[k, lane] = max(0.0, 1.0 - abs(float(nm) - knot) / step)
+    return basis
+
+
+def adjoint_parameters():
+    """Base parameters of the adjoint workload: albedo coefficients (white, red, green, icosphere
+    x 8 knots), the GGX alpha of the conductor and of the dielectric, the light's radiance scale."""
+    albedo = np.array([[0.73] * 8, tabulated_spectrum(RED_WALL, SPECTRAL_KNOTS),
+                       tabulated_spectrum(GREEN_WALL, SPECTRAL_KNOTS), [0.5] * 8], np.float64)
+    return {"albedo": albedo, "alpha": np.array([0.2, 0.05]), "light_scale": 1.0}
+
+
+def perturbed_parameters(params, seed=7, sigma=0.1):
+    """params + N(0, sigma) (seeded), kept in the valid range (albedo in [0.02, 0.98], alpha in
+    [0.01, 1], scale > 0.1): the parameters of the target image."""
+    rng = np.random.default_rng(seed)
+    return {"albedo": np.clip(params["albedo"] + rng.normal(0.0, sigma, params["albedo"].shape), 0.02, 0.98),
+            "alpha": np.clip(params["alpha"] + rng.normal(0.0, sigma, 2), 0.01, 1.0),
+            "light_scale": max(0.1, params["light_scale"] + rng.normal(0.0, sigma))}
+
+
+def cornell_shell(builder, white, red, green, light):
+    """The five walls and the emitter quad of the Cornell workloads (6 meshes, then 6 instances)."""
+    meshes = [quad([(-1, -1, 0), (-1, -1, 2), (1, -1, 2), (1, -1, 0)], (0, 1, 0)),
+              quad([(-1, 1, 0), (1, 1, 0), (1, 1, 2), (-1, 1, 2)], (0, -1, 0)),
+              quad([(-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0)], (0, 0, 1)),
+              quad([(-1, -1, 0), (-1, 1, 0), (-1, 1, 2), (-1, -1, 2)], (1, 0, 0)),
+              quad([(1, -1, 0), (1, -1, 2), (1, 1, 2), (1, 1, 0)], (-1, 0, 0)),
+              quad([(-0.125, 0.985, 0.875), (0.125, 0.985, 0.875), (0.125, 0.985, 1.125),
+                    (-0.125, 0.985, 1.125)], (0, -1, 0))]
+    index = [builder.add_mesh(m) for m in meshes]
+    for mesh, material in zip(index, (white, white, white, red, green, light)):
+        builder.add_instance(mesh, material)
+
+
+def adjoint_icosphere(builder, params, subdivisions=6):
+    """The adjoint workload's scene at `params` (see adjoint_parameters). The icosphere is
+    subdivision 6 (81,920 triangles), displaced by 0.05 * U[-1, 1] (seed 0), radius 0.35. Materials
+    are in ADJOINT_* order."""
+    nm = builder.nanometers
+    lanes = params["albedo"] @ spectral_basis(nm)
+    white = builder.add_material(lambertian(lanes[0]))
+    red = builder.add_material(lambertian(lanes[1]))
+    green = builder.add_material(lambertian(lanes[2]))
+    light = builder.add_material(lambertian([0.0] * 4),
+                                 emission=(ADJOINT_LIGHT_RADIANCE * params["light_scale"],) * 4)
+    conductor = builder.add_material(rough_conductor(
+        [1.0] * 4, tabulated_spectrum(GOLD_ETA, nm), tabulated_spectrum(GOLD_K, nm), params["alpha"][0],
+        params["alpha"][0]))
+    dielectric = builder.add_material(rough_dielectric([1.0] * 4, 1.0, 1.5, params["alpha"][1], params["alpha"][1]))
+    ico = builder.add_material(lambertian(lanes[3]))
+    cornell_shell(builder, white, red, green, light)
+    sphere = builder.add_mesh(uv_sphere())
+    builder.add_instance(sphere, conductor, uniform_scale_translate(0.25, (0.4, -0.15, 1.25)))
+    builder.add_instance(sphere, dielectric, uniform_scale_translate(0.25, (-0.3, -0.75, 1.55)))
+    blob = builder.add_mesh(displaced_icosphere(subdivisions, 0.05, 0))
+    builder.add_instance(blob, ico, uniform_scale_translate(0.35, (-0.35, -0.6, 0.75)))
+    return builder
+
+
+def basis_gradients(material_gradients, nanometers):
+    """dLoss/d(albedo coefficient k) of each albedo material from the per-lane closure-weight
+    gradients (records of 8 doubles: weight lanes 0..3 first): sum over lanes of dLoss/dw_l B_k(l)."""
+    basis = spectral_basis(nanometers)
+    g = np.asarray(material_gradients, np.float64)
+    return np.stack([basis @ g[m, :4] for m in ADJOINT_ALBEDO_MATERIALS])
+
+
 BVH_STRESS_CAMERA = ((0.0, 2.0, 24.0), (0.0, -3.0, 0.0))  # origin, target
 BVH_STRESS_VFOV = 0.9
 
@@ -589,6 +676,7 @@ WORKLOADS = {
     "cornell_plain_64": (64, 64, 16, 8, "balance", "cornell"),
     "cornell_spheres_256": (256, 256, 256, 16, "power", "cornell_spheres"),
     "bvh_stress_1080p": (1920, 1080, 64, 16, "power", "bvh_stress"),
+    "adjoint_icosphere_256": (256, 256, 64, 8, "power", "adjoint_icosphere"),
 }
 
 
@@ -596,6 +684,11 @@ def build_workload(name):
     width, height, spp, depth, mis, scene = WORKLOADS[name]
     if scene == "bvh_stress":
         builder = bvh_stress(SceneBuilder(environment=(0.5, 0.5, 0.5, 0.5)))
+    elif scene == "adjoint_icosphere":
+        # Russian roulette off: with fixed samples the weight and emission gradients are then the
+        # exact derivatives of the rendered loss
+        builder = adjoint_icosphere(SceneBuilder(), adjoint_parameters())
+        return builder, abi.default_options(mis=mis, max_depth=depth, roulette=False), (width, height, spp)
     else:
         builder = cornell_box(SceneBuilder(), with_spheres=scene == "cornell_spheres")
     options = abi.default_options(mis=mis, max_depth=depth)

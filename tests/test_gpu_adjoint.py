@@ -203,6 +203,47 @@ def test_roughness_gradient_agrees_with_finite_differences_on_average(setup):
             assert abs(mean_fd) > 8.0 * stderr
 
 
+def test_basis_coefficient_gradients_of_the_adjoint_workload(setup):
+    """The adjoint workload's parameters (albedo = 8 spectral basis coefficients per material,
+    light radiance scale) at 32 x 32 x 4 spp: the per-lane gradients projected on the basis match
+    central finite differences of the coefficients (relative step 1e-3, same samples)."""
+    torch, ctx, _, _, sensor, _ = setup
+    width = height = 32
+    params = scenes.adjoint_parameters()
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+    options = abi.default_options(mis="power", max_depth=8, roulette=False)
+    target = torch.rand((height, width, 3), generator=torch.Generator().manual_seed(3)).mul_(0.3).cuda()
+
+    def render(p, adjoint):
+        builder = scenes.adjoint_icosphere(scenes.SceneBuilder(), p, subdivisions=4)
+        scene = ctx.create_scene(builder)
+        sums = torch.zeros((height, width, 8), dtype=torch.float64, device="cuda")
+        counts = torch.zeros((height, width), dtype=torch.int64, device="cuda")
+        grads = torch.zeros((len(builder.materials), 8), dtype=torch.float64, device="cuda")
+        emission = torch.zeros(1, dtype=torch.float64, device="cuda")
+        if adjoint:
+            ctx.render_adjoint_device(scene, cam, sensor, options, 4, 5, 0, 1, sums.data_ptr(), counts.data_ptr(),
+                                      target.data_ptr(), grads.data_ptr(), emission.data_ptr())
+        else:
+            ctx.render_film_device(scene, cam, sensor, options, 4, 5, 0, 1, sums.data_ptr(), counts.data_ptr())
+        scene.close()
+        loss = film_loss(sums.cpu().numpy(), target.cpu().numpy())
+        return loss, scenes.basis_gradients(grads.cpu().numpy(), builder.nanometers), float(emission.cpu()[0])
+
+    _, basis, light = render(params, True)
+    for row, k in [(0, 1), (3, 4), (1, 4)]:  # (white, 427 nm), (icosphere, 629 nm), (red, 629 nm)
+        h = 1e-3 * params["albedo"][row, k]
+        up, down = copy.deepcopy(params), copy.deepcopy(params)
+        up["albedo"][row, k] += h
+        down["albedo"][row, k] -= h
+        fd = (render(up, False)[0] - render(down, False)[0]) / (2.0 * h)
+        print(f"albedo ({row}, {k}): adjoint {basis[row, k]:.6g}, finite difference {fd:.6g}")
+        assert abs(basis[row, k] - fd) <= 5e-3 * abs(fd) + 1e-4 * np.abs(basis).max()
+    up, down = dict(params, light_scale=1.001), dict(params, light_scale=0.999)
+    fd = (render(up, False)[0] - render(down, False)[0]) / 0.002
+    assert abs(light - fd) <= 5e-3 * abs(fd), (light, fd)
+
+
 def test_film_is_the_calls_render(setup):
     _, _, builder, _, _, _ = setup
     first = gpu_adjoint(setup, builder)
