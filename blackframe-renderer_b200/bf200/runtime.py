@@ -25,6 +25,7 @@ EXPORTED_SYMBOLS = [
     "bf200_trace_paths_device_noalloc", "bf200_sobol_bits", "bf200_owen_sobol_bits",
     "bf200_render_films_device",
     "bf200_render_adjoint_device",
+    "bf200_render_backward_device",
 ]
 
 
@@ -78,6 +79,10 @@ def library():
                                                 C.POINTER(abi.FilmRequest), C.POINTER(abi.TransportOptions),
                                                 C.POINTER(abi.Film), C.POINTER(abi.Adjoint), C.POINTER(abi.Report)]
     lib.bf200_render_adjoint_device.restype = C.c_uint32
+    lib.bf200_render_backward_device.argtypes = [vp, vp, C.POINTER(abi.Camera), C.POINTER(abi.Sensor),
+                                                 C.POINTER(abi.FilmRequest), C.POINTER(abi.TransportOptions),
+                                                 C.POINTER(abi.Film), vp, vp, vp, C.POINTER(abi.Report)]
+    lib.bf200_render_backward_device.restype = C.c_uint32
     lib.bf200_sobol_bits.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
     lib.bf200_sobol_bits.restype = C.c_uint32
     lib.bf200_owen_sobol_bits.argtypes = [C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(C.c_uint64)]
@@ -228,6 +233,23 @@ class Context:
                                                           C.byref(film), C.byref(adjoint), C.byref(report)),
                     "render_adjoint_device")
         return adjoint.loss, report
+
+    def render_backward_device(self, scene, camera, sensor, options, samples_per_pixel, seed, first_sample,
+                               precision, sums, counts, image_adjoint, gradients, emission_gradient):
+        """bf200_render_backward_device: gradients for dLoss/d(image) = `image_adjoint` (device,
+        H x W x 3 floats) of the film that render_film_device wrote to (sums, counts) with the same
+        arguments. Returns the report of the re-trace."""
+        request = abi.FilmRequest(C.sizeof(abi.FilmRequest), samples_per_pixel, first_sample, seed, precision)
+        film = abi.Film(camera.width, camera.height, precision, 0, C.c_void_p(sums),
+                        C.cast(C.c_void_p(counts), C.POINTER(abi.u64)))
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_render_backward_device(self.handle, scene.handle, C.byref(camera),
+                                                           C.byref(sensor), C.byref(request), C.byref(options),
+                                                           C.byref(film), C.c_void_p(image_adjoint),
+                                                           C.c_void_p(gradients), C.c_void_p(emission_gradient),
+                                                           C.byref(report)), "render_backward_device")
+        return report
 
     def render_film(self, scene, camera, sensor, options, samples_per_pixel, seed=0, first_sample=0,
                     precision=0, film=None):

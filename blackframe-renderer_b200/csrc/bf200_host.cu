@@ -1862,63 +1862,49 @@ BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const 
     return st;
 }
 
-// Path-replay adjoint of a film render: forward render, loss and pixel adjoint, then one replay per
-// film chunk. A chunk's forward radiance is still in the chunk buffer after the forward render
-// when the film is a single chunk; otherwise the replay of each chunk re-traces it forward first.
-BF200_EXPORT blackframe_status bf200_render_adjoint_device(bf200_context* c, const bf200_scene* s,
-                                                            const bf200_camera_v1* cam, const bf200_sensor_v1* sensor,
-                                                            const bf200_film_request_v1* req,
-                                                            const bf200_transport_options_v1* o, bf200_film_v1* film,
-                                                            bf200_adjoint_v1* adj, bf200_report_v1* report) noexcept {
-    if (c == nullptr || s == nullptr || cam == nullptr || sensor == nullptr || req == nullptr || film == nullptr ||
-        adj == nullptr) {
-        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
-    }
-    if (adj->struct_size < sizeof(bf200_adjoint_v1) || adj->reserved != 0U || adj->target == nullptr ||
-        adj->gradients == nullptr || adj->emission_gradient == nullptr) {
-        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "incomplete adjoint request");
-    }
-    if (s->context != c) {
-        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "scene belongs to another context");
-    }
-    if (s->material_count > kAdjointMaterials) {
-        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "the adjoint takes scenes of at most 64 materials");
-    }
-    if (film->sums == nullptr || film->sample_counts == nullptr || film->precision > 1U) {
-        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "inconsistent film request");
-    }
-    cudaSetDevice(c->device);
+}  // extern "C"
+
+namespace {
+
+// The replay half of the path-replay adjoint, shared by the one-call loss entry point and the
+// backward entry point. `film` (device) holds the forward render of `req` and gives every pixel's
+// weight; `target` (loss mode) or `image_adjoint` (the caller's dLoss/d(image)) gives the loss
+// derivative. Each chunk of paths is traced forward again before its replay, to recover every
+// path's radiance (vertices are recomputed, not stored), unless `forward_resident`: the chunk
+// buffer still holds the radiance of a forward render that was a single chunk.
+blackframe_status adjoint_pass(bf200_context* c, const bf200_scene* s, const bf200_camera_v1* cam,
+                               const bf200_sensor_v1* sensor, const bf200_film_request_v1* req,
+                               const bf200_transport_options_v1* o, const bf200_film_v1* film, const float* target,
+                               const float* image_adjoint, bool forward_resident, bf200_material_gradient_v1* gradients,
+                               double* emission_gradient, double* loss_out, bf200_report_v1* retrace_report) {
     const uint64_t pixels = static_cast<uint64_t>(film->width) * film->height;
-    cudaError_t e = cudaMemsetAsync(film->sums, 0, pixels * (film->precision == 0U ? 16U : 64U), c->stream);
-    if (e == cudaSuccess) {
-        e = cudaMemsetAsync(film->sample_counts, 0, pixels * 8U, c->stream);
-    }
-    if (e != cudaSuccess) {
-        return cuda_fail(c, e, "adjoint film reset");
-    }
-    blackframe_status st = bf200_render_film_device(c, s, cam, sensor, req, o, film, report);
-    if (st != BLACKFRAME_STATUS_SUCCESS) {
+    const uint64_t samples_per_chunk = film_samples_per_chunk(pixels, req->samples_per_pixel);
+    const size_t radiance_bytes = std::max<uint64_t>(1, samples_per_chunk * pixels) * sizeof(float4);
+    if (const auto st = grow_workspace(c, &c->film_radiance, &c->film_radiance_bytes, radiance_bytes + 256,
+                                       "film chunk workspace");
+        st != BLACKFRAME_STATUS_SUCCESS) {
         return st;
     }
     // workspace: pixel adjoint | gradient sums + loss | pending scores | shadow scores
     const size_t pixel_bytes = ((pixels * sizeof(float4)) + 255) & ~size_t(255);
     const size_t sum_bytes = ((kAdjointWords + 1) * sizeof(double) + 255) & ~size_t(255);
     const size_t slot_bytes = c->capacity * sizeof(uint4);
-    if (const auto gst = grow_workspace(c, &c->adjoint_workspace, &c->adjoint_workspace_bytes,
-                                        pixel_bytes + sum_bytes + 2 * slot_bytes, "adjoint workspace");
-        gst != BLACKFRAME_STATUS_SUCCESS) {
-        return gst;
+    if (const auto st = grow_workspace(c, &c->adjoint_workspace, &c->adjoint_workspace_bytes,
+                                       pixel_bytes + sum_bytes + 2 * slot_bytes, "adjoint workspace");
+        st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
     }
     char* base = static_cast<char*>(c->adjoint_workspace);
     AdjointView av{};
-    av.pixel_adjoint = reinterpret_cast<float4*>(base);
     auto* pixel_adjoint = reinterpret_cast<float4*>(base);
+    av.pixel_adjoint = pixel_adjoint;
     av.gradients = reinterpret_cast<double*>(base + pixel_bytes);
     double* loss = av.gradients + kAdjointWords;
     av.pending = reinterpret_cast<uint4*>(base + pixel_bytes + sum_bytes);
     av.shadow_score = reinterpret_cast<uint4*>(base + pixel_bytes + sum_bytes + slot_bytes);
     av.pixels = static_cast<uint32_t>(pixels);
-    av.forward = static_cast<const float4*>(c->film_radiance);
+    auto* radiance = static_cast<float4*>(c->film_radiance);
+    av.forward = radiance;
     // d(sample rgb)/d(radiance lane): the linear map of k_film (sensor term, then XYZ to linear sRGB)
     static const double kXyzToRgb[3][3] = {{3.2404542, -1.5371385, -0.4985314},
                                            {-0.9692660, 1.8760108, 0.0415560},
@@ -1932,11 +1918,11 @@ BF200_EXPORT blackframe_status bf200_render_adjoint_device(bf200_context* c, con
             av.lane_rgb[ch][l] = static_cast<float>(v * sensor->normalization / sensor->wavelength_pdf[l]);
         }
     }
-    e = cudaMemsetAsync(av.gradients, 0, (kAdjointWords + 1) * sizeof(double), c->stream);
+    cudaError_t e = cudaMemsetAsync(av.gradients, 0, (kAdjointWords + 1) * sizeof(double), c->stream);
     if (e == cudaSuccess) {
         e = launch_adjoint_image(film->precision == 0U ? static_cast<const float4*>(film->sums) : nullptr,
-                                 film->precision == 1U ? static_cast<const double*>(film->sums) : nullptr,
-                                 adj->target, static_cast<uint32_t>(pixels), film->precision, pixel_adjoint, loss,
+                                 film->precision == 1U ? static_cast<const double*>(film->sums) : nullptr, target,
+                                 image_adjoint, static_cast<uint32_t>(pixels), film->precision, pixel_adjoint, loss,
                                  c->stream);
     }
     if (e != cudaSuccess) {
@@ -1947,15 +1933,14 @@ BF200_EXPORT blackframe_status bf200_render_adjoint_device(bf200_context* c, con
     if (const auto sst = sobol_table(c, *o, &sobol); sst != BLACKFRAME_STATUS_SUCCESS) {
         return sst;
     }
-    const uint64_t samples_per_chunk = film_samples_per_chunk(pixels, req->samples_per_pixel);
-    const bool one_chunk = samples_per_chunk >= req->samples_per_pixel;
-    auto* radiance = static_cast<float4*>(c->film_radiance);
+    const bool resident = forward_resident && samples_per_chunk >= req->samples_per_pixel;
+    blackframe_status st = BLACKFRAME_STATUS_SUCCESS;
     for (uint64_t first = 0; first < req->samples_per_pixel && st == BLACKFRAME_STATUS_SUCCESS;
          first += samples_per_chunk) {
         const uint64_t chunk = std::min<uint64_t>(samples_per_chunk, req->samples_per_pixel - first);
         const PathSource src = film_source(cam, req, first, chunk, radiance, sobol);
-        if (!one_chunk) {
-            st = run_wavefront_graph(c, s, src, params, nullptr);
+        if (!resident) {
+            st = run_wavefront_graph(c, s, src, params, retrace_report);
         }
         if (st == BLACKFRAME_STATUS_SUCCESS) {
             // pending tags of an earlier replay must not match this chunk's paths
@@ -1967,14 +1952,14 @@ BF200_EXPORT blackframe_status bf200_render_adjoint_device(bf200_context* c, con
     if (st != BLACKFRAME_STATUS_SUCCESS) {
         return st;
     }
-    e = cudaMemcpyAsync(adj->gradients, av.gradients, s->material_count * sizeof(bf200_material_gradient_v1),
+    e = cudaMemcpyAsync(gradients, av.gradients, s->material_count * sizeof(bf200_material_gradient_v1),
                         cudaMemcpyDeviceToDevice, c->stream);
     if (e == cudaSuccess) {
-        e = cudaMemcpyAsync(adj->emission_gradient, av.gradients + kAdjointEmission, sizeof(double),
+        e = cudaMemcpyAsync(emission_gradient, av.gradients + kAdjointEmission, sizeof(double),
                             cudaMemcpyDeviceToDevice, c->stream);
     }
     double host_loss = 0.0;
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && loss_out != nullptr) {
         e = cudaMemcpyAsync(&host_loss, loss, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     }
     if (e == cudaSuccess) {
@@ -1983,8 +1968,97 @@ BF200_EXPORT blackframe_status bf200_render_adjoint_device(bf200_context* c, con
     if (e != cudaSuccess) {
         return cuda_fail(c, e, "adjoint results");
     }
-    adj->loss = host_loss;
+    if (loss_out != nullptr) {
+        *loss_out = host_loss;
+    }
     return BLACKFRAME_STATUS_SUCCESS;
+}
+
+blackframe_status check_adjoint_scene(bf200_context* c, const bf200_scene* s) {
+    if (s->context != c) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "scene belongs to another context");
+    }
+    if (s->material_count > kAdjointMaterials) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "the adjoint takes scenes of at most 64 materials");
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+// One-call loss mode: forward render (film cleared first), L2 loss against the target and replay.
+// With a single-chunk film the forward render's radiance is reused and not traced again.
+BF200_EXPORT blackframe_status bf200_render_adjoint_device(bf200_context* c, const bf200_scene* s,
+                                                            const bf200_camera_v1* cam, const bf200_sensor_v1* sensor,
+                                                            const bf200_film_request_v1* req,
+                                                            const bf200_transport_options_v1* o, bf200_film_v1* film,
+                                                            bf200_adjoint_v1* adj, bf200_report_v1* report) noexcept {
+    if (c == nullptr || s == nullptr || cam == nullptr || sensor == nullptr || req == nullptr || film == nullptr ||
+        adj == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (adj->struct_size < sizeof(bf200_adjoint_v1) || adj->reserved != 0U || adj->target == nullptr ||
+        adj->gradients == nullptr || adj->emission_gradient == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "incomplete adjoint request");
+    }
+    if (const auto st = check_adjoint_scene(c, s); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    if (film->sums == nullptr || film->sample_counts == nullptr || film->precision > 1U) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "inconsistent film request");
+    }
+    cudaSetDevice(c->device);
+    const uint64_t pixels = static_cast<uint64_t>(film->width) * film->height;
+    cudaError_t e = cudaMemsetAsync(film->sums, 0, pixels * (film->precision == 0U ? 16U : 64U), c->stream);
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(film->sample_counts, 0, pixels * 8U, c->stream);
+    }
+    if (e != cudaSuccess) {
+        return cuda_fail(c, e, "adjoint film reset");
+    }
+    if (const auto st = bf200_render_film_device(c, s, cam, sensor, req, o, film, report);
+        st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    return adjoint_pass(c, s, cam, sensor, req, o, film, adj->target, nullptr, true, adj->gradients,
+                        adj->emission_gradient, &adj->loss, nullptr);
+}
+
+// Backward half of the forward/backward pair (the forward is bf200_render_film_device).
+BF200_EXPORT blackframe_status bf200_render_backward_device(
+    bf200_context* c, const bf200_scene* s, const bf200_camera_v1* cam, const bf200_sensor_v1* sensor,
+    const bf200_film_request_v1* req, const bf200_transport_options_v1* o, const bf200_film_v1* film,
+    const float* image_adjoint, bf200_material_gradient_v1* gradients, double* emission_gradient,
+    bf200_report_v1* report) noexcept {
+    if (c == nullptr || s == nullptr || cam == nullptr || sensor == nullptr || req == nullptr || film == nullptr ||
+        image_adjoint == nullptr || gradients == nullptr || emission_gradient == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (const auto st = check_adjoint_scene(c, s); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    if (req->struct_size < sizeof(bf200_film_request_v1) || req->precision > 1 || film->precision != req->precision ||
+        film->width != cam->width || film->height != cam->height || cam->width == 0 || cam->height == 0 ||
+        film->sums == nullptr || film->sample_counts == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "inconsistent film request");
+    }
+    if (const auto st = validate_options(c, o); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    if (static_cast<uint64_t>(cam->width) * cam->height > 0xFFFFFFFFULL) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "film too large");
+    }
+    if (report != nullptr) {
+        std::memset(report, 0, sizeof(*report));
+    }
+    cudaSetDevice(c->device);
+    if (const auto st = ensure_capacity(c); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    return adjoint_pass(c, s, cam, sensor, req, o, film, nullptr, image_adjoint, false, gradients, emission_gradient,
+                        nullptr, report);
 }
 
 BF200_EXPORT blackframe_status bf200_render_film(bf200_context* c, const bf200_scene* s, const bf200_camera_v1* cam,

@@ -2043,13 +2043,14 @@ __global__ void k_film(const float4* path_radiance, uint32_t pixels, uint32_t sa
     counts[p] = count;
 }
 
-// Loss of a film against a target image and its adjoint per pixel. The image is the film's
-// weighted mean, rgb / weight (the Neumaier sum plus its compensation for a float64 film). The loss
-// is sum over pixels and channels of (image - target)^2; pixel_adjoint receives
-// dLoss/d(image) / weight = 2 (image - target) / weight, the derivative per unit-weight sample.
+// Per-pixel adjoint of the path-replay adjoint: dLoss/d(image) / weight, the derivative per
+// unit-weight sample, where the image is the film's weighted mean rgb / weight (the Neumaier sum
+// plus its compensation for a float64 film). With a target, the loss is the sum over pixels and
+// channels of (image - target)^2 (added to *loss) and dLoss/d(image) = 2 (image - target);
+// without one, dLoss/d(image) is the caller's image_adjoint.
 __global__ void __launch_bounds__(256) k_adjoint_image(const float4* film32, const double* film64, const float* target,
-                                                       uint32_t pixels, uint32_t precision, float4* pixel_adjoint,
-                                                       double* loss) {
+                                                       const float* image_adjoint, uint32_t pixels, uint32_t precision,
+                                                       float4* pixel_adjoint, double* loss) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     double part = 0.0;
     if (p < pixels) {
@@ -2068,12 +2069,17 @@ __global__ void __launch_bounds__(256) k_adjoint_image(const float4* film32, con
             weight = film64[8ULL * p + 3] + film64[8ULL * p + 7];
         }
         float adj[3] = {0.0F, 0.0F, 0.0F};
-        if (weight > 0.0) {
+        if (weight > 0.0 && target != nullptr) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const double d = rgb[k] / weight - static_cast<double>(target[3ULL * p + k]);
                 part += d * d;
                 adj[k] = static_cast<float>(2.0 * d / weight);
+            }
+        } else if (weight > 0.0) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                adj[k] = static_cast<float>(static_cast<double>(image_adjoint[3ULL * p + k]) / weight);
             }
         }
         pixel_adjoint[p] = make_float4(adj[0], adj[1], adj[2], 0.0F);
@@ -2081,7 +2087,7 @@ __global__ void __launch_bounds__(256) k_adjoint_image(const float4* film32, con
     for (int off = 16; off > 0; off >>= 1) {
         part += __shfl_down_sync(0xFFFFFFFFU, part, off);
     }
-    if ((threadIdx.x & 31U) == 0U && part != 0.0) {
+    if ((threadIdx.x & 31U) == 0U && part != 0.0 && loss != nullptr) {
         atomicAdd(loss, part);
     }
 }
@@ -2249,10 +2255,11 @@ cudaError_t launch_film(const float4* path_radiance, uint32_t pixels, uint32_t s
     return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint_image(const float4* film32, const double* film64, const float* target, uint32_t pixels,
-                                 uint32_t precision, float4* pixel_adjoint, double* loss, cudaStream_t stream) {
-    k_adjoint_image<<<(pixels + 255U) / 256U, 256, 0, stream>>>(film32, film64, target, pixels, precision,
-                                                                pixel_adjoint, loss);
+cudaError_t launch_adjoint_image(const float4* film32, const double* film64, const float* target,
+                                 const float* image_adjoint, uint32_t pixels, uint32_t precision, float4* pixel_adjoint,
+                                 double* loss, cudaStream_t stream) {
+    k_adjoint_image<<<(pixels + 255U) / 256U, 256, 0, stream>>>(film32, film64, target, image_adjoint, pixels,
+                                                                precision, pixel_adjoint, loss);
     return cudaGetLastError();
 }
 

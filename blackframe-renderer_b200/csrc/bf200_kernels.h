@@ -33,10 +33,11 @@ cudaError_t launch_retire(const Wavefront& w, const PathSource& src, uint32_t gr
 cudaError_t launch_film(const float4* path_radiance, uint32_t pixels, uint32_t samples, const float* response12,
                         const float* pdf4, float normalization, uint32_t precision, float4* film32, double* film64,
                         unsigned long long* counts, unsigned long long* skipped, cudaStream_t stream);
-// Loss of a film against a target image (sum of squared rgb differences, added to *loss) and the
-// per-pixel adjoint of the path-replay adjoint.
-cudaError_t launch_adjoint_image(const float4* film32, const double* film64, const float* target, uint32_t pixels,
-                                 uint32_t precision, float4* pixel_adjoint, double* loss, cudaStream_t stream);
+// Per-pixel adjoint of the path-replay adjoint, from a target image (the loss, the sum of squared
+// rgb differences, is added to *loss) or, with target null, from the caller's dLoss/d(image).
+cudaError_t launch_adjoint_image(const float4* film32, const double* film64, const float* target,
+                                 const float* image_adjoint, uint32_t pixels, uint32_t precision, float4* pixel_adjoint,
+                                 double* loss, cudaStream_t stream);
 cudaError_t launch_queries(const SceneView& s, const bf200_ray_v1* rays, uint64_t n, bf200_hit_v1* hits,
                            uint32_t* occluded, cudaStream_t stream);
 

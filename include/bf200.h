@@ -570,6 +570,18 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_adjoint_device(
     const bf200_transport_options_v1* options, bf200_film_v1* film, bf200_adjoint_v1* adjoint,
     bf200_report_v1* report) BF200_NOEXCEPT;
 
+/* The same adjoint as a forward/backward pair for any image loss. The forward is
+ * bf200_render_film_device. The caller computes dLoss/d(image) (device, height x width x 3 floats,
+ * image = film rgb / film weight) and passes it here with the forward's film (its weights) and
+ * arguments. The backward traces every path again to recover its radiance (path vertices are
+ * recomputed, not stored, so memory stays bounded by one film chunk), then replays it. It costs
+ * about two forward renders; the report counts the re-trace. Gradients as described above. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_backward_device(
+    bf200_context* context, const bf200_scene* scene, const bf200_camera_v1* camera,
+    const bf200_sensor_v1* sensor, const bf200_film_request_v1* request,
+    const bf200_transport_options_v1* options, const bf200_film_v1* film, const float* image_adjoint,
+    bf200_material_gradient_v1* gradients, double* emission_gradient, bf200_report_v1* report) BF200_NOEXCEPT;
+
 /* Closest-hit query for a batch of world rays (trace_cuda_closest_hits, ClosestHit.hpp:21-28).
  * Per ray writes t, barycentrics b0..b2, instance index and primitive index (0xffffffff on a
  * miss). Host pointers. */

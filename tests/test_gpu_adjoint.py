@@ -244,6 +244,42 @@ def test_basis_coefficient_gradients_of_the_adjoint_workload(setup):
     assert abs(light - fd) <= 5e-3 * abs(fd), (light, fd)
 
 
+def test_forward_backward_pair_matches_the_loss_call(setup):
+    """Forward (bf200_render_film_device), dLoss/d(image) computed by the caller, backward
+    (bf200_render_backward_device): the same gradients as the one-call loss mode, also for a film
+    of several chunks (512 x 512 x 300 spp is 78.6 M paths, more than one 64 M-path chunk)."""
+    torch, ctx, builder, cam, sensor, target = setup
+    scene = ctx.create_scene(builder)
+    for width, height, spp in [(WIDTH, HEIGHT, SPP), (512, 512, 300)]:
+        camera = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV,
+                                       scenes.PATH_TIME)
+        tgt = torch.rand((height, width, 3), generator=torch.Generator().manual_seed(5)).mul_(0.3).cuda()
+        sums = torch.zeros((height, width, 8), dtype=torch.float64, device="cuda")
+        counts = torch.zeros((height, width), dtype=torch.int64, device="cuda")
+        one = torch.zeros((len(builder.materials), 8), dtype=torch.float64, device="cuda")
+        one_e = torch.zeros(1, dtype=torch.float64, device="cuda")
+        loss, _ = ctx.render_adjoint_device(scene, camera, sensor, transport_options(), spp, SEED, 0, 1,
+                                            sums.data_ptr(), counts.data_ptr(), tgt.data_ptr(), one.data_ptr(),
+                                            one_e.data_ptr())
+        sums.zero_()
+        counts.zero_()
+        ctx.render_film_device(scene, camera, sensor, transport_options(), spp, SEED, 0, 1, sums.data_ptr(),
+                               counts.data_ptr())
+        image = (sums[..., :3] + sums[..., 4:7]) / (sums[..., 3:4] + sums[..., 7:8])
+        assert abs(float(((image - tgt.double()) ** 2).sum()) - loss) <= 1e-9 * loss
+        image_adjoint = (2.0 * (image - tgt.double())).float().contiguous()
+        two = torch.zeros_like(one)
+        two_e = torch.zeros_like(one_e)
+        report = ctx.render_backward_device(scene, camera, sensor, transport_options(), spp, SEED, 0, 1,
+                                            sums.data_ptr(), counts.data_ptr(), image_adjoint.data_ptr(),
+                                            two.data_ptr(), two_e.data_ptr())
+        assert report.path_count == width * height * spp
+        a, b = one.cpu().numpy(), two.cpu().numpy()
+        assert np.allclose(a, b, rtol=1e-5, atol=1e-7 * np.abs(a).max()), (a, b)
+        assert abs(float(one_e.cpu()[0]) - float(two_e.cpu()[0])) <= 1e-5 * abs(float(one_e.cpu()[0]))
+    scene.close()
+
+
 def test_film_is_the_calls_render(setup):
     _, _, builder, _, _, _ = setup
     first = gpu_adjoint(setup, builder)
