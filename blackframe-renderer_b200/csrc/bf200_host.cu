@@ -978,11 +978,12 @@ blackframe_status run_wavefront_graph(bf200_context* c, const bf200_scene* s, Pa
 
 // Runs the persistent wavefront until every path of `src` has been traced and retired. Without
 // instrumentation the loop runs on the device inside one graph; with it, the host drives every
-// iteration so each stage can be timed with events.
+// iteration so each stage can be timed with events (and profilers, which do not see the kernels of
+// a device-side loop, see every launch). `adjoint` makes the run a path-replay adjoint replay.
 blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSource src, const TransportParams& p,
-                                bool instrument, bf200_report_v1* report) {
+                                bool instrument, bf200_report_v1* report, const AdjointView* adjoint = nullptr) {
     if (!instrument) {
-        return run_wavefront_graph(c, s, src, p, report);
+        return run_wavefront_graph(c, s, src, p, report, adjoint);
     }
     Wavefront& w = c->w;
     cudaStream_t st = c->stream;
@@ -1021,7 +1022,7 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
             if (instrument) {
                 cudaEventRecord(ev[stage], st);
             }
-            e = launch_stage(stage, s->view, w, src, p, grid, st, &stage_launches);
+            e = launch_stage(stage, s->view, w, src, p, grid, st, &stage_launches, adjoint);
         }
         if (instrument) {
             cudaEventRecord(ev[4], st);
@@ -1939,13 +1940,14 @@ blackframe_status adjoint_pass(bf200_context* c, const bf200_scene* s, const bf2
          first += samples_per_chunk) {
         const uint64_t chunk = std::min<uint64_t>(samples_per_chunk, req->samples_per_pixel - first);
         const PathSource src = film_source(cam, req, first, chunk, radiance, sobol);
+        const bool instrument = o->instrumentation != 0U;
         if (!resident) {
-            st = run_wavefront_graph(c, s, src, params, retrace_report);
+            st = run_wavefront(c, s, src, params, instrument, retrace_report);
         }
         if (st == BLACKFRAME_STATUS_SUCCESS) {
             // pending tags of an earlier replay must not match this chunk's paths
             e = cudaMemsetAsync(av.pending, 0, slot_bytes, c->stream);
-            st = e == cudaSuccess ? run_wavefront_graph(c, s, src, params, nullptr, &av)
+            st = e == cudaSuccess ? run_wavefront(c, s, src, params, instrument, nullptr, &av)
                                   : cuda_fail(c, e, "adjoint scores reset");
         }
     }
