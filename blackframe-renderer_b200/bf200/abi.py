@@ -74,9 +74,14 @@ class Material(C.Structure):
                 ("reserved", u32 * 3)]
 
 
+GEOMETRY_TRIANGLES = 0
+GEOMETRY_SPHERE = 1
+
+
 class Geometry(C.Structure):
     _fields_ = [("geometry_id", u32), ("vertex_offset", u32), ("vertex_count", u32),
-                ("triangle_offset", u32), ("triangle_count", u32), ("reserved", u32 * 3)]
+                ("triangle_offset", u32), ("triangle_count", u32), ("kind", u32), ("radius", C.c_float),
+                ("reserved", u32)]
 
 
 class Instance(C.Structure):

@@ -148,6 +148,18 @@ def uniform_scale_translate(radius, center):
 # meshes
 # ------------------------------------------------------------------------------------------------
 
+class Sphere:
+    """An analytic sphere geometry: centre and radius in object space."""
+
+    def __init__(self, centre, radius):
+        self.centre = np.asarray(centre, F32).reshape(3)
+        self.radius = F32(radius)
+        self.positions = self.centre.reshape(1, 3)
+        self.normals = np.zeros((1, 3), F32)
+        self.uvs = np.zeros((1, 2), F32)
+        self.triangles = np.zeros((0, 3), np.uint32)
+
+
 class Mesh:
     def __init__(self, positions, normals, uvs, triangles):
         self.positions = np.asarray(positions, dtype=F32).reshape(-1, 3)
@@ -286,6 +298,8 @@ class SceneBuilder:
             g.geometry_id = 100 + index
             g.vertex_offset, g.vertex_count = vertex_offset, len(mesh.positions)
             g.triangle_offset, g.triangle_count = triangle_offset, len(mesh.triangles)
+            if isinstance(mesh, Sphere):
+                g.kind, g.radius = abi.GEOMETRY_SPHERE, float(mesh.radius)
             positions.append(mesh.positions)
             normals.append(mesh.normals)
             uvs.append(mesh.uvs)
@@ -362,8 +376,10 @@ GOLD_ETA = [(360, 1.5), (450, 1.3), (500, 0.9), (550, 0.40), (600, 0.25), (700, 
 GOLD_K = [(360, 1.9), (450, 1.85), (500, 1.85), (550, 2.3), (600, 2.9), (700, 3.9), (830, 5.3)]
 
 
-def cornell_box(builder, with_spheres):
-    """Walls, emitter and cuboids of the Cornell workloads; spheres when `with_spheres`."""
+def cornell_box(builder, with_spheres, analytic_spheres=False):
+    """Walls, emitter and cuboids of the Cornell workloads; spheres when `with_spheres`: 64 x 32
+    UV-sphere meshes, or analytic spheres (centre and radius in world space, identity instance
+    transforms, as renderer::Sphere takes them) when `analytic_spheres`."""
     nm = builder.nanometers
     white = builder.add_material(lambertian([0.73] * 4))
     red = builder.add_material(lambertian(tabulated_spectrum(RED_WALL, nm)))
@@ -391,10 +407,14 @@ def cornell_box(builder, with_spheres):
     builder.add_instance(box, white, rotation_y_scale_translate(-15.0, (0.6, 0.6, 0.6),
                                                                (0.4, -0.7, 1.25)))
     if with_spheres:
-        sphere = builder.add_mesh(uv_sphere())
         conductor = builder.add_material(rough_conductor(
             [1.0] * 4, tabulated_spectrum(GOLD_ETA, nm), tabulated_spectrum(GOLD_K, nm), 0.2, 0.2))
         dielectric = builder.add_material(rough_dielectric([1.0] * 4, 1.0, 1.5, 0.05, 0.05))
+        if analytic_spheres:
+            builder.add_instance(builder.add_mesh(Sphere((0.4, -0.15, 1.25), 0.25)), conductor)
+            builder.add_instance(builder.add_mesh(Sphere((-0.3, -0.75, 1.55), 0.25)), dielectric)
+            return builder
+        sphere = builder.add_mesh(uv_sphere())
         builder.add_instance(sphere, conductor, uniform_scale_translate(0.25, (0.4, -0.15, 1.25)))
         builder.add_instance(sphere, dielectric,
                              uniform_scale_translate(0.25, (-0.3, -0.75, 1.55)))
@@ -677,6 +697,7 @@ WORKLOADS = {
     "cornell_spheres_256": (256, 256, 256, 16, "power", "cornell_spheres"),
     "bvh_stress_1080p": (1920, 1080, 64, 16, "power", "bvh_stress"),
     "adjoint_icosphere_256": (256, 256, 64, 8, "power", "adjoint_icosphere"),
+    "cornell_analytic_256": (256, 256, 256, 16, "power", "cornell_analytic"),
 }
 
 
@@ -690,7 +711,8 @@ def build_workload(name):
         builder = adjoint_icosphere(SceneBuilder(), adjoint_parameters())
         return builder, abi.default_options(mis=mis, max_depth=depth, roulette=False), (width, height, spp)
     else:
-        builder = cornell_box(SceneBuilder(), with_spheres=scene == "cornell_spheres")
+        builder = cornell_box(SceneBuilder(), with_spheres=scene in ("cornell_spheres", "cornell_analytic"),
+                              analytic_spheres=scene == "cornell_analytic")
     options = abi.default_options(mis=mis, max_depth=depth)
     return builder, options, (width, height, spp)
 

@@ -58,7 +58,7 @@ struct SceneView {
     const uint4* inst_info;        // geometry, material, visibility mask, light index or ~0
     const uint8_t* inst_route;     // shading route of a hit on the instance (kRoute*)
     const uint32_t* inst_normal_offset;
-    const uint4* geom_info;        // vertex offset, triangle offset, bvh root node, -
+    const uint4* geom_info;        // vertex offset (sphere: leaf record), triangle offset, bvh root node, kind
     const float* positions;        // object space, 3 per vertex
     const float* normals;          // 3 per vertex
     const uint32_t* triangles;     // geometry-local vertex indices, 3 per triangle
@@ -75,7 +75,17 @@ struct SceneView {
     const float* light_tri_areas;
     const float* light_tri_cdf;
     float4 environment;
+    uint32_t sphere_count;  // analytic sphere geometries (0: the walks run their triangle-only form)
 };
+
+// geom_info.w: the geometry's kind. A sphere's geom_info.x is its leaf record (centre, radius).
+constexpr uint32_t kGeometryTriangles = 0U, kGeometrySphere = 1U;
+// A sphere's leaf record in the leaf-triangle array: v0 = centre (w: primitive index 0),
+// v1 = (radius, 0, 0, kSphereLeaf as bits), v2 = 0. Triangle records have 0 in v1.w.
+constexpr uint32_t kSphereLeaf = 0x53504845U;
+// A sphere's leaf code carries the record count 8, which no triangle leaf has (at most 4), so the
+// walks branch to the sphere test once per leaf, outside the triangle loop.
+constexpr uint32_t kSphereLeafCount = 8U;
 
 // Transport options resolved for the device.
 struct TransportParams {

@@ -190,6 +190,8 @@ struct Prim {
 };
 
 constexpr int kLeafSize = 4;
+static_assert(kLeafSize < static_cast<int>(kSphereLeafCount) && kSphereLeafCount == kMaxLeafSize,
+              "triangle leaves never carry the sphere leaf count");
 constexpr int kBins = 16;
 
 struct Builder {
@@ -312,10 +314,56 @@ struct Builder {
     }
 };
 
-// Builds the BLAS of one geometry; returns the root node index.
+// Rounds a double down (dir < 0) or up (dir > 0) to a float.
+float round_outward(double x, int dir) {
+    float f = static_cast<float>(x);
+    if (dir < 0 && static_cast<double>(f) > x) {
+        f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+    }
+    if (dir > 0 && static_cast<double>(f) < x) {
+        f = std::nextafter(f, std::numeric_limits<float>::infinity());
+    }
+    return f;
+}
+
+// Object box of a sphere: centre -+ radius, rounded outward.
+Box sphere_box(const bf200_scene_desc_v1& d, uint32_t g) {
+    const float* centre = d.positions + 3ULL * d.geometries[g].vertex_offset;
+    const double r = d.geometries[g].radius;
+    Box b;
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = round_outward(static_cast<double>(centre[a]) - r, -1);
+        b.hi[a] = round_outward(static_cast<double>(centre[a]) + r, 1);
+    }
+    return b;
+}
+
+// Builds the BLAS of one geometry; returns the root node index. A sphere's BLAS is one node whose
+// single leaf is the sphere's record (centre, radius; see kSphereLeaf).
 uint32_t build_blas(const bf200_scene_desc_v1& d, uint32_t g, std::vector<BvhNode>& nodes,
                     std::vector<float4>& leaf_tris, uint32_t& depth) {
     const auto& geom = d.geometries[g];
+    if (geom.kind == BF200_GEOMETRY_SPHERE) {
+        const float* centre = d.positions + 3ULL * geom.vertex_offset;
+        const uint32_t first = static_cast<uint32_t>(leaf_tris.size() / 3);
+        float marker;
+        std::memcpy(&marker, &kSphereLeaf, 4);
+        leaf_tris.push_back(make_float4(centre[0], centre[1], centre[2], 0.0F));  // primitive 0
+        leaf_tris.push_back(make_float4(geom.radius, 0.0F, 0.0F, marker));
+        leaf_tris.push_back(make_float4(0.0F, 0.0F, 0.0F, 0.0F));
+        const int leaf = ~static_cast<int>((first << kLeafCountBits) | (kSphereLeafCount - 1U));
+        const Box lb = sphere_box(d, g);
+        const float inf = std::numeric_limits<float>::infinity();
+        const uint32_t root = static_cast<uint32_t>(nodes.size());
+        BvhNode node{};
+        node.a = make_float4(lb.lo[0], lb.hi[0], lb.lo[1], lb.hi[1]);
+        node.b = make_float4(inf, -inf, inf, -inf);
+        node.c = make_float4(lb.lo[2], lb.hi[2], inf, -inf);
+        node.d = make_int4(leaf, leaf, 0, 0);
+        nodes.push_back(node);
+        depth = 1;
+        return root;
+    }
     const float* positions = d.positions + 3ULL * geom.vertex_offset;
     const uint32_t* tris = d.triangles + 3ULL * geom.triangle_offset;
     std::vector<Prim> prims(geom.triangle_count);
@@ -347,18 +395,6 @@ uint32_t build_blas(const bf200_scene_desc_v1& d, uint32_t g, std::vector<BvhNod
     const int r = b.build(0, static_cast<int>(prims.size()), 1);
     depth = b.max_depth;
     return static_cast<uint32_t>(r);
-}
-
-// Rounds a double down (dir < 0) or up (dir > 0) to a float.
-float round_outward(double x, int dir) {
-    float f = static_cast<float>(x);
-    if (dir < 0 && static_cast<double>(f) > x) {
-        f = std::nextafter(f, -std::numeric_limits<float>::infinity());
-    }
-    if (dir > 0 && static_cast<double>(f) < x) {
-        f = std::nextafter(f, std::numeric_limits<float>::infinity());
-    }
-    return f;
 }
 
 // World box of an instance: the object box's eight corners through object_to_world in double,
@@ -652,6 +688,27 @@ blackframe_status validate_desc(bf200_context* c, const bf200_scene_desc_v1* d) 
     }
     for (uint32_t g = 0; g < d->geometry_count; ++g) {
         const auto& geom = d->geometries[g];
+        if (geom.reserved != 0U || geom.kind > BF200_GEOMETRY_SPHERE) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "unknown geometry kind or reserved field set");
+        }
+        if (geom.kind == BF200_GEOMETRY_SPHERE) {
+            // SphereT::create (Sphere.hpp:303-315): finite centre, finite positive radius
+            if (geom.vertex_count != 1U || geom.triangle_count != 0U ||
+                geom.vertex_offset + 1ULL > d->vertex_count) {
+                return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "a sphere is one centre vertex and no triangles");
+            }
+            const float* centre = d->positions + 3ULL * geom.vertex_offset;
+            if (!std::isfinite(centre[0]) || !std::isfinite(centre[1]) || !std::isfinite(centre[2])) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "A sphere center must be finite.");
+            }
+            if (!std::isfinite(geom.radius) || geom.radius <= 0.0F) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "A sphere radius must be finite and positive.");
+            }
+            continue;
+        }
+        if (geom.radius != 0.0F) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "a triangle mesh has no radius");
+        }
         if (geom.vertex_offset + static_cast<uint64_t>(geom.vertex_count) > d->vertex_count ||
             geom.triangle_offset + static_cast<uint64_t>(geom.triangle_count) > d->triangle_count ||
             geom.triangle_count == 0) {
@@ -1300,9 +1357,16 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
             Collapser collapser{nodes, nodes4};
             const int root4 = collapser.collapse(static_cast<int>(root), 1, depth4);
             blas_depth = std::max(blas_depth, 3 * depth4 + 1);  // at most 3 net entries per level
-            geom_info[g] = make_uint4(d->geometries[g].vertex_offset, d->geometries[g].triangle_offset,
-                                      static_cast<uint32_t>(root4), 0);
             const auto& geom = d->geometries[g];
+            if (geom.kind == BF200_GEOMETRY_SPHERE) {
+                // the sphere's leaf record is the last one this BLAS added
+                geom_info[g] = make_uint4(static_cast<uint32_t>(leaf_tris.size() / 3 - 1), 0U,
+                                          static_cast<uint32_t>(root4), kGeometrySphere);
+                object_box[g] = sphere_box(*d, g);
+                continue;
+            }
+            geom_info[g] = make_uint4(d->geometries[g].vertex_offset, d->geometries[g].triangle_offset,
+                                      static_cast<uint32_t>(root4), kGeometryTriangles);
             const uint32_t* local = d->triangles + 3ULL * geom.triangle_offset;
             for (uint32_t t = 0; t < 3 * geom.triangle_count; ++t) {
                 object_box[g].grow(d->positions + 3ULL * (geom.vertex_offset + local[t]));
@@ -1377,6 +1441,11 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
                 return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "instance transform orientation is singular");
             }
             uint32_t light_index = 0x7FFFFFFFU;
+            if (is_black4(d->materials[inst.material_index].emitted_radiance) == false &&
+                d->geometries[inst.geometry_index].kind == BF200_GEOMETRY_SPHERE) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
+                            "emissive analytic spheres are not supported: lights are meshes (no substitution)");
+            }
             if (is_black4(d->materials[inst.material_index].emitted_radiance) == false) {
                 LightInfo info{};
                 std::string error;
@@ -1448,6 +1517,10 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         SceneView& v = scene->view;
         v.instance_count = d->instance_count;
         v.light_count = scene->light_count;
+        v.sphere_count = 0U;
+        for (uint32_t g = 0; g < d->geometry_count; ++g) {
+            v.sphere_count += d->geometries[g].kind == BF200_GEOMETRY_SPHERE ? 1U : 0U;
+        }
         v.tlas_root = tlas_root;
         blackframe_status st = BLACKFRAME_STATUS_SUCCESS;
         auto up = [&](auto& host, auto& dst) {

@@ -20,6 +20,7 @@
 
 #include "bf200_device.cuh"
 #include "bf200_kernels.h"
+#include "bf200_sphere.cuh"
 
 // Resident 256-thread blocks per SM the register allocation must allow, per stage kernel.
 #ifndef BF200_INTERSECT_MIN_BLOCKS
@@ -541,6 +542,11 @@ __device__ __forceinline__ bool instance_step(const SceneView& s, int entry, con
     return true;
 }
 
+// A sphere leaf's outcome codes are the triangle test's, so the walks treat both alike.
+static_assert(int(kSphereMiss) == int(kTriMiss) && int(kSphereHit) == int(kTriHit) &&
+                  int(kSphereFailure) == int(kTriFailure),
+              "outcome codes");
+
 // Per-lane walk state shared by the two traversals.
 struct Walk {
     RayInv r;       // current ray (object space of the current instance)
@@ -617,6 +623,8 @@ __device__ __forceinline__ void closest_begin(const SceneView& s, F3 o, F3 d, fl
     push_instances(s, c.world, t_min, t_max, mask, stack, c.w.sp);
 }
 
+// SPH: the scene has analytic spheres (the walks of triangle-only scenes carry no sphere code).
+template <bool SPH>
 __device__ __forceinline__ bool closest_step(const SceneView& s, TraversalStack& stack, ClosestWalk& c) {
     const int leaf_code =
         next_leaf(s, c.world, c.o, c.d, c.t_min, c.found ? c.best.t : c.t_max, c.mask, stack, c.w);
@@ -626,6 +634,22 @@ __device__ __forceinline__ bool closest_step(const SceneView& s, TraversalStack&
     const uint32_t packed = static_cast<uint32_t>(~leaf_code);
     const uint32_t first = packed >> kLeafCountBits;
     const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
+    if (SPH && n == kSphereLeafCount) {  // an analytic sphere: one record, tested apart from the triangle loop
+        const float4 v0 = s.leaf_tris[3ULL * first];
+        const SphereHit h = sphere_intersect(v0, s.leaf_tris[3ULL * first + 1].x, c.w.ro, c.w.rd, c.t_min,
+                                             c.found ? c.best.t : c.t_max);
+        const uint32_t prim = __float_as_uint(v0.w);
+        if (h.outcome == kSphereFailure) {
+            c.w.failed = true;
+        } else if (h.outcome == kSphereHit && (!c.found || precedes(h.t, c.w.inst, prim, c.best))) {
+            c.best.t = h.t;
+            c.best.instance = c.w.inst;
+            c.best.primitive = prim;
+            c.best.leaf = first;
+            c.found = true;
+        }
+        return true;
+    }
     for (uint32_t j = 0; j < n; ++j) {
         const uint32_t leaf = first + j;
         const float4 v0 = s.leaf_tris[3ULL * leaf];
@@ -663,11 +687,12 @@ __device__ __forceinline__ ClosestResult closest_end(ClosestWalk& c) {
 
 // Closest hit of one ray (the standalone query kernel); k_trace runs the same steps with dynamic
 // ray fetch.
+template <bool SPH>
 __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
                                      TraversalStack& stack) {
     ClosestWalk c;
     closest_begin(s, o, d, t_min, t_max, mask, stack, c);
-    while (closest_step(s, stack, c)) {
+    while (closest_step<SPH>(s, stack, c)) {
     }
     return closest_end(c);
 }
@@ -675,6 +700,7 @@ __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min
 // Any hit in [t_min, t_max] (AccelBackend.cpp:114-147). One loop serves both levels, and leaves
 // are tested as soon as they are met so a lane stops at its first hit. Returns 1 occluded,
 // 0 clear, -1 failure.
+template <bool SPH>
 __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
                        TraversalStack& stack) {
     bool failed = false;
@@ -709,6 +735,16 @@ __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
             const uint32_t packed = static_cast<uint32_t>(~child);
             const uint32_t first = packed >> kLeafCountBits;
             const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
+            if (SPH && n == kSphereLeafCount) {
+                const int res = sphere_intersect(s.leaf_tris[3ULL * first], s.leaf_tris[3ULL * first + 1].x, ro, rd,
+                                                 t_min, t_max)
+                                    .outcome;
+                if (res == kSphereHit) {
+                    return 1;
+                }
+                failed = failed || res == kSphereFailure;
+                continue;
+            }
             for (uint32_t j = 0; j < n; ++j) {
                 const uint32_t leaf = first + j;
                 TriangleHit th;
@@ -726,12 +762,23 @@ __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
     return failed ? -1 : 0;
 }
 
-// Barycentrics of the winning triangle (correctly rounded e_i / det).
+// Barycentrics of the winning triangle (correctly rounded e_i / det); for a sphere, its outward
+// object-space normal at the hit.
+template <bool SPH>
 __device__ bool hit_barycentrics(const SceneView& s, const ClosestResult& c, F3 o, F3 d, float t_min, float t_max,
                                  TriangleHit& th) {
     const float4* m = s.inst_to_object + 3ULL * c.instance;
     const F3 lo = xform_point(m, o);
     const F3 ld = xform_vector(m, d);
+    const float4 v1 = s.leaf_tris[3ULL * c.leaf + 1];
+    if (SPH && __float_as_uint(v1.w) == kSphereLeaf) {
+        const SphereHit h = sphere_intersect(s.leaf_tris[3ULL * c.leaf], v1.x, lo, ld, t_min, t_max);
+        th.t = h.t;
+        th.b0 = h.normal.x;
+        th.b1 = h.normal.y;
+        th.b2 = h.normal.z;
+        return h.outcome == kSphereHit && h.t == c.t;
+    }
     const int res = triangle_test(s.leaf_tris[3ULL * c.leaf], s.leaf_tris[3ULL * c.leaf + 1],
                                   s.leaf_tris[3ULL * c.leaf + 2], lo, ld, t_min, t_max, true, th);
     return res == kTriHit && th.t == c.t;
@@ -956,6 +1003,7 @@ __global__ void __launch_bounds__(256) k_regenerate(Wavefront w, PathSource src)
 
 // Finishes one slot's trace: writes the hit (t and the barycentrics of the winning triangle) or
 // the miss or failure, and the slot's shading route.
+template <bool SPH>
 __device__ __forceinline__ void trace_finish(const SceneView& s, const Wavefront& w, uint32_t slot,
                                              const ClosestResult& c, F3 o, F3 d, float t_min, float t_max) {
     if (c.failed) {
@@ -970,7 +1018,7 @@ __device__ __forceinline__ void trace_finish(const SceneView& s, const Wavefront
         return;
     }
     TriangleHit th;
-    if (!hit_barycentrics(s, c, o, d, t_min, t_max, th)) {
+    if (!hit_barycentrics<SPH>(s, c, o, d, t_min, t_max, th)) {
         w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneNumerical;
         w.state[slot] = kSlotDone;
         w.route[slot] = kRouteNone;
@@ -985,6 +1033,7 @@ __device__ __forceinline__ void trace_finish(const SceneView& s, const Wavefront
 // is finished, takes the next slot from a cursor over [0, capacity) (one atomic per warp for all
 // of the warp's idle lanes), so a warp's lanes stay busy instead of waiting for its slowest ray.
 // Slots that are not active are marked unrouted as they are fetched.
+template <bool SPH>
 __global__ void __launch_bounds__(256, BF200_INTERSECT_MIN_BLOCKS) k_trace(SceneView s, Wavefront w) {
     __shared__ int stack_columns[kSharedStackEntries * 256];
     TraversalStack stack = thread_stack(stack_columns);
@@ -1033,8 +1082,8 @@ __global__ void __launch_bounds__(256, BF200_INTERSECT_MIN_BLOCKS) k_trace(Scene
                 atomicAdd(&w.counters[3], static_cast<unsigned long long>(__popc(started)));
             }
         }
-        if (busy && !closest_step(s, stack, c)) {
-            trace_finish(s, w, slot, closest_end(c), c.o, c.d, c.t_min, c.t_max);
+        if (busy && !closest_step<SPH>(s, stack, c)) {
+            trace_finish<SPH>(s, w, slot, closest_end(c), c.o, c.d, c.t_min, c.t_max);
             slot = 0xFFFFFFFFU;
         }
     }
@@ -1049,8 +1098,119 @@ struct Surface {
     Frame frame;
 };
 
+// transform_position_with_error (SurfaceInteraction :135-189): an object-space point with its
+// per-axis error bound into world space; the bound also covers the point's distance from the
+// ray's own hit position.
+__device__ bool transform_position_with_error(const SceneView& s, uint32_t inst, const float (&point)[3],
+                                              const float (&perr)[3], F3 hit_position, Surface& out, Lane& lane) {
+    const float4* mw = s.inst_to_world + 3ULL * inst;
+    const F3 world = xform_point(mw, F3{point[0], point[1], point[2]});
+    const float wv[3] = {world.x, world.y, world.z};
+    const float hv[3] = {hit_position.x, hit_position.y, hit_position.z};
+    const double eps = static_cast<double>(kEps);
+    const double g7 = (7.0 * eps) / (1.0 - 7.0 * eps);
+    float err[3];
+#pragma unroll
+    for (int row = 0; row < 3; ++row) {
+        const float4 r = mw[row];
+        const float rr[4] = {r.x, r.y, r.z, r.w};
+        double magnitude = fabs(static_cast<double>(rr[3]));
+        double propagated = 0.0;
+#pragma unroll
+        for (int col = 0; col < 3; ++col) {
+            const double coefficient = fabs(static_cast<double>(rr[col]));
+            magnitude += coefficient * fabs(static_cast<double>(point[col]));
+            propagated += coefficient * static_cast<double>(perr[col]);
+        }
+        const double discrepancy = fabs(static_cast<double>(wv[row]) - static_cast<double>(hv[row]));
+        const double bound = g7 * magnitude + (1.0 + g7) * propagated + discrepancy;
+        if (!isfinite(bound) || bound < 0.0 || bound > 3.4028234663852886e38) {
+            lane.fail();
+            return false;
+        }
+        err[row] = __double2float_rn(bound);
+        if (static_cast<double>(err[row]) < bound) {
+            err[row] = nextafterf(err[row], kInf);
+        }
+    }
+    out.position = world;
+    out.error = F3{err[0], err[1], err[2]};
+    return true;
+}
+
+// robust_transformed_normal (:252-295): an object-space normal through the inverse transpose, in
+// double, scaled by its largest component and normalised.
+__device__ bool transform_normal(const SceneView& s, uint32_t inst, F3 on, F3& ns, Lane& lane) {
+    const float4* mi = s.inst_to_object + 3ULL * inst;
+    const float4 i0 = mi[0], i1 = mi[1], i2 = mi[2];
+    const double n[3] = {on.x, on.y, on.z};
+    const double tr[3] = {fma(double(i0.x), n[0], fma(double(i1.x), n[1], double(i2.x) * n[2])),
+                          fma(double(i0.y), n[0], fma(double(i1.y), n[1], double(i2.y) * n[2])),
+                          fma(double(i0.z), n[0], fma(double(i1.z), n[1], double(i2.z) * n[2]))};
+    double mc = fabs(tr[0]);
+    mc = mc < fabs(tr[1]) ? fabs(tr[1]) : mc;
+    mc = mc < fabs(tr[2]) ? fabs(tr[2]) : mc;
+    if (!isfinite(mc) || mc == 0.0) {
+        lane.fail();
+        return false;
+    }
+    const double sc[3] = {tr[0] / mc, tr[1] / mc, tr[2] / mc};
+    const double mag = sqrt(fma(sc[0], sc[0], fma(sc[1], sc[1], sc[2] * sc[2])));
+    ns = F3{__double2float_rn(sc[0] / mag), __double2float_rn(sc[1] / mag), __double2float_rn(sc[2] / mag)};
+    return true;
+}
+
+// Surface of an analytic sphere hit (a design of this backend: the reference has no scene-level
+// spheres). The outward normal is robust_outward_normal of the object-space hit point minus the
+// centre, as in Sphere.hpp. The shading point is moved onto the sphere along that normal
+// (centre + r n), so the error of t does not enter the spawn offset; its bound is 7 ulps of
+// |centre| + r per axis. The geometric normal is the world normal through the inverse transpose,
+// and the shading normal equals it.
+__device__ bool resolve_sphere_surface(const SceneView& s, uint32_t inst, const uint4 geom, F3 hit_position,
+                                       uint32_t material, Surface& out, Lane& lane) {
+    const float4 c4 = s.leaf_tris[3ULL * geom.x];
+    const float radius = s.leaf_tris[3ULL * geom.x + 1].x;
+    const float centre[3] = {c4.x, c4.y, c4.z};
+    const F3 local = xform_point(s.inst_to_object + 3ULL * inst, hit_position);
+    F3 n;
+    if (!sphere_outward_normal(local - F3{c4.x, c4.y, c4.z}, n)) {
+        lane.fail();
+        return false;
+    }
+    const float nv[3] = {n.x, n.y, n.z};
+    const float gamma7 = (7.0F * kEps) / (1.0F - 7.0F * kEps);
+    float point[3], perr[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        point[a] = centre[a] + nv[a] * radius;
+        perr[a] = gamma7 * (fabsf(centre[a]) + radius);
+    }
+    if (!transform_position_with_error(s, inst, point, perr, hit_position, out, lane)) {
+        return false;
+    }
+    F3 ng;
+    if (!transform_normal(s, inst, n, ng, lane)) {
+        return false;
+    }
+    out.ng = ng;
+    out.ns = ng;
+    const uint4 minfo = s.material_info[material];
+    if (minfo.y != 0U) {
+        lane.fail(kLaneUnsupported);
+        return false;
+    }
+    out.frame = rotated_about_normal(frame_from_normal(ng, lane), __uint_as_float(minfo.z), lane);
+    return lane.err == 0;
+}
+
 __device__ bool resolve_surface(const SceneView& s, uint32_t inst, uint32_t prim, const float4 tb, F3 hit_position,
                                 uint32_t material, Surface& out, Lane& lane) {
+    {
+        const uint4 geom = s.geom_info[s.inst_info[inst].x];
+        if (geom.w == kGeometrySphere) {
+            return resolve_sphere_surface(s, inst, geom, hit_position, material, out, lane);
+        }
+    }
     const float b0 = tb.y, b1 = tb.z, b2 = tb.w;
     const float tolerance = 32.0F * kEps;
     if (!isfinite(b0) || b0 < -tolerance || b0 > 1.0F + tolerance || !isfinite(b1) || b1 < -tolerance ||
@@ -1094,60 +1254,18 @@ __device__ bool resolve_surface(const SceneView& s, uint32_t inst, uint32_t prim
         const float magnitude = fabsf(q0) + fabsf(q1) + fabsf(q2);
         perr[a] = bf_max(gamma7 * magnitude, floor_error);
     }
-    // transform_position_with_error (:135-189)
-    const float4* mw = s.inst_to_world + 3ULL * inst;
-    const F3 world = xform_point(mw, F3{point[0], point[1], point[2]});
-    const float wv[3] = {world.x, world.y, world.z};
-    const float hv[3] = {hit_position.x, hit_position.y, hit_position.z};
-    const double eps = static_cast<double>(kEps);
-    const double g7 = (7.0 * eps) / (1.0 - 7.0 * eps);
-    float err[3];
-#pragma unroll
-    for (int row = 0; row < 3; ++row) {
-        const float4 r = mw[row];
-        const float rr[4] = {r.x, r.y, r.z, r.w};
-        double magnitude = fabs(static_cast<double>(rr[3]));
-        double propagated = 0.0;
-#pragma unroll
-        for (int col = 0; col < 3; ++col) {
-            const double coefficient = fabs(static_cast<double>(rr[col]));
-            magnitude += coefficient * fabs(static_cast<double>(point[col]));
-            propagated += coefficient * static_cast<double>(perr[col]);
-        }
-        const double discrepancy = fabs(static_cast<double>(wv[row]) - static_cast<double>(hv[row]));
-        const double bound = g7 * magnitude + (1.0 + g7) * propagated + discrepancy;
-        if (!isfinite(bound) || bound < 0.0 || bound > 3.4028234663852886e38) {
-            lane.fail();
-            return false;
-        }
-        err[row] = __double2float_rn(bound);
-        if (static_cast<double>(err[row]) < bound) {
-            err[row] = nextafterf(err[row], kInf);
-        }
+    if (!transform_position_with_error(s, inst, point, perr, hit_position, out, lane)) {
+        return false;
     }
-    out.position = world;
-    out.error = F3{err[0], err[1], err[2]};
     const float4 ngw = s.world_normals[s.inst_normal_offset[inst] + prim];
     out.ng = F3{ngw.x, ngw.y, ngw.z};
     // interpolate_shading_normal (:305-349) with robust_transformed_normal (:252-295)
     const F3 on{fmaf(b0, n0.x, fmaf(b1, n1.x, b2 * n2.x)), fmaf(b0, n0.y, fmaf(b1, n1.y, b2 * n2.y)),
                 fmaf(b0, n0.z, fmaf(b1, n1.z, b2 * n2.z))};
-    const float4* mi = s.inst_to_object + 3ULL * inst;
-    const float4 i0 = mi[0], i1 = mi[1], i2 = mi[2];
-    const double n[3] = {on.x, on.y, on.z};
-    const double tr[3] = {fma(double(i0.x), n[0], fma(double(i1.x), n[1], double(i2.x) * n[2])),
-                          fma(double(i0.y), n[0], fma(double(i1.y), n[1], double(i2.y) * n[2])),
-                          fma(double(i0.z), n[0], fma(double(i1.z), n[1], double(i2.z) * n[2]))};
-    double mc = fabs(tr[0]);
-    mc = mc < fabs(tr[1]) ? fabs(tr[1]) : mc;
-    mc = mc < fabs(tr[2]) ? fabs(tr[2]) : mc;
-    if (!isfinite(mc) || mc == 0.0) {
-        lane.fail();
+    F3 ns;
+    if (!transform_normal(s, inst, on, ns, lane)) {
         return false;
     }
-    const double sc[3] = {tr[0] / mc, tr[1] / mc, tr[2] / mc};
-    const double mag = sqrt(fma(sc[0], sc[0], fma(sc[1], sc[1], sc[2] * sc[2])));
-    F3 ns{__double2float_rn(sc[0] / mag), __double2float_rn(sc[1] / mag), __double2float_rn(sc[2] / mag)};
     if (info.w >> 31) {  // orientation flag precomputed at scene build (transform_orientation)
         ns = -ns;
     }
@@ -1909,7 +2027,7 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
 // k_occlude: shadow rays of the compacted queue; unoccluded contributions join the path radiance
 // ------------------------------------------------------------------------------------------------
 
-template <bool ADJ>
+template <bool ADJ, bool SPH>
 __global__ void __launch_bounds__(256, BF200_OCCLUDE_MIN_BLOCKS) k_occlude(SceneView s, Wavefront w, AdjointView a) {
     __shared__ int stack_columns[kSharedStackEntries * 256];
     __shared__ double adjoint_sum[ADJ ? kAdjointWords : 1];
@@ -1922,7 +2040,7 @@ __global__ void __launch_bounds__(256, BF200_OCCLUDE_MIN_BLOCKS) k_occlude(Scene
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
         const uint32_t slot = w.shadow_queue[i];
         const float4 o = w.shadow_o[slot], d = w.shadow_d[slot];
-        const int occluded = any_hit(s, ld3(o), ld3(d), 0.0F, o.w, w.mask[slot], stack);
+        const int occluded = any_hit<SPH>(s, ld3(o), ld3(d), 0.0F, o.w, w.mask[slot], stack);
         if (occluded < 0) {
             w.status[slot] = (w.status[slot] & ~0xFFU) | kLaneTraversal;
             w.state[slot] = kSlotDone;
@@ -2093,6 +2211,7 @@ __global__ void __launch_bounds__(256) k_adjoint_image(const float4* film32, con
 }
 
 // Standalone closest-hit / occlusion queries (ClosestHit.hpp:21-28, Occlusion.hpp:19-26).
+template <bool SPH>
 __global__ void __launch_bounds__(128) k_query_closest(SceneView s, const bf200_ray_v1* rays, uint64_t n,
                                                       bf200_hit_v1* hits) {
     __shared__ int stack_columns[kSharedStackEntries * 128];
@@ -2101,7 +2220,7 @@ __global__ void __launch_bounds__(128) k_query_closest(SceneView s, const bf200_
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const bf200_ray_v1 r = rays[i];
         const F3 o{r.origin[0], r.origin[1], r.origin[2]}, d{r.direction[0], r.direction[1], r.direction[2]};
-        const ClosestResult c = closest_hit(s, o, d, r.t_min, r.t_max, r.mask, stack);
+        const ClosestResult c = closest_hit<SPH>(s, o, d, r.t_min, r.t_max, r.mask, stack);
         bf200_hit_v1 h;
         h.t = 0.0F;
         h.barycentrics[0] = h.barycentrics[1] = h.barycentrics[2] = 0.0F;
@@ -2111,7 +2230,7 @@ __global__ void __launch_bounds__(128) k_query_closest(SceneView s, const bf200_
         h.reserved = 0U;
         if (!c.failed && c.instance != 0xFFFFFFFFU) {
             TriangleHit th;
-            if (hit_barycentrics(s, c, o, d, r.t_min, r.t_max, th)) {
+            if (hit_barycentrics<SPH>(s, c, o, d, r.t_min, r.t_max, th)) {
                 h.t = c.t;
                 h.barycentrics[0] = th.b0;
                 h.barycentrics[1] = th.b1;
@@ -2126,6 +2245,7 @@ __global__ void __launch_bounds__(128) k_query_closest(SceneView s, const bf200_
     }
 }
 
+template <bool SPH>
 __global__ void __launch_bounds__(128) k_query_occlusion(SceneView s, const bf200_ray_v1* rays, uint64_t n,
                                                         uint32_t* out) {
     __shared__ int stack_columns[kSharedStackEntries * 128];
@@ -2134,7 +2254,7 @@ __global__ void __launch_bounds__(128) k_query_occlusion(SceneView s, const bf20
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const bf200_ray_v1 r = rays[i];
         const F3 o{r.origin[0], r.origin[1], r.origin[2]}, d{r.direction[0], r.direction[1], r.direction[2]};
-        const int occ = any_hit(s, o, d, r.t_min, r.t_max, r.mask, stack);
+        const int occ = any_hit<SPH>(s, o, d, r.t_min, r.t_max, r.mask, stack);
         out[i] = occ < 0 ? 2U : static_cast<uint32_t>(occ);
     }
 }
@@ -2202,7 +2322,11 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
         return cudaGetLastError();
     }
     if (stage == 1) {
-        k_trace<<<grid, 256, 0, stream>>>(s, w);
+        if (s.sphere_count != 0U) {
+            k_trace<true><<<grid, 256, 0, stream>>>(s, w);
+        } else {
+            k_trace<false><<<grid, 256, 0, stream>>>(s, w);
+        }
         *launches += 1U;
         return cudaGetLastError();
     }
@@ -2225,10 +2349,17 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
         return launch_compaction(w.shadow_key, w.capacity, 1U, w.tile_counts, w.shadow_queue, w.shadow_offsets,
                                  w.counters + 0, nullptr, stream, launches);
     }
-    if (adjoint != nullptr) {
-        k_occlude<true><<<grid, 256, 0, stream>>>(s, w, *adjoint);
+    const AdjointView a = adjoint != nullptr ? *adjoint : AdjointView{};
+    if (s.sphere_count != 0U) {
+        if (adjoint != nullptr) {
+            k_occlude<true, true><<<grid, 256, 0, stream>>>(s, w, a);
+        } else {
+            k_occlude<false, true><<<grid, 256, 0, stream>>>(s, w, a);
+        }
+    } else if (adjoint != nullptr) {
+        k_occlude<true, false><<<grid, 256, 0, stream>>>(s, w, a);
     } else {
-        k_occlude<false><<<grid, 256, 0, stream>>>(s, w, AdjointView{});
+        k_occlude<false, false><<<grid, 256, 0, stream>>>(s, w, a);
     }
     *launches += 1U;
     return cudaGetLastError();
@@ -2268,9 +2399,17 @@ cudaError_t launch_queries(const SceneView& s, const bf200_ray_v1* rays, uint64_
     const uint64_t blocks64 = (n + 127U) / 128U;
     const uint32_t blocks = static_cast<uint32_t>(blocks64 < 65535U ? (blocks64 == 0 ? 1 : blocks64) : 65535U);
     if (hits != nullptr) {
-        k_query_closest<<<blocks, 128, 0, stream>>>(s, rays, n, hits);
+        if (s.sphere_count != 0U) {
+            k_query_closest<true><<<blocks, 128, 0, stream>>>(s, rays, n, hits);
+        } else {
+            k_query_closest<false><<<blocks, 128, 0, stream>>>(s, rays, n, hits);
+        }
     } else {
-        k_query_occlusion<<<blocks, 128, 0, stream>>>(s, rays, n, occluded);
+        if (s.sphere_count != 0U) {
+            k_query_occlusion<true><<<blocks, 128, 0, stream>>>(s, rays, n, occluded);
+        } else {
+            k_query_occlusion<false><<<blocks, 128, 0, stream>>>(s, rays, n, occluded);
+        }
     }
     return cudaGetLastError();
 }

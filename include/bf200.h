@@ -214,13 +214,23 @@ typedef struct bf200_material_v1 {
     uint32_t reserved[3];
 } bf200_material_v1;
 
+/* Geometry kinds. A sphere (renderer::SphereT, Sphere.hpp:303-437; FrameScene has no analytic
+ * primitive, so this kind is an addition) is its centre, the geometry's one vertex
+ * (vertex_count = 1, triangle_count = 0), and `radius`, in object space. Its hits are the
+ * reference's exact quadratic roots; closest-hit queries report its outward normal in the
+ * barycentric words. Emissive spheres are refused (no substitution): lights are meshes. */
+#define BF200_GEOMETRY_TRIANGLES 0u
+#define BF200_GEOMETRY_SPHERE 1u
+
 typedef struct bf200_geometry_v1 {
     uint32_t geometry_id;
     uint32_t vertex_offset;
     uint32_t vertex_count;
     uint32_t triangle_offset;
     uint32_t triangle_count;
-    uint32_t reserved[3];
+    uint32_t kind;      /* BF200_GEOMETRY_*; 0 for a triangle mesh */
+    float radius;       /* spheres; 0 for a triangle mesh */
+    uint32_t reserved;
 } bf200_geometry_v1;
 
 /* An instance after hierarchy resolution, in the committed (identifier-sorted) order. The
@@ -547,8 +557,8 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_films_device(bf200_co
  * the weight gradients are compared with finite differences.
  *
  * The film (device, as in bf200_render_film_device) is cleared and holds this call's render on
- * return. Gradients are summed in float64 by atomics in no fixed order, so their last bits vary
- * between calls. At most 64 materials. The report counts the forward render. */
+ * return. The loss and the gradients are summed in float64 by atomics in no fixed order, so their
+ * last bits vary between calls. At most 64 materials. The report counts the forward render. */
 typedef struct bf200_material_gradient_v1 {
     double weight[4];     /* dLoss / d(closure weight of packet lane l) */
     double roughness[2];  /* dLoss / d(alpha_x), dLoss / d(alpha_y); 0 for Lambert */

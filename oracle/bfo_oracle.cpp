@@ -323,6 +323,238 @@ struct Hit {
     V3 position, normal;
 };
 
+// ---------------------------------------------------------------------------------------------
+// Analytic spheres: renderer::SphereT::intersect (Sphere.hpp:321-437) restated in float. The
+// constant term and the discriminant are exact float expansions (add_component :48-81,
+// add_product :83-95, multiply_expansions :109-122); their values are the in-order float sums of
+// the components, the roots q / a and c / q, as in the reference.
+// ---------------------------------------------------------------------------------------------
+
+struct FloatExpansion {
+    float c[128];
+    int n = 0;
+};
+
+bool is_normal_float(float x) { return std::isnormal(x); }
+
+bool fe_add(FloatExpansion& e, float component) {
+    float accumulated = component;
+    int out = 0;
+    const int n = e.n;
+    for (int i = 0; i < n; ++i) {
+        const float existing = e.c[i];
+        const float sum = accumulated + existing;
+        const float existing_from_sum = sum - accumulated;
+        const float accumulated_from_sum = sum - existing_from_sum;
+        const float error = (existing - existing_from_sum) + (accumulated - accumulated_from_sum);
+        if (!std::isfinite(sum) || !std::isfinite(error)) {
+            return false;
+        }
+        if (error != 0.0F) {
+            if (out == 128) {
+                return false;
+            }
+            e.c[out++] = error;
+        }
+        accumulated = sum;
+    }
+    if (accumulated != 0.0F || out == 0) {
+        if (out == 128) {
+            return false;
+        }
+        e.c[out++] = accumulated;
+    }
+    e.n = out;
+    return true;
+}
+
+bool fe_add_product(FloatExpansion& e, float left, float right, float sign = 1.0F) {
+    const float rounded = left * right;
+    const float error = std::fma(left, right, -rounded);
+    if (!std::isfinite(rounded) || !std::isfinite(error) ||
+        (left != 0.0F && right != 0.0F && !is_normal_float(rounded)) ||
+        (error != 0.0F && !is_normal_float(error))) {
+        return false;
+    }
+    return fe_add(e, sign * error) && fe_add(e, sign * rounded);
+}
+
+bool fe_add_expansion(FloatExpansion& destination, const FloatExpansion& source, float sign = 1.0F) {
+    for (int i = 0; i < source.n; ++i) {
+        if (!fe_add(destination, sign * source.c[i])) {
+            return false;
+        }
+    }
+    return true;
+}
+
+bool fe_multiply(const FloatExpansion& left, const FloatExpansion& right, FloatExpansion& product) {
+    product = FloatExpansion{};
+    for (int i = 0; i < left.n; ++i) {
+        for (int j = 0; j < right.n; ++j) {
+            if (!fe_add_product(product, left.c[i], right.c[j])) {
+                return false;
+            }
+        }
+    }
+    return true;
+}
+
+int fe_sign(const FloatExpansion& e) {
+    for (int i = e.n; i > 0; --i) {
+        if (e.c[i - 1] != 0.0F) {
+            return e.c[i - 1] > 0.0F ? 1 : -1;
+        }
+    }
+    return 0;
+}
+
+float fe_value(const FloatExpansion& e) {
+    float value = 0.0F;
+    for (int i = 0; i < e.n; ++i) {
+        value += e.c[i];
+    }
+    return value;
+}
+
+bool fe_squared_norm(V3 v, FloatExpansion& out) {
+    out = FloatExpansion{};
+    return fe_add_product(out, v.x, v.x) && fe_add_product(out, v.y, v.y) && fe_add_product(out, v.z, v.z);
+}
+
+float fused_dot(V3 a, V3 b) { return std::fma(a.x, b.x, std::fma(a.y, b.y, a.z * b.z)); }
+
+// robust_outward_normal (Sphere.hpp:245-267)
+bool sphere_outward_normal(V3 outward, V3& normal) {
+    if (!std::isfinite(outward.x) || !std::isfinite(outward.y) || !std::isfinite(outward.z)) {
+        return false;
+    }
+    const float m = std::max({std::abs(outward.x), std::abs(outward.y), std::abs(outward.z)});
+    if (m == 0.0F) {
+        return false;
+    }
+    const V3 scaled{outward.x / m, outward.y / m, outward.z / m};
+    const float magnitude = std::sqrt(fused_dot(scaled, scaled));
+    if (!std::isfinite(magnitude) || magnitude <= 0.0F) {
+        return false;
+    }
+    normal = V3{scaled.x / magnitude, scaled.y / magnitude, scaled.z / magnitude};
+    return true;
+}
+
+enum class SphereResult { miss, hit, failure };
+
+SphereResult intersect_sphere(V3 centre, float radius, V3 o, V3 d, float t_min, float t_max, float& t_out,
+                              V3& normal) {
+    const V3 rel{o.x - centre.x, o.y - centre.y, o.z - centre.z};
+    if (!std::isfinite(rel.x) || !std::isfinite(rel.y) || !std::isfinite(rel.z)) {
+        return SphereResult::failure;
+    }
+    const float spatial_maximum = std::max({std::abs(rel.x), std::abs(rel.y), std::abs(rel.z), radius});
+    const float direction_maximum = std::max({std::abs(d.x), std::abs(d.y), std::abs(d.z)});
+    int se = 0, de = 0;
+    static_cast<void>(std::frexp(spatial_maximum, &se));
+    static_cast<void>(std::frexp(direction_maximum, &de));
+    const V3 srel{std::ldexp(rel.x, -se), std::ldexp(rel.y, -se), std::ldexp(rel.z, -se)};
+    const V3 sd{std::ldexp(d.x, -de), std::ldexp(d.y, -de), std::ldexp(d.z, -de)};
+    const float sr = std::ldexp(radius, -se);
+    auto preserved = [](float original, float scaled) { return original == 0.0F || std::isnormal(scaled); };
+    if (!std::isfinite(direction_maximum) || direction_maximum <= 0.0F || !preserved(rel.x, srel.x) ||
+        !preserved(rel.y, srel.y) || !preserved(rel.z, srel.z) || !preserved(d.x, sd.x) ||
+        !preserved(d.y, sd.y) || !preserved(d.z, sd.z) || !preserved(radius, sr)) {
+        return SphereResult::failure;
+    }
+    const float a = fused_dot(sd, sd);
+    const float half_b = fused_dot(srel, sd);
+    // exact_quadratic_constant (:147-181)
+    float c = 0.0F;
+    {
+        FloatExpansion origin_squared, radius_squared;
+        if (!fe_squared_norm(srel, origin_squared) || !fe_add_product(radius_squared, sr, sr) ||
+            !fe_add_expansion(origin_squared, radius_squared, -1.0F)) {
+            return SphereResult::failure;
+        }
+        const int sign = fe_sign(origin_squared);
+        if (sign != 0) {
+            c = fe_value(origin_squared);
+            if (!std::isfinite(c) || c == 0.0F || (c > 0.0F ? 1 : -1) != sign) {
+                return SphereResult::failure;
+            }
+        }
+    }
+    // exact_discriminant (:183-243)
+    int disc_sign = 0;
+    float disc = 0.0F;
+    {
+        FloatExpansion direction_squared, radius_squared, radial;
+        if (!fe_squared_norm(sd, direction_squared) || !fe_add_product(radius_squared, sr, sr) ||
+            !fe_multiply(direction_squared, radius_squared, radial)) {
+            return SphereResult::failure;
+        }
+        const float terms[3][4] = {{srel.y, sd.z, srel.z, sd.y}, {srel.z, sd.x, srel.x, sd.z},
+                                   {srel.x, sd.y, srel.y, sd.x}};
+        FloatExpansion perpendicular;
+        for (const auto& t : terms) {
+            FloatExpansion cross, cross_squared;
+            if (!fe_add_product(cross, t[0], t[1]) || !fe_add_product(cross, t[2], t[3], -1.0F) ||
+                !fe_multiply(cross, cross, cross_squared) || !fe_add_expansion(perpendicular, cross_squared)) {
+                return SphereResult::failure;
+            }
+        }
+        if (!fe_add_expansion(radial, perpendicular, -1.0F)) {
+            return SphereResult::failure;
+        }
+        disc_sign = fe_sign(radial);
+        if (disc_sign > 0) {
+            disc = fe_value(radial);
+            if (!std::isfinite(disc) || disc <= 0.0F) {
+                return SphereResult::failure;
+            }
+        }
+    }
+    if (!std::isfinite(a) || !std::isfinite(half_b) || !std::isfinite(c) || a <= 0.0F || sr <= 0.0F) {
+        return SphereResult::failure;
+    }
+    if (disc_sign < 0) {
+        return SphereResult::miss;
+    }
+    float r0, r1;
+    if (disc_sign == 0) {
+        r0 = -half_b / a;
+        r1 = r0;
+    } else {
+        const float root = std::sqrt(disc);
+        const float q = -half_b - std::copysign(root, half_b);
+        if (!std::isfinite(root) || !std::isfinite(q) || q == 0.0F) {
+            return SphereResult::failure;
+        }
+        r0 = q / a;
+        r1 = c / q;
+        if (r0 > r1) {
+            std::swap(r0, r1);
+        }
+    }
+    const float t0 = std::ldexp(r0, se - de), t1 = std::ldexp(r1, se - de);
+    if (!std::isfinite(t0) || !std::isfinite(t1) || (r0 != 0.0F && t0 == 0.0F) || (r1 != 0.0F && t1 == 0.0F)) {
+        return SphereResult::failure;
+    }
+    float t;
+    if (!std::isnan(t0) && t0 >= t_min && t0 <= t_max) {
+        t = t0;
+    } else if (!std::isnan(t1) && t1 >= t_min && t1 <= t_max) {
+        t = t1;
+    } else {
+        return SphereResult::miss;
+    }
+    const V3 position = o + d * t;  // Ray::at (Ray.hpp:81-95)
+    if (!std::isfinite(position.x) || !std::isfinite(position.y) || !std::isfinite(position.z) ||
+        !sphere_outward_normal(V3{position.x - centre.x, position.y - centre.y, position.z - centre.z}, normal)) {
+        return SphereResult::failure;
+    }
+    t_out = t;
+    return SphereResult::hit;
+}
+
 // Conservative double prefilter: true only when the three edge functions certainly have mixed
 // signs, in which case the exact test is certain to report a miss (or a coplanar skip).
 bool certainly_missed(V3 v0, V3 v1, V3 v2, V3 o, V3 d) {
@@ -367,6 +599,27 @@ bool closest_hit(const Scene& scene, V3 origin, V3 dir, float t_min, float t_max
         const V3 lo = transform_point(inst.to_object, origin);
         const V3 ld = transform_vector(inst.to_object, dir);
         const auto& g = scene.geometries[inst.geometry];
+        if (g.kind == BF200_GEOMETRY_SPHERE) {
+            float t = 0.0F;
+            V3 n{};
+            const SphereResult r = intersect_sphere(scene.positions[g.vertex_offset], g.radius, lo, ld, t_min,
+                                                    found ? best.t : t_max, t, n);
+            if (r == SphereResult::failure) {
+                fail("A sphere intersection is not representable.");
+            }
+            if (r != SphereResult::hit || (found && best.t <= t)) {
+                continue;
+            }
+            best.t = t;
+            best.b0 = n.x;  // the object-space outward normal
+            best.b1 = n.y;
+            best.b2 = n.z;
+            best.instance = i;
+            best.primitive = 0;
+            best.position = origin + dir * t;  // Ray::at (Ray.hpp:81-95)
+            found = true;
+            continue;
+        }
         for (uint32_t t = 0; t < g.triangle_count; ++t) {
             const uint32_t* tri = &scene.triangles[3 * (g.triangle_offset + t)];
             const V3 v0 = scene.positions[g.vertex_offset + tri[0]];
@@ -409,6 +662,19 @@ bool occluded(const Scene& scene, V3 origin, V3 dir, float t_min, float t_max, u
         const V3 lo = transform_point(inst.to_object, origin);
         const V3 ld = transform_vector(inst.to_object, dir);
         const auto& g = scene.geometries[inst.geometry];
+        if (g.kind == BF200_GEOMETRY_SPHERE) {
+            float t = 0.0F;
+            V3 n{};
+            const SphereResult r =
+                intersect_sphere(scene.positions[g.vertex_offset], g.radius, lo, ld, t_min, t_max, t, n);
+            if (r == SphereResult::failure) {
+                fail("A sphere intersection is not representable.");
+            }
+            if (r == SphereResult::hit) {
+                return true;
+            }
+            continue;
+        }
         for (uint32_t t = 0; t < g.triangle_count; ++t) {
             const uint32_t* tri = &scene.triangles[3 * (g.triangle_offset + t)];
             const V3 v0 = scene.positions[g.vertex_offset + tri[0]];
@@ -1843,11 +2109,84 @@ struct Surface {
     const Material* material;
 };
 
+// Surface of an analytic sphere hit, the backend's design (the reference has no scene-level
+// spheres): the outward normal of the object-space hit point (robust_outward_normal), the point
+// moved onto the sphere along it with a 7-ulp bound of |centre| + r per axis, carried into world
+// space as transform_position_with_error does; geometric normal = shading normal = the world
+// normal through the inverse transpose (robust_transformed_normal).
+Surface resolve_sphere_surface(const Scene& scene, const Instance& inst, const bf200_geometry_v1& g, const Hit& hit,
+                               Surface s) {
+    const V3 centre = scene.positions[g.vertex_offset];
+    const float radius = g.radius;
+    const V3 local = transform_point(inst.to_object, hit.position);
+    V3 n{};
+    if (!sphere_outward_normal(V3{local.x - centre.x, local.y - centre.y, local.z - centre.z}, n)) {
+        fail("A sphere hit normal is not representable.");
+    }
+    constexpr float gamma7 = (7.0F * kEpsilon) / (1.0F - 7.0F * kEpsilon);
+    const float c[3] = {centre.x, centre.y, centre.z}, nv[3] = {n.x, n.y, n.z};
+    float point[3], perr[3];
+    for (int a = 0; a < 3; ++a) {
+        point[a] = c[a] + nv[a] * radius;
+        perr[a] = gamma7 * (std::abs(c[a]) + radius);
+    }
+    const V3 world = transform_point(inst.to_world, V3{point[0], point[1], point[2]});
+    const float w[3] = {world.x, world.y, world.z};
+    const float h[3] = {hit.position.x, hit.position.y, hit.position.z};
+    constexpr double eps = static_cast<double>(kEpsilon);
+    constexpr double g7 = (7.0 * eps) / (1.0 - 7.0 * eps);
+    float err[3];
+    for (int row = 0; row < 3; ++row) {
+        double magnitude = std::abs(static_cast<double>(inst.to_world(row, 3)));
+        double propagated = 0.0;
+        for (int col = 0; col < 3; ++col) {
+            const double coefficient = std::abs(static_cast<double>(inst.to_world(row, col)));
+            magnitude += coefficient * std::abs(static_cast<double>(point[col]));
+            propagated += coefficient * static_cast<double>(perr[col]);
+        }
+        const double discrepancy = std::abs(static_cast<double>(w[row]) - static_cast<double>(h[row]));
+        const double bound = g7 * magnitude + (1.0 + g7) * propagated + discrepancy;
+        if (!std::isfinite(bound) || bound < 0.0 || bound > static_cast<double>(std::numeric_limits<float>::max())) {
+            fail("A transformed sphere position error is not representable.");
+        }
+        err[row] = static_cast<float>(bound);
+        if (static_cast<double>(err[row]) < bound) {
+            err[row] = std::nextafter(err[row], kInfinity);
+        }
+    }
+    s.position = world;
+    s.error = V3{err[0], err[1], err[2]};
+    const Mat4& inv = inst.to_object;
+    const double nd[3] = {n.x, n.y, n.z};
+    const double tr[3] = {
+        std::fma(double(inv(0, 0)), nd[0], std::fma(double(inv(1, 0)), nd[1], double(inv(2, 0)) * nd[2])),
+        std::fma(double(inv(0, 1)), nd[0], std::fma(double(inv(1, 1)), nd[1], double(inv(2, 1)) * nd[2])),
+        std::fma(double(inv(0, 2)), nd[0], std::fma(double(inv(1, 2)), nd[1], double(inv(2, 2)) * nd[2]))};
+    const double mc = std::max({std::abs(tr[0]), std::abs(tr[1]), std::abs(tr[2])});
+    if (!std::isfinite(mc) || mc == 0.0) {
+        fail("A sphere normal cannot be normalized.");
+    }
+    const double sc[3] = {tr[0] / mc, tr[1] / mc, tr[2] / mc};
+    const double magnitude = std::sqrt(std::fma(sc[0], sc[0], std::fma(sc[1], sc[1], sc[2] * sc[2])));
+    const V3 ng{static_cast<float>(sc[0] / magnitude), static_cast<float>(sc[1] / magnitude),
+                static_cast<float>(sc[2] / magnitude)};
+    s.ng = ng;
+    s.ns = ng;
+    if (s.material->frame_mode != 0) {
+        fail("surface-tangent closure frames are not part of this restatement");
+    }
+    s.frame = rotated_about_normal(frame_from_normal(ng), s.material->rotation);
+    return s;
+}
+
 Surface resolve_surface(const Scene& scene, const Hit& hit) {
     Surface s{};
     const Instance& inst = scene.instances[hit.instance];
     const auto& g = scene.geometries[inst.geometry];
     s.material = &scene.materials[inst.material];
+    if (g.kind == BF200_GEOMETRY_SPHERE) {
+        return resolve_sphere_surface(scene, inst, g, hit, s);
+    }
     // validate_barycentrics (:54-76)
     constexpr float tolerance = 32.0F * kEpsilon;
     const float bs[3] = {hit.b0, hit.b1, hit.b2};
@@ -2513,6 +2852,11 @@ __attribute__((visibility("default"))) int bfo_scene_create(const bf200_scene_de
             if (is_black(mat.emission)) {
                 continue;
             }
+            if (s->geometries[s->instances[i].geometry].kind == BF200_GEOMETRY_SPHERE) {
+                set_error("emissive analytic spheres are not supported: lights are meshes");
+                delete s;
+                return 3;
+            }
             MeshLight light{};
             light.instance = i;
             if (!transform_mesh_positions(*s, s->instances[i], light)) {
@@ -2704,6 +3048,46 @@ __attribute__((visibility("default"))) uint64_t bfo_owen_sobol_bits(uint32_t px,
 // Float32 or Neumaier float64 film of the caller-side path: CIE XYZ (Cie1931Sensor.cpp:104-176),
 // linear sRGB (Color.hpp:77-88), add_sample(x, y, rgb, 1) (Film.hpp:150-182). `sums` holds
 // (r, g, b, weight) per pixel as double; for precision 1 also the compensations are applied.
+// intersect_sphere on ray k against sphere k (centre xyz, radius), in world space. Per ray, out
+// receives 8 floats: status (0 miss, 1 hit, 2 not representable), t, outward normal xyz, position xyz.
+__attribute__((visibility("default"))) int bfo_sphere_intersect(const float* spheres, const bf200_ray_v1* rays,
+                                                                uint64_t count, float* out) {
+    for (uint64_t k = 0; k < count; ++k) {
+        float* o = out + 8 * k;
+        for (int i = 0; i < 8; ++i) {
+            o[i] = 0.0F;
+        }
+        const float* sp = spheres + 4 * k;
+        const auto& r = rays[k];
+        const V3 origin{r.origin[0], r.origin[1], r.origin[2]}, dir{r.direction[0], r.direction[1], r.direction[2]};
+        if (!std::isfinite(sp[0]) || !std::isfinite(sp[1]) || !std::isfinite(sp[2]) || !std::isfinite(sp[3]) ||
+            sp[3] <= 0.0F) {
+            o[0] = 2.0F;
+            continue;
+        }
+        float t = 0.0F;
+        V3 n{};
+        const SphereResult res = intersect_sphere(V3{sp[0], sp[1], sp[2]}, sp[3], origin, dir, r.t_min, r.t_max, t, n);
+        if (res == SphereResult::failure) {
+            o[0] = 2.0F;
+            continue;
+        }
+        if (res == SphereResult::miss) {
+            continue;
+        }
+        const V3 p = origin + dir * t;
+        o[0] = 1.0F;
+        o[1] = t;
+        o[2] = n.x;
+        o[3] = n.y;
+        o[4] = n.z;
+        o[5] = p.x;
+        o[6] = p.y;
+        o[7] = p.z;
+    }
+    return 0;
+}
+
 __attribute__((visibility("default"))) int bfo_film_accumulate(const float* radiance,
                                                                const bf200_sample_index_v1* samples,
                                                                uint64_t n, const bf200_sensor_v1* sensor,

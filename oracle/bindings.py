@@ -58,6 +58,18 @@ class _Checker:
     def destroy(self, handle):
         getattr(self.lib, self.prefix + "_scene_destroy")(handle)
 
+    def sphere_intersect(self, spheres, rays):
+        """Ray k against sphere k (centre xyz, radius): float32 [n, 8] of status (0 miss, 1 hit,
+        2 not representable), t, outward normal xyz, position xyz."""
+        import numpy as np
+        spheres = np.ascontiguousarray(spheres, np.float32).reshape(-1, 4)
+        out = np.zeros((len(rays), 8), np.float32)
+        f = getattr(self.lib, self.prefix + "_sphere_intersect")
+        f.argtypes = [C.c_void_p, C.POINTER(abi.Ray), C.c_uint64, C.c_void_p]
+        f.restype = C.c_int
+        f(spheres.ctypes.data_as(C.c_void_p), rays, len(rays), out.ctypes.data_as(C.c_void_p))
+        return out
+
     def trace(self, handle, inputs, options, threads=None):
         n = len(inputs)
         results = (abi.PathResult * n)()

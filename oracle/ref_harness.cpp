@@ -30,6 +30,7 @@
 #include <Blackframe/Renderer/LightSampler.hpp>
 #include <Blackframe/Renderer/OwenScrambling.hpp>
 #include <Blackframe/Renderer/PinholeCamera.hpp>
+#include <Blackframe/Renderer/Sphere.hpp>
 #include <Blackframe/Renderer/WavelengthSampling.hpp>
 
 #include <atomic>
@@ -496,6 +497,48 @@ __attribute__((visibility("default"))) int bfr_sensor(const float* nm, const flo
     }
     constexpr auto inverse_lane_count = 1.0F / 4.0F;
     out->normalization = inverse_lane_count / static_cast<float>(renderer::Cie1931YIntegralNanometers);
+    return 0;
+}
+
+// renderer::Sphere (float) on ray k against sphere k (centre xyz, radius). Per ray, out receives
+// 8 floats: status (0 miss, 1 hit, 2 the reference reported an error), t, outward normal xyz,
+// hit position xyz.
+__attribute__((visibility("default"))) int
+bfr_sphere_intersect(const float* spheres, const bf200_ray_v1* rays, uint64_t count, float* out) {
+    for (uint64_t k = 0; k < count; ++k) {
+        float* o = out + 8 * k;
+        for (int i = 0; i < 8; ++i) {
+            o[i] = 0.0F;
+        }
+        const float* sp = spheres + 4 * k;
+        const auto sphere = renderer::Sphere::create(renderer::Point3{.x = sp[0], .y = sp[1], .z = sp[2]}, sp[3]);
+        const auto& r = rays[k];
+        const auto ray = renderer::Ray::create(
+            renderer::Point3{.x = r.origin[0], .y = r.origin[1], .z = r.origin[2]},
+            renderer::Vector3{.x = r.direction[0], .y = r.direction[1], .z = r.direction[2]}, r.t_min, r.t_max,
+            r.time, r.mask, renderer::MediumId{.value = r.medium});
+        if (!sphere.has_value() || !ray.has_value()) {
+            o[0] = 2.0F;
+            continue;
+        }
+        const auto hit = sphere->intersect(*ray);
+        if (!hit.has_value()) {
+            o[0] = 2.0F;
+            continue;
+        }
+        if (!hit->has_value()) {
+            continue;
+        }
+        const auto& h = **hit;
+        o[0] = 1.0F;
+        o[1] = h.parameter;
+        o[2] = h.geometric_normal.x;
+        o[3] = h.geometric_normal.y;
+        o[4] = h.geometric_normal.z;
+        o[5] = h.position.x;
+        o[6] = h.position.y;
+        o[7] = h.position.z;
+    }
     return 0;
 }
 

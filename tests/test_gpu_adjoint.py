@@ -284,7 +284,9 @@ def test_film_is_the_calls_render(setup):
     _, _, builder, _, _, _ = setup
     first = gpu_adjoint(setup, builder)
     second = gpu_adjoint(setup, builder)
-    assert np.array_equal(first[3], second[3]) and first[0] == second[0]
+    # the film is bit-identical; the loss and the gradients are float64 sums by atomics in no
+    # fixed order
+    assert np.array_equal(first[3], second[3]) and abs(first[0] - second[0]) <= 1e-12 * abs(first[0])
     assert np.allclose(first[1], second[1], rtol=1e-9, atol=0.0)
 
 
