@@ -186,6 +186,100 @@ __device__ bool sphere_discriminant(F3 rel, F3 d, float radius, int& sign, float
 
 __device__ __forceinline__ float fused_dot3(F3 a, F3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
 
+// ------------------------------------------------------------------------------------------------
+// Fast path for the two expansion values. Two facts make it exact:
+// * With every scaled input component 0 or of magnitude >= 2^-8 (least significant bit
+//   >= 2^-31), every nonzero product and product error the expansions form is a multiple of at
+//   least 2^-124, so none is subnormal and the reference's representability checks all pass.
+// * Summing a nonoverlapping expansion from its smallest component up, as the reference does,
+//   lands within about 2 u_f ulp of its exact value X (u_f = 2^-24). So when X lies farther than
+//   2^-12 ulp from every float rounding boundary, that sum is the float nearest to X.
+// X is evaluated in double-double with an error bound; anything uncertain takes the expansions.
+// ------------------------------------------------------------------------------------------------
+
+struct DoubleDouble {
+    double hi, lo;
+};
+
+__device__ __forceinline__ DoubleDouble dd_two_sum(double a, double b) {
+    const double s = a + b;
+    const double bb = s - a;
+    return {s, (a - (s - bb)) + (b - bb)};
+}
+
+__device__ __forceinline__ DoubleDouble dd_add(DoubleDouble x, DoubleDouble y) {
+    DoubleDouble s = dd_two_sum(x.hi, y.hi);
+    s.lo += x.lo + y.lo;
+    return dd_two_sum(s.hi, s.lo);
+}
+
+__device__ __forceinline__ DoubleDouble dd_square(DoubleDouble x) {
+    const double p = x.hi * x.hi;
+    const double e = fma(x.hi, x.hi, -p) + (2.0 * x.hi * x.lo + x.lo * x.lo);
+    return dd_two_sum(p, e);
+}
+
+__device__ __forceinline__ DoubleDouble dd_scale(DoubleDouble x, double y) {
+    const double p = x.hi * y;
+    const double e = fma(x.hi, y, -p) + x.lo * y;
+    return dd_two_sum(p, e);
+}
+
+__device__ __forceinline__ bool coarse_component(float x) { return x == 0.0F || fabsf(x) >= 0.00390625F; }
+
+// The float nearest to X = x.hi + x.lo (known to within err) when X is certainly farther than
+// 2^-12 ulp from each rounding boundary of that float; false otherwise.
+__device__ __forceinline__ bool certified_nearest(DoubleDouble x, double err, float& out) {
+    const float f = __double2float_rn(x.hi);
+    if (!isfinite(f) || fabsf(f) < 1.17549435e-38F) {
+        return false;
+    }
+    const double fd = f;
+    const double up = static_cast<double>(nextafterf(f, kInf)) - fd;
+    const double down = fd - static_cast<double>(nextafterf(f, -kInf));
+    const double dist = (x.hi - fd) + x.lo;
+    const double margin = 0x1p-12;
+    if (dist + err + margin * up < 0.5 * up && err - dist + margin * down < 0.5 * down) {
+        out = f;
+        return true;
+    }
+    return false;
+}
+
+// c = |rel|^2 - r^2 and the discriminant |d|^2 r^2 - |rel x d|^2 of the scaled inputs by the fast
+// path; false when the fast path is not certain (the expansions then decide).
+__device__ __forceinline__ bool sphere_values_fast(F3 srel, F3 sd, float sr, float& c, int& disc_sign, float& disc) {
+    if (!coarse_component(srel.x) || !coarse_component(srel.y) || !coarse_component(srel.z) ||
+        !coarse_component(sd.x) || !coarse_component(sd.y) || !coarse_component(sd.z) || !coarse_component(sr)) {
+        return false;
+    }
+    const double rx = srel.x, ry = srel.y, rz = srel.z, dx = sd.x, dy = sd.y, dz = sd.z, r2 = double(sr) * sr;
+    const double ox2 = rx * rx, oy2 = ry * ry, oz2 = rz * rz;
+    const DoubleDouble cc = dd_add(dd_add(dd_two_sum(ox2, oy2), DoubleDouble{oz2, 0.0}), DoubleDouble{-r2, 0.0});
+    const double c_err = 0x1p-100 * (ox2 + oy2 + oz2 + r2);
+    if (!(fabs(cc.hi) > 2.0 * c_err) || !certified_nearest(cc, c_err, c)) {
+        return false;
+    }
+    const DoubleDouble dir2 = dd_add(dd_two_sum(dx * dx, dy * dy), DoubleDouble{dz * dz, 0.0});
+    const DoubleDouble radial = dd_scale(dir2, r2);
+    const DoubleDouble cx = dd_two_sum(ry * dz, -(rz * dy));
+    const DoubleDouble cy = dd_two_sum(rz * dx, -(rx * dz));
+    const DoubleDouble cz = dd_two_sum(rx * dy, -(ry * dx));
+    const DoubleDouble perpendicular = dd_add(dd_add(dd_square(cx), dd_square(cy)), dd_square(cz));
+    const DoubleDouble x = dd_add(radial, DoubleDouble{-perpendicular.hi, -perpendicular.lo});
+    const double err = 0x1p-98 * (fabs(radial.hi) + fabs(perpendicular.hi));
+    if (x.hi < -2.0 * err) {
+        disc_sign = -1;
+        disc = 0.0F;
+        return true;
+    }
+    if (!(x.hi > 2.0 * err)) {
+        return false;
+    }
+    disc_sign = 1;
+    return certified_nearest(x, err, disc);
+}
+
 // robust_outward_normal (Sphere.hpp:245-267)
 __device__ __forceinline__ bool sphere_outward_normal(F3 outward, F3& normal) {
     if (!finite3(outward)) {
@@ -257,13 +351,15 @@ __device__ __noinline__ SphereHit sphere_intersect(float4 centre4, float radius,
     const float a = fused_dot3(sd, sd);
     const float half_b = fused_dot3(srel, sd);
     float c = 0.0F;
-    if (!sphere_constant(srel, sr, c)) {
-        return SphereHit{kSphereFailure, 0.0F, F3{0.0F, 0.0F, 0.0F}};
-    }
     int disc_sign = 0;
     float disc = 0.0F;
-    if (!sphere_discriminant(srel, sd, sr, disc_sign, disc)) {
-        return SphereHit{kSphereFailure, 0.0F, F3{0.0F, 0.0F, 0.0F}};
+    if (!sphere_values_fast(srel, sd, sr, c, disc_sign, disc)) {
+        if (!sphere_constant(srel, sr, c)) {
+            return SphereHit{kSphereFailure, 0.0F, F3{0.0F, 0.0F, 0.0F}};
+        }
+        if (!sphere_discriminant(srel, sd, sr, disc_sign, disc)) {
+            return SphereHit{kSphereFailure, 0.0F, F3{0.0F, 0.0F, 0.0F}};
+        }
     }
     if (!isfinite(a) || !isfinite(half_b) || !isfinite(c) || a <= 0.0F || sr <= 0.0F) {
         return SphereHit{kSphereFailure, 0.0F, F3{0.0F, 0.0F, 0.0F}};
