@@ -356,6 +356,58 @@ def run_adjoint(args, torch, rank):
     print(json.dumps(line), flush=True)
 
 
+IMPORT_WORKLOAD = "mesh_import_obj"
+
+
+def run_mesh_import(args):
+    """Scene ingestion: bf200_mesh_load on a seeded 327,680-triangle OBJ (a displaced subdivision-7
+    icosphere written with 9 significant digits, about 37 MB), beside the reference's own loader
+    (oracle/_ref) on the same file. Host code on both sides; the arrays must be identical."""
+    import tempfile
+    v, f = scenes.icosphere(7)
+    rng = np.random.default_rng(1)
+    p = v * (1.0 + 0.02 * rng.uniform(-1.0, 1.0, len(v)))[:, None]
+    n = (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+    uv = rng.uniform(0.0, 1.0, (len(v), 2))
+    lines = ["v %.9g %.9g %.9g" % tuple(r) for r in p] + ["vt %.9g %.9g" % tuple(r) for r in uv]
+    lines += ["vn %.9g %.9g %.9g" % tuple(map(float, r)) for r in n]
+    lines += ["f %d/%d/%d %d/%d/%d %d/%d/%d" % (a + 1, a + 1, a + 1, b + 1, b + 1, b + 1, c + 1, c + 1, c + 1)
+              for a, b, c in f]
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "icosphere7.obj")
+        with open(path, "w") as handle:
+            handle.write("\n".join(lines) + "\n")
+        size = os.path.getsize(path)
+        for _ in range(args.warmup):
+            runtime.load_mesh(path)
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            mesh = runtime.load_mesh(path)
+            times.append(time.perf_counter() - t0)
+        reference = None
+        from oracle.bindings import Reference, reference_available
+        if reference_available():
+            ref = Reference()
+            ref_times = []
+            for _ in range(max(1, args.steps)):
+                t0 = time.perf_counter()
+                want, _, _ = ref.load_mesh(path)
+                ref_times.append(time.perf_counter() - t0)
+            same = all(np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
+                       for a, b in zip(mesh, want))
+            reference = {"value": len(f) / statistics.median(ref_times), "seconds": statistics.median(ref_times),
+                         "identical_arrays": same, "kind": "reference"}
+    seconds = statistics.median(times)
+    line = {"metric": "imported triangles/s", "value": len(f) / seconds, "unit": "triangles/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": seconds * 1000.0, "higher_is_better": True,
+            "scaling": "none", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": IMPORT_WORKLOAD, "triangles": len(f), "vertices": len(v), "bytes": size,
+                       "host": "one thread"},
+            "mb_per_s": size / seconds / 1e6, "reference_loader": reference, "gpu_launches": 0}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -390,10 +442,11 @@ def main():
     parser.add_argument("--reference-seconds", type=float, default=8.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's)")
-    parser.add_argument("--workload", default=WORKLOAD, choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD],
+    parser.add_argument("--workload", default=WORKLOAD,
+                        choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD, IMPORT_WORKLOAD],
                         help="scene and frame (default: the headline Cornell + spheres frame); "
                              f"{BATCH_WORKLOAD}: the 64-scene batch against 64 serial renders; "
-                             f"{ADJOINT_WORKLOAD}: the path-replay adjoint")
+                             f"{ADJOINT_WORKLOAD}: the path-replay adjoint; {IMPORT_WORKLOAD}: OBJ ingestion")
     parser.add_argument("--lanes", type=int, default=0, help="batch lanes (0: autotuned)")
     args = parser.parse_args()
 
@@ -403,6 +456,10 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.workload == IMPORT_WORKLOAD:
+        if rank == 0:
+            run_mesh_import(args)
         return
 
     import torch

@@ -158,6 +158,12 @@ class FilmJob(C.Structure):
                 ("report", C.c_void_p)]
 
 
+class MeshView(C.Structure):
+    _fields_ = [("struct_size", u32), ("vertex_count", u32), ("triangle_count", u32), ("reserved", u32),
+                ("positions", C.POINTER(C.c_float)), ("normals", C.POINTER(C.c_float)),
+                ("texture_coordinates", C.POINTER(C.c_float)), ("triangles", C.POINTER(u32))]
+
+
 class MaterialGradient(C.Structure):
     _fields_ = [("weight", C.c_double * 4), ("roughness", C.c_double * 2), ("reserved", C.c_double * 2)]
 
@@ -186,7 +192,7 @@ class Hit(C.Structure):
 EXPECTED_SIZES = {
     Closure: 64, Material: 80, Geometry: 32, Instance: 160, Ray: 48, SampleIndex: 24,
     PathInput: 80, PathResult: 128, TransportOptions: 64, Camera: 88, Sensor: 80,
-    FilmRequest: 40, FilmJob: 64, MaterialGradient: 64, Adjoint: 40, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
+    FilmRequest: 40, FilmJob: 64, MeshView: 48, MaterialGradient: 64, Adjoint: 40, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,
 }
 
 

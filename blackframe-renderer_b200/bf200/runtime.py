@@ -26,6 +26,9 @@ EXPORTED_SYMBOLS = [
     "bf200_render_films_device",
     "bf200_render_adjoint_device",
     "bf200_render_backward_device",
+    "bf200_mesh_load",
+    "bf200_mesh_view",
+    "bf200_mesh_destroy",
 ]
 
 
@@ -83,6 +86,12 @@ def library():
                                                  C.POINTER(abi.FilmRequest), C.POINTER(abi.TransportOptions),
                                                  C.POINTER(abi.Film), vp, vp, vp, C.POINTER(abi.Report)]
     lib.bf200_render_backward_device.restype = C.c_uint32
+    lib.bf200_mesh_load.argtypes = [C.c_char_p, C.POINTER(vp), C.c_char_p, C.c_uint64]
+    lib.bf200_mesh_load.restype = C.c_uint32
+    lib.bf200_mesh_view.argtypes = [vp, C.POINTER(abi.MeshView)]
+    lib.bf200_mesh_view.restype = C.c_uint32
+    lib.bf200_mesh_destroy.argtypes = [vp]
+    lib.bf200_mesh_destroy.restype = None
     lib.bf200_sobol_bits.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
     lib.bf200_sobol_bits.restype = C.c_uint32
     lib.bf200_owen_sobol_bits.argtypes = [C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(C.c_uint64)]
@@ -287,6 +296,28 @@ class Context:
         self._check(library().bf200_occlusions(self.handle, scene.handle, C.cast(rays, C.c_void_p), n,
                                                out.ctypes.data_as(C.c_void_p)), "occlusions")
         return out
+
+
+def load_mesh(path):
+    """bf200_mesh_load: an OBJ or ASCII PLY file as (positions [V, 3], normals [V, 3], texture
+    coordinates [V, 2], triangles [T, 3]) numpy arrays; raises Bf200Error when the file is refused."""
+    lib = library()
+    handle = C.c_void_p()
+    message = C.create_string_buffer(512)
+    status = lib.bf200_mesh_load(os.fsencode(path), C.byref(handle), message, len(message))
+    if status != 0:
+        raise Bf200Error(status, message.value.decode(errors="replace"))
+    try:
+        view = abi.MeshView()
+        view.struct_size = C.sizeof(abi.MeshView)
+        lib.bf200_mesh_view(handle, C.byref(view))
+        nv, nt = view.vertex_count, view.triangle_count
+        return (np.ctypeslib.as_array(view.positions, (nv, 3)).copy(),
+                np.ctypeslib.as_array(view.normals, (nv, 3)).copy(),
+                np.ctypeslib.as_array(view.texture_coordinates, (nv, 2)).copy(),
+                np.ctypeslib.as_array(view.triangles, (nt, 3)).copy())
+    finally:
+        lib.bf200_mesh_destroy(handle)
 
 
 def camera_create(origin, normal, tangent_seed, width, height, vfov, time=0.5, jitter=1):

@@ -592,6 +592,33 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_backward_device(
     const bf200_transport_options_v1* options, const bf200_film_v1* film, const float* image_adjoint,
     bf200_material_gradient_v1* gradients, double* emission_gradient, bf200_report_v1* report) BF200_NOEXCEPT;
 
+/* Triangle-mesh import for callers that hold meshes as OBJ or ASCII PLY files
+ * (engine::load_obj_triangle_mesh / load_ply_triangle_mesh, TriangleMeshImport.hpp:9-17): the
+ * same files are accepted and refused, and an accepted file gives the same aligned arrays (one
+ * vertex per distinct OBJ v/vt/vn corner, in order of first use). The path must be absolute and end
+ * in ".obj" or ".ply". On failure `message` (when given) receives the reason. The mesh is host
+ * memory owned by the library until bf200_mesh_destroy; its arrays fill one geometry of a
+ * bf200_scene_desc_v1. Host code only: no GPU is needed. */
+typedef struct bf200_mesh bf200_mesh;
+
+typedef struct bf200_mesh_view_v1 {
+    uint32_t struct_size;
+    uint32_t vertex_count;
+    uint32_t triangle_count;
+    uint32_t reserved;
+    const float* positions;           /* 3 per vertex */
+    const float* normals;             /* 3 per vertex, unit length */
+    const float* texture_coordinates; /* 2 per vertex */
+    const uint32_t* triangles;        /* 3 per triangle */
+} bf200_mesh_view_v1;
+
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_mesh_load(const char* absolute_path, bf200_mesh** mesh,
+                                                              char* message, uint64_t message_capacity)
+    BF200_NOEXCEPT;
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_mesh_view(const bf200_mesh* mesh, bf200_mesh_view_v1* view)
+    BF200_NOEXCEPT;
+BF200_EXTERN_C BF200_EXPORT void bf200_mesh_destroy(bf200_mesh* mesh) BF200_NOEXCEPT;
+
 /* Closest-hit query for a batch of world rays (trace_cuda_closest_hits, ClosestHit.hpp:21-28).
  * Per ray writes t, barycentrics b0..b2, instance index and primitive index (0xffffffff on a
  * miss). Host pointers. */

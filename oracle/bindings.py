@@ -134,6 +134,31 @@ class Oracle(_Checker):
 class Reference(_Checker):
     prefix = "bfr"
 
+    def load_mesh(self, path):
+        """The reference's own OBJ/PLY loader: (positions, normals, uvs, triangles) as numpy arrays,
+        or (None, reference status code, message) when it refuses the file."""
+        import numpy as np
+        f = self.lib.bfr_mesh_load
+        f.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
+        f.restype = C.c_void_p
+        code = C.c_int(0)
+        handle = f(path.encode(), C.byref(code))
+        if not handle:
+            return None, code.value, self.last_error()
+        nv, nt = C.c_uint32(), C.c_uint32()
+        self.lib.bfr_mesh_counts.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        self.lib.bfr_mesh_counts(handle, C.byref(nv), C.byref(nt))
+        p = np.zeros((nv.value, 3), np.float32)
+        n = np.zeros((nv.value, 3), np.float32)
+        uv = np.zeros((nv.value, 2), np.float32)
+        t = np.zeros((nt.value, 3), np.uint32)
+        self.lib.bfr_mesh_copy.argtypes = [C.c_void_p] * 5
+        self.lib.bfr_mesh_copy(handle, p.ctypes.data_as(C.c_void_p), n.ctypes.data_as(C.c_void_p),
+                               uv.ctypes.data_as(C.c_void_p), t.ctypes.data_as(C.c_void_p))
+        self.lib.bfr_mesh_free.argtypes = [C.c_void_p]
+        self.lib.bfr_mesh_free(handle)
+        return (p, n, uv, t), 0, ""
+
     def __init__(self):
         super().__init__(REFERENCE_LIB)
         f = self.lib.bfr_camera_rays

@@ -24,6 +24,7 @@
 #include <Blackframe/Engine/FrameScene.hpp>
 #include <Blackframe/Engine/SceneMisPathLoop.hpp>
 #include <Blackframe/Engine/TriangleMesh.hpp>
+#include <Blackframe/Engine/TriangleMeshImport.hpp>
 #include <Blackframe/Renderer/Color.hpp>
 #include <Blackframe/Renderer/Film.hpp>
 #include <Blackframe/Renderer/IndependentSampler.hpp>
@@ -498,6 +499,52 @@ __attribute__((visibility("default"))) int bfr_sensor(const float* nm, const flo
     constexpr auto inverse_lane_count = 1.0F / 4.0F;
     out->normalization = inverse_lane_count / static_cast<float>(renderer::Cie1931YIntegralNanometers);
     return 0;
+}
+
+// engine::load_obj_triangle_mesh / load_ply_triangle_mesh (by the path's extension). Returns a
+// handle (null on failure, with *code = the reference's StatusCode and the message in
+// bfr_last_error); bfr_mesh_counts and bfr_mesh_copy read it, bfr_mesh_free releases it.
+__attribute__((visibility("default"))) void* bfr_mesh_load(const char* path, int* code) {
+    const std::string p(path);
+    const bool ply = p.size() >= 4 && p.compare(p.size() - 4, 4, ".ply") == 0;
+    auto mesh = ply ? engine::load_ply_triangle_mesh(p) : engine::load_obj_triangle_mesh(p);
+    if (!mesh) {
+        *code = static_cast<int>(mesh.error().code);
+        set_error(mesh.error().message);
+        return nullptr;
+    }
+    *code = 0;
+    return new engine::TriangleMesh(std::move(*mesh));
+}
+
+__attribute__((visibility("default"))) void bfr_mesh_counts(void* handle, uint32_t* vertices, uint32_t* triangles) {
+    const auto* m = static_cast<const engine::TriangleMesh*>(handle);
+    *vertices = static_cast<uint32_t>(m->positions().size());
+    *triangles = static_cast<uint32_t>(m->triangles().size());
+}
+
+__attribute__((visibility("default"))) void bfr_mesh_copy(void* handle, float* positions, float* normals, float* uvs,
+                                                          uint32_t* triangles) {
+    const auto* m = static_cast<const engine::TriangleMesh*>(handle);
+    for (size_t i = 0; i < m->positions().size(); ++i) {
+        positions[3 * i] = m->positions()[i].x;
+        positions[3 * i + 1] = m->positions()[i].y;
+        positions[3 * i + 2] = m->positions()[i].z;
+        normals[3 * i] = m->normals()[i].x;
+        normals[3 * i + 1] = m->normals()[i].y;
+        normals[3 * i + 2] = m->normals()[i].z;
+        uvs[2 * i] = m->texture_coordinates()[i].x;
+        uvs[2 * i + 1] = m->texture_coordinates()[i].y;
+    }
+    for (size_t t = 0; t < m->triangles().size(); ++t) {
+        for (int k = 0; k < 3; ++k) {
+            triangles[3 * t + k] = m->triangles()[t].vertices[k];
+        }
+    }
+}
+
+__attribute__((visibility("default"))) void bfr_mesh_free(void* handle) {
+    delete static_cast<engine::TriangleMesh*>(handle);
 }
 
 // renderer::Sphere (float) on ray k against sphere k (centre xyz, radius). Per ray, out receives
