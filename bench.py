@@ -357,6 +357,56 @@ def run_adjoint(args, torch, rank):
 
 
 IMPORT_WORKLOAD = "mesh_import_obj"
+REFIT_WORKLOAD = "refit_bvh_stress"
+
+
+def run_refit(args, torch):
+    """Transform-only refit of the BVH-stress scene (985k triangles, 42 instances, TLAS): each step
+    moves every instance (new seeded transforms) with bf200_scene_refit, beside bf200_scene_create
+    of the same description (BLAS builds included). Host wall time around each C call (the
+    descriptions are made before); the refit's device work (uploads, world normals) is inside it,
+    since the call returns after its stream."""
+    import copy
+    builder, _, _, _, _ = workload_setup("bvh_stress_1080p")
+    ctx = runtime.Context(0, path_capacity=args.capacity)
+    scene = ctx.create_scene(builder)
+    rng = np.random.default_rng(2)
+    targets = []
+    for step in range(args.warmup + args.steps):
+        b = copy.copy(builder)
+        b.instances = []
+        for mesh, material, matrix, mask in builder.instances:
+            m = np.array(matrix, np.float32)
+            m[:3, 3] = (m[:3, 3] + rng.uniform(-0.5, 0.5, 3)).astype(np.float32)
+            b.instances.append((mesh, material, m, mask))
+        targets.append(b)
+    refit_s = []
+    for step, b in enumerate(targets):
+        desc = b.desc()  # the caller's description, made before the timed call
+        t0 = time.perf_counter()
+        scene.refit(b, desc)
+        torch.cuda.synchronize()
+        if step >= args.warmup:
+            refit_s.append(time.perf_counter() - t0)
+    create_s = []
+    for step in range(max(1, min(args.steps, 2))):
+        desc = targets[-1].desc()
+        t0 = time.perf_counter()
+        fresh = ctx.create_scene(targets[-1], desc)
+        torch.cuda.synchronize()
+        create_s.append(time.perf_counter() - t0)
+        fresh.close()
+    scene.close()
+    ctx.close()
+    refit_ms = statistics.median(refit_s) * 1000.0
+    create_ms = statistics.median(create_s) * 1000.0
+    line = {"metric": "refit ms", "value": refit_ms, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": refit_ms, "higher_is_better": False, "scaling": "none",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": REFIT_WORKLOAD, "instances": len(builder.instances),
+                       "triangles": builder.triangle_count},
+            "scene_create_ms": create_ms, "create_over_refit": create_ms / refit_ms, "gpu_launches": 1}
+    print(json.dumps(line), flush=True)
 
 
 def run_mesh_import(args):
@@ -443,7 +493,7 @@ def main():
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's)")
     parser.add_argument("--workload", default=WORKLOAD,
-                        choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD, IMPORT_WORKLOAD],
+                        choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD, IMPORT_WORKLOAD, REFIT_WORKLOAD],
                         help="scene and frame (default: the headline Cornell + spheres frame); "
                              f"{BATCH_WORKLOAD}: the 64-scene batch against 64 serial renders; "
                              f"{ADJOINT_WORKLOAD}: the path-replay adjoint; {IMPORT_WORKLOAD}: OBJ ingestion")
@@ -472,6 +522,10 @@ def main():
         return
     if args.workload == ADJOINT_WORKLOAD:
         run_adjoint(args, torch, rank)
+        return
+    if args.workload == REFIT_WORKLOAD:
+        if rank == 0:
+            run_refit(args, torch)
         return
     distributed = world > 1
     if distributed:

@@ -26,6 +26,7 @@ EXPORTED_SYMBOLS = [
     "bf200_render_films_device",
     "bf200_render_adjoint_device",
     "bf200_render_backward_device",
+    "bf200_scene_refit",
     "bf200_mesh_load",
     "bf200_mesh_view",
     "bf200_mesh_destroy",
@@ -86,6 +87,8 @@ def library():
                                                  C.POINTER(abi.FilmRequest), C.POINTER(abi.TransportOptions),
                                                  C.POINTER(abi.Film), vp, vp, vp, C.POINTER(abi.Report)]
     lib.bf200_render_backward_device.restype = C.c_uint32
+    lib.bf200_scene_refit.argtypes = [vp, C.POINTER(abi.SceneDesc)]
+    lib.bf200_scene_refit.restype = C.c_uint32
     lib.bf200_mesh_load.argtypes = [C.c_char_p, C.POINTER(vp), C.c_char_p, C.c_uint64]
     lib.bf200_mesh_load.restype = C.c_uint32
     lib.bf200_mesh_view.argtypes = [vp, C.POINTER(abi.MeshView)]
@@ -116,6 +119,13 @@ class Scene:
     def __init__(self, context, handle, builder):
         self.context = context
         self.handle = handle
+        self.builder = builder
+
+    def refit(self, builder, desc=None):
+        """bf200_scene_refit with `builder`'s description (or `desc`, already made from it): only
+        instance transforms may differ."""
+        desc = builder.desc() if desc is None else desc
+        self.context._check(library().bf200_scene_refit(self.handle, C.byref(desc)), "scene_refit")
         self.builder = builder
 
     def close(self):
@@ -149,8 +159,9 @@ class Context:
     def __exit__(self, *exc):
         self.close()
 
-    def create_scene(self, builder):
-        desc = builder.desc()
+    def create_scene(self, builder, desc=None):
+        """bf200_scene_create from `builder`'s description (or `desc`, already made from it)."""
+        desc = builder.desc() if desc is None else desc
         handle = C.c_void_p()
         self._check(library().bf200_scene_create(self.handle, C.byref(desc), C.byref(handle)), "scene")
         return Scene(self, handle, builder)

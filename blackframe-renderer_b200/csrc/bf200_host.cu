@@ -68,6 +68,16 @@ struct bf200_scene {
     uint32_t material_count = 0;
     uint64_t triangle_count = 0;
     uint64_t node_count = 0;
+    // transform-only refit (bf200_scene_refit): what the instance level is rebuilt from
+    uint64_t fingerprint = 0;           // the description without its instance transforms
+    std::vector<float> object_boxes;    // per geometry: lo xyz, hi xyz
+    uint32_t tlas_first = 0;            // first TLAS node in the node array (when there is a TLAS)
+    std::vector<BvhNode4> tlas_nodes;   // host copy of the TLAS nodes
+    const uint32_t* tri_instance = nullptr;  // device: instance of every instance triangle
+    const uint32_t* tri_local = nullptr;     // device: its triangle within the geometry
+    uint32_t instance_triangles = 0;
+    uint32_t* normal_failures = nullptr;     // device counter of k_world_normals
+    size_t light_triangles = 0;
 };
 
 namespace {
@@ -673,6 +683,49 @@ bool build_light(const bf200_scene_desc_v1& d, uint32_t inst_index, LightInfo& i
     }
     info.instance = inst_index;
     return true;
+}
+
+// A 64-bit hash (FNV-1a's step over 8-byte words, then the tail bytes) of everything a
+// description holds except its instance transforms: a refit must leave all of it unchanged.
+uint64_t description_fingerprint(const bf200_scene_desc_v1& d) {
+    uint64_t h = 0xcbf29ce484222325ULL;
+    auto mix = [&h](const void* p, size_t bytes) {
+        const auto* b = static_cast<const unsigned char*>(p);
+        size_t i = 0;
+        for (; i + 8 <= bytes; i += 8) {
+            uint64_t word;
+            std::memcpy(&word, b + i, 8);
+            h = (h ^ word) * 0x100000001b3ULL;
+            h ^= h >> 29;
+        }
+        for (; i < bytes; ++i) {
+            h = (h ^ b[i]) * 0x100000001b3ULL;
+        }
+    };
+    const uint32_t counts[7] = {d.geometry_count, d.vertex_count, d.triangle_count, d.material_count,
+                                d.closure_count, d.instance_count, d.punctual_light_count};
+    mix(counts, sizeof(counts));
+    mix(d.geometries, sizeof(bf200_geometry_v1) * d.geometry_count);
+    mix(d.positions, sizeof(float) * 3 * d.vertex_count);
+    mix(d.normals, sizeof(float) * 3 * d.vertex_count);
+    if (d.texture_coordinates != nullptr) {
+        mix(d.texture_coordinates, sizeof(float) * 2 * d.vertex_count);
+    }
+    mix(d.triangles, sizeof(uint32_t) * 3 * d.triangle_count);
+    mix(d.materials, sizeof(bf200_material_v1) * d.material_count);
+    if (d.closures != nullptr) {
+        mix(d.closures, sizeof(bf200_closure_v1) * d.closure_count);
+    }
+    for (uint32_t i = 0; i < d.instance_count; ++i) {
+        const bf200_instance_v1& inst = d.instances[i];
+        const uint32_t fields[5] = {inst.instance_id, inst.object_id, inst.geometry_index, inst.material_index,
+                                    inst.visibility_mask};
+        mix(fields, sizeof(fields));
+    }
+    mix(d.wavelength_nanometers, sizeof(d.wavelength_nanometers));
+    mix(d.wavelength_pdf, sizeof(d.wavelength_pdf));
+    mix(d.environment_radiance, sizeof(d.environment_radiance));
+    return h;
 }
 
 blackframe_status validate_desc(bf200_context* c, const bf200_scene_desc_v1* d) {
@@ -1389,10 +1442,16 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
             std::vector<BvhNode> tlas2;
             const int root2 = build_tlas(world_boxes, tlas2);
             uint32_t tlas_depth4 = 1;
+            scene->tlas_first = static_cast<uint32_t>(nodes4.size());
             Collapser collapser{tlas2, nodes4};
             tlas_root = collapser.collapse(root2, 1, tlas_depth4);
             instance_level_depth = 3 * tlas_depth4 + 1;
+            scene->tlas_nodes.assign(nodes4.begin() + scene->tlas_first, nodes4.end());
         }
+        for (const Box& b : object_box) {
+            scene->object_boxes.insert(scene->object_boxes.end(), {b.lo[0], b.lo[1], b.lo[2], b.hi[0], b.hi[1], b.hi[2]});
+        }
+        scene->fingerprint = description_fingerprint(*d);
         std::vector<uint32_t> roots;
         for (const uint4& g : geom_info) {
             roots.push_back(g.z);
@@ -1553,6 +1612,10 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         const uint32_t* d_tri_local = nullptr;
         up(tri_instance, d_tri_instance);
         up(tri_local, d_tri_local);
+        scene->tri_instance = d_tri_instance;
+        scene->tri_local = d_tri_local;
+        scene->instance_triangles = static_cast<uint32_t>(tri_instance.size());
+        scene->light_triangles = light_areas.size();
         if (st != BLACKFRAME_STATUS_SUCCESS) {
             return st;
         }
@@ -1588,10 +1651,157 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
             return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "a world-space triangle normal is not representable");
         }
         v.world_normals = world_normals;
+        scene->normal_failures = failures;
     } catch (const std::bad_alloc&) {
         return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "scene build exhausted host memory");
     }
     *out_scene = scene.release();
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+// Transform-only refit: instance matrices, orientation flags, world boxes, the TLAS boxes (same
+// topology, each node the union of its children bottom-up; children follow their parents in the
+// node array), mesh lights and the world normals of every instance triangle are recomputed in
+// place; the BLASes and every buffer size stay as they are.
+BF200_EXPORT blackframe_status bf200_scene_refit(bf200_scene* s, const bf200_scene_desc_v1* d) noexcept {
+    if (s == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    bf200_context* c = s->context;
+    if (d == nullptr || d->struct_size < sizeof(bf200_scene_desc_v1) || d->geometries == nullptr ||
+        d->positions == nullptr || d->normals == nullptr || d->triangles == nullptr || d->materials == nullptr ||
+        d->instances == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "scene description missing or too small");
+    }
+    // everything but the transforms was validated when the scene was created and must be unchanged
+    if (description_fingerprint(*d) != s->fingerprint) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
+                    "a refit accepts only instance transform changes (no rebuild fallback)");
+    }
+    for (uint32_t i = 0; i < d->instance_count; ++i) {
+        const float* m = d->instances[i].object_to_world;
+        if (m[12] != 0.0F || m[13] != 0.0F || m[14] != 0.0F || m[15] != 1.0F) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "an instance transform must be affine");
+        }
+    }
+    cudaSetDevice(c->device);
+    try {
+        const uint32_t n = d->instance_count;
+        std::vector<float4> to_object(3ULL * n), to_world(3ULL * n), world_box(2ULL * n);
+        std::vector<uint4> inst_info(n);
+        std::vector<Box> boxes(n);
+        std::vector<LightInfo> lights;
+        std::vector<float4> light_vertices, light_normals;
+        std::vector<float> light_areas, light_cdf;
+        for (uint32_t i = 0; i < n; ++i) {
+            const auto& inst = d->instances[i];
+            for (int r = 0; r < 3; ++r) {
+                const float* a = inst.world_to_object + 4 * r;
+                const float* b = inst.object_to_world + 4 * r;
+                to_object[3ULL * i + r] = make_float4(a[0], a[1], a[2], a[3]);
+                to_world[3ULL * i + r] = make_float4(b[0], b[1], b[2], b[3]);
+            }
+            int orientation = 1;
+            if (!transform_orientation(inst.object_to_world, orientation)) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "instance transform orientation is singular");
+            }
+            uint32_t light_index = 0x7FFFFFFFU;
+            if (!is_black4(d->materials[inst.material_index].emitted_radiance)) {
+                LightInfo info{};
+                std::string error;
+                if (!build_light(*d, i, info, light_vertices, light_normals, light_areas, light_cdf, error)) {
+                    return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, error);
+                }
+                light_index = static_cast<uint32_t>(lights.size());
+                lights.push_back(info);
+            }
+            inst_info[i] = make_uint4(inst.geometry_index, inst.material_index, inst.visibility_mask,
+                                      light_index | (orientation < 0 ? 0x80000000U : 0U));
+            Box object;
+            const float* ob = &s->object_boxes[6ULL * inst.geometry_index];
+            for (int a = 0; a < 3; ++a) {
+                object.lo[a] = ob[a];
+                object.hi[a] = ob[3 + a];
+            }
+            boxes[i] = instance_world_box(object, inst.object_to_world);
+            world_box[2ULL * i] = make_float4(boxes[i].lo[0], boxes[i].lo[1], boxes[i].lo[2], 0.0F);
+            std::memcpy(&world_box[2ULL * i].w, &inst.visibility_mask, 4);  // mask bits, not a number
+            world_box[2ULL * i + 1] = make_float4(boxes[i].hi[0], boxes[i].hi[1], boxes[i].hi[2], 0.0F);
+        }
+        if (lights.size() != s->light_count || light_areas.size() != s->light_triangles) {
+            return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "internal error: refit changed the light layout");
+        }
+        // TLAS refit, deepest nodes first
+        std::vector<BvhNode4>& tlas = s->tlas_nodes;
+        for (size_t k = tlas.size(); k-- > 0;) {
+            BvhNode4& node = tlas[k];
+            float* lo_x = &node.lo_x.x;
+            float* hi_x = &node.hi_x.x;
+            float* lo_y = &node.lo_y.x;
+            float* hi_y = &node.hi_y.x;
+            float* lo_z = &node.lo_z.x;
+            float* hi_z = &node.hi_z.x;
+            const int* child = &node.child.x;
+            for (int slot = 0; slot < node.info.x; ++slot) {
+                Box b;
+                if (child[slot] < 0) {
+                    b = boxes[static_cast<uint32_t>(~child[slot])];
+                } else {
+                    const BvhNode4& sub = tlas[static_cast<size_t>(child[slot]) - s->tlas_first];
+                    for (int q = 0; q < sub.info.x; ++q) {
+                        Box cb;
+                        cb.lo[0] = (&sub.lo_x.x)[q], cb.hi[0] = (&sub.hi_x.x)[q];
+                        cb.lo[1] = (&sub.lo_y.x)[q], cb.hi[1] = (&sub.hi_y.x)[q];
+                        cb.lo[2] = (&sub.lo_z.x)[q], cb.hi[2] = (&sub.hi_z.x)[q];
+                        b.grow(cb);
+                    }
+                }
+                lo_x[slot] = b.lo[0], hi_x[slot] = b.hi[0];
+                lo_y[slot] = b.lo[1], hi_y[slot] = b.hi[1];
+                lo_z[slot] = b.lo[2], hi_z[slot] = b.hi[2];
+            }
+        }
+        SceneView& v = s->view;
+        cudaStream_t st = c->stream;
+        auto put = [&](auto& host, const void* device) {
+            return host.empty() ? cudaSuccess
+                                : cudaMemcpyAsync(const_cast<void*>(device), host.data(),
+                                                  host.size() * sizeof(host[0]), cudaMemcpyHostToDevice, st);
+        };
+        cudaError_t e = put(to_object, v.inst_to_object);
+        if (e == cudaSuccess) e = put(to_world, v.inst_to_world);
+        if (e == cudaSuccess) e = put(inst_info, v.inst_info);
+        if (e == cudaSuccess) e = put(world_box, v.inst_world_box);
+        if (e == cudaSuccess) e = put(lights, v.lights);
+        if (e == cudaSuccess) e = put(light_vertices, v.light_tri_vertices);
+        if (e == cudaSuccess) e = put(light_normals, v.light_tri_normals);
+        if (e == cudaSuccess) e = put(light_areas, v.light_tri_areas);
+        if (e == cudaSuccess) e = put(light_cdf, v.light_tri_cdf);
+        if (e == cudaSuccess && !tlas.empty()) {
+            e = cudaMemcpyAsync(const_cast<BvhNode4*>(v.nodes) + s->tlas_first, tlas.data(),
+                                tlas.size() * sizeof(BvhNode4), cudaMemcpyHostToDevice, st);
+        }
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->normal_failures, 0, sizeof(uint32_t), st);
+        if (e == cudaSuccess) {
+            e = launch_world_normals(v, s->tri_instance, s->tri_local, s->instance_triangles,
+                                     const_cast<float4*>(v.world_normals), s->normal_failures, st);
+        }
+        uint32_t failures = 0;
+        if (e == cudaSuccess) {
+            e = cudaMemcpyAsync(&failures, s->normal_failures, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        }
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(st);
+        }
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "scene refit");
+        }
+        if (failures != 0) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "a world-space triangle normal is not representable");
+        }
+    } catch (const std::bad_alloc&) {
+        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "scene refit exhausted host memory");
+    }
     return BLACKFRAME_STATUS_SUCCESS;
 }
 

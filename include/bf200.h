@@ -592,6 +592,15 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_backward_device(
     const bf200_transport_options_v1* options, const bf200_film_v1* film, const float* image_adjoint,
     bf200_material_gradient_v1* gradients, double* emission_gradient, bf200_report_v1* report) BF200_NOEXCEPT;
 
+/* Transform-only refit (engine::AccelBackend::refit, AccelBackend.hpp:55-86): `desc` must be the
+ * scene's description with nothing but instance transforms (object_to_world and world_to_object)
+ * changed; anything else is refused with INVALID_STATE and never turned into a rebuild. The
+ * instance level (matrices, world boxes, the TLAS boxes on its existing topology), the mesh lights
+ * and the world normals are recomputed in place; the BLASes are kept. Hits after a refit equal
+ * those of a scene created from `desc`. Must not run while a trace of this scene is in flight. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_refit(bf200_scene* scene, const bf200_scene_desc_v1* desc)
+    BF200_NOEXCEPT;
+
 /* Triangle-mesh import for callers that hold meshes as OBJ or ASCII PLY files
  * (engine::load_obj_triangle_mesh / load_ply_triangle_mesh, TriangleMeshImport.hpp:9-17): the
  * same files are accepted and refused, and an accepted file gives the same aligned arrays (one
