@@ -27,6 +27,8 @@ EXPORTED_SYMBOLS = [
     "bf200_render_adjoint_device",
     "bf200_render_backward_device",
     "bf200_scene_refit",
+    "bf200_scene_set_light_powers",
+    "bf200_light_power_cdf",
     "bf200_mesh_load",
     "bf200_mesh_view",
     "bf200_mesh_destroy",
@@ -87,6 +89,10 @@ def library():
                                                  C.POINTER(abi.FilmRequest), C.POINTER(abi.TransportOptions),
                                                  C.POINTER(abi.Film), vp, vp, vp, C.POINTER(abi.Report)]
     lib.bf200_render_backward_device.restype = C.c_uint32
+    lib.bf200_scene_set_light_powers.argtypes = [vp, vp, C.c_uint32]
+    lib.bf200_scene_set_light_powers.restype = C.c_uint32
+    lib.bf200_light_power_cdf.argtypes = [vp, C.c_uint32, vp]
+    lib.bf200_light_power_cdf.restype = C.c_uint32
     lib.bf200_scene_refit.argtypes = [vp, C.POINTER(abi.SceneDesc)]
     lib.bf200_scene_refit.restype = C.c_uint32
     lib.bf200_mesh_load.argtypes = [C.c_char_p, C.POINTER(vp), C.c_char_p, C.c_uint64]
@@ -120,6 +126,18 @@ class Scene:
         self.context = context
         self.handle = handle
         self.builder = builder
+
+    def set_light_powers(self, powers):
+        """bf200_scene_set_light_powers: power-weighted selection from 4-lane spectral powers per
+        light (None: uniform again)."""
+        if powers is None:
+            lights = sum(1 for inst in self.builder.instances if any(v != 0 for v in self.builder.materials[inst[1]][1]))
+            status = library().bf200_scene_set_light_powers(self.handle, None, lights)
+        else:
+            powers = np.ascontiguousarray(powers, np.float32).reshape(-1, 4)
+            status = library().bf200_scene_set_light_powers(self.handle, powers.ctypes.data_as(C.c_void_p),
+                                                            len(powers))
+        self.context._check(status, "scene_set_light_powers")
 
     def refit(self, builder, desc=None):
         """bf200_scene_refit with `builder`'s description (or `desc`, already made from it): only
@@ -307,6 +325,17 @@ class Context:
         self._check(library().bf200_occlusions(self.handle, scene.handle, C.cast(rays, C.c_void_p), n,
                                                out.ctypes.data_as(C.c_void_p)), "occlusions")
         return out
+
+
+def light_power_cdf(powers):
+    """bf200_light_power_cdf: the light_count + 1 selection boundaries of 4-lane spectral powers."""
+    powers = np.ascontiguousarray(powers, np.float32).reshape(-1, 4)
+    out = np.zeros(len(powers) + 1, np.float32)
+    status = library().bf200_light_power_cdf(powers.ctypes.data_as(C.c_void_p), len(powers),
+                                             out.ctypes.data_as(C.c_void_p))
+    if status != 0:
+        raise Bf200Error(status, "light power CDF refused")
+    return out
 
 
 def load_mesh(path):

@@ -601,6 +601,21 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_backward_device(
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_refit(bf200_scene* scene, const bf200_scene_desc_v1* desc)
     BF200_NOEXCEPT;
 
+/* Power-weighted light selection (LightSampler::create_power_weighted, LightSampler.hpp:110-113;
+ * the reference CUDA backend refuses it, WavefrontTransport.cpp:612-617). `spectral_powers` holds
+ * the caller's four-lane spectral flux of every scene light in registry order (mesh lights in
+ * instance order). Each light's weight is the compensated sum of its lanes over the largest lane
+ * of all lights, and the CDF is built from compensated prefix sums, as the reference builds it
+ * (bit for bit). Selection and the MIS probability of a light then follow that CDF. A null
+ * `spectral_powers` restores uniform selection. Must not run while a trace of the scene is in
+ * flight. bf200_light_power_cdf computes the light_count + 1 boundaries alone (host only). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_set_light_powers(bf200_scene* scene,
+                                                                            const float* spectral_powers,
+                                                                            uint32_t light_count) BF200_NOEXCEPT;
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_power_cdf(const float* spectral_powers,
+                                                                     uint32_t light_count, float* boundaries)
+    BF200_NOEXCEPT;
+
 /* Triangle-mesh import for callers that hold meshes as OBJ or ASCII PLY files
  * (engine::load_obj_triangle_mesh / load_ply_triangle_mesh, TriangleMeshImport.hpp:9-17): the
  * same files are accepted and refused, and an accepted file gives the same aligned arrays (one

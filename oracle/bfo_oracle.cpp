@@ -3048,6 +3048,97 @@ __attribute__((visibility("default"))) uint64_t bfo_owen_sobol_bits(uint32_t px,
 // Float32 or Neumaier float64 film of the caller-side path: CIE XYZ (Cie1931Sensor.cpp:104-176),
 // linear sRGB (Color.hpp:77-88), add_sample(x, y, rgb, 1) (Film.hpp:150-182). `sums` holds
 // (r, g, b, weight) per pixel as double; for precision 1 also the compensations are applied.
+// LightSampler::create_power_weighted (LightSampler.cpp:605-625, power_weights :200-245,
+// build_power_cdf :117-190, add_compensated :78-95) restated: the scene's selection CDF from four-
+// lane spectral powers. Returns 0, or 1 with the reason in last_error.
+bool neumaier_add(float value, float& sum, float& correction) {
+    if (!std::isfinite(value) || value < 0.0F) {
+        return false;
+    }
+    const float next = sum + value;
+    if (!std::isfinite(next)) {
+        return false;
+    }
+    correction += sum >= value ? (sum - next) + value : (value - next) + sum;
+    if (!std::isfinite(correction)) {
+        return false;
+    }
+    sum = next;
+    return true;
+}
+
+__attribute__((visibility("default"))) int bfo_scene_set_light_powers(void* handle, const float* powers,
+                                                                      uint32_t count) {
+    auto* s = static_cast<Scene*>(handle);
+    if (count == 0 || count != s->lights.size()) {
+        set_error("one spectral power per scene light is required");
+        return 1;
+    }
+    float peak = 0.0F;
+    for (uint64_t i = 0; i < 4ULL * count; ++i) {
+        if (!std::isfinite(powers[i]) || powers[i] < 0.0F) {
+            set_error("Power-weighted light sampling requires finite non-negative spectral lanes.");
+            return 1;
+        }
+        peak = std::max(peak, powers[i]);
+    }
+    if (peak == 0.0F) {
+        set_error("Power-weighted light sampling requires positive spectral power.");
+        return 1;
+    }
+    std::vector<float> weights(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        float sum = 0.0F, correction = 0.0F;
+        for (int l = 0; l < 4; ++l) {
+            if (!neumaier_add(powers[4 * i + l] / peak, sum, correction)) {
+                set_error("A spectral light-selection weight is not representable.");
+                return 1;
+            }
+        }
+        weights[i] = sum + correction;
+    }
+    float ts = 0.0F, tc = 0.0F;
+    for (float w : weights) {
+        if (!neumaier_add(w, ts, tc)) {
+            set_error("Light-selection power accumulation is not representable.");
+            return 1;
+        }
+    }
+    const float total = ts + tc;
+    if (!(total > 0.0F)) {
+        set_error("Power-weighted light sampling requires positive spectral power.");
+        return 1;
+    }
+    uint32_t last = count;
+    for (uint32_t i = count; i > 0; --i) {
+        if (weights[i - 1] > 0.0F) {
+            last = i - 1;
+            break;
+        }
+    }
+    std::vector<float> cdf(count + 1, 0.0F);
+    float ps = 0.0F, pc = 0.0F, previous = 0.0F;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (weights[i] == 0.0F) {
+            cdf[i + 1] = previous;
+            continue;
+        }
+        if (!neumaier_add(weights[i], ps, pc)) {
+            set_error("Light-selection power prefix is not representable.");
+            return 1;
+        }
+        const float boundary = i != last ? (ps + pc) / total : 1.0F;
+        if (i != last && !(boundary > previous && boundary < 1.0F)) {
+            set_error("A positive light-selection probability is not representable.");
+            return 1;
+        }
+        cdf[i + 1] = boundary;
+        previous = boundary;
+    }
+    s->light_cdf = cdf;
+    return 0;
+}
+
 // intersect_sphere on ray k against sphere k (centre xyz, radius), in world space. Per ray, out
 // receives 8 floats: status (0 miss, 1 hit, 2 not representable), t, outward normal xyz, position xyz.
 __attribute__((visibility("default"))) int bfo_sphere_intersect(const float* spheres, const bf200_ray_v1* rays,

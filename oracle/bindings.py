@@ -70,6 +70,16 @@ class _Checker:
         f(spheres.ctypes.data_as(C.c_void_p), rays, len(rays), out.ctypes.data_as(C.c_void_p))
         return out
 
+    def set_light_powers(self, handle, powers):
+        """Power-weighted light selection for the scene from 4-lane spectral powers per light."""
+        import numpy as np
+        powers = np.ascontiguousarray(powers, np.float32).reshape(-1, 4)
+        f = getattr(self.lib, self.prefix + "_scene_set_light_powers")
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        f.restype = C.c_int
+        if f(handle, powers.ctypes.data_as(C.c_void_p), len(powers)) != 0:
+            raise CheckerError(self.last_error())
+
     def trace(self, handle, inputs, options, threads=None):
         n = len(inputs)
         results = (abi.PathResult * n)()
@@ -133,6 +143,25 @@ class Oracle(_Checker):
 
 class Reference(_Checker):
     prefix = "bfr"
+
+    def power_sampler(self, powers, samples):
+        """The reference's power-weighted LightSampler: (probability of every light, selected index
+        and probability for every canonical sample), or (None, StatusCode) when it refuses."""
+        import numpy as np
+        powers = np.ascontiguousarray(powers, np.float32).reshape(-1, 4)
+        samples = np.ascontiguousarray(samples, np.float32)
+        probabilities = np.zeros(len(powers), np.float32)
+        selected = np.zeros(len(samples), np.uint32)
+        selected_probability = np.zeros(len(samples), np.float32)
+        f = self.lib.bfr_power_sampler
+        f.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        f.restype = C.c_int
+        code = f(powers.ctypes.data_as(C.c_void_p), len(powers), probabilities.ctypes.data_as(C.c_void_p),
+                 samples.ctypes.data_as(C.c_void_p), len(samples), selected.ctypes.data_as(C.c_void_p),
+                 selected_probability.ctypes.data_as(C.c_void_p))
+        if code != 0:
+            return None, code
+        return (probabilities, selected, selected_probability), 0
 
     def load_mesh(self, path):
         """The reference's own OBJ/PLY loader: (positions, normals, uvs, triangles) as numpy arrays,

@@ -501,6 +501,53 @@ __attribute__((visibility("default"))) int bfr_sensor(const float* nm, const flo
     return 0;
 }
 
+// LightSampler::create_power_weighted over 4-lane spectral powers: probability(i) of every light
+// into `probabilities`, and sample(u_k) (index, probability) for every u in `samples`. Returns 0,
+// or the reference StatusCode when it refuses the powers.
+__attribute__((visibility("default"))) int bfr_power_sampler(const float* powers, uint32_t count, float* probabilities,
+                                                             const float* samples, uint32_t sample_count,
+                                                             uint32_t* selected, float* selected_probability) {
+    std::vector<renderer::LightSpectrumT<renderer::TransportScalar>> spectra(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        for (int l = 0; l < 4; ++l) {
+            spectra[i].values[l] = powers[4 * i + l];
+        }
+    }
+    auto sampler = renderer::LightSampler::create_power_weighted(spectra);
+    if (!sampler) {
+        set_error(sampler.error().message);
+        return static_cast<int>(sampler.error().code);
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        probabilities[i] = sampler->probability(i)->value();
+    }
+    for (uint32_t k = 0; k < sample_count; ++k) {
+        const auto selection = sampler->sample(samples[k]);
+        selected[k] = selection ? selection->light_index() : 0xFFFFFFFFU;
+        selected_probability[k] = selection ? selection->probability().value() : -1.0F;
+    }
+    return 0;
+}
+
+// Replaces a scene's light sampler by the power-weighted one (traces then select by power).
+__attribute__((visibility("default"))) int bfr_scene_set_light_powers(void* handle, const float* powers,
+                                                                      uint32_t count) {
+    auto* scene = static_cast<RefScene*>(handle);
+    std::vector<renderer::LightSpectrumT<renderer::TransportScalar>> spectra(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        for (int l = 0; l < 4; ++l) {
+            spectra[i].values[l] = powers[4 * i + l];
+        }
+    }
+    auto sampler = renderer::LightSampler::create_power_weighted(spectra);
+    if (!sampler) {
+        set_error(sampler.error().message);
+        return static_cast<int>(sampler.error().code);
+    }
+    scene->sampler = std::make_unique<renderer::LightSampler>(std::move(*sampler));
+    return 0;
+}
+
 // engine::load_obj_triangle_mesh / load_ply_triangle_mesh (by the path's extension). Returns a
 // handle (null on failure, with *code = the reference's StatusCode and the message in
 // bfr_last_error); bfr_mesh_counts and bfr_mesh_copy read it, bfr_mesh_free releases it.
