@@ -161,18 +161,29 @@ def cpu_sample_rate(target_seconds=15.0):
 BATCH_WORKLOAD = "batch64"
 
 
-def run_batch(args, torch, rank):
+def run_batch(args, torch, rank, world, local_rank):
     """The 64-scene batch: one bf200_render_films_device call over 64 uneven jobs against the same
     64 jobs rendered one after another with bf200_render_film_device. Each step renders every job
-    once; both arms are timed with CUDA events around the whole step (films zeroed before)."""
-    if rank != 0:
-        return
+    once; both arms are timed with CUDA events around the whole step (films zeroed before). With N
+    GPUs the jobs are sharded whole (multigpu.batch_shard, no exchange) and each step's time is the
+    maximum over ranks."""
+    import torch.distributed as dist
+    from datetime import timedelta
+    distributed = world > 1
+    if distributed:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
     g = np.load(os.path.join(REPO, "tests", "golden", f"{WORKLOAD}.npz"))
     from helpers import sensor_from_golden
     sensor = sensor_from_golden(g)
-    ctx = runtime.Context(0, path_capacity=args.capacity)
-    jobs, films, paths, triangles = [], [], 0, 0
+    ctx = runtime.Context(local_rank, path_capacity=args.capacity)
+    all_paths = []
     for seed in range(64):
+        _, _, (w, h, spp) = scenes.batch_job(seed)
+        all_paths.append(w * h * spp)
+    mine = multigpu.batch_shard(all_paths, rank, world)
+    jobs, films, paths, triangles = [], [], 0, 0
+    for seed in mine:
         builder, options, (w, h, spp) = scenes.batch_job(seed)
         scene = ctx.create_scene(builder)
         cam = runtime.camera_create(*scenes.camera_frame_inputs(), w, h, scenes.CAMERA_VFOV, scenes.PATH_TIME)
@@ -196,18 +207,25 @@ def run_batch(args, torch, rank):
             counts.zero_()
         flush.fill_(step & 0xFF)
         torch.cuda.synchronize()
+        if distributed:
+            dist.barrier()
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         reports = fn()
         stop.record()
         torch.cuda.synchronize()
-        return start.elapsed_time(stop), reports
+        ms = start.elapsed_time(stop)
+        if distributed:
+            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, reports
 
     for step in range(args.warmup):
         timed(batched, step)
         timed(serial, step)
     batch_ms, serial_ms, failed = [], [], 0
-    with ClockSampler(0) as clocks:
+    with ClockSampler(local_rank) as clocks:
         for step in range(args.steps):
             ms, reports = timed(batched, step)
             batch_ms.append(ms)
@@ -215,13 +233,20 @@ def run_batch(args, torch, rank):
             ms, _ = timed(serial, step)
             serial_ms.append(ms)
     batch_total, serial_total = sum(batch_ms), sum(serial_ms)
-    value = paths * args.steps / (batch_total / 1000.0)
-    serial_value = paths * args.steps / (serial_total / 1000.0)
+    total_paths = sum(all_paths)
+    value = total_paths * args.steps / (batch_total / 1000.0)
+    serial_value = total_paths * args.steps / (serial_total / 1000.0)
+    if distributed:
+        f = torch.tensor([failed], dtype=torch.int64, device="cuda")
+        dist.all_reduce(f)
+        failed = int(f.item())
     line = {
-        "metric": "batched path samples/s", "value": value, "unit": "path samples/s", "n_gpus": 1,
+        "metric": "batched path samples/s", "value": value, "unit": "path samples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_total / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": BATCH_WORKLOAD, "jobs": 64, "paths_per_step": paths, "unique_triangles": triangles,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "jobs": 64, "jobs_per_gpu": len(mine), "paths_per_step": total_paths,
+                   "unique_triangles_rank0": triangles,
+                   "parallelism": f"whole scenes sharded x{world}" if distributed else "single GPU",
                    "lanes": args.lanes or "autotuned", "path_capacity": args.capacity,
                    "l2": "flushed between steps (256 MiB write)"},
         "serial": {"value": serial_value, "ms_per_step": serial_total / args.steps},
@@ -230,7 +255,11 @@ def run_batch(args, torch, rank):
     for j in jobs:
         j[0].close()
     ctx.close()
-    print(json.dumps(line), flush=True)
+    if distributed:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 ADJOINT_WORKLOAD = "adjoint_icosphere_256"
@@ -518,7 +547,7 @@ def main():
 
     torch.cuda.set_device(local_rank)
     if args.workload == BATCH_WORKLOAD:
-        run_batch(args, torch, rank)
+        run_batch(args, torch, rank, world, local_rank)
         return
     if args.workload == ADJOINT_WORKLOAD:
         run_adjoint(args, torch, rank)

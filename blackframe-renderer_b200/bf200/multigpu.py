@@ -15,6 +15,20 @@ def rank_sample_range(step, rank, world, samples_per_pixel):
     return first, first + samples_per_pixel
 
 
+def batch_shard(job_paths, rank, world):
+    """The jobs of a multi-scene batch that `rank` of `world` renders: whole jobs, no exchange.
+    Jobs go largest first to the rank with the fewest paths so far (ties to the lowest rank), so
+    uneven jobs balance; every job goes to exactly one rank. Returns job indices in ascending order."""
+    order = sorted(range(len(job_paths)), key=lambda j: (-job_paths[j], j))
+    load = [0] * world
+    owner = [0] * len(job_paths)
+    for j in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[j] = r
+        load[r] += job_paths[j]
+    return [j for j in range(len(job_paths)) if owner[j] == rank]
+
+
 def reduce_film(sums, counts=None):
     """Sums the per-rank films in place on every rank (torch tensors on the process group's
     device). Sample counts are summed as well when given."""

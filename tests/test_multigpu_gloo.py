@@ -68,6 +68,20 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def test_batch_shards_are_disjoint_complete_and_balanced():
+    from bf200 import multigpu, scenes
+    paths = []
+    for seed in range(64):
+        _, _, (w, h, spp) = scenes.batch_job(seed)
+        paths.append(w * h * spp)
+    for world in (1, 2, 4, 8):
+        shards = [multigpu.batch_shard(paths, r, world) for r in range(world)]
+        every = sorted(j for shard in shards for j in shard)
+        assert every == list(range(64))
+        loads = [sum(paths[j] for j in shard) for shard in shards]
+        assert max(loads) - min(loads) <= max(paths)  # greedy largest-first: within one job
+
+
 def test_sample_ranges_are_disjoint_and_complete():
     world, spp = 4, 3
     covered = []
