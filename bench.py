@@ -265,6 +265,95 @@ def run_batch(args, torch, rank, world, local_rank):
 ADJOINT_WORKLOAD = "adjoint_icosphere_256"
 
 
+def run_adjoint_distributed(args, torch, rank, world, local_rank):
+    """The adjoint on N GPUs (weak in nothing: the 64 spp of the frame are split across ranks). One
+    step: each rank renders its samples (bf200_render_film_device), the films are summed (NCCL
+    all-reduce), every rank forms dLoss/d(image) = 2 (image - target), runs
+    bf200_render_backward_device on its samples, and the gradients are summed (all-reduce). The
+    target is uploaded from pinned host memory and the gradients read back every step (so the
+    step is also the end-to-end figure); time = max over ranks of CUDA events around the step."""
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+    builder, options, camera, sensor, (width, height, spp) = workload_setup(ADJOINT_WORKLOAD)
+    if args.spp > 0:
+        spp = args.spp
+    share = spp // world
+    if share * world != spp:
+        raise SystemExit("the adjoint bench splits the samples evenly: spp must be a multiple of the GPU count")
+    ctx = runtime.Context(local_rank, path_capacity=args.capacity)
+    target_builder = scenes.adjoint_icosphere(scenes.SceneBuilder(), scenes.perturbed_parameters(scenes.adjoint_parameters()))
+    target_scene = ctx.create_scene(target_builder)
+    sums = torch.zeros((height, width, 8), dtype=torch.float64, device="cuda")
+    counts = torch.zeros((height, width), dtype=torch.int64, device="cuda")
+    ctx.render_film_device(target_scene, camera, sensor, options, spp, 7, 0, 1, sums.data_ptr(), counts.data_ptr())
+    target_host = ((sums[..., :3] + sums[..., 4:7]) / (sums[..., 3:4] + sums[..., 7:8])).float().cpu().pin_memory()
+    target_scene.close()
+    scene = ctx.create_scene(builder)
+    target = torch.empty_like(target_host, device="cuda")
+    grads = torch.zeros((len(builder.materials), 8), dtype=torch.float64, device="cuda")
+    emission = torch.zeros(1, dtype=torch.float64, device="cuda")
+    host_grads = torch.empty((len(builder.materials) * 8 + 1,), dtype=torch.float64).pin_memory()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def step_once():
+        target.copy_(target_host, non_blocking=True)
+        sums.zero_()
+        counts.zero_()
+        forward = ctx.render_film_device(scene, camera, sensor, options, share, 0, rank * share, 1, sums.data_ptr(),
+                                         counts.data_ptr())
+        multigpu.reduce_film(sums, counts)
+        image = (sums[..., :3] + sums[..., 4:7]) / (sums[..., 3:4] + sums[..., 7:8])
+        image_adjoint = (2.0 * (image - target.double())).float().contiguous()
+        retrace = ctx.render_backward_device(scene, camera, sensor, options, share, 0, rank * share, 1,
+                                             sums.data_ptr(), counts.data_ptr(), image_adjoint.data_ptr(),
+                                             grads.data_ptr(), emission.data_ptr())
+        packed = torch.cat([grads.flatten(), emission])
+        dist.all_reduce(packed)
+        host_grads.copy_(packed, non_blocking=True)
+        # forward, loss image, re-trace, and a replay with as many launches as the re-trace
+        launches[0] += forward.kernel_launches + 1 + 2 * retrace.kernel_launches
+        return float(((image - target.double()) ** 2).sum().item())
+
+    launches = [0]
+    for w in range(args.warmup):
+        step_once()
+    launches[0] = 0
+    step_ms = []
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
+            dist.barrier()
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            loss = step_once()
+            stop.record()
+            torch.cuda.synchronize()
+            t = torch.tensor([start.elapsed_time(stop)], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            step_ms.append(float(t.item()))
+    total = sum(step_ms)
+    paths = width * height * spp
+    value = paths * args.steps / (total / 1000.0)
+    scene.close()
+    ctx.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "adjoint path samples/s", "value": value, "unit": "path samples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": ADJOINT_WORKLOAD, "width": width, "height": height, "spp": spp,
+                       "parallelism": f"samples split x{world}; film and gradient all-reduce",
+                       "l2": "flushed between steps (256 MiB write); path state > L2"},
+            "loss": loss, "clocks": clocks.summary(),
+            "e2e": {"value": value, "unit": "path samples/s", "h2d_bytes_per_step": target_host.numel() * 4,
+                    "d2h_bytes_per_step": host_grads.numel() * 8},
+            "gpu_launches": launches[0]}), flush=True)
+
+
 def run_adjoint(args, torch, rank):
     """The path-replay adjoint: one step = one bf200_render_adjoint_device call (forward render of
     256 x 256 x 64 spp, L2 loss against a target rendered at perturbed parameters, replay of every
@@ -527,6 +616,9 @@ def main():
                              f"{BATCH_WORKLOAD}: the 64-scene batch against 64 serial renders; "
                              f"{ADJOINT_WORKLOAD}: the path-replay adjoint; {IMPORT_WORKLOAD}: OBJ ingestion")
     parser.add_argument("--lanes", type=int, default=0, help="batch lanes (0: autotuned)")
+    parser.add_argument("--adjoint-pair", action="store_true",
+                        help="run the adjoint workload as the forward/backward pair with NCCL reductions "
+                             "(always so on more than one GPU)")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -550,7 +642,10 @@ def main():
         run_batch(args, torch, rank, world, local_rank)
         return
     if args.workload == ADJOINT_WORKLOAD:
-        run_adjoint(args, torch, rank)
+        if world > 1 or args.adjoint_pair:
+            run_adjoint_distributed(args, torch, rank, world, local_rank)
+        else:
+            run_adjoint(args, torch, rank)
         return
     if args.workload == REFIT_WORKLOAD:
         if rank == 0:
