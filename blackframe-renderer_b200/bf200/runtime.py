@@ -27,6 +27,7 @@ EXPORTED_SYMBOLS = [
     "bf200_render_adjoint_device",
     "bf200_render_backward_device",
     "bf200_scene_refit",
+    "bf200_scene_create_from_soa",
     "bf200_scene_set_light_powers",
     "bf200_light_power_cdf",
     "bf200_mesh_load",
@@ -93,6 +94,8 @@ def library():
     lib.bf200_scene_set_light_powers.restype = C.c_uint32
     lib.bf200_light_power_cdf.argtypes = [vp, C.c_uint32, vp]
     lib.bf200_light_power_cdf.restype = C.c_uint32
+    lib.bf200_scene_create_from_soa.argtypes = [vp, vp, C.c_uint64, C.POINTER(vp), C.c_char_p, C.c_uint64]
+    lib.bf200_scene_create_from_soa.restype = C.c_uint32
     lib.bf200_scene_refit.argtypes = [vp, C.POINTER(abi.SceneDesc)]
     lib.bf200_scene_refit.restype = C.c_uint32
     lib.bf200_mesh_load.argtypes = [C.c_char_p, C.POINTER(vp), C.c_char_p, C.c_uint64]
@@ -182,6 +185,17 @@ class Context:
         desc = builder.desc() if desc is None else desc
         handle = C.c_void_p()
         self._check(library().bf200_scene_create(self.handle, C.byref(desc), C.byref(handle)), "scene")
+        return Scene(self, handle, builder)
+
+    def create_scene_from_soa(self, blob, builder=None):
+        """bf200_scene_create_from_soa from a scene SoA v4 blob (bytes)."""
+        handle = C.c_void_p()
+        message = C.create_string_buffer(512)
+        data = C.create_string_buffer(bytes(blob), len(blob))
+        status = library().bf200_scene_create_from_soa(self.handle, data, len(blob), C.byref(handle), message,
+                                                        len(message))
+        if status != 0:
+            raise Bf200Error(status, message.value.decode(errors="replace"))
         return Scene(self, handle, builder)
 
     def trace_paths(self, scene, inputs, options):

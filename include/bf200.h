@@ -592,6 +592,18 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_backward_device(
     const bf200_transport_options_v1* options, const bf200_film_v1* film, const float* image_adjoint,
     bf200_material_gradient_v1* gradients, double* emission_gradient, bf200_report_v1* report) BF200_NOEXCEPT;
 
+/* Scene upload from the reference's scene SoA blob, ABI v4 (SceneSoaHeader + 194 columns,
+ * Blackframe/XPU/Shared/Include/Blackframe/XPU/Shared/SceneSoaAbi.hpp, as CudaSceneSoA::upload
+ * serialises a FrameScene; replaces SceneSoA.hpp:33): the header is validated as
+ * validate_scene_soa_header does and the FNV-1a content hash is checked; then the scene is created
+ * as bf200_scene_create creates it. Punctual lights, normal/bump maps and materials resolved at
+ * different wavelength packets are refused with INVALID_STATE (no substitution). On failure
+ * `message` (when given) receives the reason. Host memory; the blob is not retained. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_create_from_soa(bf200_context* context,
+                                                                           const void* blob, uint64_t size,
+                                                                           bf200_scene** scene, char* message,
+                                                                           uint64_t message_capacity) BF200_NOEXCEPT;
+
 /* Transform-only refit (engine::AccelBackend::refit, AccelBackend.hpp:55-86): `desc` must be the
  * scene's description with nothing but instance transforms (object_to_world and world_to_object)
  * changed; anything else is refused with INVALID_STATE and never turned into a rebuild. The
