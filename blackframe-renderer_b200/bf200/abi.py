@@ -189,7 +189,13 @@ class Hit(C.Structure):
                 ("primitive_index", u32), ("status", u32), ("reserved", u32)]
 
 
+class RayCone(C.Structure):
+    """bf200_ray_cone_v1: radius at the ray origin and radial slope."""
+    _fields_ = [("width", C.c_float), ("spread", C.c_float)]
+
+
 EXPECTED_SIZES = {
+    RayCone: 8,
     Closure: 64, Material: 80, Geometry: 32, Instance: 160, Ray: 48, SampleIndex: 24,
     PathInput: 80, PathResult: 128, TransportOptions: 64, Camera: 88, Sensor: 80,
     FilmRequest: 40, FilmJob: 64, MeshView: 48, MaterialGradient: 64, Adjoint: 40, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,

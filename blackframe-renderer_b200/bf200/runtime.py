@@ -33,6 +33,8 @@ EXPORTED_SYMBOLS = [
     "bf200_mesh_load",
     "bf200_mesh_view",
     "bf200_mesh_destroy",
+    "bf200_trace_paths_with_cones",
+    "bf200_trace_paths_with_cones_device",
 ]
 
 
@@ -68,6 +70,9 @@ def library():
     lib.bf200_trace_paths_device_noalloc.argtypes = [vp, vp, vp, C.c_uint64, C.POINTER(abi.TransportOptions), vp,
                                                      C.c_uint32, C.POINTER(abi.Report)]
     lib.bf200_trace_paths_device_noalloc.restype = C.c_uint32
+    for f in (lib.bf200_trace_paths_with_cones, lib.bf200_trace_paths_with_cones_device):
+        f.argtypes = [vp, vp, vp, vp, C.c_uint64, C.POINTER(abi.TransportOptions), vp, vp, C.POINTER(abi.Report)]
+        f.restype = C.c_uint32
     for name in ("bf200_render_film", "bf200_render_film_device"):
         f = getattr(lib, name)
         f.argtypes = [vp, vp, C.POINTER(abi.Camera), C.POINTER(abi.Sensor), C.POINTER(abi.FilmRequest),
@@ -207,6 +212,32 @@ class Context:
                                                 C.byref(options), C.cast(results, C.c_void_p),
                                                 C.byref(report)), "trace_paths")
         return results, report
+
+    def trace_paths_with_cones(self, scene, inputs, cones, options):
+        """bf200_trace_paths_with_cones: cones is float32 [n, 2] of primary (width, spread); returns
+        (results, terminal cones float32 [n, 2], report)."""
+        import numpy as np
+        n = len(inputs)
+        cones = np.ascontiguousarray(cones, np.float32).reshape(n, 2)
+        terminal = np.zeros((n, 2), np.float32)
+        results = (abi.PathResult * n)()
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_trace_paths_with_cones(
+            self.handle, scene.handle, C.cast(inputs, C.c_void_p), cones.ctypes.data_as(C.c_void_p), n,
+            C.byref(options), C.cast(results, C.c_void_p), terminal.ctypes.data_as(C.c_void_p), C.byref(report)),
+            "trace_paths_with_cones")
+        return results, terminal, report
+
+    def trace_paths_with_cones_device(self, scene, device_inputs, device_cones, path_count, options,
+                                      device_results, device_terminal_cones):
+        """bf200_trace_paths_with_cones_device: every array is a device pointer (int)."""
+        report = abi.Report()
+        report.struct_size = C.sizeof(abi.Report)
+        self._check(library().bf200_trace_paths_with_cones_device(
+            self.handle, scene.handle, device_inputs, device_cones, path_count, C.byref(options), device_results,
+            device_terminal_cones, C.byref(report)), "trace_paths_with_cones_device")
+        return report
 
     def trace_paths_device(self, scene, device_inputs, path_count, options, device_results):
         """bf200_trace_paths_device: inputs and results are device pointers (ints)."""

@@ -126,6 +126,10 @@ struct PathSource {
     const bf200_path_input_v1* inputs;
     bf200_path_result_v1* results;
     float4* path_radiance;  // film mode: radiance per path id of the chunk
+    // batch mode with ray cones: the primary cone of every input (width, spread) and the cone at
+    // every result's terminal-ray origin; both null when the caller traces without cones
+    const float2* cones_in;
+    float2* cones_out;
     // sampler: null for the hash SampleStream; otherwise the Owen-scrambled Sobol direction heads
     // (kDeviceSobolDimensions x 64 leading 32-bit direction numbers)
     const uint32_t* sobol;
@@ -172,6 +176,7 @@ struct Wavefront {
     uint4* sobol_index; // Owen-Sobol sampler only: sample index, seed (64-bit each, split)
     uint2* pixel_hash;  // Owen-Sobol sampler only: mix_bits of the packed pixel
     uint32_t* mask;     // ray visibility mask of the path
+    float2* cone;       // ray cone (width, spread) at the ray origin; null unless cones are traced
     float4* hit_tb;     // t, b0, b1, b2
     uint2* hit_id;      // instance, primitive (instance = ~0 on a miss)
     // routing: shading route per slot, and the slots of every route in slot order

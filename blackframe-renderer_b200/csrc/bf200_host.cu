@@ -58,6 +58,9 @@ struct bf200_context {
     // path-replay adjoint: pixel adjoint, gradient sums, loss, per-slot scores
     void* adjoint_workspace = nullptr;
     size_t adjoint_workspace_bytes = 0;
+    // ray cones of the wavefront slots (bf200_trace_paths_with_cones*), capacity x (width, spread)
+    void* cone_column = nullptr;
+    size_t cone_column_bytes = 0;
 };
 
 struct bf200_scene {
@@ -873,6 +876,69 @@ uint64_t description_fingerprint(const bf200_scene_desc_v1& d) {
     return h;
 }
 
+// The payload checks of ClosureSet's append_* (ClosureSet.hpp:76-111, 140-260): reflectances in
+// [0, 1], conductor eta > 0 and k >= 0, dielectric etas > 0 and distinct, a representable GGX
+// alpha pair (GgxMicrofacet.hpp:62-104), and the lobes each kind is appended with.
+bool unit_interval4(const float* v) {
+    for (int i = 0; i < 4; ++i) {
+        if (!std::isfinite(v[i]) || v[i] < 0.0F || v[i] > 1.0F) {
+            return false;
+        }
+    }
+    return true;
+}
+
+bool representable_alpha_pair(float alpha_x, float alpha_y) {
+    if (!std::isfinite(alpha_x) || !(alpha_x > 0.0F) || !std::isfinite(alpha_y) || !(alpha_y > 0.0F)) {
+        return false;
+    }
+    const float maximum_alpha = std::sqrt(std::numeric_limits<float>::max()) * std::sqrt(3.14159265358979323846F);
+    const float minimum_alpha = 1.0F / maximum_alpha;
+    if (alpha_x < minimum_alpha || alpha_x > maximum_alpha || alpha_y < minimum_alpha || alpha_y > maximum_alpha) {
+        return false;
+    }
+    if (alpha_x == alpha_y) {
+        return true;
+    }
+    // D = 1 / (pi ax ay q^4) with q between min and max of {1, 1/ax, 1/ay}: both extremes of the
+    // density must stay inside float range (evaluated in logs, in long double)
+    using Wide = long double;
+    const Wide ax = alpha_x, ay = alpha_y;
+    const Wide min_q = std::min({Wide{1}, Wide{1} / ax, Wide{1} / ay});
+    const Wide max_q = std::max({Wide{1}, Wide{1} / ax, Wide{1} / ay});
+    const Wide log_scale = std::log(Wide{1} / Wide{3.141592653589793238462643383279502884L}) - std::log(ax) -
+                           std::log(ay);
+    const Wide max_log_density = log_scale - Wide{4} * std::log(min_q);
+    const Wide min_log_density = log_scale - Wide{4} * std::log(max_q);
+    return std::isfinite(max_log_density) && std::isfinite(min_log_density) &&
+           max_log_density <= std::log(static_cast<Wide>(std::numeric_limits<float>::max())) &&
+           min_log_density >= std::log(static_cast<Wide>(std::numeric_limits<float>::denorm_min()));
+}
+
+bool valid_closure_payload(const bf200_closure_v1& c) {
+    const float* p = c.parameters;
+    if (!unit_interval4(c.weight)) {
+        return false;
+    }
+    switch (c.kind) {
+    case BF200_CLOSURE_LAMBERTIAN_REFLECTION:
+        return c.lobes == (BF200_LOBE_DIFFUSE | BF200_LOBE_REFLECTION);
+    case BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION:
+        for (int i = 0; i < 4; ++i) {
+            if (!std::isfinite(p[i]) || !(p[i] > 0.0F) || !std::isfinite(p[4 + i]) || p[4 + i] < 0.0F) {
+                return false;
+            }
+        }
+        return c.lobes == (BF200_LOBE_GLOSSY | BF200_LOBE_REFLECTION) && representable_alpha_pair(p[8], p[9]);
+    case BF200_CLOSURE_ROUGH_DIELECTRIC:
+        return c.lobes == (BF200_LOBE_GLOSSY | BF200_LOBE_REFLECTION | BF200_LOBE_TRANSMISSION) &&
+               std::isfinite(p[0]) && p[0] > 0.0F && std::isfinite(p[1]) && p[1] > 0.0F && p[0] != p[1] &&
+               representable_alpha_pair(p[2], p[3]);
+    default:
+        return false;
+    }
+}
+
 blackframe_status validate_desc(bf200_context* c, const bf200_scene_desc_v1* d) {
     if (d == nullptr || d->struct_size < sizeof(bf200_scene_desc_v1)) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "scene description missing or too small");
@@ -937,6 +1003,10 @@ blackframe_status validate_desc(bf200_context* c, const bf200_scene_desc_v1* d) 
             if (kind != BF200_CLOSURE_LAMBERTIAN_REFLECTION && kind != BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION &&
                 kind != BF200_CLOSURE_ROUGH_DIELECTRIC) {
                 return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "closure kind not supported by this backend");
+            }
+            if (!valid_closure_payload(d->closures[mat.closure_offset])) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
+                            "material " + std::to_string(m) + " has an invalid closure payload");
             }
         }
     }
@@ -1500,7 +1570,8 @@ BF200_EXPORT blackframe_status bf200_context_destroy(bf200_context* c) noexcept 
     if (c->pinned_counters != nullptr) {
         cudaFreeHost(c->pinned_counters);
     }
-    for (void* p : {c->film_radiance, c->film_staging, c->batch_staging, c->lane_arena, c->adjoint_workspace}) {
+    for (void* p : {c->film_radiance, c->film_staging, c->batch_staging, c->lane_arena, c->adjoint_workspace,
+                    c->cone_column}) {
         if (p != nullptr) {
             cudaFree(p);
         }
@@ -2021,11 +2092,16 @@ BF200_EXPORT blackframe_status bf200_scene_destroy(bf200_scene* s) noexcept {
     return BLACKFRAME_STATUS_SUCCESS;
 }
 
-BF200_EXPORT blackframe_status bf200_trace_paths_device(bf200_context* c, const bf200_scene* s,
-                                                         const bf200_path_input_v1* device_inputs,
-                                                         uint64_t path_count, const bf200_transport_options_v1* o,
-                                                         bf200_path_result_v1* device_results,
-                                                         bf200_report_v1* report) noexcept {
+}  // extern "C"
+
+namespace {
+
+// The batch trace from device inputs to device results; cones_in / cones_out (both or neither)
+// carry every path's ray cone through the wavefront.
+blackframe_status trace_batch_device(bf200_context* c, const bf200_scene* s, const bf200_path_input_v1* device_inputs,
+                                     const float2* cones_in, uint64_t path_count, const bf200_transport_options_v1* o,
+                                     bf200_path_result_v1* device_results, float2* cones_out,
+                                     bf200_report_v1* report) {
     if (c == nullptr || s == nullptr || (path_count != 0 && (device_inputs == nullptr || device_results == nullptr))) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
     }
@@ -2050,10 +2126,114 @@ BF200_EXPORT blackframe_status bf200_trace_paths_device(bf200_context* c, const 
     src.total = path_count;
     src.inputs = device_inputs;
     src.results = device_results;
+    if (cones_in != nullptr) {
+        if (const auto st = grow_workspace(c, &c->cone_column, &c->cone_column_bytes, c->capacity * sizeof(float2),
+                                           "ray-cone column");
+            st != BLACKFRAME_STATUS_SUCCESS) {
+            return st;
+        }
+        c->w.cone = static_cast<float2*>(c->cone_column);
+        src.cones_in = cones_in;
+        src.cones_out = cones_out;
+    }
     if (const auto st = sobol_table(c, *o, &src.sobol); st != BLACKFRAME_STATUS_SUCCESS) {
         return st;
     }
     return run_wavefront(c, s, src, make_params(*o), o->instrumentation != 0, report);
+}
+
+// Host inputs (and cones) to host results (and cones) through the context's batch staging.
+blackframe_status trace_batch_host(bf200_context* c, const bf200_scene* s, const bf200_path_input_v1* inputs,
+                                   const bf200_ray_cone_v1* cones_in, uint64_t path_count,
+                                   const bf200_transport_options_v1* o, bf200_path_result_v1* results,
+                                   bf200_ray_cone_v1* cones_out, bf200_report_v1* report) {
+    const bool cones = cones_in != nullptr;
+    if (path_count == 0) {
+        return trace_batch_device(c, s, nullptr, nullptr, 0, o, nullptr, nullptr, report);
+    }
+    cudaSetDevice(c->device);
+    const auto span = [](size_t bytes) { return (bytes + 255) & ~size_t(255); };
+    const size_t in_bytes = path_count * sizeof(bf200_path_input_v1);
+    const size_t out_bytes = path_count * sizeof(bf200_path_result_v1);
+    const size_t cone_bytes = cones ? path_count * sizeof(bf200_ray_cone_v1) : 0;
+    if (const auto st = grow_workspace(c, &c->batch_staging, &c->batch_staging_bytes,
+                                       span(in_bytes) + span(out_bytes) + 2 * span(cone_bytes), "batch staging");
+        st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    char* base = static_cast<char*>(c->batch_staging);
+    auto* d_in = reinterpret_cast<bf200_path_input_v1*>(base);
+    auto* d_out = reinterpret_cast<bf200_path_result_v1*>(base + span(in_bytes));
+    auto* d_cone_in = cones ? reinterpret_cast<float2*>(base + span(in_bytes) + span(out_bytes)) : nullptr;
+    auto* d_cone_out = cones ? reinterpret_cast<float2*>(base + span(in_bytes) + span(out_bytes) + span(cone_bytes))
+                             : nullptr;
+    cudaError_t e = cudaMemcpyAsync(d_in, inputs, in_bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && cones) {
+        e = cudaMemcpyAsync(d_cone_in, cones_in, cone_bytes, cudaMemcpyHostToDevice, c->stream);
+    }
+    blackframe_status st = e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "batch upload");
+    if (st == BLACKFRAME_STATUS_SUCCESS) {
+        st = trace_batch_device(c, s, d_in, d_cone_in, path_count, o, d_out, d_cone_out, report);
+    }
+    if (st == BLACKFRAME_STATUS_SUCCESS) {
+        e = cudaMemcpyAsync(results, d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess && cones) {
+            e = cudaMemcpyAsync(cones_out, d_cone_out, cone_bytes, cudaMemcpyDeviceToHost, c->stream);
+        }
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(c->stream);
+        }
+        if (e != cudaSuccess) {
+            st = cuda_fail(c, e, "batch download");
+        }
+    }
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+BF200_EXPORT blackframe_status bf200_trace_paths_device(bf200_context* c, const bf200_scene* s,
+                                                         const bf200_path_input_v1* device_inputs,
+                                                         uint64_t path_count, const bf200_transport_options_v1* o,
+                                                         bf200_path_result_v1* device_results,
+                                                         bf200_report_v1* report) noexcept {
+    return trace_batch_device(c, s, device_inputs, nullptr, path_count, o, device_results, nullptr, report);
+}
+
+BF200_EXPORT blackframe_status bf200_trace_paths_with_cones_device(
+    bf200_context* c, const bf200_scene* s, const bf200_path_input_v1* device_inputs,
+    const bf200_ray_cone_v1* device_primary_cones, uint64_t path_count, const bf200_transport_options_v1* o,
+    bf200_path_result_v1* device_results, bf200_ray_cone_v1* device_terminal_cones, bf200_report_v1* report) noexcept {
+    if (path_count != 0 && (device_primary_cones == nullptr || device_terminal_cones == nullptr)) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    return trace_batch_device(c, s, device_inputs, reinterpret_cast<const float2*>(device_primary_cones), path_count,
+                              o, device_results, reinterpret_cast<float2*>(device_terminal_cones), report);
+}
+
+BF200_EXPORT blackframe_status bf200_trace_paths_with_cones(bf200_context* c, const bf200_scene* s,
+                                                             const bf200_path_input_v1* inputs,
+                                                             const bf200_ray_cone_v1* primary_cones,
+                                                             uint64_t path_count, const bf200_transport_options_v1* o,
+                                                             bf200_path_result_v1* results,
+                                                             bf200_ray_cone_v1* terminal_cones,
+                                                             bf200_report_v1* report) noexcept {
+    if (c == nullptr || s == nullptr ||
+        (path_count != 0 && (inputs == nullptr || results == nullptr || primary_cones == nullptr ||
+                             terminal_cones == nullptr))) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    // every primary cone finite and non-negative (WavefrontTransport.cpp:524-531)
+    for (uint64_t i = 0; i < path_count; ++i) {
+        const bf200_ray_cone_v1& cone = primary_cones[i];
+        if (!std::isfinite(cone.width) || cone.width < 0.0F || !std::isfinite(cone.spread) || cone.spread < 0.0F) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
+                        "path " + std::to_string(i) + " has a primary ray cone that is not finite and non-negative");
+        }
+    }
+    return trace_batch_host(c, s, inputs, primary_cones, path_count, o, results, terminal_cones, report);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2226,35 +2406,7 @@ BF200_EXPORT blackframe_status bf200_trace_paths(bf200_context* c, const bf200_s
     if (c == nullptr || s == nullptr || (path_count != 0 && (inputs == nullptr || results == nullptr))) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
     }
-    if (path_count == 0) {
-        return bf200_trace_paths_device(c, s, nullptr, 0, o, nullptr, report);
-    }
-    cudaSetDevice(c->device);
-    const size_t in_bytes = path_count * sizeof(bf200_path_input_v1);
-    const size_t in_span = (in_bytes + 255) & ~size_t(255);
-    if (const auto st = grow_workspace(c, &c->batch_staging, &c->batch_staging_bytes,
-                                       in_span + path_count * sizeof(bf200_path_result_v1), "batch staging");
-        st != BLACKFRAME_STATUS_SUCCESS) {
-        return st;
-    }
-    auto* d_in = static_cast<bf200_path_input_v1*>(c->batch_staging);
-    auto* d_out = reinterpret_cast<bf200_path_result_v1*>(static_cast<char*>(c->batch_staging) + in_span);
-    cudaError_t e = cudaMemcpyAsync(d_in, inputs, in_bytes, cudaMemcpyHostToDevice, c->stream);
-    blackframe_status st = e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "batch upload");
-    if (st == BLACKFRAME_STATUS_SUCCESS) {
-        st = bf200_trace_paths_device(c, s, d_in, path_count, o, d_out, report);
-    }
-    if (st == BLACKFRAME_STATUS_SUCCESS) {
-        e = cudaMemcpyAsync(results, d_out, path_count * sizeof(bf200_path_result_v1), cudaMemcpyDeviceToHost,
-                            c->stream);
-        if (e == cudaSuccess) {
-            e = cudaStreamSynchronize(c->stream);
-        }
-        if (e != cudaSuccess) {
-            st = cuda_fail(c, e, "batch download");
-        }
-    }
-    return st;
+    return trace_batch_host(c, s, inputs, nullptr, path_count, o, results, nullptr, report);
 }
 
 BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const bf200_scene* s,
@@ -3143,3 +3295,4 @@ static_assert(sizeof(bf200_ray_v1) == 48, "ray layout");
 static_assert(sizeof(bf200_material_gradient_v1) == kAdjointStride * sizeof(double), "gradient record layout");
 static_assert(sizeof(bf200_adjoint_v1) == 40, "adjoint request layout");
 static_assert(sizeof(bf200_instance_v1) == 160, "instance layout");
+static_assert(sizeof(bf200_ray_cone_v1) == sizeof(float2), "ray cone layout (the device cone column is float2)");

@@ -886,6 +886,14 @@ __device__ bool start_path(const Wavefront& w, const PathSource& src, uint32_t s
         tmin = in.primary_ray.t_min;
         tmax = in.primary_ray.t_max;
         mask = in.primary_ray.mask;
+        if (src.cones_in != nullptr) {
+            // the camera stage's valid_ray_cone check (CudaWavefrontStages.cu:1378-1380)
+            const float2 cone = src.cones_in[id];
+            w.cone[slot] = cone;
+            if (!cone_valid(cone)) {
+                lane.fail();
+            }
+        }
     }
     w.path_id[slot] = id;
     w.ray_o[slot] = make_float4(o.x, o.y, o.z, tmax);
@@ -949,6 +957,9 @@ __device__ void finish_path(const Wavefront& w, const PathSource& src, uint32_t 
     r.terminal_ray.medium = 0U;
     r.terminal_ray.reserved = 0U;
     src.results[id] = r;
+    if (src.cones_out != nullptr) {
+        src.cones_out[id] = w.cone[slot];  // defined at the terminal ray's origin
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1685,7 +1696,9 @@ __device__ __forceinline__ void adjoint_flush(double* sum, double* gradients) {
 // One launch per route: K is the closure kind the route's slots all share (0: generic route,
 // misses and any other material). The route queue lists the route's slots in slot order.
 // ADJ: the replay of the path-replay adjoint (`a` is read only then).
-template <int K, bool ADJ>
+// K: closure kind (0 reads it from the record); ADJ: path-replay adjoint; CONE: the slots carry ray
+// cones (the cone column is read and written only then).
+template <int K, bool ADJ, bool CONE>
 __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView s, Wavefront w, PathSource src, TransportParams p,
                                                uint32_t route, AdjointView a) {
     __shared__ double adjoint_sum[ADJ ? kAdjointWords : 1];
@@ -1934,7 +1947,18 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                             if (origin == surf.position) {
                                 lane.fail();
                             }
+                            // the continuation's ray cone: advanced to this hit, then scattered
+                            // (CudaWavefrontStages.cu:4606-4623)
+                            float2 next_cone = make_float2(0.0F, 0.0F);
+                            if (CONE && lane.err == 0 &&
+                                (!cone_advance(w.cone[slot], rd, tb.x, next_cone) ||
+                                 !cone_scatter<K>(next_cone, closure, bs.lobes, wo, bs.wi, next_cone))) {
+                                lane.fail();
+                            }
                             if (lane.err == 0) {
+                                if constexpr (CONE) {
+                                    w.cone[slot] = next_cone;
+                                }
                                 beta = make_float4(nb[0], nb[1], nb[2], nb[3]);
                                 w.beta[slot] = beta;
                                 w.depth[slot] = next_depth;
@@ -2303,13 +2327,15 @@ cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instanc
     return cudaGetLastError();
 }
 
-template <bool ADJ>
+template <bool ADJ, bool CONE>
 void launch_shading(const SceneView& s, const Wavefront& w, const PathSource& src, const TransportParams& p,
                     uint32_t grid, const AdjointView& a, cudaStream_t stream) {
-    k_shade<0, ADJ><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteGeneric, a);
-    k_shade<static_cast<int>(kClosureLambert), ADJ><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteLambert, a);
-    k_shade<static_cast<int>(kClosureConductor), ADJ><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteConductor, a);
-    k_shade<static_cast<int>(kClosureDielectric), ADJ><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteDielectric, a);
+    k_shade<0, ADJ, CONE><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteGeneric, a);
+    k_shade<static_cast<int>(kClosureLambert), ADJ, CONE><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteLambert, a);
+    k_shade<static_cast<int>(kClosureConductor), ADJ, CONE><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteConductor,
+                                                                                      a);
+    k_shade<static_cast<int>(kClosureDielectric), ADJ, CONE><<<grid, 256, 0, stream>>>(s, w, src, p,
+                                                                                       kRouteDielectric, a);
 }
 
 cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
@@ -2338,9 +2364,11 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
             return e;
         }
         if (adjoint != nullptr) {
-            launch_shading<true>(s, w, src, p, grid, *adjoint, stream);
+            launch_shading<true, false>(s, w, src, p, grid, *adjoint, stream);
+        } else if (src.cones_in != nullptr) {
+            launch_shading<false, true>(s, w, src, p, grid, AdjointView{}, stream);
         } else {
-            launch_shading<false>(s, w, src, p, grid, AdjointView{}, stream);
+            launch_shading<false, false>(s, w, src, p, grid, AdjointView{}, stream);
         }
         *launches += 4U;
         if ((e = cudaGetLastError()) != cudaSuccess) {

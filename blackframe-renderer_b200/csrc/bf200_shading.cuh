@@ -1214,6 +1214,140 @@ __device__ __forceinline__ bool kind_is(const ClosureData& c, uint32_t kind) {
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Ray cones of the wavefront transport (CudaWavefrontStages.cu:540-543, 2803-2870, 3675-3781; the
+// CPU twin is RayCone.hpp). A cone is (width, spread): its radius at the ray origin and its radial
+// slope. It advances to a hit as width + spread * distance and is re-spread at every scattering
+// event by the selected closure's footprint policy (unit slope for diffuse, max(alpha_x, alpha_y)
+// for GGX, Snell's singular values through a refraction). Every product and ratio is checked as
+// the reference checks it: a non-finite result, or two non-zero factors whose product underflows
+// to zero, fails the lane.
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ bool cone_valid(float2 cone) {
+    return isfinite(cone.x) && cone.x >= 0.0F && isfinite(cone.y) && cone.y >= 0.0F;
+}
+
+__device__ __forceinline__ bool cone_product(float left, float right, float& product) {
+    product = left * right;
+    return isfinite(product) && !(left != 0.0F && right != 0.0F && product == 0.0F);
+}
+
+__device__ __forceinline__ bool cone_ratio(float numerator, float denominator, float& ratio) {
+    if (!isfinite(numerator) || !(numerator > 0.0F) || !isfinite(denominator) || !(denominator > 0.0F)) {
+        return false;
+    }
+    ratio = numerator / denominator;
+    return isfinite(ratio) && ratio > 0.0F;
+}
+
+// advance_ray_cone_to_hit: the cone carried from the ray origin to the hit at parameter t of a ray
+// whose direction d need not be unit (its length taken as max|d| * |d / max|d||).
+static __device__ bool cone_advance(float2 cone, F3 d, float t, float2& out) {
+    if (!cone_valid(cone) || !isfinite(t) || t < 0.0F) {
+        return false;
+    }
+    const float scale = fmaxf(fabsf(d.x), fmaxf(fabsf(d.y), fabsf(d.z)));
+    if (!isfinite(scale) || !(scale > 0.0F)) {
+        return false;
+    }
+    const float inverse = 1.0F / scale;
+    const float sx = d.x * inverse, sy = d.y * inverse, sz = d.z * inverse;
+    const float normalized_length = sqrtf(fmaf(sx, sx, fmaf(sy, sy, sz * sz)));
+    float length = 0.0F, distance = 0.0F, growth = 0.0F;
+    if (!isfinite(normalized_length) || !(normalized_length > 0.0F) ||
+        !cone_product(scale, normalized_length, length) || !(length > 0.0F)) {
+        return false;
+    }
+    if (!cone_product(t, length, distance) || distance < 0.0F || !cone_product(cone.y, distance, growth)) {
+        return false;
+    }
+    const float width = fmaf(cone.y, distance, cone.x);
+    if (!isfinite(width) || width < cone.x || (growth != 0.0F && width == cone.x)) {
+        return false;
+    }
+    out = make_float2(width, cone.y);
+    return cone_valid(out);
+}
+
+// unit_vector (TransportDevice.cuh:325-333): squared length within 128 ulp of one
+__device__ __forceinline__ bool cone_unit(F3 v) {
+    if (!finite3(v)) {
+        return false;
+    }
+    const float squared = fmaf(v.x, v.x, fmaf(v.y, v.y, v.z * v.z));
+    return isfinite(squared) && fabsf(squared - 1.0F) <= 128.0F * kEps;
+}
+
+// valid_surface_event: exactly one lobe family and one direction, no volume lobe
+__device__ __forceinline__ bool cone_surface_event(uint32_t bits) {
+    const uint32_t family = bits & (kLobeDiffuse | kLobeGlossy | kLobeSpecular);
+    const uint32_t direction = bits & (kLobeReflection | kLobeTransmission);
+    return bits != 0U && (bits & ~0x3FU) == 0U && (bits & kLobeVolume) == 0U &&
+           (family == kLobeDiffuse || family == kLobeGlossy || family == kLobeSpecular) &&
+           (direction == kLobeReflection || direction == kLobeTransmission);
+}
+
+// propagate_ray_cone_scattering: the cone after the closure `c` scattered wo (local, outgoing)
+// into wi (local, incoming) with the sampled event lobes.
+template <int K>
+__device__ bool cone_scatter(float2 cone, const ClosureData& c, uint32_t event, F3 wo, F3 wi, float2& out) {
+    if (!cone_valid(cone) || !cone_surface_event(event) || !cone_unit(wo) || !cone_unit(wi) || wo.z == 0.0F ||
+        wi.z == 0.0F) {
+        return false;
+    }
+    const bool reflection = (event & kLobeReflection) != 0U;
+    const bool transmission = (event & kLobeTransmission) != 0U;
+    const bool same_hemisphere = (wo.z > 0.0F) == (wi.z > 0.0F);
+    if ((reflection && !same_hemisphere) || (transmission && same_hemisphere)) {
+        return false;
+    }
+    float spread_floor = 0.0F, transmission_scale = 1.0F, width_scale = 1.0F;
+    bool dielectric = false;
+    if (kind_is<K>(c, kClosureLambert)) {
+        if (!reflection || (event & kLobeDiffuse) == 0U) {
+            return false;
+        }
+        spread_floor = 1.0F;
+    } else if (kind_is<K>(c, kClosureConductor)) {
+        if (!reflection || (event & kLobeGlossy) == 0U || !isfinite(c.p[8]) || c.p[8] < 0.0F ||
+            !isfinite(c.p[9]) || c.p[9] < 0.0F) {
+            return false;
+        }
+        spread_floor = fmaxf(c.p[8], c.p[9]);
+    } else if (kind_is<K>(c, kClosureDielectric)) {
+        if ((event & kLobeGlossy) == 0U || !isfinite(c.p[2]) || c.p[2] < 0.0F || !isfinite(c.p[3]) ||
+            c.p[3] < 0.0F) {
+            return false;
+        }
+        spread_floor = fmaxf(c.p[2], c.p[3]);
+        dielectric = true;
+    } else {
+        return false;
+    }
+    if (transmission) {
+        if (!dielectric) {
+            return false;
+        }
+        const float incident = wo.z > 0.0F ? c.p[0] : c.p[1];
+        const float transmitted = wo.z > 0.0F ? c.p[1] : c.p[0];
+        float eta_ratio = 0.0F, cosine_ratio = 0.0F, inverse_cosine_ratio = 0.0F, meridional = 0.0F;
+        if (!cone_ratio(incident, transmitted, eta_ratio) || !cone_ratio(fabsf(wo.z), fabsf(wi.z), cosine_ratio) ||
+            !cone_ratio(fabsf(wi.z), fabsf(wo.z), inverse_cosine_ratio) ||
+            !cone_product(eta_ratio, cosine_ratio, meridional)) {
+            return false;
+        }
+        transmission_scale = fmaxf(eta_ratio, meridional);
+        width_scale = fmaxf(1.0F, inverse_cosine_ratio);
+    }
+    float width = 0.0F, spread = 0.0F;
+    if (!cone_product(cone.x, width_scale, width) || !cone_product(cone.y, transmission_scale, spread)) {
+        return false;
+    }
+    out = make_float2(width, fmaxf(spread, spread_floor));
+    return cone_valid(out);
+}
+
 template <int K>
 static __device__ void closure_eval(const ClosureData& c, uint32_t allowed, F3 wo, F3 wi, float (&out)[4], Lane& lane) {
     if (kind_is<K>(c, kClosureLambert)) {  // LambertianReflection.hpp:76-85

@@ -458,6 +458,34 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths(
     uint64_t path_count, const bf200_transport_options_v1* options,
     bf200_path_result_v1* results, bf200_report_v1* report) BF200_NOEXCEPT;
 
+/* renderer::RayCone (RayCone.hpp:160-189): the cone's radius at the ray origin and its radial
+ * slope, 8 bytes (the reference's WavefrontRayCone). */
+typedef struct bf200_ray_cone_v1 {
+    float width;
+    float spread;
+} bf200_ray_cone_v1;
+
+/* bf200_trace_paths carrying every path's ray cone as the reference wavefront does:
+ * CudaWavefrontPathInput::primary_cone in, CudaWavefrontTransportBatch::terminal_cones out
+ * (WavefrontTransport.hpp:27-32, 127-132). The cone advances to every hit and is re-spread by the
+ * selected closure at every scattering event (CudaWavefrontStages.cu:2832-2870, 3675-3781);
+ * terminal_cones[i] is the cone at results[i].terminal_ray's origin. A primary cone that is not
+ * finite and non-negative refuses the whole call with INVALID_ARGUMENT
+ * (WavefrontTransport.cpp:524-531); a cone that becomes unrepresentable fails its lane with
+ * BF200_LANE_NUMERICAL_FAILURE, as the reference's shade stage does. Path results are identical
+ * to bf200_trace_paths for every lane that does not fail. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_with_cones(
+    bf200_context* context, const bf200_scene* scene, const bf200_path_input_v1* inputs,
+    const bf200_ray_cone_v1* primary_cones, uint64_t path_count, const bf200_transport_options_v1* options,
+    bf200_path_result_v1* results, bf200_ray_cone_v1* terminal_cones, bf200_report_v1* report) BF200_NOEXCEPT;
+/* The same with inputs, cones and results in device memory; an invalid primary cone fails its
+ * lane instead of the call (the camera stage's check, CudaWavefrontStages.cu:1378-1380). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_with_cones_device(
+    bf200_context* context, const bf200_scene* scene, const bf200_path_input_v1* device_inputs,
+    const bf200_ray_cone_v1* device_primary_cones, uint64_t path_count, const bf200_transport_options_v1* options,
+    bf200_path_result_v1* device_results, bf200_ray_cone_v1* device_terminal_cones,
+    bf200_report_v1* report) BF200_NOEXCEPT;
+
 /* Same as bf200_trace_paths with inputs and results in device memory. */
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_device(
     bf200_context* context, const bf200_scene* scene, const bf200_path_input_v1* device_inputs,

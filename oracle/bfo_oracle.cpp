@@ -2458,7 +2458,153 @@ struct PathOut {
     uint32_t delta_flags, termination, blocked, segments;
     V3 ray_o, ray_d;
     float ray_tmin, ray_tmax;
+    float cone_width = 0.0F, cone_spread = 0.0F;  // the ray cone at ray_o (traced with cones only)
 };
+
+// ---------------------------------------------------------------------------------------------
+// Ray cones of the reference's wavefront (CudaWavefrontStages.cu:540-543, 2816-2870, 3675-3781;
+// the CPU twin is RayCone.hpp:133-156, 222-240, 316-437, which measures the direction with
+// std::hypot and tests unit directions to 256 ulp where the wavefront uses max|d| * |d / max|d||
+// and 128 ulp). Every product and ratio is checked: not finite, or non-zero factors whose
+// product underflows to zero, is a failure.
+// ---------------------------------------------------------------------------------------------
+
+bool cone_valid(float width, float spread) {
+    return std::isfinite(width) && width >= 0.0F && std::isfinite(spread) && spread >= 0.0F;
+}
+
+bool cone_product(float left, float right, float& product) {  // checked_ray_cone_product
+    product = left * right;
+    return std::isfinite(product) && !(left != 0.0F && right != 0.0F && product == 0.0F);
+}
+
+bool cone_ratio(float numerator, float denominator, float& ratio) {  // checked_ray_cone_ratio
+    if (!std::isfinite(numerator) || !(numerator > 0.0F) || !std::isfinite(denominator) ||
+        !(denominator > 0.0F)) {
+        return false;
+    }
+    ratio = numerator / denominator;
+    return std::isfinite(ratio) && ratio > 0.0F;
+}
+
+// advance_ray_cone_to_hit (CudaWavefrontStages.cu:2832-2870)
+bool cone_advance(float width, float spread, V3 d, float t, float& out_width) {
+    if (!cone_valid(width, spread) || !std::isfinite(t) || t < 0.0F) {
+        return false;
+    }
+    const float scale = std::fmax(std::fabs(d.x), std::fmax(std::fabs(d.y), std::fabs(d.z)));
+    if (!std::isfinite(scale) || !(scale > 0.0F)) {
+        return false;
+    }
+    const float inverse = 1.0F / scale;
+    const float sx = d.x * inverse, sy = d.y * inverse, sz = d.z * inverse;
+    const float normalized_length = std::sqrt(std::fma(sx, sx, std::fma(sy, sy, sz * sz)));
+    float length = 0.0F, distance = 0.0F, growth = 0.0F;
+    if (!std::isfinite(normalized_length) || !(normalized_length > 0.0F) ||
+        !cone_product(scale, normalized_length, length) || !(length > 0.0F)) {
+        return false;
+    }
+    if (!cone_product(t, length, distance) || distance < 0.0F || !cone_product(spread, distance, growth)) {
+        return false;
+    }
+    const float advanced = std::fma(spread, distance, width);
+    if (!std::isfinite(advanced) || advanced < width || (growth != 0.0F && advanced == width)) {
+        return false;
+    }
+    out_width = advanced;
+    return cone_valid(advanced, spread);
+}
+
+// transport::unit_vector (TransportDevice.cuh:325-333)
+bool cone_unit(V3 v) {
+    if (!std::isfinite(v.x) || !std::isfinite(v.y) || !std::isfinite(v.z)) {
+        return false;
+    }
+    const float squared = std::fma(v.x, v.x, std::fma(v.y, v.y, v.z * v.z));
+    return std::isfinite(squared) && std::fabs(squared - 1.0F) <= 128.0F * kEpsilon;
+}
+
+// valid_surface_event (CudaWavefrontStages.cu:2803-2814)
+bool cone_surface_event(uint32_t bits) {
+    const uint32_t family = bits & 0x07U, direction = bits & 0x18U;
+    return bits != 0U && (bits & ~0x3FU) == 0U && (bits & 0x20U) == 0U &&
+           (family == 0x01U || family == 0x02U || family == 0x04U) && (direction == 0x08U || direction == 0x10U);
+}
+
+// propagate_ray_cone_scattering (CudaWavefrontStages.cu:3675-3781). Closure kinds follow
+// ClosureKind: 1 lambertian, 2 rough diffuse, 3 rough conductor, 4 rough dielectric,
+// 5 specular reflection, 6 specular transmission.
+bool cone_scatter(float width, float spread, uint32_t kind, const float* p, uint32_t event, V3 wo, V3 wi,
+                  float& out_width, float& out_spread) {
+    if (!cone_valid(width, spread) || !cone_surface_event(event) || !cone_unit(wo) || !cone_unit(wi) ||
+        wo.z == 0.0F || wi.z == 0.0F) {
+        return false;
+    }
+    const bool reflection = (event & 0x08U) != 0U, transmission = (event & 0x10U) != 0U;
+    const bool same_hemisphere = (wo.z > 0.0F) == (wi.z > 0.0F);
+    if ((reflection && !same_hemisphere) || (transmission && same_hemisphere)) {
+        return false;
+    }
+    float spread_floor = 0.0F, transmission_scale = 1.0F, width_scale = 1.0F;
+    switch (kind) {
+    case 1U:
+    case 2U:
+        if (!reflection || (event & 0x01U) == 0U) {
+            return false;
+        }
+        spread_floor = 1.0F;
+        break;
+    case 3U:
+        if (!reflection || (event & 0x02U) == 0U || !std::isfinite(p[8]) || p[8] < 0.0F ||
+            !std::isfinite(p[9]) || p[9] < 0.0F) {
+            return false;
+        }
+        spread_floor = std::fmax(p[8], p[9]);
+        break;
+    case 4U:
+        if ((event & 0x02U) == 0U || !std::isfinite(p[2]) || p[2] < 0.0F || !std::isfinite(p[3]) || p[3] < 0.0F) {
+            return false;
+        }
+        spread_floor = std::fmax(p[2], p[3]);
+        break;
+    case 5U:
+        if (!reflection || (event & 0x04U) == 0U) {
+            return false;
+        }
+        break;
+    case 6U:
+        if (!transmission || (event & 0x04U) == 0U) {
+            return false;
+        }
+        break;
+    default:
+        return false;
+    }
+    if (transmission) {
+        if (kind != 4U && kind != 6U) {
+            return false;
+        }
+        const float incident = wo.z > 0.0F ? p[0] : p[1];
+        const float transmitted = wo.z > 0.0F ? p[1] : p[0];
+        float eta_ratio = 0.0F, cosine_ratio = 0.0F, inverse_cosine_ratio = 0.0F, meridional = 0.0F;
+        if (!cone_ratio(incident, transmitted, eta_ratio) ||
+            !cone_ratio(std::fabs(wo.z), std::fabs(wi.z), cosine_ratio) ||
+            !cone_ratio(std::fabs(wi.z), std::fabs(wo.z), inverse_cosine_ratio) ||
+            !cone_product(eta_ratio, cosine_ratio, meridional)) {
+            return false;
+        }
+        transmission_scale = std::fmax(eta_ratio, meridional);
+        width_scale = std::fmax(1.0F, inverse_cosine_ratio);
+    }
+    float scattered_width = 0.0F, scattered_spread = 0.0F;
+    if (!cone_product(width, width_scale, scattered_width) ||
+        !cone_product(spread, transmission_scale, scattered_spread)) {
+        return false;
+    }
+    out_width = scattered_width;
+    out_spread = std::fmax(scattered_spread, spread_floor);
+    return cone_valid(out_width, out_spread);
+}
 
 // SceneMisPathLoop.cpp:129-275 (estimate): returns the unoccluded-tested direct contribution.
 Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& surf,
@@ -2549,7 +2695,10 @@ Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& 
     return out;
 }
 
-PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Options& opt) {
+// cone: null, or the path's primary ray cone (width, spread), carried as the reference's wavefront
+// carries it (CudaWavefrontStages.cu:4602-4624) and returned in PathOut::cone_*.
+PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Options& opt,
+              const float* cone = nullptr) {
     PathOut out{};
     out.beta = Spectrum{1.0F, 1.0F, 1.0F, 1.0F};
     out.radiance = Spectrum{};
@@ -2566,6 +2715,13 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
     float tmin = input.primary_ray.t_min, tmax = input.primary_ray.t_max;
     const uint32_t mask = input.primary_ray.mask;
     const float time = input.primary_ray.time;
+    if (cone != nullptr) {
+        out.cone_width = cone[0];
+        out.cone_spread = cone[1];
+        if (!cone_valid(out.cone_width, out.cone_spread)) {
+            fail("A primary ray cone must be finite and non-negative.");
+        }
+    }
     PrevBsdf prev;
     auto finish = [&](uint32_t termination) {
         out.termination = termination;
@@ -2704,6 +2860,14 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
         const V3 origin = offset_ray_origin(surf.position, surf.error, surf.ng, wi_world);
         if (origin == surf.position) {
             fail("The derived triangle error did not move the MIS continuation-ray origin.");
+        }
+        if (cone != nullptr) {
+            float advanced = 0.0F;
+            if (!cone_advance(out.cone_width, out.cone_spread, rd, hit.t, advanced) ||
+                !cone_scatter(advanced, out.cone_spread, closure.kind, closure.p, bs.lobes, wo, bs.wi,
+                              out.cone_width, out.cone_spread)) {
+                fail("A scattered ray cone is not representable.");
+            }
         }
         // record_bsdf_sample (SceneMisPathLoop.cpp:358-390): continuous lobes only here.
         prev.valid = true;
@@ -2922,10 +3086,10 @@ __attribute__((visibility("default"))) int bfo_scene_world_normal(void* h, uint3
 }
 
 // Traces paths; returns how many failed (lane_status 1, first message in bfo_last_error()).
-__attribute__((visibility("default"))) int64_t bfo_trace_paths(void* h, const bf200_path_input_v1* in,
-                                                               uint64_t n,
-                                                               const bf200_transport_options_v1* o,
-                                                               bf200_path_result_v1* res, int threads) {
+// cones_in / cones_out (both or neither, 2 floats per path) carry the ray cones.
+static int64_t trace_batch(void* h, const bf200_path_input_v1* in, const float* cones_in, uint64_t n,
+                    const bf200_transport_options_v1* o, bf200_path_result_v1* res, float* cones_out,
+                    int threads) {
     const auto* s = static_cast<Scene*>(h);
     const Options opt = make_options(*o);
     std::atomic<uint64_t> next{0};
@@ -2933,11 +3097,18 @@ __attribute__((visibility("default"))) int64_t bfo_trace_paths(void* h, const bf
     auto worker = [&] {
         for (uint64_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {
             try {
-                const PathOut p = trace(*s, in[i], opt);
+                const PathOut p = trace(*s, in[i], opt, cones_in != nullptr ? cones_in + 2 * i : nullptr);
                 store_result(p, res[i], in[i].primary_ray.time, in[i].primary_ray.mask);
+                if (cones_out != nullptr) {
+                    cones_out[2 * i] = p.cone_width;
+                    cones_out[2 * i + 1] = p.cone_spread;
+                }
             } catch (const Failure& f) {
                 std::memset(&res[i], 0, sizeof(res[i]));
                 res[i].lane_status = BF200_LANE_NUMERICAL_FAILURE;
+                if (cones_out != nullptr) {
+                    cones_out[2 * i] = cones_out[2 * i + 1] = 0.0F;
+                }
                 if (failures.fetch_add(1) == 0) {
                     set_error(f.message);
                 }
@@ -2956,6 +3127,62 @@ __attribute__((visibility("default"))) int64_t bfo_trace_paths(void* h, const bf
         }
     }
     return failures.load();
+}
+
+__attribute__((visibility("default"))) int64_t bfo_trace_paths(void* h, const bf200_path_input_v1* in,
+                                                               uint64_t n,
+                                                               const bf200_transport_options_v1* o,
+                                                               bf200_path_result_v1* res, int threads) {
+    return trace_batch(h, in, nullptr, n, o, res, nullptr, threads);
+}
+
+// bfo_trace_paths with ray cones (width, spread per path) in and at every terminal-ray origin out.
+__attribute__((visibility("default"))) int64_t bfo_trace_paths_cones(void* h, const bf200_path_input_v1* in,
+                                                                     const float* cones_in, uint64_t n,
+                                                                     const bf200_transport_options_v1* o,
+                                                                     bf200_path_result_v1* res, float* cones_out,
+                                                                     int threads) {
+    return trace_batch(h, in, cones_in, n, o, res, cones_out, threads);
+}
+
+// One ray-cone advance per case: cones (width, spread), ray directions, hit parameters; writes the
+// advanced width (NaN where the advance fails). Returns the number of failures.
+__attribute__((visibility("default"))) int64_t bfo_cone_advance(const float* cones, const float* directions,
+                                                                const float* parameters, uint64_t n,
+                                                                float* widths) {
+    int64_t failures = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const V3 d{directions[3 * i], directions[3 * i + 1], directions[3 * i + 2]};
+        float width = 0.0F;
+        if (!cone_advance(cones[2 * i], cones[2 * i + 1], d, parameters[i], width)) {
+            width = std::numeric_limits<float>::quiet_NaN();
+            ++failures;
+        }
+        widths[i] = width;
+    }
+    return failures;
+}
+
+// One ray-cone scattering per case: cone (width, spread), closure kind and its 10 parameters, the
+// event lobes, local wo and wi; writes (width, spread), NaN where it fails. Returns the failures.
+__attribute__((visibility("default"))) int64_t bfo_cone_scatter(const float* cones, const uint32_t* kinds,
+                                                                const float* parameters, const uint32_t* events,
+                                                                const float* wo, const float* wi, uint64_t n,
+                                                                float* out) {
+    int64_t failures = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const V3 o{wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]};
+        const V3 w{wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
+        float width = 0.0F, spread = 0.0F;
+        if (!cone_scatter(cones[2 * i], cones[2 * i + 1], kinds[i], parameters + 10 * i, events[i], o, w, width,
+                          spread)) {
+            width = spread = std::numeric_limits<float>::quiet_NaN();
+            ++failures;
+        }
+        out[2 * i] = width;
+        out[2 * i + 1] = spread;
+    }
+    return failures;
 }
 
 // Closest hits for world rays (the accel contract; AccelBackend.cpp:43-112).

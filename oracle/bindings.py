@@ -80,6 +80,21 @@ class _Checker:
         if f(handle, powers.ctypes.data_as(C.c_void_p), len(powers)) != 0:
             raise CheckerError(self.last_error())
 
+    def cone_scatter(self, cones, kinds, parameters, events, wo, wi):
+        """propagate_ray_cone_scattering per case: float32 [n, 2] of (width, spread), NaN where it
+        fails, and the failure count."""
+        import numpy as np
+        arrays = [np.ascontiguousarray(cones, np.float32), np.ascontiguousarray(kinds, np.uint32),
+                  np.ascontiguousarray(parameters, np.float32), np.ascontiguousarray(events, np.uint32),
+                  np.ascontiguousarray(wo, np.float32), np.ascontiguousarray(wi, np.float32)]
+        n = len(arrays[1])
+        out = np.zeros((n, 2), np.float32)
+        f = getattr(self.lib, self.prefix + "_cone_scatter")
+        f.argtypes = [C.c_void_p] * 6 + [C.c_uint64, C.c_void_p]
+        f.restype = C.c_int64
+        failures = f(*[a.ctypes.data_as(C.c_void_p) for a in arrays], n, out.ctypes.data_as(C.c_void_p))
+        return out, failures
+
     def trace(self, handle, inputs, options, threads=None):
         n = len(inputs)
         results = (abi.PathResult * n)()
@@ -109,6 +124,38 @@ class Oracle(_Checker):
         self.lib.bfo_sobol_bits.restype = C.c_uint64
         self.lib.bfo_owen_sobol_bits.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]
         self.lib.bfo_owen_sobol_bits.restype = C.c_uint64
+
+    def cone_advance(self, cones, directions, parameters):
+        """advance_ray_cone_to_hit per case: the advanced widths (NaN where it fails) and the
+        failure count."""
+        import numpy as np
+        cones = np.ascontiguousarray(cones, np.float32)
+        directions = np.ascontiguousarray(directions, np.float32)
+        parameters = np.ascontiguousarray(parameters, np.float32)
+        out = np.zeros(len(parameters), np.float32)
+        f = self.lib.bfo_cone_advance
+        f.argtypes = [C.c_void_p] * 3 + [C.c_uint64, C.c_void_p]
+        f.restype = C.c_int64
+        failures = f(cones.ctypes.data_as(C.c_void_p), directions.ctypes.data_as(C.c_void_p),
+                     parameters.ctypes.data_as(C.c_void_p), len(parameters), out.ctypes.data_as(C.c_void_p))
+        return out, failures
+
+    def trace_cones(self, handle, inputs, cones, options, threads=None):
+        """trace() carrying ray cones: (results, terminal cones float32 [n, 2], failures)."""
+        import numpy as np
+        n = len(inputs)
+        cones = np.ascontiguousarray(cones, np.float32).reshape(n, 2)
+        results = (abi.PathResult * n)()
+        out = np.zeros((n, 2), np.float32)
+        f = self.lib.bfo_trace_paths_cones
+        f.argtypes = [C.c_void_p, C.POINTER(abi.PathInput), C.c_void_p, C.c_uint64, C.POINTER(abi.TransportOptions),
+                      C.POINTER(abi.PathResult), C.c_void_p, C.c_int]
+        f.restype = C.c_int64
+        failures = f(handle, inputs, cones.ctypes.data_as(C.c_void_p), n, C.byref(options), results,
+                     out.ctypes.data_as(C.c_void_p), threads or os.cpu_count() or 1)
+        if failures < 0:
+            raise CheckerError(self.last_error())
+        return results, out, failures
 
     def camera_rays(self, camera, samples, sampler=0):
         rays = (abi.Ray * len(samples))()
@@ -162,6 +209,32 @@ class Reference(_Checker):
         if code != 0:
             return None, code
         return (probabilities, selected, selected_probability), 0
+
+    def cone_advance(self, cones, distances):
+        """renderer::advance_ray_cone(cone, distance) per case: widths (NaN on error), errors."""
+        import numpy as np
+        cones = np.ascontiguousarray(cones, np.float32)
+        distances = np.ascontiguousarray(distances, np.float32)
+        out = np.zeros(len(distances), np.float32)
+        f = self.lib.bfr_cone_advance
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]
+        f.restype = C.c_int64
+        failures = f(cones.ctypes.data_as(C.c_void_p), distances.ctypes.data_as(C.c_void_p), len(distances),
+                     out.ctypes.data_as(C.c_void_p))
+        return out, failures
+
+    def camera_cones(self, origin, normal, tangent, width, height, vfov, time, samples):
+        """PinholeCamera::generate_primary_ray_cone for every sample: float32 [n, 2]."""
+        import numpy as np
+        out = np.zeros((len(samples), 2), np.float32)
+        f = self.lib.bfr_camera_cones
+        f.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_uint32, C.c_uint32, C.c_float, C.c_float,
+                                                  C.POINTER(abi.SampleIndex), C.c_uint64, C.c_void_p]
+        f.restype = C.c_int
+        if f(self._f3(origin), self._f3(normal), self._f3(tangent), width, height, vfov, time, samples,
+             len(samples), out.ctypes.data_as(C.c_void_p)) != 0:
+            raise CheckerError(self.last_error())
+        return out
 
     def load_mesh(self, path):
         """The reference's own OBJ/PLY loader: (positions, normals, uvs, triangles) as numpy arrays,

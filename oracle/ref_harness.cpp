@@ -31,6 +31,7 @@
 #include <Blackframe/Renderer/LightSampler.hpp>
 #include <Blackframe/Renderer/OwenScrambling.hpp>
 #include <Blackframe/Renderer/PinholeCamera.hpp>
+#include <Blackframe/Renderer/RayCone.hpp>
 #include <Blackframe/Renderer/Sphere.hpp>
 #include <Blackframe/Renderer/WavelengthSampling.hpp>
 
@@ -483,6 +484,104 @@ bfr_camera_rays(const float* origin, const float* normal, const float* tangent, 
         store_ray(*ray, rays[index]);
     }
     return 0;
+}
+
+// Reference primary ray cones (PinholeCamera::generate_primary_ray_cone through the ray
+// differential, RayCone.hpp:194-220) for (pixel, sample) indices with uniform jitter: 2 floats
+// (width, spread) per sample.
+__attribute__((visibility("default"))) int
+bfr_camera_cones(const float* origin, const float* normal, const float* tangent, uint32_t width,
+                 uint32_t height, float vfov, float time, const bf200_sample_index_v1* samples,
+                 uint64_t count, float* cones) {
+    const auto frame = renderer::OrthonormalFrame::from_normal_and_tangent(
+        renderer::Normal3{.x = normal[0], .y = normal[1], .z = normal[2]},
+        renderer::Vector3{.x = tangent[0], .y = tangent[1], .z = tangent[2]});
+    const auto camera = renderer::PinholeCamera::create(
+        renderer::Point3{.x = origin[0], .y = origin[1], .z = origin[2]}, *frame,
+        renderer::RenderExtent{.width = width, .height = height}, vfov, 0.0F,
+        std::numeric_limits<float>::infinity(), renderer::AllRayVisibility,
+        renderer::VacuumMedium);
+    if (!camera) {
+        set_error(camera.error().message);
+        return 1;
+    }
+    for (uint64_t index = 0; index < count; ++index) {
+        const auto pixel_sample = renderer::PixelSampleIndex{
+            .pixel_x = samples[index].pixel_x,
+            .pixel_y = samples[index].pixel_y,
+            .sample_index = samples[index].sample_index,
+            .seed = samples[index].seed,
+        };
+        const auto sample = renderer::generate_pixel_sample<float>(pixel_sample, renderer::PixelJitterMode::uniform);
+        if (!sample) {
+            set_error(sample.error().message);
+            return 2;
+        }
+        const auto cone = camera->generate_primary_ray_cone(*sample, time);
+        if (!cone) {
+            set_error(cone.error().message);
+            return 3;
+        }
+        cones[2 * index] = cone->width();
+        cones[2 * index + 1] = cone->spread();
+    }
+    return 0;
+}
+
+// renderer::advance_ray_cone(cone, distance) (RayCone.hpp:222-241) per case: the advanced width,
+// NaN where the reference returns an error. Returns the number of errors.
+__attribute__((visibility("default"))) int64_t bfr_cone_advance(const float* cones, const float* distances,
+                                                                uint64_t count, float* widths) {
+    int64_t failures = 0;
+    for (uint64_t i = 0; i < count; ++i) {
+        widths[i] = std::numeric_limits<float>::quiet_NaN();
+        const auto cone = renderer::RayCone::create(cones[2 * i], cones[2 * i + 1]);
+        if (!cone) {
+            ++failures;
+            continue;
+        }
+        const auto advanced = renderer::advance_ray_cone(*cone, distances[i]);
+        if (!advanced) {
+            ++failures;
+            continue;
+        }
+        widths[i] = advanced->width();
+    }
+    return failures;
+}
+
+// renderer::propagate_ray_cone_scattering (RayCone.hpp:316-437) per case: closure kind, lobes
+// and 10 parameters, event lobes, local wo and wi; (width, spread), NaN where the reference
+// returns an error. Returns the number of errors.
+__attribute__((visibility("default"))) int64_t bfr_cone_scatter(const float* cones, const uint32_t* kinds,
+                                                                const float* parameters, const uint32_t* events,
+                                                                const float* wo, const float* wi, uint64_t count,
+                                                                float* out) {
+    int64_t failures = 0;
+    for (uint64_t i = 0; i < count; ++i) {
+        out[2 * i] = out[2 * i + 1] = std::numeric_limits<float>::quiet_NaN();
+        const auto cone = renderer::RayCone::create(cones[2 * i], cones[2 * i + 1]);
+        if (!cone) {
+            ++failures;
+            continue;
+        }
+        renderer::Closure closure{};
+        closure.kind = static_cast<renderer::ClosureKind>(kinds[i]);
+        for (std::size_t k = 0; k < 10; ++k) {
+            closure.parameters[k] = parameters[10 * i + k];
+        }
+        const auto scattered = renderer::propagate_ray_cone_scattering(
+            *cone, closure, static_cast<renderer::ScatteringLobe>(events[i]),
+            renderer::Vector3{.x = wo[3 * i], .y = wo[3 * i + 1], .z = wo[3 * i + 2]},
+            renderer::Vector3{.x = wi[3 * i], .y = wi[3 * i + 1], .z = wi[3 * i + 2]});
+        if (!scattered) {
+            ++failures;
+            continue;
+        }
+        out[2 * i] = scattered->width();
+        out[2 * i + 1] = scattered->spread();
+    }
+    return failures;
 }
 
 // CIE 1931 sensor constants at a packet: response at each lane, lane pdf, normalisation.

@@ -104,7 +104,12 @@ def gpu_adjoint(setup, builder, spp=SPP, seed=SEED):
 
 
 def steps(value, h):
-    lo, hi = np.float32(value * (1.0 - h)), np.float32(value * (1.0 + h))
+    """Difference points value (1 -+ h). A closure weight is a reflectance, refused above 1 as
+    ClosureSet refuses it, so a weight at 1 takes the one-sided points value (1 - 2h) and value."""
+    lo, hi = value * (1.0 - h), value * (1.0 + h)
+    if hi > 1.0 >= value:
+        lo, hi = value * (1.0 - 2.0 * h), value
+    lo, hi = np.float32(lo), np.float32(hi)
     return lo, hi, float(hi) - float(lo)
 
 
