@@ -13,17 +13,17 @@
 //     with bf200_scene_create_from_soa, which validates the v4 header and content hash and builds
 //     bf200's own BLAS/TLAS; the serialized CudaSceneBvh is therefore only checked for presence
 //     and device, never read;
-//   * every batch goes through bf200_trace_paths_with_cones, which carries the primary ray cones
-//     and returns the terminal cones.
+//   * every batch goes through bf200_trace_paths_with_cones, which carries each path's depth-zero
+//     initial state (throughput, radiance, eta scale) and primary ray cone, and returns the
+//     terminal cones.
 //
 // Beyond the reference's own refusals (validate_options_and_inputs and validate_light_sampler,
 // WavefrontTransport.cpp:481-626) this backend refuses, with StatusCode::unavailable and without
-// substitution: initial path states other than PathState::create_initial (bf200 starts every path
-// with unit throughput, no radiance and unit eta scale), input wavelength packets other than the
-// scene blob's, and scenes bf200_scene_create_from_soa refuses (punctual lights, normal or bump
-// maps, textures). Lane failures fail the batch as the reference's stage audits do
-// (stage_failure, WavefrontTransport.cpp:875-922): numerical failures map to internal_error,
-// unsupported lanes to unavailable, traversal failures to incompatible.
+// substitution: input wavelength packets other than the scene blob's, and scenes
+// bf200_scene_create_from_soa refuses (punctual lights, normal or bump maps, textures). Lane
+// failures fail the batch as the reference's stage audits do (stage_failure,
+// WavefrontTransport.cpp:875-922): numerical failures map to internal_error, unsupported lanes
+// to unavailable, traversal failures to incompatible.
 //
 // The report fills the fields bf200 measures: schema, light registry and sampler, the echoed
 // options, path count, the camera/intersection/shadow lane counts, closure and light samples,
@@ -272,6 +272,7 @@ struct CudaWavefrontTransportWorkspace::Storage final {
     // host staging reused across batches
     std::vector<std::uint8_t> blob;
     std::vector<bf200_path_input_v1> inputs;
+    std::vector<bf200_path_state_v1> states;
     std::vector<bf200_ray_cone_v1> primary_cones;
     std::vector<bf200_ray_cone_v1> terminal_cones;
     std::vector<bf200_path_result_v1> results;
@@ -444,18 +445,21 @@ trace_cuda_wavefront_transport(CudaWavefrontTransportWorkspace& workspace, const
         storage.scene_hash = header.content_hash;
     }
 
-    // inputs: primary ray, sample and cone; the initial state must be PathState::create_initial
+    // inputs: primary ray, sample, cone and the depth-zero initial state
     const auto n = inputs.size();
     storage.inputs.assign(n, bf200_path_input_v1{});
+    storage.states.assign(n, bf200_path_state_v1{});
     storage.primary_cones.resize(n);
     storage.terminal_cones.resize(n);
     storage.results.resize(n);
     for (std::size_t i = 0; i < n; ++i) {
         const auto& input = inputs[i];
         const auto& state = input.initial_state;
-        bool initial = state.eta_scale() == 1.0F && state.delta_flags() == renderer::PathDeltaFlags::none;
+        auto& initial = storage.states[i];
+        initial.eta_scale = state.eta_scale();
         for (std::size_t lane = 0; lane < 4; ++lane) {
-            initial = initial && state.beta().values[lane] == 1.0F && state.accumulated_radiance().values[lane] == 0.0F;
+            initial.beta[lane] = state.beta().values[lane];
+            initial.radiance[lane] = state.accumulated_radiance().values[lane];
             const auto& w = state.wavelengths()[lane];
             if (storage.scene_nanometers[lane] != 0.0F &&
                 (w.nanometers != storage.scene_nanometers[lane] || w.probability.value != storage.scene_pdfs[lane])) {
@@ -464,12 +468,6 @@ trace_cuda_wavefront_transport(CudaWavefrontTransportWorkspace& workspace, const
                     "bf200 resolves the scene at the blob's wavelength packet; path " + std::to_string(i) +
                         " carries another packet, which is not substituted."));
             }
-        }
-        if (!initial) {
-            return std::unexpected(adapter_error(
-                core::StatusCode::unavailable,
-                "bf200 starts every path from PathState::create_initial; path " + std::to_string(i) +
-                    " supplies another depth-zero state, which is not substituted."));
         }
         auto& out = storage.inputs[i];
         const auto& ray = input.primary_ray;
@@ -509,8 +507,9 @@ trace_cuda_wavefront_transport(CudaWavefrontTransportWorkspace& workspace, const
     bf200_report_v1 report{};
     report.struct_size = sizeof(report);
     if (const auto status = bf200_trace_paths_with_cones(storage.context, storage.scene, storage.inputs.data(),
-                                                         storage.primary_cones.data(), n, &bf, storage.results.data(),
-                                                         storage.terminal_cones.data(), &report);
+                                                         storage.states.data(), storage.primary_cones.data(), n, &bf,
+                                                         storage.results.data(), storage.terminal_cones.data(),
+                                                         &report);
         status != BLACKFRAME_STATUS_SUCCESS) {
         return std::unexpected(bf200_error(storage.context, status, "trace"));
     }

@@ -194,8 +194,14 @@ class RayCone(C.Structure):
     _fields_ = [("width", C.c_float), ("spread", C.c_float)]
 
 
+class PathState(C.Structure):
+    """bf200_path_state_v1: a depth-zero initial path state."""
+    _fields_ = [("beta", C.c_float * 4), ("radiance", C.c_float * 4), ("eta_scale", C.c_float),
+                ("reserved", C.c_uint32 * 3)]
+
+
 EXPECTED_SIZES = {
-    RayCone: 8,
+    RayCone: 8, PathState: 48,
     Closure: 64, Material: 80, Geometry: 32, Instance: 160, Ray: 48, SampleIndex: 24,
     PathInput: 80, PathResult: 128, TransportOptions: 64, Camera: 88, Sensor: 80,
     FilmRequest: 40, FilmJob: 64, MeshView: 48, MaterialGradient: 64, Adjoint: 40, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,

@@ -71,7 +71,7 @@ def library():
                                                      C.c_uint32, C.POINTER(abi.Report)]
     lib.bf200_trace_paths_device_noalloc.restype = C.c_uint32
     for f in (lib.bf200_trace_paths_with_cones, lib.bf200_trace_paths_with_cones_device):
-        f.argtypes = [vp, vp, vp, vp, C.c_uint64, C.POINTER(abi.TransportOptions), vp, vp, C.POINTER(abi.Report)]
+        f.argtypes = [vp, vp, vp, vp, vp, C.c_uint64, C.POINTER(abi.TransportOptions), vp, vp, C.POINTER(abi.Report)]
         f.restype = C.c_uint32
     for name in ("bf200_render_film", "bf200_render_film_device"):
         f = getattr(lib, name)
@@ -213,9 +213,10 @@ class Context:
                                                 C.byref(report)), "trace_paths")
         return results, report
 
-    def trace_paths_with_cones(self, scene, inputs, cones, options):
-        """bf200_trace_paths_with_cones: cones is float32 [n, 2] of primary (width, spread); returns
-        (results, terminal cones float32 [n, 2], report)."""
+    def trace_paths_with_cones(self, scene, inputs, cones, options, states=None):
+        """bf200_trace_paths_with_cones: cones is float32 [n, 2] of primary (width, spread); states
+        (optional) an array of abi.PathState; returns (results, terminal cones float32 [n, 2],
+        report)."""
         import numpy as np
         n = len(inputs)
         cones = np.ascontiguousarray(cones, np.float32).reshape(n, 2)
@@ -224,19 +225,21 @@ class Context:
         report = abi.Report()
         report.struct_size = C.sizeof(abi.Report)
         self._check(library().bf200_trace_paths_with_cones(
-            self.handle, scene.handle, C.cast(inputs, C.c_void_p), cones.ctypes.data_as(C.c_void_p), n,
+            self.handle, scene.handle, C.cast(inputs, C.c_void_p),
+            C.cast(states, C.c_void_p) if states is not None else None, cones.ctypes.data_as(C.c_void_p), n,
             C.byref(options), C.cast(results, C.c_void_p), terminal.ctypes.data_as(C.c_void_p), C.byref(report)),
             "trace_paths_with_cones")
         return results, terminal, report
 
     def trace_paths_with_cones_device(self, scene, device_inputs, device_cones, path_count, options,
-                                      device_results, device_terminal_cones):
-        """bf200_trace_paths_with_cones_device: every array is a device pointer (int)."""
+                                      device_results, device_terminal_cones, device_states=None):
+        """bf200_trace_paths_with_cones_device: every array is a device pointer (int); device_states
+        may be None (every path starts from the initial state)."""
         report = abi.Report()
         report.struct_size = C.sizeof(abi.Report)
         self._check(library().bf200_trace_paths_with_cones_device(
-            self.handle, scene.handle, device_inputs, device_cones, path_count, C.byref(options), device_results,
-            device_terminal_cones, C.byref(report)), "trace_paths_with_cones_device")
+            self.handle, scene.handle, device_inputs, device_states, device_cones, path_count, C.byref(options),
+            device_results, device_terminal_cones, C.byref(report)), "trace_paths_with_cones_device")
         return report
 
     def trace_paths_device(self, scene, device_inputs, path_count, options, device_results):

@@ -130,6 +130,8 @@ struct PathSource {
     // every result's terminal-ray origin; both null when the caller traces without cones
     const float2* cones_in;
     float2* cones_out;
+    // batch mode: depth-zero initial states (beta, radiance, eta scale); null = PathState::create_initial
+    const bf200_path_state_v1* states_in;
     // sampler: null for the hash SampleStream; otherwise the Owen-scrambled Sobol direction heads
     // (kDeviceSobolDimensions x 64 leading 32-bit direction numbers)
     const uint32_t* sobol;

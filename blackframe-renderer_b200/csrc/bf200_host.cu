@@ -2096,10 +2096,12 @@ BF200_EXPORT blackframe_status bf200_scene_destroy(bf200_scene* s) noexcept {
 
 namespace {
 
-// The batch trace from device inputs to device results; cones_in / cones_out (both or neither)
-// carry every path's ray cone through the wavefront.
+// The batch trace from device inputs to device results. cones_in / cones_out (both or neither)
+// carry every path's ray cone through the wavefront; states_in (optional) gives every path's
+// depth-zero initial state.
 blackframe_status trace_batch_device(bf200_context* c, const bf200_scene* s, const bf200_path_input_v1* device_inputs,
-                                     const float2* cones_in, uint64_t path_count, const bf200_transport_options_v1* o,
+                                     const bf200_path_state_v1* states_in, const float2* cones_in,
+                                     uint64_t path_count, const bf200_transport_options_v1* o,
                                      bf200_path_result_v1* device_results, float2* cones_out,
                                      bf200_report_v1* report) {
     if (c == nullptr || s == nullptr || (path_count != 0 && (device_inputs == nullptr || device_results == nullptr))) {
@@ -2126,6 +2128,7 @@ blackframe_status trace_batch_device(bf200_context* c, const bf200_scene* s, con
     src.total = path_count;
     src.inputs = device_inputs;
     src.results = device_results;
+    src.states_in = states_in;
     if (cones_in != nullptr) {
         if (const auto st = grow_workspace(c, &c->cone_column, &c->cone_column_bytes, c->capacity * sizeof(float2),
                                            "ray-cone column");
@@ -2142,42 +2145,53 @@ blackframe_status trace_batch_device(bf200_context* c, const bf200_scene* s, con
     return run_wavefront(c, s, src, make_params(*o), o->instrumentation != 0, report);
 }
 
-// Host inputs (and cones) to host results (and cones) through the context's batch staging.
+// Host arrays to host arrays through the context's batch staging (one 256-byte aligned piece per
+// array that is present).
 blackframe_status trace_batch_host(bf200_context* c, const bf200_scene* s, const bf200_path_input_v1* inputs,
-                                   const bf200_ray_cone_v1* cones_in, uint64_t path_count,
-                                   const bf200_transport_options_v1* o, bf200_path_result_v1* results,
-                                   bf200_ray_cone_v1* cones_out, bf200_report_v1* report) {
-    const bool cones = cones_in != nullptr;
+                                   const bf200_path_state_v1* states_in, const bf200_ray_cone_v1* cones_in,
+                                   uint64_t path_count, const bf200_transport_options_v1* o,
+                                   bf200_path_result_v1* results, bf200_ray_cone_v1* cones_out,
+                                   bf200_report_v1* report) {
     if (path_count == 0) {
-        return trace_batch_device(c, s, nullptr, nullptr, 0, o, nullptr, nullptr, report);
+        return trace_batch_device(c, s, nullptr, nullptr, nullptr, 0, o, nullptr, nullptr, report);
     }
     cudaSetDevice(c->device);
     const auto span = [](size_t bytes) { return (bytes + 255) & ~size_t(255); };
     const size_t in_bytes = path_count * sizeof(bf200_path_input_v1);
     const size_t out_bytes = path_count * sizeof(bf200_path_result_v1);
-    const size_t cone_bytes = cones ? path_count * sizeof(bf200_ray_cone_v1) : 0;
+    const size_t state_bytes = states_in != nullptr ? path_count * sizeof(bf200_path_state_v1) : 0;
+    const size_t cone_bytes = cones_in != nullptr ? path_count * sizeof(bf200_ray_cone_v1) : 0;
     if (const auto st = grow_workspace(c, &c->batch_staging, &c->batch_staging_bytes,
-                                       span(in_bytes) + span(out_bytes) + 2 * span(cone_bytes), "batch staging");
+                                       span(in_bytes) + span(out_bytes) + span(state_bytes) + 2 * span(cone_bytes),
+                                       "batch staging");
         st != BLACKFRAME_STATUS_SUCCESS) {
         return st;
     }
-    char* base = static_cast<char*>(c->batch_staging);
-    auto* d_in = reinterpret_cast<bf200_path_input_v1*>(base);
-    auto* d_out = reinterpret_cast<bf200_path_result_v1*>(base + span(in_bytes));
-    auto* d_cone_in = cones ? reinterpret_cast<float2*>(base + span(in_bytes) + span(out_bytes)) : nullptr;
-    auto* d_cone_out = cones ? reinterpret_cast<float2*>(base + span(in_bytes) + span(out_bytes) + span(cone_bytes))
-                             : nullptr;
+    char* cursor = static_cast<char*>(c->batch_staging);
+    const auto take = [&](size_t bytes) {
+        char* piece = bytes != 0 ? cursor : nullptr;
+        cursor += span(bytes);
+        return piece;
+    };
+    auto* d_in = reinterpret_cast<bf200_path_input_v1*>(take(in_bytes));
+    auto* d_out = reinterpret_cast<bf200_path_result_v1*>(take(out_bytes));
+    auto* d_states = reinterpret_cast<bf200_path_state_v1*>(take(state_bytes));
+    auto* d_cone_in = reinterpret_cast<float2*>(take(cone_bytes));
+    auto* d_cone_out = reinterpret_cast<float2*>(take(cone_bytes));
     cudaError_t e = cudaMemcpyAsync(d_in, inputs, in_bytes, cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess && cones) {
+    if (e == cudaSuccess && states_in != nullptr) {
+        e = cudaMemcpyAsync(d_states, states_in, state_bytes, cudaMemcpyHostToDevice, c->stream);
+    }
+    if (e == cudaSuccess && cones_in != nullptr) {
         e = cudaMemcpyAsync(d_cone_in, cones_in, cone_bytes, cudaMemcpyHostToDevice, c->stream);
     }
     blackframe_status st = e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "batch upload");
     if (st == BLACKFRAME_STATUS_SUCCESS) {
-        st = trace_batch_device(c, s, d_in, d_cone_in, path_count, o, d_out, d_cone_out, report);
+        st = trace_batch_device(c, s, d_in, d_states, d_cone_in, path_count, o, d_out, d_cone_out, report);
     }
     if (st == BLACKFRAME_STATUS_SUCCESS) {
         e = cudaMemcpyAsync(results, d_out, out_bytes, cudaMemcpyDeviceToHost, c->stream);
-        if (e == cudaSuccess && cones) {
+        if (e == cudaSuccess && cones_out != nullptr) {
             e = cudaMemcpyAsync(cones_out, d_cone_out, cone_bytes, cudaMemcpyDeviceToHost, c->stream);
         }
         if (e == cudaSuccess) {
@@ -2199,22 +2213,25 @@ BF200_EXPORT blackframe_status bf200_trace_paths_device(bf200_context* c, const 
                                                          uint64_t path_count, const bf200_transport_options_v1* o,
                                                          bf200_path_result_v1* device_results,
                                                          bf200_report_v1* report) noexcept {
-    return trace_batch_device(c, s, device_inputs, nullptr, path_count, o, device_results, nullptr, report);
+    return trace_batch_device(c, s, device_inputs, nullptr, nullptr, path_count, o, device_results, nullptr, report);
 }
 
 BF200_EXPORT blackframe_status bf200_trace_paths_with_cones_device(
     bf200_context* c, const bf200_scene* s, const bf200_path_input_v1* device_inputs,
-    const bf200_ray_cone_v1* device_primary_cones, uint64_t path_count, const bf200_transport_options_v1* o,
-    bf200_path_result_v1* device_results, bf200_ray_cone_v1* device_terminal_cones, bf200_report_v1* report) noexcept {
+    const bf200_path_state_v1* device_initial_states, const bf200_ray_cone_v1* device_primary_cones,
+    uint64_t path_count, const bf200_transport_options_v1* o, bf200_path_result_v1* device_results,
+    bf200_ray_cone_v1* device_terminal_cones, bf200_report_v1* report) noexcept {
     if (path_count != 0 && (device_primary_cones == nullptr || device_terminal_cones == nullptr)) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
     }
-    return trace_batch_device(c, s, device_inputs, reinterpret_cast<const float2*>(device_primary_cones), path_count,
-                              o, device_results, reinterpret_cast<float2*>(device_terminal_cones), report);
+    return trace_batch_device(c, s, device_inputs, device_initial_states,
+                              reinterpret_cast<const float2*>(device_primary_cones), path_count, o, device_results,
+                              reinterpret_cast<float2*>(device_terminal_cones), report);
 }
 
 BF200_EXPORT blackframe_status bf200_trace_paths_with_cones(bf200_context* c, const bf200_scene* s,
                                                              const bf200_path_input_v1* inputs,
+                                                             const bf200_path_state_v1* initial_states,
                                                              const bf200_ray_cone_v1* primary_cones,
                                                              uint64_t path_count, const bf200_transport_options_v1* o,
                                                              bf200_path_result_v1* results,
@@ -2225,15 +2242,30 @@ BF200_EXPORT blackframe_status bf200_trace_paths_with_cones(bf200_context* c, co
                              terminal_cones == nullptr))) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
     }
-    // every primary cone finite and non-negative (WavefrontTransport.cpp:524-531)
+    // the reference's preflight: finite non-negative cones and path spectra (WavefrontTransport.cpp:524-566)
     for (uint64_t i = 0; i < path_count; ++i) {
         const bf200_ray_cone_v1& cone = primary_cones[i];
         if (!std::isfinite(cone.width) || cone.width < 0.0F || !std::isfinite(cone.spread) || cone.spread < 0.0F) {
             return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
                         "path " + std::to_string(i) + " has a primary ray cone that is not finite and non-negative");
         }
+        if (initial_states != nullptr) {
+            const bf200_path_state_v1& st = initial_states[i];
+            bool valid = std::isfinite(st.eta_scale) && st.eta_scale > 0.0F && st.reserved[0] == 0U &&
+                         st.reserved[1] == 0U && st.reserved[2] == 0U;
+            for (int l = 0; l < 4; ++l) {
+                valid = valid && std::isfinite(st.beta[l]) && st.beta[l] >= 0.0F && std::isfinite(st.radiance[l]) &&
+                        st.radiance[l] >= 0.0F;
+            }
+            if (!valid) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
+                            "path " + std::to_string(i) +
+                                " has an initial state with a non-finite or negative spectrum or eta scale");
+            }
+        }
     }
-    return trace_batch_host(c, s, inputs, primary_cones, path_count, o, results, terminal_cones, report);
+    return trace_batch_host(c, s, inputs, initial_states, primary_cones, path_count, o, results, terminal_cones,
+                            report);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2406,7 +2438,7 @@ BF200_EXPORT blackframe_status bf200_trace_paths(bf200_context* c, const bf200_s
     if (c == nullptr || s == nullptr || (path_count != 0 && (inputs == nullptr || results == nullptr))) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
     }
-    return trace_batch_host(c, s, inputs, nullptr, path_count, o, results, nullptr, report);
+    return trace_batch_host(c, s, inputs, nullptr, nullptr, path_count, o, results, nullptr, report);
 }
 
 BF200_EXPORT blackframe_status bf200_render_film_device(bf200_context* c, const bf200_scene* s,
@@ -3296,3 +3328,4 @@ static_assert(sizeof(bf200_material_gradient_v1) == kAdjointStride * sizeof(doub
 static_assert(sizeof(bf200_adjoint_v1) == 40, "adjoint request layout");
 static_assert(sizeof(bf200_instance_v1) == 160, "instance layout");
 static_assert(sizeof(bf200_ray_cone_v1) == sizeof(float2), "ray cone layout (the device cone column is float2)");
+static_assert(sizeof(bf200_path_state_v1) == 48, "path state layout");

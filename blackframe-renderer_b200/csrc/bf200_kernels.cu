@@ -895,13 +895,33 @@ __device__ bool start_path(const Wavefront& w, const PathSource& src, uint32_t s
             }
         }
     }
+    float4 beta = make_float4(1.0F, 1.0F, 1.0F, 1.0F);
+    float4 radiance = make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+    float eta = 1.0F;
+    if (src.mode == 1U && src.states_in != nullptr) {
+        // a depth-zero initial state; the camera stage's valid_path_state check
+        // (CudaWavefrontStages.cu:545-560, 1378-1380)
+        const bf200_path_state_v1& st = src.states_in[id];
+        beta = make_float4(st.beta[0], st.beta[1], st.beta[2], st.beta[3]);
+        radiance = make_float4(st.radiance[0], st.radiance[1], st.radiance[2], st.radiance[3]);
+        eta = st.eta_scale;
+        bool valid = isfinite(eta) && eta > 0.0F;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            valid = valid && isfinite(st.beta[l]) && st.beta[l] >= 0.0F && isfinite(st.radiance[l]) &&
+                    st.radiance[l] >= 0.0F;
+        }
+        if (!valid) {
+            lane.fail();
+        }
+    }
     w.path_id[slot] = id;
     w.ray_o[slot] = make_float4(o.x, o.y, o.z, tmax);
     w.ray_d[slot] = make_float4(d.x, d.y, d.z, tmin);
-    w.beta[slot] = make_float4(1.0F, 1.0F, 1.0F, 1.0F);
-    w.radiance[slot] = make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+    w.beta[slot] = beta;
+    w.radiance[slot] = radiance;
     w.depth[slot] = 0U;
-    w.eta[slot] = 1.0F;
+    w.eta[slot] = eta;
     w.prev[slot] = make_float4(0.0F, 0.0F, 0.0F, 0.0F);
     w.flags[slot] = 0U;
     w.status[slot] = lane.err;

@@ -465,26 +465,42 @@ typedef struct bf200_ray_cone_v1 {
     float spread;
 } bf200_ray_cone_v1;
 
-/* bf200_trace_paths carrying every path's ray cone as the reference wavefront does:
- * CudaWavefrontPathInput::primary_cone in, CudaWavefrontTransportBatch::terminal_cones out
- * (WavefrontTransport.hpp:27-32, 127-132). The cone advances to every hit and is re-spread by the
- * selected closure at every scattering event (CudaWavefrontStages.cu:2832-2870, 3675-3781);
- * terminal_cones[i] is the cone at results[i].terminal_ray's origin. A primary cone that is not
- * finite and non-negative refuses the whole call with INVALID_ARGUMENT
- * (WavefrontTransport.cpp:524-531); a cone that becomes unrepresentable fails its lane with
- * BF200_LANE_NUMERICAL_FAILURE, as the reference's shade stage does. Path results are identical
- * to bf200_trace_paths for every lane that does not fail. */
+/* A depth-zero path state: PathState's throughput, accumulated radiance and eta scale
+ * (PathState.hpp:79-160) for a path that starts with depth 0, no delta history and the vacuum
+ * medium. 48 bytes. PathState::create_initial is beta 1, radiance 0, eta scale 1. */
+typedef struct bf200_path_state_v1 {
+    float beta[4];
+    float radiance[4];
+    float eta_scale;
+    uint32_t reserved[3];
+} bf200_path_state_v1;
+
+/* bf200_trace_paths with the rest of CudaWavefrontPathInput: every path's ray cone and,
+ * optionally, its depth-zero initial state (WavefrontTransport.hpp:27-32). Primary cones go in,
+ * and CudaWavefrontTransportBatch::terminal_cones come out (WavefrontTransport.hpp:127-132).
+ * - The cone advances to every hit and is re-spread by the selected closure at every scattering
+ *   event (CudaWavefrontStages.cu:2832-2870, 3675-3781).
+ * - terminal_cones[i] is the cone at results[i].terminal_ray's origin.
+ * - initial_states may be null: every path then starts from PathState::create_initial.
+ * - The whole call is refused with INVALID_ARGUMENT when a primary cone is not finite and
+ *   non-negative, or an initial state has a non-finite or negative spectrum, an eta scale that is
+ *   not finite and positive, or a non-zero reserved word (WavefrontTransport.cpp:524-566).
+ * - A cone that becomes unrepresentable fails its lane with BF200_LANE_NUMERICAL_FAILURE, as the
+ *   reference's shade stage does.
+ * Path results are identical to bf200_trace_paths for every lane that starts from the initial
+ * state and does not fail. */
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_with_cones(
     bf200_context* context, const bf200_scene* scene, const bf200_path_input_v1* inputs,
-    const bf200_ray_cone_v1* primary_cones, uint64_t path_count, const bf200_transport_options_v1* options,
-    bf200_path_result_v1* results, bf200_ray_cone_v1* terminal_cones, bf200_report_v1* report) BF200_NOEXCEPT;
-/* The same with inputs, cones and results in device memory; an invalid primary cone fails its
- * lane instead of the call (the camera stage's check, CudaWavefrontStages.cu:1378-1380). */
+    const bf200_path_state_v1* initial_states, const bf200_ray_cone_v1* primary_cones, uint64_t path_count,
+    const bf200_transport_options_v1* options, bf200_path_result_v1* results, bf200_ray_cone_v1* terminal_cones,
+    bf200_report_v1* report) BF200_NOEXCEPT;
+/* The same with every array in device memory. An invalid primary cone or initial state fails its
+ * lane instead of the call (the camera stage's checks, CudaWavefrontStages.cu:1378-1380). */
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_with_cones_device(
     bf200_context* context, const bf200_scene* scene, const bf200_path_input_v1* device_inputs,
-    const bf200_ray_cone_v1* device_primary_cones, uint64_t path_count, const bf200_transport_options_v1* options,
-    bf200_path_result_v1* device_results, bf200_ray_cone_v1* device_terminal_cones,
-    bf200_report_v1* report) BF200_NOEXCEPT;
+    const bf200_path_state_v1* device_initial_states, const bf200_ray_cone_v1* device_primary_cones,
+    uint64_t path_count, const bf200_transport_options_v1* options, bf200_path_result_v1* device_results,
+    bf200_ray_cone_v1* device_terminal_cones, bf200_report_v1* report) BF200_NOEXCEPT;
 
 /* Same as bf200_trace_paths with inputs and results in device memory. */
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_device(

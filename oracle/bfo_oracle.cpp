@@ -2697,13 +2697,32 @@ Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& 
 
 // cone: null, or the path's primary ray cone (width, spread), carried as the reference's wavefront
 // carries it (CudaWavefrontStages.cu:4602-4624) and returned in PathOut::cone_*.
+// state: null (PathState::create_initial), or a depth-zero initial state whose throughput,
+// radiance and eta scale the path starts from (trace_scene_mis takes any such PathState).
 PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Options& opt,
-              const float* cone = nullptr) {
+              const float* cone = nullptr, const bf200_path_state_v1* state = nullptr) {
     PathOut out{};
     out.beta = Spectrum{1.0F, 1.0F, 1.0F, 1.0F};
     out.radiance = Spectrum{};
+    if (state != nullptr) {
+        for (int lane = 0; lane < 4; ++lane) {
+            out.beta[lane] = state->beta[lane];
+            out.radiance[lane] = state->radiance[lane];
+        }
+    }
     out.depth = Depth{{0, 0, 0, 0, 0}};
-    out.eta_scale = 1.0F;
+    out.eta_scale = state != nullptr ? state->eta_scale : 1.0F;
+    if (state != nullptr) {  // PathState::create's checks (PathState.hpp:84-96)
+        for (int lane = 0; lane < 4; ++lane) {
+            if (!std::isfinite(out.beta[lane]) || out.beta[lane] < 0.0F || !std::isfinite(out.radiance[lane]) ||
+                out.radiance[lane] < 0.0F) {
+                fail("An initial path spectrum must be finite and non-negative.");
+            }
+        }
+        if (!std::isfinite(out.eta_scale) || !(out.eta_scale > 0.0F)) {
+            fail("Path eta scale must be finite and strictly positive.");
+        }
+    }
     out.delta_flags = 0;
     out.blocked = 0;
     out.segments = 0;
@@ -3087,9 +3106,9 @@ __attribute__((visibility("default"))) int bfo_scene_world_normal(void* h, uint3
 
 // Traces paths; returns how many failed (lane_status 1, first message in bfo_last_error()).
 // cones_in / cones_out (both or neither, 2 floats per path) carry the ray cones.
-static int64_t trace_batch(void* h, const bf200_path_input_v1* in, const float* cones_in, uint64_t n,
-                    const bf200_transport_options_v1* o, bf200_path_result_v1* res, float* cones_out,
-                    int threads) {
+static int64_t trace_batch(void* h, const bf200_path_input_v1* in, const bf200_path_state_v1* states,
+                           const float* cones_in, uint64_t n, const bf200_transport_options_v1* o,
+                           bf200_path_result_v1* res, float* cones_out, int threads) {
     const auto* s = static_cast<Scene*>(h);
     const Options opt = make_options(*o);
     std::atomic<uint64_t> next{0};
@@ -3097,7 +3116,8 @@ static int64_t trace_batch(void* h, const bf200_path_input_v1* in, const float* 
     auto worker = [&] {
         for (uint64_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {
             try {
-                const PathOut p = trace(*s, in[i], opt, cones_in != nullptr ? cones_in + 2 * i : nullptr);
+                const PathOut p = trace(*s, in[i], opt, cones_in != nullptr ? cones_in + 2 * i : nullptr,
+                                        states != nullptr ? states + i : nullptr);
                 store_result(p, res[i], in[i].primary_ray.time, in[i].primary_ray.mask);
                 if (cones_out != nullptr) {
                     cones_out[2 * i] = p.cone_width;
@@ -3133,16 +3153,18 @@ __attribute__((visibility("default"))) int64_t bfo_trace_paths(void* h, const bf
                                                                uint64_t n,
                                                                const bf200_transport_options_v1* o,
                                                                bf200_path_result_v1* res, int threads) {
-    return trace_batch(h, in, nullptr, n, o, res, nullptr, threads);
+    return trace_batch(h, in, nullptr, nullptr, n, o, res, nullptr, threads);
 }
 
-// bfo_trace_paths with ray cones (width, spread per path) in and at every terminal-ray origin out.
+// bfo_trace_paths with ray cones (width, spread per path) in and at every terminal-ray origin out,
+// and optional depth-zero initial states (null: PathState::create_initial).
 __attribute__((visibility("default"))) int64_t bfo_trace_paths_cones(void* h, const bf200_path_input_v1* in,
+                                                                     const bf200_path_state_v1* states,
                                                                      const float* cones_in, uint64_t n,
                                                                      const bf200_transport_options_v1* o,
                                                                      bf200_path_result_v1* res, float* cones_out,
                                                                      int threads) {
-    return trace_batch(h, in, cones_in, n, o, res, cones_out, threads);
+    return trace_batch(h, in, states, cones_in, n, o, res, cones_out, threads);
 }
 
 // One ray-cone advance per case: cones (width, spread), ray directions, hit parameters; writes the

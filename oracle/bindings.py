@@ -140,18 +140,20 @@ class Oracle(_Checker):
                      parameters.ctypes.data_as(C.c_void_p), len(parameters), out.ctypes.data_as(C.c_void_p))
         return out, failures
 
-    def trace_cones(self, handle, inputs, cones, options, threads=None):
-        """trace() carrying ray cones: (results, terminal cones float32 [n, 2], failures)."""
+    def trace_cones(self, handle, inputs, cones, options, states=None, threads=None):
+        """trace() carrying ray cones and, optionally, depth-zero initial states (an array of
+        abi.PathState): (results, terminal cones float32 [n, 2], failures)."""
         import numpy as np
         n = len(inputs)
         cones = np.ascontiguousarray(cones, np.float32).reshape(n, 2)
         results = (abi.PathResult * n)()
         out = np.zeros((n, 2), np.float32)
         f = self.lib.bfo_trace_paths_cones
-        f.argtypes = [C.c_void_p, C.POINTER(abi.PathInput), C.c_void_p, C.c_uint64, C.POINTER(abi.TransportOptions),
-                      C.POINTER(abi.PathResult), C.c_void_p, C.c_int]
+        f.argtypes = [C.c_void_p, C.POINTER(abi.PathInput), C.c_void_p, C.c_void_p, C.c_uint64,
+                      C.POINTER(abi.TransportOptions), C.POINTER(abi.PathResult), C.c_void_p, C.c_int]
         f.restype = C.c_int64
-        failures = f(handle, inputs, cones.ctypes.data_as(C.c_void_p), n, C.byref(options), results,
+        failures = f(handle, inputs, C.cast(states, C.c_void_p) if states is not None else None,
+                     cones.ctypes.data_as(C.c_void_p), n, C.byref(options), results,
                      out.ctypes.data_as(C.c_void_p), threads or os.cpu_count() or 1)
         if failures < 0:
             raise CheckerError(self.last_error())
@@ -209,6 +211,21 @@ class Reference(_Checker):
         if code != 0:
             return None, code
         return (probabilities, selected, selected_probability), 0
+
+    def trace_states(self, handle, inputs, states, options, threads=None):
+        """trace_scene_mis from a depth-zero initial PathState per path (an array of
+        abi.PathState): (results, failures)."""
+        n = len(inputs)
+        results = (abi.PathResult * n)()
+        f = self.lib.bfr_trace_paths_states
+        f.argtypes = [C.c_void_p, C.POINTER(abi.PathInput), C.c_void_p, C.c_uint64, C.POINTER(abi.TransportOptions),
+                      C.POINTER(abi.PathResult), C.c_int]
+        f.restype = C.c_int64
+        failures = f(handle, inputs, C.cast(states, C.c_void_p), n, C.byref(options), results,
+                     threads or os.cpu_count() or 1)
+        if failures < 0:
+            raise CheckerError(self.last_error())
+        return results, failures
 
     def cone_advance(self, cones, distances):
         """renderer::advance_ray_cone(cone, distance) per case: widths (NaN on error), errors."""

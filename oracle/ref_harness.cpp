@@ -155,9 +155,26 @@ core::Result<renderer::RussianRoulettePolicy> make_policy(const bf200_transport_
 void trace_one(const RefScene& scene, const bf200_path_input_v1& input,
                const bf200_transport_options_v1& options,
                const renderer::RussianRoulettePolicy& policy, bf200_path_result_v1& out,
-               std::string* error) {
+               std::string* error, const bf200_path_state_v1* initial = nullptr) {
     std::memset(&out, 0, sizeof(out));
-    const auto state = renderer::PathState::create_initial(scene.wavelengths, renderer::VacuumMedium);
+    auto state = renderer::PathState::create_initial(scene.wavelengths, renderer::VacuumMedium);
+    if (initial != nullptr) {
+        renderer::TransportSpectrum beta{}, radiance{};
+        for (std::size_t lane = 0; lane < 4; ++lane) {
+            beta.values[lane] = initial->beta[lane];
+            radiance.values[lane] = initial->radiance[lane];
+        }
+        state = renderer::PathState::create(beta, radiance, renderer::PathDepthCounters{}, initial->eta_scale,
+                                            scene.wavelengths, renderer::PathDeltaFlags::none,
+                                            renderer::VacuumMedium);
+        if (!state) {
+            out.lane_status = BF200_LANE_NUMERICAL_FAILURE;
+            if (error != nullptr && error->empty()) {
+                *error = state.error().message;
+            }
+            return;
+        }
+    }
     const auto stream = renderer::SampleStream{renderer::SampleStreamIndex{
         .pixel_x = input.sample.pixel_x,
         .pixel_y = input.sample.pixel_y,
@@ -389,6 +406,38 @@ bfr_trace_paths(void* handle, const bf200_path_input_v1* inputs, uint64_t count,
     parallel_for(count, threads, [&](uint64_t index) {
         std::string error;
         trace_one(*scene, inputs[index], *options, *policy, results[index], &error);
+        if (results[index].lane_status != 0) {
+            failures.fetch_add(1);
+            std::lock_guard<std::mutex> lock{error_mutex};
+            if (first_error.empty()) {
+                first_error = error;
+            }
+        }
+    });
+    if (!first_error.empty()) {
+        set_error(first_error);
+    }
+    return failures.load();
+}
+
+// bfr_trace_paths with a depth-zero initial PathState per path (PathState::create with the
+// given throughput, radiance and eta scale, no depth and no delta history).
+__attribute__((visibility("default"))) int64_t
+bfr_trace_paths_states(void* handle, const bf200_path_input_v1* inputs, const bf200_path_state_v1* states,
+                       uint64_t count, const bf200_transport_options_v1* options, bf200_path_result_v1* results,
+                       int threads) {
+    const auto* scene = static_cast<RefScene*>(handle);
+    const auto policy = make_policy(*options);
+    if (!policy) {
+        set_error(policy.error().message);
+        return -1;
+    }
+    std::atomic<int64_t> failures{0};
+    std::string first_error;
+    std::mutex error_mutex;
+    parallel_for(count, threads, [&](uint64_t index) {
+        std::string error;
+        trace_one(*scene, inputs[index], *options, *policy, results[index], &error, states + index);
         if (results[index].lane_status != 0) {
             failures.fetch_add(1);
             std::lock_guard<std::mutex> lock{error_mutex};

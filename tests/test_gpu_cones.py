@@ -1,4 +1,4 @@
-"""Ray cones through the device wavefront (bf200_trace_paths_with_cones*).
+"""Ray cones and initial path states through the device wavefront (bf200_trace_paths_with_cones*).
 
 * Paths of the Cornell box with its conductor and dielectric spheres, started with the reference
   camera's own primary cones (tests/golden/cones.npz, PinholeCamera::generate_primary_ray_cone):
@@ -9,6 +9,8 @@
   cones do not fail.
 * Invalid primary cones: refused for the whole host call (INVALID_ARGUMENT), failed per lane in
   the device call.
+* Depth-zero initial states other than PathState::create_initial: device paths vs the oracle
+  (whose results are pinned on the reference by tests/test_initial_states.py).
 """
 import ctypes as C
 
@@ -128,3 +130,52 @@ def test_invalid_primary_cones(ctx, workload):
         assert bytes(results[k]) == bytes(host[k])
     assert np.array_equal(d_terminal.cpu().numpy().reshape(n, 2)[others].view(np.uint32),
                           host_cones[others].view(np.uint32))
+
+
+def test_initial_states_match_the_oracle(ctx, golden):
+    """Depth-zero initial states other than PathState::create_initial (zero and 1e30 throughput,
+    accumulated radiance, eta scales other than 1; tests/golden/initial_states.npz, whose oracle
+    results are pinned on the reference by tests/test_initial_states.py): device paths against the
+    oracle, with the parity tolerances, and the same lane failures."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        "make_state_golden", os.path.join(os.path.dirname(__file__), "golden", "make_state_golden.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    g = golden("initial_states")
+    builder, options, (width, height, _) = scenes.build_workload(m.WORKLOAD)
+    table = g["samples"]
+    samples = (abi.SampleIndex * len(table))()
+    for k in range(len(table)):
+        samples[k].pixel_x, samples[k].pixel_y = int(table[k, 0]), int(table[k, 1])
+        samples[k].sample_index, samples[k].seed = int(table[k, 2]), int(table[k, 3])
+    inputs = m.inputs_for(samples, width, height)
+    states = m.states_from(g["beta_in"], g["radiance_in"], g["eta_in"])
+    cones = np.tile(np.array([0.0, 0.0025], np.float32), (len(table), 1))
+    oracle = Oracle()
+    handle = oracle.scene(builder)
+    expected, expected_cones, _ = oracle.trace_cones(handle, inputs, cones, options, states=states)
+    oracle.destroy(handle)
+    scene = ctx.create_scene(builder)
+    results, got_cones, report = ctx.trace_paths_with_cones(scene, inputs, cones, options, states=states)
+    scene.close()
+    got, want = arrays(results), arrays(expected)
+    assert np.array_equal(got["lane_status"] != 0, want["lane_status"] != 0)
+    keep = want["lane_status"] == 0
+    exact, close = check_paths({k: v[keep] for k, v in got.items()}, {k: v[keep] for k, v in want.items()},
+                               "initial states")
+    assert exact >= 0.95
+    zero = (g["beta_in"] == 0.0).all(axis=1)
+    assert (got["depth"][zero] == 0).all() and set(got["termination"][zero].tolist()) <= {0, 3}
+    same_path = bit_equal(got["radiance"], want["radiance"]).all(axis=1) & (got["depth"] == want["depth"]) & keep
+    assert bit_equal(got_cones, expected_cones).all(axis=1)[same_path].all()
+    # invalid states: refused for the whole host call
+    bad = m.states_from(g["beta_in"][:4], g["radiance_in"][:4], g["eta_in"][:4])
+    bad[2].eta_scale = 0.0
+    scene = ctx.create_scene(builder)
+    sub = (abi.PathInput * 4)(*inputs[:4])
+    with pytest.raises(runtime.Bf200Error) as info:
+        ctx.trace_paths_with_cones(scene, sub, cones[:4], options, states=bad)
+    scene.close()
+    assert info.value.status == 1
