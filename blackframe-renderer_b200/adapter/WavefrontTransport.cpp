@@ -25,11 +25,12 @@
 // WavefrontTransport.cpp:875-922): numerical failures map to internal_error, unsupported lanes
 // to unavailable, traversal failures to incompatible.
 //
-// The report fills the fields bf200 measures: schema, light registry and sampler, the echoed
-// options, path count, the camera/intersection/shadow lane counts, closure and light samples,
-// shadow queries and terminated paths. bf200 does not split its lanes into the reference's
-// hit/miss/shade/continuation queues, so those counts and the per-stage metrics stay zero;
-// device_size_bytes() is 0 because bf200 does not expose its arena size.
+// The report fills every counting field: schema, light registry and sampler, the echoed options,
+// path count, the stage lanes (camera, intersection, hit, miss, shade, shadow, continuation),
+// closure and light samples, shadow queries and terminated paths. The per-stage metrics
+// (dispatches, lanes and GPU time of the reference's own stage kernels) describe a kernel
+// structure bf200 does not have and stay zero; device_size_bytes() is 0 because bf200 does not
+// expose its arena size.
 #include <Blackframe/Backends/GPU/CUDA/WavefrontTransport.hpp>
 
 #include <cuda_runtime_api.h>
@@ -583,9 +584,14 @@ trace_cuda_wavefront_transport(CudaWavefrontTransportWorkspace& workspace, const
     out.path_count = n;
     out.transfer_mode = options.transfer_mode;
     out.instrumentation_mode = options.instrumentation_mode;
+    // every traced extension segment either hit (and was shaded) or missed
     out.stage_lanes.camera = n;
     out.stage_lanes.intersection = report.extension_segments;
+    out.stage_lanes.miss = report.miss_segments;
+    out.stage_lanes.hit = report.extension_segments - std::min(report.extension_segments, report.miss_segments);
+    out.stage_lanes.shade = out.stage_lanes.hit;
     out.stage_lanes.shadow = report.shadow_segments;
+    out.stage_lanes.continuation = report.continuation_segments;
     out.closure_samples = report.closure_samples;
     out.light_samples = report.light_samples;
     out.shadow_queries = report.shadow_segments;

@@ -181,7 +181,7 @@ class Report(C.Structure):
                 ("first_failure_path", u32), ("kernel_launches", u64),
                 ("gpu_milliseconds", f64), ("intersect_milliseconds", f64), ("shade_milliseconds", f64),
                 ("occlude_milliseconds", f64), ("film_milliseconds", f64), ("iterations", u64),
-                ("regenerate_milliseconds", f64), ("reserved", u64 * 2)]
+                ("regenerate_milliseconds", f64), ("miss_segments", u64), ("continuation_segments", u64)]
 
 
 class Hit(C.Structure):

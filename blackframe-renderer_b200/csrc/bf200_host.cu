@@ -1291,6 +1291,11 @@ blackframe_status run_wavefront_graph(bf200_context* c, const bf200_scene* s, Pa
         report->extension_segments += k[3];
         report->shadow_segments += k[4];
         report->failed_lanes += k[5];
+        report->terminated_paths += src.total - std::min<uint64_t>(src.total, k[5]);
+        report->closure_samples += k[11];
+        report->light_samples += k[12];
+        report->miss_segments += k[13];
+        report->continuation_segments += k[14];
         if (k[5] != 0 && report->first_failure_status == 0) {
             report->first_failure_status = static_cast<uint32_t>(k[7]);
             report->first_failure_path = static_cast<uint32_t>(k[6]);
@@ -1314,7 +1319,7 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
     cudaStream_t st = c->stream;
     cudaError_t e = cudaMemsetAsync(w.state, 0, w.capacity, st);
     if (e == cudaSuccess) {
-        e = cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), st);
+        e = cudaMemsetAsync(w.counters, 0, 16 * sizeof(unsigned long long), st);
     }
     if (e != cudaSuccess) {
         return cuda_fail(c, e, "wavefront reset");
@@ -1386,7 +1391,7 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
     e = launch_retire(w, src, grid, st);
     ++launches;
     if (e == cudaSuccess) {
-        e = cudaMemcpyAsync(c->pinned_counters, w.counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+        e = cudaMemcpyAsync(c->pinned_counters, w.counters, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             st);
     }
     cudaEventRecord(stop, st);
@@ -1410,6 +1415,11 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
         report->extension_segments += c->pinned_counters[3];
         report->shadow_segments += shadow_segments;
         report->failed_lanes += c->pinned_counters[5];
+        report->terminated_paths += src.total - std::min<uint64_t>(src.total, c->pinned_counters[5]);
+        report->closure_samples += c->pinned_counters[11];
+        report->light_samples += c->pinned_counters[12];
+        report->miss_segments += c->pinned_counters[13];
+        report->continuation_segments += c->pinned_counters[14];
         if (c->pinned_counters[5] != 0 && report->first_failure_status == 0) {
             report->first_failure_status = static_cast<uint32_t>(c->pinned_counters[7]);
             report->first_failure_path = static_cast<uint32_t>(c->pinned_counters[6]);
@@ -2920,6 +2930,7 @@ void lane_report(const bf200_film_job_v1& job, const LaneState& lane) {
     r->extension_segments += lane.counters[3];
     r->shadow_segments += lane.shadow_segments;
     r->failed_lanes += lane.counters[5];
+    r->terminated_paths += lane.src.total - std::min<uint64_t>(lane.src.total, lane.counters[5]);
     if (lane.counters[5] != 0 && r->first_failure_status == 0) {
         r->first_failure_status = static_cast<uint32_t>(lane.counters[7]);
         r->first_failure_path = static_cast<uint32_t>(lane.counters[6]);

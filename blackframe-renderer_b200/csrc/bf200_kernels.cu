@@ -1728,6 +1728,9 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
     const uint32_t begin = w.route_offsets[route], end = w.route_offsets[route + 1U];
     const uint32_t stride = gridDim.x * blockDim.x;
     uint32_t active_here = 0;
+    // the reference's stage counts, kept by the cone-carrying instantiations only: closure samples,
+    // light samples and misses (CudaWavefrontStages.cu:4348, 4384, 4985-4997)
+    uint32_t closures_here = 0, lights_here = 0, misses_here = 0;
     for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
         const uint32_t slot = w.route_queue[i];
         ShadowRecord rec;
@@ -1760,6 +1763,9 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                 }
             }
             if (K == 0 && id.x == 0xFFFFFFFFU) {
+                if constexpr (CONE) {
+                    ++misses_here;
+                }
                 const float env[4] = {s.environment.x, s.environment.y, s.environment.z, s.environment.w};
                 add_product(rad, beta, env, lane);
                 w.radiance[slot] = rad;
@@ -1875,6 +1881,12 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                     BsdfSample bs;
                     closure_sample<K>(closure, allowed, wo, stream.sample_1d(dims + 3), stream.sample_1d(dims + 4),
                                    stream.sample_1d(dims + 5), bs, lane);
+                    if constexpr (CONE) {
+                        ++closures_here;
+                        if (s.light_count != 0U && !is_black4(closure.w)) {
+                            ++lights_here;
+                        }
+                    }
                     uint32_t next_depth = depth;
                     if (bs.valid) {
                         if (!isfinite(bs.pdf) || !(bs.pdf > 0.0F) || bs.wi.z == 0.0F ||
@@ -2061,6 +2073,21 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
     }
     if ((threadIdx.x & 31U) == 0U && active_here != 0U) {
         atomicAdd(&w.counters[2], static_cast<unsigned long long>(active_here));
+    }
+    if constexpr (CONE) {
+        for (int off = 16; off > 0; off >>= 1) {
+            closures_here += __shfl_down_sync(0xFFFFFFFFU, closures_here, off);
+            lights_here += __shfl_down_sync(0xFFFFFFFFU, lights_here, off);
+            misses_here += __shfl_down_sync(0xFFFFFFFFU, misses_here, off);
+        }
+        if ((threadIdx.x & 31U) == 0U) {
+            // cumulative over the trace: [11] closure samples, [12] light samples, [13] misses,
+            // [14] continuations
+            atomicAdd(&w.counters[11], static_cast<unsigned long long>(closures_here));
+            atomicAdd(&w.counters[12], static_cast<unsigned long long>(lights_here));
+            atomicAdd(&w.counters[13], static_cast<unsigned long long>(misses_here));
+            atomicAdd(&w.counters[14], static_cast<unsigned long long>(active_here));
+        }
     }
     if constexpr (ADJ) {
         adjoint_flush(adjoint_sum, a.gradients);

@@ -393,7 +393,13 @@ typedef struct bf200_film_v1 {
     uint64_t* sample_counts;
 } bf200_film_v1;
 
-/* engine::CudaWavefrontTransportReport (WavefrontTransport.hpp:97-125), counting subset. */
+/* engine::CudaWavefrontTransportReport (WavefrontTransport.hpp:97-125), counting subset.
+ * terminated_paths counts the paths that finished without a lane failure (every call but
+ * bf200_trace_paths_device_noalloc, which leaves it zero). closure_samples,
+ * light_samples (the shade stage's WavefrontShadeDetailClosureSampled / LightSampled lanes),
+ * miss_segments and continuation_segments are counted by the traces that carry ray cones
+ * (bf200_trace_paths_with_cones*), the reference-facing path; other calls leave them zero, so
+ * their shading kernels carry no extra counters. */
 typedef struct bf200_report_v1 {
     uint32_t struct_size;
     uint32_t registered_light_count;
@@ -417,7 +423,10 @@ typedef struct bf200_report_v1 {
     double film_milliseconds;
     uint64_t iterations;
     double regenerate_milliseconds;
-    uint64_t reserved[2];
+    /* the reference's stage-lane counts (CudaWavefrontStageLaneCounts, WavefrontTransport.hpp:59-70):
+     * extension segments that missed every surface, and paths that continued after shading */
+    uint64_t miss_segments;
+    uint64_t continuation_segments;
 } bf200_report_v1;
 
 typedef struct bf200_context bf200_context;

@@ -88,6 +88,18 @@ def test_terminal_cones_match_the_oracle(ctx, workload):
     assert cone_equal[same_path].mean() >= 0.999, np.nonzero(same_path & ~cone_equal)[0][:10]
     near = (relative_error(got_cones, expected_cones) <= RELATIVE_TOLERANCE).all(axis=1)
     assert near[same_path].all() and near[keep].mean() >= 0.99
+    # the reference's stage counts (CudaWavefrontStageLaneCounts): every extension segment is a
+    # camera ray or a continuation, each hit or missed, and every shaded lane drew a closure sample
+    # and (with lights and a non-black closure) a light sample
+    n = len(inputs)
+    assert report.terminated_paths == n - report.failed_lanes
+    if report.failed_lanes == 0:
+        assert report.extension_segments == n + report.continuation_segments
+    assert 0 < report.miss_segments < report.extension_segments
+    hits = report.extension_segments - report.miss_segments
+    assert report.continuation_segments <= report.closure_samples <= hits
+    assert report.shadow_segments <= report.light_samples <= report.closure_samples
+    assert report.light_samples > report.shadow_segments > 0
     # the cones grew: every path that scattered left with a spread of at least the smallest policy
     scattered = keep & (got["depth"] > 0)
     assert scattered.sum() > 1000 and (got_cones[scattered, 1] >= 0.05).all()
