@@ -98,3 +98,6 @@ def test_invalid_arguments_are_rejected_without_a_device():
     assert lib.bf200_context_create(-1, 0, C.byref(handle)) == 5
     assert lib.bf200_trace_paths(None, None, None, 1, None, None, None) == 1
     assert lib.bf200_context_destroy(None) == 1
+    # the cone and initial-state entry points: null arrays are refused before any device work
+    assert lib.bf200_trace_paths_with_cones(None, None, None, None, None, 1, None, None, None, None) == 1
+    assert lib.bf200_trace_paths_with_cones_device(None, None, None, None, None, 1, None, None, None, None) == 1
