@@ -200,8 +200,13 @@ class PathState(C.Structure):
                 ("reserved", C.c_uint32 * 3)]
 
 
+class LightTreeInput(C.Structure):
+    """bf200_light_tree_input_v1: a light's world bounds and four-lane spectral power."""
+    _fields_ = [("bounds_min", C.c_float * 3), ("bounds_max", C.c_float * 3), ("spectral_power", C.c_float * 4)]
+
+
 EXPECTED_SIZES = {
-    RayCone: 8, PathState: 48,
+    RayCone: 8, PathState: 48, LightTreeInput: 40,
     Closure: 64, Material: 80, Geometry: 32, Instance: 160, Ray: 48, SampleIndex: 24,
     PathInput: 80, PathResult: 128, TransportOptions: 64, Camera: 88, Sensor: 80,
     FilmRequest: 40, FilmJob: 64, MeshView: 48, MaterialGradient: 64, Adjoint: 40, Report: 152, Hit: 32, ExtensionApi: 40, XpuDeviceDescriptor: 88,

@@ -35,6 +35,8 @@ EXPORTED_SYMBOLS = [
     "bf200_mesh_destroy",
     "bf200_trace_paths_with_cones",
     "bf200_trace_paths_with_cones_device",
+    "bf200_light_tree_select",
+    "bf200_light_tree_probability",
 ]
 
 
@@ -384,6 +386,57 @@ def light_power_cdf(powers):
     if status != 0:
         raise Bf200Error(status, "light power CDF refused")
     return out
+
+
+
+def _light_tree_inputs(bounds_min, bounds_max, powers):
+    import numpy as np
+    bounds_min = np.ascontiguousarray(bounds_min, np.float32).reshape(-1, 3)
+    bounds_max = np.ascontiguousarray(bounds_max, np.float32).reshape(-1, 3)
+    powers = np.ascontiguousarray(powers, np.float32).reshape(-1, 4)
+    lights = (abi.LightTreeInput * len(powers))()
+    for k in range(len(powers)):
+        lights[k].bounds_min[:] = [float(v) for v in bounds_min[k]]
+        lights[k].bounds_max[:] = [float(v) for v in bounds_max[k]]
+        lights[k].spectral_power[:] = [float(v) for v in powers[k]]
+    return lights
+
+
+def light_tree_select(bounds_min, bounds_max, powers, positions, samples):
+    """bf200_light_tree_select: (selected slots uint32, probabilities float32); a refused query
+    gives 0xFFFFFFFF and -1. Raises Bf200Error when the tree itself is refused."""
+    import numpy as np
+    lights = _light_tree_inputs(bounds_min, bounds_max, powers)
+    positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    samples = np.ascontiguousarray(samples, np.float32)
+    selected = np.zeros(len(samples), np.uint32)
+    probabilities = np.zeros(len(samples), np.float32)
+    f = library().bf200_light_tree_select
+    f.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    f.restype = C.c_uint32
+    status = f(C.cast(lights, C.c_void_p), len(lights), positions.ctypes.data_as(C.c_void_p),
+               samples.ctypes.data_as(C.c_void_p), len(samples), selected.ctypes.data_as(C.c_void_p),
+               probabilities.ctypes.data_as(C.c_void_p))
+    if status != 0:
+        raise Bf200Error(status, "light tree refused")
+    return selected, probabilities
+
+
+def light_tree_probability(bounds_min, bounds_max, powers, positions, light_indices):
+    """bf200_light_tree_probability: float32 probabilities (-1 where a query is refused)."""
+    import numpy as np
+    lights = _light_tree_inputs(bounds_min, bounds_max, powers)
+    positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    light_indices = np.ascontiguousarray(light_indices, np.uint32)
+    probabilities = np.zeros(len(light_indices), np.float32)
+    f = library().bf200_light_tree_probability
+    f.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]
+    f.restype = C.c_uint32
+    status = f(C.cast(lights, C.c_void_p), len(lights), positions.ctypes.data_as(C.c_void_p),
+               light_indices.ctypes.data_as(C.c_void_p), len(light_indices), probabilities.ctypes.data_as(C.c_void_p))
+    if status != 0:
+        raise Bf200Error(status, "light tree refused")
+    return probabilities
 
 
 def load_mesh(path):

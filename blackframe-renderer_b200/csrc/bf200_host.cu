@@ -24,6 +24,7 @@
 #include "bf200.h"
 #include "bf200_device.cuh"
 #include "bf200_kernels.h"
+#include "bf200_light_tree.h"
 #include "bf200_sobol.h"
 
 using namespace bf200;
@@ -717,7 +718,8 @@ bool compensated_add(float value, float& sum, float& correction) {
 }
 
 // The selection CDF (light_count + 1 boundaries) of four-lane spectral powers in registry order.
-blackframe_status power_cdf(const float* powers, uint32_t count, std::vector<float>& cdf, std::string& error) {
+blackframe_status power_cdf(const float* powers, uint32_t count, std::vector<float>& cdf, std::string& error,
+                            std::vector<float>* weights_out = nullptr) {
     if (count == 0) {
         error = "Light sampling requires at least one registry slot.";
         return BLACKFRAME_STATUS_INVALID_ARGUMENT;
@@ -829,6 +831,9 @@ blackframe_status power_cdf(const float* powers, uint32_t count, std::vector<flo
             error = "Light-selection CDF lost or created probability support.";
             return BLACKFRAME_STATUS_OUT_OF_RANGE;
         }
+    }
+    if (weights_out != nullptr) {
+        *weights_out = std::move(weights);
     }
     return BLACKFRAME_STATUS_SUCCESS;
 }
@@ -1436,6 +1441,15 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
 }
 
 }  // namespace
+
+namespace bf200 {
+
+blackframe_status light_power_weights(const float* powers, uint32_t count, std::vector<float>& weights,
+                                      std::vector<float>& cdf, std::string& error) {
+    return power_cdf(powers, count, cdf, error, &weights);
+}
+
+}  // namespace bf200
 
 // =============================================================================================
 // C ABI

@@ -681,6 +681,35 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_power_cdf(const float*
                                                                      uint32_t light_count, float* boundaries)
     BF200_NOEXCEPT;
 
+/* One light of a spatial light tree: LightTreeInput (LightSampler.hpp:19-25), its conservative
+ * world bounds (min <= max, no NaN; +-infinity on every axis for an unbounded light) and its
+ * four-lane spectral power, in registry order. 40 bytes. */
+typedef struct bf200_light_tree_input_v1 {
+    float bounds_min[3];
+    float bounds_max[3];
+    float spectral_power[4];
+} bf200_light_tree_input_v1;
+
+/* LightSampler::create_spatial_tree (LightSampler.cpp:626-951) and its selection at query points
+ * (sample(context, u), LightSampler.cpp:1058-1129), bit for bit: for every query the selected slot
+ * and its discrete probability, or 0xFFFFFFFF and -1 where the reference refuses that query. A
+ * tree the reference refuses to build fails the call (INVALID_ARGUMENT for invalid inputs,
+ * OUT_OF_RANGE for unrepresentable powers or bounds). positions: 3 floats per query. Host
+ * computation; transport does not select by tree yet. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_tree_select(const bf200_light_tree_input_v1* lights,
+                                                                      uint32_t light_count, const float* positions,
+                                                                      const float* samples, uint64_t query_count,
+                                                                      uint32_t* light_indices,
+                                                                      float* probabilities) BF200_NOEXCEPT;
+/* The tree's probability of selecting light_indices[q] at positions[q] (probability(context, i),
+ * LightSampler.cpp:1151-1225); -1 where the reference refuses the query. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_tree_probability(const bf200_light_tree_input_v1* lights,
+                                                                           uint32_t light_count,
+                                                                           const float* positions,
+                                                                           const uint32_t* light_indices,
+                                                                           uint64_t query_count,
+                                                                           float* probabilities) BF200_NOEXCEPT;
+
 /* Triangle-mesh import for callers that hold meshes as OBJ or ASCII PLY files
  * (engine::load_obj_triangle_mesh / load_ply_triangle_mesh, TriangleMeshImport.hpp:9-17): the
  * same files are accepted and refused, and an accepted file gives the same aligned arrays (one

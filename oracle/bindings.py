@@ -227,6 +227,32 @@ class Reference(_Checker):
             raise CheckerError(self.last_error())
         return results, failures
 
+    def light_tree(self, bounds_min, bounds_max, powers, positions, samples=None, light_indices=None):
+        """The reference's spatial light tree at query points: with samples, (selected slots,
+        probabilities) of sample(context, u); with light_indices, (light_indices, probabilities)
+        of probability(context, i). Refused queries give 0xFFFFFFFF / -1. Returns (None, code)
+        when the tree itself is refused."""
+        import numpy as np
+        bounds_min = np.ascontiguousarray(bounds_min, np.float32).reshape(-1, 3)
+        bounds_max = np.ascontiguousarray(bounds_max, np.float32).reshape(-1, 3)
+        powers = np.ascontiguousarray(powers, np.float32).reshape(-1, 4)
+        positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        n = len(positions)
+        mode = 0 if samples is not None else 1
+        samples = np.ascontiguousarray(samples if samples is not None else np.zeros(n), np.float32)
+        selected = np.ascontiguousarray(light_indices if light_indices is not None else np.zeros(n), np.uint32).copy()
+        probabilities = np.zeros(n, np.float32)
+        f = self.lib.bfr_light_tree
+        f.argtypes = [C.c_void_p] * 3 + [C.c_uint32, C.c_int] + [C.c_void_p] * 2 + [C.c_uint64] + [C.c_void_p] * 2
+        f.restype = C.c_int
+        code = f(bounds_min.ctypes.data_as(C.c_void_p), bounds_max.ctypes.data_as(C.c_void_p),
+                 powers.ctypes.data_as(C.c_void_p), len(powers), mode, positions.ctypes.data_as(C.c_void_p),
+                 samples.ctypes.data_as(C.c_void_p), n, selected.ctypes.data_as(C.c_void_p),
+                 probabilities.ctypes.data_as(C.c_void_p))
+        if code != 0:
+            return None, code
+        return (selected, probabilities), 0
+
     def cone_advance(self, cones, distances):
         """renderer::advance_ray_cone(cone, distance) per case: widths (NaN on error), errors."""
         import numpy as np

@@ -677,6 +677,57 @@ __attribute__((visibility("default"))) int bfr_power_sampler(const float* powers
     return 0;
 }
 
+// The reference's spatial light tree (LightSampler::create_spatial_tree) queried at points:
+// mode 0 samples (samples[q] -> selected[q], probability[q]), mode 1 evaluates the probability of
+// selected[q]. A refused query gives 0xFFFFFFFF / -1; a refused tree returns its StatusCode.
+__attribute__((visibility("default"))) int bfr_light_tree(const float* bounds_min, const float* bounds_max,
+                                                          const float* powers, uint32_t count, int mode,
+                                                          const float* positions, const float* samples,
+                                                          uint64_t query_count, uint32_t* selected,
+                                                          float* probabilities) {
+    std::vector<renderer::LightTreeInputT<renderer::TransportScalar>> lights;
+    lights.reserve(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        const auto bounds = renderer::Bounds3::from_minimum_maximum(
+            renderer::Point3{.x = bounds_min[3 * i], .y = bounds_min[3 * i + 1], .z = bounds_min[3 * i + 2]},
+            renderer::Point3{.x = bounds_max[3 * i], .y = bounds_max[3 * i + 1], .z = bounds_max[3 * i + 2]});
+        if (!bounds) {
+            set_error(bounds.error().message);
+            return static_cast<int>(bounds.error().code);
+        }
+        renderer::LightSpectrumT<renderer::TransportScalar> power{};
+        for (int l = 0; l < 4; ++l) {
+            power.values[l] = powers[4 * i + l];
+        }
+        lights.push_back({.bounds = *bounds, .spectral_power = power});
+    }
+    auto sampler = renderer::LightSampler::create_spatial_tree(lights);
+    if (!sampler) {
+        set_error(sampler.error().message);
+        return static_cast<int>(sampler.error().code);
+    }
+    for (uint64_t q = 0; q < query_count; ++q) {
+        const auto context = renderer::LightSampleContext::create(
+            renderer::Point3{.x = positions[3 * q], .y = positions[3 * q + 1], .z = positions[3 * q + 2]}, 0.5F);
+        if (!context) {
+            if (mode == 0) {
+                selected[q] = 0xFFFFFFFFU;
+            }
+            probabilities[q] = -1.0F;
+            continue;
+        }
+        if (mode == 0) {
+            const auto selection = sampler->sample(*context, samples[q]);
+            selected[q] = selection ? selection->light_index() : 0xFFFFFFFFU;
+            probabilities[q] = selection ? selection->probability().value() : -1.0F;
+        } else {
+            const auto probability = sampler->probability(*context, selected[q]);
+            probabilities[q] = probability ? probability->value() : -1.0F;
+        }
+    }
+    return 0;
+}
+
 // Replaces a scene's light sampler by the power-weighted one (traces then select by power).
 __attribute__((visibility("default"))) int bfr_scene_set_light_powers(void* handle, const float* powers,
                                                                       uint32_t count) {
