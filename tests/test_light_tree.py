@@ -74,3 +74,72 @@ def test_fresh_sets_against_the_compiled_reference():
         assert code == 0
         selected, probability = runtime.light_tree_select(lo, hi, p, positions, samples)
         assert np.array_equal(selected, want[0]) and same(probability, want[1])
+
+
+# The known answers of the reference's own LightTreeTest (Tests/Renderer/Light/LightTreeTest.cpp),
+# float transport scalar.
+
+def point(*xyz):
+    return np.array([xyz], np.float32)
+
+
+def test_spatial_importance_is_symmetric_and_scale_invariant():
+    """LightTreeTest.cpp:125-165: two unit-power point lights at x = -10 and 10."""
+    lo = hi = np.concatenate([point(-10, 0, 0), point(10, 0, 0)])
+    p = np.ones((2, 4), np.float32)
+    q = runtime.light_tree_probability(lo, hi, p, [[-10, 0, 0], [-10, 0, 0], [10, 0, 0], [10, 0, 0]], [0, 1, 0, 1])
+    left_from_left, right_from_left, left_from_right, right_from_right = (float(v) for v in q)
+    eps = float(np.finfo(np.float32).eps)
+    assert abs(left_from_left - 2.0 / 3.0) <= 8 * eps
+    assert abs(left_from_left - right_from_right) <= 2 * eps
+    assert abs(right_from_left - left_from_right) <= 2 * eps
+    assert left_from_left > right_from_left
+    scaled = np.concatenate([point(-1000, 20, 30), point(1000, 20, 30)])
+    again = runtime.light_tree_probability(scaled, scaled, p, [[-1000, 20, 30]], [0])
+    assert again[0] == np.float32(left_from_left)
+
+
+def test_extreme_finite_distances_keep_relative_probability():
+    """LightTreeTest.cpp:208-242: a query at FLT_MAX, and lights at -FLT_MAX and FLT_MAX."""
+    big = np.finfo(np.float32).max
+    eps = float(np.finfo(np.float32).eps)
+    lights = np.concatenate([point(0, 0, 0), point(1, 0, 0)])
+    p = np.ones((2, 4), np.float32)
+    far = runtime.light_tree_probability(lights, lights, p, [[big, 0, 0], [big, 0, 0]], [0, 1])
+    assert all(abs(float(v) - 0.5) <= 8 * eps for v in far)
+    wide = np.concatenate([point(-big, 0, 0), point(big, 0, 0)])
+    assert list(runtime.light_tree_probability(wide, wide, p, [[0, 0, 0], [0, 0, 0]], [0, 1])) == [0.5, 0.5]
+
+
+def test_upper_edge_remap_stays_inside_the_canonical_domain():
+    """LightTreeTest.cpp:244-272: the largest sample below 1 selects the last light of three
+    unbounded lights, with the probability the tree gives that light."""
+    small = np.float32(0.00003418326)
+    half = (np.float32(1) - small) / np.float32(2)
+    lo = np.full((3, 3), -np.inf, np.float32)
+    hi = np.full((3, 3), np.inf, np.float32)
+    p = np.array([[small] * 4, [half] * 4, [half] * 4], np.float32)
+    u = np.nextafter(np.float32(1), np.float32(0))
+    selected, probability = runtime.light_tree_select(lo, hi, p, [[0, 0, 0]], [u])
+    assert selected[0] == 2
+    assert probability[0] == runtime.light_tree_probability(lo, hi, p, [[0, 0, 0]], [2])[0]
+
+
+def test_large_balanced_distribution_is_exactly_normalized():
+    """LightTreeTest.cpp:275-314: 1,024 equal unbounded lights give every light exactly 1/1024 and
+    65,536 stratified samples select each light 64 times."""
+    n = 1024
+    lo = np.full((n, 3), -np.inf, np.float32)
+    hi = np.full((n, 3), np.inf, np.float32)
+    p = np.ones((n, 4), np.float32)
+    where = np.tile(np.array([[17, -3, 9]], np.float32), (n, 1))
+    probabilities = runtime.light_tree_probability(lo, hi, p, where, np.arange(n, dtype=np.uint32))
+    assert (probabilities == np.float32(1) / np.float32(1024)).all()
+    total = np.float32(0)
+    for v in probabilities:
+        total = np.float32(total + v)
+    assert total == np.float32(1)
+    samples = ((np.arange(65536, dtype=np.float32) + np.float32(0.5)) / np.float32(65536)).astype(np.float32)
+    selected, selection = runtime.light_tree_select(lo, hi, p, np.tile(where[:1], (65536, 1)), samples)
+    assert (selection == np.float32(1) / np.float32(1024)).all()
+    assert (np.bincount(selected, minlength=n) == 64).all()
