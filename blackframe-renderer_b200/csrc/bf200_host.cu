@@ -3315,6 +3315,8 @@ blackframe_status get_interface(void*, blackframe_interface_id id, uint32_t majo
         api->render_film = &bf200_render_film;
         api->closest_hits = &bf200_closest_hits;
         api->occlusions = &bf200_occlusions;
+        api->scene_create_from_soa = &bf200_scene_create_from_soa;
+        api->trace_paths_with_cones = &bf200_trace_paths_with_cones;
         return BLACKFRAME_STATUS_SUCCESS;
     }
     return BLACKFRAME_STATUS_INTERFACE_NOT_FOUND;

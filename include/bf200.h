@@ -154,7 +154,7 @@ typedef struct blackframe_xpu_backend_api_v1 {
 /* ---------------------------------------------------------------------------------------- */
 
 #define BF200_RENDER_ABI_MAJOR UINT32_C(1)
-#define BF200_RENDER_ABI_MINOR UINT32_C(0)
+#define BF200_RENDER_ABI_MINOR UINT32_C(1)
 #define BF200_RENDER_INTERFACE_ID_HIGH UINT64_C(0x6266323030726e64) /* "bf200rnd" */
 #define BF200_RENDER_INTERFACE_ID_LOW UINT64_C(0x7761766566726e31) /* "wavefrn1" */
 
@@ -785,7 +785,15 @@ typedef struct bf200_render_api_v1 {
                                       uint64_t, bf200_hit_v1*) BF200_NOEXCEPT;
     blackframe_status (*occlusions)(bf200_context*, const bf200_scene*, const bf200_ray_v1*,
                                     uint64_t, uint32_t*) BF200_NOEXCEPT;
-    uint64_t reserved_slots[4];
+    /* abi_minor 1: the entry points a reference-side adapter needs for the SoA blob and for the
+     * cones and initial states of CudaWavefrontPathInput */
+    blackframe_status (*scene_create_from_soa)(bf200_context*, const void*, uint64_t, bf200_scene**, char*,
+                                               uint64_t) BF200_NOEXCEPT;
+    blackframe_status (*trace_paths_with_cones)(bf200_context*, const bf200_scene*, const bf200_path_input_v1*,
+                                                const bf200_path_state_v1*, const bf200_ray_cone_v1*, uint64_t,
+                                                const bf200_transport_options_v1*, bf200_path_result_v1*,
+                                                bf200_ray_cone_v1*, bf200_report_v1*) BF200_NOEXCEPT;
+    uint64_t reserved_slots[2];
 } bf200_render_api_v1;
 
 /* Derives a pinhole camera the way PinholeCamera::create does (PinholeCamera.hpp:60-99): the

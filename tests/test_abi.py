@@ -71,7 +71,10 @@ def test_extension_query_and_interfaces():
     render_id = abi.InterfaceId(0x6266323030726E64, 0x7761766566726E31)
     assert api.get_interface(None, render_id, 1, 0, C.cast(render, C.c_void_p), 256) == 0
     header = np.frombuffer(bytes(render[:16]), np.uint32)
-    assert header[1] == 1
+    assert header[0] == 120 and header[1] == 1 and header[2] == 1
+    # nine v1.0 entry points, the two of minor 1 (SoA scenes, cones and initial states), two zeros
+    slots = np.frombuffer(bytes(render[16:120]), np.uint64)
+    assert (slots[:11] != 0).all() and (slots[11:] == 0).all()
     # errors: unknown id, wrong major, short output
     assert api.get_interface(None, abi.InterfaceId(1, 2), 1, 0, C.cast(render, C.c_void_p), 256) == 3
     assert api.get_interface(None, render_id, 2, 0, C.cast(render, C.c_void_p), 256) == 2
