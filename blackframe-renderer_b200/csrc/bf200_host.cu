@@ -689,155 +689,6 @@ bool build_light(const bf200_scene_desc_v1& d, uint32_t inst_index, LightInfo& i
     return true;
 }
 
-// ------------------------------------------------------------------------------------------------
-// Power-weighted light selection (LightSampler::create_power_weighted,
-// Blackframe/Renderer/Source/LightSampler.cpp:605-625 with power_weights :200-245 and
-// build_power_cdf :117-190). The steps and their float order are kept alike: the boundaries must be
-// the reference's, bit for bit, or selections and their probabilities would differ.
-// ------------------------------------------------------------------------------------------------
-
-// Neumaier step (add_compensated :78-95): false for a negative or non-finite value or sum.
-bool compensated_add(float value, float& sum, float& correction) {
-    if (!std::isfinite(value) || value < 0.0F) {
-        return false;
-    }
-    const float next = sum + value;
-    if (!std::isfinite(next)) {
-        return false;
-    }
-    if (sum >= value) {
-        correction += (sum - next) + value;
-    } else {
-        correction += (value - next) + sum;
-    }
-    if (!std::isfinite(correction)) {
-        return false;
-    }
-    sum = next;
-    return true;
-}
-
-// The selection CDF (light_count + 1 boundaries) of four-lane spectral powers in registry order.
-blackframe_status power_cdf(const float* powers, uint32_t count, std::vector<float>& cdf, std::string& error,
-                            std::vector<float>* weights_out = nullptr) {
-    if (count == 0) {
-        error = "Light sampling requires at least one registry slot.";
-        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
-    }
-    float peak = 0.0F;
-    for (uint64_t i = 0; i < 4ULL * count; ++i) {
-        if (!std::isfinite(powers[i]) || powers[i] < 0.0F) {
-            error = "Power-weighted light sampling requires finite non-negative spectral lanes.";
-            return BLACKFRAME_STATUS_INVALID_ARGUMENT;
-        }
-        peak = std::max(peak, powers[i]);
-    }
-    if (peak == 0.0F) {
-        error = "Power-weighted light sampling requires positive spectral power.";
-        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
-    }
-    std::vector<float> weights(count);
-    for (uint32_t i = 0; i < count; ++i) {
-        float sum = 0.0F, correction = 0.0F;
-        bool positive = false;
-        for (int l = 0; l < 4; ++l) {
-            const float lane = powers[4ULL * i + l];
-            const float ratio = lane / peak;
-            if (lane > 0.0F) {
-                positive = true;
-                if (!(ratio > 0.0F)) {
-                    error = "A positive spectral power lane is not representable after scaling.";
-                    return BLACKFRAME_STATUS_OUT_OF_RANGE;
-                }
-            }
-            if (!compensated_add(ratio, sum, correction)) {
-                error = "A spectral light-selection weight is not representable.";
-                return BLACKFRAME_STATUS_OUT_OF_RANGE;
-            }
-        }
-        const float weight = sum + correction;
-        if (!std::isfinite(weight) || weight < 0.0F || (positive && !(weight > 0.0F))) {
-            error = "A spectral light-selection weight is not representable.";
-            return BLACKFRAME_STATUS_OUT_OF_RANGE;
-        }
-        weights[i] = weight == 0.0F ? 0.0F : weight;
-    }
-    float total_sum = 0.0F, total_correction = 0.0F;
-    for (float w : weights) {
-        if (!compensated_add(w, total_sum, total_correction)) {
-            error = "Light-selection power accumulation is not representable.";
-            return BLACKFRAME_STATUS_OUT_OF_RANGE;
-        }
-    }
-    float total = total_sum + total_correction;
-    if (!std::isfinite(total) || total < 0.0F) {
-        error = "Light-selection power accumulation is not representable.";
-        return BLACKFRAME_STATUS_OUT_OF_RANGE;
-    }
-    total = total == 0.0F ? 0.0F : total;
-    if (total == 0.0F) {
-        error = "Power-weighted light sampling requires positive spectral power.";
-        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
-    }
-    uint32_t last_positive = count;
-    for (uint32_t i = count; i > 0; --i) {
-        if (weights[i - 1] > 0.0F) {
-            last_positive = i - 1;
-            break;
-        }
-    }
-    cdf.assign(count + 1ULL, 0.0F);
-    float prefix_sum = 0.0F, prefix_correction = 0.0F, previous = 0.0F;
-    for (uint32_t i = 0; i < count; ++i) {
-        const float weight = weights[i];
-        if (weight == 0.0F) {
-            cdf[i + 1ULL] = previous;
-            continue;
-        }
-        if (!compensated_add(weight, prefix_sum, prefix_correction)) {
-            error = "Light-selection power prefix is not representable.";
-            return BLACKFRAME_STATUS_OUT_OF_RANGE;
-        }
-        const float prefix = prefix_sum + prefix_correction;
-        if (!std::isfinite(prefix) || !(prefix > 0.0F)) {
-            error = "Light-selection power prefix is not representable.";
-            return BLACKFRAME_STATUS_OUT_OF_RANGE;
-        }
-        float boundary = 1.0F;
-        if (i != last_positive) {
-            boundary = prefix / total;
-            if (!std::isfinite(boundary) || !(boundary > previous) || !(boundary < 1.0F)) {
-                error = "A positive light-selection probability is not representable.";
-                return BLACKFRAME_STATUS_OUT_OF_RANGE;
-            }
-        } else {
-            const float nominal = weight / total;
-            const float candidate = previous + nominal;
-            if (!std::isfinite(nominal) || !(nominal > 0.0F) || !std::isfinite(candidate) || !(candidate > previous)) {
-                error = "The terminal positive light-selection probability is not representable.";
-                return BLACKFRAME_STATUS_OUT_OF_RANGE;
-            }
-        }
-        cdf[i + 1ULL] = boundary;
-        previous = boundary;
-    }
-    if (cdf[count] != 1.0F) {
-        error = "Light-selection CDF does not terminate at one.";
-        return BLACKFRAME_STATUS_EXTENSION_FAILURE;
-    }
-    for (uint32_t i = 0; i < count; ++i) {
-        const float probability = cdf[i + 1ULL] - cdf[i];
-        if (!std::isfinite(probability) || probability < 0.0F || ((weights[i] > 0.0F) != (probability > 0.0F))) {
-            error = "Light-selection CDF lost or created probability support.";
-            return BLACKFRAME_STATUS_OUT_OF_RANGE;
-        }
-    }
-    if (weights_out != nullptr) {
-        *weights_out = std::move(weights);
-    }
-    return BLACKFRAME_STATUS_SUCCESS;
-}
-
 // A 64-bit hash (FNV-1a's step over 8-byte words, then the tail bytes) of everything a
 // description holds except its instance transforms: a refit must leave all of it unchanged.
 uint64_t description_fingerprint(const bf200_scene_desc_v1& d) {
@@ -1442,15 +1293,6 @@ blackframe_status run_wavefront(bf200_context* c, const bf200_scene* s, PathSour
 
 }  // namespace
 
-namespace bf200 {
-
-blackframe_status light_power_weights(const float* powers, uint32_t count, std::vector<float>& weights,
-                                      std::vector<float>& cdf, std::string& error) {
-    return power_cdf(powers, count, cdf, error, &weights);
-}
-
-}  // namespace bf200
-
 // =============================================================================================
 // C ABI
 // =============================================================================================
@@ -2053,7 +1895,7 @@ BF200_EXPORT blackframe_status bf200_light_power_cdf(const float* spectral_power
     try {
         std::vector<float> cdf;
         std::string error;
-        const blackframe_status st = power_cdf(spectral_powers, light_count, cdf, error);
+        const blackframe_status st = bf200::light_power_cdf(spectral_powers, light_count, cdf, error);
         if (st == BLACKFRAME_STATUS_SUCCESS) {
             std::memcpy(boundaries, cdf.data(), cdf.size() * sizeof(float));
         }
@@ -2084,7 +1926,8 @@ BF200_EXPORT blackframe_status bf200_scene_set_light_powers(bf200_scene* s, cons
             cdf[light_count] = 1.0F;
         } else {
             std::string error;
-            if (const auto st = power_cdf(spectral_powers, light_count, cdf, error); st != BLACKFRAME_STATUS_SUCCESS) {
+            if (const auto st = bf200::light_power_cdf(spectral_powers, light_count, cdf, error);
+                st != BLACKFRAME_STATUS_SUCCESS) {
                 return fail(c, st, error);
             }
         }

@@ -1,4 +1,5 @@
-// Spatial light tree of the reference's LightSampler::create_spatial_tree
+// Power-weighted light selection and the spatial light tree of the reference's LightSampler:
+// LightSampler::create_power_weighted and LightSampler::create_spatial_tree
 // (Blackframe/Renderer/Source/LightSampler.cpp:626-951), built on the host as a flat node array
 // the device can read, and its selection at a shading point (LightSampler.cpp:953-1226).
 #pragma once
@@ -11,8 +12,10 @@
 
 namespace bf200 {
 
-// Power weights and the selection CDF of four-lane spectral powers, as bf200_light_power_cdf
-// computes them (LightSampler.cpp:116-249).
+// The selection CDF (count + 1 boundaries) of four-lane spectral powers in registry order, as
+// LightSampler::create_power_weighted builds it (LightSampler.cpp:116-249, 605-625), and the
+// same with the per-light power weights.
+blackframe_status light_power_cdf(const float* powers, uint32_t count, std::vector<float>& cdf, std::string& error);
 blackframe_status light_power_weights(const float* powers, uint32_t count, std::vector<float>& weights,
                                       std::vector<float>& cdf, std::string& error);
 

@@ -17,6 +17,7 @@
 #include "bfo_exact.h"
 
 #include "../include/bf200.h"
+#include "bf200_light_tree.h"
 
 #include <algorithm>
 #include <array>
@@ -224,6 +225,10 @@ struct Scene {
     std::vector<Instance> instances;
     std::vector<MeshLight> lights;
     std::vector<float> light_cdf;  // uniform boundaries, size light_count + 1
+    // spatial light tree (LightSampler::create_spatial_tree), when installed: selection and MIS
+    // probabilities then depend on the shading / previous vertex position
+    bf200::LightTree tree;
+    bool use_tree = false;
     std::vector<int32_t> light_of_instance;
     Spectrum environment;
     float nm[4], pdf[4];
@@ -2392,7 +2397,16 @@ void add_weighted_emission(Spectrum& acc, const Spectrum& beta, const Spectrum& 
 }
 
 // LightSampler.cpp:1023-1056 (uniform sample) and :1133-1149 (probability).
-uint32_t select_light(const Scene& scene, float u, float& probability) {
+uint32_t select_light(const Scene& scene, float u, float& probability, V3 position) {
+    if (scene.use_tree) {  // LightSampler::sample(context, u) (LightSampler.cpp:1058-1129)
+        const float p[3] = {position.x, position.y, position.z};
+        uint32_t light = 0;
+        std::string error;
+        if (bf200::light_tree_sample(scene.tree, p, u, light, probability, error) != BLACKFRAME_STATUS_SUCCESS) {
+            fail("The light tree refused a selection.");
+        }
+        return light;
+    }
     const auto begin = scene.light_cdf.begin() + 1;
     const auto it = std::upper_bound(begin, scene.light_cdf.end(), u);
     if (it == scene.light_cdf.end()) {
@@ -2403,8 +2417,30 @@ uint32_t select_light(const Scene& scene, float u, float& probability) {
     return static_cast<uint32_t>(index);
 }
 
-float light_probability(const Scene& scene, uint32_t index) {
+float light_probability(const Scene& scene, uint32_t index, V3 position) {
+    if (scene.use_tree) {  // LightSampler::probability(context, i) (LightSampler.cpp:1151-1225)
+        const float p[3] = {position.x, position.y, position.z};
+        float probability = 0.0F;
+        std::string error;
+        if (bf200::light_tree_probability(scene.tree, p, index, probability, error) != BLACKFRAME_STATUS_SUCCESS) {
+            fail("The light tree refused a selection probability.");
+        }
+        return probability;
+    }
     return scene.light_cdf[index + 1] - scene.light_cdf[index];
+}
+
+// validate_sampler_support (SceneMisPathLoop.cpp:397-430) under the light tree: every mesh light
+// must have a representable, positive selection probability at the shading point.
+void validate_tree_support(const Scene& scene, V3 position) {
+    if (!scene.use_tree) {
+        return;
+    }
+    for (uint32_t i = 0; i < scene.lights.size(); ++i) {
+        if (!(light_probability(scene, i, position) > 0.0F)) {
+            fail("The light sampler gives zero support to a non-black mesh area light.");
+        }
+    }
 }
 
 // RussianRoulette.cpp (evaluate): returns false when the path terminates.
@@ -2615,7 +2651,8 @@ Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& 
         return zero;
     }
     float selection;
-    const uint32_t light_index = select_light(scene, stream.sample_1d(dims.light_selection), selection);
+    validate_tree_support(scene, surf.position);
+    const uint32_t light_index = select_light(scene, stream.sample_1d(dims.light_selection), selection, surf.position);
     const MeshLight& light = scene.lights[light_index];
     if ((scene.instances[light.instance].mask & mask) == 0U) {
         return zero;
@@ -2773,7 +2810,7 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
             if (light_index < 0) {
                 fail("A non-black emissive hit is absent from the committed mesh-light registry.");
             }
-            const float selection = light_probability(scene, static_cast<uint32_t>(light_index));
+            const float selection = light_probability(scene, static_cast<uint32_t>(light_index), prev.position);
             const float conditional = mesh_light_pdf_at_surface(scene.lights[light_index], prev.position,
                                                                 surf.position, surf.ng);
             const float light_pdf = joint_light_pdf(selection, conditional);
@@ -3314,6 +3351,25 @@ bool neumaier_add(float value, float& sum, float& correction) {
     }
     sum = next;
     return true;
+}
+
+// Installs the spatial light tree of the scene's mesh lights (bounds and spectral power per light,
+// in registry order); selection and MIS then follow the tree.
+__attribute__((visibility("default"))) int bfo_scene_set_light_tree(void* handle,
+                                                                    const bf200_light_tree_input_v1* lights,
+                                                                    uint32_t count) {
+    auto* s = static_cast<Scene*>(handle);
+    if (count != s->lights.size()) {
+        set_error("one light-tree input per scene light is required");
+        return 1;
+    }
+    std::string error;
+    if (bf200::build_light_tree(lights, count, s->tree, error) != BLACKFRAME_STATUS_SUCCESS) {
+        set_error(error.c_str());
+        return 1;
+    }
+    s->use_tree = true;
+    return 0;
 }
 
 __attribute__((visibility("default"))) int bfo_scene_set_light_powers(void* handle, const float* powers,

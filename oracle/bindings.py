@@ -95,6 +95,15 @@ class _Checker:
         failures = f(*[a.ctypes.data_as(C.c_void_p) for a in arrays], n, out.ctypes.data_as(C.c_void_p))
         return out, failures
 
+    def set_light_tree(self, handle, lights):
+        """Selection (and MIS) by the spatial light tree of `lights`, an array of
+        abi.LightTreeInput in registry order."""
+        f = getattr(self.lib, self.prefix + "_scene_set_light_tree")
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        f.restype = C.c_int
+        if f(handle, C.cast(lights, C.c_void_p), len(lights)) != 0:
+            raise CheckerError(self.last_error())
+
     def trace(self, handle, inputs, options, threads=None):
         n = len(inputs)
         results = (abi.PathResult * n)()

@@ -728,6 +728,35 @@ __attribute__((visibility("default"))) int bfr_light_tree(const float* bounds_mi
     return 0;
 }
 
+// Replaces a scene's light sampler by the spatial light tree of the given per-light bounds and
+// spectral powers (registry order); traces then select by the tree.
+__attribute__((visibility("default"))) int bfr_scene_set_light_tree(void* handle, const bf200_light_tree_input_v1* in,
+                                                                    uint32_t count) {
+    auto* scene = static_cast<RefScene*>(handle);
+    std::vector<renderer::LightTreeInputT<renderer::TransportScalar>> lights;
+    for (uint32_t i = 0; i < count; ++i) {
+        const auto bounds = renderer::Bounds3::from_minimum_maximum(
+            renderer::Point3{.x = in[i].bounds_min[0], .y = in[i].bounds_min[1], .z = in[i].bounds_min[2]},
+            renderer::Point3{.x = in[i].bounds_max[0], .y = in[i].bounds_max[1], .z = in[i].bounds_max[2]});
+        if (!bounds) {
+            set_error(bounds.error().message);
+            return static_cast<int>(bounds.error().code);
+        }
+        renderer::LightSpectrumT<renderer::TransportScalar> power{};
+        for (int l = 0; l < 4; ++l) {
+            power.values[l] = in[i].spectral_power[l];
+        }
+        lights.push_back({.bounds = *bounds, .spectral_power = power});
+    }
+    auto sampler = renderer::LightSampler::create_spatial_tree(lights);
+    if (!sampler) {
+        set_error(sampler.error().message);
+        return static_cast<int>(sampler.error().code);
+    }
+    scene->sampler = std::make_unique<renderer::LightSampler>(std::move(*sampler));
+    return 0;
+}
+
 // Replaces a scene's light sampler by the power-weighted one (traces then select by power).
 __attribute__((visibility("default"))) int bfr_scene_set_light_powers(void* handle, const float* powers,
                                                                       uint32_t count) {

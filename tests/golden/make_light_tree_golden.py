@@ -6,7 +6,9 @@ canonical samples (slot and probability) and the probability of every light.
 The sets cover one light, clustered and spread boxes, flat and point-like boxes, zero-power
 lights, canonically unbounded lights beside finite ones and alone, and coincident centroids.
 
-Run from the repository root: python tests/golden/make_light_tree_golden.py
+Run from the repository root: python tests/golden/make_light_tree_golden.py, and with the argument
+`transport` for tests/golden/light_tree_transport.npz: the reference's trace_scene_mis selecting
+by the tree on a three-light Cornell box.
 """
 import os
 import sys
@@ -99,5 +101,55 @@ def main():
     print(f"{len(sets)} light sets written")
 
 
+def tree_box_inputs(builder):
+    """bf200_light_tree_input_v1 per emissive instance of a builder (registry order): the world
+    bounds of its mesh and its flux per lane (radiance x area x pi)."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from bf200 import abi
+    from test_gpu_light_power import light_powers
+    powers = light_powers(builder)
+    lights = (abi.LightTreeInput * len(powers))()
+    k = 0
+    for mesh_index, material, to_world, _ in builder.instances:
+        if not any(v != 0 for v in builder.materials[material][1]):
+            continue
+        m = np.asarray(to_world, np.float64).reshape(4, 4)
+        p = np.asarray(builder.meshes[mesh_index].positions, np.float64)
+        world = (p @ m[:3, :3].T + m[:3, 3]).astype(np.float32)
+        lights[k].bounds_min[:] = [float(v) for v in world.min(axis=0)]
+        lights[k].bounds_max[:] = [float(v) for v in world.max(axis=0)]
+        lights[k].spectral_power[:] = [float(v) for v in powers[k]]
+        k += 1
+    return lights
+
+
+def transport():
+    """The reference's trace_scene_mis with the spatial light tree on the three-light box:
+    tests/golden/light_tree_transport.npz."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from bf200 import abi
+    from oracle.bindings import Oracle
+    from test_gpu_light_power import path_inputs, three_light_box
+    builder = three_light_box()
+    lights = tree_box_inputs(builder)
+    inputs = path_inputs(Oracle(), 512, 23)
+    options = abi.default_options(mis="power", max_depth=8)
+    ref = Reference()
+    h = ref.scene(builder)
+    ref.set_light_tree(h, lights)
+    results, failures = ref.trace(h, inputs, options)
+    ref.destroy(h)
+    np.savez_compressed(os.path.join(HERE, "light_tree_transport.npz"),
+                        radiance=np.array([list(r.radiance) for r in results], np.float32),
+                        beta=np.array([list(r.beta) for r in results], np.float32),
+                        depth=np.array([r.depth for r in results], np.uint32),
+                        termination=np.array([r.termination for r in results], np.uint32),
+                        lane_status=np.array([r.lane_status for r in results], np.uint32))
+    print(f"tree transport: 512 paths, {failures} refused")
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "transport":
+        transport()
+    else:
+        main()

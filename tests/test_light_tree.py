@@ -143,3 +143,40 @@ def test_large_balanced_distribution_is_exactly_normalized():
     selected, selection = runtime.light_tree_select(lo, hi, p, np.tile(where[:1], (65536, 1)), samples)
     assert (selection == np.float32(1) / np.float32(1024)).all()
     assert (np.bincount(selected, minlength=n) == 64).all()
+
+
+def test_oracle_tree_transport_matches_the_reference(golden):
+    """The oracle selecting by the tree inside transport (NEE at the shading point, emission MIS at
+    the previous vertex, every light's support checked at each shading point) against the
+    reference's trace_scene_mis with LightSampler::create_spatial_tree on the three-light box
+    (tests/golden/light_tree_transport.npz, `make_light_tree_golden.py transport`)."""
+    from bf200 import abi
+    from helpers import arrays, bit_equal
+    from oracle.bindings import Oracle
+    from test_gpu_light_power import path_inputs, three_light_box
+    spec = importlib.util.spec_from_file_location(
+        "make_light_tree_golden", os.path.join(os.path.dirname(__file__), "golden", "make_light_tree_golden.py"))
+    maker = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(maker)
+    g = golden("light_tree_transport")
+    builder = three_light_box()
+    oracle = Oracle()
+    inputs = path_inputs(oracle, 512, 23)
+    h = oracle.scene(builder)
+    oracle.set_light_tree(h, maker.tree_box_inputs(builder))
+    results, failures = oracle.trace(h, inputs, abi.default_options(mis="power", max_depth=8))
+    plain, _ = oracle.trace(h, inputs, abi.default_options(mis="power", max_depth=8))
+    oracle.destroy(h)
+    got = arrays(results)
+    assert failures == 0 and (g["lane_status"] == 0).all()
+    for key in ("radiance", "beta"):
+        assert bit_equal(got[key], g[key]).all(), key
+    for key in ("depth", "termination"):
+        assert np.array_equal(got[key], g[key]), key
+    # the tree changes the selection, so the radiance differs from uniform selection on most paths
+    uniform = Oracle()
+    h = uniform.scene(builder)
+    base, _ = uniform.trace(h, inputs, abi.default_options(mis="power", max_depth=8))
+    uniform.destroy(h)
+    assert (~bit_equal(arrays(base)["radiance"], got["radiance"]).all(axis=1)).mean() > 0.3
+    assert bit_equal(arrays(plain)["radiance"], got["radiance"]).all()
