@@ -16,7 +16,7 @@ CSRC = os.path.join(os.path.dirname(PACKAGE_DIR), "csrc")
 REPO = os.path.dirname(os.path.dirname(PACKAGE_DIR))
 INCLUDE = os.path.join(REPO, "include")
 LIBRARY = os.path.join(PACKAGE_DIR, "libbf200.so")
-SOURCES = ["bf200_kernels.cu", "bf200_compact.cu", "bf200_sobol.cu", "bf200_host.cu", "bf200_import.cpp", "bf200_soa.cpp", "bf200_light_tree.cpp"]
+SOURCES = ["bf200_kernels.cu", "bf200_compact.cu", "bf200_sobol.cu", "bf200_host.cu", "bf200_import.cpp", "bf200_soa.cpp", "bf200_light_tree.cpp", "bf200_light_tree.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-std=c++17", "-O3", "-lineinfo", "-fmad=false",

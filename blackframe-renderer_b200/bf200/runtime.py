@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = [
     "bf200_trace_paths_with_cones_device",
     "bf200_light_tree_select",
     "bf200_light_tree_probability",
+    "bf200_light_tree_select_device",
 ]
 
 
@@ -420,6 +421,19 @@ def light_tree_select(bounds_min, bounds_max, powers, positions, samples):
     if status != 0:
         raise Bf200Error(status, "light tree refused")
     return selected, probabilities
+
+
+def light_tree_select_device(bounds_min, bounds_max, powers, device_positions, device_samples, query_count,
+                             device_light_indices, device_probabilities):
+    """bf200_light_tree_select_device: positions, samples and outputs are device pointers (ints)."""
+    lights = _light_tree_inputs(bounds_min, bounds_max, powers)
+    f = library().bf200_light_tree_select_device
+    f.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    f.restype = C.c_uint32
+    status = f(C.cast(lights, C.c_void_p), len(lights), device_positions, device_samples, query_count,
+               device_light_indices, device_probabilities)
+    if status != 0:
+        raise Bf200Error(status, "light tree refused")
 
 
 def light_tree_probability(bounds_min, bounds_max, powers, positions, light_indices):

@@ -701,6 +701,15 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_tree_select(const bf20
                                                                       const float* samples, uint64_t query_count,
                                                                       uint32_t* light_indices,
                                                                       float* probabilities) BF200_NOEXCEPT;
+/* bf200_light_tree_select with positions, samples and results in device memory: the tree is built
+ * on the host and traversed on the device, one query per thread. Logarithms and exponentials are
+ * the double-precision values rounded to float, within about an ulp of the C library's, so a
+ * probability may differ from bf200_light_tree_select's in its last bits. Synchronises before
+ * returning. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_tree_select_device(
+    const bf200_light_tree_input_v1* lights, uint32_t light_count, const float* device_positions,
+    const float* device_samples, uint64_t query_count, uint32_t* device_light_indices,
+    float* device_probabilities) BF200_NOEXCEPT;
 /* The tree's probability of selecting light_indices[q] at positions[q] (probability(context, i),
  * LightSampler.cpp:1151-1225); -1 where the reference refuses the query. */
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_tree_probability(const bf200_light_tree_input_v1* lights,
