@@ -1107,7 +1107,7 @@ __global__ void __launch_bounds__(256, BF200_INTERSECT_MIN_BLOCKS) k_trace(Scene
             continue;
         }
         if (lane == static_cast<uint32_t>(__ffs(busy_mask) - 1) && idle_mask != 0U) {
-            // extension segments started in this round (lanes that took an active slot)
+            // extension segments started in this pass (lanes that took an active slot)
             const unsigned started = busy_mask & idle_mask;
             if (started != 0U) {
                 atomicAdd(&w.counters[3], static_cast<unsigned long long>(__popc(started)));
