@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = [
     "bf200_light_tree_select",
     "bf200_light_tree_probability",
     "bf200_light_tree_select_device",
+    "bf200_scene_set_light_tree",
 ]
 
 
@@ -156,6 +157,17 @@ class Scene:
         desc = builder.desc() if desc is None else desc
         self.context._check(library().bf200_scene_refit(self.handle, C.byref(desc)), "scene_refit")
         self.builder = builder
+
+    def set_light_tree(self, lights):
+        """bf200_scene_set_light_tree: select lights by the spatial tree of `lights` (an array of
+        abi.LightTreeInput in registry order), or by the scene's CDF again with None."""
+        f = library().bf200_scene_set_light_tree
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        f.restype = C.c_uint32
+        status = f(self.handle, C.cast(lights, C.c_void_p) if lights is not None else None,
+                   len(lights) if lights is not None else 0)
+        if status != 0:
+            raise Bf200Error(status, "set_light_tree")
 
     def close(self):
         if self.handle:

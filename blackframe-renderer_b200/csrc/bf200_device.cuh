@@ -5,6 +5,7 @@
 
 #include "bf200.h"
 #include "bf200_shading.cuh"
+#include "bf200_light_tree.h"
 
 namespace bf200 {
 
@@ -76,6 +77,13 @@ struct SceneView {
     const float* light_tri_cdf;
     float4 environment;
     uint32_t sphere_count;  // analytic sphere geometries (0: the walks run their triangle-only form)
+    // spatial light tree (bf200_scene_set_light_tree); null: selection by light_select_cdf
+    const LightTreeNode* tree;
+    const uint32_t* tree_light_to_node;
+    uint32_t tree_node_count;
+    uint32_t tree_root;
+    float tree_log_extent;
+    uint32_t tree_has_extent;
 };
 
 // geom_info.w: the geometry's kind. A sphere's geom_info.x is its leaf record (centre, radius).

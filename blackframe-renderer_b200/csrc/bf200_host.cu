@@ -1907,6 +1907,61 @@ BF200_EXPORT blackframe_status bf200_light_power_cdf(const float* spectral_power
 
 // The scene's light-selection CDF: power-weighted from `spectral_powers` (4 per light), or uniform
 // again (LightSampler::create_uniform) when it is null.
+BF200_EXPORT blackframe_status bf200_scene_set_light_tree(bf200_scene* s, const bf200_light_tree_input_v1* lights,
+                                                          uint32_t light_count) noexcept {
+    if (s == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    bf200_context* c = s->context;
+    if (lights == nullptr) {  // back to selection by the scene's CDF
+        s->view.tree = nullptr;
+        s->view.tree_light_to_node = nullptr;
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    if (light_count != s->light_count) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "one light-tree input per scene light is required");
+    }
+    try {
+        bf200::LightTree tree;
+        std::string error;
+        if (const auto st = bf200::build_light_tree(lights, light_count, tree, error); st != BLACKFRAME_STATUS_SUCCESS) {
+            return fail(c, st, error);
+        }
+        cudaSetDevice(c->device);
+        void* nodes = nullptr;
+        void* map = nullptr;
+        const size_t node_bytes = tree.nodes.size() * sizeof(bf200::LightTreeNode);
+        const size_t map_bytes = tree.light_to_node.size() * sizeof(uint32_t);
+        cudaError_t e = cudaMalloc(&nodes, node_bytes);
+        if (e == cudaSuccess) {
+            s->allocations.push_back(nodes);
+            e = cudaMalloc(&map, map_bytes);
+        }
+        if (e == cudaSuccess) {
+            s->allocations.push_back(map);
+            e = cudaMemcpyAsync(nodes, tree.nodes.data(), node_bytes, cudaMemcpyHostToDevice, c->stream);
+        }
+        if (e == cudaSuccess) {
+            e = cudaMemcpyAsync(map, tree.light_to_node.data(), map_bytes, cudaMemcpyHostToDevice, c->stream);
+        }
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(c->stream);
+        }
+        if (e != cudaSuccess) {
+            return cuda_fail(c, e, "light-tree upload");
+        }
+        s->view.tree = static_cast<const bf200::LightTreeNode*>(nodes);
+        s->view.tree_light_to_node = static_cast<const uint32_t*>(map);
+        s->view.tree_node_count = static_cast<uint32_t>(tree.nodes.size());
+        s->view.tree_root = tree.root;
+        s->view.tree_log_extent = tree.root_log_extent;
+        s->view.tree_has_extent = tree.root_has_extent ? 1U : 0U;
+    } catch (const std::bad_alloc&) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "light-tree construction exhausted host memory");
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
 BF200_EXPORT blackframe_status bf200_scene_set_light_powers(bf200_scene* s, const float* spectral_powers,
                                                             uint32_t light_count) noexcept {
     if (s == nullptr) {
@@ -1916,6 +1971,8 @@ BF200_EXPORT blackframe_status bf200_scene_set_light_powers(bf200_scene* s, cons
     if (light_count != s->light_count) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "one spectral power per scene light is required");
     }
+    s->view.tree = nullptr;  // selection by the CDF this call installs
+    s->view.tree_light_to_node = nullptr;
     try {
         std::vector<float> cdf;
         if (spectral_powers == nullptr) {
@@ -2519,6 +2576,9 @@ blackframe_status check_adjoint_scene(bf200_context* c, const bf200_scene* s) {
     }
     if (s->material_count > kAdjointMaterials) {
         return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "the adjoint takes scenes of at most 64 materials");
+    }
+    if (s->view.tree != nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "the adjoint does not replay light-tree selection");
     }
     return BLACKFRAME_STATUS_SUCCESS;
 }

@@ -21,6 +21,7 @@
 #include "bf200_device.cuh"
 #include "bf200_kernels.h"
 #include "bf200_sphere.cuh"
+#include "bf200_light_tree_device.cuh"
 
 // Resident 256-thread blocks per SM the register allocation must allow, per stage kernel.
 #ifndef BF200_INTERSECT_MIN_BLOCKS
@@ -1482,7 +1483,7 @@ __device__ __forceinline__ bool is_black4(const float (&v)[4]) {
 
 // SceneMisPathLoop.cpp:136-275 (estimate) without the visibility query: the record carries the
 // shadow ray and the contribution it adds when unoccluded (transmittance 1).
-template <int K>
+template <int K, bool TREE>
 __device__ void direct_lighting(const SceneView& s, const TransportParams& p, const Surface& surf,
                                 const ClosureData& closure, uint32_t allowed, const float4 beta4, F3 wo_world,
                                 uint64_t dims, const Stream& stream, uint32_t mask, ShadowRecord& rec, Lane& lane) {
@@ -1492,12 +1493,23 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
         return;
     }
     const float u_sel = stream.sample_1d(dims + 0);
-    const uint32_t b = upper_bound(s.light_select_cdf + 1, s.light_count, u_sel);
-    if (b >= s.light_count) {
-        lane.fail();
-        return;
+    uint32_t b = 0;
+    float selection = 0.0F;
+    if constexpr (TREE) {  // LightSampler::sample(context, u) at the shading point
+        const float at[3] = {surf.position.x, surf.position.y, surf.position.z};
+        if (!d_tree_select(s.tree, s.tree_node_count, s.tree_root, s.light_count, s.tree_log_extent,
+                           s.tree_has_extent != 0U, at, u_sel, b, selection)) {
+            lane.fail();
+            return;
+        }
+    } else {
+        b = upper_bound(s.light_select_cdf + 1, s.light_count, u_sel);
+        if (b >= s.light_count) {
+            lane.fail();
+            return;
+        }
+        selection = s.light_select_cdf[b + 1] - s.light_select_cdf[b];
     }
-    const float selection = s.light_select_cdf[b + 1] - s.light_select_cdf[b];
     const LightInfo light = s.lights[b];
     if ((s.inst_info[light.instance].z & mask) == 0U) {
         return;
@@ -1717,8 +1729,9 @@ __device__ __forceinline__ void adjoint_flush(double* sum, double* gradients) {
 // misses and any other material). The route queue lists the route's slots in slot order.
 // ADJ: the replay of the path-replay adjoint (`a` is read only then).
 // K: closure kind (0 reads it from the record); ADJ: path-replay adjoint; CONE: the slots carry ray
-// cones (the cone column is read and written only then).
-template <int K, bool ADJ, bool CONE>
+// cones (the cone column is read and written only then); TREE: lights are selected by the scene's
+// spatial light tree.
+template <int K, bool ADJ, bool CONE, bool TREE>
 __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView s, Wavefront w, PathSource src, TransportParams p,
                                                uint32_t route, AdjointView a) {
     __shared__ double adjoint_sum[ADJ ? kAdjointWords : 1];
@@ -1799,7 +1812,17 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                             lane.fail();
                         } else {
                             const LightInfo light = s.lights[light_index];
-                            const float selection = s.light_select_cdf[light_index + 1] - s.light_select_cdf[light_index];
+                            float selection = 0.0F;
+                            if constexpr (TREE) {  // probability(context, i) at the previous vertex
+                                const float at[3] = {prev.x, prev.y, prev.z};
+                                if (!d_tree_probability(s.tree, s.tree_node_count, s.tree_root, s.tree_light_to_node,
+                                                        s.light_count, s.tree_log_extent, s.tree_has_extent != 0U, at,
+                                                        light_index, selection)) {
+                                    lane.fail();
+                                }
+                            } else {
+                                selection = s.light_select_cdf[light_index + 1] - s.light_select_cdf[light_index];
+                            }
                             const F3 pp = ld3(prev);
                             float conditional = 0.0F;
                             if (emission_side(surf.ng, pp - surf.position, lane) > 0) {
@@ -1896,7 +1919,8 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                         next_depth = depth_advance(depth, bs.lobes);
                     }
                     if (lane.err == 0) {
-                        direct_lighting<K>(s, p, surf, closure, allowed, beta, wo_world, dims, stream, mask, rec, lane);
+                        direct_lighting<K, TREE>(s, p, surf, closure, allowed, beta, wo_world, dims, stream, mask, rec,
+                                                 lane);
                         if constexpr (ADJ) {
                             if (al.on && rec.valid) {
                                 double2 score = make_double2(0.0, 0.0);
@@ -2374,15 +2398,16 @@ cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instanc
     return cudaGetLastError();
 }
 
-template <bool ADJ, bool CONE>
+template <bool ADJ, bool CONE, bool TREE>
 void launch_shading(const SceneView& s, const Wavefront& w, const PathSource& src, const TransportParams& p,
                     uint32_t grid, const AdjointView& a, cudaStream_t stream) {
-    k_shade<0, ADJ, CONE><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteGeneric, a);
-    k_shade<static_cast<int>(kClosureLambert), ADJ, CONE><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteLambert, a);
-    k_shade<static_cast<int>(kClosureConductor), ADJ, CONE><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteConductor,
-                                                                                      a);
-    k_shade<static_cast<int>(kClosureDielectric), ADJ, CONE><<<grid, 256, 0, stream>>>(s, w, src, p,
-                                                                                       kRouteDielectric, a);
+    k_shade<0, ADJ, CONE, TREE><<<grid, 256, 0, stream>>>(s, w, src, p, kRouteGeneric, a);
+    k_shade<static_cast<int>(kClosureLambert), ADJ, CONE, TREE><<<grid, 256, 0, stream>>>(s, w, src, p,
+                                                                                           kRouteLambert, a);
+    k_shade<static_cast<int>(kClosureConductor), ADJ, CONE, TREE><<<grid, 256, 0, stream>>>(s, w, src, p,
+                                                                                             kRouteConductor, a);
+    k_shade<static_cast<int>(kClosureDielectric), ADJ, CONE, TREE><<<grid, 256, 0, stream>>>(s, w, src, p,
+                                                                                              kRouteDielectric, a);
 }
 
 cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, const PathSource& src,
@@ -2411,11 +2436,17 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
             return e;
         }
         if (adjoint != nullptr) {
-            launch_shading<true, false>(s, w, src, p, grid, *adjoint, stream);
+            launch_shading<true, false, false>(s, w, src, p, grid, *adjoint, stream);
+        } else if (s.tree != nullptr) {
+            if (src.cones_in != nullptr) {
+                launch_shading<false, true, true>(s, w, src, p, grid, AdjointView{}, stream);
+            } else {
+                launch_shading<false, false, true>(s, w, src, p, grid, AdjointView{}, stream);
+            }
         } else if (src.cones_in != nullptr) {
-            launch_shading<false, true>(s, w, src, p, grid, AdjointView{}, stream);
+            launch_shading<false, true, false>(s, w, src, p, grid, AdjointView{}, stream);
         } else {
-            launch_shading<false, false>(s, w, src, p, grid, AdjointView{}, stream);
+            launch_shading<false, false, false>(s, w, src, p, grid, AdjointView{}, stream);
         }
         *launches += 4U;
         if ((e = cudaGetLastError()) != cudaSuccess) {

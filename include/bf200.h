@@ -701,6 +701,17 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_tree_select(const bf20
                                                                       const float* samples, uint64_t query_count,
                                                                       uint32_t* light_indices,
                                                                       float* probabilities) BF200_NOEXCEPT;
+/* Selects the scene's lights by the spatial light tree of `lights` (one per scene light, registry
+ * order) in every later trace and render: next-event estimation draws a light with
+ * LightSampler::sample(context, u) at the shading point, and the MIS weight of an emissive hit
+ * uses probability(context, i) at the previous vertex (SceneMisPathLoop.cpp:153-172, 324-329).
+ * The per-light support check the reference makes at each shading point
+ * (validate_sampler_support) is not repeated on the device. lights == NULL returns to the
+ * scene's CDF selection; bf200_scene_set_light_powers also replaces the tree. The adjoint refuses
+ * a scene that selects by a tree (INVALID_STATE). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_set_light_tree(bf200_scene* scene,
+                                                                         const bf200_light_tree_input_v1* lights,
+                                                                         uint32_t light_count) BF200_NOEXCEPT;
 /* bf200_light_tree_select with positions, samples and results in device memory: the tree is built
  * on the host and traversed on the device, one query per thread. Logarithms and exponentials are
  * the double-precision values rounded to float, within about an ulp of the C library's, so a

@@ -41,3 +41,46 @@ def test_device_light_tree_matches_the_reference(golden):
         exact += int((valid & (probabilities.view(np.uint32) == want_probabilities.view(np.uint32))).sum())
     assert agree >= 0.99 * total, (agree, total)
     print(f"light tree on the device: {agree}/{total} selections agree, {exact} probabilities bit-exact")
+
+
+def test_tree_selected_paths_match_the_oracle():
+    """Transport selecting lights by the tree (bf200_scene_set_light_tree) on the three-light box:
+    per-path radiance against the oracle's tree transport, whose results are bit-exact against the
+    reference's trace_scene_mis with the tree (tests/test_light_tree.py), with the tolerances of the
+    other parity tests. Clearing the tree gives the uniform-selection render again, bit for bit."""
+    import importlib.util
+    import os
+    from bf200 import abi
+    from helpers import arrays, bit_equal, check_paths
+    from oracle.bindings import Oracle
+    from test_gpu_light_power import path_inputs, three_light_box
+    spec = importlib.util.spec_from_file_location(
+        "make_light_tree_golden", os.path.join(os.path.dirname(__file__), "golden", "make_light_tree_golden.py"))
+    maker = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(maker)
+    builder = three_light_box()
+    lights = maker.tree_box_inputs(builder)
+    oracle = Oracle()
+    inputs = path_inputs(oracle, 4096, 31)
+    options = abi.default_options(mis="power", max_depth=8)
+    h = oracle.scene(builder)
+    oracle.set_light_tree(h, lights)
+    expected, failures = oracle.trace(h, inputs, options)
+    oracle.destroy(h)
+    with runtime.Context(0, path_capacity=1 << 16) as ctx:
+        scene = ctx.create_scene(builder)
+        uniform, _ = ctx.trace_paths(scene, inputs, options)
+        scene.set_light_tree(lights)
+        results, report = ctx.trace_paths(scene, inputs, options)
+        scene.set_light_tree(None)
+        again, _ = ctx.trace_paths(scene, inputs, options)
+        scene.close()
+    got, want = arrays(results), arrays(expected)
+    assert failures == 0 and report.failed_lanes == 0
+    # the device's rounded double logarithms and exponentials leave about 1 % of tree probabilities
+    # an ulp from the C library's; a path evaluates several, so fewer paths are bit-exact than in the
+    # CDF-selection tests, while all stay within the relative 1e-5 gate
+    exact, close = check_paths(got, want, "light-tree selection")
+    assert exact >= 0.8
+    assert (~bit_equal(arrays(uniform)["radiance"], got["radiance"]).all(axis=1)).mean() > 0.3
+    assert bit_equal(arrays(again)["radiance"], arrays(uniform)["radiance"]).all()
