@@ -707,8 +707,9 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_light_tree_select(const bf20
  * uses probability(context, i) at the previous vertex (SceneMisPathLoop.cpp:153-172, 324-329).
  * The per-light support check the reference makes at each shading point
  * (validate_sampler_support) is not repeated on the device. lights == NULL returns to the
- * scene's CDF selection; bf200_scene_set_light_powers also replaces the tree. The adjoint refuses
- * a scene that selects by a tree (INVALID_STATE). */
+ * scene's CDF selection; bf200_scene_set_light_powers also replaces the tree. A refit keeps the
+ * tree as given: set it again with the moved lights' bounds. The adjoint refuses a scene that
+ * selects by a tree (INVALID_STATE). */
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_set_light_tree(bf200_scene* scene,
                                                                          const bf200_light_tree_input_v1* lights,
                                                                          uint32_t light_count) BF200_NOEXCEPT;
