@@ -1,17 +1,25 @@
 """Benchmark of the wavefront path-tracing hot path (one JSON line on rank 0).
 
-Workload (one step = one full frame): the Cornell box at 256 x 256, 256 samples per pixel, with
-a GGX conductor sphere and a GGX rough dielectric sphere (64 x 32 UV spheres), power MIS, depth
-16, Russian roulette from depth 3 — 16,777,216 path samples per frame and GPU. The scene,
-camera rays, transport and film accumulation all run on the device (inputs resident in HBM);
-`e2e` times the public C-ABI call with host film buffers (bf200_render_film), copies included.
+Workload (one step = one full frame): the BVH-stress scene -- 985,090 unique float32 triangles
+(three seeded displaced subdivision-7 icospheres instanced 40 times by seeded affine transforms in
+a 20^3 volume over a ground plane; 50 % Lambert, 30 % anisotropic GGX conductor, 20 % GGX
+dielectric), a 2,048-triangle emissive mesh light and a constant environment of radiance 0.5 --
+at 1920 x 1080, 64 samples per pixel, depth 16, power MIS, Russian roulette from depth 3:
+132,710,400 path samples per frame and GPU. The scene, camera rays, transport and film
+accumulation all run on the device (inputs resident in HBM); `e2e` times the public C-ABI call
+with host film buffers (bf200_render_film), copies included. `--workload cornell_spheres_256`
+selects the 256 x 256 x 256 spp Cornell box with its GGX conductor and dielectric spheres.
 
 Metric: path samples per second (whole job; weak scaling: every rank renders its own disjoint
 sample range of the same frame and the per-GPU films are summed with one NCCL all-reduce).
 
 `--impl reference` times the reference's own CPU implementation of the path (oracle/_ref: the
-reference sources compiled as-is, trace_scene_mis + analytic accel + caller-side film) on the
-host cores over a bounded sample of the same workload.
+reference sources compiled as-is, trace_scene_mis + analytic accel + caller-side film, primary
+rays from the reference's PinholeCamera) on the host cores over a bounded sample of the same
+workload. `--impl reference-cuda` times the reference's own CUDA backend (oracle/_ref/
+libbfrefcuda.so: trace_cuda_wavefront_transport with a reused workspace, as its benchmark calls
+it) on one-sample-per-pixel batches of the same frame (2,073,600 paths per call at 1080p), and
+bf200_trace_paths_with_cones on the same inputs in the same process.
 """
 import argparse
 import ctypes as C
@@ -32,8 +40,11 @@ import numpy as np  # noqa: E402
 
 from bf200 import abi, multigpu, runtime, scenes  # noqa: E402
 
-WORKLOAD = "cornell_spheres_256"
+WORKLOAD = "bvh_stress_1080p"
 METRIC = "path samples/s"
+# every workload resolves its materials at the same wavelength packet (sample 0.1), whose CIE
+# sensor constants the reference computed into this Cornell fixture
+SENSOR_FIXTURE = "cornell_spheres_256"
 # algorithmic bytes (the per-unit model of the path: rays, hits, path state, queue slots, film)
 CAMERA_RAY_BYTES = 28
 EXTENSION_SEGMENT_BYTES = 240
@@ -45,11 +56,12 @@ FILM_SAMPLE_BYTES = 24
 STAGE_BYTES_PER_UNIT = {"trace": 48, "shade": EXTENSION_SEGMENT_BYTES - 48, "occlude": SHADOW_SEGMENT_BYTES}
 STAGE_KERNELS = {"trace": "k_trace", "shade": "k_shade<kind> x4 + route/shadow compaction",
                  "occlude": "k_occlude"}
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per processed unit, from one ncu
-# capture of a full-wavefront launch (2,097,152 segments) of each stage's kernels in this build;
-# profiles/stages_cornell_spheres_256_spp64.md holds the capture and its command
-MEASURED_TRAFFIC_PER_UNIT = {"trace": 56.5, "shade": 372.0, "occlude": None}
-TRAFFIC_SOURCE = "profiles/stages_cornell_spheres_256_spp64.md"
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per processed unit, per workload, from
+# one ncu capture of a full-wavefront launch of each stage's kernels in this build (the stage
+# kernels' launches at 2,097,152 slots)
+MEASURED_TRAFFIC_PER_UNIT = {
+    "cornell_spheres_256": {"trace": 56.5, "shade": 372.0, "occlude": None},
+}
 
 
 def measured_peaks():
@@ -109,9 +121,7 @@ class ClockSampler:
 
 def workload_setup(workload):
     builder, options, (width, height, spp) = scenes.build_workload(workload)
-    # every workload resolves its materials at the same wavelength packet (sample 0.1), whose CIE
-    # sensor constants the reference computed into the Cornell fixture
-    g = np.load(os.path.join(REPO, "tests", "golden", f"{WORKLOAD}.npz"))
+    g = np.load(os.path.join(REPO, "tests", "golden", f"{SENSOR_FIXTURE}.npz"))
     from helpers import sensor_from_golden
     sensor = sensor_from_golden(g)
     origin, normal, tangent, vfov = scenes.workload_camera(workload)
@@ -119,43 +129,115 @@ def workload_setup(workload):
     return builder, options, camera, sensor, (width, height, spp)
 
 
-def cpu_sample_rate(target_seconds=15.0):
-    """Times the reference CPU path (oracle/_ref when built, else the oracle restatement) on a
-    bounded sample of the workload's paths; returns (paths/s, threads, kind, sample text)."""
-    from oracle.bindings import Oracle, Reference, reference_available
-    builder, options, (width, height, spp) = scenes.build_workload(WORKLOAD)
-    checker = Reference() if reference_available() else Oracle()
-    kind = "reference" if reference_available() else "port"
-    threads = os.cpu_count() or 1
-    handle = checker.scene(builder)
-    cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV,
-                                scenes.PATH_TIME)
-    rng = np.random.default_rng(5)
+def frame_samples(width, height, sample_index, seed=0, pixels=None):
+    """SampleIndex records of a frame's pixels (row-major, or the given (x, y) pairs) at one sample
+    index, built in bulk."""
+    if pixels is None:
+        ys, xs = np.divmod(np.arange(width * height, dtype=np.uint64), np.uint64(width))
+    else:
+        xs, ys = pixels[:, 0], pixels[:, 1]
+    n = len(xs)
+    table = np.zeros(n, dtype=[("x", "<u4"), ("y", "<u4"), ("s", "<u8"), ("seed", "<u8")])
+    table["x"], table["y"] = xs, ys
+    table["s"], table["seed"] = sample_index, seed
+    return (abi.SampleIndex * n).from_buffer_copy(table.tobytes())
 
-    def batch(n):
-        samples = (abi.SampleIndex * n)()
-        for k in range(n):
-            samples[k].pixel_x, samples[k].pixel_y = int(rng.integers(width)), int(rng.integers(height))
-            samples[k].sample_index = int(rng.integers(spp))
-        from oracle.bindings import Oracle as _O
-        rays = _O().camera_rays(cam, samples)
-        inputs = (abi.PathInput * n)()
-        for k in range(n):
-            inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
+
+def path_inputs(rays, samples):
+    """PathInput records (primary ray, sample index) built in bulk."""
+    n = len(samples)
+    table = np.zeros(n, dtype=[("ray", "V48"), ("sample", "V24"), ("reserved", "<u8")])
+    table["ray"] = np.frombuffer(bytes(rays), dtype="V48")
+    table["sample"] = np.frombuffer(bytes(samples), dtype="V24")
+    return (abi.PathInput * n).from_buffer_copy(table.tobytes())
+
+
+def reference_camera_inputs(workload, samples, cones=False):
+    """Primary rays (and, with cones, primary ray cones) of the reference's own PinholeCamera for
+    the workload's camera (oracle/_ref): no bf200 library is loaded on this path."""
+    from oracle.bindings import Reference
+    _, _, (width, height, _) = scenes.build_workload(workload)
+    origin, normal, tangent, vfov = scenes.workload_camera(workload)
+    ref = Reference()
+    rays = ref.camera_rays(origin, normal, tangent, width, height, vfov, scenes.PATH_TIME, samples)
+    inputs = path_inputs(rays, samples)
+    if not cones:
         return inputs
+    return inputs, ref.camera_cones(origin, normal, tangent, width, height, vfov, scenes.PATH_TIME, samples)
 
-    probe = batch(threads)
-    t0 = time.perf_counter()
-    checker.trace(handle, probe, options, threads)
-    per_path = max(1e-6, (time.perf_counter() - t0) / len(probe))
-    n = int(max(threads, min(200000, target_seconds / per_path)))
-    inputs = batch(n)
-    t0 = time.perf_counter()
-    checker.trace(handle, inputs, options, threads)
-    elapsed = time.perf_counter() - t0
-    checker.destroy(handle)
-    sample = f"{n} random (pixel, sample) paths of {WORKLOAD} ({elapsed:.1f} s, {threads} threads)"
-    return n / elapsed, threads, kind, sample, n, elapsed
+
+# Workloads whose CPU baseline is the oracle restatement instead of the compiled reference: the
+# reference's only CPU accel here is its analytic one (Embree is absent), which tests every triangle
+# of every instance for every ray -- on the 985k-triangle, 40-instance scene more than five minutes
+# per path on one core -- so a bounded sample of it cannot finish in a bench step. The restatement
+# computes the same paths (pinned bit-exact against the reference by the CPU tests) and rejects
+# triangles with a conservative double prefilter first, about 1.4 s per path on one core.
+PORT_BASELINE_WORKLOADS = {"bvh_stress_1080p"}
+
+
+class CpuReference:
+    """The reference CPU path on all host threads over bounded random samples of a workload's paths:
+    oracle/_ref (trace_scene_mis with the analytic accel), or the oracle restatement for the
+    workloads above; primary rays of the reference's own PinholeCamera either way. No bf200 library
+    is loaded on this path."""
+
+    def __init__(self, workload):
+        from oracle.bindings import CheckerError, Oracle, Reference, reference_available
+        if not reference_available():
+            raise CheckerError("the CPU reference arm needs oracle/_ref/libbfref.so (oracle/Makefile, target ref)")
+        self.workload = workload
+        self.builder, self.options, (self.width, self.height, self.spp) = scenes.build_workload(workload)
+        self.kind = "port" if workload in PORT_BASELINE_WORKLOADS else "reference"
+        self.checker = Oracle() if self.kind == "port" else Reference()
+        self.threads = os.cpu_count() or 1
+        self.handle = self.checker.scene(self.builder)
+        self.rng = np.random.default_rng(5)
+        self.per_path = None
+
+    def batch(self, n):
+        pixels = np.stack([self.rng.integers(self.width, size=n), self.rng.integers(self.height, size=n)],
+                          axis=1).astype(np.uint64)
+        samples = frame_samples(self.width, self.height, 0, pixels=pixels)
+        sample_index = self.rng.integers(self.spp, size=n)
+        for k in range(n):
+            samples[k].sample_index = int(sample_index[k])
+        return reference_camera_inputs(self.workload, samples)
+
+    def run(self, n):
+        """Traces n random paths; returns the seconds taken."""
+        inputs = self.batch(n)
+        t0 = time.perf_counter()
+        self.checker.trace(self.handle, inputs, self.options, self.threads)
+        elapsed = time.perf_counter() - t0
+        if self.per_path is None:
+            self.per_path = max(1e-6, elapsed / n)
+        return elapsed
+
+    def sized(self, target_seconds):
+        """Paths for about target_seconds of work (at least one per thread)."""
+        if self.per_path is None:
+            self.run(self.threads)
+        return int(max(self.threads, min(200000, target_seconds / self.per_path)))
+
+    def close(self):
+        self.checker.destroy(self.handle)
+
+    def describe(self, n):
+        what = ("the oracle restatement (pinned bit-exact on the reference; triangles rejected by a conservative "
+                "double prefilter before the exact test)" if self.kind == "port" else
+                "oracle/_ref: the reference's trace_scene_mis with its analytic accel")
+        return (f"{n} random (pixel, sample) paths of {self.workload} per step, primary rays of the reference's "
+                f"PinholeCamera, traced by {what} on {self.threads} threads")
+
+
+def cpu_sample_rate(workload, target_seconds=15.0):
+    """One bounded sample of the reference CPU path: (paths/s, threads, kind, sample text, paths,
+    seconds)."""
+    ref = CpuReference(workload)
+    n = ref.sized(target_seconds)
+    elapsed = ref.run(n)
+    ref.close()
+    return n / elapsed, ref.threads, ref.kind, ref.describe(n), n, elapsed
 
 
 BATCH_WORKLOAD = "batch64"
@@ -577,25 +659,106 @@ def run_mesh_import(args):
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's own CPU implementation of the path, on the host cores of rank 0: each step
+    traces a bounded random sample of the workload's paths (about --reference-seconds of work; a
+    warm-up step traces one path per thread)."""
     if rank != 0:
         return
-    rates = []
-    for step in range(args.warmup + args.steps):
-        rate, threads, kind, sample, n, elapsed = cpu_sample_rate(target_seconds=args.reference_seconds)
-        if step >= args.warmup:
-            rates.append((rate, threads, kind, sample, elapsed))
-    value = statistics.median(r[0] for r in rates)
-    ms_per_step = statistics.median(r[4] for r in rates) * 1000.0
-    _, threads, kind, sample, _ = rates[-1]
+    ref = CpuReference(args.workload)
+    for _ in range(args.warmup):
+        ref.run(ref.threads)
+    n = ref.sized(args.reference_seconds)
+    seconds = [ref.run(n) for _ in range(args.steps)]
+    ref.close()
+    total = sum(seconds)
+    value = n * args.steps / total
+    width, height, spp, depth, mis, _ = scenes.WORKLOADS[args.workload]
+    sample = ref.describe(n)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "width": 256, "height": 256, "spp": 256, "max_depth": 16,
-                   "mis": "power", "sample_per_step": sample},
-        "cpu_baseline": {"value": value, "unit": "path samples/s", "cores": threads, "kind": kind,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "width": width, "height": height, "spp": spp, "max_depth": depth,
+                   "mis": mis, "sample_per_step": sample},
+        "cpu_baseline": {"value": value, "unit": "path samples/s", "cores": ref.threads, "kind": ref.kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "path samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_cuda_arm(args, rank, world):
+    """The reference's own CUDA backend on the workload: each step is one
+    trace_cuda_wavefront_transport call on a reused workspace over one sample per pixel of the frame
+    (2,073,600 paths at 1080p; the reference benchmark's call shape, Benchmarks/Renderer/
+    CudaWavefrontTransportBenchmark.cpp:163-393), inputs from the reference's own camera (rays and
+    cones) and results back in host memory. bf200_trace_paths_with_cones runs the same inputs the
+    same way (host inputs, host results) beside it, and the per-path results of the two are
+    compared. Host wall time around each call (each returns after its device work)."""
+    if rank != 0:
+        return
+    import torch
+    from oracle.bindings import ReferenceCuda
+    builder, options, (width, height, spp) = scenes.build_workload(args.workload)
+    ref = ReferenceCuda()
+    t0 = time.perf_counter()
+    handle = ref.scene(builder)
+    ref_setup_s = time.perf_counter() - t0
+    stats = ref.stats(handle)
+    ctx = runtime.Context(0, path_capacity=args.capacity)
+    t0 = time.perf_counter()
+    scene = ctx.create_scene(builder)
+    bf_setup_s = time.perf_counter() - t0
+
+    def inputs_for(step):
+        samples = frame_samples(width, height, step % spp, seed=0)
+        return reference_camera_inputs(args.workload, samples, cones=True)
+
+    ref_ms, bf_ms = [], []
+    agreement = None
+    for step in range(args.warmup + args.steps):
+        inputs, cones = inputs_for(step)
+        want, ref_report, ms = ref.trace(handle, inputs, options, cones=cones, results=step == args.warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        got, _, report = ctx.trace_paths_with_cones(scene, inputs, cones, options)
+        torch.cuda.synchronize()
+        bf = (time.perf_counter() - t0) * 1000.0
+        if step >= args.warmup:
+            ref_ms.append(ms)
+            bf_ms.append(bf)
+        if want is not None:
+            from helpers import arrays, relative_error
+            a, b = arrays(got), arrays(want)
+            ok = a["lane_status"] == 0
+            close = (relative_error(a["radiance"], b["radiance"]) <= 1e-5).all(axis=1) & ok
+            same = (a["radiance"].view(np.uint32) == b["radiance"].view(np.uint32)).all(axis=1) & ok
+            agreement = {"paths": len(inputs), "bit_exact": float(same.mean()), "within_1e-5": float(close.mean()),
+                         "same_termination": float(((a["termination"] == b["termination"]) & ok).mean()),
+                         "segments_bf200": [int(report.extension_segments), int(report.shadow_segments)],
+                         "segments_reference": [int(ref_report.extension_segments), int(ref_report.shadow_segments)]}
+    paths = width * height
+    value = paths * len(ref_ms) / (sum(ref_ms) / 1000.0)
+    bf_value = paths * len(bf_ms) / (sum(bf_ms) / 1000.0)
+    scene.close()
+    ctx.close()
+    ref.destroy(handle)
+    line = {
+        "impl": "reference-cuda", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(ref_ms) / len(ref_ms),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "width": width, "height": height, "paths_per_call": paths,
+                   "call": "trace_cuda_wavefront_transport, reused workspace, synchronous transfer, host inputs "
+                           "and results (one sample per pixel per call, sample index = step)",
+                   "mis": scenes.WORKLOADS[args.workload][4], "max_depth": scenes.WORKLOADS[args.workload][3]},
+        "reference_setup": {"seconds": ref_setup_s, **stats},
+        "bf200_same_inputs": {"value": bf_value, "ms_per_step": sum(bf_ms) / len(bf_ms),
+                              "call": "bf200_trace_paths_with_cones, host inputs and results",
+                              "scene_create_seconds": bf_setup_s},
+        "bf200_over_reference_cuda": bf_value / value,
+        "agreement": agreement,
+        "e2e": {"value": value, "unit": "path samples/s", "h2d_bytes_per_step": paths * 80 + paths * 8,
+                "d2h_bytes_per_step": paths * C.sizeof(abi.PathResult)},
     }
     print(json.dumps(line), flush=True)
 
@@ -605,9 +768,9 @@ def main():
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=5)
     parser.add_argument("--warmup", type=int, default=3)
-    parser.add_argument("--impl", default="bf200", choices=["bf200", "reference"])
+    parser.add_argument("--impl", default="bf200", choices=["bf200", "reference", "reference-cuda"])
     parser.add_argument("--capacity", type=int, default=1 << 21)
-    parser.add_argument("--reference-seconds", type=float, default=8.0)
+    parser.add_argument("--reference-seconds", type=float, default=4.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's)")
     parser.add_argument("--workload", default=WORKLOAD,
@@ -627,6 +790,9 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.impl == "reference-cuda":
+        run_reference_cuda_arm(args, rank, world)
         return
     if args.workload == IMPORT_WORKLOAD:
         if rank == 0:
@@ -768,7 +934,7 @@ def main():
     bytes_per_launch = STAGE_BYTES_PER_UNIT[dominant] * units / max(1, staged.iterations)
     achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
     units_per_launch = units / max(1, staged.iterations)
-    traffic_per_unit = MEASURED_TRAFFIC_PER_UNIT.get(dominant)
+    traffic_per_unit = MEASURED_TRAFFIC_PER_UNIT.get(args.workload, {}).get(dominant)
     traffic = traffic_per_unit * units_per_launch if traffic_per_unit is not None else None
     whole_bytes = (CAMERA_RAY_BYTES * paths_per_step * args.steps + EXTENSION_SEGMENT_BYTES * ext +
                    SHADOW_SEGMENT_BYTES * shadow + FILM_SAMPLE_BYTES * paths_per_step * args.steps)
@@ -792,14 +958,16 @@ def main():
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": STAGE_KERNELS[dominant], "achieved": achieved, "peak": peak,
                      "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "traffic_source": TRAFFIC_SOURCE,
+                     "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit, scaled to a launch"
+                     if traffic is not None else None,
                      "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind,
                      "whole_path_algorithmic_gbs": whole_bytes / (total_ms / 1000.0) / 1e9},
     }
     scene.close()
     ctx.close()
-    if rank == 0 and not args.no_cpu_baseline and args.workload == WORKLOAD:
-        rate, threads, kind, sample, _, _ = cpu_sample_rate()
+    if rank == 0 and not args.no_cpu_baseline and args.workload in scenes.WORKLOADS:
+        rate, threads, kind, sample, _, _ = cpu_sample_rate(args.workload, target_seconds=args.reference_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": "path samples/s", "cores": threads, "kind": kind,
                                 "sample": sample}
     if distributed:

@@ -16,7 +16,8 @@ CSRC = os.path.join(os.path.dirname(PACKAGE_DIR), "csrc")
 REPO = os.path.dirname(os.path.dirname(PACKAGE_DIR))
 INCLUDE = os.path.join(REPO, "include")
 LIBRARY = os.path.join(PACKAGE_DIR, "libbf200.so")
-SOURCES = ["bf200_kernels.cu", "bf200_compact.cu", "bf200_sobol.cu", "bf200_host.cu", "bf200_import.cpp", "bf200_soa.cpp", "bf200_light_tree.cpp", "bf200_light_tree.cu"]
+SOURCES = ["bf200_kernels.cu", "bf200_shade_plain.cu", "bf200_shade_cone.cu", "bf200_shade_tree.cu",
+           "bf200_shade_cone_tree.cu", "bf200_shade_adjoint.cu", "bf200_compact.cu", "bf200_sobol.cu", "bf200_host.cu", "bf200_import.cpp", "bf200_soa.cpp", "bf200_light_tree.cpp", "bf200_light_tree.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-std=c++17", "-O3", "-lineinfo", "-fmad=false",
@@ -40,13 +41,34 @@ def _stale(target, inputs):
 
 
 def build_library(force=False, verbose=False):
+    """Compiles every translation unit to an object under _build/ (in parallel, one nvcc per
+    source; the units share no device symbols, so this is the same program as one nvcc call over
+    all of them) and links the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
+
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "bf200.h")]
     if not force and not _stale(LIBRARY, deps):
         return LIBRARY
-    cmd = [nvcc()] + NVCC_FLAGS + ["-I" + INCLUDE, "-I" + CSRC, "-o", LIBRARY]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+    objdir = os.path.join(REPO, "_build", "bf200")
+    os.makedirs(objdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    headers = [p for p in deps if not p.endswith((".cu", ".cpp"))]
+
+    def compile_one(source):
+        src = os.path.join(CSRC, source)
+        obj = os.path.join(objdir, source + ".o")
+        if force or _stale(obj, [src] + headers):
+            cmd = [nvcc()] + compile_flags + ["-I" + INCLUDE, "-I" + CSRC, "-c", "-o", obj, src]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as pool:
+        objects = list(pool.map(compile_one, SOURCES))
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIBRARY] + objects
     if verbose:
-        print(" ".join(cmd))
+        print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     return LIBRARY
 

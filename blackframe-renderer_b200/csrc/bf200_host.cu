@@ -82,6 +82,12 @@ struct bf200_scene {
     uint32_t instance_triangles = 0;
     uint32_t* normal_failures = nullptr;     // device counter of k_world_normals
     size_t light_triangles = 0;
+    // the spatial light tree (bf200_scene_set_light_tree): device node array and light-to-node map,
+    // owned here (not in `allocations`) so a new tree reuses them and a cleared tree frees them
+    void* tree_nodes = nullptr;
+    void* tree_map = nullptr;
+    size_t tree_node_bytes = 0;
+    size_t tree_map_bytes = 0;
 };
 
 namespace {
@@ -1905,17 +1911,64 @@ BF200_EXPORT blackframe_status bf200_light_power_cdf(const float* spectral_power
     }
 }
 
-// The scene's light-selection CDF: power-weighted from `spectral_powers` (4 per light), or uniform
-// again (LightSampler::create_uniform) when it is null.
+}  // extern "C"
+
+namespace {
+
+// Frees the scene's light-tree buffers (after the stream that may still read them) and returns the
+// scene to selection by its CDF.
+void release_light_tree(bf200_scene* s) {
+    s->view.tree = nullptr;
+    s->view.tree_light_to_node = nullptr;
+    if (s->tree_nodes == nullptr && s->tree_map == nullptr) {
+        return;
+    }
+    cudaSetDevice(s->context->device);
+    cudaStreamSynchronize(s->context->stream);
+    cudaFree(s->tree_nodes);
+    cudaFree(s->tree_map);
+    s->tree_nodes = s->tree_map = nullptr;
+    s->tree_node_bytes = s->tree_map_bytes = 0;
+}
+
+// Device buffer of at least `bytes` in `slot` (capacity `held`): reused when it fits, else the old
+// one is freed after the stream and a new one allocated.
+cudaError_t fit_buffer(bf200_context* c, void*& slot, size_t& held, size_t bytes) {
+    if (slot != nullptr && held >= bytes) {
+        return cudaSuccess;
+    }
+    if (slot != nullptr) {
+        if (const cudaError_t e = cudaStreamSynchronize(c->stream); e != cudaSuccess) {
+            return e;
+        }
+        cudaFree(slot);
+        slot = nullptr;
+        held = 0;
+    }
+    const cudaError_t e = cudaMalloc(&slot, bytes);
+    if (e == cudaSuccess) {
+        held = bytes;
+    } else {
+        slot = nullptr;
+    }
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Selection by the spatial light tree of `lights` (one input per scene light), or back to the
+// scene's CDF when `lights` is null. A new tree reuses the previous tree's device buffers when it
+// fits in them; a refused call leaves the scene's selection as it was.
 BF200_EXPORT blackframe_status bf200_scene_set_light_tree(bf200_scene* s, const bf200_light_tree_input_v1* lights,
                                                           uint32_t light_count) noexcept {
     if (s == nullptr) {
         return BLACKFRAME_STATUS_INVALID_ARGUMENT;
     }
     bf200_context* c = s->context;
-    if (lights == nullptr) {  // back to selection by the scene's CDF
-        s->view.tree = nullptr;
-        s->view.tree_light_to_node = nullptr;
+    if (lights == nullptr) {
+        release_light_tree(s);
         return BLACKFRAME_STATUS_SUCCESS;
     }
     if (light_count != s->light_count) {
@@ -1927,31 +1980,32 @@ BF200_EXPORT blackframe_status bf200_scene_set_light_tree(bf200_scene* s, const 
         if (const auto st = bf200::build_light_tree(lights, light_count, tree, error); st != BLACKFRAME_STATUS_SUCCESS) {
             return fail(c, st, error);
         }
-        cudaSetDevice(c->device);
-        void* nodes = nullptr;
-        void* map = nullptr;
+        if (const cudaError_t e = cudaSetDevice(c->device); e != cudaSuccess) {
+            return cuda_fail(c, e, "select the scene's device");
+        }
         const size_t node_bytes = tree.nodes.size() * sizeof(bf200::LightTreeNode);
         const size_t map_bytes = tree.light_to_node.size() * sizeof(uint32_t);
-        cudaError_t e = cudaMalloc(&nodes, node_bytes);
+        // the stream may still read the old tree: it is replaced only after the stream drained
+        // (fit_buffer synchronises before it frees; an in-place rewrite is ordered on the stream)
+        cudaError_t e = fit_buffer(c, s->tree_nodes, s->tree_node_bytes, node_bytes);
         if (e == cudaSuccess) {
-            s->allocations.push_back(nodes);
-            e = cudaMalloc(&map, map_bytes);
+            e = fit_buffer(c, s->tree_map, s->tree_map_bytes, map_bytes);
         }
         if (e == cudaSuccess) {
-            s->allocations.push_back(map);
-            e = cudaMemcpyAsync(nodes, tree.nodes.data(), node_bytes, cudaMemcpyHostToDevice, c->stream);
+            e = cudaMemcpyAsync(s->tree_nodes, tree.nodes.data(), node_bytes, cudaMemcpyHostToDevice, c->stream);
         }
         if (e == cudaSuccess) {
-            e = cudaMemcpyAsync(map, tree.light_to_node.data(), map_bytes, cudaMemcpyHostToDevice, c->stream);
+            e = cudaMemcpyAsync(s->tree_map, tree.light_to_node.data(), map_bytes, cudaMemcpyHostToDevice, c->stream);
         }
         if (e == cudaSuccess) {
             e = cudaStreamSynchronize(c->stream);
         }
         if (e != cudaSuccess) {
+            release_light_tree(s);  // the buffers' contents are unknown: back to the CDF
             return cuda_fail(c, e, "light-tree upload");
         }
-        s->view.tree = static_cast<const bf200::LightTreeNode*>(nodes);
-        s->view.tree_light_to_node = static_cast<const uint32_t*>(map);
+        s->view.tree = static_cast<const bf200::LightTreeNode*>(s->tree_nodes);
+        s->view.tree_light_to_node = static_cast<const uint32_t*>(s->tree_map);
         s->view.tree_node_count = static_cast<uint32_t>(tree.nodes.size());
         s->view.tree_root = tree.root;
         s->view.tree_log_extent = tree.root_log_extent;
@@ -1962,6 +2016,9 @@ BF200_EXPORT blackframe_status bf200_scene_set_light_tree(bf200_scene* s, const 
     return BLACKFRAME_STATUS_SUCCESS;
 }
 
+// The scene's light-selection CDF: power-weighted from `spectral_powers` (4 per light), or uniform
+// again (LightSampler::create_uniform) when it is null. Selection by a light tree, if one was set,
+// ends once the new CDF is in place; a refused call changes nothing.
 BF200_EXPORT blackframe_status bf200_scene_set_light_powers(bf200_scene* s, const float* spectral_powers,
                                                             uint32_t light_count) noexcept {
     if (s == nullptr) {
@@ -1971,8 +2028,6 @@ BF200_EXPORT blackframe_status bf200_scene_set_light_powers(bf200_scene* s, cons
     if (light_count != s->light_count) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "one spectral power per scene light is required");
     }
-    s->view.tree = nullptr;  // selection by the CDF this call installs
-    s->view.tree_light_to_node = nullptr;
     try {
         std::vector<float> cdf;
         if (spectral_powers == nullptr) {
@@ -1997,6 +2052,7 @@ BF200_EXPORT blackframe_status bf200_scene_set_light_powers(bf200_scene* s, cons
         if (e != cudaSuccess) {
             return cuda_fail(c, e, "light selection upload");
         }
+        release_light_tree(s);  // selection by the CDF this call installed
     } catch (const std::bad_alloc&) {
         return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "light selection exhausted host memory");
     }
@@ -2012,6 +2068,8 @@ BF200_EXPORT blackframe_status bf200_scene_destroy(bf200_scene* s) noexcept {
     for (void* p : s->allocations) {
         cudaFree(p);
     }
+    cudaFree(s->tree_nodes);
+    cudaFree(s->tree_map);
     delete s;
     return BLACKFRAME_STATUS_SUCCESS;
 }
@@ -2335,7 +2393,9 @@ BF200_EXPORT blackframe_status bf200_trace_paths_device_noalloc(bf200_context* c
     if (path_count == 0) {
         return BLACKFRAME_STATUS_SUCCESS;
     }
-    cudaSetDevice(c->device);
+    if (const cudaError_t e = cudaSetDevice(c->device); e != cudaSuccess) {
+        return cuda_fail(c, e, "select the context's device");
+    }
     void* base = nullptr;
     if (const auto st = noalloc_scratch(c, &base); st != BLACKFRAME_STATUS_SUCCESS) {
         return st;

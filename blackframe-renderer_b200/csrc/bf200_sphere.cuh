@@ -127,7 +127,7 @@ __device__ bool expansion_squared_norm(F3 v, FloatExpansion<N>& out) {
 }
 
 // exact_quadratic_constant (Sphere.hpp:147-181): false when not representable
-__device__ bool sphere_constant(F3 rel, float radius, float& value) {
+static __device__ bool sphere_constant(F3 rel, float radius, float& value) {
     FloatExpansion<8> origin_squared;
     FloatExpansion<2> radius_squared;
     radius_squared.n = 0;
@@ -146,7 +146,7 @@ __device__ bool sphere_constant(F3 rel, float radius, float& value) {
 }
 
 // exact_discriminant (Sphere.hpp:183-243): false when not representable; sign and value otherwise
-__device__ bool sphere_discriminant(F3 rel, F3 d, float radius, int& sign, float& value) {
+static __device__ bool sphere_discriminant(F3 rel, F3 d, float radius, int& sign, float& value) {
     FloatExpansion<6> direction_squared;
     FloatExpansion<2> radius_squared;
     radius_squared.n = 0;
@@ -309,7 +309,7 @@ struct SphereHit {
 // outward normal are formed too, as the reference does before it reports a hit. Out of line, with
 // every operand and the result by value: the expansions live in this call's frame, and no state of
 // the calling walk needs an address (which would move it out of registers).
-__device__ __noinline__ SphereHit sphere_intersect(float4 centre4, float radius, F3 o, F3 d, float t_min,
+static __device__ __noinline__ SphereHit sphere_intersect(float4 centre4, float radius, F3 o, F3 d, float t_min,
                                                    float t_max) {
     SphereHit out{kSphereMiss, 0.0F, F3{0.0F, 0.0F, 0.0F}};
     const F3 centre{centre4.x, centre4.y, centre4.z};

@@ -539,7 +539,10 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_trace_paths_device(
  * The device address of the scratch array is looked up once per device with
  * cudaGetSymbolAddress, at the first call on that device. That first call can also make the CUDA
  * driver load the library's device code, so make it during setup, before any stream capture
- * begins. All calls on one device share the one scratch array: calls that overlap in time, from
+ * begins. With BF200_SAMPLER_OWEN_SOBOL, the first call on a device (of this or any other entry
+ * point) also fills the library's static Sobol direction table with one blocking
+ * cudaMemcpyToSymbol (no allocation, but a synchronous host-to-device copy): make one such call
+ * during setup as well if later calls must not block. All calls on one device share the one scratch array: calls that overlap in time, from
  * any context or thread, race and corrupt each other's results, so the caller must serialise
  * them. instrumentation is ignored (no events); the report's timing fields are zero. */
 #define BF200_NOALLOC_SCRATCH_BYTES (16u << 20)

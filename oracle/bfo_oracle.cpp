@@ -42,6 +42,21 @@ constexpr float kPi = 3.14159265358979323846F;      // std::numbers::pi_v<float>
 
 using Spectrum = std::array<float, 4>;
 
+// Rounding of the sine and cosine of sampled angles. 0: the C library's float functions, which the
+// reference calls (std::sin / std::cos of a float); 1: the float nearest to the double-precision
+// value, which is how the device computes them. The two differ by an ulp on a small share of
+// angles, which can send a path in a direction one ulp apart. Set before a call, never during one.
+std::atomic<int> g_device_trig{0};
+
+float sin_f(float a) {
+    return g_device_trig.load(std::memory_order_relaxed) != 0 ? static_cast<float>(std::sin(static_cast<double>(a)))
+                                                              : std::sin(a);
+}
+float cos_f(float a) {
+    return g_device_trig.load(std::memory_order_relaxed) != 0 ? static_cast<float>(std::cos(static_cast<double>(a)))
+                                                              : std::cos(a);
+}
+
 // Failure of one path: the reference returns std::unexpected for the whole path.
 struct Failure {
     const char* message;
@@ -799,8 +814,8 @@ Frame frame_from_normal(V3 normal) {
 // LocalFrame.hpp:116-135 (rotated_about_normal).
 Frame rotated_about_normal(const Frame& f, float angle) {
     const float reduced = std::remainder(angle, 2.0F * kPi);
-    const float c = std::cos(reduced);
-    const float s = std::sin(reduced);
+    const float c = cos_f(reduced);
+    const float s = sin_f(reduced);
     const V3 rotated = f.t * c + f.b * s;
     return frame_from_unit_normal_and_tangent(f.n, rotated);
 }
@@ -1249,8 +1264,8 @@ V3 map_cosine_hemisphere(float u, float v) {
             r = oy;
             phi = 2.0F * quarter_pi - quarter_pi * (ox / oy);
         }
-        px = r * std::cos(phi);
-        py = r * std::sin(phi);
+        px = r * cos_f(phi);
+        py = r * sin_f(phi);
         radius = std::abs(r);
     }
     const float z = std::sqrt((1.0F - radius) * (1.0F + radius));
@@ -1425,8 +1440,8 @@ bool ggx_sample_vndf(const Ggx& g, V3 wo, float u, float v, V3& m_out, float& pd
     const V3 bitangent = cross(hv, tangent);
     const float disk_radius = std::sqrt(u);
     const float azimuth = 2.0F * kPi * v;
-    const float disk_x = disk_radius * std::cos(azimuth);
-    const float initial_disk_y = disk_radius * std::sin(azimuth);
+    const float disk_x = disk_radius * cos_f(azimuth);
+    const float initial_disk_y = disk_radius * sin_f(azimuth);
     const float limit_sq = (1.0F - disk_x) * (1.0F + disk_x);
     const float checked_limit_sq = nonnegative_roundoff(limit_sq, 1.0F + std::abs(disk_x));
     const float disk_y_limit = std::sqrt(checked_limit_sq);
@@ -3007,6 +3022,9 @@ using namespace bfo;
 extern "C" {
 
 __attribute__((visibility("default"))) const char* bfo_last_error() { return g_error.c_str(); }
+
+// 1: sampled-angle sines and cosines rounded as the device rounds them; 0: as the reference does.
+__attribute__((visibility("default"))) void bfo_set_device_trig(int enabled) { g_device_trig.store(enabled != 0); }
 
 __attribute__((visibility("default"))) int bfo_scene_create(const bf200_scene_desc_v1* d, void** out) {
     try {

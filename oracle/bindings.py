@@ -104,7 +104,11 @@ class _Checker:
         if f(handle, C.cast(lights, C.c_void_p), len(lights)) != 0:
             raise CheckerError(self.last_error())
 
+    def _before_trace(self):
+        pass
+
     def trace(self, handle, inputs, options, threads=None):
+        self._before_trace()
         n = len(inputs)
         results = (abi.PathResult * n)()
         threads = threads or os.cpu_count() or 1
@@ -115,10 +119,16 @@ class _Checker:
 
 
 class Oracle(_Checker):
+    """The restatement. device_trig=True rounds the sine and cosine of sampled angles as the device
+    does (the float nearest to the double value) instead of as the C library's float functions,
+    which the reference calls: the checker of the device path is then exact on every path whose
+    other arithmetic is."""
     prefix = "bfo"
 
-    def __init__(self):
+    def __init__(self, device_trig=False):
         super().__init__(ORACLE_LIB)
+        self.device_trig = bool(device_trig)
+        self.lib.bfo_set_device_trig.argtypes = [C.c_int]
         f = self.lib.bfo_film_accumulate
         f.argtypes = [C.c_void_p, C.POINTER(abi.SampleIndex), C.c_uint64, C.POINTER(abi.Sensor), C.c_uint32,
                       C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
@@ -133,6 +143,9 @@ class Oracle(_Checker):
         self.lib.bfo_sobol_bits.restype = C.c_uint64
         self.lib.bfo_owen_sobol_bits.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]
         self.lib.bfo_owen_sobol_bits.restype = C.c_uint64
+
+    def _before_trace(self):
+        self.lib.bfo_set_device_trig(1 if self.device_trig else 0)
 
     def cone_advance(self, cones, directions, parameters):
         """advance_ray_cone_to_hit per case: the advanced widths (NaN where it fails) and the
@@ -153,6 +166,7 @@ class Oracle(_Checker):
         """trace() carrying ray cones and, optionally, depth-zero initial states (an array of
         abi.PathState): (results, terminal cones float32 [n, 2], failures)."""
         import numpy as np
+        self._before_trace()
         n = len(inputs)
         cones = np.ascontiguousarray(cones, np.float32).reshape(n, 2)
         results = (abi.PathResult * n)()
@@ -397,3 +411,74 @@ class Reference(_Checker):
 
 def reference_available():
     return os.path.exists(REFERENCE_LIB)
+
+
+REFERENCE_CUDA_LIB = os.path.join(ORACLE_DIR, "_ref", "libbfrefcuda.so")
+
+
+def reference_cuda_available():
+    return os.path.exists(REFERENCE_CUDA_LIB)
+
+
+class ReferenceCuda:
+    """oracle/_ref/libbfrefcuda.so: the reference's own CUDA backend (CudaSceneSoA::upload,
+    CudaSceneBvh::build, trace_cuda_closest_hits, trace_cuda_wavefront_transport with a reused
+    workspace), compiled unchanged for sm_100a by oracle/Makefile. Needs a GPU."""
+
+    def __init__(self):
+        if not reference_cuda_available():
+            raise CheckerError(f"{REFERENCE_CUDA_LIB} is not built")
+        self.lib = C.CDLL(REFERENCE_CUDA_LIB)
+        self.lib.bfrc_last_error.restype = C.c_char_p
+        self.lib.bfrc_scene_create.argtypes = [C.POINTER(abi.SceneDesc), C.POINTER(C.c_void_p)]
+        self.lib.bfrc_scene_create.restype = C.c_int
+        self.lib.bfrc_scene_destroy.argtypes = [C.c_void_p]
+        self.lib.bfrc_scene_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                              C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        self.lib.bfrc_closest_hits.argtypes = [C.c_void_p, C.POINTER(abi.Ray), C.c_uint64, C.POINTER(abi.Hit)]
+        self.lib.bfrc_closest_hits.restype = C.c_int
+        self.lib.bfrc_trace.argtypes = [C.c_void_p, C.POINTER(abi.PathInput), C.c_void_p, C.c_uint64,
+                                        C.POINTER(abi.TransportOptions), C.c_void_p, C.POINTER(abi.Report),
+                                        C.POINTER(C.c_double)]
+        self.lib.bfrc_trace.restype = C.c_int
+
+    def last_error(self):
+        return self.lib.bfrc_last_error().decode()
+
+    def scene(self, builder, desc=None):
+        desc = desc if desc is not None else builder.desc()
+        handle = C.c_void_p()
+        rc = self.lib.bfrc_scene_create(C.byref(desc), C.byref(handle))
+        if rc != 0:
+            raise CheckerError(f"reference CUDA scene creation failed ({rc}): {self.last_error()}")
+        return handle
+
+    def destroy(self, handle):
+        self.lib.bfrc_scene_destroy(handle)
+
+    def stats(self, handle):
+        up, build = C.c_double(), C.c_double()
+        sb, bb = C.c_uint64(), C.c_uint64()
+        self.lib.bfrc_scene_stats(handle, C.byref(up), C.byref(build), C.byref(sb), C.byref(bb))
+        return {"upload_ms": up.value, "bvh_build_ms": build.value, "scene_bytes": sb.value, "bvh_bytes": bb.value}
+
+    def closest_hits(self, handle, rays):
+        hits = (abi.Hit * len(rays))()
+        if self.lib.bfrc_closest_hits(handle, rays, len(rays), hits) != 0:
+            raise CheckerError(self.last_error())
+        return hits
+
+    def trace(self, handle, inputs, options, cones=None, results=True):
+        """One trace_cuda_wavefront_transport call: (results or None, report, host milliseconds)."""
+        import numpy as np
+        n = len(inputs)
+        out = (abi.PathResult * n)() if results else None
+        report = abi.Report()
+        ms = C.c_double()
+        c = np.ascontiguousarray(cones, np.float32).reshape(n, 2) if cones is not None else None
+        rc = self.lib.bfrc_trace(handle, inputs, c.ctypes.data_as(C.c_void_p) if c is not None else None, n,
+                                 C.byref(options), C.cast(out, C.c_void_p) if out is not None else None,
+                                 C.byref(report), C.byref(ms))
+        if rc != 0:
+            raise CheckerError(self.last_error())
+        return out, report, ms.value

@@ -15,7 +15,7 @@ NAME = "bvh_stress_1080p"
 @pytest.fixture(scope="module")
 def setup():
     builder, options, (width, height, spp) = scenes.build_workload(NAME)
-    oracle = Oracle()
+    oracle = Oracle(device_trig=True)
     handle = oracle.scene(builder)
     with runtime.Context(0, path_capacity=1 << 16) as ctx:
         scene = ctx.create_scene(builder)

@@ -43,7 +43,7 @@ def workload(golden):
         samples[k].pixel_x, samples[k].pixel_y = int(table[k, 0]), int(table[k, 1])
         samples[k].sample_index, samples[k].seed = int(table[k, 2]), int(table[k, 3])
     cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)
-    rays = Oracle().camera_rays(cam, samples)
+    rays = Oracle(device_trig=True).camera_rays(cam, samples)
     inputs = (abi.PathInput * n)()
     for k in range(n):
         inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
@@ -63,7 +63,7 @@ def same_paths(results, expected, got, want):
 
 def test_terminal_cones_match_the_oracle(ctx, workload):
     builder, options, inputs, cones = workload
-    oracle = Oracle()
+    oracle = Oracle(device_trig=True)
     handle = oracle.scene(builder)
     expected, expected_cones, failures = oracle.trace_cones(handle, inputs, cones, options)
     oracle.destroy(handle)
@@ -180,7 +180,7 @@ def test_initial_states_match_the_oracle(ctx, golden):
     inputs = m.inputs_for(samples, width, height)
     states = m.states_from(g["beta_in"], g["radiance_in"], g["eta_in"])
     cones = np.tile(np.array([0.0, 0.0025], np.float32), (len(table), 1))
-    oracle = Oracle()
+    oracle = Oracle(device_trig=True)
     handle = oracle.scene(builder)
     expected, expected_cones, _ = oracle.trace_cones(handle, inputs, cones, options, states=states)
     oracle.destroy(handle)

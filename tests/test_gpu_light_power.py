@@ -61,7 +61,7 @@ def test_power_weighted_paths_match_the_oracle_and_the_reference():
     powers = light_powers(builder)
     assert len(powers) == 3 and not np.allclose(powers[0], powers[1])
     options = abi.default_options(mis="power", max_depth=8)
-    oracle = Oracle()
+    oracle = Oracle(device_trig=True)
     inputs = path_inputs(oracle, 2048, 21)
     handle = oracle.scene(builder)
     oracle.set_light_powers(handle, powers)

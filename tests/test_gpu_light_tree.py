@@ -60,7 +60,7 @@ def test_tree_selected_paths_match_the_oracle():
     spec.loader.exec_module(maker)
     builder = three_light_box()
     lights = maker.tree_box_inputs(builder)
-    oracle = Oracle()
+    oracle = Oracle(device_trig=True)
     inputs = path_inputs(oracle, 4096, 31)
     options = abi.default_options(mis="power", max_depth=8)
     h = oracle.scene(builder)

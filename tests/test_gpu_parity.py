@@ -28,7 +28,7 @@ def ctx():
 
 @pytest.fixture(scope="module")
 def oracle():
-    return Oracle()
+    return Oracle(device_trig=True)
 
 
 @pytest.mark.parametrize("name", WORKLOADS)

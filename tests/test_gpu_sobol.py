@@ -35,7 +35,7 @@ def _inputs(oracle, cam, width, height, spp, n, seed):
 
 @pytest.mark.parametrize("name", ["cornell_plain_64", "cornell_spheres_256"])
 def test_owen_sobol_paths_match_oracle(ctx, name):
-    oracle = Oracle()
+    oracle = Oracle(device_trig=True)
     builder, options, (width, height, spp) = scenes.build_workload(name)
     options.sampler = OWEN
     cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)
@@ -52,7 +52,7 @@ def test_owen_sobol_paths_match_oracle(ctx, name):
 
 
 def test_owen_sobol_plain_frame_film_matches_oracle(ctx):
-    oracle = Oracle()
+    oracle = Oracle(device_trig=True)
     builder, options, (width, height, spp) = scenes.build_workload("cornell_plain_64")
     options.sampler = OWEN
     cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)

@@ -105,7 +105,7 @@ def test_reference_sphere_cases_on_the_device(ctx):
 
 def test_analytic_sphere_paths_match_the_oracle(ctx):
     builder, options, (width, height, spp) = scenes.build_workload("cornell_analytic_256")
-    oracle = Oracle()
+    oracle = Oracle(device_trig=True)
     rng = np.random.default_rng(77)
     n = 2048
     cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)

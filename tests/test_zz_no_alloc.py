@@ -28,7 +28,7 @@ def _inputs(name, n, seed):
     for k in range(n):
         samples[k].pixel_x, samples[k].pixel_y = int(rng.integers(width)), int(rng.integers(height))
         samples[k].sample_index, samples[k].seed = int(rng.integers(spp)), 0
-    rays = Oracle().camera_rays(cam, samples)
+    rays = Oracle(device_trig=True).camera_rays(cam, samples)
     inputs = (abi.PathInput * n)()
     for k in range(n):
         inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
