@@ -13,8 +13,11 @@ BLACKFRAME_STATUS = {
 }
 
 CLOSURE_LAMBERTIAN = 1
+CLOSURE_ROUGH_DIFFUSE = 2
 CLOSURE_ROUGH_CONDUCTOR = 3
 CLOSURE_ROUGH_DIELECTRIC = 4
+CLOSURE_SPECULAR_REFLECTION = 5
+CLOSURE_SPECULAR_TRANSMISSION = 6
 
 LOBE_DIFFUSE, LOBE_GLOSSY, LOBE_SPECULAR = 0x01, 0x02, 0x04
 LOBE_REFLECTION, LOBE_TRANSMISSION, LOBE_VOLUME = 0x08, 0x10, 0x20
@@ -90,6 +93,14 @@ class Instance(C.Structure):
                 ("object_to_world", f32 * 16), ("world_to_object", f32 * 16)]
 
 
+class PunctualLight(C.Structure):
+    _fields_ = [("kind", u32), ("reserved", u32), ("position", f32 * 3), ("position_error", f32 * 3),
+                ("direction", f32 * 3), ("inner_half_angle", f32), ("outer_half_angle", f32), ("spectrum", f32 * 4)]
+
+
+PUNCTUAL_POINT, PUNCTUAL_DIRECTIONAL, PUNCTUAL_SPOT = 1, 2, 3
+
+
 class SceneDesc(C.Structure):
     _fields_ = [("struct_size", u32), ("geometry_count", u32), ("vertex_count", u32),
                 ("triangle_count", u32), ("material_count", u32), ("closure_count", u32),
@@ -99,7 +110,8 @@ class SceneDesc(C.Structure):
                 ("triangles", C.POINTER(u32)), ("materials", C.POINTER(Material)),
                 ("closures", C.POINTER(Closure)), ("instances", C.POINTER(Instance)),
                 ("wavelength_nanometers", f32 * 4), ("wavelength_pdf", f32 * 4),
-                ("environment_radiance", f32 * 4), ("reserved", u32 * 4)]
+                ("environment_radiance", f32 * 4), ("reserved", u32 * 4),
+                ("punctual_lights", C.POINTER(PunctualLight))]
 
 
 class Ray(C.Structure):

@@ -263,6 +263,22 @@ def rough_dielectric(coefficient, exterior_eta, interior_eta, alpha_x, alpha_y):
              [F32(v) for v in coefficient], [F32(v) for v in params])]
 
 
+def rough_diffuse(reflectance, roughness):
+    """Energy-preserving Oren-Nayar reflection (ClosureSet::append_rough_diffuse_reflection)."""
+    return [(abi.CLOSURE_ROUGH_DIFFUSE, abi.LOBE_DIFFUSE | abi.LOBE_REFLECTION, [F32(v) for v in reflectance],
+             [F32(roughness)] + [0.0] * 9)]
+
+
+def specular_reflection(reflectance):
+    return [(abi.CLOSURE_SPECULAR_REFLECTION, abi.LOBE_SPECULAR | abi.LOBE_REFLECTION,
+             [F32(v) for v in reflectance], [0.0] * 10)]
+
+
+def specular_transmission(transmittance, exterior_eta, interior_eta):
+    return [(abi.CLOSURE_SPECULAR_TRANSMISSION, abi.LOBE_SPECULAR | abi.LOBE_TRANSMISSION,
+             [F32(v) for v in transmittance], [F32(exterior_eta), F32(interior_eta)] + [0.0] * 8)]
+
+
 class SceneBuilder:
     """Accumulates meshes, materials and root instances; `desc()` returns a SceneDesc whose
     arrays stay alive as long as the builder does."""
@@ -271,14 +287,44 @@ class SceneBuilder:
         self.nanometers, self.pdfs = sample_uniform_visible_wavelengths(wavelength_sample)
         self.environment = [F32(v) for v in environment]
         self.meshes, self.materials, self.instances = [], [], []
+        self.punctual = []  # abi.PunctualLight records, registry order
+        self.probabilities = {}  # material index -> component probabilities (default uniform)
 
     def add_mesh(self, mesh):
         self.meshes.append(mesh)
         return len(self.meshes) - 1
 
-    def add_material(self, closures, emission=(0.0, 0.0, 0.0, 0.0), frame_mode=0):
+    def add_material(self, closures, emission=(0.0, 0.0, 0.0, 0.0), frame_mode=0, probabilities=None):
+        """closures: up to 8 (kind, lobes, weight[4], parameters[10]) records; probabilities: their
+        component probabilities (SceneClosureMixture), uniform when not given."""
         self.materials.append((closures, [F32(v) for v in emission], frame_mode))
+        if probabilities is not None:
+            self.probabilities[len(self.materials) - 1] = [F32(v) for v in probabilities]
         return len(self.materials) - 1
+
+    def add_point_light(self, position, intensity, error=(0.0, 0.0, 0.0)):
+        return self._punctual(abi.PUNCTUAL_POINT, position, error, (0.0, 0.0, 0.0), 0.0, 0.0, intensity)
+
+    def add_directional_light(self, propagation_direction, irradiance):
+        return self._punctual(abi.PUNCTUAL_DIRECTIONAL, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), propagation_direction, 0.0,
+                              0.0, irradiance)
+
+    def add_spot_light(self, position, emission_direction, inner_half_angle, outer_half_angle, intensity,
+                       error=(0.0, 0.0, 0.0)):
+        return self._punctual(abi.PUNCTUAL_SPOT, position, error, emission_direction, inner_half_angle,
+                              outer_half_angle, intensity)
+
+    def _punctual(self, kind, position, error, direction, inner, outer, spectrum):
+        light = abi.PunctualLight()
+        light.kind = kind
+        for a in range(3):
+            light.position[a], light.position_error[a] = F32(position[a]), F32(error[a])
+            light.direction[a] = F32(direction[a])
+        light.inner_half_angle, light.outer_half_angle = F32(inner), F32(outer)
+        for lane in range(4):
+            light.spectrum[lane] = F32(spectrum[lane])
+        self.punctual.append(light)
+        return len(self.punctual) - 1
 
     def add_instance(self, mesh_index, material_index, object_to_world=None, mask=0xFFFFFFFF):
         matrix = identity() if object_to_world is None else np.asarray(object_to_world, F32)
@@ -320,7 +366,7 @@ class SceneBuilder:
             m.frame_mode = frame_mode
             m.tangent_rotation_radians = 0.0
             for c in range(len(closures)):
-                m.component_probabilities[c] = 1.0 / len(closures)
+                m.component_probabilities[c] = self.probabilities.get(index, [1.0 / len(closures)] * len(closures))[c]
             for lane in range(4):
                 m.emitted_radiance[lane] = emission[lane]
             closure_records.extend(closures)
@@ -364,7 +410,10 @@ class SceneBuilder:
             desc.wavelength_nanometers[lane] = self.nanometers[lane]
             desc.wavelength_pdf[lane] = self.pdfs[lane]
             desc.environment_radiance[lane] = self.environment[lane]
-        self._keep = (geometries, materials, closures, instances)
+        punctual = (abi.PunctualLight * max(1, len(self.punctual)))(*self.punctual)
+        desc.punctual_light_count = len(self.punctual)
+        desc.punctual_lights = punctual
+        self._keep = (geometries, materials, closures, instances, punctual)
         return desc
 
 
@@ -418,6 +467,54 @@ def cornell_box(builder, with_spheres, analytic_spheres=False):
         builder.add_instance(sphere, conductor, uniform_scale_translate(0.25, (0.4, -0.15, 1.25)))
         builder.add_instance(sphere, dielectric,
                              uniform_scale_translate(0.25, (-0.3, -0.75, 1.55)))
+    return builder
+
+
+def cornell_layered(builder):
+    """The Cornell box with every closure kind, closure mixtures and punctual lights: an
+    energy-preserving Oren-Nayar back wall, a layered floor (Lambert under a GGX conductor coat,
+    component probabilities 0.6 / 0.4), a mirror cuboid, a glass cuboid (specular reflection and
+    transmission, 0.1 / 0.9, coincident delta atoms never merge here since their directions
+    differ), a rough-diffuse plus conductor sphere, the ceiling emitter, a point light, a spot light
+    and a directional light entering through the open front."""
+    nm = builder.nanometers
+    white = builder.add_material(lambertian([0.73] * 4))
+    back_eon = builder.add_material(rough_diffuse([0.7, 0.72, 0.75, 0.73], 0.6))
+    red = builder.add_material(lambertian(tabulated_spectrum(RED_WALL, nm)))
+    green = builder.add_material(lambertian(tabulated_spectrum(GREEN_WALL, nm)))
+    light = builder.add_material(lambertian([0.0] * 4), emission=(17.0, 17.0, 17.0, 17.0))
+    gold_eta, gold_k = tabulated_spectrum(GOLD_ETA, nm), tabulated_spectrum(GOLD_K, nm)
+    layered = builder.add_material(lambertian([0.5, 0.45, 0.4, 0.42]) +
+                                   rough_conductor([0.6] * 4, gold_eta, gold_k, 0.3, 0.15), probabilities=[0.6, 0.4])
+    mirror = builder.add_material(specular_reflection([0.9, 0.92, 0.95, 0.9]))
+    glass = builder.add_material(specular_reflection([0.08] * 4) + specular_transmission([0.92] * 4, 1.0, 1.5),
+                                 probabilities=[0.1, 0.9])
+    rough_metal = builder.add_material(rough_diffuse([0.3, 0.5, 0.4, 0.35], 1.0) +
+                                       rough_conductor([0.5] * 4, gold_eta, gold_k, 0.2, 0.2))
+
+    floor = builder.add_mesh(quad([(-1, -1, 0), (-1, -1, 2), (1, -1, 2), (1, -1, 0)], (0, 1, 0)))
+    ceiling = builder.add_mesh(quad([(-1, 1, 0), (1, 1, 0), (1, 1, 2), (-1, 1, 2)], (0, -1, 0)))
+    back = builder.add_mesh(quad([(-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0)], (0, 0, 1)))
+    left = builder.add_mesh(quad([(-1, -1, 0), (-1, 1, 0), (-1, 1, 2), (-1, -1, 2)], (1, 0, 0)))
+    right = builder.add_mesh(quad([(1, -1, 0), (1, -1, 2), (1, 1, 2), (1, 1, 0)], (-1, 0, 0)))
+    emitter = builder.add_mesh(quad([(-0.125, 0.985, 0.875), (0.125, 0.985, 0.875),
+                                     (0.125, 0.985, 1.125), (-0.125, 0.985, 1.125)],
+                                    (0, -1, 0)))
+    box = builder.add_mesh(unit_box())
+    builder.add_instance(floor, layered)
+    builder.add_instance(ceiling, white)
+    builder.add_instance(back, back_eon)
+    builder.add_instance(left, red)
+    builder.add_instance(right, green)
+    builder.add_instance(emitter, light)
+    builder.add_instance(box, mirror, rotation_y_scale_translate(18.0, (0.6, 1.2, 0.6), (-0.35, -0.4, 0.65)))
+    builder.add_instance(box, glass, rotation_y_scale_translate(-15.0, (0.6, 0.6, 0.6), (0.4, -0.7, 1.25)))
+    sphere = builder.add_mesh(uv_sphere())
+    builder.add_instance(sphere, rough_metal, uniform_scale_translate(0.25, (0.45, 0.1, 0.7)))
+    builder.add_point_light((-0.5, 0.7, 1.4), (0.8, 0.7, 0.6, 0.5), error=(1e-6, 1e-6, 1e-6))
+    builder.add_spot_light((0.6, 0.8, 1.8), (-0.37139067, -0.74278134, -0.55708601), 0.3, 0.6,
+                           (2.0, 2.2, 2.4, 2.6))
+    builder.add_directional_light((0.0, -0.6, -0.8), (0.4, 0.35, 0.3, 0.25))
     return builder
 
 
@@ -698,6 +795,7 @@ WORKLOADS = {
     "bvh_stress_1080p": (1920, 1080, 64, 16, "power", "bvh_stress"),
     "adjoint_icosphere_256": (256, 256, 64, 8, "power", "adjoint_icosphere"),
     "cornell_analytic_256": (256, 256, 256, 16, "power", "cornell_analytic"),
+    "cornell_layered_256": (256, 256, 64, 16, "power", "cornell_layered"),
 }
 
 
@@ -710,6 +808,8 @@ def build_workload(name):
         # exact derivatives of the rendered loss
         builder = adjoint_icosphere(SceneBuilder(), adjoint_parameters())
         return builder, abi.default_options(mis=mis, max_depth=depth, roulette=False), (width, height, spp)
+    elif scene == "cornell_layered":
+        builder = cornell_layered(SceneBuilder())
     else:
         builder = cornell_box(SceneBuilder(), with_spheres=scene in ("cornell_spheres", "cornell_analytic"),
                               analytic_spheres=scene == "cornell_analytic")

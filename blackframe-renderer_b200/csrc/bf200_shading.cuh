@@ -20,7 +20,9 @@ constexpr float kPi = 3.14159265358979323846F;
 
 constexpr uint32_t kLobeDiffuse = 0x01U, kLobeGlossy = 0x02U, kLobeSpecular = 0x04U;
 constexpr uint32_t kLobeReflection = 0x08U, kLobeTransmission = 0x10U, kLobeVolume = 0x20U;
-constexpr uint32_t kClosureLambert = 1U, kClosureConductor = 3U, kClosureDielectric = 4U;
+constexpr uint32_t kClosureLambert = 1U, kClosureRoughDiffuse = 2U, kClosureConductor = 3U, kClosureDielectric = 4U;
+constexpr uint32_t kClosureSpecularReflection = 5U, kClosureSpecularTransmission = 6U;
+constexpr uint32_t kMaxClosures = 8U;  // MaximumClosureCount (ClosureSet.hpp:15)
 
 // Lane failure codes (include/bf200.h BF200_LANE_*)
 constexpr uint32_t kLaneNumerical = 1U, kLaneUnsupported = 2U, kLaneTraversal = 3U;
@@ -586,6 +588,8 @@ struct BsdfSample {
     float pdf;
     uint32_t lobes;
     float eta_scale;
+    bool delta;         // pdf is a discrete mass (specular), not a solid-angle density
+    uint32_t selected;  // the sampled closure, as an index into the depth-filtered mixture
 };
 
 // SamplingMappings.hpp:33-60, 128-141
@@ -1304,11 +1308,20 @@ __device__ bool cone_scatter(float2 cone, const ClosureData& c, uint32_t event, 
     }
     float spread_floor = 0.0F, transmission_scale = 1.0F, width_scale = 1.0F;
     bool dielectric = false;
-    if (kind_is<K>(c, kClosureLambert)) {
+    if (kind_is<K>(c, kClosureLambert) || kind_is<K>(c, kClosureRoughDiffuse)) {
         if (!reflection || (event & kLobeDiffuse) == 0U) {
             return false;
         }
         spread_floor = 1.0F;
+    } else if (kind_is<K>(c, kClosureSpecularReflection)) {
+        if (!reflection || (event & kLobeSpecular) == 0U) {
+            return false;
+        }
+    } else if (kind_is<K>(c, kClosureSpecularTransmission)) {
+        if (!transmission || (event & kLobeSpecular) == 0U) {
+            return false;
+        }
+        dielectric = true;
     } else if (kind_is<K>(c, kClosureConductor)) {
         if (!reflection || (event & kLobeGlossy) == 0U || !isfinite(c.p[8]) || c.p[8] < 0.0F ||
             !isfinite(c.p[9]) || c.p[9] < 0.0F) {
@@ -1556,6 +1569,591 @@ static __device__ void closure_sample(const ClosureData& c, uint32_t allowed, F3
         return;
     }
     s.pdf = dielectric_pdf_masked(c, allowed, wo, s.wi, lane);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Energy-preserving Oren-Nayar rough diffuse reflection (RoughDiffuseReflection.hpp:62-283). The
+// arctangent is the double-precision value rounded once to float.
+// ------------------------------------------------------------------------------------------------
+
+constexpr float kFonCoefficient = 0.5F - 2.0F * kInvPi / 3.0F;
+constexpr float kFonAverageCoefficient = 2.0F / 3.0F - 28.0F * kInvPi / 15.0F;
+constexpr float kFonAverageLossCoefficient = kFonCoefficient - kFonAverageCoefficient;
+
+static __device__ __noinline__ float atan2_f(float y, float x) {
+    return static_cast<float>(atan2(static_cast<double>(y), static_cast<double>(x)));
+}
+
+// directional_loss_shape: 1 - E_FON for unit albedo without the factor A_F * r
+static __device__ float eon_loss_shape(F3 d, Lane& lane) {
+    const float sine = hypot2f(d.x, d.y);
+    const float cosine = d.z;
+    const float angle = atan2_f(sine, cosine);
+    const float stable_ratio = sine * cosine * (1.0F + sine + sine * sine) / (1.0F + sine);
+    const float g = sine * (angle - sine * cosine) + (2.0F / 3.0F) * (stable_ratio - sine);
+    const float loss = kFonCoefficient - g * kInvPi;
+    if (!isfinite(loss) || loss < 0.0F) {
+        lane.fail();
+    }
+    return loss;
+}
+
+static __device__ void eon_eval(const ClosureData& c, F3 wo, F3 wi, float (&out)[4], Lane& lane) {
+    out[0] = out[1] = out[2] = out[3] = 0.0F;
+    if (!unit_length(wo) || !unit_length(wi)) {
+        lane.fail();
+        return;
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F) || (c.w[0] == 0.0F && c.w[1] == 0.0F && c.w[2] == 0.0F && c.w[3] == 0.0F)) {
+        return;
+    }
+    const float r = c.p[0];
+    if (r == 0.0F) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            out[l] = c.w[l] * kInvPi;
+        }
+        return;
+    }
+    const float tangent_dot = fmaf(wo.x, wi.x, wo.y * wi.y);
+    const float s_over_t = tangent_dot > 0.0F ? tangent_dot / bf_max(wo.z, wi.z) : tangent_dot;
+    const float a = 1.0F / (1.0F + kFonCoefficient * r);
+    const float single = kInvPi * a * (1.0F + r * s_over_t);
+    if (!isfinite(single) || single < 0.0F) {
+        lane.fail();
+        return;
+    }
+    const float outgoing_loss = eon_loss_shape(wo, lane);
+    const float incoming_loss = eon_loss_shape(wi, lane);
+    const float average = a * (1.0F + kFonAverageCoefficient * r);
+    const float loss_over_average = a * r * incoming_loss * outgoing_loss / kFonAverageLossCoefficient;
+    if (!isfinite(average) || !(average > 0.0F) || average > 1.0F || !isfinite(loss_over_average) ||
+        loss_over_average < 0.0F) {
+        lane.fail();
+        return;
+    }
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        const float rho = c.w[l];
+        const float den = (1.0F - rho) + rho * average;
+        if (!isfinite(den) || !(den > 0.0F)) {
+            lane.fail();
+        }
+        const float ms = rho * rho * average / den;
+        const float value = rho * single + ms * kInvPi * loss_over_average;
+        if (!isfinite(value) || value < 0.0F) {
+            lane.fail();
+        }
+        out[l] = value;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Ideal specular reflection and transmission (SpecularDelta.hpp:85-495): eval and pdf queries
+// exclude the Dirac atom, sample() returns it with a discrete mass of one.
+// ------------------------------------------------------------------------------------------------
+
+// checked_positive_product_quotient
+__device__ __forceinline__ float delta_product_quotient(float left, float right, float den, Lane& lane) {
+    if (left == 0.0F) {
+        return 0.0F;
+    }
+    if (!isfinite(left) || !(left > 0.0F) || !isfinite(right) || !(right > 0.0F) || !isfinite(den) || !(den > 0.0F)) {
+        lane.fail();
+        return 0.0F;
+    }
+    int le = 0, re = 0, de = 0, ne = 0;
+    const float ls = frexpf(left, &le), rs = frexpf(right, &re), ds = frexpf(den, &de);
+    const float normalized = frexpf((ls * rs) / ds, &ne);
+    const float result = scalbnf(normalized, le + re - de + ne);
+    if (!isfinite(result) || !(result > 0.0F)) {
+        lane.fail();
+    }
+    return result;
+}
+
+// checked_squared_ratio
+__device__ __forceinline__ float delta_squared_ratio(float num, float den, Lane& lane) {
+    if (!isfinite(num) || !(num > 0.0F) || !isfinite(den) || !(den > 0.0F)) {
+        lane.fail();
+        return 1.0F;
+    }
+    int ne = 0, de = 0, re = 0;
+    const float ns = frexpf(num, &ne), ds = frexpf(den, &de);
+    const float ratio = ns / ds;
+    const float normalized = frexpf(ratio * ratio, &re);
+    const float result = scalbnf(normalized, 2 * (ne - de) + re);
+    if (!isfinite(result) || !(result > 0.0F)) {
+        lane.fail();
+    }
+    return result;
+}
+
+static __device__ void specular_sample(const ClosureData& c, F3 wo, BsdfSample& s, Lane& lane) {
+    s.valid = false;
+    s.delta = true;
+    s.pdf = 1.0F;
+    s.eta_scale = 1.0F;
+    if (!unit_length(wo)) {
+        lane.fail();
+        return;
+    }
+    if (wo.z == 0.0F) {
+        return;
+    }
+    if (c.kind == kClosureSpecularReflection) {
+        s.wi = F3{-wo.x, -wo.y, wo.z};
+        s.lobes = kLobeSpecular | kLobeReflection;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            s.value[l] = delta_product_quotient(c.w[l], 1.0F, fabsf(s.wi.z), lane);
+        }
+        s.valid = true;
+        return;
+    }
+    const bool entering = wo.z > 0.0F;
+    const float incident = entering ? c.p[0] : c.p[1];
+    const float transmitted = entering ? c.p[1] : c.p[0];
+    s.lobes = kLobeSpecular | kLobeTransmission;
+    if (incident == transmitted) {
+        s.wi = F3{-wo.x, -wo.y, -wo.z};
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            s.value[l] = delta_product_quotient(c.w[l], 1.0F, fabsf(s.wi.z), lane);
+        }
+        s.valid = true;
+        return;
+    }
+    const float raw_sine = hypot2f(wo.x, wo.y);
+    if (!isfinite(raw_sine)) {
+        lane.fail();
+        return;
+    }
+    float sine = raw_sine, normalization = 1.0F;
+    if (raw_sine > 1.0F) {
+        const float cosine = fabsf(wo.z);
+        if (cosine > 1.0F) {
+            lane.fail();
+            return;
+        }
+        sine = sqrtf((1.0F - cosine) * (1.0F + cosine));
+        normalization = sine / raw_sine;
+        if (!isfinite(sine) || !isfinite(normalization) || !(normalization > 0.0F)) {
+            lane.fail();
+            return;
+        }
+    }
+    if (sine > 0.0F) {
+        const float critical = transmitted / incident;
+        if (critical <= 1.0F && sine >= critical) {
+            return;  // total internal reflection: no transmission support
+        }
+    }
+    const float ratio = incident / transmitted;
+    if (!isfinite(ratio) || !(ratio > 0.0F)) {
+        lane.fail();
+        return;
+    }
+    const float ix = -ratio * normalization * wo.x;
+    const float iy = -ratio * normalization * wo.y;
+    if (!isfinite(ix) || !isfinite(iy) || (wo.x != 0.0F && ix == 0.0F) || (wo.y != 0.0F && iy == 0.0F)) {
+        lane.fail();
+        return;
+    }
+    const float transmitted_sine = hypot2f(ix, iy);
+    if (!isfinite(transmitted_sine) || transmitted_sine >= 1.0F) {
+        lane.fail();
+        return;
+    }
+    const float transmitted_cosine = sqrtf((1.0F - transmitted_sine) * (1.0F + transmitted_sine));
+    if (!isfinite(transmitted_cosine) || !(transmitted_cosine > 0.0F)) {
+        lane.fail();
+        return;
+    }
+    s.wi = F3{ix, iy, entering ? -transmitted_cosine : transmitted_cosine};
+    if (!unit_length(s.wi)) {
+        lane.fail();
+        return;
+    }
+    const float adjoint = delta_squared_ratio(incident, transmitted, lane);  // radiance mode
+    s.eta_scale = delta_squared_ratio(transmitted, incident, lane);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        s.value[l] = delta_product_quotient(c.w[l], adjoint, transmitted_cosine, lane);
+    }
+    s.valid = true;
+}
+
+// ------------------------------------------------------------------------------------------------
+// One closure record of any kind, the rough dielectric restricted to `allowed`
+// (DepthFilteredClosureMixture.hpp:182-252, ClosureMixture.hpp:527-748)
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ bool is_delta_kind(uint32_t kind) {
+    return kind == kClosureSpecularReflection || kind == kClosureSpecularTransmission;
+}
+
+static __device__ void record_eval(const ClosureData& c, uint32_t allowed, F3 wo, F3 wi, float (&out)[4], Lane& lane) {
+    if (c.kind == kClosureRoughDiffuse) {
+        eon_eval(c, wo, wi, out, lane);
+    } else if (is_delta_kind(c.kind)) {
+        out[0] = out[1] = out[2] = out[3] = 0.0F;
+        if (!unit_length(wo) || !unit_length(wi)) {
+            lane.fail();
+        }
+    } else {
+        closure_eval<0>(c, allowed, wo, wi, out, lane);
+    }
+}
+
+static __device__ float record_pdf(const ClosureData& c, uint32_t allowed, F3 wo, F3 wi, Lane& lane) {
+    if (c.kind == kClosureRoughDiffuse || is_delta_kind(c.kind)) {
+        if (!unit_length(wo) || !unit_length(wi)) {
+            lane.fail();
+            return 0.0F;
+        }
+        if (is_delta_kind(c.kind) || !(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return 0.0F;
+        }
+        return wi.z * kInvPi;
+    }
+    return closure_pdf<0>(c, allowed, wo, wi, lane);
+}
+
+static __device__ void record_sample(const ClosureData& c, uint32_t allowed, F3 wo, float event, float u, float v,
+                                     BsdfSample& s, Lane& lane) {
+    s.delta = false;
+    s.valid = false;
+    if (is_delta_kind(c.kind)) {
+        specular_sample(c, wo, s, lane);
+        return;
+    }
+    if (c.kind == kClosureRoughDiffuse) {  // RoughDiffuseReflection.hpp:235-266
+        s.eta_scale = 1.0F;
+        s.lobes = c.lobes;
+        if (!unit_length(wo)) {
+            lane.fail();
+            return;
+        }
+        const F3 wi = map_cosine_hemisphere(u, v);
+        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+            return;
+        }
+        s.wi = wi;
+        eon_eval(c, wo, wi, s.value, lane);
+        s.pdf = record_pdf(c, allowed, wo, wi, lane);
+        s.valid = true;
+        return;
+    }
+    closure_sample<0>(c, allowed, wo, event, u, v, s, lane);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Depth-filtered closure mixtures (DepthFilteredClosureMixture.hpp:254-552; ClosureMixture.hpp:
+// 79-334, 760-876). A material's closures are filtered by the depth limits; the survivors keep
+// their component probabilities, renormalised on the sampler grid when some were dropped.
+// ------------------------------------------------------------------------------------------------
+
+// A material's projected component distribution (build_component_distribution at upload).
+struct MixDistribution {
+    float p[kMaxClosures];
+    float cdf[kMaxClosures + 1];
+    uint32_t closure_offset;  // first closure in SceneView::mix_closures
+    uint32_t pad[2];
+};
+
+struct Mix {
+    ClosureData first;             // single-closure routes (K != 0): the closure itself
+    const ClosureData* closures;   // generic route (K == 0): the material's closures
+    uint32_t count, blocked;
+    uint8_t source[kMaxClosures], allowed[kMaxClosures];
+    float p[kMaxClosures];
+    float cdf[kMaxClosures + 1];
+};
+
+template <int K>
+__device__ __forceinline__ ClosureData mix_closure(const Mix& m, uint32_t i) {
+    if constexpr (K != 0) {
+        return m.first;
+    } else {
+        return m.closures[m.source[i]];
+    }
+}
+
+// add_compensated (ClosureMixture.hpp:78-99)
+__device__ __forceinline__ bool add_compensated(float value, float& sum, float& correction) {
+    if (!isfinite(value) || value < 0.0F) {
+        return false;
+    }
+    const float next = sum + value;
+    if (!isfinite(next)) {
+        return false;
+    }
+    if (sum >= value) {
+        correction += (sum - next) + value;
+    } else {
+        correction += (value - next) + sum;
+    }
+    if (!isfinite(correction)) {
+        return false;
+    }
+    sum = next;
+    return true;
+}
+
+// build_component_distribution (ClosureMixture.hpp:122-234) for n >= 2 renormalised probabilities
+static __device__ bool component_distribution(const float* probabilities, uint32_t n, float* out_p, float* out_cdf) {
+#pragma unroll
+    for (uint32_t i = 0; i <= kMaxClosures; ++i) {
+        out_cdf[i] = 0.0F;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!isfinite(probabilities[i]) || !(probabilities[i] > 0.0F) || !(probabilities[i] < 1.0F)) {
+            return false;
+        }
+    }
+    constexpr int digits = 24;
+    constexpr uint64_t scale = 1ULL << digits;
+    uint64_t masses[kMaxClosures];
+    float remainders[kMaxClosures];
+    uint64_t base_mass = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float scaled = ldexpf(probabilities[i], digits);
+        const float base = floorf(scaled);
+        if (!isfinite(scaled) || !(scaled > 0.0F) || base < 0.0F || base > static_cast<float>(scale)) {
+            return false;
+        }
+        masses[i] = static_cast<uint64_t>(base);
+        remainders[i] = scaled - base;
+        if (!isfinite(remainders[i]) || remainders[i] < 0.0F || remainders[i] >= 1.0F) {
+            return false;
+        }
+        base_mass += masses[i];
+    }
+    if (base_mass > scale) {
+        return false;
+    }
+    float rs = 0.0F, rc = 0.0F;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!add_compensated(remainders[i], rs, rc)) {
+            return false;
+        }
+    }
+    const float remainder_total = rs + rc;
+    if (!isfinite(remainder_total) || remainder_total < 0.0F) {
+        return false;
+    }
+    const uint64_t missing = scale - base_mass;
+    if (missing > n || fabsf(remainder_total - static_cast<float>(missing)) > 0.5F + kEps * 16.0F) {
+        return false;
+    }
+    uint32_t received = 0U;
+    for (uint64_t unit = 0; unit < missing; ++unit) {
+        uint32_t selected = n;
+        for (uint32_t i = 0; i < n; ++i) {
+            if ((received >> i) & 1U || !(remainders[i] > 0.0F)) {
+                continue;
+            }
+            if (selected == n || remainders[i] > remainders[selected]) {
+                selected = i;
+            }
+        }
+        if (selected == n) {
+            return false;
+        }
+        ++masses[selected];
+        received |= 1U << selected;
+    }
+    uint64_t cumulative = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (masses[i] == 0U || cumulative > scale - masses[i]) {
+            return false;
+        }
+        cumulative += masses[i];
+        out_p[i] = ldexpf(static_cast<float>(masses[i]), -digits);
+        out_cdf[i + 1] = ldexpf(static_cast<float>(cumulative), -digits);
+    }
+    return cumulative == scale && out_cdf[n] == 1.0F;
+}
+
+
+// positive_probability_product (ClosureMixture.hpp:249-268)
+__device__ __forceinline__ float positive_probability_product(float selection, float conditional, Lane& lane) {
+    if (conditional == 0.0F) {
+        return 0.0F;
+    }
+    int se = 0, ce = 0, ne = 0;
+    const float ss = frexpf(selection, &se), cs = frexpf(conditional, &ce);
+    const float normalized = frexpf(ss * cs, &ne);
+    const float product = scalbnf(normalized, se + ce + ne);
+    if (!isfinite(product) || !(product > 0.0F)) {
+        lane.fail();
+    }
+    return product;
+}
+
+// mix_probability_densities (ClosureMixture.hpp:270-334)
+static __device__ float mix_densities(const float* probabilities, const float* conditional, uint32_t n, Lane& lane) {
+    float maximum = 0.0F;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!isfinite(conditional[i]) || conditional[i] < 0.0F) {
+            lane.fail();
+            return 0.0F;
+        }
+        maximum = bf_max(maximum, conditional[i]);
+    }
+    if (n == 1U) {
+        return conditional[0];
+    }
+    if (maximum == 0.0F) {
+        return 0.0F;
+    }
+    float sum = 0.0F, correction = 0.0F;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float density = conditional[i];
+        const float ratio = density / maximum;
+        if (density > 0.0F && (!isfinite(ratio) || !(ratio > 0.0F))) {
+            lane.fail();
+            return 0.0F;
+        }
+        if (!add_compensated(positive_probability_product(probabilities[i], ratio, lane), sum, correction)) {
+            lane.fail();
+            return 0.0F;
+        }
+    }
+    const float normalized = sum + correction;
+    if (!isfinite(normalized) || !(normalized > 0.0F) || normalized > 1.0F) {
+        lane.fail();
+        return 0.0F;
+    }
+    return positive_probability_product(normalized, maximum, lane);
+}
+
+template <int K>
+__device__ void mix_eval(const Mix& m, F3 wo, F3 wi, float (&out)[4], Lane& lane) {
+    if constexpr (K != 0) {
+        closure_eval<K>(m.first, m.allowed[0], wo, wi, out, lane);
+    } else {
+        out[0] = out[1] = out[2] = out[3] = 0.0F;
+        if (!unit_length(wo) || !unit_length(wi)) {
+            lane.fail();
+            return;
+        }
+        for (uint32_t i = 0; i < m.count; ++i) {
+            float component[4];
+            record_eval(m.closures[m.source[i]], m.allowed[i], wo, wi, component, lane);
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+                out[l] = out[l] + component[l];
+                if (!isfinite(out[l])) {
+                    lane.fail();
+                }
+            }
+        }
+    }
+}
+
+template <int K>
+__device__ float mix_pdf(const Mix& m, F3 wo, F3 wi, Lane& lane) {
+    if constexpr (K != 0) {
+        return closure_pdf<K>(m.first, m.allowed[0], wo, wi, lane);
+    } else {
+        if (!unit_length(wo) || !unit_length(wi)) {
+            lane.fail();
+            return 0.0F;
+        }
+        float conditional[kMaxClosures];
+        for (uint32_t i = 0; i < m.count; ++i) {
+            conditional[i] = record_pdf(m.closures[m.source[i]], m.allowed[i], wo, wi, lane);
+        }
+        return mix_densities(m.p, conditional, m.count, lane);
+    }
+}
+
+// aggregate_delta_atom (ClosureMixture.hpp:760-870)
+static __device__ void aggregate_delta_atom(const Mix& m, F3 wo, F3 wi, float (&value)[4], float& probability,
+                                            Lane& lane) {
+    float vs[4] = {0.0F, 0.0F, 0.0F, 0.0F}, vc[4] = {0.0F, 0.0F, 0.0F, 0.0F};
+    float ps = 0.0F, pc = 0.0F;
+    uint32_t matching = 0;
+    for (uint32_t i = 0; i < m.count; ++i) {
+        const ClosureData c = m.closures[m.source[i]];
+        if (!is_delta_kind(c.kind)) {
+            continue;
+        }
+        BsdfSample candidate;
+        specular_sample(c, wo, candidate, lane);
+        if (!candidate.valid || candidate.wi.x != wi.x || candidate.wi.y != wi.y || candidate.wi.z != wi.z) {
+            continue;
+        }
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            if (!add_compensated(candidate.value[l], vs[l], vc[l])) {
+                lane.fail();
+            }
+        }
+        if (!add_compensated(positive_probability_product(m.p[i], candidate.pdf, lane), ps, pc)) {
+            lane.fail();
+        }
+        ++matching;
+    }
+    probability = ps + pc;
+    if (matching == 0U || !isfinite(probability) || !(probability > 0.0F) || probability > 1.0F) {
+        lane.fail();
+    }
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        value[l] = vs[l] + vc[l];
+        if (!isfinite(value[l]) || value[l] < 0.0F) {
+            lane.fail();
+        }
+    }
+}
+
+// DepthFilteredClosureMixture::sample (DepthFilteredClosureMixture.hpp:460-552)
+template <int K>
+__device__ void mix_sample(const Mix& m, F3 wo, float component, float u, float v, BsdfSample& s, Lane& lane) {
+    s.valid = false;
+    s.delta = false;
+    s.selected = 0U;
+    if constexpr (K != 0) {
+        closure_sample<K>(m.first, m.allowed[0], wo, component, u, v, s, lane);
+    } else {
+        if (!unit_length(wo) || !(component >= 0.0F && component < 1.0F) || !(u >= 0.0F && u < 1.0F) ||
+            !(v >= 0.0F && v < 1.0F)) {
+            lane.fail();
+            return;
+        }
+        uint32_t selected = m.count;
+        for (uint32_t i = 0; i < m.count; ++i) {
+            if (component < m.cdf[i + 1]) {
+                selected = i;
+                break;
+            }
+        }
+        if (selected == m.count) {
+            lane.fail();
+            return;
+        }
+        const float event = (component - m.cdf[selected]) / m.p[selected];
+        if (!isfinite(event) || event < 0.0F || !(event < 1.0F)) {
+            lane.fail();
+            return;
+        }
+        record_sample(m.closures[m.source[selected]], m.allowed[selected], wo, event, u, v, s, lane);
+        if (!s.valid) {
+            return;
+        }
+        if (m.count > 1U) {
+            if (!s.delta) {
+                mix_eval<0>(m, wo, s.wi, s.value, lane);
+                s.pdf = mix_pdf<0>(m, wo, s.wi, lane);
+            } else {
+                aggregate_delta_atom(m, wo, s.wi, s.value, s.pdf, lane);
+            }
+        }
+        s.selected = selected;
+    }
 }
 
 }  // namespace bf200

@@ -248,10 +248,34 @@ typedef struct bf200_instance_v1 {
     float world_to_object[16];
 } bf200_instance_v1;
 
+/* Punctual lights: engine::ScenePointLight, SceneDirectionalLight and SceneSpotLight
+ * (FrameScene.hpp:191-215), sampled as renderer::PointLight, DirectionalLight and SpotLight
+ * (PunctualLights.hpp:370-815). spectrum: the point light's spectral radiant intensity, the
+ * directional light's spectral irradiance, or the spot light's on-axis spectral radiant intensity,
+ * at the frame's packet. direction: the directional light's propagation direction (from the source
+ * into the scene) or the spot light's emission direction; unit length. 72 bytes. */
+#define BF200_PUNCTUAL_POINT 1u
+#define BF200_PUNCTUAL_DIRECTIONAL 2u
+#define BF200_PUNCTUAL_SPOT 3u
+
+typedef struct bf200_punctual_light_v1 {
+    uint32_t kind;                 /* BF200_PUNCTUAL_* */
+    uint32_t reserved;
+    float position[3];             /* point and spot */
+    float position_error[3];       /* point and spot: absolute world-space position error, >= 0 */
+    float direction[3];            /* directional and spot */
+    float inner_half_angle;        /* spot, radians: 0 <= inner <= outer < pi, outer > 0 */
+    float outer_half_angle;
+    float spectrum[4];
+} bf200_punctual_light_v1;
+
 /* A committed frame scene (engine::FrameScene, FrameScene.hpp:101-316), flattened. Triangle
- * vertex indices are local to their geometry. Mesh area lights are derived exactly as
- * FrameScene derives them (FrameScene.cpp:201-261): one light per instance whose material
- * emits, in instance order, after the punctual lights. */
+ * vertex indices are local to their geometry. The light registry is the punctual lights in the
+ * given order, then the mesh area lights, derived exactly as FrameScene derives them
+ * (FrameScene.cpp:201-261): one light per instance whose material emits, in instance order.
+ * A material may hold up to 8 closures (MaximumClosureCount), sampled by its component
+ * probabilities as SceneClosureMixture samples them. A caller built against the layout without
+ * `punctual_lights` passes struct_size = BF200_SCENE_DESC_V1_BASE_SIZE and no punctual lights. */
 typedef struct bf200_scene_desc_v1 {
     uint32_t struct_size;
     uint32_t geometry_count;
@@ -260,7 +284,7 @@ typedef struct bf200_scene_desc_v1 {
     uint32_t material_count;
     uint32_t closure_count;
     uint32_t instance_count;
-    uint32_t punctual_light_count; /* must be 0 in this version: punctual lights are rejected */
+    uint32_t punctual_light_count; /* entries of punctual_lights */
     const bf200_geometry_v1* geometries;
     const float* positions;        /* 3 * vertex_count */
     const float* normals;          /* 3 * vertex_count */
@@ -273,7 +297,9 @@ typedef struct bf200_scene_desc_v1 {
     float wavelength_pdf[4];
     float environment_radiance[4];
     uint32_t reserved[4];
+    const bf200_punctual_light_v1* punctual_lights;
 } bf200_scene_desc_v1;
+#define BF200_SCENE_DESC_V1_BASE_SIZE ((uint32_t)offsetof(bf200_scene_desc_v1, punctual_lights))
 
 /* renderer::Ray (48 bytes, the same size as the reference TransportRay). */
 typedef struct bf200_ray_v1 {

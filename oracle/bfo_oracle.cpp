@@ -56,6 +56,11 @@ float cos_f(float a) {
     return g_device_trig.load(std::memory_order_relaxed) != 0 ? static_cast<float>(std::cos(static_cast<double>(a)))
                                                               : std::cos(a);
 }
+float atan2_f(float y, float x) {
+    return g_device_trig.load(std::memory_order_relaxed) != 0
+               ? static_cast<float>(std::atan2(static_cast<double>(y), static_cast<double>(x)))
+               : std::atan2(y, x);
+}
 
 // Failure of one path: the reference returns std::unexpected for the whole path.
 struct Failure {
@@ -205,9 +210,13 @@ struct Closure {
     float p[10];
 };
 
+constexpr uint32_t kMaxClosures = 8;  // MaximumClosureCount (ClosureSet.hpp:15)
+
 struct Material {
-    Closure closure;
+    Closure closures[kMaxClosures];
     uint32_t closure_count;
+    float probability[kMaxClosures];  // the mixture's projected component distribution
+    float cdf[kMaxClosures + 1];
     uint32_t frame_mode;
     float rotation;
     Spectrum emission;
@@ -231,7 +240,17 @@ struct Instance {
     std::vector<V3> world_normals;   // per triangle
 };
 
+// A punctual light of the registry (FrameScene.hpp:191-215) with the constants its sampling uses.
+struct Punctual {
+    uint32_t kind;
+    V3 position, error, direction;
+    float cos_inner, cos_outer;
+    bool hard;
+    Spectrum spectrum;
+};
+
 struct Scene {
+    std::vector<Punctual> punctual;  // registry slots [0, punctual.size())
     std::vector<bf200_geometry_v1> geometries;
     std::vector<V3> positions, normals;
     std::vector<float> uvs;
@@ -1142,8 +1161,11 @@ struct LightSample {
     V3 position, error, normal;
     V3 direction;
     float distance;
-    float pdf;  // solid angle
+    float pdf;  // solid angle, or the discrete mass of a punctual light
     Spectrum radiance;
+    bool discrete = false;  // punctual: the pdf is a discrete probability
+    bool point = false;     // finite point endpoint (point and spot lights)
+    bool infinite = false;  // directional light: no endpoint
 };
 
 // IncidentLightSample::create_finite (Light.hpp:401-441): direction and distance.
@@ -1236,6 +1258,173 @@ float mesh_light_pdf_at_surface(const MeshLight& light, V3 context, V3 surface, 
     return pdf;
 }
 
+// scale_radiometric_value (PunctualLights.hpp:131-183): value x numerators / denominators, each
+// factor taken as a significand and an exponent so no partial product under- or overflows.
+float scale_radiometric(float value, const float* num, int nn, const float* den, int nd) {
+    if (!std::isfinite(value) || value < 0.0F) {
+        fail("Punctual light radiometric values must be finite and non-negative.");
+    }
+    for (int i = 0; i < nn; ++i) {
+        if (!std::isfinite(num[i]) || !(num[i] > 0.0F)) {
+            fail("A punctual light radiometric numerator is not representable.");
+        }
+    }
+    for (int i = 0; i < nd; ++i) {
+        if (!std::isfinite(den[i]) || !(den[i] > 0.0F)) {
+            fail("A punctual light radiometric denominator is not representable.");
+        }
+    }
+    if (value == 0.0F) {
+        return 0.0F;
+    }
+    int exponent = 0;
+    float fraction = std::frexp(value, &exponent);
+    long long accumulated = exponent;
+    for (int i = 0; i < nn; ++i) {
+        int e = 0;
+        fraction *= std::frexp(num[i], &e);
+        accumulated += e;
+    }
+    for (int i = 0; i < nd; ++i) {
+        int e = 0;
+        fraction /= std::frexp(den[i], &e);
+        accumulated -= e;
+    }
+    int ne = 0;
+    fraction = std::frexp(fraction, &ne);
+    accumulated += ne;
+    const float result = std::scalbn(fraction, static_cast<int>(accumulated));
+    if (!std::isfinite(result) || !(result > 0.0F)) {
+        fail("A positive punctual light result is not representable in the requested precision.");
+    }
+    return result;
+}
+
+// PointLight / DirectionalLight / SpotLight::sample_li (PunctualLights.hpp:390-430, 510-530,
+// 654-720) with IncidentLightSample::create_finite / create_infinite (Light.hpp:404-456).
+LightSample sample_punctual_light(const Punctual& light, V3 context, float u, float v) {
+    LightSample out;
+    if (!std::isfinite(u) || !std::isfinite(v) || u < 0.0F || u >= 1.0F || v < 0.0F || v >= 1.0F) {
+        fail("Punctual light sampling requires a finite canonical sample in [0, 1)^2.");
+    }
+    out.discrete = true;
+    out.pdf = 1.0F;
+    if (light.kind == BF200_PUNCTUAL_DIRECTIONAL) {
+        if (is_black(light.spectrum)) {
+            return out;
+        }
+        out.direction = V3{-light.direction.x, -light.direction.y, -light.direction.z};
+        if (!unit_length(out.direction)) {
+            fail("An incident light sample requires a finite unit direction.");
+        }
+        out.distance = kInfinity;
+        out.radiance = light.spectrum;
+        out.infinite = true;
+        out.valid = true;
+        return out;
+    }
+    // finite_light_geometry (PunctualLights.hpp:102-129)
+    const V3 disp = light.position - context;
+    if (!std::isfinite(disp.x) || !std::isfinite(disp.y) || !std::isfinite(disp.z)) {
+        fail("Finite punctual light separation is not representable in the requested precision.");
+    }
+    const float scale = max_abs3(disp);
+    if (!(scale > 0.0F) || !std::isfinite(scale)) {
+        fail("A finite punctual light cannot be sampled at its own position.");
+    }
+    const V3 scaled = disp / scale;
+    const float squared = std::fma(scaled.x, scaled.x, std::fma(scaled.y, scaled.y, scaled.z * scaled.z));
+    const float root = std::sqrt(squared);
+    const float distance = scale * root;
+    if (!std::isfinite(squared) || !(squared > 0.0F) || !std::isfinite(root) || !(root > 0.0F) ||
+        !std::isfinite(distance) || !(distance > 0.0F)) {
+        fail("Finite punctual light distance is not representable in the requested precision.");
+    }
+    const V3 to_light = scaled / root;
+    if (!unit_length(to_light)) {
+        fail("Finite punctual light direction is not representable as a unit vector.");
+    }
+    float falloff[3] = {1.0F, 1.0F, 1.0F};
+    int falloff_count = 0;
+    if (light.kind == BF200_PUNCTUAL_SPOT) {
+        const V3 from_light{-to_light.x, -to_light.y, -to_light.z};
+        const float cone = std::fma(light.direction.x, from_light.x,
+                                    std::fma(light.direction.y, from_light.y, light.direction.z * from_light.z));
+        if (!std::isfinite(cone)) {
+            fail("Spot light cone evaluation is not representable.");
+        }
+        if (cone <= light.cos_outer) {
+            return out;
+        }
+        falloff_count = 3;
+        if (!light.hard && cone < light.cos_inner) {
+            const float transition = (cone - light.cos_outer) / (light.cos_inner - light.cos_outer);
+            const float smooth = 3.0F - 2.0F * transition;
+            if (!std::isfinite(transition) || !(transition > 0.0F) || !(transition < 1.0F) ||
+                !std::isfinite(smooth) || !(smooth > 0.0F)) {
+                fail("Spot light smooth falloff is not representable.");
+            }
+            falloff[0] = transition;
+            falloff[1] = transition;
+            falloff[2] = smooth;
+        }
+    }
+    const float den[3] = {scale, scale, squared};
+    for (int lane = 0; lane < 4; ++lane) {
+        out.radiance[lane] = scale_radiometric(light.spectrum[lane], falloff, falloff_count, den, 3);
+    }
+    if (is_black(light.spectrum)) {
+        return out;
+    }
+    incident_direction(context, light.position, out.direction, out.distance);
+    out.position = light.position;
+    out.error = light.error;
+    out.point = true;
+    out.valid = true;
+    return out;
+}
+
+// contract_point_endpoint (ShadowRay.hpp:66-113): the point light's endpoint moved toward the
+// shading point past its position error, so the shadow ray's interval excludes the light.
+V3 contract_point_endpoint(V3 point, V3 error, V3 to_light) {
+    float contraction = 0.0F;
+    auto support = [&](float direction, float e) {
+        const float candidate = std::fma(std::abs(direction), e, contraction);
+        if (!std::isfinite(candidate) || candidate < contraction) {
+            fail("A shadow-ray point-endpoint contraction is not representable.");
+        }
+        if (direction != 0.0F && e != 0.0F) {
+            contraction = std::nextafter(candidate, kInfinity);
+            if (!std::isfinite(contraction)) {
+                fail("A shadow-ray point-endpoint contraction is not representable.");
+            }
+        } else {
+            contraction = candidate;
+        }
+    };
+    support(to_light.x, error.x);
+    support(to_light.y, error.y);
+    support(to_light.z, error.z);
+    if (contraction == 0.0F) {
+        return point;
+    }
+    V3 c{std::fma(-to_light.x, contraction, point.x), std::fma(-to_light.y, contraction, point.y),
+         std::fma(-to_light.z, contraction, point.z)};
+    if (to_light.x != 0.0F) {
+        c.x = std::nextafter(c.x, to_light.x > 0.0F ? -kInfinity : kInfinity);
+    }
+    if (to_light.y != 0.0F) {
+        c.y = std::nextafter(c.y, to_light.y > 0.0F ? -kInfinity : kInfinity);
+    }
+    if (to_light.z != 0.0F) {
+        c.z = std::nextafter(c.z, to_light.z > 0.0F ? -kInfinity : kInfinity);
+    }
+    if (!std::isfinite(c.x) || !std::isfinite(c.y) || !std::isfinite(c.z)) {
+        fail("A shadow-ray point endpoint exceeds the finite coordinate range.");
+    }
+    return c;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Closures
 // ---------------------------------------------------------------------------------------------
@@ -1245,8 +1434,10 @@ struct BsdfSample {
     V3 wi;
     Spectrum value{};
     float pdf = 0.0F;
+    bool delta = false;  // pdf is a discrete (delta) mass rather than a solid-angle density
     uint32_t lobes = 0;
     float eta_scale = 1.0F;
+    uint32_t selected = 0;  // the source index of the sampled closure
 };
 
 // SamplingMappings.hpp:33-60 and 128-141 (concentric disk, cosine hemisphere).
@@ -1982,6 +2173,445 @@ struct Depth {
     uint32_t total() const { return c[0] + c[1] + c[2] + c[4]; }
 };
 
+
+// ---------------------------------------------------------------------------------------------
+// Energy-preserving Oren-Nayar rough diffuse reflection (RoughDiffuseReflection.hpp:62-283)
+// ---------------------------------------------------------------------------------------------
+
+constexpr float kFonCoefficient = 0.5F - 2.0F * kInvPi / 3.0F;
+constexpr float kFonAverageCoefficient = 2.0F / 3.0F - 28.0F * kInvPi / 15.0F;
+constexpr float kFonAverageLossCoefficient = kFonCoefficient - kFonAverageCoefficient;
+
+// directional_loss_shape: 1 - E_FON for unit albedo without the factor A_F * r.
+float eon_loss_shape(V3 d) {
+    const float sine = std::hypot(d.x, d.y);
+    const float cosine = d.z;
+    const float angle = atan2_f(sine, cosine);
+    const float stable_ratio = sine * cosine * (1.0F + sine + sine * sine) / (1.0F + sine);
+    const float g = sine * (angle - sine * cosine) + (2.0F / 3.0F) * (stable_ratio - sine);
+    const float loss = kFonCoefficient - g * kInvPi;
+    if (!std::isfinite(loss) || loss < 0.0F) {
+        fail("The rough-diffuse directional albedo is not representable for the supplied direction.");
+    }
+    return loss;
+}
+
+Spectrum eon_eval(const Closure& c, V3 wo, V3 wi) {
+    if (!unit_length(wo) || !unit_length(wi)) {
+        fail("Rough-diffuse directions must be finite unit vectors.");
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F) || is_black(c.weight)) {
+        return Spectrum{};
+    }
+    const float r = c.p[0];
+    if (r == 0.0F) {
+        return Spectrum{c.weight[0] * kInvPi, c.weight[1] * kInvPi, c.weight[2] * kInvPi, c.weight[3] * kInvPi};
+    }
+    const float tangent_dot = std::fma(wo.x, wi.x, wo.y * wi.y);
+    const float s_over_t = tangent_dot > 0.0F ? tangent_dot / std::max(wo.z, wi.z) : tangent_dot;
+    const float a = 1.0F / (1.0F + kFonCoefficient * r);
+    const float single = kInvPi * a * (1.0F + r * s_over_t);
+    if (!std::isfinite(single) || single < 0.0F) {
+        fail("The rough-diffuse single-scattering value is not representable.");
+    }
+    const float outgoing_loss = eon_loss_shape(wo);
+    const float incoming_loss = eon_loss_shape(wi);
+    const float average = a * (1.0F + kFonAverageCoefficient * r);
+    const float loss_over_average = a * r * incoming_loss * outgoing_loss / kFonAverageLossCoefficient;
+    if (!std::isfinite(average) || !(average > 0.0F) || average > 1.0F || !std::isfinite(loss_over_average) ||
+        loss_over_average < 0.0F) {
+        fail("The rough-diffuse energy compensation is not representable.");
+    }
+    Spectrum out{};
+    for (int lane = 0; lane < 4; ++lane) {
+        const float rho = c.weight[lane];
+        const float den = (1.0F - rho) + rho * average;
+        if (!std::isfinite(den) || !(den > 0.0F)) {
+            fail("The rough-diffuse multiple-scattering albedo is not representable.");
+        }
+        const float ms = rho * rho * average / den;
+        const float value = rho * single + ms * kInvPi * loss_over_average;
+        if (!std::isfinite(value) || value < 0.0F) {
+            fail("The rough-diffuse BRDF value is not representable.");
+        }
+        out[lane] = value;
+    }
+    return out;
+}
+
+float cosine_pdf(V3 wo, V3 wi, const char* message) {  // Lambertian / rough-diffuse pdf
+    if (!unit_length(wo) || !unit_length(wi)) {
+        fail(message);
+    }
+    if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
+        return 0.0F;
+    }
+    const float v = wi.z * kInvPi;
+    if (!(v > 0.0F) || !std::isfinite(v)) {
+        fail("A diffuse PDF is not representable for the supplied direction.");
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ideal specular reflection and transmission (SpecularDelta.hpp:85-495). Directional eval/pdf
+// queries exclude the Dirac atom (zero value, zero solid-angle density); only sample() exposes
+// the discrete mass.
+// ---------------------------------------------------------------------------------------------
+
+float delta_product_quotient(float left, float right, float den) {  // checked_positive_product_quotient
+    if (left == 0.0F) {
+        return 0.0F;
+    }
+    if (!std::isfinite(left) || !(left > 0.0F) || !std::isfinite(right) || !(right > 0.0F) ||
+        !std::isfinite(den) || !(den > 0.0F)) {
+        fail("A specular delta value is not representable in the requested precision.");
+    }
+    int le = 0, re = 0, de = 0, ne = 0;
+    const float ls = std::frexp(left, &le), rs = std::frexp(right, &re), ds = std::frexp(den, &de);
+    const float normalized = std::frexp((ls * rs) / ds, &ne);
+    const float result = std::scalbn(normalized, le + re - de + ne);
+    if (!std::isfinite(result) || !(result > 0.0F)) {
+        fail("A specular delta value is not representable in the requested precision.");
+    }
+    return result;
+}
+
+float delta_squared_ratio(float num, float den) {  // checked_squared_ratio
+    if (!std::isfinite(num) || !(num > 0.0F) || !std::isfinite(den) || !(den > 0.0F)) {
+        fail("A specular transmission factor is not representable.");
+    }
+    int ne = 0, de = 0, re = 0;
+    const float ns = std::frexp(num, &ne), ds = std::frexp(den, &de);
+    const float ratio = ns / ds;
+    const float normalized = std::frexp(ratio * ratio, &re);
+    const float result = std::scalbn(normalized, 2 * (ne - de) + re);
+    if (!std::isfinite(result) || !(result > 0.0F)) {
+        fail("A specular transmission factor is not representable.");
+    }
+    return result;
+}
+
+BsdfSample specular_reflection_sample(const Closure& c, V3 wo) {
+    BsdfSample s;
+    if (!unit_length(wo)) {
+        fail("Specular delta directions must be finite unit vectors.");
+    }
+    if (wo.z == 0.0F) {
+        return s;
+    }
+    s.wi = V3{-wo.x, -wo.y, wo.z};
+    for (int lane = 0; lane < 4; ++lane) {
+        s.value[lane] = delta_product_quotient(c.weight[lane], 1.0F, std::abs(s.wi.z));
+    }
+    s.pdf = 1.0F;
+    s.delta = true;
+    s.lobes = BF200_LOBE_SPECULAR | BF200_LOBE_REFLECTION;
+    s.valid = true;
+    return s;
+}
+
+BsdfSample specular_transmission_sample(const Closure& c, V3 wo) {
+    BsdfSample s;
+    if (!unit_length(wo)) {
+        fail("Specular delta directions must be finite unit vectors.");
+    }
+    if (wo.z == 0.0F) {
+        return s;
+    }
+    const bool entering = wo.z > 0.0F;
+    const float incident = entering ? c.p[0] : c.p[1];
+    const float transmitted = entering ? c.p[1] : c.p[0];
+    s.lobes = BF200_LOBE_SPECULAR | BF200_LOBE_TRANSMISSION;
+    s.delta = true;
+    s.pdf = 1.0F;
+    if (incident == transmitted) {
+        s.wi = V3{-wo.x, -wo.y, -wo.z};
+        for (int lane = 0; lane < 4; ++lane) {
+            s.value[lane] = delta_product_quotient(c.weight[lane], 1.0F, std::abs(s.wi.z));
+        }
+        s.valid = true;
+        return s;
+    }
+    const float raw_sine = std::hypot(wo.x, wo.y);
+    if (!std::isfinite(raw_sine)) {
+        fail("The specular transmission incident sine is not representable.");
+    }
+    float sine = raw_sine, normalization = 1.0F;
+    if (raw_sine > 1.0F) {
+        const float cosine = std::abs(wo.z);
+        if (cosine > 1.0F) {
+            fail("The specular transmission incident direction is inconsistent.");
+        }
+        sine = std::sqrt((1.0F - cosine) * (1.0F + cosine));
+        normalization = sine / raw_sine;
+        if (!std::isfinite(sine) || !std::isfinite(normalization) || !(normalization > 0.0F)) {
+            fail("The specular transmission incident sine is not representable.");
+        }
+    }
+    if (sine > 0.0F) {
+        const float critical = transmitted / incident;
+        if (critical <= 1.0F && sine >= critical) {
+            return BsdfSample{};
+        }
+    }
+    const float ratio = incident / transmitted;
+    if (!std::isfinite(ratio) || !(ratio > 0.0F)) {
+        fail("The specular transmission relative index is not representable.");
+    }
+    const float ix = -ratio * normalization * wo.x;
+    const float iy = -ratio * normalization * wo.y;
+    if (!std::isfinite(ix) || !std::isfinite(iy) || (wo.x != 0.0F && ix == 0.0F) || (wo.y != 0.0F && iy == 0.0F)) {
+        fail("The specular transmission tangent is not representable.");
+    }
+    const float transmitted_sine = std::hypot(ix, iy);
+    if (!std::isfinite(transmitted_sine)) {
+        fail("The specular transmission sine is not representable.");
+    }
+    if (transmitted_sine >= 1.0F) {
+        fail("A subcritical specular transmission direction is not representable.");
+    }
+    const float transmitted_cosine = std::sqrt((1.0F - transmitted_sine) * (1.0F + transmitted_sine));
+    if (!std::isfinite(transmitted_cosine) || !(transmitted_cosine > 0.0F)) {
+        fail("The specular transmission cosine is not representable.");
+    }
+    s.wi = V3{ix, iy, entering ? -transmitted_cosine : transmitted_cosine};
+    if (!unit_length(s.wi)) {
+        fail("The refracted specular direction is not a representable unit vector.");
+    }
+    const float adjoint = delta_squared_ratio(incident, transmitted);  // radiance mode
+    s.eta_scale = delta_squared_ratio(transmitted, incident);
+    for (int lane = 0; lane < 4; ++lane) {
+        s.value[lane] = delta_product_quotient(c.weight[lane], adjoint, transmitted_cosine);
+    }
+    s.valid = true;
+    return s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Depth limits (PathDepthLimits.cpp) and the depth-filtered closure mixture
+// (DepthFilteredClosureMixture.hpp:254-552, ClosureMixture.hpp:79-334, 760-876)
+// ---------------------------------------------------------------------------------------------
+
+bool valid_surface_event(uint32_t lobes) {  // TransportConventions.hpp:101-109
+    const uint32_t family = lobes & (BF200_LOBE_DIFFUSE | BF200_LOBE_GLOSSY | BF200_LOBE_SPECULAR);
+    const uint32_t direction = lobes & (BF200_LOBE_REFLECTION | BF200_LOBE_TRANSMISSION);
+    return lobes != 0U && (lobes & ~0x3FU) == 0U && (lobes & BF200_LOBE_VOLUME) == 0U &&
+           (family == BF200_LOBE_DIFFUSE || family == BF200_LOBE_GLOSSY || family == BF200_LOBE_SPECULAR) &&
+           (direction == BF200_LOBE_REFLECTION || direction == BF200_LOBE_TRANSMISSION);
+}
+
+bool is_delta_kind(uint32_t kind) {
+    return kind == BF200_CLOSURE_SPECULAR_REFLECTION || kind == BF200_CLOSURE_SPECULAR_TRANSMISSION;
+}
+
+// add_compensated (ClosureMixture.hpp:78-99): a Neumaier step over non-negative values.
+bool add_compensated(float value, float& sum, float& correction) {
+    if (!std::isfinite(value) || value < 0.0F) {
+        return false;
+    }
+    const float next = sum + value;
+    if (!std::isfinite(next)) {
+        return false;
+    }
+    if (sum >= value) {
+        correction += (sum - next) + value;
+    } else {
+        correction += (value - next) + sum;
+    }
+    if (!std::isfinite(correction)) {
+        return false;
+    }
+    sum = next;
+    return true;
+}
+
+float compensated_sum(const float* values, uint32_t n) {  // ClosureMixture.hpp:105-120
+    float sum = 0.0F, correction = 0.0F;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!add_compensated(values[i], sum, correction)) {
+            fail("Closure-mixture probability accumulation is not representable.");
+        }
+    }
+    const float total = sum + correction;
+    if (!std::isfinite(total) || total < 0.0F) {
+        fail("Closure-mixture probability accumulation is not representable.");
+    }
+    return total == 0.0F ? 0.0F : total;
+}
+
+// build_component_distribution (ClosureMixture.hpp:122-234): the probabilities projected onto the
+// 2^-24 sampler grid (largest remainders first) and their CDF. Returns false with `error` set
+// instead of failing, so scene creation can report it.
+bool component_distribution(const float* probabilities, uint32_t n, bool allow_empty, float* out_p, float* out_cdf,
+                            const char** error) {
+    for (uint32_t i = 0; i <= kMaxClosures; ++i) {
+        out_cdf[i] = 0.0F;
+        if (i < kMaxClosures) {
+            out_p[i] = 0.0F;
+        }
+    }
+    if (n > kMaxClosures) {
+        *error = "Closure-mixture probabilities must match the active closure count.";
+        return false;
+    }
+    if (n == 0U) {
+        if (!allow_empty) {
+            *error = "A probability mixture requires at least one component.";
+        }
+        return allow_empty;
+    }
+    if (n == 1U) {
+        if (probabilities[0] != 1.0F) {
+            *error = "A singleton closure mixture requires probability one.";
+            return false;
+        }
+        out_p[0] = 1.0F;
+        out_cdf[1] = 1.0F;
+        return true;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!std::isfinite(probabilities[i]) || !(probabilities[i] > 0.0F) || !(probabilities[i] < 1.0F)) {
+            *error = "A multi-closure mixture requires finite probabilities strictly between zero and one.";
+            return false;
+        }
+    }
+    constexpr int digits = std::numeric_limits<float>::digits;
+    constexpr uint64_t scale = uint64_t{1} << digits;
+    uint64_t masses[kMaxClosures] = {};
+    float remainders[kMaxClosures] = {};
+    uint64_t base_mass = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float scaled = std::ldexp(probabilities[i], digits);
+        const float base = std::floor(scaled);
+        if (!std::isfinite(scaled) || !(scaled > 0.0F) || base < 0.0F || base > static_cast<float>(scale)) {
+            *error = "A closure-mixture probability cannot be projected onto the sampler grid.";
+            return false;
+        }
+        masses[i] = static_cast<uint64_t>(base);
+        remainders[i] = scaled - base;
+        if (!std::isfinite(remainders[i]) || remainders[i] < 0.0F || remainders[i] >= 1.0F) {
+            *error = "A closure-mixture probability cannot be projected onto the sampler grid.";
+            return false;
+        }
+        base_mass += masses[i];
+    }
+    if (base_mass > scale) {
+        *error = "Closure-mixture probabilities exceed one on the sampler grid.";
+        return false;
+    }
+    float remainder_sum = 0.0F, remainder_correction = 0.0F;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!add_compensated(remainders[i], remainder_sum, remainder_correction)) {
+            *error = "Closure-mixture probability accumulation is not representable.";
+            return false;
+        }
+    }
+    float remainder_total = remainder_sum + remainder_correction;
+    if (!std::isfinite(remainder_total) || remainder_total < 0.0F) {
+        *error = "Closure-mixture probability accumulation is not representable.";
+        return false;
+    }
+    if (remainder_total == 0.0F) {
+        remainder_total = 0.0F;
+    }
+    const uint64_t missing = scale - base_mass;
+    if (missing > n) {
+        *error = "Closure-mixture probabilities do not sum to one at sampler precision.";
+        return false;
+    }
+    constexpr float tolerance = std::numeric_limits<float>::epsilon() * 16.0F;
+    if (std::abs(remainder_total - static_cast<float>(missing)) > 0.5F + tolerance) {
+        *error = "Closure-mixture probabilities do not round to one at sampler precision.";
+        return false;
+    }
+    bool received[kMaxClosures] = {};
+    for (uint64_t unit = 0; unit < missing; ++unit) {
+        uint32_t selected = n;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (received[i] || !(remainders[i] > 0.0F)) {
+                continue;
+            }
+            if (selected == n || remainders[i] > remainders[selected]) {
+                selected = i;
+            }
+        }
+        if (selected == n) {
+            *error = "Closure-mixture rounding cannot preserve every positive component.";
+            return false;
+        }
+        ++masses[selected];
+        received[selected] = true;
+    }
+    uint64_t cumulative = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (masses[i] == 0U || cumulative > scale - masses[i]) {
+            *error = "A positive closure-mixture probability is not representable on the sampler grid.";
+            return false;
+        }
+        cumulative += masses[i];
+        out_p[i] = std::ldexp(static_cast<float>(masses[i]), -digits);
+        out_cdf[i + 1] = std::ldexp(static_cast<float>(cumulative), -digits);
+    }
+    if (cumulative != scale || out_cdf[n] != 1.0F) {
+        *error = "The closure-mixture CDF does not terminate at one.";
+        return false;
+    }
+    return true;
+}
+
+// positive_probability_product (ClosureMixture.hpp:249-268)
+float positive_probability_product(float selection, float conditional) {
+    if (conditional == 0.0F) {
+        return 0.0F;
+    }
+    int se = 0, ce = 0, ne = 0;
+    const float ss = std::frexp(selection, &se), cs = std::frexp(conditional, &ce);
+    const float normalized = std::frexp(ss * cs, &ne);
+    const float product = std::scalbn(normalized, se + ce + ne);
+    if (!std::isfinite(product) || !(product > 0.0F)) {
+        fail("A positive weighted closure PDF is not representable in the requested precision.");
+    }
+    return product;
+}
+
+// mix_probability_densities (ClosureMixture.hpp:270-334) over solid-angle densities.
+float mix_densities(const float* probabilities, const float* conditional, uint32_t n) {
+    if (n == 0U) {
+        fail("Closure PDF components require a non-empty matching sampling distribution.");
+    }
+    float maximum = 0.0F;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!std::isfinite(conditional[i]) || conditional[i] < 0.0F) {
+            fail("Closure PDF components require finite non-negative solid-angle densities.");
+        }
+        maximum = std::max(maximum, conditional[i]);
+    }
+    if (n == 1U) {
+        return conditional[0];
+    }
+    if (maximum == 0.0F) {
+        return 0.0F;
+    }
+    float sum = 0.0F, correction = 0.0F;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float density = conditional[i];
+        const float ratio = density / maximum;
+        if (density > 0.0F && (!std::isfinite(ratio) || !(ratio > 0.0F))) {
+            fail("A positive normalized closure PDF is not representable in the requested precision.");
+        }
+        const float contribution = positive_probability_product(probabilities[i], ratio);
+        if (!add_compensated(contribution, sum, correction)) {
+            fail("The weighted closure PDF sum is not representable in the requested precision.");
+        }
+    }
+    const float normalized = sum + correction;
+    if (!std::isfinite(normalized) || !(normalized > 0.0F) || normalized > 1.0F) {
+        fail("The normalized closure PDF sum is not representable in the requested precision.");
+    }
+    return positive_probability_product(normalized, maximum);
+}
+
 uint32_t blocked_limits(const uint32_t* limits, const Depth& d, uint32_t lobes) {
     uint32_t blocked = 0;
     if ((lobes & BF200_LOBE_DIFFUSE) && d.c[0] >= limits[0]) blocked |= BF200_LOBE_DIFFUSE;
@@ -2002,34 +2632,87 @@ Depth advanced(const Depth& d, uint32_t lobes) {
     return r;
 }
 
-struct Filtered {
-    bool active = false;
-    uint32_t allowed = 0;  // direction mask
+// One material's closures after the depth filter: the active closures (source order), their
+// allowed directions and their renormalised component distribution.
+struct Mixture {
+    uint32_t count = 0;
+    uint32_t source[kMaxClosures] = {};
+    uint32_t allowed[kMaxClosures] = {};
+    float p[kMaxClosures] = {};
+    float cdf[kMaxClosures + 1] = {};
     uint32_t blocked = 0;
+    const Material* material = nullptr;
+    const Closure& closure(uint32_t i) const { return material->closures[source[i]]; }
 };
 
-// DepthFilteredClosureMixture.hpp:262-364 for a one-closure mixture.
-Filtered depth_filter(const Closure& c, const uint32_t* limits, const Depth& d) {
-    Filtered f;
-    auto consider = [&](uint32_t event, uint32_t direction) {
-        const uint32_t b = blocked_limits(limits, d, event);
-        if (b == 0U) {
-            f.allowed |= direction;
+// DepthFilteredClosureMixture::create (DepthFilteredClosureMixture.hpp:262-364)
+Mixture depth_filter(const Material& material, const uint32_t* limits, const Depth& d) {
+    Mixture m;
+    m.material = &material;
+    for (uint32_t i = 0; i < material.closure_count; ++i) {
+        const Closure& c = material.closures[i];
+        uint32_t allowed = 0;
+        auto consider = [&](uint32_t event, uint32_t direction) {
+            const uint32_t b = blocked_limits(limits, d, event);
+            if (b == 0U) {
+                allowed |= direction;
+            } else {
+                m.blocked |= b;
+            }
+        };
+        if (c.kind == BF200_CLOSURE_ROUGH_DIELECTRIC) {
+            consider(BF200_LOBE_GLOSSY | BF200_LOBE_REFLECTION, BF200_LOBE_REFLECTION);
+            consider(BF200_LOBE_GLOSSY | BF200_LOBE_TRANSMISSION, BF200_LOBE_TRANSMISSION);
         } else {
-            f.blocked |= b;
+            if (!valid_surface_event(c.lobes)) {
+                fail("A depth-filtered closure record requires a concrete surface event.");
+            }
+            consider(c.lobes, c.lobes & (BF200_LOBE_REFLECTION | BF200_LOBE_TRANSMISSION));
         }
-    };
-    if (c.kind == BF200_CLOSURE_ROUGH_DIELECTRIC) {
-        consider(BF200_LOBE_GLOSSY | BF200_LOBE_REFLECTION, BF200_LOBE_REFLECTION);
-        consider(BF200_LOBE_GLOSSY | BF200_LOBE_TRANSMISSION, BF200_LOBE_TRANSMISSION);
-    } else {
-        consider(c.lobes, c.lobes & (BF200_LOBE_REFLECTION | BF200_LOBE_TRANSMISSION));
+        if (allowed == 0U) {
+            continue;
+        }
+        m.source[m.count] = i;
+        m.allowed[m.count] = allowed;
+        m.p[m.count] = material.probability[i];
+        ++m.count;
     }
-    f.active = f.allowed != 0U;
-    return f;
+    if (m.count == 0U) {
+        return m;
+    }
+    if (m.count == material.closure_count) {
+        for (uint32_t i = 0; i < m.count; ++i) {
+            m.p[i] = material.probability[i];
+        }
+        for (uint32_t i = 0; i <= m.count; ++i) {
+            m.cdf[i] = material.cdf[i];
+        }
+        return m;
+    }
+    if (m.count == 1U) {
+        m.p[0] = 1.0F;
+        m.cdf[0] = 0.0F;
+        m.cdf[1] = 1.0F;
+        return m;
+    }
+    const float total = compensated_sum(m.p, m.count);
+    if (!std::isfinite(total) || !(total > 0.0F)) {
+        fail("Active depth-filtered closure probabilities have no representable mass.");
+    }
+    float normalized[kMaxClosures] = {};
+    for (uint32_t i = 0; i < m.count; ++i) {
+        normalized[i] = m.p[i] / total;
+    }
+    const char* error = nullptr;
+    if (!component_distribution(normalized, m.count, false, m.p, m.cdf, &error)) {
+        fail(error);
+    }
+    return m;
 }
 
-Spectrum closure_eval(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
+// eval / pdf / sample of one closure record, the rough dielectric restricted to `allowed`
+// (DepthFilteredClosureMixture.hpp:182-252, ClosureMixture.hpp:527-748)
+Spectrum record_eval(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
     switch (c.kind) {
     case BF200_CLOSURE_LAMBERTIAN_REFLECTION: {  // LambertianReflection.hpp:76-85
         if (!unit_length(wo) || !unit_length(wi)) {
@@ -2041,56 +2724,60 @@ Spectrum closure_eval(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
         return Spectrum{c.weight[0] * kInvPi, c.weight[1] * kInvPi, c.weight[2] * kInvPi,
                         c.weight[3] * kInvPi};
     }
+    case BF200_CLOSURE_ROUGH_DIFFUSE_REFLECTION:
+        return eon_eval(c, wo, wi);
     case BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION:
         return conductor_eval(c, wo, wi);
     case BF200_CLOSURE_ROUGH_DIELECTRIC:
         return dielectric_eval_masked(c, allowed, wo, wi);
+    case BF200_CLOSURE_SPECULAR_REFLECTION:
+    case BF200_CLOSURE_SPECULAR_TRANSMISSION:
+        if (!unit_length(wo) || !unit_length(wi)) {
+            fail("Specular delta directions must be finite unit vectors.");
+        }
+        return Spectrum{};
     default:
         fail("unsupported closure");
     }
 }
 
-float closure_pdf(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
+float record_pdf(const Closure& c, uint32_t allowed, V3 wo, V3 wi) {
     switch (c.kind) {
-    case BF200_CLOSURE_LAMBERTIAN_REFLECTION: {  // LambertianReflection.hpp:87-106
-        if (!unit_length(wo) || !unit_length(wi)) {
-            fail("Lambertian directions must be finite unit vectors.");
-        }
-        if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
-            return 0.0F;
-        }
-        const float v = wi.z * kInvPi;
-        if (!(v > 0.0F) || !std::isfinite(v)) {
-            fail("Lambertian PDF is not representable for the supplied direction.");
-        }
-        return v;
-    }
+    case BF200_CLOSURE_LAMBERTIAN_REFLECTION:  // LambertianReflection.hpp:87-106
+        return cosine_pdf(wo, wi, "Lambertian directions must be finite unit vectors.");
+    case BF200_CLOSURE_ROUGH_DIFFUSE_REFLECTION:
+        return cosine_pdf(wo, wi, "Rough-diffuse directions must be finite unit vectors.");
     case BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION:
         return conductor_pdf(c, wo, wi);
     case BF200_CLOSURE_ROUGH_DIELECTRIC:
         return dielectric_pdf_masked(c, allowed, wo, wi);
+    case BF200_CLOSURE_SPECULAR_REFLECTION:
+    case BF200_CLOSURE_SPECULAR_TRANSMISSION:
+        if (!unit_length(wo) || !unit_length(wi)) {
+            fail("Specular delta directions must be finite unit vectors.");
+        }
+        return 0.0F;
     default:
         fail("unsupported closure");
     }
 }
 
-// DepthFilteredClosureMixture.hpp:460-552 for one active closure: the event sample is the
-// component sample itself; dielectric directions restricted by the depth filter are forced.
-BsdfSample closure_sample(const Closure& c, uint32_t allowed, V3 wo, float component, float u,
-                          float v) {
-    if (!unit_length(wo)) {
-        fail("Closure sampling requires a finite unit direction.");
-    }
+BsdfSample record_sample(const Closure& c, uint32_t allowed, V3 wo, float event, float u, float v) {
     switch (c.kind) {
-    case BF200_CLOSURE_LAMBERTIAN_REFLECTION: {  // LambertianReflection.hpp:108-140
+    case BF200_CLOSURE_LAMBERTIAN_REFLECTION:  // LambertianReflection.hpp:108-140
+    case BF200_CLOSURE_ROUGH_DIFFUSE_REFLECTION: {  // RoughDiffuseReflection.hpp:235-266
+        if (!unit_length(wo)) {
+            fail(c.kind == BF200_CLOSURE_LAMBERTIAN_REFLECTION ? "Lambertian directions must be finite unit vectors."
+                                                                : "Rough-diffuse directions must be finite unit vectors.");
+        }
         BsdfSample s;
         const V3 wi = map_cosine_hemisphere(u, v);
         if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
             return s;
         }
         s.wi = wi;
-        s.value = closure_eval(c, allowed, wo, wi);
-        s.pdf = closure_pdf(c, allowed, wo, wi);
+        s.value = record_eval(c, allowed, wo, wi);
+        s.pdf = record_pdf(c, allowed, wo, wi);
         s.lobes = c.lobes;
         s.valid = true;
         return s;
@@ -2098,13 +2785,13 @@ BsdfSample closure_sample(const Closure& c, uint32_t allowed, V3 wo, float compo
     case BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION:
         return conductor_sample(c, wo, u, v);
     case BF200_CLOSURE_ROUGH_DIELECTRIC: {  // DepthFilteredClosureMixture.hpp:135-180
-        float event = component;
+        float e = event;
         if (allowed == BF200_LOBE_REFLECTION) {
-            event = 0.0F;
+            e = 0.0F;
         } else if (allowed == BF200_LOBE_TRANSMISSION) {
-            event = std::nextafter(1.0F, 0.0F);
+            e = std::nextafter(1.0F, 0.0F);
         }
-        BsdfSample s = dielectric_sample(c, wo, event, u, v);
+        BsdfSample s = dielectric_sample(c, wo, e, u, v);
         if (!s.valid) {
             return s;
         }
@@ -2114,9 +2801,127 @@ BsdfSample closure_sample(const Closure& c, uint32_t allowed, V3 wo, float compo
         s.pdf = dielectric_pdf_masked(c, allowed, wo, s.wi);
         return s;
     }
+    case BF200_CLOSURE_SPECULAR_REFLECTION:
+        return specular_reflection_sample(c, wo);
+    case BF200_CLOSURE_SPECULAR_TRANSMISSION:
+        return specular_transmission_sample(c, wo);
     default:
         fail("unsupported closure");
     }
+}
+
+void require_unit_queries(V3 wo, V3 wi) {
+    if (!unit_length(wo) || !unit_length(wi)) {
+        fail("Depth-filtered closure queries require finite unit directions and a supported transport mode.");
+    }
+}
+
+Spectrum mixture_eval(const Mixture& m, V3 wo, V3 wi) {
+    require_unit_queries(wo, wi);
+    Spectrum result{};
+    for (uint32_t i = 0; i < m.count; ++i) {
+        const Spectrum component = record_eval(m.closure(i), m.allowed[i], wo, wi);
+        for (int lane = 0; lane < 4; ++lane) {
+            const float sum = result[lane] + component[lane];
+            if (!std::isfinite(sum)) {
+                fail("A depth-filtered closure value is not representable.");
+            }
+            result[lane] = sum;
+        }
+    }
+    return result;
+}
+
+float mixture_pdf(const Mixture& m, V3 wo, V3 wi) {
+    require_unit_queries(wo, wi);
+    if (m.count == 0U) {
+        return 0.0F;
+    }
+    float conditional[kMaxClosures] = {};
+    for (uint32_t i = 0; i < m.count; ++i) {
+        conditional[i] = record_pdf(m.closure(i), m.allowed[i], wo, wi);
+    }
+    return mix_densities(m.p, conditional, m.count);
+}
+
+// aggregate_delta_atom (ClosureMixture.hpp:760-870): the discrete mass and value of every active
+// delta closure whose deterministic direction is exactly `wi`.
+void aggregate_delta_atom(const Mixture& m, V3 wo, V3 wi, Spectrum& value, float& probability) {
+    float value_sum[4] = {}, value_correction[4] = {};
+    float p_sum = 0.0F, p_correction = 0.0F;
+    uint32_t matching = 0;
+    for (uint32_t i = 0; i < m.count; ++i) {
+        const Closure& c = m.closure(i);
+        if (!is_delta_kind(c.kind)) {
+            continue;
+        }
+        const BsdfSample candidate = record_sample(c, BF200_LOBE_REFLECTION | BF200_LOBE_TRANSMISSION, wo, 0.0F, 0.0F, 0.0F);
+        if (!candidate.valid || candidate.wi.x != wi.x || candidate.wi.y != wi.y || candidate.wi.z != wi.z) {
+            continue;
+        }
+        if (!candidate.delta || !std::isfinite(candidate.pdf) || !(candidate.pdf > 0.0F) || candidate.pdf > 1.0F) {
+            fail("A sampled delta closure requires a finite positive discrete probability.");
+        }
+        for (int lane = 0; lane < 4; ++lane) {
+            if (!add_compensated(candidate.value[lane], value_sum[lane], value_correction[lane])) {
+                fail("A coincident delta value is not representable in the requested precision.");
+            }
+        }
+        if (!add_compensated(positive_probability_product(m.p[i], candidate.pdf), p_sum, p_correction)) {
+            fail("A coincident delta probability is not representable in the requested precision.");
+        }
+        ++matching;
+    }
+    probability = p_sum + p_correction;
+    if (matching == 0U || !std::isfinite(probability) || !(probability > 0.0F) || probability > 1.0F) {
+        fail("The sampled delta atom is absent from the closure mixture.");
+    }
+    for (int lane = 0; lane < 4; ++lane) {
+        value[lane] = value_sum[lane] + value_correction[lane];
+        if (!std::isfinite(value[lane]) || value[lane] < 0.0F) {
+            fail("A coincident delta value is not representable in the requested precision.");
+        }
+    }
+}
+
+// DepthFilteredClosureMixture::sample (DepthFilteredClosureMixture.hpp:460-552)
+BsdfSample mixture_sample(const Mixture& m, V3 wo, float component, float u, float v) {
+    if (!unit_length(wo) || !(component >= 0.0F && component < 1.0F) || !(u >= 0.0F && u < 1.0F) ||
+        !(v >= 0.0F && v < 1.0F)) {
+        fail("Depth-filtered closure sampling requires canonical samples, a finite unit direction, and a supported "
+             "transport mode.");
+    }
+    if (m.count == 0U) {
+        return BsdfSample{};
+    }
+    uint32_t selected = m.count;
+    for (uint32_t i = 0; i < m.count; ++i) {
+        if (component < m.cdf[i + 1]) {
+            selected = i;
+            break;
+        }
+    }
+    if (selected == m.count) {
+        fail("The depth-filtered closure CDF did not select a component.");
+    }
+    const float event = (component - m.cdf[selected]) / m.p[selected];
+    if (!std::isfinite(event) || event < 0.0F || !(event < 1.0F)) {
+        fail("The depth-filtered closure sample cannot be remapped to [0, 1).");
+    }
+    BsdfSample s = record_sample(m.closure(selected), m.allowed[selected], wo, event, u, v);
+    if (!s.valid) {
+        return s;
+    }
+    if (m.count > 1U) {
+        if (!s.delta) {
+            s.value = mixture_eval(m, wo, s.wi);
+            s.pdf = mixture_pdf(m, wo, s.wi);
+        } else {
+            aggregate_delta_atom(m, wo, s.wi, s.value, s.pdf);
+        }
+    }
+    s.selected = m.source[selected];
+    return s;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2451,8 +3256,14 @@ void validate_tree_support(const Scene& scene, V3 position) {
     if (!scene.use_tree) {
         return;
     }
+    for (uint32_t i = 0; i < scene.punctual.size(); ++i) {
+        if (!is_black(scene.punctual[i].spectrum) && !(light_probability(scene, i, position) > 0.0F)) {
+            fail("The light sampler gives zero support to a non-black punctual light.");
+        }
+    }
     for (uint32_t i = 0; i < scene.lights.size(); ++i) {
-        if (!(light_probability(scene, i, position) > 0.0F)) {
+        const uint32_t slot = static_cast<uint32_t>(scene.punctual.size()) + i;
+        if (!(light_probability(scene, slot, position) > 0.0F)) {
             fail("The light sampler gives zero support to a non-black mesh area light.");
         }
     }
@@ -2657,23 +3468,36 @@ bool cone_scatter(float width, float spread, uint32_t kind, const float* p, uint
     return cone_valid(out_width, out_spread);
 }
 
-// SceneMisPathLoop.cpp:129-275 (estimate): returns the unoccluded-tested direct contribution.
-Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& surf,
-                         const Closure& closure, uint32_t allowed, const Spectrum& beta, V3 wo_world,
-                         const Dims& dims, const Stream& stream, uint32_t mask, float time) {
+// SceneMisPathLoop.cpp:136-275 (estimate): the direct contribution of one light sample, its
+// shadow ray traced.
+Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& surf, const Mixture& mix,
+                         const Spectrum& beta, V3 wo_world, const Dims& dims, const Stream& stream, uint32_t mask,
+                         float time) {
     const Spectrum zero{};
-    if (is_black(beta) || is_black(closure.weight)) {
+    if (is_black(beta)) {
+        return zero;
+    }
+    bool all_black = true;
+    for (uint32_t i = 0; i < mix.count; ++i) {
+        all_black = all_black && is_black(mix.closure(i).weight);
+    }
+    if (all_black) {
         return zero;
     }
     float selection;
     validate_tree_support(scene, surf.position);
     const uint32_t light_index = select_light(scene, stream.sample_1d(dims.light_selection), selection, surf.position);
-    const MeshLight& light = scene.lights[light_index];
-    if ((scene.instances[light.instance].mask & mask) == 0U) {
-        return zero;
+    const float lu = stream.sample_1d(dims.light_u), lv = stream.sample_1d(dims.light_v);
+    LightSample ls;
+    if (light_index < scene.punctual.size()) {
+        ls = sample_punctual_light(scene.punctual[light_index], surf.position, lu, lv);
+    } else {
+        const MeshLight& light = scene.lights[light_index - scene.punctual.size()];
+        if ((scene.instances[light.instance].mask & mask) == 0U) {
+            return zero;
+        }
+        ls = sample_mesh_light(light, surf.position, lu, lv);
     }
-    const LightSample ls = sample_mesh_light(light, surf.position, stream.sample_1d(dims.light_u),
-                                             stream.sample_1d(dims.light_v));
     if (!ls.valid) {
         return zero;
     }
@@ -2682,10 +3506,10 @@ Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& 
     if (wo.z == 0.0F || wi.z == 0.0F) {
         return zero;
     }
-    const bool lambert = closure.kind == BF200_CLOSURE_LAMBERTIAN_REFLECTION;
+    const bool lambert = mix.count == 1U && mix.closure(0).kind == BF200_CLOSURE_LAMBERTIAN_REFLECTION;
     Spectrum f{};
     if (!lambert) {
-        f = closure_eval(closure, allowed, wo, wi);
+        f = mixture_eval(mix, wo, wi);
         if (is_black(f)) {
             return zero;
         }
@@ -2694,24 +3518,39 @@ Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& 
     if (correction == 0.0F) {
         return zero;
     }
-    const float bsdf_pdf = closure_pdf(closure, allowed, wo, wi);
-    const float light_pdf = joint_light_pdf(selection, ls.pdf);
-    const float weight = mis_weight(opt.heuristic, light_pdf, bsdf_pdf);
-    // make_shadow_ray (ShadowRay.hpp:181-253) for a finite surface endpoint.
+    float weight = 1.0F;
+    if (!ls.discrete) {
+        const float bsdf_pdf = mixture_pdf(mix, wo, wi);
+        const float light_pdf = joint_light_pdf(selection, ls.pdf);
+        weight = mis_weight(opt.heuristic, light_pdf, bsdf_pdf);
+    }
+    // make_shadow_ray (ShadowRay.hpp:181-253)
     const V3 origin = offset_surface_point(surf.position, surf.error, surf.ng, ls.direction);
-    const V3 endpoint = offset_surface_point(ls.position, ls.error, ls.normal, origin - ls.position);
-    V3 sd;
-    float length;
-    unit_segment(origin, endpoint, ls.direction, sd, length);
-    const float t_max = std::nextafter(length, 0.0F);
-    if (!(t_max > 0.0F) || !std::isfinite(t_max)) {
-        fail("A finite shadow-ray interval is not representable in the requested precision.");
+    V3 sd = ls.direction;
+    float t_max = kInfinity;
+    if (!ls.infinite) {
+        V3 endpoint;
+        if (ls.point) {
+            V3 nominal;
+            float nominal_length;
+            unit_segment(origin, ls.position, ls.direction, nominal, nominal_length);
+            endpoint = contract_point_endpoint(ls.position, ls.error, nominal);
+        } else {
+            endpoint = offset_surface_point(ls.position, ls.error, ls.normal, origin - ls.position);
+        }
+        float length;
+        unit_segment(origin, endpoint, ls.direction, sd, length);
+        t_max = std::nextafter(length, 0.0F);
+        if (!(t_max > 0.0F) || !std::isfinite(t_max)) {
+            fail("A finite shadow-ray interval is not representable in the requested precision.");
+        }
     }
     (void)time;
     const bool blocked = occluded(scene, origin, sd, 0.0F, t_max, mask);
     const float transmittance = blocked ? 0.0F : 1.0F;
     Spectrum out{};
     for (int lane = 0; lane < 4; ++lane) {
+        const Closure& closure = mix.closure(0);
         if (lambert) {
             // evaluate_lambertian_direct_lighting (DirectLighting.hpp:171-236)
             if (!(wo.z > 0.0F) || !(wi.z > 0.0F)) {
@@ -2825,7 +3664,8 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
             if (light_index < 0) {
                 fail("A non-black emissive hit is absent from the committed mesh-light registry.");
             }
-            const float selection = light_probability(scene, static_cast<uint32_t>(light_index), prev.position);
+            const uint32_t slot = static_cast<uint32_t>(scene.punctual.size()) + static_cast<uint32_t>(light_index);
+            const float selection = light_probability(scene, slot, prev.position);
             const float conditional = mesh_light_pdf_at_surface(scene.lights[light_index], prev.position,
                                                                 surf.position, surf.ng);
             const float light_pdf = joint_light_pdf(selection, conditional);
@@ -2835,16 +3675,12 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
         if (is_black(out.beta)) {
             return finish(BF200_TERMINATION_ZERO_THROUGHPUT);
         }
-        if (material.closure_count != 1) {
-            if (material.closure_count == 0) {
+        const Mixture mix = depth_filter(material, opt.limits, out.depth);
+        if (mix.count == 0U) {
+            if (material.closure_count == 0U) {
                 return finish(BF200_TERMINATION_OUTSIDE_BSDF_SUPPORT);
             }
-            fail("multi-closure mixtures are not part of this restatement");
-        }
-        const Closure& closure = material.closure;
-        const Filtered filtered = depth_filter(closure, opt.limits, out.depth);
-        if (!filtered.active) {
-            out.blocked = filtered.blocked;
+            out.blocked = mix.blocked;
             return finish(BF200_TERMINATION_DEPTH_LIMIT);
         }
         const V3 wo_world = robust_unit(-rd);
@@ -2853,10 +3689,15 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
         const float bu = stream.sample_1d(dims.bsdf_u);
         const float bv = stream.sample_1d(dims.bsdf_v);
         const float bc = stream.sample_1d(dims.bsdf_component);
-        const BsdfSample bs = closure_sample(closure, filtered.allowed, wo, bc, bu, bv);
+        const BsdfSample bs = mixture_sample(mix, wo, bc, bu, bv);
         Depth next_depth = out.depth;
         if (bs.valid) {
-            if (!std::isfinite(bs.pdf) || !(bs.pdf > 0.0F) || bs.wi.z == 0.0F) {
+            bool finite_value = true;
+            for (int lane = 0; lane < 4; ++lane) {
+                finite_value = finite_value && std::isfinite(bs.value[lane]) && bs.value[lane] >= 0.0F;
+            }
+            if (!valid_surface_event(bs.lobes) || !finite_value || !std::isfinite(bs.pdf) || !(bs.pdf > 0.0F) ||
+                bs.wi.z == 0.0F) {
                 fail("The closure mixture returned an invalid MIS continuation sample.");
             }
             if (blocked_limits(opt.limits, out.depth, bs.lobes) != 0U) {
@@ -2864,8 +3705,7 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
             }
             next_depth = advanced(out.depth, bs.lobes);
         }
-        const Spectrum direct = direct_lighting(scene, opt, surf, closure, filtered.allowed, out.beta,
-                                                wo_world, dims, stream, mask, time);
+        const Spectrum direct = direct_lighting(scene, opt, surf, mix, out.beta, wo_world, dims, stream, mask, time);
         for (int lane = 0; lane < 4; ++lane) {
             if (!std::isfinite(direct[lane]) || direct[lane] < 0.0F) {
                 fail("A direct-lighting contribution must be finite and non-negative.");
@@ -2881,9 +3721,17 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
             return finish(BF200_TERMINATION_OUTSIDE_BSDF_SUPPORT);
         }
         // update_closure_throughput (BsdfOnlyPathLoop.hpp:64-131)
+        const bool delta = (bs.lobes & BF200_LOBE_SPECULAR) != 0U;
+        if (bs.delta != delta || (delta && bs.pdf > 1.0F)) {
+            fail("A closure sample uses an incompatible probability measure.");
+        }
         Spectrum next_beta{};
         const float cosine = std::abs(bs.wi.z);
-        if (closure.kind == BF200_CLOSURE_LAMBERTIAN_REFLECTION && correction == 1.0F) {
+        if (!std::isfinite(cosine) || !(cosine > 0.0F)) {
+            fail("A closure direction has no representable projected measure.");
+        }
+        if (mix.count == 1U && mix.closure(0).kind == BF200_CLOSURE_LAMBERTIAN_REFLECTION && correction == 1.0F) {
+            const Closure& closure = mix.closure(0);
             for (int lane = 0; lane < 4; ++lane) {
                 next_beta[lane] = out.beta[lane] * closure.weight[lane];
                 if (!std::isfinite(next_beta[lane]) ||
@@ -2934,21 +3782,25 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
         }
         if (cone != nullptr) {
             float advanced = 0.0F;
+            const Closure& closure = material.closures[bs.selected];
             if (!cone_advance(out.cone_width, out.cone_spread, rd, hit.t, advanced) ||
                 !cone_scatter(advanced, out.cone_spread, closure.kind, closure.p, bs.lobes, wo, bs.wi,
                               out.cone_width, out.cone_spread)) {
                 fail("A scattered ray cone is not representable.");
             }
         }
-        // record_bsdf_sample (SceneMisPathLoop.cpp:358-390): continuous lobes only here.
-        prev.valid = true;
+        // record_bsdf_sample (SceneMisPathLoop.cpp:358-390): a delta continuation leaves no density
+        // for the next emissive hit's MIS weight
+        prev.valid = !delta;
         prev.position = surf.position;
         prev.pdf = bs.pdf;
         prev.direction = wi_world;
         out.beta = next_beta;
         out.depth = next_depth;
         out.eta_scale = next_eta;
-        out.delta_flags = 2U;  // any_non_delta_bounces (continuous lobes only)
+        // next_delta_flags (SceneMisPathLoop.cpp:39-52): previous_bounce_was_delta 1,
+        // any_non_delta_bounces 2
+        out.delta_flags = (out.delta_flags & 2U) | (delta ? 1U : 2U);
         ro = origin;
         rd = wi_world;
         tmin = 0.0F;
@@ -3045,14 +3897,27 @@ __attribute__((visibility("default"))) int bfo_scene_create(const bf200_scene_de
             for (int lane = 0; lane < 4; ++lane) {
                 mat.emission[lane] = src.emitted_radiance[lane];
             }
-            if (src.closure_count >= 1) {
-                const auto& c = d->closures[src.closure_offset];
-                mat.closure.kind = c.kind;
-                mat.closure.lobes = c.lobes;
+            if (src.closure_count > kMaxClosures) {
+                set_error("A closure mixture contains an invalid active closure count.");
+                delete s;
+                return 6;
+            }
+            for (uint32_t k = 0; k < src.closure_count; ++k) {
+                const auto& c = d->closures[src.closure_offset + k];
+                Closure& dst = mat.closures[k];
+                dst.kind = c.kind;
+                dst.lobes = c.lobes;
                 for (int lane = 0; lane < 4; ++lane) {
-                    mat.closure.weight[lane] = c.weight[lane];
+                    dst.weight[lane] = c.weight[lane];
                 }
-                std::memcpy(mat.closure.p, c.parameters, sizeof(mat.closure.p));
+                std::memcpy(dst.p, c.parameters, sizeof(dst.p));
+            }
+            const char* error = nullptr;
+            if (!component_distribution(src.component_probabilities, src.closure_count, true, mat.probability,
+                                        mat.cdf, &error)) {
+                set_error(error);
+                delete s;
+                return 6;
             }
             s->materials.push_back(mat);
         }
@@ -3082,6 +3947,77 @@ __attribute__((visibility("default"))) int bfo_scene_create(const bf200_scene_de
                 inst.world_normals.push_back(n);
             }
             s->instances.push_back(std::move(inst));
+        }
+        // Punctual lights, first in the registry (PunctualLights.hpp create checks).
+        const uint32_t punctual_count =
+            d->struct_size >= sizeof(bf200_scene_desc_v1) && d->punctual_lights != nullptr ? d->punctual_light_count : 0U;
+        if (punctual_count != d->punctual_light_count) {
+            set_error("punctual lights require the full scene description layout");
+            delete s;
+            return 7;
+        }
+        for (uint32_t k = 0; k < punctual_count; ++k) {
+            const auto& src = d->punctual_lights[k];
+            Punctual light{};
+            light.kind = src.kind;
+            light.position = load3(src.position, 0);
+            light.error = load3(src.position_error, 0);
+            light.direction = load3(src.direction, 0);
+            for (int lane = 0; lane < 4; ++lane) {
+                light.spectrum[lane] = src.spectrum[lane];
+                if (!std::isfinite(light.spectrum[lane]) || light.spectrum[lane] < 0.0F) {
+                    set_error("A punctual light spectrum must be finite and non-negative.");
+                    delete s;
+                    return 7;
+                }
+            }
+            const bool finite_point = std::isfinite(light.position.x) && std::isfinite(light.position.y) &&
+                                      std::isfinite(light.position.z) && std::isfinite(light.error.x) &&
+                                      std::isfinite(light.error.y) && std::isfinite(light.error.z) &&
+                                      light.error.x >= 0.0F && light.error.y >= 0.0F && light.error.z >= 0.0F;
+            if (src.kind == BF200_PUNCTUAL_POINT) {
+                if (!finite_point) {
+                    set_error("A finite punctual light requires a finite position and non-negative error.");
+                    delete s;
+                    return 7;
+                }
+            } else if (src.kind == BF200_PUNCTUAL_DIRECTIONAL) {
+                if (!unit_length(light.direction)) {
+                    set_error("A directional light requires a finite unit propagation direction.");
+                    delete s;
+                    return 7;
+                }
+            } else if (src.kind == BF200_PUNCTUAL_SPOT) {
+                const float inner = src.inner_half_angle, outer = src.outer_half_angle;
+                if (!finite_point || !unit_length(light.direction) || !std::isfinite(inner) || !std::isfinite(outer) ||
+                    inner < 0.0F || inner > outer || !(outer > 0.0F) || outer >= kPi) {
+                    set_error("Spot half angles require 0 <= inner <= outer < pi and a positive outer cone.");
+                    delete s;
+                    return 7;
+                }
+                // exact_special_cosine (PunctualLights.hpp:186-197)
+                auto special_cosine = [](float angle) {
+                    if (angle == 0.0F) return 1.0F;
+                    if (angle == kPi / 2.0F) return 0.0F;
+                    if (angle == kPi) return -1.0F;
+                    return std::cos(angle);
+                };
+                light.cos_inner = special_cosine(inner);
+                light.cos_outer = special_cosine(outer);
+                light.hard = inner == outer;
+                if (!std::isfinite(light.cos_inner) || !std::isfinite(light.cos_outer) || light.cos_outer == 1.0F ||
+                    light.cos_outer == -1.0F || (inner > 0.0F && light.cos_inner == 1.0F) ||
+                    light.cos_inner < light.cos_outer || (inner < outer && light.cos_inner == light.cos_outer)) {
+                    set_error("Spot cone cosines are not distinguishable in the requested precision.");
+                    delete s;
+                    return 7;
+                }
+            } else {
+                set_error("unknown punctual light kind");
+                delete s;
+                return 7;
+            }
+            s->punctual.push_back(light);
         }
         // Mesh-light registry (FrameScene.cpp:201-261): one light per emissive instance.
         s->light_of_instance.assign(d->instance_count, -1);
@@ -3114,10 +4050,11 @@ __attribute__((visibility("default"))) int bfo_scene_create(const bf200_scene_de
             s->light_of_instance[i] = static_cast<int32_t>(s->lights.size());
             s->lights.push_back(std::move(light));
         }
-        // LightSampler::create_uniform (LightSampler.cpp:574-602).
-        const size_t count = s->lights.size();
+        // LightSampler::create_uniform (LightSampler.cpp:574-602) over the registry: punctual
+        // lights, then mesh lights.
+        const size_t count = s->punctual.size() + s->lights.size();
         if (count == 0) {
-            set_error("MIS requires at least one emissive mesh light.");
+            set_error("MIS requires at least one punctual or emissive mesh light in the committed scene.");
             delete s;
             return 5;
         }
@@ -3377,7 +4314,7 @@ __attribute__((visibility("default"))) int bfo_scene_set_light_tree(void* handle
                                                                     const bf200_light_tree_input_v1* lights,
                                                                     uint32_t count) {
     auto* s = static_cast<Scene*>(handle);
-    if (count != s->lights.size()) {
+    if (count != s->punctual.size() + s->lights.size()) {
         set_error("one light-tree input per scene light is required");
         return 1;
     }
@@ -3393,7 +4330,7 @@ __attribute__((visibility("default"))) int bfo_scene_set_light_tree(void* handle
 __attribute__((visibility("default"))) int bfo_scene_set_light_powers(void* handle, const float* powers,
                                                                       uint32_t count) {
     auto* s = static_cast<Scene*>(handle);
-    if (count == 0 || count != s->lights.size()) {
+    if (count == 0 || count != s->punctual.size() + s->lights.size()) {
         set_error("one spectral power per scene light is required");
         return 1;
     }

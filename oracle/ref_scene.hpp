@@ -62,6 +62,15 @@ inline core::Result<engine::SceneClosureMixture> make_mixture(const bf200_materi
                                                  record.parameters[1], record.parameters[2],
                                                  record.parameters[3]);
             break;
+        case BF200_CLOSURE_ROUGH_DIFFUSE_REFLECTION:
+            status = set.append_rough_diffuse_reflection(weight, record.parameters[0]);
+            break;
+        case BF200_CLOSURE_SPECULAR_REFLECTION:
+            status = set.append_specular_reflection(weight);
+            break;
+        case BF200_CLOSURE_SPECULAR_TRANSMISSION:
+            status = set.append_specular_transmission(weight, record.parameters[0], record.parameters[1]);
+            break;
         default:
             break;
         }
@@ -196,6 +205,30 @@ inline engine::FrameSceneHandle make_frame_scene(const bf200_scene_desc_v1* desc
             .local_to_parent = matrix,
             .visibility_mask = instance.visibility_mask,
         });
+    }
+    const uint32_t punctual_count =
+        desc->struct_size >= sizeof(bf200_scene_desc_v1) && desc->punctual_lights != nullptr ? desc->punctual_light_count : 0U;
+    for (uint32_t k = 0; k < punctual_count; ++k) {
+        const auto& light = desc->punctual_lights[k];
+        const auto position = renderer::Point3{.x = light.position[0], .y = light.position[1], .z = light.position[2]};
+        const auto error =
+            renderer::Vector3{.x = light.position_error[0], .y = light.position_error[1], .z = light.position_error[2]};
+        const auto direction = renderer::Vector3{.x = light.direction[0], .y = light.direction[1], .z = light.direction[2]};
+        if (light.kind == BF200_PUNCTUAL_POINT) {
+            description.punctual_lights.emplace_back(engine::ScenePointLight{
+                .position = position, .absolute_position_error = error, .spectral_radiant_intensity = spectrum4(light.spectrum)});
+        } else if (light.kind == BF200_PUNCTUAL_DIRECTIONAL) {
+            description.punctual_lights.emplace_back(engine::SceneDirectionalLight{
+                .propagation_direction = direction, .spectral_irradiance = spectrum4(light.spectrum)});
+        } else {
+            description.punctual_lights.emplace_back(engine::SceneSpotLight{
+                .position = position,
+                .absolute_position_error = error,
+                .emission_direction = direction,
+                .inner_half_angle_radians = light.inner_half_angle,
+                .outer_half_angle_radians = light.outer_half_angle,
+                .on_axis_spectral_radiant_intensity = spectrum4(light.spectrum)});
+        }
     }
     description.spectral_environment = engine::SceneSpectralEnvironment{
         .wavelengths = wavelengths,
