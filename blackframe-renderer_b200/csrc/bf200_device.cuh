@@ -48,6 +48,18 @@ struct LightInfo {
     float radiance[4];
 };
 
+// A punctual light of the registry (slots [0, punctual_count)), with the cone cosines a spot light
+// samples with (PunctualLights.hpp:593-815).
+struct PunctualLight {
+    uint32_t kind;  // BF200_PUNCTUAL_*
+    uint32_t hard;  // spot: inner == outer
+    float px, py, pz;
+    float ex, ey, ez;
+    float dx, dy, dz;
+    float cos_inner, cos_outer;
+    float spectrum[4];
+};
+
 // Everything a kernel needs about a committed scene; passed by value as a kernel parameter.
 struct SceneView {
     uint32_t instance_count;
@@ -66,11 +78,15 @@ struct SceneView {
     const BvhNode4* nodes;
     const float4* leaf_tris;       // 3 per leaf triangle: v0 (w = primitive index bits), v1, v2
     const float4* world_normals;   // per instance triangle
-    const ClosureData* closures;   // one per material
+    const ClosureData* closures;   // per material: its first closure (the single-closure routes)
+    const ClosureData* mix_closures;       // every material's closures, material_info.w the first
+    const MixDistribution* mix_dist;       // per material: projected component distribution
+    const PunctualLight* punctual;         // registry slots [0, punctual_count)
+    uint32_t punctual_count;
     const float4* emission;        // per material
-    const uint4* material_info;    // closure count, frame mode, rotation bits, -
-    const float* light_select_cdf; // light_count + 1 uniform boundaries
-    const LightInfo* lights;
+    const uint4* material_info;    // closure count, frame mode, rotation bits, first closure
+    const float* light_select_cdf; // light_count + 1 boundaries over the registry (punctual, then mesh)
+    const LightInfo* lights;       // mesh lights: registry slot punctual_count + index
     const float4* light_tri_vertices;  // 3 per light triangle, world space
     const float4* light_tri_normals;
     const float* light_tri_areas;

@@ -82,6 +82,8 @@ struct bf200_scene {
     uint32_t instance_triangles = 0;
     uint32_t* normal_failures = nullptr;     // device counter of k_world_normals
     size_t light_triangles = 0;
+    uint32_t punctual_count = 0;        // light registry slots [0, punctual_count) are punctual
+    bool plain_materials = true;        // no mixtures and only Lambert / GGX conductor / dielectric
     // the spatial light tree (bf200_scene_set_light_tree): device node array and light-to-node map,
     // owned here (not in `allocations`) so a new tree reuses them and a cleared tree frees them
     void* tree_nodes = nullptr;
@@ -726,6 +728,9 @@ uint64_t description_fingerprint(const bf200_scene_desc_v1& d) {
     if (d.closures != nullptr) {
         mix(d.closures, sizeof(bf200_closure_v1) * d.closure_count);
     }
+    if (d.struct_size >= sizeof(bf200_scene_desc_v1) && d.punctual_lights != nullptr) {
+        mix(d.punctual_lights, sizeof(bf200_punctual_light_v1) * d.punctual_light_count);
+    }
     for (uint32_t i = 0; i < d.instance_count; ++i) {
         const bf200_instance_v1& inst = d.instances[i];
         const uint32_t fields[5] = {inst.instance_id, inst.object_id, inst.geometry_index, inst.material_index,
@@ -796,18 +801,197 @@ bool valid_closure_payload(const bf200_closure_v1& c) {
         return c.lobes == (BF200_LOBE_GLOSSY | BF200_LOBE_REFLECTION | BF200_LOBE_TRANSMISSION) &&
                std::isfinite(p[0]) && p[0] > 0.0F && std::isfinite(p[1]) && p[1] > 0.0F && p[0] != p[1] &&
                representable_alpha_pair(p[2], p[3]);
+    case BF200_CLOSURE_ROUGH_DIFFUSE_REFLECTION:  // append_rough_diffuse_reflection: roughness in [0, 1]
+        for (int i = 1; i < 10; ++i) {
+            if (p[i] != 0.0F) {
+                return false;
+            }
+        }
+        return c.lobes == (BF200_LOBE_DIFFUSE | BF200_LOBE_REFLECTION) && std::isfinite(p[0]) && p[0] >= 0.0F &&
+               p[0] <= 1.0F;
+    case BF200_CLOSURE_SPECULAR_REFLECTION:
+        for (int i = 0; i < 10; ++i) {
+            if (p[i] != 0.0F) {
+                return false;
+            }
+        }
+        return c.lobes == (BF200_LOBE_SPECULAR | BF200_LOBE_REFLECTION);
+    case BF200_CLOSURE_SPECULAR_TRANSMISSION:  // append_specular_transmission: finite positive indices
+        for (int i = 2; i < 10; ++i) {
+            if (p[i] != 0.0F) {
+                return false;
+            }
+        }
+        return c.lobes == (BF200_LOBE_SPECULAR | BF200_LOBE_TRANSMISSION) && std::isfinite(p[0]) && p[0] > 0.0F &&
+               std::isfinite(p[1]) && p[1] > 0.0F;
     default:
         return false;
     }
 }
 
+// build_component_distribution (ClosureMixture.hpp:122-234): the component probabilities of a
+// closure mixture projected onto the 2^-24 sampler grid (largest remainders first) and their CDF.
+// False when the probabilities do not form a distribution at that precision.
+bool project_component_distribution(const float* probabilities, uint32_t n, float* out_p, float* out_cdf) {
+    for (uint32_t i = 0; i <= bf200::kMaxClosures; ++i) {
+        out_cdf[i] = 0.0F;
+        if (i < bf200::kMaxClosures) {
+            out_p[i] = 0.0F;
+        }
+    }
+    if (n == 0U) {
+        return true;
+    }
+    if (n > bf200::kMaxClosures) {
+        return false;
+    }
+    if (n == 1U) {
+        out_p[0] = 1.0F;
+        out_cdf[1] = 1.0F;
+        return probabilities[0] == 1.0F;
+    }
+    constexpr int digits = 24;
+    constexpr uint64_t scale = uint64_t{1} << digits;
+    uint64_t masses[bf200::kMaxClosures] = {};
+    float remainders[bf200::kMaxClosures] = {};
+    uint64_t base_mass = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float q = probabilities[i];
+        if (!std::isfinite(q) || !(q > 0.0F) || !(q < 1.0F)) {
+            return false;
+        }
+        const float scaled = std::ldexp(q, digits);
+        const float base = std::floor(scaled);
+        masses[i] = static_cast<uint64_t>(base);
+        remainders[i] = scaled - base;
+        base_mass += masses[i];
+    }
+    if (base_mass > scale) {
+        return false;
+    }
+    float sum = 0.0F, correction = 0.0F;  // add_compensated over non-negative remainders
+    for (uint32_t i = 0; i < n; ++i) {
+        const float next = sum + remainders[i];
+        correction += sum >= remainders[i] ? (sum - next) + remainders[i] : (remainders[i] - next) + sum;
+        sum = next;
+    }
+    const uint64_t missing = scale - base_mass;
+    if (missing > n ||
+        std::fabs((sum + correction) - static_cast<float>(missing)) > 0.5F + std::numeric_limits<float>::epsilon() * 16.0F) {
+        return false;
+    }
+    bool received[bf200::kMaxClosures] = {};
+    for (uint64_t unit = 0; unit < missing; ++unit) {
+        uint32_t selected = n;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (received[i] || !(remainders[i] > 0.0F)) {
+                continue;
+            }
+            if (selected == n || remainders[i] > remainders[selected]) {
+                selected = i;
+            }
+        }
+        if (selected == n) {
+            return false;
+        }
+        ++masses[selected];
+        received[selected] = true;
+    }
+    uint64_t cumulative = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (masses[i] == 0U || cumulative > scale - masses[i]) {
+            return false;
+        }
+        cumulative += masses[i];
+        out_p[i] = std::ldexp(static_cast<float>(masses[i]), -digits);
+        out_cdf[i + 1] = std::ldexp(static_cast<float>(cumulative), -digits);
+    }
+    return cumulative == scale && out_cdf[n] == 1.0F;
+}
+
+bool unit_direction3(const float* d) {  // unit_direction: squared length within 128 ulp of one
+    if (!std::isfinite(d[0]) || !std::isfinite(d[1]) || !std::isfinite(d[2])) {
+        return false;
+    }
+    const float squared = std::fma(d[0], d[0], std::fma(d[1], d[1], d[2] * d[2]));
+    return std::isfinite(squared) && std::fabs(squared - 1.0F) <= 128.0F * std::numeric_limits<float>::epsilon();
+}
+
+// exact_special_cosine (PunctualLights.hpp:186-197)
+float special_cosine(float angle) {
+    constexpr float pi = 3.14159265358979323846F;
+    if (angle == 0.0F) {
+        return 1.0F;
+    }
+    if (angle == pi / 2.0F) {
+        return 0.0F;
+    }
+    if (angle == pi) {
+        return -1.0F;
+    }
+    return std::cos(angle);
+}
+
+// The device record of a punctual light after the create() checks of PointLight, DirectionalLight
+// and SpotLight (PunctualLights.hpp:373-388, 494-509, 595-650); false when they refuse it.
+bool punctual_record(const bf200_punctual_light_v1& src, bf200::PunctualLight& out) {
+    constexpr float pi = 3.14159265358979323846F;
+    out = bf200::PunctualLight{};
+    out.kind = src.kind;
+    out.px = src.position[0], out.py = src.position[1], out.pz = src.position[2];
+    out.ex = src.position_error[0], out.ey = src.position_error[1], out.ez = src.position_error[2];
+    out.dx = src.direction[0], out.dy = src.direction[1], out.dz = src.direction[2];
+    for (int l = 0; l < 4; ++l) {
+        if (!std::isfinite(src.spectrum[l]) || src.spectrum[l] < 0.0F) {
+            return false;
+        }
+        out.spectrum[l] = src.spectrum[l];
+    }
+    if (src.reserved != 0U) {
+        return false;
+    }
+    bool finite_point = true;
+    for (int a = 0; a < 3; ++a) {
+        finite_point = finite_point && std::isfinite(src.position[a]) && std::isfinite(src.position_error[a]) &&
+                       src.position_error[a] >= 0.0F;
+    }
+    if (src.kind == BF200_PUNCTUAL_POINT) {
+        return finite_point;
+    }
+    if (src.kind == BF200_PUNCTUAL_DIRECTIONAL) {
+        return unit_direction3(src.direction);
+    }
+    if (src.kind != BF200_PUNCTUAL_SPOT || !finite_point || !unit_direction3(src.direction)) {
+        return false;
+    }
+    const float inner = src.inner_half_angle, outer = src.outer_half_angle;
+    if (!std::isfinite(inner) || !std::isfinite(outer) || inner < 0.0F || inner > outer || !(outer > 0.0F) ||
+        outer >= pi) {
+        return false;
+    }
+    out.cos_inner = special_cosine(inner);
+    out.cos_outer = special_cosine(outer);
+    out.hard = inner == outer ? 1U : 0U;
+    return std::isfinite(out.cos_inner) && std::isfinite(out.cos_outer) && out.cos_outer != 1.0F &&
+           out.cos_outer != -1.0F && !(inner > 0.0F && out.cos_inner == 1.0F) && !(out.cos_inner < out.cos_outer) &&
+           !(inner < outer && out.cos_inner == out.cos_outer);
+}
+
 blackframe_status validate_desc(bf200_context* c, const bf200_scene_desc_v1* d) {
-    if (d == nullptr || d->struct_size < sizeof(bf200_scene_desc_v1)) {
+    if (d == nullptr || d->struct_size < BF200_SCENE_DESC_V1_BASE_SIZE) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "scene description missing or too small");
     }
     if (d->punctual_light_count != 0) {
-        return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
-                    "punctual lights are not supported by this backend version (no substitution)");
+        if (d->struct_size < sizeof(bf200_scene_desc_v1) || d->punctual_lights == nullptr) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "punctual lights need the punctual_lights array");
+        }
+        for (uint32_t k = 0; k < d->punctual_light_count; ++k) {
+            bf200::PunctualLight record;
+            if (!punctual_record(d->punctual_lights[k], record)) {
+                return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
+                            "punctual light " + std::to_string(k) + " is refused by its light model's checks");
+            }
+        }
     }
     if (d->instance_count == 0 || d->geometry_count == 0 || d->material_count == 0) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "a scene needs geometry, materials and instances");
@@ -850,26 +1034,29 @@ blackframe_status validate_desc(bf200_context* c, const bf200_scene_desc_v1* d) 
     }
     for (uint32_t m = 0; m < d->material_count; ++m) {
         const auto& mat = d->materials[m];
-        if (mat.closure_count > 1) {
-            return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
-                        "closure mixtures with more than one closure are not supported (no substitution)");
+        if (mat.closure_count > bf200::kMaxClosures) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "a closure mixture holds at most 8 closures");
         }
         if (mat.frame_mode != 0) {
             return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "surface-tangent closure frames are not supported");
         }
-        if (mat.closure_count == 1) {
-            if (mat.closure_offset >= d->closure_count) {
-                return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "closure index out of range");
-            }
-            const uint32_t kind = d->closures[mat.closure_offset].kind;
-            if (kind != BF200_CLOSURE_LAMBERTIAN_REFLECTION && kind != BF200_CLOSURE_ROUGH_CONDUCTOR_REFLECTION &&
-                kind != BF200_CLOSURE_ROUGH_DIELECTRIC) {
+        if (mat.closure_count != 0 && static_cast<uint64_t>(mat.closure_offset) + mat.closure_count > d->closure_count) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "closure index out of range");
+        }
+        for (uint32_t k = 0; k < mat.closure_count; ++k) {
+            const uint32_t kind = d->closures[mat.closure_offset + k].kind;
+            if (kind < BF200_CLOSURE_LAMBERTIAN_REFLECTION || kind > BF200_CLOSURE_SPECULAR_TRANSMISSION) {
                 return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "closure kind not supported by this backend");
             }
-            if (!valid_closure_payload(d->closures[mat.closure_offset])) {
+            if (!valid_closure_payload(d->closures[mat.closure_offset + k])) {
                 return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
                             "material " + std::to_string(m) + " has an invalid closure payload");
             }
+        }
+        float p[bf200::kMaxClosures], cdf[bf200::kMaxClosures + 1];
+        if (!project_component_distribution(mat.component_probabilities, mat.closure_count, p, cdf)) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
+                        "material " + std::to_string(m) + " has component probabilities that are not a distribution");
         }
     }
     for (uint32_t i = 0; i < d->instance_count; ++i) {
@@ -1610,41 +1797,68 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
                 tri_local.push_back(t);
             }
         }
-        if (lights.empty()) {
+        // the light registry: punctual lights (slots [0, P)), then the mesh lights
+        std::vector<bf200::PunctualLight> punctual(d->punctual_light_count);
+        for (uint32_t k = 0; k < d->punctual_light_count; ++k) {
+            punctual_record(d->punctual_lights[k], punctual[k]);
+        }
+        const size_t registry = punctual.size() + lights.size();
+        if (registry == 0) {
             return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
-                        "MIS requires at least one emissive mesh light in the committed scene");
+                        "MIS requires at least one punctual or emissive mesh light in the committed scene");
         }
         // LightSampler::create_uniform (LightSampler.cpp:574-602)
-        std::vector<float> select(lights.size() + 1, 0.0F);
-        for (size_t k = 1; k < lights.size(); ++k) {
-            select[k] = static_cast<float>(k) / static_cast<float>(lights.size());
+        std::vector<float> select(registry + 1, 0.0F);
+        for (size_t k = 1; k < registry; ++k) {
+            select[k] = static_cast<float>(k) / static_cast<float>(registry);
         }
-        select[lights.size()] = 1.0F;
-        scene->light_count = static_cast<uint32_t>(lights.size());
+        select[registry] = 1.0F;
+        scene->light_count = static_cast<uint32_t>(registry);
+        scene->punctual_count = static_cast<uint32_t>(punctual.size());
         scene->material_count = d->material_count;
-        // materials
+        // materials: the first closure per material (single-closure routes), every closure and the
+        // projected component distribution (the generic route's mixtures)
         std::vector<ClosureData> closures(d->material_count);
+        std::vector<ClosureData> mix_closures;
+        std::vector<bf200::MixDistribution> mix_dist(d->material_count);
         std::vector<float4> emission(d->material_count);
         std::vector<uint4> material_info(d->material_count);
+        bool plain_materials = true;  // every material a single Lambert, conductor or dielectric closure
         for (uint32_t m = 0; m < d->material_count; ++m) {
             const auto& mat = d->materials[m];
-            ClosureData cd{};
-            if (mat.closure_count == 1) {
-                const auto& src = d->closures[mat.closure_offset];
+            bf200::MixDistribution& dist = mix_dist[m];
+            dist = bf200::MixDistribution{};
+            dist.closure_offset = static_cast<uint32_t>(mix_closures.size());
+            project_component_distribution(mat.component_probabilities, mat.closure_count, dist.p, dist.cdf);
+            for (uint32_t k = 0; k < mat.closure_count; ++k) {
+                const auto& src = d->closures[mat.closure_offset + k];
+                ClosureData cd{};
                 cd.kind = src.kind;
                 cd.lobes = src.lobes;
                 std::memcpy(cd.w, src.weight, sizeof(cd.w));
                 std::memcpy(cd.p, src.parameters, sizeof(cd.p));
+                mix_closures.push_back(cd);
+                if (k == 0) {
+                    closures[m] = cd;
+                }
             }
-            closures[m] = cd;
+            if (mat.closure_count > 1 ||
+                (mat.closure_count == 1 && closures[m].kind != kClosureLambert &&
+                 closures[m].kind != kClosureConductor && closures[m].kind != kClosureDielectric)) {
+                plain_materials = false;
+            }
             emission[m] = make_float4(mat.emitted_radiance[0], mat.emitted_radiance[1], mat.emitted_radiance[2],
                                       mat.emitted_radiance[3]);
             uint32_t rotation_bits;
             std::memcpy(&rotation_bits, &mat.tangent_rotation_radians, 4);
-            material_info[m] = make_uint4(mat.closure_count, mat.frame_mode, rotation_bits, 0);
+            material_info[m] = make_uint4(mat.closure_count, mat.frame_mode, rotation_bits, dist.closure_offset);
         }
+        if (mix_closures.empty()) {
+            mix_closures.push_back(ClosureData{});
+        }
+        scene->plain_materials = plain_materials;
         // shading route of a hit on each instance: the kernel specialised for its material's single
-        // closure kind, or the generic one
+        // closure kind, or the generic one (several closures, or another kind)
         std::vector<uint8_t> inst_route(d->instance_count, static_cast<uint8_t>(kRouteGeneric));
         for (uint32_t i = 0; i < d->instance_count; ++i) {
             const uint32_t m = d->instances[i].material_index;
@@ -1688,6 +1902,12 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         up(nodes4, v.nodes);
         up(leaf_tris, v.leaf_tris);
         up(closures, v.closures);
+        up(mix_closures, v.mix_closures);
+        up(mix_dist, v.mix_dist);
+        v.punctual_count = static_cast<uint32_t>(punctual.size());
+        if (!punctual.empty()) {
+            up(punctual, v.punctual);
+        }
         up(emission, v.emission);
         up(material_info, v.material_info);
         up(select, v.light_select_cdf);
@@ -1756,7 +1976,7 @@ BF200_EXPORT blackframe_status bf200_scene_refit(bf200_scene* s, const bf200_sce
         return BLACKFRAME_STATUS_INVALID_ARGUMENT;
     }
     bf200_context* c = s->context;
-    if (d == nullptr || d->struct_size < sizeof(bf200_scene_desc_v1) || d->geometries == nullptr ||
+    if (d == nullptr || d->struct_size < BF200_SCENE_DESC_V1_BASE_SIZE || d->geometries == nullptr ||
         d->positions == nullptr || d->normals == nullptr || d->triangles == nullptr || d->materials == nullptr ||
         d->instances == nullptr) {
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "scene description missing or too small");
@@ -2639,6 +2859,11 @@ blackframe_status check_adjoint_scene(bf200_context* c, const bf200_scene* s) {
     }
     if (s->view.tree != nullptr) {
         return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "the adjoint does not replay light-tree selection");
+    }
+    if (!s->plain_materials || s->punctual_count != 0U) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_STATE,
+                    "the adjoint replays single Lambert, GGX conductor or GGX dielectric closures and mesh "
+                    "lights only (no closure mixtures, rough-diffuse or specular closures, punctual lights)");
     }
     return BLACKFRAME_STATUS_SUCCESS;
 }

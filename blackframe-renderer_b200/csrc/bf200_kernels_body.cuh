@@ -1330,8 +1330,9 @@ static __device__ bool resolve_surface(const SceneView& s, uint32_t inst, uint32
 struct LightSample {
     bool valid;
     F3 position, error, normal, direction;
-    float pdf;
+    float pdf;  // solid angle, or the discrete mass (1) of a punctual light
     float radiance[4];
+    uint32_t endpoint;  // 0 surface point, 1 finite point (point, spot), 2 infinite (directional)
 };
 
 __device__ __forceinline__ uint32_t upper_bound(const float* a, uint32_t n, float u) {
@@ -1419,7 +1420,251 @@ static __device__ void sample_mesh_light(const SceneView& s, const LightInfo& li
         out.radiance[l] = light.radiance[l];
         black = black && light.radiance[l] == 0.0F;
     }
+    out.endpoint = 0U;
     out.valid = !black && lane.err == 0;
+}
+
+// scale_radiometric_value (PunctualLights.hpp:131-183) with n numerator and three denominator factors
+__device__ __forceinline__ float scale_radiometric(float value, const float* num, int n, const float (&den)[3],
+                                                   Lane& lane) {
+    if (!isfinite(value) || value < 0.0F) {
+        lane.fail();
+        return 0.0F;
+    }
+    for (int i = 0; i < n; ++i) {
+        if (!isfinite(num[i]) || !(num[i] > 0.0F)) {
+            lane.fail();
+            return 0.0F;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (!isfinite(den[i]) || !(den[i] > 0.0F)) {
+            lane.fail();
+            return 0.0F;
+        }
+    }
+    if (value == 0.0F) {
+        return 0.0F;
+    }
+    int exponent = 0;
+    float fraction = frexpf(value, &exponent);
+    int accumulated = exponent;
+    for (int i = 0; i < n; ++i) {
+        int e = 0;
+        fraction *= frexpf(num[i], &e);
+        accumulated += e;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        int e = 0;
+        fraction /= frexpf(den[i], &e);
+        accumulated -= e;
+    }
+    int ne = 0;
+    fraction = frexpf(fraction, &ne);
+    const float result = scalbnf(fraction, accumulated + ne);
+    if (!isfinite(result) || !(result > 0.0F)) {
+        lane.fail();
+    }
+    return result;
+}
+
+// PointLight / DirectionalLight / SpotLight::sample_li (PunctualLights.hpp:390-430, 510-530,
+// 654-720) with IncidentLightSample::create_finite / create_infinite (Light.hpp:404-456).
+static __device__ void sample_punctual_light(const PunctualLight& light, F3 context, float u, float v,
+                                             LightSample& out, Lane& lane) {
+    out.valid = false;
+    out.pdf = 1.0F;
+    if (!isfinite(u) || !isfinite(v) || u < 0.0F || u >= 1.0F || v < 0.0F || v >= 1.0F) {
+        lane.fail();
+        return;
+    }
+    const bool black = light.spectrum[0] == 0.0F && light.spectrum[1] == 0.0F && light.spectrum[2] == 0.0F &&
+                       light.spectrum[3] == 0.0F;
+    if (light.kind == BF200_PUNCTUAL_DIRECTIONAL) {
+        if (black) {
+            return;
+        }
+        out.direction = F3{-light.dx, -light.dy, -light.dz};
+        if (!unit_length(out.direction)) {
+            lane.fail();
+            return;
+        }
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            out.radiance[l] = light.spectrum[l];
+        }
+        out.endpoint = 2U;
+        out.valid = true;
+        return;
+    }
+    // finite_light_geometry (PunctualLights.hpp:102-129)
+    const F3 position{light.px, light.py, light.pz};
+    const F3 disp = position - context;
+    if (!finite3(disp)) {
+        lane.fail();
+        return;
+    }
+    const float scale = max_abs3(disp);
+    if (!(scale > 0.0F) || !isfinite(scale)) {
+        lane.fail();
+        return;
+    }
+    const F3 scaled = disp / scale;
+    const float squared = fmaf(scaled.x, scaled.x, fmaf(scaled.y, scaled.y, scaled.z * scaled.z));
+    const float root = sqrtf(squared);
+    const float distance = scale * root;
+    if (!isfinite(squared) || !(squared > 0.0F) || !isfinite(root) || !(root > 0.0F) || !isfinite(distance) ||
+        !(distance > 0.0F)) {
+        lane.fail();
+        return;
+    }
+    const F3 to_light = scaled / root;
+    if (!unit_length(to_light)) {
+        lane.fail();
+        return;
+    }
+    float falloff[3] = {1.0F, 1.0F, 1.0F};
+    int falloff_count = 0;
+    if (light.kind == BF200_PUNCTUAL_SPOT) {
+        const float cone = fmaf(light.dx, -to_light.x, fmaf(light.dy, -to_light.y, light.dz * -to_light.z));
+        if (!isfinite(cone)) {
+            lane.fail();
+            return;
+        }
+        if (cone <= light.cos_outer) {
+            return;
+        }
+        falloff_count = 3;
+        if (light.hard == 0U && cone < light.cos_inner) {
+            const float transition = (cone - light.cos_outer) / (light.cos_inner - light.cos_outer);
+            const float smooth = 3.0F - 2.0F * transition;
+            if (!isfinite(transition) || !(transition > 0.0F) || !(transition < 1.0F) || !isfinite(smooth) ||
+                !(smooth > 0.0F)) {
+                lane.fail();
+                return;
+            }
+            falloff[0] = transition;
+            falloff[1] = transition;
+            falloff[2] = smooth;
+        }
+    }
+    const float den[3] = {scale, scale, squared};
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        out.radiance[l] = scale_radiometric(light.spectrum[l], falloff, falloff_count, den, lane);
+    }
+    if (black) {
+        return;
+    }
+    out.direction = to_light;  // create_finite repeats the same arithmetic
+    out.position = position;
+    out.error = F3{light.ex, light.ey, light.ez};
+    out.endpoint = 1U;
+    out.valid = lane.err == 0;
+}
+
+// contract_point_endpoint (ShadowRay.hpp:66-113)
+__device__ __forceinline__ F3 contract_point_endpoint(F3 point, F3 error, F3 to_light, Lane& lane) {
+    float contraction = 0.0F;
+    const float d[3] = {to_light.x, to_light.y, to_light.z}, e[3] = {error.x, error.y, error.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float candidate = fmaf(fabsf(d[a]), e[a], contraction);
+        if (!isfinite(candidate) || candidate < contraction) {
+            lane.fail();
+        }
+        contraction = (d[a] != 0.0F && e[a] != 0.0F) ? nextafterf(candidate, kInf) : candidate;
+    }
+    if (!isfinite(contraction)) {
+        lane.fail();
+    }
+    if (contraction == 0.0F) {
+        return point;
+    }
+    float c[3] = {fmaf(-d[0], contraction, point.x), fmaf(-d[1], contraction, point.y),
+                  fmaf(-d[2], contraction, point.z)};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (d[a] != 0.0F) {
+            c[a] = nextafterf(c[a], d[a] > 0.0F ? -kInf : kInf);
+        }
+    }
+    const F3 out{c[0], c[1], c[2]};
+    if (!finite3(out)) {
+        lane.fail();
+    }
+    return out;
+}
+
+// DepthFilteredClosureMixture::create (DepthFilteredClosureMixture.hpp:262-364) on the generic
+// route: the material's closures filtered by the depth limits into `m`.
+static __device__ void mix_filter(const SceneView& s, uint32_t material, const TransportParams& p, uint32_t depth,
+                                  Mix& m, Lane& lane) {
+    const uint4 minfo = s.material_info[material];
+    const MixDistribution& dist = s.mix_dist[material];
+    m.closures = s.mix_closures + minfo.w;
+    m.count = 0U;
+    m.blocked = 0U;
+    for (uint32_t i = 0; i < minfo.x; ++i) {
+        const ClosureData c = m.closures[i];
+        uint32_t allowed = 0U;
+        if (c.kind == kClosureDielectric) {
+            const uint32_t br = depth_blocked(p, depth, kLobeGlossy | kLobeReflection);
+            const uint32_t bt = depth_blocked(p, depth, kLobeGlossy | kLobeTransmission);
+            if (br == 0U) allowed |= kLobeReflection; else m.blocked |= br;
+            if (bt == 0U) allowed |= kLobeTransmission; else m.blocked |= bt;
+        } else {
+            if (!cone_surface_event(c.lobes)) {  // is_valid_surface_scattering_event
+                lane.fail();
+                return;
+            }
+            const uint32_t bl = depth_blocked(p, depth, c.lobes);
+            if (bl == 0U) allowed |= c.lobes & (kLobeReflection | kLobeTransmission); else m.blocked |= bl;
+        }
+        if (allowed == 0U) {
+            continue;
+        }
+        m.source[m.count] = static_cast<uint8_t>(i);
+        m.allowed[m.count] = static_cast<uint8_t>(allowed);
+        m.p[m.count] = dist.p[i];
+        ++m.count;
+    }
+    if (m.count == 0U) {
+        return;
+    }
+    if (m.count == minfo.x) {
+        for (uint32_t i = 0; i <= m.count; ++i) {
+            m.cdf[i] = dist.cdf[i];
+        }
+        return;
+    }
+    if (m.count == 1U) {
+        m.p[0] = 1.0F;
+        m.cdf[0] = 0.0F;
+        m.cdf[1] = 1.0F;
+        return;
+    }
+    float sum = 0.0F, correction = 0.0F;
+    for (uint32_t i = 0; i < m.count; ++i) {
+        if (!add_compensated(m.p[i], sum, correction)) {
+            lane.fail();
+            return;
+        }
+    }
+    const float total = sum + correction;
+    if (!isfinite(total) || !(total > 0.0F)) {
+        lane.fail();
+        return;
+    }
+    float normalized[kMaxClosures];
+    for (uint32_t i = 0; i < m.count; ++i) {
+        normalized[i] = m.p[i] / total;
+    }
+    if (!component_distribution(normalized, m.count, m.p, m.cdf)) {
+        lane.fail();
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1490,14 +1735,22 @@ __device__ __forceinline__ bool is_black4(const float (&v)[4]) {
 }
 
 // SceneMisPathLoop.cpp:136-275 (estimate) without the visibility query: the record carries the
-// shadow ray and the contribution it adds when unoccluded (transmittance 1).
+// shadow ray and the contribution it adds when unoccluded (transmittance 1). The light is a
+// punctual light (registry slots [0, punctual_count), a discrete sample without MIS) or a mesh light.
 template <int K, bool TREE>
-__device__ void direct_lighting(const SceneView& s, const TransportParams& p, const Surface& surf,
-                                const ClosureData& closure, uint32_t allowed, const float4 beta4, F3 wo_world,
-                                uint64_t dims, const Stream& stream, uint32_t mask, ShadowRecord& rec, Lane& lane) {
+__device__ void direct_lighting(const SceneView& s, const TransportParams& p, const Surface& surf, const Mix& mix,
+                                const float4 beta4, F3 wo_world, uint64_t dims, const Stream& stream, uint32_t mask,
+                                ShadowRecord& rec, Lane& lane) {
     rec.valid = false;
     const float beta[4] = {beta4.x, beta4.y, beta4.z, beta4.w};
-    if (is_black4(beta) || is_black4(closure.w)) {
+    if (is_black4(beta)) {
+        return;
+    }
+    bool all_black = true;
+    for (uint32_t i = 0; i < (K != 0 ? 1U : mix.count); ++i) {
+        all_black = all_black && is_black4(mix_closure<K>(mix, i).w);
+    }
+    if (all_black) {
         return;
     }
     const float u_sel = stream.sample_1d(dims + 0);
@@ -1518,12 +1771,17 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
         }
         selection = s.light_select_cdf[b + 1] - s.light_select_cdf[b];
     }
-    const LightInfo light = s.lights[b];
-    if ((s.inst_info[light.instance].z & mask) == 0U) {
-        return;
-    }
     LightSample ls;
-    sample_mesh_light(s, light, surf.position, stream.sample_1d(dims + 1), stream.sample_1d(dims + 2), ls, lane);
+    const float lu = stream.sample_1d(dims + 1), lv = stream.sample_1d(dims + 2);
+    if (b < s.punctual_count) {
+        sample_punctual_light(s.punctual[b], surf.position, lu, lv, ls, lane);
+    } else {
+        const LightInfo light = s.lights[b - s.punctual_count];
+        if ((s.inst_info[light.instance].z & mask) == 0U) {
+            return;
+        }
+        sample_mesh_light(s, light, surf.position, lu, lv, ls, lane);
+    }
     if (!ls.valid) {
         return;
     }
@@ -1532,10 +1790,11 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
     if (wo.z == 0.0F || wi.z == 0.0F) {
         return;
     }
-    const bool lambert = kind_is<K>(closure, kClosureLambert);
+    const ClosureData first = mix_closure<K>(mix, 0);
+    const bool lambert = (K != 0 || mix.count == 1U) && kind_is<K>(first, kClosureLambert);
     float f[4] = {0.0F, 0.0F, 0.0F, 0.0F};
     if (!lambert) {
-        closure_eval<K>(closure, allowed, wo, wi, f, lane);
+        mix_eval<K>(mix, wo, wi, f, lane);
         if (is_black4(f)) {
             return;
         }
@@ -1549,18 +1808,32 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
             return;
         }
     }
-    const float bsdf_pdf = closure_pdf<K>(closure, allowed, wo, wi, lane);
-    const float light_pdf = joint_light_pdf(selection, ls.pdf, lane);
-    const float weight = mis_weight(p.heuristic, light_pdf, bsdf_pdf, lane);
-    // make_shadow_ray (ShadowRay.hpp:181-253) for a finite surface endpoint
+    float weight = 1.0F;
+    if (ls.endpoint == 0U) {  // a solid-angle density: MIS against the closures' density
+        const float bsdf_pdf = mix_pdf<K>(mix, wo, wi, lane);
+        const float light_pdf = joint_light_pdf(selection, ls.pdf, lane);
+        weight = mis_weight(p.heuristic, light_pdf, bsdf_pdf, lane);
+    }
+    // make_shadow_ray (ShadowRay.hpp:181-253)
     const F3 origin = offset_surface_point(surf.position, surf.error, surf.ng, ls.direction, lane);
-    const F3 endpoint = offset_surface_point(ls.position, ls.error, ls.normal, origin - ls.position, lane);
-    F3 sd{0.0F, 0.0F, 1.0F};
-    float length = 1.0F;
-    unit_segment(origin, endpoint, ls.direction, sd, length, lane);
-    const float t_max = nextafterf(length, 0.0F);
-    if (!(t_max > 0.0F) || !isfinite(t_max)) {
-        lane.fail();
+    F3 sd = ls.direction;
+    float t_max = kInf;
+    if (ls.endpoint != 2U) {
+        F3 endpoint;
+        if (ls.endpoint == 1U) {
+            F3 nominal{0.0F, 0.0F, 1.0F};
+            float nominal_length = 1.0F;
+            unit_segment(origin, ls.position, ls.direction, nominal, nominal_length, lane);
+            endpoint = contract_point_endpoint(ls.position, ls.error, nominal, lane);
+        } else {
+            endpoint = offset_surface_point(ls.position, ls.error, ls.normal, origin - ls.position, lane);
+        }
+        float length = 1.0F;
+        unit_segment(origin, endpoint, ls.direction, sd, length, lane);
+        t_max = nextafterf(length, 0.0F);
+        if (!(t_max > 0.0F) || !isfinite(t_max)) {
+            lane.fail();
+        }
     }
     if (lane.err != 0) {
         return;
@@ -1575,10 +1848,10 @@ __device__ void direct_lighting(const SceneView& s, const TransportParams& p, co
         for (int l = 0; l < 4; ++l) {
             const float den[2] = {selection, ls.pdf};
             if (weight == 1.0F) {
-                const float num[6] = {beta[l], closure.w[l], kInvPi, ls.radiance[l], wi.z, 1.0F};
+                const float num[6] = {beta[l], first.w[l], kInvPi, ls.radiance[l], wi.z, 1.0F};
                 out[l] = checked_product_quotient(num, den, lane);
             } else {
-                const float num[7] = {beta[l], closure.w[l], kInvPi, ls.radiance[l], wi.z, 1.0F, weight};
+                const float num[7] = {beta[l], first.w[l], kInvPi, ls.radiance[l], wi.z, 1.0F, weight};
                 out[l] = checked_product_quotient(num, den, lane);
             }
         }
@@ -1815,11 +2088,12 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                     const float emitted[4] = {emission4.x, emission4.y, emission4.z, emission4.w};
                     float emission_weight = 1.0F;
                     if (!is_black4(emitted) && prev.w > 0.0F) {
-                        const uint32_t light_index = inst.w & 0x7FFFFFFFU;
+                        const uint32_t mesh_index = inst.w & 0x7FFFFFFFU;
+                        const uint32_t light_index = s.punctual_count + mesh_index;  // registry slot
                         if (light_index >= s.light_count) {
                             lane.fail();
                         } else {
-                            const LightInfo light = s.lights[light_index];
+                            const LightInfo light = s.lights[mesh_index];
                             float selection = 0.0F;
                             if constexpr (TREE) {  // probability(context, i) at the previous vertex
                                 const float at[3] = {prev.x, prev.y, prev.z};
@@ -1854,8 +2128,8 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                         done = true;
                     }
                 }
-                ClosureData closure;
-                uint32_t allowed = 0U;
+                Mix mix;
+                mix.count = 0U;
                 if (!done) {
                     if (beta.x == 0.0F && beta.y == 0.0F && beta.z == 0.0F && beta.w == 0.0F) {
                         done = true;
@@ -1867,10 +2141,18 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                     if (minfo.x == 0U) {
                         done = true;
                         termination = 2U;  // outside_bsdf_support
-                    } else if (minfo.x != 1U) {
-                        lane.fail(kLaneUnsupported);
-                        done = true;
+                    } else if (K == 0) {
+                        mix_filter(s, material, p, depth, mix, lane);
+                        if (lane.err != 0) {
+                            done = true;
+                        } else if (mix.count == 0U) {
+                            done = true;
+                            termination = 1U;  // depth_limit
+                            blocked = mix.blocked;
+                        }
                     } else {
+                        ClosureData& closure = mix.first;
+                        uint32_t allowed = 0U;
                         closure = s.closures[material];
                         // depth filter of one closure (DepthFilteredClosureMixture.hpp:262-364)
                         uint32_t block_mask = 0U;
@@ -1889,9 +2171,17 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                             termination = 1U;  // depth_limit
                             blocked = block_mask;
                         }
+                        mix.count = 1U;
+                        mix.source[0] = 0U;
+                        mix.allowed[0] = static_cast<uint8_t>(allowed);
+                        mix.p[0] = 1.0F;
+                        mix.cdf[0] = 0.0F;
+                        mix.cdf[1] = 1.0F;
                     }
                 }
                 if (!done) {
+                    // the single closure of the adjoint's scenes (mixtures are refused there)
+                    const ClosureData closure = mix_closure<K>(mix, 0);
                     if constexpr (ADJ) {
                         if (al.on) {  // everything after this vertex scales with its closure weight
                             const float fv[4] = {al.forward.x, al.forward.y, al.forward.z, al.forward.w};
@@ -1910,25 +2200,33 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                     const F3 wo = surf.frame.to_local(wo_world);
                     const uint64_t dims = bounce_base(depth_total(depth));
                     BsdfSample bs;
-                    closure_sample<K>(closure, allowed, wo, stream.sample_1d(dims + 3), stream.sample_1d(dims + 4),
-                                   stream.sample_1d(dims + 5), bs, lane);
+                    mix_sample<K>(mix, wo, stream.sample_1d(dims + 3), stream.sample_1d(dims + 4),
+                                  stream.sample_1d(dims + 5), bs, lane);
                     if constexpr (CONE) {
                         ++closures_here;
-                        if (s.light_count != 0U && !is_black4(closure.w)) {
+                        bool all_black = true;
+                        for (uint32_t i = 0; i < (K != 0 ? 1U : mix.count); ++i) {
+                            all_black = all_black && is_black4(mix_closure<K>(mix, i).w);
+                        }
+                        if (s.light_count != 0U && !all_black) {
                             ++lights_here;
                         }
                     }
                     uint32_t next_depth = depth;
                     if (bs.valid) {
-                        if (!isfinite(bs.pdf) || !(bs.pdf > 0.0F) || bs.wi.z == 0.0F ||
-                            depth_blocked(p, depth, bs.lobes) != 0U) {
+                        bool finite_value = true;
+#pragma unroll
+                        for (int l = 0; l < 4; ++l) {
+                            finite_value = finite_value && isfinite(bs.value[l]) && bs.value[l] >= 0.0F;
+                        }
+                        if (!cone_surface_event(bs.lobes) || !finite_value || !isfinite(bs.pdf) || !(bs.pdf > 0.0F) ||
+                            bs.wi.z == 0.0F || depth_blocked(p, depth, bs.lobes) != 0U) {
                             lane.fail();
                         }
                         next_depth = depth_advance(depth, bs.lobes);
                     }
                     if (lane.err == 0) {
-                        direct_lighting<K, TREE>(s, p, surf, closure, allowed, beta, wo_world, dims, stream, mask, rec,
-                                                 lane);
+                        direct_lighting<K, TREE>(s, p, surf, mix, beta, wo_world, dims, stream, mask, rec, lane);
                         if constexpr (ADJ) {
                             if (al.on && rec.valid) {
                                 double2 score = make_double2(0.0, 0.0);
@@ -1957,9 +2255,13 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                             termination = 2U;
                         } else {
                             // update_closure_throughput (BsdfOnlyPathLoop.hpp:64-131), correction 1
+                            const bool delta = (bs.lobes & kLobeSpecular) != 0U;
+                            if (bs.delta != delta || (delta && bs.pdf > 1.0F)) {
+                                lane.fail();
+                            }
                             const float bv[4] = {beta.x, beta.y, beta.z, beta.w};
                             float nb[4];
-                            if (kind_is<K>(closure, kClosureLambert)) {
+                            if ((K != 0 || mix.count == 1U) && kind_is<K>(closure, kClosureLambert)) {
 #pragma unroll
                                 for (int l = 0; l < 4; ++l) {
                                     nb[l] = bv[l] * closure.w[l];
@@ -2016,7 +2318,8 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                             float2 next_cone = make_float2(0.0F, 0.0F);
                             if (CONE && lane.err == 0 &&
                                 (!cone_advance(w.cone[slot], rd, tb.x, next_cone) ||
-                                 !cone_scatter<K>(next_cone, closure, bs.lobes, wo, bs.wi, next_cone))) {
+                                 !cone_scatter<K>(next_cone, mix_closure<K>(mix, bs.selected), bs.lobes, wo, bs.wi,
+                                                  next_cone))) {
                                 lane.fail();
                             }
                             if (lane.err == 0) {
@@ -2027,8 +2330,13 @@ __global__ void __launch_bounds__(256, BF200_SHADE_MIN_BLOCKS) k_shade(SceneView
                                 w.beta[slot] = beta;
                                 w.depth[slot] = next_depth;
                                 w.eta[slot] = next_eta;
-                                w.prev[slot] = make_float4(surf.position.x, surf.position.y, surf.position.z, bs.pdf);
-                                w.flags[slot] = (w.flags[slot] & ~0xFFU) | 2U;  // any_non_delta_bounces
+                                // record_bsdf_sample: a delta continuation leaves no density (w = 0) for
+                                // the next emissive hit's MIS weight; next_delta_flags: bit 0 previous
+                                // bounce was delta, bit 1 any non-delta bounce
+                                w.prev[slot] = make_float4(surf.position.x, surf.position.y, surf.position.z,
+                                                           delta ? 0.0F : bs.pdf);
+                                const uint32_t old_flags = w.flags[slot];
+                                w.flags[slot] = (old_flags & ~0xFFU) | (old_flags & 2U) | (delta ? 1U : 2U);
                                 w.ray_o[slot] = make_float4(origin.x, origin.y, origin.z, kInf);
                                 w.ray_d[slot] = make_float4(wi_world.x, wi_world.y, wi_world.z, 0.0F);
                                 if (nb[0] == 0.0F && nb[1] == 0.0F && nb[2] == 0.0F && nb[3] == 0.0F) {

@@ -3590,8 +3590,23 @@ Spectrum direct_lighting(const Scene& scene, const Options& opt, const Surface& 
 // carries it (CudaWavefrontStages.cu:4602-4624) and returned in PathOut::cone_*.
 // state: null (PathState::create_initial), or a depth-zero initial state whose throughput,
 // radiance and eta scale the path starts from (trace_scene_mis takes any such PathState).
+// The radiance contributions of one path as the float transport adds them, for the float64
+// gradient (bfo_weight_gradients): each contribution's value, the closure vertices whose weights
+// multiply into it (the first `vertices` entries of `materials`), and whether an emitter's radiance
+// is one of its factors (emission hits and light samples; not the environment).
+struct PathRecord {
+    struct Contribution {
+        std::array<double, 4> value;
+        uint32_t vertices;
+        bool emitter;
+    };
+    std::vector<Contribution> contributions;
+    std::vector<uint32_t> materials;  // material of every scattering vertex, in path order
+};
+
 PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Options& opt,
-              const float* cone = nullptr, const bf200_path_state_v1* state = nullptr) {
+              const float* cone = nullptr, const bf200_path_state_v1* state = nullptr,
+              PathRecord* record = nullptr) {
     PathOut out{};
     out.beta = Spectrum{1.0F, 1.0F, 1.0F, 1.0F};
     out.radiance = Spectrum{};
@@ -3645,6 +3660,13 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
         Hit hit{};
         ++out.segments;
         if (!closest_hit(scene, ro, rd, tmin, tmax, mask, hit)) {
+            if (record != nullptr) {
+                std::array<double, 4> c{};
+                for (int lane = 0; lane < 4; ++lane) {
+                    c[lane] = static_cast<double>(out.beta[lane]) * scene.environment[lane];
+                }
+                record->contributions.push_back({c, static_cast<uint32_t>(record->materials.size()), false});
+            }
             add_spectrum_product(out.radiance, out.beta, scene.environment);
             return finish(BF200_TERMINATION_ESCAPED_ENVIRONMENT);
         }
@@ -3670,6 +3692,13 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
                                                                 surf.position, surf.ng);
             const float light_pdf = joint_light_pdf(selection, conditional);
             emission_weight = mis_weight(opt.heuristic, prev.pdf, light_pdf);
+        }
+        if (record != nullptr && !is_black(emitted)) {
+            std::array<double, 4> c{};
+            for (int lane = 0; lane < 4; ++lane) {
+                c[lane] = static_cast<double>(out.beta[lane]) * emitted[lane] * emission_weight;
+            }
+            record->contributions.push_back({c, static_cast<uint32_t>(record->materials.size()), true});
         }
         add_weighted_emission(out.radiance, out.beta, emitted, emission_weight);
         if (is_black(out.beta)) {
@@ -3711,6 +3740,16 @@ PathOut trace(const Scene& scene, const bf200_path_input_v1& input, const Option
                 fail("A direct-lighting contribution must be finite and non-negative.");
             }
             out.radiance[lane] = out.radiance[lane] + direct[lane];
+        }
+        if (record != nullptr) {
+            record->materials.push_back(scene.instances[hit.instance].material);
+            if (!is_black(direct)) {
+                std::array<double, 4> c{};
+                for (int lane = 0; lane < 4; ++lane) {
+                    c[lane] = direct[lane];
+                }
+                record->contributions.push_back({c, static_cast<uint32_t>(record->materials.size()), true});
+            }
         }
         if (!bs.valid) {
             return finish(BF200_TERMINATION_OUTSIDE_BSDF_SUPPORT);
@@ -4146,6 +4185,58 @@ __attribute__((visibility("default"))) int64_t bfo_trace_paths(void* h, const bf
                                                                const bf200_transport_options_v1* o,
                                                                bf200_path_result_v1* res, int threads) {
     return trace_batch(h, in, nullptr, nullptr, n, o, res, nullptr, threads);
+}
+
+// Float64 gradient of a loss with respect to every material's closure weight (per packet lane) and
+// a common emitter radiance scale, along the float transport's own paths. path_adjoint holds
+// dLoss/dL per path and lane. With the sampled directions fixed every radiance contribution is a
+// product in which the closure weight of each scattering vertex before it appears once (Lambert: in
+// the throughput update; GGX and specular: in the BSDF value) and an emitter's radiance at most
+// once, so its derivative with respect to material m's lane-l weight is value * (vertices of m) /
+// weight. The sums run in double over the recorded contributions; they restate the derivative
+// independently of the device replay's per-vertex "radiance after this vertex" bookkeeping.
+// Materials must be single closures. Returns the number of failed paths (left out).
+__attribute__((visibility("default"))) int64_t bfo_weight_gradients(void* h, const bf200_path_input_v1* in, uint64_t n,
+                                                                    const bf200_transport_options_v1* o,
+                                                                    const double* path_adjoint, double* gradients,
+                                                                    double* emission_gradient) {
+    const auto* s = static_cast<Scene*>(h);
+    const Options opt = make_options(*o);
+    const size_t materials = s->materials.size();
+    std::vector<double> g(materials * 4, 0.0);
+    double e = 0.0;
+    int64_t failures = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        PathRecord record;
+        try {
+            trace(*s, in[i], opt, nullptr, nullptr, &record);
+        } catch (const Failure&) {
+            ++failures;
+            continue;
+        }
+        const double* adj = path_adjoint + 4 * i;
+        for (const auto& c : record.contributions) {
+            for (int lane = 0; lane < 4; ++lane) {
+                const double weighted = adj[lane] * c.value[lane];
+                if (weighted == 0.0) {
+                    continue;
+                }
+                if (c.emitter) {
+                    e += weighted;
+                }
+                for (uint32_t v = 0; v < c.vertices; ++v) {
+                    const uint32_t m = record.materials[v];
+                    const float w = s->materials[m].closures[0].weight[lane];
+                    if (w != 0.0F) {
+                        g[4 * m + lane] += weighted / w;
+                    }
+                }
+            }
+        }
+    }
+    std::memcpy(gradients, g.data(), g.size() * sizeof(double));
+    *emission_gradient = e;
+    return failures;
 }
 
 // bfo_trace_paths with ray cones (width, spread per path) in and at every terminal-ray origin out,

@@ -199,6 +199,22 @@ class Oracle(_Checker):
         self.lib.bfo_closest_hits(handle, rays, len(rays), hits)
         return hits
 
+    def weight_gradients(self, handle, inputs, options, path_adjoint, materials):
+        """Float64 dLoss/d(closure weight) per material and lane, and dLoss/d(emitter scale), along
+        the oracle's paths, from dLoss/dL per path and lane (bfo_weight_gradients)."""
+        import numpy as np
+        self._before_trace()
+        adj = np.ascontiguousarray(path_adjoint, np.float64).reshape(len(inputs), 4)
+        grads = np.zeros((materials, 4), np.float64)
+        emission = C.c_double()
+        f = self.lib.bfo_weight_gradients
+        f.argtypes = [C.c_void_p, C.POINTER(abi.PathInput), C.c_uint64, C.POINTER(abi.TransportOptions), C.c_void_p,
+                      C.c_void_p, C.POINTER(C.c_double)]
+        f.restype = C.c_int64
+        failures = f(handle, inputs, len(inputs), C.byref(options), adj.ctypes.data_as(C.c_void_p),
+                     grads.ctypes.data_as(C.c_void_p), C.byref(emission))
+        return grads, emission.value, failures
+
     def film(self, radiance, samples, sensor, width, height, precision):
         import numpy as np
         n = len(samples)

@@ -5,7 +5,8 @@ linear in each closure weight and in the emitted radiance, so those gradients ar
 derivatives of the rendered loss. They are compared with central finite differences of the same
 render (same sample indices), with a relative step of 1e-3 on the float32 parameter:
 tolerance 2e-3 of the finite difference, plus 1e-4 of the largest gradient tested. They are also
-compared with finite differences of the oracle's films (the CPU restatement of the reference
+compared with a float64 differentiation of the same paths on the CPU (within 1 %) and with finite
+differences of the oracle's films (the CPU restatement of the reference
 transport). There the tolerance is 3 %, because up to 1 % of paths may take a different route on
 the device (the sine/cosine rounding note of the parity tests).
 
@@ -170,6 +171,53 @@ def oracle_loss(oracle, builder, cam, sensor, target):
     film, _ = oracle.film(arrays(results)["radiance"], samples, sensor, WIDTH, HEIGHT, 1)  # compensated sums
     image = film[..., :3] / film[..., 3:4]
     return float(((image - target) ** 2).sum())
+
+
+def test_gradients_match_the_float64_path_replay(setup):
+    """The adjoint's weight and emission gradients against a float64 computation on the CPU along
+    the same paths (the oracle's float transport with the device's sine/cosine rounding): every
+    radiance contribution of every path is recorded and differentiated with respect to the closure
+    weights and the emitter scale in double precision (bfo_weight_gradients), with dLoss/dL per
+    path from the device film's image and the film's linear spectrum-to-rgb map. Within 1 %."""
+    torch, ctx, builder, cam, sensor, target = setup
+    loss, grads, emission, sums = gpu_adjoint(setup, builder)
+    image = (sums[..., :3] + sums[..., 4:7]) / (sums[..., 3:4] + sums[..., 7:8])
+    weight = sums[..., 3] + sums[..., 7]
+    oracle = Oracle(device_trig=True)
+    # the film's map from a sample's 4 radiance lanes to its rgb (linear: one film per unit lane)
+    one = (abi.SampleIndex * 1)()
+    basis = np.zeros((4, 3))
+    for lane in range(4):
+        radiance = np.zeros((1, 4), np.float32)
+        radiance[0, lane] = 1.0
+        film, _ = oracle.film(radiance, one, sensor, 1, 1, 1)
+        basis[lane] = film[0, 0, :3]
+    probe = np.array([[0.3, 1.7, 0.2, 2.5]], np.float32)
+    film, _ = oracle.film(probe, one, sensor, 1, 1, 1)
+    assert np.allclose(film[0, 0, :3], probe[0].astype(np.float64) @ basis, rtol=1e-6)
+    px, py, s = np.meshgrid(np.arange(WIDTH), np.arange(HEIGHT), np.arange(SPP), indexing="ij")
+    px, py, s = px.ravel(), py.ravel(), s.ravel()
+    samples = (abi.SampleIndex * len(px))()
+    for k in range(len(px)):
+        samples[k].pixel_x, samples[k].pixel_y = int(px[k]), int(py[k])
+        samples[k].sample_index, samples[k].seed = int(s[k]), SEED
+    rays = oracle.camera_rays(cam, samples)
+    inputs = (abi.PathInput * len(px))()
+    for k in range(len(px)):
+        inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
+    d_image = 2.0 * (image - target) / weight[..., None]  # dLoss / d(sample rgb), weight-1 samples
+    path_adjoint = d_image[py, px] @ basis.T
+    handle = oracle.scene(builder)
+    g64, e64, failures = oracle.weight_gradients(handle, inputs, transport_options(), path_adjoint,
+                                                 len(builder.materials))
+    oracle.destroy(handle)
+    assert failures <= max(1, len(px) // 10000)
+    scale = max(abs(g64[m, l]) for m, l in WEIGHTS)
+    for m, l in WEIGHTS:
+        print(f"weight ({m}, {l}): adjoint {grads[m, l]:.8g}, float64 replay {g64[m, l]:.8g}")
+        assert abs(grads[m, l] - g64[m, l]) <= 1e-2 * abs(g64[m, l]) + 1e-5 * scale, (m, l, grads[m, l], g64[m, l])
+    print(f"emission: adjoint {emission:.8g}, float64 replay {e64:.8g}")
+    assert abs(emission - e64) <= 1e-2 * abs(e64)
 
 
 def test_gradients_match_oracle_finite_differences(setup):

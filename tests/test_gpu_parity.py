@@ -150,11 +150,16 @@ def test_full_plain_frame_film_matches_oracle(ctx, oracle):
 
 def test_unsupported_features_are_rejected(ctx):
     builder = scenes.cornell_box(scenes.SceneBuilder(), with_spheres=False)
-    closures = scenes.lambertian([0.5] * 4) + scenes.lambertian([0.2] * 4)
-    builder.add_material(closures)
+    builder.add_material(scenes.lambertian([0.5] * 4), frame_mode=1)  # surface-tangent closure frame
     with pytest.raises(runtime.Bf200Error) as info:
         ctx.create_scene(builder)
     assert info.value.status == 4  # INVALID_STATE: no substitution
+    # component probabilities that are not a distribution are refused as ClosureMixture refuses them
+    builder = scenes.cornell_box(scenes.SceneBuilder(), with_spheres=False)
+    builder.add_material(scenes.lambertian([0.5] * 4) + scenes.lambertian([0.2] * 4), probabilities=[0.7, 0.7])
+    with pytest.raises(runtime.Bf200Error) as info:
+        ctx.create_scene(builder)
+    assert info.value.status == 1
 
 
 def test_scene_without_emitters_is_rejected(ctx):
@@ -171,3 +176,46 @@ def test_empty_batch_and_reuse(ctx):
     results, report = ctx.trace_paths(scene, (abi.PathInput * 0)(), options)
     assert len(results) == 0 and report.path_count == 0
     scene.close()
+
+
+@pytest.mark.parametrize("name", WORKLOADS)
+def test_film_within_the_monte_carlo_interval_of_the_compensated_film(ctx, oracle, golden, name):
+    """The device's float film against the oracle's compensated-double film (Film with Neumaier
+    sums) of the same paths: every pixel's mean within three standard errors of the double film's
+    Monte Carlo estimate (the per-pixel sample standard deviation over its samples / sqrt(spp)),
+    with a 1e-6 relative floor for pixels whose samples all agree."""
+    g = golden(name)
+    builder, options, _ = scenes.build_workload(name)
+    width, height, spp = 32, 32, 8
+    sensor = sensor_from_golden(g)
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+    scene = ctx.create_scene(builder)
+    sums, counts, report = ctx.render_film(scene, cam, sensor, options, spp, seed=0, precision=0)
+    scene.close()
+    assert (counts == spp).all() and report.failed_lanes == 0
+    device_mean = sums[..., :3].astype(np.float64) / sums[..., 3:4]
+    handle = oracle.scene(builder)
+    per_sample = []
+    for s in range(spp):  # one film per sample index: its pixels hold that sample's rgb
+        px, py = np.meshgrid(np.arange(width), np.arange(height), indexing="ij")
+        px, py = px.ravel(), py.ravel()
+        samples = (abi.SampleIndex * len(px))()
+        for k in range(len(px)):
+            samples[k].pixel_x, samples[k].pixel_y, samples[k].sample_index = int(px[k]), int(py[k]), s
+        rays = oracle.camera_rays(cam, samples)
+        inputs = (abi.PathInput * len(px))()
+        for k in range(len(px)):
+            inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
+        results, failures = oracle.trace(handle, inputs, options)
+        assert failures == 0
+        film, _ = oracle.film(arrays(results)["radiance"], samples, sensor, width, height, 1)
+        per_sample.append(film[..., :3] / film[..., 3:4])
+    oracle.destroy(handle)
+    per_sample = np.stack(per_sample)
+    mean = per_sample.mean(axis=0)
+    stderr = per_sample.std(axis=0, ddof=1) / np.sqrt(spp)
+    bound = 3.0 * stderr + 1e-6 * np.abs(mean)
+    inside = np.abs(device_mean - mean) <= bound
+    print(f"{name}: {inside.sum()}/{inside.size} pixel channels inside 3 standard errors; largest "
+          f"|difference| / standard error {np.max(np.abs(device_mean - mean) / np.maximum(stderr, 1e-30)):.3g}")
+    assert inside.all()
