@@ -29,8 +29,8 @@
 // path count, the stage lanes (camera, intersection, hit, miss, shade, shadow, continuation),
 // closure and light samples, shadow queries and terminated paths. The per-stage metrics
 // (dispatches, lanes and GPU time of the reference's own stage kernels) describe a kernel
-// structure bf200 does not have and stay zero; device_size_bytes() is 0 because bf200 does not
-// expose its arena size.
+// structure bf200 does not have and stay zero; device_size_bytes() is the context's device arena
+// and workspaces (bf200_context_device_bytes).
 #include <Blackframe/Backends/GPU/CUDA/WavefrontTransport.hpp>
 
 #include <cuda_runtime_api.h>
@@ -354,7 +354,12 @@ std::size_t CudaWavefrontTransportWorkspace::capacity() const noexcept {
 }
 
 std::size_t CudaWavefrontTransportWorkspace::device_size_bytes() const noexcept {
-    return 0U;
+    std::uint64_t bytes = 0;
+    if (storage_ == nullptr || storage_->context == nullptr ||
+        bf200_context_device_bytes(storage_->context, &bytes) != BLACKFRAME_STATUS_SUCCESS) {
+        return 0U;
+    }
+    return static_cast<std::size_t>(bytes);
 }
 
 std::int32_t CudaWavefrontTransportWorkspace::device_ordinal() const noexcept {

@@ -73,12 +73,23 @@ def build_library(force=False, verbose=False):
     return LIBRARY
 
 
-def build_oracle(reference_root=None, verbose=False):
+# Where this build script reads the reference sources for the checkers (oracle/_ref) when they are
+# present: BF200_REFERENCE, else the reference checkout of the build machine.
+REFERENCE_CHECKOUT = "/root/reference"
+
+
+def reference_root():
+    """The reference source tree the checkers are built from, or None where it is absent."""
+    root = os.environ.get("BF200_REFERENCE", REFERENCE_CHECKOUT)
+    return root if os.path.isdir(os.path.join(root, "Blackframe")) else None
+
+
+def build_oracle(reference=None, verbose=False):
     oracle_dir = os.path.join(REPO, "oracle")
     subprocess.run(["make", "-s", "-C", oracle_dir, "oracle"], check=True)
-    reference_root = reference_root or os.environ.get("BF200_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(reference_root, "Blackframe")):
-        subprocess.run(["make", "-s", "-j8", "-C", oracle_dir, "ref", "REF=" + reference_root], check=True)
+    reference = reference or reference_root()
+    if reference is not None:
+        subprocess.run(["make", "-s", "-j8", "-C", oracle_dir, "ref", "refcuda", "REF=" + reference], check=True)
 
 
 if __name__ == "__main__":

@@ -2279,6 +2279,26 @@ BF200_EXPORT blackframe_status bf200_scene_set_light_powers(bf200_scene* s, cons
     return BLACKFRAME_STATUS_SUCCESS;
 }
 
+// Device bytes the context holds: the wavefront arena and every grow-only workspace of the film,
+// batch, cone and adjoint entry points (not its scenes, which own their buffers).
+BF200_EXPORT blackframe_status bf200_context_device_bytes(const bf200_context* c, uint64_t* out_bytes) noexcept {
+    if (c == nullptr || out_bytes == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    uint64_t bytes = 0;
+    if (c->arena != nullptr) {
+        Wavefront w{};
+        bytes += carve_wavefront(nullptr, static_cast<uint32_t>(c->capacity), &w);
+    }
+    bytes += c->film_radiance_bytes + c->film_staging_bytes + c->batch_staging_bytes + c->lane_arena_bytes +
+             c->adjoint_workspace_bytes + c->cone_column_bytes;
+    for (size_t b : c->lane_radiance_bytes) {
+        bytes += b;
+    }
+    *out_bytes = bytes;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
 BF200_EXPORT blackframe_status bf200_scene_destroy(bf200_scene* s) noexcept {
     if (s == nullptr) {
         return BLACKFRAME_STATUS_INVALID_ARGUMENT;

@@ -9,7 +9,7 @@ writing. Each output row holds one dimension's parameters packed little-endian i
 words: the polynomial coefficient bits a (degree - 1 bits), then the initial direction numbers
 m_1 .. m_degree with m_k taking k bits.
 
-Usage: python gen_sobol_table.py [path to SobolDirectionNumbers.inc]
+Usage: python gen_sobol_table.py <path to the reference's Blackframe/Renderer/Source/SobolDirectionNumbers.inc>
 """
 import hashlib
 import os
@@ -17,7 +17,6 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SOURCE = "/root/reference/Blackframe/Renderer/Source/SobolDirectionNumbers.inc"
 DEGREE_ROW_ENDS = [1, 2, 4, 6, 12, 18, 36, 52, 100, 160, 336, 480, 1110, 1866, 3666, 5714, 13424, 21200]
 
 
@@ -29,7 +28,9 @@ def degree_for_row(row):
 
 
 def main():
-    source = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SOURCE
+    if len(sys.argv) != 2:
+        raise SystemExit(__doc__)
+    source = sys.argv[1]
     text = open(source).read()
     rows = [tuple(int(v, 16) for v in m) for m in re.findall(r"\{(0x[0-9a-fA-F]+)ULL,\s*(0x[0-9a-fA-F]+)ULL,\s*"
                                                              r"(0x[0-9a-fA-F]+)ULL\}", text)]

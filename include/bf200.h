@@ -471,6 +471,11 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_context_create(int32_t devic
     BF200_NOEXCEPT;
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_context_destroy(bf200_context* context)
     BF200_NOEXCEPT;
+/* Device memory the context holds: its wavefront arena and the grow-only workspaces of the film,
+ * batch, cone and adjoint calls, in bytes (not its scenes). Replaces
+ * CudaWavefrontTransportWorkspace::device_size_bytes (WavefrontTransport.hpp:166). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_context_device_bytes(const bf200_context* context,
+                                                                          uint64_t* out_bytes) BF200_NOEXCEPT;
 /* Last error text of a context (UTF-8, owned by the context, valid until the next call). */
 BF200_EXTERN_C BF200_EXPORT const char* bf200_context_last_error(const bf200_context* context)
     BF200_NOEXCEPT;

@@ -16,7 +16,9 @@ import subprocess
 
 import pytest
 
-REFERENCE = os.environ.get("BLACKFRAME_REFERENCE", "/root/reference")
+from bf200.build import reference_root
+
+REFERENCE = reference_root() or ""
 ROOTS = ["Core/Include", "Renderer/Include", "Engine/Include", "XPU/CUDA/Host/Include", "XPU/Shared/Include",
          "XPU/CUDA/Include", "Backends/GPU/CUDA/Include"]
 
