@@ -3,11 +3,14 @@ import numpy as np
 
 from bf200 import abi, scenes
 
-# Per-path radiance tolerance of the parity tests, and the share of paths allowed outside it: a
-# path may differ when a sine or cosine of a sampled angle rounds differently on the device (the
-# device uses the correctly rounded value, glibc's sinf/cosf are within 0.56 ulp).
+# Per-path radiance tolerance of the parity tests, and the share of paths allowed outside it.
+# Against the oracle in its device-rounding mode (Oracle(device_trig=True)) no path may diverge.
+# Against outputs of the reference itself, which takes sampled-angle sines and cosines from glibc's
+# sinf/cosf (within 0.56 ulp, off the correctly rounded value for about 1.3 % of arguments), a path
+# that draws such an angle continues one ulp apart: up to 1 % of paths may then differ.
 RELATIVE_TOLERANCE = 1e-5
-DIVERGED_FRACTION = 0.01
+DIVERGED_FRACTION = 0.0
+REFERENCE_DIVERGED_FRACTION = 0.01
 
 
 def golden_inputs(g):

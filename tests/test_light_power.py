@@ -51,7 +51,7 @@ def test_oracle_power_weighted_transport_matches_the_compiled_reference():
     if not reference_available():
         pytest.skip("oracle/_ref not built here")
     from bf200 import abi
-    from helpers import arrays, check_paths
+    from helpers import REFERENCE_DIVERGED_FRACTION, arrays, check_paths
     from test_gpu_light_power import light_powers, path_inputs, three_light_box
     builder = three_light_box()
     powers = light_powers(builder)
@@ -67,5 +67,6 @@ def test_oracle_power_weighted_transport_matches_the_compiled_reference():
     want, ref_failures = ref.trace(h, inputs, options)
     ref.destroy(h)
     assert failures == 0 and ref_failures == 0
-    exact, _ = check_paths(arrays(got), arrays(want), "oracle vs reference, power-weighted")
+    exact, _ = check_paths(arrays(got), arrays(want), "oracle vs reference, power-weighted",
+                           diverged=REFERENCE_DIVERGED_FRACTION)
     assert exact >= 0.99
