@@ -3,7 +3,8 @@ serialises a FrameScene into (SceneSoaHeader + 194 columns, 16-byte aligned, FNV
 hash over the blob with the hash field read as zero; layout of
 Blackframe/XPU/Shared/Include/Blackframe/XPU/Shared/SceneSoaAbi.hpp). bf200_scene_create_from_soa
 reads such blobs. Every material is written as spectral at the builder's packet; instances have no
-parents; there are no punctual lights or textures."""
+parents; punctual lights are written as SceneSoA serialises them (kind 0 point, 1 directional,
+2 spot; SceneSoA.cpp:241-300); there are no textures."""
 import struct
 
 import numpy as np
@@ -42,7 +43,8 @@ def write(builder):
                 if any(materials[inst.material_index].emitted_radiance[l] != 0 for l in range(4))]
     counts = {
         "object": len(instances), "geometry": len(geometries), "vertex": len(positions), "triangle": len(triangles),
-        "material": len(materials), "closure": len(closures), "instance": len(instances), "punctual": 0,
+        "material": len(materials), "closure": len(closures), "instance": len(instances),
+        "punctual": len(builder.punctual),
         "mesh_light": len(emissive), "environment": 1, "texture": 0, "image_texture": 0, "image_mip": 0,
         "image_texel": 0}
     nm = [desc.wavelength_nanometers[l] for l in range(4)]
@@ -101,6 +103,16 @@ def write(builder):
         col(79 + e, "f", [inst.world_to_object[e] for inst in instances])
         col(95 + e, "f", [inst.object_to_world[e] for inst in instances])
         col(111 + e, "f", [inst.world_to_object[e] for inst in instances])
+    lights = builder.punctual
+    col(127, "I", [{1: 0, 2: 1, 3: 2}[light.kind] for light in lights])
+    for a in range(3):
+        col(128 + a, "f", [light.position[a] for light in lights])
+        col(131 + a, "f", [light.position_error[a] for light in lights])
+        col(134 + a, "f", [light.direction[a] for light in lights])
+    col(137, "f", [light.inner_half_angle for light in lights])
+    col(138, "f", [light.outer_half_angle for light in lights])
+    for l in range(4):
+        col(139 + l, "f", [light.spectrum[l] for light in lights])
     col(143, "I", emissive)
     for l in range(4):
         col(144 + l, "f", [nm[l]])

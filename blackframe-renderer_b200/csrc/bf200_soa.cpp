@@ -8,7 +8,7 @@
 //
 // Kept alike with the reference, because a blob is an interchange format: the magic, version,
 // header size (4,848 bytes), column numbering, element sizes, the 16-byte column alignment, and
-// the hash. What the backend does not render is refused (no substitution): punctual lights,
+// the hash. What the backend does not render is refused (no substitution):
 // normal and bump maps, materials whose spectral packets differ.
 #include <cmath>
 #include <cstdint>
@@ -188,9 +188,6 @@ BF200_EXPORT blackframe_status bf200_scene_create_from_soa(bf200_context* contex
         if (hash != h.content_hash) {
             return refuse(BLACKFRAME_STATUS_INVALID_ARGUMENT, "scene SoA content hash mismatch");
         }
-        if (h.punctual_light_count != 0) {
-            return refuse(BLACKFRAME_STATUS_INVALID_STATE, "punctual lights are not supported (no substitution)");
-        }
         for (uint64_t m = 0; m < h.material_count; ++m) {
             if (read<uint8_t>(blob, h, material_normal_map_present, m) != 0 ||
                 read<uint8_t>(blob, h, material_bump_map_present, m) != 0) {
@@ -335,14 +332,40 @@ BF200_EXPORT blackframe_status bf200_scene_create_from_soa(bf200_context* contex
                 return refuse(BLACKFRAME_STATUS_INVALID_STATE, "scene SoA mesh lights differ from its emissive instances");
             }
         }
+        // punctual lights (SceneSoA.cpp:241-300: kind 0 point, 1 directional, 2 spot), first in the
+        // light registry
+        if (h.punctual_light_count > UINT32_MAX) {
+            return refuse(BLACKFRAME_STATUS_OUT_OF_RANGE, "scene SoA counts exceed the 32-bit descriptor");
+        }
+        std::vector<bf200_punctual_light_v1> punctual(h.punctual_light_count);
+        for (uint64_t k = 0; k < h.punctual_light_count; ++k) {
+            bf200_punctual_light_v1& out = punctual[k];
+            std::memset(&out, 0, sizeof(out));
+            const uint32_t kind = read<uint32_t>(blob, h, punctual_kind, k);
+            if (kind > 2U) {
+                return refuse(BLACKFRAME_STATUS_INVALID_ARGUMENT, "scene SoA punctual light of an unknown kind");
+            }
+            out.kind = kind == 0U ? BF200_PUNCTUAL_POINT : (kind == 1U ? BF200_PUNCTUAL_DIRECTIONAL : BF200_PUNCTUAL_SPOT);
+            for (uint32_t a = 0; a < 3; ++a) {
+                out.position[a] = read<float>(blob, h, punctual_kind + 1 + a, k);
+                out.position_error[a] = read<float>(blob, h, punctual_kind + 4 + a, k);
+                out.direction[a] = read<float>(blob, h, punctual_kind + 7 + a, k);
+            }
+            out.inner_half_angle = read<float>(blob, h, punctual_kind + 10, k);
+            out.outer_half_angle = read<float>(blob, h, punctual_kind + 11, k);
+            for (uint32_t l = 0; l < 4; ++l) {
+                out.spectrum[l] = read<float>(blob, h, punctual_kind + 12 + l, k);
+            }
+        }
         desc.struct_size = sizeof(desc);
+        desc.punctual_lights = punctual.empty() ? nullptr : punctual.data();
         desc.geometry_count = static_cast<uint32_t>(h.geometry_count);
         desc.vertex_count = static_cast<uint32_t>(h.vertex_count);
         desc.triangle_count = static_cast<uint32_t>(h.triangle_count);
         desc.material_count = static_cast<uint32_t>(h.material_count);
         desc.closure_count = static_cast<uint32_t>(h.closure_count);
         desc.instance_count = static_cast<uint32_t>(h.instance_count);
-        desc.punctual_light_count = 0;
+        desc.punctual_light_count = static_cast<uint32_t>(h.punctual_light_count);
         desc.geometries = geometries.data();
         desc.positions = positions.data();
         desc.normals = normals.data();

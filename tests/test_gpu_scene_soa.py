@@ -1,6 +1,7 @@
 """Scenes uploaded as scene SoA v4 blobs (bf200_scene_create_from_soa) render exactly like the same
 scenes given as descriptors: closest hits and per-path radiance bit for bit, for the Cornell box
-with spheres and for a many-instance (TLAS) scene."""
+with spheres, for a many-instance (TLAS) scene and for the layered Cornell box (closure mixtures,
+every closure kind, punctual lights in the blob's punctual columns)."""
 import numpy as np
 import pytest
 
@@ -9,10 +10,13 @@ from bf200 import abi, runtime, scenes, soa
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("kind", ["cornell", "instances"])
+@pytest.mark.parametrize("kind", ["cornell", "instances", "layered"])
 def test_soa_blob_scene_equals_descriptor_scene(kind):
     if kind == "cornell":
         builder = scenes.cornell_box(scenes.SceneBuilder(), with_spheres=True)
+        centre, spread = np.array([0.0, 0.0, 1.0]), 0.6
+    elif kind == "layered":
+        builder = scenes.cornell_layered(scenes.SceneBuilder())
         centre, spread = np.array([0.0, 0.0, 1.0]), 0.6
     else:
         builder = scenes.bvh_stress(scenes.SceneBuilder(environment=(0.5,) * 4), subdivisions=2)
