@@ -322,6 +322,7 @@ struct RayInv {
     F3 o;
     F3 inv;
     bool px, py, pz;  // axis-parallel components
+    bool parallel;    // any of them
 };
 
 __device__ __forceinline__ RayInv make_ray_inv(F3 o, F3 d) {
@@ -331,14 +332,27 @@ __device__ __forceinline__ RayInv make_ray_inv(F3 o, F3 d) {
     r.py = d.y == 0.0F;
     r.pz = d.z == 0.0F;
     r.inv = F3{r.px ? 0.0F : 1.0F / d.x, r.py ? 0.0F : 1.0F / d.y, r.pz ? 0.0F : 1.0F / d.z};
+    r.parallel = r.px || r.py || r.pz;
     return r;
 }
 
 // Conservative slab test: never rejects a box that contains a point of the ray with parameter
 // in [t_min, t_max] (each computed slab parameter is within a relative gamma(3) of the exact one,
-// and its sign is exact).
+// and its sign is exact). A ray with no axis-parallel component takes the first branch, where the
+// slack factors scale the largest entry and smallest exit parameter once: rounding a product with
+// a positive factor is monotonic, so that equals scaling each axis's parameter first.
 __device__ __forceinline__ bool slab(const RayInv& r, float lox, float hix, float loy, float hiy, float loz, float hiz,
                                      float t_min, float t_max, float& near_out) {
+    if (!r.parallel) {
+        const float ax = (lox - r.o.x) * r.inv.x, bx = (hix - r.o.x) * r.inv.x;
+        const float ay = (loy - r.o.y) * r.inv.y, by = (hiy - r.o.y) * r.inv.y;
+        const float az = (loz - r.o.z) * r.inv.z, bz = (hiz - r.o.z) * r.inv.z;
+        const float entry = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+        const float exit = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+        const float near = fmaxf(t_min, entry * kSlackLo);
+        near_out = near;
+        return near <= fminf(t_max, exit * kSlackHi);
+    }
     float near = t_min, far = t_max;
     bool inside = true;
     if (r.px) {
@@ -500,32 +514,32 @@ __device__ __forceinline__ void push_instances(const SceneView& s, const RayInv&
     }
 }
 
-// One instance-level entry of a walk. A TLAS node pushes the children the world ray meets within
-// [t_min, limit] (nodes as TLAS entries, instance leaves as one-instance ranges, the nearest on
-// top) and returns false. An instance range yields its first instance: false when the ray's
-// visibility mask excludes it or its world box is not met; otherwise the ray moves into its
-// object space, its BLAS root goes on above the rest of the range, and the call returns true.
-__device__ __forceinline__ bool instance_step(const SceneView& s, int entry, const RayInv& world, F3 o, F3 d,
-                                              float t_min, float limit, uint32_t mask, TraversalStack& stack,
-                                              int& sp, bool& failed, uint32_t& inst_out, F3& ro, F3& rd,
-                                              RayInv& r) {
-    const uint32_t code = static_cast<uint32_t>(entry - kInstanceEntry);
-    if (code & kTlasFlag) {
-        int kids[4];
-        const int count = hit_children(world, s.nodes[code & (kTlasFlag - 1U)], t_min, limit, kids);
+// Pushes the children a node visit returned, the farthest first so that the nearest comes next.
+// Children of a TLAS node go on as TLAS entries (nodes) and one-instance ranges (instance leaves).
+__device__ __forceinline__ void push_children(const int (&kids)[4], int count, bool tlas, TraversalStack& stack,
+                                              int& sp, bool& failed) {
 #pragma unroll
-        for (int k = 3; k >= 0; --k) {
-            if (k < count) {
-                if (sp < kTraversalStack) {
-                    stack.set(sp++, kids[k] >= 0 ? tlas_entry(kids[k])
-                                                 : instance_range(static_cast<uint32_t>(~kids[k]), 1U));
-                } else {
-                    failed = true;
-                }
+    for (int k = 3; k >= 0; --k) {
+        if (k < count) {
+            if (sp < kTraversalStack) {
+                const int kid = kids[k];
+                stack.set(sp++, !tlas ? kid
+                                      : kid >= 0 ? tlas_entry(kid) : instance_range(static_cast<uint32_t>(~kid), 1U));
+            } else {
+                failed = true;
             }
         }
-        return false;
     }
+}
+
+// An instance range (code = first << 15 | count) yields its first instance: false when the ray's
+// visibility mask excludes it or its world box is not met within [t_min, limit]; otherwise the ray
+// moves into its object space, its BLAS root goes on above the rest of the range, and the call
+// returns true.
+__device__ __forceinline__ bool enter_instance(const SceneView& s, uint32_t code, const RayInv& world, F3 o, F3 d,
+                                               float t_min, float limit, uint32_t mask, TraversalStack& stack,
+                                               int& sp, bool& failed, uint32_t& inst_out, F3& ro, F3& rd,
+                                               RayInv& r) {
     const uint32_t inst = code >> kInstanceBits, count = code & ((1U << kInstanceBits) - 1U);
     if (count > 1U) {
         stack.set(sp++, instance_range(inst + 1U, count - 1U));
@@ -564,33 +578,26 @@ struct Walk {
 };
 
 // Advances the walk until this lane holds a leaf (returned, in [-2^30, 0)) or its stack is empty
-// (returns 0). An instance range yields its first instance: skipped when the ray's visibility mask
-// excludes it or its world box is not met within [t_min, limit], otherwise the ray moves into its
-// object space and its BLAS root is pushed above the rest of the range. Children are pushed far
-// first, so the nearer one comes next.
+// (returns 0). TLAS and BLAS nodes share one visit (with the world or the object-space ray), so
+// lanes at either level run it together; instance ranges are entered by enter_instance. Children
+// are pushed far first, so the nearer one comes next.
 __device__ __forceinline__ int next_leaf(const SceneView& s, const RayInv& world, F3 o, F3 d, float t_min,
                                          float limit, uint32_t mask, TraversalStack& stack, Walk& w) {
     while (w.sp > 0) {
         const int entry = stack.get(--w.sp);
-        if (entry < kLeafEntryMin) {
-            instance_step(s, entry, world, o, d, t_min, limit, mask, stack, w.sp, w.failed, w.inst, w.ro, w.rd, w.r);
+        const uint32_t code = static_cast<uint32_t>(entry) ^ 0x80000000U;
+        const bool instance_level = entry < kLeafEntryMin;
+        if (instance_level && (code & kTlasFlag) == 0U) {
+            enter_instance(s, code, world, o, d, t_min, limit, mask, stack, w.sp, w.failed, w.inst, w.ro, w.rd, w.r);
             continue;
         }
-        if (entry < 0) {
+        if (!instance_level && entry < 0) {
             return entry;
         }
+        const int node = instance_level ? static_cast<int>(code & (kTlasFlag - 1U)) : entry;
         int kids[4];
-        const int count = hit_children(w.r, s.nodes[entry], t_min, limit, kids);
-#pragma unroll
-        for (int k = 3; k >= 0; --k) {
-            if (k < count) {
-                if (w.sp < kTraversalStack) {
-                    stack.set(w.sp++, kids[k]);
-                } else {
-                    w.failed = true;
-                }
-            }
-        }
+        const int count = hit_children(instance_level ? world : w.r, s.nodes[node], t_min, limit, kids);
+        push_children(kids, count, instance_level, stack, w.sp, w.failed);
     }
     return 0;
 }
@@ -704,9 +711,12 @@ __device__ ClosestResult closest_hit(const SceneView& s, F3 o, F3 d, float t_min
     return closest_end(c);
 }
 
-// Any hit in [t_min, t_max] (AccelBackend.cpp:114-147). One loop serves both levels, and leaves
-// are tested as soon as they are met so a lane stops at its first hit. Returns 1 occluded,
-// 0 clear, -1 failure.
+// Any hit in [t_min, t_max] (AccelBackend.cpp:114-147). One loop serves both levels, with one
+// visit for TLAS and BLAS nodes as in next_leaf; leaves go through the stack like nodes (the
+// nearest child on top), so every pass of the loop handles one entry per lane -- a node, an
+// instance range or one leaf -- and a lane stops at its first hit.
+// The set of leaves met does not depend on the order (the interval never shrinks), so neither does
+// the answer. Returns 1 occluded, 0 clear, -1 failure.
 template <bool SPH>
 __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max, uint32_t mask,
                        TraversalStack& stack) {
@@ -718,28 +728,15 @@ __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
     F3 ro = o, rd = d;
     while (sp > 0) {
         const int entry = stack.get(--sp);
-        if (entry < kLeafEntryMin) {
+        const uint32_t code = static_cast<uint32_t>(entry) ^ 0x80000000U;
+        const bool instance_level = entry < kLeafEntryMin;
+        if (instance_level && (code & kTlasFlag) == 0U) {
             uint32_t inst = 0U;
-            instance_step(s, entry, world, o, d, t_min, t_max, mask, stack, sp, failed, inst, ro, rd, r);
+            enter_instance(s, code, world, o, d, t_min, t_max, mask, stack, sp, failed, inst, ro, rd, r);
             continue;
         }
-        int kids[4];
-        const int count = hit_children(r, s.nodes[entry], t_min, t_max, kids);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (k >= count) {
-                break;
-            }
-            const int child = kids[k];
-            if (child >= 0) {
-                if (sp < kTraversalStack) {
-                    stack.set(sp++, child);
-                } else {
-                    failed = true;
-                }
-                continue;
-            }
-            const uint32_t packed = static_cast<uint32_t>(~child);
+        if (!instance_level && entry < 0) {
+            const uint32_t packed = static_cast<uint32_t>(~entry);
             const uint32_t first = packed >> kLeafCountBits;
             const uint32_t n = (packed & (kMaxLeafSize - 1)) + 1U;
             if (SPH && n == kSphereLeafCount) {
@@ -764,7 +761,12 @@ __device__ int any_hit(const SceneView& s, F3 o, F3 d, float t_min, float t_max,
                     failed = true;
                 }
             }
+            continue;
         }
+        const int node = instance_level ? static_cast<int>(code & (kTlasFlag - 1U)) : entry;
+        int kids[4];
+        const int count = hit_children(instance_level ? world : r, s.nodes[node], t_min, t_max, kids);
+        push_children(kids, count, instance_level, stack, sp, failed);
     }
     return failed ? -1 : 0;
 }
