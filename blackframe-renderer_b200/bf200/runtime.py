@@ -39,6 +39,12 @@ EXPORTED_SYMBOLS = [
     "bf200_light_tree_probability",
     "bf200_light_tree_select_device",
     "bf200_scene_set_light_tree",
+    "bf200_environment_map_create",
+    "bf200_environment_map_destroy",
+    "bf200_environment_map_sample",
+    "bf200_environment_map_pdf",
+    "bf200_environment_map_le",
+    "bf200_environment_map_power",
 ]
 
 

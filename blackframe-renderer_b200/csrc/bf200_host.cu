@@ -23,6 +23,7 @@
 
 #include "bf200.h"
 #include "bf200_device.cuh"
+#include "bf200_envmap.h"
 #include "bf200_kernels.h"
 #include "bf200_light_tree.h"
 #include "bf200_sobol.h"
@@ -3421,6 +3422,242 @@ BF200_EXPORT blackframe_status bf200_occlusions(bf200_context* c, const bf200_sc
         return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null output");
     }
     return run_queries(c, s, rays, n, nullptr, occluded);
+}
+
+// --------------------------------------------------------------------------------------------
+// Environment-map light (EnvironmentLights.hpp:468-1075): host tables, device batch queries
+// --------------------------------------------------------------------------------------------
+
+struct bf200_environment_map {
+    bf200_context* context = nullptr;
+    bf200::EnvironmentTables tables;
+    void* device = nullptr;  // texels, azimuth, cosine, row CDF, column CDFs, densities
+    bf200::EnvironmentView view{};
+};
+
+namespace {
+
+bool same_packet(const bf200_environment_map* m, const float nanometers[4]) {
+    for (int lane = 0; lane < 4; ++lane) {
+        if (nanometers[lane] != m->tables.nanometers[lane]) {
+            return false;
+        }
+    }
+    return true;
+}
+
+// Validates a batch call; on success leaves the map's device current.
+blackframe_status environment_batch_check(bf200_context* c, const bf200_environment_map* m,
+                                          const float nanometers[4], const void* in, uint64_t n, const void* out) {
+    if (c == nullptr || m == nullptr || nanometers == nullptr || (n != 0 && (in == nullptr || out == nullptr))) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (m->context != c) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "environment map belongs to another context");
+    }
+    if (!same_packet(m, nanometers)) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
+                    "A packet-bound environment map cannot be evaluated at different wavelengths.");
+    }
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "cudaSetDevice failed");
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+BF200_EXPORT blackframe_status bf200_environment_map_create(bf200_context* c, const bf200_environment_map_desc_v1* d,
+                                                            bf200_environment_map** out) noexcept {
+    if (c == nullptr || d == nullptr || out == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    *out = nullptr;
+    if (d->struct_size < sizeof(bf200_environment_map_desc_v1)) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "environment map descriptor too small");
+    }
+    std::unique_ptr<bf200_environment_map> m(new (std::nothrow) bf200_environment_map);
+    if (!m) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "out of host memory");
+    }
+    const char* message = nullptr;
+    int code = bf200::kEnvironmentOk;
+    try {
+        code = bf200::build_environment_tables(d->width, d->height, d->texels, d->nanometers, d->environment_to_world,
+                                               m->tables, message);
+    } catch (const std::bad_alloc&) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "Environment-map distribution exhausted host memory.");
+    }
+    if (code != bf200::kEnvironmentOk) {
+        return fail(c,
+                    code == bf200::kEnvironmentExhausted ? BLACKFRAME_STATUS_OUT_OF_RANGE
+                                                         : BLACKFRAME_STATUS_INVALID_ARGUMENT,
+                    message != nullptr ? message : "invalid environment map");
+    }
+    const bf200::EnvironmentTables& t = m->tables;
+    const size_t parts[6] = {t.texels.size(), t.azimuth.size(), t.cosine.size(), t.row_cdf.size(),
+                             t.column_cdfs.size(), t.density.size()};
+    const std::vector<float>* sources[6] = {&t.texels, &t.azimuth, &t.cosine, &t.row_cdf, &t.column_cdfs, &t.density};
+    size_t total = 0;
+    for (const size_t p : parts) {
+        total += p;
+    }
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "cudaSetDevice failed");
+    }
+    cudaError_t e = cudaMalloc(&m->device, total * sizeof(float));
+    float* base = static_cast<float*>(m->device);
+    const float* placed[6] = {};
+    size_t offset = 0;
+    for (int k = 0; k < 6 && e == cudaSuccess; ++k) {
+        placed[k] = base + offset;
+        e = cudaMemcpy(base + offset, sources[k]->data(), parts[k] * sizeof(float), cudaMemcpyHostToDevice);
+        offset += parts[k];
+    }
+    if (e != cudaSuccess) {
+        cudaFree(m->device);
+        m->device = nullptr;
+        return cuda_fail(c, e, "environment map upload");
+    }
+    bf200::EnvironmentView& v = m->view;
+    v.width = t.width;
+    v.height = t.height;
+    v.texels = placed[0];
+    v.azimuth = placed[1];
+    v.cosine = placed[2];
+    v.row_cdf = placed[3];
+    v.column_cdfs = placed[4];
+    v.density = placed[5];
+    for (int k = 0; k < 9; ++k) {
+        v.matrix[k] = t.matrix[k];
+        v.inverse[k] = t.inverse[k];
+    }
+    v.black = t.black ? 1U : 0U;
+    m->context = c;
+    *out = m.release();
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT blackframe_status bf200_environment_map_destroy(bf200_environment_map* m) noexcept {
+    if (m == nullptr) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    if (m->device != nullptr && m->context != nullptr) {
+        cudaSetDevice(m->context->device);
+        cudaFree(m->device);
+    }
+    delete m;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+extern "C++" {
+namespace {
+
+// One device batch: copy `in_bytes` in, launch, copy the outputs back, synchronize.
+template <typename Launch>
+blackframe_status environment_batch(bf200_context* c, const void* in, size_t in_bytes, void* out0, size_t out0_bytes,
+                                    void* out1, size_t out1_bytes, Launch launch) {
+    void* d_in = nullptr;
+    void* d_out0 = nullptr;
+    void* d_out1 = nullptr;
+    cudaError_t e = cudaMalloc(&d_in, in_bytes);
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&d_out0, out0_bytes);
+    }
+    if (e == cudaSuccess && out1 != nullptr) {
+        e = cudaMalloc(&d_out1, out1_bytes);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(d_in, in, in_bytes, cudaMemcpyHostToDevice, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = launch(d_in, d_out0, d_out1);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(out0, d_out0, out0_bytes, cudaMemcpyDeviceToHost, c->stream);
+    }
+    if (e == cudaSuccess && out1 != nullptr) {
+        e = cudaMemcpyAsync(out1, d_out1, out1_bytes, cudaMemcpyDeviceToHost, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(d_in);
+    cudaFree(d_out0);
+    cudaFree(d_out1);
+    return e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "environment map query");
+}
+
+}  // namespace
+}  // extern "C++"
+
+BF200_EXPORT blackframe_status bf200_environment_map_sample(bf200_context* c, const bf200_environment_map* m,
+                                                            const float nanometers[4], const float* canonical,
+                                                            uint64_t n, bf200_environment_sample_v1* samples) noexcept {
+    const blackframe_status st = environment_batch_check(c, m, nanometers, canonical, n, samples);
+    if (st != BLACKFRAME_STATUS_SUCCESS || n == 0) {
+        return st;
+    }
+    return environment_batch(c, canonical, n * 2 * sizeof(float), samples, n * sizeof(bf200_environment_sample_v1),
+                             nullptr, 0, [&](void* in, void* out0, void*) {
+                                 return bf200::launch_environment_sample(
+                                     m->view, static_cast<const float2*>(in), n,
+                                     static_cast<bf200_environment_sample_v1*>(out0), c->stream);
+                             });
+}
+
+BF200_EXPORT blackframe_status bf200_environment_map_pdf(bf200_context* c, const bf200_environment_map* m,
+                                                         const float nanometers[4], const float* directions,
+                                                         uint64_t n, float* pdf, uint32_t* status) noexcept {
+    blackframe_status st = environment_batch_check(c, m, nanometers, directions, n, pdf);
+    if (st == BLACKFRAME_STATUS_SUCCESS && n != 0 && status == nullptr) {
+        st = fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null status");
+    }
+    if (st != BLACKFRAME_STATUS_SUCCESS || n == 0) {
+        return st;
+    }
+    return environment_batch(c, directions, n * 3 * sizeof(float), pdf, n * sizeof(float), status,
+                             n * sizeof(uint32_t), [&](void* in, void* out0, void* out1) {
+                                 return bf200::launch_environment_pdf(m->view, static_cast<const float*>(in), n,
+                                                                      static_cast<float*>(out0),
+                                                                      static_cast<uint32_t*>(out1), c->stream);
+                             });
+}
+
+BF200_EXPORT blackframe_status bf200_environment_map_le(bf200_context* c, const bf200_environment_map* m,
+                                                        const float nanometers[4], const float* directions, uint64_t n,
+                                                        float* radiance, uint32_t* status) noexcept {
+    blackframe_status st = environment_batch_check(c, m, nanometers, directions, n, radiance);
+    if (st == BLACKFRAME_STATUS_SUCCESS && n != 0 && status == nullptr) {
+        st = fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null status");
+    }
+    if (st != BLACKFRAME_STATUS_SUCCESS || n == 0) {
+        return st;
+    }
+    return environment_batch(c, directions, n * 3 * sizeof(float), radiance, n * 4 * sizeof(float), status,
+                             n * sizeof(uint32_t), [&](void* in, void* out0, void* out1) {
+                                 return bf200::launch_environment_le(m->view, static_cast<const float*>(in), n,
+                                                                     static_cast<float4*>(out0),
+                                                                     static_cast<uint32_t*>(out1), c->stream);
+                             });
+}
+
+BF200_EXPORT blackframe_status bf200_environment_map_power(bf200_context* c, const bf200_environment_map* m,
+                                                           const float nanometers[4], const float bounds_min[3],
+                                                           const float bounds_max[3], float power[4]) noexcept {
+    if (c == nullptr || m == nullptr || nanometers == nullptr || bounds_min == nullptr || bounds_max == nullptr ||
+        power == nullptr) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (!same_packet(m, nanometers)) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT,
+                    "A packet-bound environment map cannot be evaluated at different wavelengths.");
+    }
+    const char* message = nullptr;
+    if (bf200::environment_power(m->tables, bounds_min, bounds_max, power, message) != bf200::kEnvironmentOk) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, message != nullptr ? message : "invalid bounds");
+    }
+    return BLACKFRAME_STATUS_SUCCESS;
 }
 
 // --------------------------------------------------------------------------------------------

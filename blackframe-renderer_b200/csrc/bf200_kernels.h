@@ -41,4 +41,13 @@ cudaError_t launch_adjoint_image(const float4* film32, const double* film64, con
 cudaError_t launch_queries(const SceneView& s, const bf200_ray_v1* rays, uint64_t n, bf200_hit_v1* hits,
                            uint32_t* occluded, cudaStream_t stream);
 
+// Environment-map light batches (bf200_envmap.cu).
+struct EnvironmentView;
+cudaError_t launch_environment_sample(const EnvironmentView& v, const float2* canonical, uint64_t n,
+                                      bf200_environment_sample_v1* out, cudaStream_t stream);
+cudaError_t launch_environment_pdf(const EnvironmentView& v, const float* directions, uint64_t n, float* pdf,
+                                   uint32_t* status, cudaStream_t stream);
+cudaError_t launch_environment_le(const EnvironmentView& v, const float* directions, uint64_t n, float4* radiance,
+                                  uint32_t* status, cudaStream_t stream);
+
 }  // namespace bf200

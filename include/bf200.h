@@ -816,6 +816,70 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_occlusions(bf200_context* co
                                                                 uint64_t ray_count,
                                                                 uint32_t* occluded) BF200_NOEXCEPT;
 
+/* Environment-map light (EnvironmentLights.hpp:468-1075, EnvironmentMapLightT<float>): a
+ * packet-bound, piecewise-constant latitude-longitude map, importance-sampled by texel (mean packet
+ * radiance times the texel's exact solid angle). Local +Y is north, u = 0 is the +X seam and u
+ * grows toward +Z; `environment_to_world` (a unit quaternion x, y, z, w) rotates local directions
+ * into world space. bf200_environment_map_create replaces EnvironmentMapLightT::create
+ * (EnvironmentLights.hpp:470-733): the sampling tables are built on the host exactly as there and
+ * uploaded to the context's device. The batch calls replace sample_li (:750-822), pdf_li
+ * (:824-843), le (:845-851) and power (:853-885); like the reference they require the packet the
+ * map was created with (`nanometers`, compared exactly), and report each query's failure in its
+ * own status (0: the reference returns a value) -- see bf200_environment_status. Host pointers.
+ * On the device, sines, cosines and the arctangent are the double-precision values rounded once
+ * to float; the reference calls the C library's float functions, which differ by an ulp on a
+ * small share of angles. */
+typedef struct bf200_environment_map bf200_environment_map;
+typedef struct bf200_environment_map_desc_v1 {
+    uint32_t struct_size;
+    uint32_t width;
+    uint32_t height;
+    uint32_t reserved;
+    const float* texels;             /* width * height records of 4 lanes, row-major, row 0 at +Y */
+    float nanometers[4];             /* the wavelength packet the map is bound to */
+    float environment_to_world[4];   /* unit quaternion x, y, z, w */
+} bf200_environment_map_desc_v1;
+
+/* Per-query status of the batch calls. */
+typedef enum bf200_environment_status {
+    BF200_ENVIRONMENT_OK = 0,
+    BF200_ENVIRONMENT_INVALID_SAMPLE = 1,     /* canonical sample outside [0, 1)^2 */
+    BF200_ENVIRONMENT_INVALID_DIRECTION = 2,  /* pdf: not a finite unit vector; le: not representable */
+    BF200_ENVIRONMENT_ESCAPED = 3,            /* a lookup escaped its angular partition or CDF */
+    BF200_ENVIRONMENT_UNSTABLE = 4,           /* the rotation cannot keep the selected texel */
+    BF200_ENVIRONMENT_NOT_REPRESENTABLE = 5   /* an interior sample or its direction is not representable */
+} bf200_environment_status;
+
+/* One sample_li: `valid` 0 with status OK is the reference's empty optional (a black map). The
+ * sample is infinite: solid-angle pdf, no distance. */
+typedef struct bf200_environment_sample_v1 {
+    float direction[3];  /* world direction to the light */
+    float radiance[4];   /* incident radiance, packet lanes */
+    float pdf;           /* solid-angle density */
+    uint32_t status;
+    uint32_t valid;
+} bf200_environment_sample_v1;
+
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_environment_map_create(
+    bf200_context* context, const bf200_environment_map_desc_v1* desc, bf200_environment_map** map) BF200_NOEXCEPT;
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_environment_map_destroy(bf200_environment_map* map) BF200_NOEXCEPT;
+/* canonical: 2 floats (u, v) per query; u picks the column within the row that v picks. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_environment_map_sample(
+    bf200_context* context, const bf200_environment_map* map, const float nanometers[4], const float* canonical,
+    uint64_t count, bf200_environment_sample_v1* samples) BF200_NOEXCEPT;
+/* directions: 3 floats per query (unit vectors toward the light). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_environment_map_pdf(
+    bf200_context* context, const bf200_environment_map* map, const float nanometers[4], const float* directions,
+    uint64_t count, float* pdf, uint32_t* status) BF200_NOEXCEPT;
+/* directions: 3 floats per query (escaped-ray directions, any length); radiance: 4 per query. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_environment_map_le(
+    bf200_context* context, const bf200_environment_map* map, const float nanometers[4], const float* directions,
+    uint64_t count, float* radiance, uint32_t* status) BF200_NOEXCEPT;
+/* Power over the bounding sphere of the scene bounds [lo, hi] (host arithmetic). */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_environment_map_power(
+    bf200_context* context, const bf200_environment_map* map, const float nanometers[4], const float bounds_min[3],
+    const float bounds_max[3], float power[4]) BF200_NOEXCEPT;
+
 /* The render interface table returned by get_interface(BF200_RENDER_INTERFACE_ID, 1, 0). */
 typedef struct bf200_render_api_v1 {
     uint32_t struct_size;

@@ -498,3 +498,93 @@ class ReferenceCuda:
         if rc != 0:
             raise CheckerError(self.last_error())
         return out, report, ms.value
+
+
+class EnvironmentCheck:
+    """An environment-map light on the CPU: the oracle's restatement (liboracle.so, prefix "bfo",
+    trig rounding chosen by device_trig) or the reference's own EnvironmentMapLightT<float>
+    (libbfref.so, prefix "bfref"). Same call shapes as bf200.envmap.EnvironmentMap; creation
+    failures raise CheckerError with the code (1 invalid argument, 2 resource exhausted)."""
+
+    def __init__(self, path, prefix, texels, nanometers, quaternion=(0.0, 0.0, 0.0, 1.0), device_trig=False):
+        import numpy as np
+        if not os.path.exists(path):
+            raise CheckerError(f"{path} is not built")
+        self.np = np
+        self.lib = C.CDLL(path)
+        self.prefix = prefix
+        self.device_trig = bool(device_trig)
+        vp, u64 = C.c_void_p, C.c_uint64
+        create = getattr(self.lib, prefix + "_envmap_create")
+        create.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp, C.POINTER(C.c_int), C.c_char_p, C.c_size_t]
+        create.restype = vp
+        getattr(self.lib, prefix + "_envmap_destroy").argtypes = [vp]
+        trig = [C.c_int] if prefix == "bfo" else []
+        getattr(self.lib, prefix + "_envmap_sample").argtypes = [vp, vp, u64] + trig + [vp]
+        getattr(self.lib, prefix + "_envmap_pdf").argtypes = [vp, vp, u64] + trig + [vp, vp]
+        getattr(self.lib, prefix + "_envmap_le").argtypes = [vp, vp, u64] + trig + [vp, vp]
+        power = getattr(self.lib, prefix + "_envmap_power")
+        power.argtypes = [vp, vp, vp, vp]
+        power.restype = C.c_int
+        self.texels = np.ascontiguousarray(texels, np.float32)
+        height, width, _ = self.texels.shape
+        nm = np.ascontiguousarray(nanometers, np.float32).reshape(4)
+        q = np.ascontiguousarray(quaternion, np.float32).reshape(4)
+        code = C.c_int(0)
+        message = C.create_string_buffer(256)
+        self.handle = create(width, height, self._ptr(self.texels), self._ptr(nm), self._ptr(q), C.byref(code), message,
+                             256)
+        if not self.handle:
+            self.code = code.value
+            raise CheckerError(f"{code.value}: {message.value.decode()}")
+
+    @staticmethod
+    def _ptr(a):
+        return a.ctypes.data_as(C.c_void_p)
+
+    def _trig(self):
+        return [int(self.device_trig)] if self.prefix == "bfo" else []
+
+    def sample(self, canonical):
+        from bf200.envmap import SAMPLE_DTYPE
+        u = self.np.ascontiguousarray(canonical, self.np.float32).reshape(-1, 2)
+        out = self.np.zeros(len(u), SAMPLE_DTYPE)
+        getattr(self.lib, self.prefix + "_envmap_sample")(self.handle, self._ptr(u), len(u), *self._trig(),
+                                                          self._ptr(out))
+        return out
+
+    def pdf(self, directions):
+        d = self.np.ascontiguousarray(directions, self.np.float32).reshape(-1, 3)
+        pdf, status = self.np.zeros(len(d), self.np.float32), self.np.zeros(len(d), self.np.uint32)
+        getattr(self.lib, self.prefix + "_envmap_pdf")(self.handle, self._ptr(d), len(d), *self._trig(), self._ptr(pdf),
+                                                       self._ptr(status))
+        return pdf, status
+
+    def le(self, directions):
+        d = self.np.ascontiguousarray(directions, self.np.float32).reshape(-1, 3)
+        radiance = self.np.zeros((len(d), 4), self.np.float32)
+        status = self.np.zeros(len(d), self.np.uint32)
+        getattr(self.lib, self.prefix + "_envmap_le")(self.handle, self._ptr(d), len(d), *self._trig(),
+                                                      self._ptr(radiance), self._ptr(status))
+        return radiance, status
+
+    def power(self, lo, hi):
+        """(status, power[4]); status 0 when the call returns a value."""
+        lo = self.np.ascontiguousarray(lo, self.np.float32).reshape(3)
+        hi = self.np.ascontiguousarray(hi, self.np.float32).reshape(3)
+        out = self.np.zeros(4, self.np.float32)
+        rc = getattr(self.lib, self.prefix + "_envmap_power")(self.handle, self._ptr(lo), self._ptr(hi), self._ptr(out))
+        return rc, out
+
+    def close(self):
+        if self.handle:
+            getattr(self.lib, self.prefix + "_envmap_destroy")(self.handle)
+            self.handle = None
+
+
+def oracle_environment(texels, nanometers, quaternion=(0.0, 0.0, 0.0, 1.0), device_trig=False):
+    return EnvironmentCheck(ORACLE_LIB, "bfo", texels, nanometers, quaternion, device_trig)
+
+
+def reference_environment(texels, nanometers, quaternion=(0.0, 0.0, 0.0, 1.0)):
+    return EnvironmentCheck(REFERENCE_LIB, "bfref", texels, nanometers, quaternion)
