@@ -61,6 +61,7 @@ STAGE_KERNELS = {"trace": "k_trace", "shade": "k_shade<kind> x4 + route/shadow c
 # kernels' launches at 2,097,152 slots)
 MEASURED_TRAFFIC_PER_UNIT = {
     "cornell_spheres_256": {"trace": 56.5, "shade": 372.0, "occlude": None},
+    "bvh_stress_1080p": {"trace": 203.0, "shade": None, "occlude": None},
 }
 
 
