@@ -45,6 +45,8 @@ EXPORTED_SYMBOLS = [
     "bf200_environment_map_pdf",
     "bf200_environment_map_le",
     "bf200_environment_map_power",
+    "bf200_camera_rays",
+    "bf200_compact_routes_device",
 ]
 
 
@@ -380,6 +382,28 @@ class Context:
                                                 C.byref(request), C.byref(options), C.byref(f),
                                                 C.byref(report)), "render_film")
         return sums, counts, report
+
+    def compact_routes_device(self, keys_ptr, count, routes, queue_ptr, offsets_ptr):
+        """bf200_compact_routes_device on device buffers (uint8 keys, uint32 queue and offsets)."""
+        lib = library()
+        lib.bf200_compact_routes_device.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                                    C.c_void_p]
+        self._check(lib.bf200_compact_routes_device(self.handle, keys_ptr, count, routes, queue_ptr, offsets_ptr),
+                    "compact_routes_device")
+
+    def camera_rays(self, camera, samples, sampler=0):
+        """Primary rays of abi.SampleIndex records through `camera` (abi.Camera), generated on the
+        device; returns (abi.Ray array, numpy uint32 statuses)."""
+        n = len(samples)
+        rays = (abi.Ray * n)()
+        status = np.zeros(n, np.uint32)
+        lib = library()
+        lib.bf200_camera_rays.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p,
+                                          C.c_void_p]
+        self._check(lib.bf200_camera_rays(self.handle, C.byref(camera), C.cast(samples, C.c_void_p), n, sampler,
+                                          C.cast(rays, C.c_void_p), status.ctypes.data_as(C.c_void_p)),
+                    "camera_rays")
+        return rays, status
 
     def closest_hits(self, scene, rays):
         n = len(rays)

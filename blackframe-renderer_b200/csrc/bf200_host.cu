@@ -3424,6 +3424,89 @@ BF200_EXPORT blackframe_status bf200_occlusions(bf200_context* c, const bf200_sc
     return run_queries(c, s, rays, n, nullptr, occluded);
 }
 
+BF200_EXPORT blackframe_status bf200_compact_routes_device(bf200_context* c, const uint8_t* keys, uint32_t n,
+                                                           uint32_t routes, uint32_t* queue, uint32_t* offsets) noexcept {
+    if (c == nullptr || offsets == nullptr || (n != 0 && (keys == nullptr || queue == nullptr))) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (routes == 0U || routes > kCompactMaxRoutes) {
+        return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "routes must be 1..4");
+    }
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "cudaSetDevice failed");
+    }
+    const uint32_t tiles = n == 0U ? 1U : (n + kCompactTile - 1U) / kCompactTile;
+    uint32_t* tile_counts = nullptr;
+    cudaError_t e = cudaMalloc(&tile_counts, static_cast<size_t>(routes) * tiles * sizeof(uint32_t));
+    uint32_t launches = 0;
+    if (e == cudaSuccess) {
+        e = launch_compaction(keys, n, routes, tile_counts, queue, offsets, nullptr, nullptr, c->stream, &launches);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(tile_counts);
+    return e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "route compaction");
+}
+
+BF200_EXPORT blackframe_status bf200_camera_rays(bf200_context* c, const bf200_camera_v1* cam,
+                                                 const bf200_sample_index_v1* samples, uint64_t n, uint32_t sampler,
+                                                 bf200_ray_v1* rays, uint32_t* status) noexcept {
+    if (c == nullptr || cam == nullptr || (n != 0 && (samples == nullptr || rays == nullptr || status == nullptr))) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    if (sampler != BF200_SAMPLER_HASH && sampler != BF200_SAMPLER_OWEN_SOBOL) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "unknown sampler");
+    }
+    if (cam->width == 0U || cam->height == 0U) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "camera without pixels");
+    }
+    if (n == 0) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "cudaSetDevice failed");
+    }
+    bf200_transport_options_v1 o{};
+    o.sampler = sampler;
+    const uint32_t* sobol = nullptr;
+    if (const auto st = sobol_table(c, o, &sobol); st != BLACKFRAME_STATUS_SUCCESS) {
+        return st;
+    }
+    bf200_film_request_v1 req{};
+    const PathSource src = film_source(cam, &req, 0, 0, nullptr, sobol);
+    void* d_samples = nullptr;
+    void* d_rays = nullptr;
+    void* d_status = nullptr;
+    cudaError_t e = cudaMalloc(&d_samples, n * sizeof(bf200_sample_index_v1));
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&d_rays, n * sizeof(bf200_ray_v1));
+    }
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&d_status, n * sizeof(uint32_t));
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(d_samples, samples, n * sizeof(bf200_sample_index_v1), cudaMemcpyHostToDevice, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = launch_camera_rays(src, static_cast<const bf200_sample_index_v1*>(d_samples), n,
+                               static_cast<bf200_ray_v1*>(d_rays), static_cast<uint32_t*>(d_status), c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(rays, d_rays, n * sizeof(bf200_ray_v1), cudaMemcpyDeviceToHost, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(status, d_status, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(d_samples);
+    cudaFree(d_rays);
+    cudaFree(d_status);
+    return e == cudaSuccess ? BLACKFRAME_STATUS_SUCCESS : cuda_fail(c, e, "camera rays");
+}
+
 // --------------------------------------------------------------------------------------------
 // Environment-map light (EnvironmentLights.hpp:468-1075): host tables, device batch queries
 // --------------------------------------------------------------------------------------------

@@ -41,6 +41,10 @@ cudaError_t launch_adjoint_image(const float4* film32, const double* film64, con
 cudaError_t launch_queries(const SceneView& s, const bf200_ray_v1* rays, uint64_t n, bf200_hit_v1* hits,
                            uint32_t* occluded, cudaStream_t stream);
 
+// Primary rays of (pixel, sample) records through the camera of `src` (k_camera_rays): one ray and
+// one lane status per record.
+cudaError_t launch_camera_rays(const PathSource& src, const bf200_sample_index_v1* samples, uint64_t n,
+                               bf200_ray_v1* rays, uint32_t* status, cudaStream_t stream);
 // Environment-map light batches (bf200_envmap.cu).
 struct EnvironmentView;
 cudaError_t launch_environment_sample(const EnvironmentView& v, const float2* canonical, uint64_t n,

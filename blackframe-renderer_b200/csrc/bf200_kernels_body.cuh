@@ -993,6 +993,45 @@ static __device__ void finish_path(const Wavefront& w, const PathSource& src, ui
 
 #ifdef BF200_KERNELS_MAIN_TU
 // ------------------------------------------------------------------------------------------------
+// k_camera_rays: primary rays of given (pixel, sample) records, as start_path generates them
+// ------------------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(128) k_camera_rays(PathSource src, const bf200_sample_index_v1* samples, uint64_t n,
+                                                     bf200_ray_v1* rays, uint32_t* status) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const bf200_sample_index_v1 si = samples[i];
+        const Stream stream = Stream::make(si.pixel_x, si.pixel_y, si.sample_index, si.seed, src.sobol);
+        Lane lane;
+        F3 o{}, d{};
+        camera_ray(src, si.pixel_x, si.pixel_y, stream, o, d, lane);
+        bf200_ray_v1 r{};
+        r.origin[0] = o.x;
+        r.origin[1] = o.y;
+        r.origin[2] = o.z;
+        r.direction[0] = d.x;
+        r.direction[1] = d.y;
+        r.direction[2] = d.z;
+        r.t_min = src.t_min;
+        r.t_max = src.t_max;
+        r.time = src.time;
+        r.mask = src.mask;
+        rays[i] = r;
+        status[i] = lane.err;
+    }
+}
+
+cudaError_t launch_camera_rays(const PathSource& src, const bf200_sample_index_v1* samples, uint64_t n,
+                               bf200_ray_v1* rays, uint32_t* status, cudaStream_t stream) {
+    const uint64_t blocks = (n + 127U) / 128U;
+    k_camera_rays<<<static_cast<uint32_t>(blocks == 0 ? 1 : (blocks < 65535U ? blocks : 65535U)), 128, 0, stream>>>(
+        src, samples, n, rays, status);
+    return cudaGetLastError();
+}
+#endif  // BF200_KERNELS_MAIN_TU
+
+#ifdef BF200_KERNELS_MAIN_TU
+// ------------------------------------------------------------------------------------------------
 // k_regenerate: retire finished slots and start new paths in empty ones (camera rays or inputs)
 // ------------------------------------------------------------------------------------------------
 

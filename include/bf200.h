@@ -923,6 +923,26 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_camera_create(
     uint32_t height, float vertical_fov_radians, float time, uint32_t jitter_mode,
     bf200_camera_v1* out_camera) BF200_NOEXCEPT;
 
+/* Stable compaction of one-byte route keys on the device: the wavefront's route queues, which
+ * replace the reference's stable appends (blackframe_cuda_launch_wavefront_queue_compaction,
+ * WavefrontQueueCompaction.hpp: the slots of one route appended in increasing slot order). Slots
+ * whose key is r < routes go to queue[offsets[r] .. offsets[r + 1]) in increasing slot order;
+ * other keys (the wavefront's 0xff: no route) are left out. routes: 1..4. Device pointers:
+ * keys[count], queue[count], offsets[routes + 1]. Runs on the context's stream and returns when
+ * it is done. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_compact_routes_device(
+    bf200_context* context, const uint8_t* keys, uint32_t count, uint32_t routes, uint32_t* queue,
+    uint32_t* offsets) BF200_NOEXCEPT;
+
+/* Primary rays of (pixel, sample) records through a camera, generated on the context's device by
+ * the same code that starts film paths: PinholeCamera::generate_primary_ray with the camera's
+ * pixel jitter drawn from the record's sample stream (PinholeCamera.hpp:144-283, PixelJitter.hpp:
+ * 47-64). sampler: BF200_SAMPLER_* of the stream. status: 0, or the lane failure code of a ray the
+ * reference would refuse. Host pointers. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_camera_rays(
+    bf200_context* context, const bf200_camera_v1* camera, const bf200_sample_index_v1* samples,
+    uint64_t count, uint32_t sampler, bf200_ray_v1* rays, uint32_t* status) BF200_NOEXCEPT;
+
 /* Sobol coordinate of a sample index in one of the 21,201 Joe-Kuo D6 dimensions, as a 64-bit
  * fixed-point fraction (sobol_sample_bits, SobolSampling.hpp:16-19). Dimensions from 21201 up
  * return BLACKFRAME_STATUS_OUT_OF_RANGE. Host computation. */
