@@ -245,3 +245,24 @@ def default_options(mis="balance", max_depth=8, roulette=True, first_eligible=3,
     options.roulette_minimum_survival = minimum_survival if roulette else 0.0
     options.roulette_maximum_survival = maximum_survival if roulette else 0.0
     return options
+
+
+# Native scene JSON (bf200_scene_json_*): core::StatusCode numbering of the codec's results.
+SCENE_JSON_CODES = {0: "success", 1: "invalid_argument", 2: "unavailable", 3: "not_found", 4: "incompatible",
+                    5: "resource_exhausted", 6: "protocol_error", 7: "platform_error", 8: "internal_error"}
+
+
+class SceneJsonLimits(C.Structure):
+    _fields_ = [("maximum_encoded_bytes", u64), ("maximum_total_values", u64),
+                ("maximum_total_string_bytes", u64), ("maximum_mesh_vertices", u64),
+                ("maximum_mesh_triangles", u64), ("maximum_image_scalar_values", u64),
+                ("maximum_decoded_bytes", u64), ("maximum_nesting_depth", u32),
+                ("maximum_records_per_registry", u32)]
+
+
+class SceneJsonFrame(C.Structure):
+    _fields_ = [("struct_size", u32), ("film_id", u32), ("camera_id", u32), ("render_options_id", u32),
+                ("width", u32), ("height", u32), ("crop", u32 * 4), ("precision", u32),
+                ("samples_per_pixel", u32), ("maximum_path_depth", u32), ("tile_edge_length", u32),
+                ("light_sampling_strategy", u32), ("reserved", u32), ("seed", u64), ("camera", Camera),
+                ("options", TransportOptions), ("scene", SceneDesc)]

@@ -47,6 +47,10 @@ EXPORTED_SYMBOLS = [
     "bf200_environment_map_power",
     "bf200_camera_rays",
     "bf200_compact_routes_device",
+    "bf200_scene_json_parse",
+    "bf200_scene_json_destroy",
+    "bf200_scene_json_write",
+    "bf200_scene_json_frame",
 ]
 
 

@@ -3,6 +3,7 @@
 // reference's, value for value, so the device's sampling and lookups can be compared bit for bit.
 // The file is compiled with floating-point contraction off.
 #include "bf200_envmap.h"
+#include "bf200_records.h"
 
 #include <algorithm>
 #include <array>
@@ -133,61 +134,6 @@ int build_cdf(const float* weights, float* cdf, size_t n) {
     return cdf[n - 1] == 1.0F ? 1 : -1;
 }
 
-// Gauss-Jordan inverse with partial pivoting of a 4x4 float matrix (MatrixOperations.hpp:31-94).
-bool invert4(const float (&m)[16], float (&out)[16]) {
-    float a[32];
-    for (int r = 0; r < 4; ++r) {
-        for (int c = 0; c < 4; ++c) {
-            if (!std::isfinite(m[r * 4 + c])) {
-                return false;
-            }
-            a[r * 8 + c] = m[r * 4 + c];
-            a[r * 8 + c + 4] = r == c ? 1.0F : 0.0F;
-        }
-    }
-    for (int pc = 0; pc < 4; ++pc) {
-        int pr = pc;
-        float magnitude = std::abs(a[pr * 8 + pc]);
-        for (int cand = pc + 1; cand < 4; ++cand) {
-            const float cm = std::abs(a[cand * 8 + pc]);
-            if (cm > magnitude) {
-                magnitude = cm;
-                pr = cand;
-            }
-        }
-        if (magnitude == 0.0F) {
-            return false;
-        }
-        if (pr != pc) {
-            for (int c = 0; c < 8; ++c) {
-                std::swap(a[pc * 8 + c], a[pr * 8 + c]);
-            }
-        }
-        const float pivot = a[pc * 8 + pc];
-        for (int c = 0; c < 8; ++c) {
-            a[pc * 8 + c] /= pivot;
-        }
-        for (int r = 0; r < 4; ++r) {
-            if (r == pc) {
-                continue;
-            }
-            const float factor = a[r * 8 + pc];
-            for (int c = 0; c < 8; ++c) {
-                a[r * 8 + c] -= factor * a[pc * 8 + c];
-            }
-        }
-    }
-    for (int r = 0; r < 4; ++r) {
-        for (int c = 0; c < 4; ++c) {
-            out[r * 4 + c] = a[r * 8 + c + 4];
-            if (!std::isfinite(out[r * 4 + c])) {
-                return false;
-            }
-        }
-    }
-    return true;
-}
-
 int invalid(const char*& message, const char* text) {
     message = text;
     return kEnvironmentInvalid;
@@ -238,7 +184,7 @@ int build_environment_tables(uint32_t width, uint32_t height, const float* texel
     m[9] = 2.0F * (yz + wx);
     m[10] = 1.0F - 2.0F * (xx + yy);
     float inv[16];
-    if (!invert4(m, inv)) {
+    if (!invert_matrix4(m, inv)) {
         return invalid(message, "A singular matrix has no inverse.");
     }
 

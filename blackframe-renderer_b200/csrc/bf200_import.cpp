@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "bf200.h"
+#include "bf200_records.h"
 
 struct bf200_mesh {
     std::vector<float> positions, normals, uvs;
@@ -159,60 +160,12 @@ bool parse_scalar(std::string_view t, float& out, const char*& problem) {
     return true;
 }
 
-bool unit_normal(float x, float y, float z) {
-    const float squared = std::fma(x, x, std::fma(y, y, z * z));
-    const float tolerance = std::numeric_limits<float>::epsilon() * 256.0F;
-    return std::isfinite(squared) && std::abs(squared - 1.0F) <= tolerance;
-}
-
-// Exactly collinear vertices: every component of (v1 - v0) x (v2 - v0) is zero. The edges and
-// products are formed in long double arithmetic from exact double differences where they are exact.
-bool collinear(const float* a, const float* b, const float* c) {
-    const long double e1[3] = {static_cast<long double>(b[0]) - a[0], static_cast<long double>(b[1]) - a[1],
-                               static_cast<long double>(b[2]) - a[2]};
-    const long double e2[3] = {static_cast<long double>(c[0]) - a[0], static_cast<long double>(c[1]) - a[1],
-                               static_cast<long double>(c[2]) - a[2]};
-    return e1[1] * e2[2] == e1[2] * e2[1] && e1[2] * e2[0] == e1[0] * e2[2] && e1[0] * e2[1] == e1[1] * e2[0];
-}
-
 // TriangleMesh::create (Blackframe/Engine/Source/TriangleMesh.cpp:60-130)
 bool validate_mesh(const bf200_mesh& m, ImportError& e) {
-    const size_t vertices = m.positions.size() / 3, triangles = m.triangles.size() / 3;
-    if (vertices == 0) {
-        return failure(e, BLACKFRAME_STATUS_INVALID_ARGUMENT, "A triangle mesh requires at least one aligned vertex.");
-    }
-    if (triangles == 0) {
-        return failure(e, BLACKFRAME_STATUS_INVALID_ARGUMENT, "A triangle mesh requires at least one indexed triangle.");
-    }
-    for (float v : m.positions) {
-        if (!std::isfinite(v)) {
-            return failure(e, BLACKFRAME_STATUS_INVALID_ARGUMENT,
-                           "Triangle mesh positions must contain only finite values.");
-        }
-    }
-    for (size_t i = 0; i < vertices; ++i) {
-        if (!unit_normal(m.normals[3 * i], m.normals[3 * i + 1], m.normals[3 * i + 2])) {
-            return failure(e, BLACKFRAME_STATUS_INVALID_ARGUMENT,
-                           "Triangle mesh normals must be finite unit-length values.");
-        }
-    }
-    for (float v : m.uvs) {
-        if (!std::isfinite(v)) {
-            return failure(e, BLACKFRAME_STATUS_INVALID_ARGUMENT,
-                           "Triangle mesh texture coordinates must contain only finite values.");
-        }
-    }
-    for (size_t t = 0; t < triangles; ++t) {
-        const uint32_t* tri = &m.triangles[3 * t];
-        if (tri[0] >= vertices || tri[1] >= vertices || tri[2] >= vertices) {
-            return failure(e, BLACKFRAME_STATUS_INVALID_ARGUMENT,
-                           "A triangle mesh index references an unknown aligned vertex.");
-        }
-        if (collinear(&m.positions[3ULL * tri[0]], &m.positions[3ULL * tri[1]], &m.positions[3ULL * tri[2]])) {
-            return failure(e, BLACKFRAME_STATUS_INVALID_ARGUMENT, "A triangle mesh triangle is degenerate.");
-        }
-    }
-    return true;
+    const char* problem = bf200::triangle_mesh_problem(m.positions.data(), m.normals.data(), m.uvs.data(),
+                                                       m.positions.size() / 3, m.triangles.data(),
+                                                       m.triangles.size() / 3);
+    return problem == nullptr || failure(e, BLACKFRAME_STATUS_INVALID_ARGUMENT, problem);
 }
 
 // Aligned OBJ vertices by their (v, vt, vn) corner: an open-addressing table sized for every
@@ -334,7 +287,7 @@ bool parse_obj(std::string_view text, bf200_mesh& m, ImportError& e) {
                     return line_failure(e, "OBJ", number, problem);
                 }
             }
-            if (normal && !unit_normal(xyz[0], xyz[1], xyz[2])) {
+            if (normal && !bf200::unit_normal(xyz[0], xyz[1], xyz[2])) {
                 return line_failure(e, "OBJ", number, "normals must be finite unit-length values.");
             }
             (normal ? src_n : src_p).insert((normal ? src_n : src_p).end(), xyz, xyz + 3);

@@ -954,6 +954,93 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_owen_sobol_bits(const bf200_
                                                                     uint64_t sobol_dimension,
                                                                     uint64_t* out_bits) BF200_NOEXCEPT;
 
+/* ---- Native scene JSON (engine::SceneDescriptionJson.hpp, schema "blackframe.scene" v1) ----
+ * bf200_scene_json_parse replaces deserialize_scene_description_json
+ * (SceneDescriptionJson.hpp:48-50; SceneDescriptionJsonReader.cpp:2430-2457) and
+ * bf200_scene_json_write replaces serialize_scene_description_json (:45-47). Both return the
+ * reference's core::StatusCode numbering (BF200_SCENE_JSON_*), so a caller sees the same accept or
+ * refuse decision and code for the same bytes. A parsed document is the validated
+ * SceneDescription (SceneDescription::create's checks included). Host-image textures and
+ * normal/bump maps are refused with BF200_SCENE_JSON_UNAVAILABLE: this backend has no image
+ * textures. bf200_scene_json_frame turns the active film, camera and render options into the
+ * arguments of bf200_scene_create and bf200_render_film. Host computation only. */
+typedef struct bf200_scene_json bf200_scene_json;
+
+/* SceneDescriptionJsonLimits (SceneDescriptionJson.hpp:18-33). Every field must be non-zero and
+ * at most MaximumSceneDescriptionJsonLimits; a null pointer means the default limits. */
+typedef struct bf200_scene_json_limits_v1 {
+    uint64_t maximum_encoded_bytes;
+    uint64_t maximum_total_values;
+    uint64_t maximum_total_string_bytes;
+    uint64_t maximum_mesh_vertices;
+    uint64_t maximum_mesh_triangles;
+    uint64_t maximum_image_scalar_values;
+    uint64_t maximum_decoded_bytes;
+    uint32_t maximum_nesting_depth;
+    uint32_t maximum_records_per_registry;
+} bf200_scene_json_limits_v1;
+
+/* core::StatusCode (Status.hpp:10-20). */
+#define BF200_SCENE_JSON_OK 0u
+#define BF200_SCENE_JSON_INVALID_ARGUMENT 1u
+#define BF200_SCENE_JSON_UNAVAILABLE 2u
+#define BF200_SCENE_JSON_NOT_FOUND 3u
+#define BF200_SCENE_JSON_INCOMPATIBLE 4u
+#define BF200_SCENE_JSON_RESOURCE_EXHAUSTED 5u
+#define BF200_SCENE_JSON_INTERNAL_ERROR 8u
+
+/* Parses and validates `size` bytes. On success *out_document owns the description; on failure it
+ * is null and `message` (when given) holds the reason. */
+BF200_EXTERN_C BF200_EXPORT uint32_t bf200_scene_json_parse(const char* bytes, uint64_t size,
+                                                            const bf200_scene_json_limits_v1* limits,
+                                                            bf200_scene_json** out_document, char* message,
+                                                            uint64_t message_capacity) BF200_NOEXCEPT;
+BF200_EXTERN_C BF200_EXPORT void bf200_scene_json_destroy(bf200_scene_json* document) BF200_NOEXCEPT;
+
+/* The canonical encoding of a document (the reference writer's bytes for the same description).
+ * *out_size receives its length; the bytes are written when out is not null and capacity holds
+ * them (BF200_SCENE_JSON_RESOURCE_EXHAUSTED otherwise, with *out_size still set). */
+BF200_EXTERN_C BF200_EXPORT uint32_t bf200_scene_json_write(const bf200_scene_json* document,
+                                                            const bf200_scene_json_limits_v1* limits, char* out,
+                                                            uint64_t capacity, uint64_t* out_size, char* message,
+                                                            uint64_t message_capacity) BF200_NOEXCEPT;
+
+/* The active selection of a document, ready to render. `scene` is the committed frame scene
+ * (registries in identifier order, instance transforms resolved through the hierarchy as
+ * FrameScene::create resolves them, punctual lights in light-registry order, the environment
+ * light's packet and radiance); its arrays belong to the document and live until it is destroyed.
+ * `camera` is the active pinhole camera over the active film with the render options' pixel
+ * jitter; `options` carries the MIS heuristic, depth limits and Russian roulette. The remaining
+ * fields echo the film and render options. A render of the document is bf200_scene_create(scene)
+ * then bf200_render_film(camera, request {samples_per_pixel, seed, precision}, options) over the
+ * full extent; the crop selects the pixels the reference's film covers. */
+typedef struct bf200_scene_json_frame_v1 {
+    uint32_t struct_size;
+    uint32_t film_id;
+    uint32_t camera_id;
+    uint32_t render_options_id;
+    uint32_t width;
+    uint32_t height;
+    uint32_t crop[4];                 /* minimum x, minimum y, maximum x, maximum y (half-open) */
+    uint32_t precision;               /* film accumulation: 0 float32, 1 float64 */
+    uint32_t samples_per_pixel;
+    uint32_t maximum_path_depth;
+    uint32_t tile_edge_length;
+    uint32_t light_sampling_strategy; /* 0 uniform, 1 power weighted, 2 spatial tree */
+    uint32_t reserved;
+    uint64_t seed;
+    bf200_camera_v1 camera;
+    bf200_transport_options_v1 options;
+    bf200_scene_desc_v1 scene;
+} bf200_scene_json_frame_v1;
+
+/* Fills *out for the document's active selection. Returns BF200_SCENE_JSON_UNAVAILABLE with a
+ * message for a document this backend cannot render: no instances, or no spectral environment
+ * light (the packet of a render). */
+BF200_EXTERN_C BF200_EXPORT uint32_t bf200_scene_json_frame(const bf200_scene_json* document,
+                                                            bf200_scene_json_frame_v1* out, char* message,
+                                                            uint64_t message_capacity) BF200_NOEXCEPT;
+
 /* Library version and build description (sm_100a arch string). */
 BF200_EXTERN_C BF200_EXPORT const char* bf200_build_info(void) BF200_NOEXCEPT;
 

@@ -47,8 +47,8 @@ class _Checker:
     def last_error(self):
         return getattr(self.lib, self.prefix + "_last_error")().decode()
 
-    def scene(self, builder):
-        desc = builder.desc()
+    def scene(self, builder, desc=None):
+        desc = builder.desc() if desc is None else desc
         handle = C.c_void_p()
         rc = getattr(self.lib, self.prefix + "_scene_create")(C.byref(desc), C.byref(handle))
         if rc != 0:
