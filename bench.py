@@ -558,6 +558,7 @@ def run_adjoint(args, torch, rank):
 
 
 IMPORT_WORKLOAD = "mesh_import_obj"
+SCENE_JSON_WORKLOAD = "scene_json"
 REFIT_WORKLOAD = "refit_bvh_stress"
 
 
@@ -590,12 +591,15 @@ def run_refit(args, torch):
         if step >= args.warmup:
             refit_s.append(time.perf_counter() - t0)
     create_s = []
+    create_stats = None
     for step in range(max(1, min(args.steps, 2))):
         desc = targets[-1].desc()
         t0 = time.perf_counter()
         fresh = ctx.create_scene(targets[-1], desc)
         torch.cuda.synchronize()
         create_s.append(time.perf_counter() - t0)
+        st = fresh.stats()
+        create_stats = {k: getattr(st, k) for k, _ in st._fields_ if k != "struct_size"}
         fresh.close()
     scene.close()
     ctx.close()
@@ -606,7 +610,8 @@ def run_refit(args, torch):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": REFIT_WORKLOAD, "instances": len(builder.instances),
                        "triangles": builder.triangle_count},
-            "scene_create_ms": create_ms, "create_over_refit": create_ms / refit_ms, "gpu_launches": 1}
+            "scene_create_ms": create_ms, "create_over_refit": create_ms / refit_ms,
+            "scene_create_phases": create_stats, "gpu_launches": 1}
     print(json.dumps(line), flush=True)
 
 
@@ -656,6 +661,103 @@ def run_mesh_import(args):
             "config": {"workload": IMPORT_WORKLOAD, "triangles": len(f), "vertices": len(v), "bytes": size,
                        "host": "one thread"},
             "mb_per_s": size / seconds / 1e6, "reference_loader": reference, "gpu_launches": 0}
+    print(json.dumps(line), flush=True)
+
+
+def scene_json_document():
+    """A native scene JSON document of 655,360 triangles: two displaced subdivision-7 icospheres
+    (327,680 triangles each), 16 instances in a two-level hierarchy, three materials, a point light
+    and the environment; about 50 MB of text written with 9 significant digits, inside every
+    default budget of the reference's reader."""
+    rng = np.random.default_rng(3)
+    geometries = []
+    for gid, level in ((10, 7), (11, 7)):
+        v, f = scenes.icosphere(level)
+        p = (v * (1.0 + 0.02 * rng.uniform(-1.0, 1.0, len(v)))[:, None]).astype(np.float32)
+        n = (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+        uv = rng.uniform(0.0, 1.0, (len(v), 2)).astype(np.float32)
+        rows = lambda a: ",".join("[" + ",".join("%.9g" % x for x in r) + "]" for r in a)
+        tris = ",".join("[%d,%d,%d]" % tuple(t) for t in f)
+        geometries.append((gid, len(f), '{"id":%d,"mesh":{"positions":[%s],"normals":[%s],"texture_coordinates":[%s],'
+                           '"triangles":[%s]}}' % (gid, rows(p), rows(n), rows(uv), tris)))
+    packet = '{"nanometers":[471.2129,588.7129,706.2129,823.7129],"pdf":[0.0021276595,0.0021276595,0.0021276595,0.0021276595]}'
+    lambert = ('{"id":%d,"spectral":{"wavelengths":' + packet + ',"closures":{"frame_mode":"shading_normal",'
+               '"tangent_rotation_radians":0,"components":[{"probability":1,"type":"lambertian_reflection",'
+               '"weight":[0.5,0.5,0.5,0.5]}]},"emission":[%s],"normal_map":null,"bump_map":null}}')
+    materials = [lambert % (20, "0,0,0,0"), lambert % (21, "0,0,0,0"), lambert % (22, "4,3,2,1")]
+    instances = []
+    for k in range(16):
+        m = np.eye(4)
+        m[:3, 3] = rng.uniform(-10, 10, 3)
+        parent = "null" if k < 4 else str(300 + k % 4)
+        instances.append('{"id":%d,"parent":%s,"object":1,"geometry":%d,"material":%d,"local_to_parent":[%s],'
+                         '"visibility_mask":4294967295}' % (300 + k, parent, 10 + k % 2, 20 + k % 3,
+                                                            ",".join("%.9g" % x for x in m.ravel())))
+    text = ('{"schema":"blackframe.scene","schema_version":1,"active":{"film":1,"camera":1,"render_options":1},'
+            '"films":[{"id":1,"extent":[1920,1080],"crop":[0,0,1920,1080],"accumulation":"float32"}],'
+            '"cameras":[{"id":1,"film":1,"model":{"type":"pinhole","origin":[0,0,30],"normal":[0,0,1],'
+            '"tangent":[1,0,0],"bitangent":[0,1,0],"vertical_fov_radians":0.8,"t_min":0,"t_max":1e30,'
+            '"visibility_mask":4294967295,"current_medium":0}}],'
+            '"render_options":[{"id":1,"film":1,"samples_per_pixel":64,"maximum_path_depth":8,"tile_edge_length":16,'
+            '"seed":0,"pixel_jitter":"uniform","mis_heuristic":"power","light_sampling_strategy":"uniform",'
+            '"depth_limits":{"diffuse":8,"glossy":8,"specular":8,"transmission":8,"volume":0},'
+            '"russian_roulette":{"mode":"disabled"}}],"constant_textures":[],"host_image_textures":[],'
+            '"objects":[{"id":1}],"geometries":[' + ",".join(g[2] for g in geometries) + '],"materials":['
+            + ",".join(materials) + '],"instances":[' + ",".join(instances) + '],"lights":[{"id":1,'
+            '"type":"environment","wavelengths":' + packet + ',"radiance":[0.1,0.1,0.1,0.1]},{"id":2,"type":"point",'
+            '"position":[0,20,0],"absolute_position_error":[0,0,0],"spectral_radiant_intensity":[50,50,50,50]}]}')
+    return text.encode(), sum(g[1] for g in geometries)
+
+
+def run_scene_json(args):
+    """Native scene JSON ingestion: bf200_scene_json_parse (strict reading, every SceneDescription
+    check, hierarchy resolution) plus bf200_scene_json_frame (the committed arrays a render takes)
+    on one large document, beside the reference's deserialize_scene_description_json (oracle/_ref)
+    on the same bytes. Host code on both sides, one thread; both must accept, and the canonical
+    bytes of the product are checked against the reference's once, outside the timing."""
+    from bf200 import scene_json
+    text, triangles = scene_json_document()
+    lim = None  # the reference's default limits, as the reference arm below uses
+    for _ in range(args.warmup):
+        scene_json.SceneJson(text, lim).close()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        doc = scene_json.SceneJson(text, lim)
+        doc.frame()
+        times.append(time.perf_counter() - t0)
+        doc.close()
+    reference = None
+    ref_path = os.path.join(REPO, "oracle", "_ref", "libbfref.so")
+    if os.path.exists(ref_path):
+        import ctypes as C
+        lib = C.CDLL(ref_path)
+        lib.bfref_scene_json_parse_only.argtypes = [C.c_char_p, C.c_uint64]
+        lib.bfref_scene_json_parse_only.restype = C.c_int
+        ref_times, codes = [], []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            codes.append(lib.bfref_scene_json_parse_only(text, len(text)))
+            ref_times.append(time.perf_counter() - t0)
+        ref_seconds = statistics.median(ref_times)
+        lib.bfref_scene_json_canonical.argtypes = [C.c_char_p, C.c_uint64, C.c_void_p, C.c_char_p, C.c_uint64,
+                                                   C.POINTER(C.c_uint64), C.c_char_p, C.c_uint64]
+        lib.bfref_scene_json_canonical.restype = C.c_int
+        out, size, message = C.create_string_buffer(2 * len(text)), C.c_uint64(), C.create_string_buffer(512)
+        rc = lib.bfref_scene_json_canonical(text, len(text), None, out, 2 * len(text), C.byref(size), message, 512)
+        with scene_json.SceneJson(text, lim) as doc:
+            identical = rc == 0 and doc.canonical() == out.raw[:size.value]
+        reference = {"mb_per_s": len(text) / ref_seconds / 1e6, "seconds": ref_seconds, "codes": sorted(set(codes)),
+                     "identical_canonical_bytes": identical, "kind": "reference"}
+    seconds = statistics.median(times)
+    line = {"metric": "scene JSON MB/s", "value": len(text) / seconds / 1e6, "unit": "MB/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": seconds * 1000.0, "higher_is_better": True,
+            "scaling": "none", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": SCENE_JSON_WORKLOAD, "bytes": len(text), "triangles": triangles, "instances": 16,
+                       "host": "one thread"},
+            "reference_reader": reference, "gpu_launches": 0}
+    if reference is not None:
+        line["speedup_vs_reference"] = reference["seconds"] / seconds
     print(json.dumps(line), flush=True)
 
 
@@ -808,7 +910,8 @@ def main():
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's)")
     parser.add_argument("--workload", default=WORKLOAD,
-                        choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD, IMPORT_WORKLOAD, REFIT_WORKLOAD],
+                        choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD, IMPORT_WORKLOAD, REFIT_WORKLOAD,
+                                                         SCENE_JSON_WORKLOAD],
                         help="scene and frame (default: the headline Cornell + spheres frame); "
                              f"{BATCH_WORKLOAD}: the 64-scene batch against 64 serial renders; "
                              f"{ADJOINT_WORKLOAD}: the path-replay adjoint; {IMPORT_WORKLOAD}: OBJ ingestion")
@@ -831,6 +934,10 @@ def main():
     if args.workload == IMPORT_WORKLOAD:
         if rank == 0:
             run_mesh_import(args)
+        return
+    if args.workload == SCENE_JSON_WORKLOAD:
+        if rank == 0:
+            run_scene_json(args)
         return
 
     import torch

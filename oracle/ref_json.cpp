@@ -71,6 +71,13 @@ __attribute__((visibility("default"))) int bfref_scene_json_canonical(const char
     return 0;
 }
 
+// deserialize_scene_description_json alone (default limits): its StatusCode. For timing the
+// reference's reader beside the product's.
+__attribute__((visibility("default"))) int bfref_scene_json_parse_only(const char* bytes, uint64_t size) {
+    const auto decoded = engine::deserialize_scene_description_json(std::string_view{bytes, size});
+    return decoded ? 0 : static_cast<int>(decoded.error().code);
+}
+
 // The frame a caller commits from a decoded description: FrameScene::create over its textures,
 // objects, geometries, materials and instances, its punctual lights in registry order and its
 // spectral environment. Per committed instance (identifier order): the identifier and the world
