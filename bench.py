@@ -256,7 +256,7 @@ def run_batch(args, torch, rank, world, local_rank):
     if distributed:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
-    g = np.load(os.path.join(REPO, "tests", "golden", f"{WORKLOAD}.npz"))
+    g = np.load(os.path.join(REPO, "tests", "golden", f"{SENSOR_FIXTURE}.npz"))
     from helpers import sensor_from_golden
     sensor = sensor_from_golden(g)
     ctx = runtime.Context(local_rank, path_capacity=args.capacity)
@@ -330,10 +330,11 @@ def run_batch(args, torch, rank, world, local_rank):
         "config": {"workload": BATCH_WORKLOAD, "jobs": 64, "jobs_per_gpu": len(mine), "paths_per_step": total_paths,
                    "unique_triangles_rank0": triangles,
                    "parallelism": f"whole scenes sharded x{world}" if distributed else "single GPU",
-                   "lanes": args.lanes or "autotuned", "path_capacity": args.capacity,
+                   "lanes": args.lanes or "measured (2, 4 or 8)", "path_capacity": args.capacity,
                    "l2": "flushed between steps (256 MiB write)"},
         "serial": {"value": serial_value, "ms_per_step": serial_total / args.steps},
-        "batched_vs_serial": value / serial_value, "failed_lanes": failed, "clocks": clocks.summary(),
+        "batched_vs_serial": value / serial_value, "lanes_used": ctx.batch_lanes(), "failed_lanes": failed,
+        "clocks": clocks.summary(),
     }
     for j in jobs:
         j[0].close()
@@ -571,6 +572,7 @@ def run_refit(args, torch):
     import copy
     builder, _, _, _, _ = workload_setup("bvh_stress_1080p")
     ctx = runtime.Context(0, path_capacity=args.capacity)
+    ctx.set_build_mode(abi.BUILD_DEVICE_LBVH if args.build_mode == "lbvh" else abi.BUILD_HOST_SAH)
     scene = ctx.create_scene(builder)
     rng = np.random.default_rng(2)
     targets = []
@@ -609,7 +611,7 @@ def run_refit(args, torch):
             "warmup": args.warmup, "ms_per_step": refit_ms, "higher_is_better": False, "scaling": "none",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": REFIT_WORKLOAD, "instances": len(builder.instances),
-                       "triangles": builder.triangle_count},
+                       "triangles": builder.triangle_count, "build_mode": args.build_mode},
             "scene_create_ms": create_ms, "create_over_refit": create_ms / refit_ms,
             "scene_create_phases": create_stats, "gpu_launches": 1}
     print(json.dumps(line), flush=True)
@@ -908,6 +910,8 @@ def main():
     parser.add_argument("--capacity", type=int, default=1 << 21)
     parser.add_argument("--reference-seconds", type=float, default=4.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--build-mode", choices=["sah", "lbvh"], default="sah",
+                        help="BLAS build of the scene: host binned SAH (default) or the device linear BVH")
     parser.add_argument("--spp", type=int, default=0, help="samples per pixel per step (default: the workload's)")
     parser.add_argument("--workload", default=WORKLOAD,
                         choices=sorted(scenes.WORKLOADS) + [BATCH_WORKLOAD, IMPORT_WORKLOAD, REFIT_WORKLOAD,
@@ -969,6 +973,7 @@ def main():
     pixels = width * height
     paths_per_step = pixels * spp
     ctx = runtime.Context(local_rank, path_capacity=args.capacity)
+    ctx.set_build_mode(abi.BUILD_DEVICE_LBVH if args.build_mode == "lbvh" else abi.BUILD_HOST_SAH)
     scene = ctx.create_scene(builder)
     lib = runtime.library()
     film = torch.zeros((height, width, 4), dtype=torch.float32, device="cuda")
@@ -1087,7 +1092,8 @@ def main():
         "config": {"workload": args.workload, "width": width, "height": height, "spp": spp, "max_depth": 16,
                    "mis": "power", "paths_per_step_per_gpu": paths_per_step, "path_capacity": args.capacity,
                    "l2": "flushed between steps (256 MiB write); path state > L2",
-                   "parallelism": f"sample-partitioned x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"sample-partitioned x{world}" if world > 1 else "single GPU",
+                   "blas_build": "device linear BVH" if args.build_mode == "lbvh" else "host binned SAH"},
         "rays_per_s": (ext + shadow) / (total_ms / 1000.0) * (world if distributed else 1),
         "segments": {"extension": ext, "shadow": shadow, "iterations": iterations},
         "stage_ms_one_frame": stage, "failed_lanes": failed,

@@ -266,3 +266,12 @@ class SceneJsonFrame(C.Structure):
                 ("samples_per_pixel", u32), ("maximum_path_depth", u32), ("tile_edge_length", u32),
                 ("light_sampling_strategy", u32), ("reserved", u32), ("seed", u64), ("camera", Camera),
                 ("options", TransportOptions), ("scene", SceneDesc)]
+
+
+class SceneStats(C.Structure):
+    _fields_ = [("struct_size", u32), ("blas_depth", u32), ("device_built_geometries", u32), ("reserved", u32),
+                ("node_count", u64), ("leaf_triangle_count", u64), ("blas_build_ms", f64), ("collapse_ms", f64),
+                ("instance_ms", f64), ("upload_ms", f64), ("total_ms", f64)]
+
+
+BUILD_HOST_SAH, BUILD_DEVICE_LBVH = 0, 1

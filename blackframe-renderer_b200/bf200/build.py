@@ -18,7 +18,7 @@ INCLUDE = os.path.join(REPO, "include")
 LIBRARY = os.path.join(PACKAGE_DIR, "libbf200.so")
 SOURCES = ["bf200_kernels.cu", "bf200_shade_plain.cu", "bf200_shade_cone.cu", "bf200_shade_tree.cu",
            "bf200_shade_cone_tree.cu", "bf200_shade_adjoint.cu", "bf200_compact.cu", "bf200_sobol.cu", "bf200_host.cu", "bf200_import.cpp", "bf200_soa.cpp", "bf200_light_tree.cpp", "bf200_light_tree.cu",
-           "bf200_envmap.cpp", "bf200_envmap.cu", "bf200_records.cpp", "bf200_scene_json.cpp"]
+           "bf200_envmap.cpp", "bf200_envmap.cu", "bf200_records.cpp", "bf200_scene_json.cpp", "bf200_lbvh.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-std=c++17", "-O3", "-lineinfo", "-fmad=false",

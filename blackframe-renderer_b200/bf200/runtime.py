@@ -51,6 +51,9 @@ EXPORTED_SYMBOLS = [
     "bf200_scene_json_destroy",
     "bf200_scene_json_write",
     "bf200_scene_json_frame",
+    "bf200_scene_stats",
+    "bf200_context_set_build_mode",
+    "bf200_context_batch_lanes",
 ]
 
 
@@ -181,6 +184,17 @@ class Scene:
         if status != 0:
             raise Bf200Error(status, "set_light_tree")
 
+    def stats(self):
+        """bf200_scene_stats: sizes and the host wall time of each scene-creation phase (abi.SceneStats)."""
+        out = abi.SceneStats()
+        out.struct_size = C.sizeof(out)
+        f = library().bf200_scene_stats
+        f.argtypes = [C.c_void_p, C.POINTER(abi.SceneStats)]
+        f.restype = C.c_uint32
+        if f(self.handle, C.byref(out)) != 0:
+            raise Bf200Error(1, "scene_stats")
+        return out
+
     def close(self):
         if self.handle:
             library().bf200_scene_destroy(self.handle)
@@ -211,6 +225,23 @@ class Context:
 
     def __exit__(self, *exc):
         self.close()
+
+    def batch_lanes(self):
+        """bf200_context_batch_lanes: the lane count of the last render_films_device call."""
+        out = C.c_uint32()
+        f = library().bf200_context_batch_lanes
+        f.argtypes = [C.c_void_p, C.POINTER(C.c_uint32)]
+        f.restype = C.c_uint32
+        self._check(f(self.handle, C.byref(out)), "context_batch_lanes")
+        return out.value
+
+    def set_build_mode(self, mode):
+        """bf200_context_set_build_mode: abi.BUILD_HOST_SAH (default) or abi.BUILD_DEVICE_LBVH for the
+        scenes created from now on."""
+        f = library().bf200_context_set_build_mode
+        f.argtypes = [C.c_void_p, C.c_uint32]
+        f.restype = C.c_uint32
+        self._check(f(self.handle, mode), "context_set_build_mode")
 
     def create_scene(self, builder, desc=None):
         """bf200_scene_create from `builder`'s description (or `desc`, already made from it)."""

@@ -10,10 +10,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <limits>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -35,6 +38,10 @@ static_assert(kClosureCapacity == kMaxClosures, "one closure capacity");
 
 struct bf200_context {
     int device = 0;
+    uint32_t build_mode = BF200_BUILD_HOST_SAH;  // bf200_context_set_build_mode
+    // measured batch lane counts per job-size class, and the count of the last batch call
+    std::map<uint32_t, uint32_t> batch_lanes_by_class;
+    uint32_t last_batch_lanes = 0;
     cudaStream_t stream = nullptr;
     uint32_t sm_count = 148;
     uint64_t capacity = 0;
@@ -81,8 +88,6 @@ struct bf200_scene {
     std::vector<float> object_boxes;    // per geometry: lo xyz, hi xyz
     uint32_t tlas_first = 0;            // first TLAS node in the node array (when there is a TLAS)
     std::vector<BvhNode4> tlas_nodes;   // host copy of the TLAS nodes
-    const uint32_t* tri_instance = nullptr;  // device: instance of every instance triangle
-    const uint32_t* tri_local = nullptr;     // device: its triangle within the geometry
     uint32_t instance_triangles = 0;
     uint32_t* normal_failures = nullptr;     // device counter of k_world_normals
     size_t light_triangles = 0;
@@ -94,6 +99,7 @@ struct bf200_scene {
     void* tree_map = nullptr;
     size_t tree_node_bytes = 0;
     size_t tree_map_bytes = 0;
+    bf200_scene_stats_v1 stats{};       // bf200_scene_stats: sizes and host wall time per build phase
 };
 
 namespace {
@@ -220,6 +226,12 @@ static_assert(kLeafSize < static_cast<int>(kSphereLeafCount) && kSphereLeafCount
               "triangle leaves never carry the sphere leaf count");
 constexpr int kBins = 16;
 
+// Subtrees of at least this many primitives are built on their own thread (down to
+// Builder::parallel_levels levels), into their own arrays that are then appended: the appended
+// result is the sequential build's, node for node and record for record.
+constexpr int kParallelPrims = 32768;
+constexpr uint32_t kDeviceBuildMinimum = 4096;  // smaller geometries build faster on the host
+
 struct Builder {
     std::vector<Prim>& prims;
     std::vector<BvhNode>& nodes;
@@ -229,6 +241,7 @@ struct Builder {
     uint32_t max_depth = 0;
     int leaf_limit = kLeafSize;
     bool instance_leaves = false;  // TLAS: one instance per leaf, encoded as ~instance
+    int parallel_levels = 0;       // levels whose large right subtrees go to their own thread
 
     int make_leaf(int begin, int end) {
         if (instance_leaves) {
@@ -329,8 +342,41 @@ struct Builder {
         const int node_index = static_cast<int>(nodes.size());
         nodes.push_back(BvhNode{});
         const Box lb = bounds(begin, mid), rb = bounds(mid, end);
-        const int left = build(begin, mid, depth + 1);
-        const int right = build(mid, end, depth + 1);
+        int left = 0, right = 0;
+        if (parallel_levels > 0 && !instance_leaves && end - mid >= kParallelPrims) {
+            // the right subtree on its own thread into its own arrays, the left one here
+            std::vector<BvhNode> right_nodes;
+            std::vector<float4> right_leaves;
+            Builder sub{prims, right_nodes, right_leaves, positions, tris};
+            sub.leaf_limit = leaf_limit;
+            sub.parallel_levels = parallel_levels - 1;
+            auto pending = std::async(std::launch::async, [&sub, mid, end, depth] { return sub.build(mid, end, depth + 1); });
+            --parallel_levels;
+            left = build(begin, mid, depth + 1);
+            ++parallel_levels;
+            const int sub_root = pending.get();
+            // append: node codes move by the nodes before them, leaf codes by the records before them
+            const int node_offset = static_cast<int>(nodes.size());
+            const uint32_t leaf_offset = static_cast<uint32_t>(leaf_tris.size() / 3);
+            const auto moved = [&](int code) {
+                if (code >= 0) {
+                    return code + node_offset;
+                }
+                const uint32_t packed = ~static_cast<uint32_t>(code);
+                return ~static_cast<int>(packed + (leaf_offset << kLeafCountBits));
+            };
+            for (BvhNode n : right_nodes) {
+                n.d.x = moved(n.d.x);
+                n.d.y = moved(n.d.y);
+                nodes.push_back(n);
+            }
+            leaf_tris.insert(leaf_tris.end(), right_leaves.begin(), right_leaves.end());
+            right = moved(sub_root);
+            max_depth = std::max(max_depth, sub.max_depth);
+        } else {
+            left = build(begin, mid, depth + 1);
+            right = build(mid, end, depth + 1);
+        }
         BvhNode& node = nodes[node_index];
         node.a = make_float4(lb.lo[0], lb.hi[0], lb.lo[1], lb.hi[1]);
         node.b = make_float4(rb.lo[0], rb.hi[0], rb.lo[1], rb.hi[1]);
@@ -404,6 +450,10 @@ uint32_t build_blas(const bf200_scene_desc_v1& d, uint32_t g, std::vector<BvhNod
         p.index = t;
     }
     Builder b{prims, nodes, leaf_tris, positions, tris};
+    const unsigned threads = std::max(1U, std::thread::hardware_concurrency());
+    while ((1U << b.parallel_levels) < threads && b.parallel_levels < 5) {
+        ++b.parallel_levels;  // up to 2^levels subtrees in flight, at most 32
+    }
     const uint32_t root = static_cast<uint32_t>(nodes.size());
     if (static_cast<int>(prims.size()) <= kLeafSize) {
         nodes.push_back(BvhNode{});
@@ -1455,6 +1505,13 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
     cudaSetDevice(c->device);
     auto scene = std::make_unique<bf200_scene>();
     scene->context = c;
+    using Clock = std::chrono::steady_clock;
+    const auto ms_since = [](Clock::time_point t0) {
+        return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    };
+    const auto t_start = Clock::now();
+    bf200_scene_stats_v1& stats = scene->stats;
+    stats.struct_size = sizeof(bf200_scene_stats_v1);
     try {
         // BLAS per geometry
         std::vector<BvhNode> nodes;
@@ -1465,12 +1522,43 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         uint32_t blas_depth = 0;
         for (uint32_t g = 0; g < d->geometry_count; ++g) {
             uint32_t depth = 0;
-            const uint32_t root = build_blas(*d, g, nodes, leaf_tris, depth);
+            const auto& geom = d->geometries[g];
+            const size_t node_mark = nodes.size(), leaf_mark = leaf_tris.size(), node4_mark = nodes4.size();
+            const bool on_device = c->build_mode == BF200_BUILD_DEVICE_LBVH && geom.kind == BF200_GEOMETRY_TRIANGLES &&
+                                   geom.triangle_count >= kDeviceBuildMinimum;
+            auto t0 = Clock::now();
+            uint32_t root = 0;
+            if (on_device) {
+                const cudaError_t e = build_blas_lbvh(
+                    d->positions + 3ULL * geom.vertex_offset, geom.vertex_count, d->triangles + 3ULL * geom.triangle_offset,
+                    geom.triangle_count, static_cast<uint32_t>(node_mark), static_cast<uint32_t>(leaf_mark / 3), nodes,
+                    leaf_tris, c->stream);
+                if (e != cudaSuccess) {
+                    return cuda_fail(c, e, "device BLAS build");
+                }
+                root = static_cast<uint32_t>(node_mark);
+            } else {
+                root = build_blas(*d, g, nodes, leaf_tris, depth);
+            }
+            stats.blas_build_ms += ms_since(t0);
+            t0 = Clock::now();
             uint32_t depth4 = 1;
             Collapser collapser{nodes, nodes4};
-            const int root4 = collapser.collapse(static_cast<int>(root), 1, depth4);
+            int root4 = collapser.collapse(static_cast<int>(root), 1, depth4);
+            if (on_device && 3 * depth4 + 1 + kEagerInstances + 3 >= static_cast<uint32_t>(kTraversalStack)) {
+                // too deep for the traversal stack: this geometry takes the host build
+                nodes.resize(node_mark);
+                leaf_tris.resize(leaf_mark);
+                nodes4.resize(node4_mark);
+                root = build_blas(*d, g, nodes, leaf_tris, depth);
+                depth4 = 1;
+                root4 = collapser.collapse(static_cast<int>(root), 1, depth4);
+            } else if (on_device) {
+                ++stats.device_built_geometries;
+            }
+            stats.collapse_ms += ms_since(t0);
+            stats.blas_depth = std::max(stats.blas_depth, depth4);
             blas_depth = std::max(blas_depth, 3 * depth4 + 1);  // at most 3 net entries per level
-            const auto& geom = d->geometries[g];
             if (geom.kind == BF200_GEOMETRY_SPHERE) {
                 // the sphere's leaf record is the last one this BLAS added
                 geom_info[g] = make_uint4(static_cast<uint32_t>(leaf_tris.size() / 3 - 1), 0U,
@@ -1485,6 +1573,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
                 object_box[g].grow(d->positions + 3ULL * (geom.vertex_offset + local[t]));
             }
         }
+        const auto t_instances = Clock::now();
         // instance ranges on the traversal stack carry 14-bit first indices
         if (d->instance_count >= (1U << 14)) {
             return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "more than 16383 instances");
@@ -1543,7 +1632,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         std::vector<float4> to_object(3ULL * d->instance_count), to_world(3ULL * d->instance_count);
         std::vector<uint4> inst_info(d->instance_count);
         std::vector<uint32_t> normal_offset(d->instance_count);
-        std::vector<uint32_t> tri_instance, tri_local;
+        uint64_t instance_triangles = 0;  // every instance's triangles, in instance order
         std::vector<LightInfo> lights;
         std::vector<float4> light_vertices, light_normals;
         std::vector<float> light_areas, light_cdf;
@@ -1576,11 +1665,11 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
             }
             inst_info[i] = make_uint4(inst.geometry_index, inst.material_index, inst.visibility_mask,
                                       light_index | (orientation < 0 ? 0x80000000U : 0U));
-            normal_offset[i] = static_cast<uint32_t>(tri_instance.size());
-            for (uint32_t t = 0; t < d->geometries[inst.geometry_index].triangle_count; ++t) {
-                tri_instance.push_back(i);
-                tri_local.push_back(t);
-            }
+            normal_offset[i] = static_cast<uint32_t>(instance_triangles);
+            instance_triangles += d->geometries[inst.geometry_index].triangle_count;
+        }
+        if (instance_triangles >= (1ULL << 32)) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "more than 2^32 - 1 instanced triangles");
         }
         // the light registry: punctual lights (slots [0, P)), then the mesh lights
         std::vector<bf200::PunctualLight> punctual(d->punctual_light_count);
@@ -1657,6 +1746,8 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
                 default: break;
             }
         }
+        stats.instance_ms = ms_since(t_instances);
+        const auto t_upload = Clock::now();
         std::vector<float> positions(d->positions, d->positions + 3ULL * d->vertex_count);
         std::vector<float> normals(d->normals, d->normals + 3ULL * d->vertex_count);
         std::vector<uint32_t> triangles(d->triangles, d->triangles + 3ULL * d->triangle_count);
@@ -1701,13 +1792,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         up(light_normals, v.light_tri_normals);
         up(light_areas, v.light_tri_areas);
         up(light_cdf, v.light_tri_cdf);
-        const uint32_t* d_tri_instance = nullptr;
-        const uint32_t* d_tri_local = nullptr;
-        up(tri_instance, d_tri_instance);
-        up(tri_local, d_tri_local);
-        scene->tri_instance = d_tri_instance;
-        scene->tri_local = d_tri_local;
-        scene->instance_triangles = static_cast<uint32_t>(tri_instance.size());
+        scene->instance_triangles = static_cast<uint32_t>(instance_triangles);
         scene->light_triangles = light_areas.size();
         if (st != BLACKFRAME_STATUS_SUCCESS) {
             return st;
@@ -1717,7 +1802,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         // world-space geometric normals of every instance triangle, on the device
         float4* world_normals = nullptr;
         uint32_t* failures = nullptr;
-        cudaError_t e = cudaMalloc(&world_normals, std::max<size_t>(16, tri_instance.size() * sizeof(float4)));
+        cudaError_t e = cudaMalloc(&world_normals, std::max<size_t>(16, instance_triangles * sizeof(float4)));
         if (e == cudaSuccess) {
             scene->allocations.push_back(world_normals);
             e = cudaMalloc(&failures, sizeof(uint32_t));
@@ -1727,8 +1812,7 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
             e = cudaMemsetAsync(failures, 0, sizeof(uint32_t), c->stream);
         }
         if (e == cudaSuccess) {
-            e = launch_world_normals(v, d_tri_instance, d_tri_local, static_cast<uint32_t>(tri_instance.size()),
-                                     world_normals, failures, c->stream);
+            e = launch_world_normals(v, scene->instance_triangles, world_normals, failures, c->stream);
         }
         uint32_t host_failures = 0;
         if (e == cudaSuccess) {
@@ -1745,10 +1829,38 @@ BF200_EXPORT blackframe_status bf200_scene_create(bf200_context* c, const bf200_
         }
         v.world_normals = world_normals;
         scene->normal_failures = failures;
+        stats.upload_ms = ms_since(t_upload);
+        stats.node_count = nodes4.size();
+        stats.leaf_triangle_count = leaf_tris.size() / 3;
+        stats.total_ms = ms_since(t_start);
     } catch (const std::bad_alloc&) {
         return fail(c, BLACKFRAME_STATUS_EXTENSION_FAILURE, "scene build exhausted host memory");
     }
     *out_scene = scene.release();
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT blackframe_status bf200_context_batch_lanes(const bf200_context* c, uint32_t* lanes) noexcept {
+    if (c == nullptr || lanes == nullptr) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    *lanes = c->last_batch_lanes;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT blackframe_status bf200_context_set_build_mode(bf200_context* c, uint32_t mode) noexcept {
+    if (c == nullptr || (mode != BF200_BUILD_HOST_SAH && mode != BF200_BUILD_DEVICE_LBVH)) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    c->build_mode = mode;
+    return BLACKFRAME_STATUS_SUCCESS;
+}
+
+BF200_EXPORT blackframe_status bf200_scene_stats(const bf200_scene* s, bf200_scene_stats_v1* out) noexcept {
+    if (s == nullptr || out == nullptr || out->struct_size < sizeof(bf200_scene_stats_v1)) {
+        return BLACKFRAME_STATUS_INVALID_ARGUMENT;
+    }
+    *out = s->stats;
     return BLACKFRAME_STATUS_SUCCESS;
 }
 
@@ -1876,8 +1988,8 @@ BF200_EXPORT blackframe_status bf200_scene_refit(bf200_scene* s, const bf200_sce
         }
         if (e == cudaSuccess) e = cudaMemsetAsync(s->normal_failures, 0, sizeof(uint32_t), st);
         if (e == cudaSuccess) {
-            e = launch_world_normals(v, s->tri_instance, s->tri_local, s->instance_triangles,
-                                     const_cast<float4*>(v.world_normals), s->normal_failures, st);
+            e = launch_world_normals(v, s->instance_triangles, const_cast<float4*>(v.world_normals), s->normal_failures,
+                                     st);
         }
         uint32_t failures = 0;
         if (e == cudaSuccess) {
@@ -2948,52 +3060,13 @@ void lane_report(const bf200_film_job_v1& job, const LaneState& lane) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-BF200_EXPORT blackframe_status bf200_render_films_device(bf200_context* c, const bf200_film_job_v1* jobs,
-                                                         uint32_t job_count, uint32_t lanes) noexcept {
-    if (c == nullptr || (job_count != 0 && jobs == nullptr)) {
-        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
-    }
-    std::vector<uint64_t> job_paths(job_count);
-    for (uint32_t j = 0; j < job_count; ++j) {
-        const bf200_film_job_v1& job = jobs[j];
-        const bf200_camera_v1* cam = job.camera;
-        const bf200_film_request_v1* req = job.request;
-        const bf200_film_v1* film = job.film;
-        if (job.struct_size < sizeof(bf200_film_job_v1) || job.scene == nullptr || cam == nullptr ||
-            job.sensor == nullptr || req == nullptr || job.options == nullptr || film == nullptr) {
-            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "film job with a missing argument");
-        }
-        if (job.scene->context != c) {
-            return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "film job scene belongs to another context");
-        }
-        if (req->struct_size < sizeof(bf200_film_request_v1) || req->precision > 1 ||
-            film->precision != req->precision || film->width != cam->width || film->height != cam->height ||
-            cam->width == 0 || cam->height == 0 || film->sums == nullptr || film->sample_counts == nullptr) {
-            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "inconsistent film request in a batch");
-        }
-        if (const auto st = validate_options(c, job.options); st != BLACKFRAME_STATUS_SUCCESS) {
-            return st;
-        }
-        const uint64_t pixels = static_cast<uint64_t>(cam->width) * cam->height;
-        if (pixels > 0xFFFFFFFFULL) {
-            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "film too large");
-        }
-        job_paths[j] = pixels * req->samples_per_pixel;
-    }
-    for (uint32_t j = 0; j < job_count; ++j) {
-        if (jobs[j].report != nullptr) {
-            std::memset(jobs[j].report, 0, sizeof(bf200_report_v1));
-        }
-    }
-    if (job_count == 0) {
-        return BLACKFRAME_STATUS_SUCCESS;
-    }
+// Renders jobs[0, job_count) in lane_count concurrent wavefront lanes (the body of
+// bf200_render_films_device once its arguments are checked); returns after every lane drained.
+blackframe_status run_batch(bf200_context* c, const bf200_film_job_v1* jobs, uint32_t job_count,
+                            uint32_t lane_count) {
     cudaSetDevice(c->device);
-    const uint32_t lane_count = std::min<uint32_t>(
-        lanes != 0 ? std::min<uint32_t>(lanes, kMaxLanes) : autotune_lanes(c->capacity, job_paths),
-        job_count);
     const uint32_t slice = static_cast<uint32_t>(std::max<uint64_t>(4096, (c->capacity / lane_count) & ~4095ULL));
     const size_t slice_bytes = (carve_wavefront(nullptr, slice, nullptr) + 255) & ~size_t(255);
     if (const auto st = grow_workspace(c, &c->lane_arena, &c->lane_arena_bytes, slice_bytes * lane_count,
@@ -3155,6 +3228,107 @@ BF200_EXPORT blackframe_status bf200_render_films_device(bf200_context* c, const
     }
     drain();
     return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+BF200_EXPORT blackframe_status bf200_render_films_device(bf200_context* c, const bf200_film_job_v1* jobs,
+                                                         uint32_t job_count, uint32_t lanes) noexcept {
+    if (c == nullptr || (job_count != 0 && jobs == nullptr)) {
+        return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "null argument");
+    }
+    std::vector<uint64_t> job_paths(job_count);
+    for (uint32_t j = 0; j < job_count; ++j) {
+        const bf200_film_job_v1& job = jobs[j];
+        const bf200_camera_v1* cam = job.camera;
+        const bf200_film_request_v1* req = job.request;
+        const bf200_film_v1* film = job.film;
+        if (job.struct_size < sizeof(bf200_film_job_v1) || job.scene == nullptr || cam == nullptr ||
+            job.sensor == nullptr || req == nullptr || job.options == nullptr || film == nullptr) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "film job with a missing argument");
+        }
+        if (job.scene->context != c) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_STATE, "film job scene belongs to another context");
+        }
+        if (req->struct_size < sizeof(bf200_film_request_v1) || req->precision > 1 ||
+            film->precision != req->precision || film->width != cam->width || film->height != cam->height ||
+            cam->width == 0 || cam->height == 0 || film->sums == nullptr || film->sample_counts == nullptr) {
+            return fail(c, BLACKFRAME_STATUS_INVALID_ARGUMENT, "inconsistent film request in a batch");
+        }
+        if (const auto st = validate_options(c, job.options); st != BLACKFRAME_STATUS_SUCCESS) {
+            return st;
+        }
+        const uint64_t pixels = static_cast<uint64_t>(cam->width) * cam->height;
+        if (pixels > 0xFFFFFFFFULL) {
+            return fail(c, BLACKFRAME_STATUS_OUT_OF_RANGE, "film too large");
+        }
+        job_paths[j] = pixels * req->samples_per_pixel;
+    }
+    for (uint32_t j = 0; j < job_count; ++j) {
+        if (jobs[j].report != nullptr) {
+            std::memset(jobs[j].report, 0, sizeof(bf200_report_v1));
+        }
+    }
+    if (job_count == 0) {
+        return BLACKFRAME_STATUS_SUCCESS;
+    }
+    if (lanes != 0) {
+        c->last_batch_lanes = std::min<uint32_t>(std::min<uint32_t>(lanes, kMaxLanes), job_count);
+        return run_batch(c, jobs, job_count, c->last_batch_lanes);
+    }
+    // The lane count by measurement: the context keeps the fastest count per job-size class (the
+    // binary order of magnitude of the median job's paths). A class seen for the first time is
+    // measured on this batch's own jobs when there are enough of them: consecutive groups of jobs
+    // run with 2, 4 and 8 lanes, each group timed to its drain, and the count with the highest
+    // path rate serves the remaining jobs and later batches. Films do not depend on the lane
+    // count, so the measured groups are part of the result. Small batches use the closed-form
+    // estimate until a larger batch has measured their class.
+    std::vector<uint64_t> sorted = job_paths;
+    std::nth_element(sorted.begin(), sorted.begin() + job_count / 2, sorted.end());
+    uint32_t size_class = 0;
+    for (uint64_t m = std::max<uint64_t>(1, sorted[job_count / 2]); m > 1; m >>= 1) {
+        ++size_class;
+    }
+    const auto known = c->batch_lanes_by_class.find(size_class);
+    if (known != c->batch_lanes_by_class.end()) {
+        c->last_batch_lanes = std::min<uint32_t>(known->second, job_count);
+        return run_batch(c, jobs, job_count, c->last_batch_lanes);
+    }
+    constexpr uint32_t kCandidates[] = {2, 4, 8};
+    const uint32_t group = std::max<uint32_t>(8, job_count / 8);
+    if (job_count < 4 * group) {
+        c->last_batch_lanes = std::min<uint32_t>(autotune_lanes(c->capacity, job_paths), job_count);
+        return run_batch(c, jobs, job_count, c->last_batch_lanes);
+    }
+    // the measured jobs are the first 3 x group, dealt round-robin to the candidates so that each
+    // count sees the same mix of job sizes
+    constexpr uint32_t kCount = sizeof(kCandidates) / sizeof(kCandidates[0]);
+    const uint32_t measured = kCount * group;
+    uint32_t best = kCandidates[0];
+    double best_rate = -1.0;
+    std::vector<bf200_film_job_v1> dealt(group);
+    for (uint32_t k = 0; k < kCount; ++k) {
+        uint64_t paths = 0;
+        for (uint32_t g = 0; g < group; ++g) {
+            dealt[g] = jobs[g * kCount + k];
+            paths += job_paths[g * kCount + k];
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        if (const auto st = run_batch(c, dealt.data(), group, kCandidates[k]); st != BLACKFRAME_STATUS_SUCCESS) {
+            return st;
+        }
+        const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        const double rate = static_cast<double>(paths) / std::max(seconds, 1e-9);
+        if (rate > best_rate) {
+            best_rate = rate;
+            best = kCandidates[k];
+        }
+    }
+    c->batch_lanes_by_class[size_class] = best;
+    c->last_batch_lanes = best;
+    return run_batch(c, jobs + measured, job_count - measured, std::min<uint32_t>(best, job_count - measured));
 }
 
 static blackframe_status run_queries(bf200_context* c, const bf200_scene* s, const bf200_ray_v1* rays, uint64_t n,

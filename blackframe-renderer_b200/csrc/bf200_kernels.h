@@ -3,12 +3,14 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "bf200_device.cuh"
 
 namespace bf200 {
 
-cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instance, const uint32_t* tri_local,
-                                 uint32_t total, float4* out, uint32_t* failures, cudaStream_t stream);
+cudaError_t launch_world_normals(const SceneView& s, uint32_t total, float4* out, uint32_t* failures,
+                                 cudaStream_t stream);
 // stage 0: k_regenerate; 1: k_trace; 2: route compaction, the per-route k_shade kernels, shadow
 // compaction; 3: k_occlude. Adds the number of kernels launched to *launches. With `adjoint`, the
 // shading and occlusion stages run as the path-replay adjoint's replay.
@@ -22,6 +24,12 @@ cudaError_t launch_stage(int stage, const SceneView& s, const Wavefront& w, cons
 cudaError_t launch_compaction(const uint8_t* keys, uint32_t n, uint32_t routes, uint32_t* tile_counts,
                               uint32_t* queue, uint32_t* offsets, unsigned long long* total, uint8_t* reset_keys,
                               cudaStream_t stream, uint32_t* launches);
+// Device BLAS build of one triangle geometry (bf200_lbvh.cu): a linear BVH whose BVH2 nodes (host
+// builder format, node codes offset by node_base, leaf records by leaf_base) and leaf triangle
+// records are appended to `nodes` and `leaf_tris`. Host arrays in; waits for the stream.
+cudaError_t build_blas_lbvh(const float* positions, uint32_t vertex_count, const uint32_t* triangles, uint32_t n,
+                            uint32_t node_base, uint32_t leaf_base, std::vector<BvhNode>& nodes,
+                            std::vector<float4>& leaf_tris, cudaStream_t stream);
 // Queues k_iteration_gate, which ends one iteration of a graph's device-side wavefront loop: it
 // accumulates the shadow segments (counters[4]), counts iterations (counters[9]), clears the
 // per-iteration counters and sets `loop` to continue until the wavefront drains or

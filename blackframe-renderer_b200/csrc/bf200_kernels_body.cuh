@@ -60,11 +60,21 @@ __device__ __forceinline__ F3 load_vertex(const float* p, uint32_t i) { return {
 #ifdef BF200_KERNELS_MAIN_TU
 // World-space geometric normal of every instance triangle: the normal the analytic accel
 // reports for a hit (AccelBackend.cpp:84-97, Triangle.hpp:374-481).
-__global__ void k_world_normals(SceneView s, const uint32_t* tri_instance, const uint32_t* tri_local,
-                                uint32_t total, float4* out, uint32_t* failures) {
+__global__ void k_world_normals(SceneView s, uint32_t total, float4* out, uint32_t* failures) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        const uint32_t inst = tri_instance[i];
-        const uint32_t prim = tri_local[i];
+        // the instance whose triangle range [inst_normal_offset[inst], next offset) holds i: the
+        // last instance starting at or before i (empty ranges start where the next one does)
+        uint32_t lo = 0, hi = s.instance_count;
+        while (hi - lo > 1U) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s.inst_normal_offset[mid] <= i) {
+                lo = mid;
+            } else {
+                hi = mid;
+            }
+        }
+        const uint32_t inst = lo;
+        const uint32_t prim = i - s.inst_normal_offset[inst];
         const uint4 info = s.inst_info[inst];
         const uint4 geom = s.geom_info[info.x];
         const uint32_t* tri = s.triangles + 3ULL * (geom.y + prim);
@@ -2773,14 +2783,13 @@ cudaError_t launch_gate(const Wavefront& w, uint64_t total, uint64_t max_iterati
 }
 
 
-cudaError_t launch_world_normals(const SceneView& s, const uint32_t* tri_instance, const uint32_t* tri_local,
-                                 uint32_t total, float4* out, uint32_t* failures, cudaStream_t stream) {
+cudaError_t launch_world_normals(const SceneView& s, uint32_t total, float4* out, uint32_t* failures,
+                                 cudaStream_t stream) {
     if (total == 0U) {
         return cudaSuccess;
     }
     const uint32_t blocks = (total + 127U) / 128U;
-    k_world_normals<<<blocks < 4096U ? blocks : 4096U, 128, 0, stream>>>(s, tri_instance, tri_local, total, out,
-                                                                          failures);
+    k_world_normals<<<blocks < 4096U ? blocks : 4096U, 128, 0, stream>>>(s, total, out, failures);
     return cudaGetLastError();
 }
 

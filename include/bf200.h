@@ -625,6 +625,15 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_render_films_device(bf200_co
                                                                         uint32_t job_count, uint32_t lanes)
     BF200_NOEXCEPT;
 
+/* The lane count the context's last bf200_render_films_device call used. With lanes = 0 the count is
+ * chosen by measurement: the context keeps the fastest of 2, 4 and 8 lanes per job-size class (the
+ * binary order of magnitude of the median job's paths), measuring a new class on the batch's own
+ * first jobs (dealt round-robin into three groups of at least eight jobs, one per count, each timed to
+ * its drain) when the
+ * batch holds at least four such groups, and using a closed-form estimate otherwise. */
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_context_batch_lanes(const bf200_context* context,
+                                                                       uint32_t* lanes) BF200_NOEXCEPT;
+
 /* Path-replay adjoint (the reference has no differentiation; its benchmark plan asks a new backend
  * for an adjoint of the film render). One call renders the film, compares the image with a target
  * and returns the gradient of the loss
@@ -953,6 +962,39 @@ BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_sobol_bits(uint64_t sample_i
 BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_owen_sobol_bits(const bf200_sample_index_v1* index,
                                                                     uint64_t sobol_dimension,
                                                                     uint64_t* out_bits) BF200_NOEXCEPT;
+
+/* BLAS build of the scenes a context creates. BF200_BUILD_HOST_SAH (the default): binned SAH on
+ * the host, collapsed to BVH4, like the reference's CudaSceneBvh::build. BF200_BUILD_DEVICE_LBVH:
+ * triangle geometries of at least 4,096 triangles are built on the GPU as a linear BVH (Morton
+ * order, Karras' hierarchy, leaves of at most four triangles) in a fraction of the time, at some
+ * cost in traversal speed; smaller geometries, spheres and the TLAS stay on the host, and a device
+ * tree too deep for the traversal stack is rebuilt on the host. Hits are identical either way.
+ * Scenes already created keep their build. */
+#define BF200_BUILD_HOST_SAH 0u
+#define BF200_BUILD_DEVICE_LBVH 1u
+
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_context_set_build_mode(bf200_context* context,
+                                                                          uint32_t mode) BF200_NOEXCEPT;
+
+/* Build statistics of a scene: its sizes and the host wall time of each phase of
+ * bf200_scene_create (BLAS builds, BVH2-to-BVH4 collapse, the instance level with its TLAS and
+ * mesh lights, then the uploads and the world-normal kernel). The caller sets struct_size. */
+typedef struct bf200_scene_stats_v1 {
+    uint32_t struct_size;
+    uint32_t blas_depth;              /* deepest BLAS, in BVH4 levels */
+    uint32_t device_built_geometries; /* BLASes built on the device (BF200_BUILD_DEVICE_LBVH) */
+    uint32_t reserved;
+    uint64_t node_count;              /* BVH4 nodes of every BLAS and the TLAS */
+    uint64_t leaf_triangle_count;     /* leaf records (triangles and spheres) */
+    double blas_build_ms;
+    double collapse_ms;
+    double instance_ms;
+    double upload_ms;
+    double total_ms;
+} bf200_scene_stats_v1;
+
+BF200_EXTERN_C BF200_EXPORT blackframe_status bf200_scene_stats(const bf200_scene* scene,
+                                                               bf200_scene_stats_v1* out) BF200_NOEXCEPT;
 
 /* ---- Native scene JSON (engine::SceneDescriptionJson.hpp, schema "blackframe.scene" v1) ----
  * bf200_scene_json_parse replaces deserialize_scene_description_json

@@ -37,7 +37,8 @@ def test_record_layouts_match_the_header(repo_root, tmp_path):
              "bf200_transport_options_v1", "bf200_camera_v1", "bf200_sensor_v1",
              "bf200_film_request_v1", "bf200_report_v1", "bf200_hit_v1", "blackframe_extension_api_v1",
              "blackframe_xpu_device_descriptor_v1", "bf200_scene_desc_v1", "bf200_film_v1", "bf200_ray_cone_v1", "bf200_path_state_v1",
-             "bf200_light_tree_input_v1", "bf200_scene_json_limits_v1", "bf200_scene_json_frame_v1"]
+             "bf200_light_tree_input_v1", "bf200_scene_json_limits_v1", "bf200_scene_json_frame_v1",
+             "bf200_scene_stats_v1"]
     body = "".join(f'printf("%zu\\n", sizeof({n}));' for n in names)
     probe.write_text(f'#include "bf200.h"\n#include <stdio.h>\nint main(void){{{body}return 0;}}\n')
     exe = tmp_path / "layout"
@@ -47,7 +48,7 @@ def test_record_layouts_match_the_header(repo_root, tmp_path):
     records = [abi.Closure, abi.Material, abi.Geometry, abi.Instance, abi.Ray, abi.SampleIndex, abi.PathInput,
                abi.PathResult, abi.TransportOptions, abi.Camera, abi.Sensor, abi.FilmRequest, abi.Report, abi.Hit,
                abi.ExtensionApi, abi.XpuDeviceDescriptor, abi.SceneDesc, abi.Film, abi.RayCone, abi.PathState, abi.LightTreeInput,
-               abi.SceneJsonLimits, abi.SceneJsonFrame]
+               abi.SceneJsonLimits, abi.SceneJsonFrame, abi.SceneStats]
     assert sizes == [C.sizeof(r) for r in records]
 
 

@@ -77,6 +77,33 @@ def test_batch_films_equal_single_renders(setup, lanes):
         assert reports[k].path_count == w * h * spp and reports[k].failed_lanes == 0
 
 
+def test_measured_lane_count_keeps_every_film(setup):
+    """A batch of 40 jobs with lanes = 0 measures 2, 4 and 8 lanes on its first 24 jobs, keeps the
+    fastest for the other 16 and for the next batch of the same job size; every film still equals
+    its single render."""
+    torch, ctx, built, sensor = setup
+    name = "cornell_plain_64"
+    scene = built[name][1]
+    options = abi.default_options(mis="balance", max_depth=6)
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), 40, 32, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+    spec = (name, 40, 32, 2, 0, 0, 0, 6, 0)
+    for batch in range(2):
+        jobs, films = [], []
+        for k in range(40):
+            sums, counts = _films(torch, spec)
+            jobs.append((scene, cam, sensor, options, 2, 100 * batch + k, 0, 0, sums.data_ptr(), counts.data_ptr()))
+            films.append((sums, counts, 100 * batch + k))
+        ctx.render_films_device(jobs, lanes=0)
+        torch.cuda.synchronize()
+        assert ctx.batch_lanes() in (2, 4, 8)
+        for sums, counts, seed in films[::7]:
+            single_sums, single_counts = _films(torch, spec)
+            ctx.render_film_device(scene, cam, sensor, options, 2, seed, 0, 0, single_sums.data_ptr(),
+                                   single_counts.data_ptr())
+            assert torch.equal(counts, single_counts)
+            assert np.array_equal(sums.cpu().numpy().view(np.uint8), single_sums.cpu().numpy().view(np.uint8))
+
+
 def test_batch_rejects_a_foreign_scene(setup):
     torch, ctx, built, sensor = setup
     builder = built["cornell_plain_64"][0]
