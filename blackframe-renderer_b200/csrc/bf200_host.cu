@@ -553,7 +553,21 @@ struct Collapser {
     // Builds the BVH4 node for BVH2 node `index`; returns its index in `out`.
     int collapse(int index, uint32_t depth, uint32_t& max_depth) {
         max_depth = std::max(max_depth, depth);
-        std::vector<Slot> slots;
+        // at most 4 slots at once: an expansion removes one slot and adds two, from at most 3
+        Slot slot_store[6];
+        struct {
+            Slot* data;
+            int count;
+            int size() const { return count; }
+            Slot& operator[](int k) { return data[k]; }
+            void push_back(const Slot& v) { data[count++] = v; }
+            void erase_at(int k) {
+                for (int m = k + 1; m < count; ++m) {
+                    data[m - 1] = data[m];
+                }
+                --count;
+            }
+        } slots{slot_store, 0};
         for (int k = 0; k < 2; ++k) {
             const Box b = child_box(bvh2[index], k);
             if (!empty(b)) {
@@ -563,7 +577,7 @@ struct Collapser {
         while (slots.size() < 4) {
             int open = -1;
             double best = -1.0;
-            for (int k = 0; k < static_cast<int>(slots.size()); ++k) {
+            for (int k = 0; k < slots.size(); ++k) {
                 if (slots[k].code >= 0 && slots[k].box.area() > best) {
                     best = slots[k].box.area();
                     open = k;
@@ -573,7 +587,7 @@ struct Collapser {
                 break;
             }
             const BvhNode& n = bvh2[slots[open].code];
-            slots.erase(slots.begin() + open);
+            slots.erase_at(open);
             for (int k = 0; k < 2; ++k) {
                 const Box b = child_box(n, k);
                 if (!empty(b)) {
@@ -584,15 +598,15 @@ struct Collapser {
         const int me = static_cast<int>(out.size());
         out.push_back(BvhNode4{});
         int child[4] = {0, 0, 0, 0};
-        for (size_t k = 0; k < slots.size(); ++k) {
+        for (int k = 0; k < slots.size(); ++k) {
             child[k] = slots[k].code >= 0 ? collapse(slots[k].code, depth + 1, max_depth) : slots[k].code;
         }
         const float inf = std::numeric_limits<float>::infinity();
         float lo[3][4], hi[3][4];
         for (int k = 0; k < 4; ++k) {
             for (int a = 0; a < 3; ++a) {
-                lo[a][k] = k < static_cast<int>(slots.size()) ? slots[k].box.lo[a] : inf;
-                hi[a][k] = k < static_cast<int>(slots.size()) ? slots[k].box.hi[a] : -inf;
+                lo[a][k] = k < slots.size() ? slots[k].box.lo[a] : inf;
+                hi[a][k] = k < slots.size() ? slots[k].box.hi[a] : -inf;
             }
         }
         BvhNode4& node = out[me];

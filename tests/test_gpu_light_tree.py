@@ -84,3 +84,32 @@ def test_tree_selected_paths_match_the_oracle():
     assert exact >= 0.8
     assert (~bit_equal(arrays(uniform)["radiance"], got["radiance"]).all(axis=1)).mean() > 0.3
     assert bit_equal(arrays(again)["radiance"], arrays(uniform)["radiance"]).all()
+
+
+def test_repeated_tree_updates_keep_device_memory_flat():
+    """A caller sets the tree again after every refit and may clear it in between: the scene reuses
+    its tree buffers (or frees them when the tree is cleared), so free device memory after 50 such
+    rounds is where the first tree left it."""
+    import importlib.util
+    import os
+    import torch
+    from test_gpu_light_power import three_light_box
+    spec = importlib.util.spec_from_file_location(
+        "make_light_tree_golden", os.path.join(os.path.dirname(__file__), "golden", "make_light_tree_golden.py"))
+    maker = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(maker)
+    builder = three_light_box()
+    lights = maker.tree_box_inputs(builder)
+    with runtime.Context(0, path_capacity=1 << 12) as ctx:
+        scene = ctx.create_scene(builder)
+        scene.set_light_tree(lights)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        for _ in range(50):
+            scene.set_light_tree(lights)
+            scene.set_light_tree(None)
+            scene.set_light_tree(lights)
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        scene.close()
+    assert free_after >= free_before - (2 << 20), f"{(free_before - free_after) >> 20} MiB lost"
