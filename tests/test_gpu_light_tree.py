@@ -113,3 +113,82 @@ def test_repeated_tree_updates_keep_device_memory_flat():
         free_after = torch.cuda.mem_get_info()[0]
         scene.close()
     assert free_after >= free_before - (2 << 20), f"{(free_before - free_after) >> 20} MiB lost"
+
+
+def _tree_box():
+    import importlib.util
+    import os
+    from test_gpu_light_power import three_light_box
+    spec = importlib.util.spec_from_file_location(
+        "make_light_tree_golden", os.path.join(os.path.dirname(__file__), "golden", "make_light_tree_golden.py"))
+    maker = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(maker)
+    builder = three_light_box()
+    return builder, maker.tree_box_inputs(builder)
+
+
+def test_tree_selection_on_the_cone_path_and_after_a_refit():
+    """With the tree set, the cone-carrying trace (its own shading instantiation) gives the plain
+    trace's radiance on every lane both complete, and a refit followed by setting the tree again
+    gives the plain trace's results bit for bit."""
+    import numpy as np
+    from bf200 import abi
+    from helpers import arrays, bit_equal
+    from oracle.bindings import Oracle
+    from test_gpu_light_power import path_inputs
+    builder, lights = _tree_box()
+    inputs = path_inputs(Oracle(device_trig=True), 4096, 37)
+    options = abi.default_options(mis="power", max_depth=8)
+    cones = np.tile(np.array([[0.0, 1e-3]], np.float32), (len(inputs), 1))
+    with runtime.Context(0, path_capacity=1 << 16) as ctx:
+        scene = ctx.create_scene(builder)
+        scene.set_light_tree(lights)
+        plain, _ = ctx.trace_paths(scene, inputs, options)
+        coned, _, report = ctx.trace_paths_with_cones(scene, inputs, cones, options)
+        scene.refit(builder)
+        scene.set_light_tree(lights)
+        again, _ = ctx.trace_paths(scene, inputs, options)
+        scene.close()
+    p, c, a = arrays(plain), arrays(coned), arrays(again)
+    both = (p["lane_status"] == 0) & (c["lane_status"] == 0)
+    assert both.mean() > 0.99 and report.closure_samples > 0
+    assert bit_equal(p["radiance"][both], c["radiance"][both]).all()
+    assert bit_equal(p["radiance"], a["radiance"]).all() and (p["termination"] == a["termination"]).all()
+
+
+def test_tree_film_equals_the_tree_trace():
+    """A film rendered with the tree set equals, pixel for pixel within the parity tolerance, the
+    film accumulated from the tree-selecting trace of the same (pixel, sample) paths (that trace is
+    checked against the oracle's tree transport above)."""
+    import os
+    import numpy as np
+    from bf200 import abi, scenes
+    from helpers import DIVERGED_FRACTION, RELATIVE_TOLERANCE, arrays, relative_error, sensor_from_golden
+    from oracle.bindings import Oracle
+    builder, lights = _tree_box()
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "cornell_spheres_256.npz"))
+    sensor = sensor_from_golden(g)
+    width, height, spp = 32, 32, 2
+    cam = runtime.camera_create(*scenes.camera_frame_inputs(), width, height, scenes.CAMERA_VFOV, scenes.PATH_TIME)
+    options = abi.default_options(mis="power", max_depth=8)
+    px, py, s = np.meshgrid(np.arange(width), np.arange(height), np.arange(spp), indexing="ij")
+    order = np.lexsort((px.ravel(), py.ravel(), s.ravel()))
+    px, py, s = px.ravel()[order], py.ravel()[order], s.ravel()[order]
+    samples = (abi.SampleIndex * len(px))()
+    for k in range(len(px)):
+        samples[k].pixel_x, samples[k].pixel_y, samples[k].sample_index = int(px[k]), int(py[k]), int(s[k])
+    oracle = Oracle(device_trig=True)
+    rays = oracle.camera_rays(cam, samples)
+    inputs = (abi.PathInput * len(px))()
+    for k in range(len(px)):
+        inputs[k].primary_ray, inputs[k].sample = rays[k], samples[k]
+    with runtime.Context(0, path_capacity=1 << 16) as ctx:
+        scene = ctx.create_scene(builder)
+        scene.set_light_tree(lights)
+        sums, counts, _ = ctx.render_film(scene, cam, sensor, options, spp, seed=0)
+        results, _ = ctx.trace_paths(scene, inputs, options)
+        scene.close()
+    expected, _ = oracle.film(arrays(results)["radiance"], samples, sensor, width, height, 0)
+    assert (counts == spp).all()
+    err = relative_error(sums.astype(np.float64), expected)
+    assert (err <= RELATIVE_TOLERANCE).mean() >= 1.0 - DIVERGED_FRACTION
