@@ -4,7 +4,7 @@
 //
 //   k_lbvh_bounds    per triangle: its box and centroid (the host build's box and 0.5 lo + 0.5 hi),
 //                    and the centroid bounds of the geometry (warp min/max, one atomic per warp)
-//   k_lbvh_morton    30-bit Morton code of the centroid on a 1024^3 grid over those bounds
+//   k_lbvh_morton    63-bit Morton code of the centroid on a 2^21-per-axis grid over those bounds
 //   sort             stable LSD radix sort of (code, triangle) pairs, 2 bits per pass: each pass is
 //                    the wavefront's stable route compaction with 4 routes (bf200_compact.cu) and a
 //                    gather, so equal codes keep triangle order and the tree is deterministic
@@ -37,7 +37,7 @@ namespace {
 
 constexpr int kLbvhLeaf = 4;  // the host build's leaf bound (kLeafSize)
 constexpr uint32_t kLbvhThreads = 256;
-constexpr int kMortonBits = 30;
+constexpr int kMortonBits = 63;
 
 __device__ __forceinline__ uint32_t ordered_bits(float f) {
     const uint32_t u = __float_as_uint(f);
@@ -89,35 +89,38 @@ __global__ void __launch_bounds__(kLbvhThreads) k_lbvh_bounds(const float* __res
     }
 }
 
-__device__ __forceinline__ uint32_t spread_bits(uint32_t x) {  // 10 bits -> every third bit
-    x = (x * 0x00010001U) & 0xFF0000FFU;
-    x = (x * 0x00000101U) & 0x0F00F00FU;
-    x = (x * 0x00000011U) & 0xC30C30C3U;
-    x = (x * 0x00000005U) & 0x49249249U;
+__device__ __forceinline__ unsigned long long spread_bits(unsigned long long x) {  // 21 bits -> every third bit
+    x &= 0x1FFFFFULL;
+    x = (x | x << 32) & 0x1F00000000FFFFULL;
+    x = (x | x << 16) & 0x1F0000FF0000FFULL;
+    x = (x | x << 8) & 0x100F00F00F00F00FULL;
+    x = (x | x << 4) & 0x10C30C30C30C30C3ULL;
+    x = (x | x << 2) & 0x1249249249249249ULL;
     return x;
 }
 
 __global__ void __launch_bounds__(kLbvhThreads) k_lbvh_morton(const float4* __restrict__ centroid, uint32_t n,
                                                               const uint32_t* __restrict__ centroid_bounds,
-                                                              uint32_t* __restrict__ keys, uint32_t* __restrict__ ids) {
+                                                              unsigned long long* __restrict__ keys,
+                                                              uint32_t* __restrict__ ids) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) {
         return;
     }
     const float4 c = centroid[t];
     const float cv[3] = {c.x, c.y, c.z};
-    uint32_t q[3];
+    unsigned long long q[3];
     for (int a = 0; a < 3; ++a) {
         const float lo = from_ordered_bits(centroid_bounds[a]);
         const float extent = from_ordered_bits(centroid_bounds[3 + a]) - lo;
-        const float u = extent > 0.0F ? (cv[a] - lo) / extent * 1024.0F : 0.0F;
-        q[a] = static_cast<uint32_t>(fminf(fmaxf(u, 0.0F), 1023.0F));
+        const float u = extent > 0.0F ? (cv[a] - lo) / extent * 2097152.0F : 0.0F;
+        q[a] = static_cast<unsigned long long>(fminf(fmaxf(u, 0.0F), 2097151.0F));
     }
     keys[t] = (spread_bits(q[0]) << 2) | (spread_bits(q[1]) << 1) | spread_bits(q[2]);
     ids[t] = t;
 }
 
-__global__ void __launch_bounds__(kLbvhThreads) k_lbvh_digits(const uint32_t* __restrict__ keys, uint32_t n,
+__global__ void __launch_bounds__(kLbvhThreads) k_lbvh_digits(const unsigned long long* __restrict__ keys, uint32_t n,
                                                               uint32_t shift, uint8_t* __restrict__ digits) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
@@ -125,10 +128,10 @@ __global__ void __launch_bounds__(kLbvhThreads) k_lbvh_digits(const uint32_t* __
     }
 }
 
-__global__ void __launch_bounds__(kLbvhThreads) k_lbvh_gather(const uint32_t* __restrict__ keys_in,
+__global__ void __launch_bounds__(kLbvhThreads) k_lbvh_gather(const unsigned long long* __restrict__ keys_in,
                                                               const uint32_t* __restrict__ ids_in,
                                                               const uint32_t* __restrict__ order, uint32_t n,
-                                                              uint32_t* __restrict__ keys_out,
+                                                              unsigned long long* __restrict__ keys_out,
                                                               uint32_t* __restrict__ ids_out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
@@ -138,22 +141,22 @@ __global__ void __launch_bounds__(kLbvhThreads) k_lbvh_gather(const uint32_t* __
     }
 }
 
-// Common-prefix length of the sorted keys at positions i and j, each made unique by its position
-// (the code in the high word); -1 outside [0, n).
-__device__ __forceinline__ int prefix(const uint32_t* keys, int n, int i, int j) {
+// Common-prefix length of the sorted keys at positions i and j, each key made unique by its
+// position appended below the code (so equal codes continue into the positions' bits); -1 outside
+// [0, n).
+__device__ __forceinline__ int prefix(const unsigned long long* keys, int n, int i, int j) {
     if (j < 0 || j >= n) {
         return -1;
     }
-    const unsigned long long a = (static_cast<unsigned long long>(keys[i]) << 32) | static_cast<uint32_t>(i);
-    const unsigned long long b = (static_cast<unsigned long long>(keys[j]) << 32) | static_cast<uint32_t>(j);
-    return __clzll(a ^ b);
+    const unsigned long long a = keys[i], b = keys[j];
+    return a != b ? __clzll(a ^ b) : 64 + __clz(static_cast<uint32_t>(i ^ j));
 }
 
 __device__ __forceinline__ int leaf_code(uint32_t first, int count) {
     return ~static_cast<int>((first << kLeafCountBits) | static_cast<uint32_t>(count - 1));
 }
 
-__global__ void __launch_bounds__(kLbvhThreads) k_lbvh_hierarchy(const uint32_t* __restrict__ keys, int n,
+__global__ void __launch_bounds__(kLbvhThreads) k_lbvh_hierarchy(const unsigned long long* __restrict__ keys, int n,
                                                                  uint32_t node_base, uint32_t leaf_base,
                                                                  BvhNode* __restrict__ nodes, int* __restrict__ parent,
                                                                  int4* __restrict__ ranges) {
@@ -312,7 +315,7 @@ cudaError_t build_blas_lbvh(const float* positions, uint32_t vertex_count, const
     //  0 positions, 1 triangles, 2 box lo, 3 box hi, 4 centroids, 5-6 keys, 7-8 triangle ids,
     //  9 sort order, 10 digits, 11 compaction tile counts, 12 centroid bounds and route offsets,
     //  13 BVH2 nodes, 14 parents + arrival counters + ranges, 15 leaf records
-    const size_t sizes[16] = {bytes_positions, bytes_triangles, 16ULL * n, 16ULL * n, 16ULL * n, 4ULL * n, 4ULL * n,
+    const size_t sizes[16] = {bytes_positions, bytes_triangles, 16ULL * n, 16ULL * n, 16ULL * n, 8ULL * n, 8ULL * n,
                               4ULL * n, 4ULL * n, 4ULL * n, static_cast<size_t>(n), 4ULL * kCompactMaxRoutes * tiles,
                               64, sizeof(BvhNode) * (n - 1), 8ULL * (n - 1) + 16 + 16ULL * (n - 1), 48ULL * n};
     size_t offsets[16] = {};
@@ -331,7 +334,8 @@ cudaError_t build_blas_lbvh(const float* positions, uint32_t vertex_count, const
     float4* d_lo = reinterpret_cast<float4*>(base + offsets[2]);
     float4* d_hi = reinterpret_cast<float4*>(base + offsets[3]);
     float4* d_centroid = reinterpret_cast<float4*>(base + offsets[4]);
-    uint32_t* keys[2] = {reinterpret_cast<uint32_t*>(base + offsets[5]), reinterpret_cast<uint32_t*>(base + offsets[6])};
+    unsigned long long* keys[2] = {reinterpret_cast<unsigned long long*>(base + offsets[5]),
+                                   reinterpret_cast<unsigned long long*>(base + offsets[6])};
     uint32_t* ids[2] = {reinterpret_cast<uint32_t*>(base + offsets[7]), reinterpret_cast<uint32_t*>(base + offsets[8])};
     uint32_t* order = reinterpret_cast<uint32_t*>(base + offsets[9]);
     uint8_t* digits = reinterpret_cast<uint8_t*>(base + offsets[10]);
