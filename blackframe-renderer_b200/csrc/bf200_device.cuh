@@ -204,7 +204,7 @@ struct Wavefront {
     uint32_t* mask;     // ray visibility mask of the path
     float2* cone;       // ray cone (width, spread) at the ray origin; null unless cones are traced
     float4* hit_tb;     // t, b0, b1, b2
-    uint2* hit_id;      // instance, primitive (instance = ~0 on a miss)
+    uint2* hit_id;      // instance, leaf record of the hit triangle (instance = ~0 on a miss)
     // routing: shading route per slot, and the slots of every route in slot order
     uint8_t* route;
     uint32_t* route_queue;

@@ -1116,7 +1116,9 @@ __device__ __forceinline__ void trace_finish(const SceneView& s, const Wavefront
         return;
     }
     w.hit_tb[slot] = make_float4(c.t, th.b0, th.b1, th.b2);
-    w.hit_id[slot] = make_uint2(c.instance, c.primitive);
+    // the winner's leaf record (its vertices, and the primitive index in the first record's w):
+    // shading reads the triangle from there, where this trace has just read it
+    w.hit_id[slot] = make_uint2(c.instance, c.leaf);
     w.route[slot] = s.inst_route[c.instance];
 }
 
@@ -1294,7 +1296,7 @@ static __device__ bool resolve_sphere_surface(const SceneView& s, uint32_t inst,
     return lane.err == 0;
 }
 
-static __device__ bool resolve_surface(const SceneView& s, uint32_t inst, uint32_t prim, const float4 tb, F3 hit_position,
+static __device__ bool resolve_surface(const SceneView& s, uint32_t inst, uint32_t leaf, const float4 tb, F3 hit_position,
                                 uint32_t material, Surface& out, Lane& lane) {
     {
         const uint4 geom = s.geom_info[s.inst_info[inst].x];
@@ -1316,10 +1318,13 @@ static __device__ bool resolve_surface(const SceneView& s, uint32_t inst, uint32
     }
     const uint4 info = s.inst_info[inst];
     const uint4 geom = s.geom_info[info.x];
+    // the hit triangle's object-space vertices from its leaf record (copies of the mesh positions)
+    const float4 r0 = s.leaf_tris[3ULL * leaf], r1 = s.leaf_tris[3ULL * leaf + 1], r2 = s.leaf_tris[3ULL * leaf + 2];
+    const uint32_t prim = __float_as_uint(r0.w);
     const uint32_t* tri = s.triangles + 3ULL * (geom.y + prim);
-    const F3 p0 = load_vertex(s.positions, geom.x + tri[0]);
-    const F3 p1 = load_vertex(s.positions, geom.x + tri[1]);
-    const F3 p2 = load_vertex(s.positions, geom.x + tri[2]);
+    const F3 p0{r0.x, r0.y, r0.z};
+    const F3 p1{r1.x, r1.y, r1.z};
+    const F3 p2{r2.x, r2.y, r2.z};
     const F3 n0 = load_vertex(s.normals, geom.x + tri[0]);
     const F3 n1 = load_vertex(s.normals, geom.x + tri[1]);
     const F3 n2 = load_vertex(s.normals, geom.x + tri[2]);
